@@ -1,0 +1,270 @@
+/*
+ * k3dom_b200.h -- C ABI of the B200-native K3DOM / DS-PHD/MIB map-and-track update.
+ *
+ * The library replaces the GPU update of the K3DOM ROS package: the classes
+ * dom::DOM_c (include/common/dom.h:16-148), dom::DOM for K3DOM
+ * (include/k3dom/dom.h:17-30) and dom::DOM for DS-PHD/MIB (include/dsphdmib/dom.h:17-37).
+ * Both variants live behind one handle type here, chosen at creation time.
+ *
+ * Conventions
+ *  - Every call returns a k3dom_status; nothing is printed and nothing traps.
+ *  - A handle is used by one host thread at a time (the caller serialises).
+ *  - `mem` arguments say where a caller buffer lives: K3DOM_MEM_HOST or K3DOM_MEM_DEVICE
+ *    (device memory of the handle's GPU).
+ *  - Particle positions/velocities are in voxel-index units (voxels, voxels/s), exactly as
+ *    in the reference (k3dom_node.cpp:352-357). Points are metres, sensor-centred and
+ *    map-axis aligned (src/k3dom/kernel/mass_update.cu:96-99).
+ *  - Cell index = x + G*y + G*G*z with x fastest (src/common/kernel/predict.cu:52-55).
+ *  - Synchronous calls (k3dom_update_grid, the stage calls, the readbacks) return after the
+ *    GPU work is complete, as DOM::updateGrid does with cudaDeviceSynchronize
+ *    (src/k3dom/dom.cu:47). The *_async forms only enqueue on the handle's stream.
+ */
+#ifndef K3DOM_B200_H
+#define K3DOM_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define K3DOM_B200_ABI_VERSION 1
+
+typedef enum k3dom_status {
+    K3DOM_OK = 0,
+    K3DOM_ERR_INVALID_ARGUMENT = 1, /* bad params, null pointers, size mismatch */
+    K3DOM_ERR_CUDA = 2,             /* a CUDA runtime call failed */
+    K3DOM_ERR_OUT_OF_MEMORY = 3,
+    K3DOM_ERR_CAPACITY = 4,         /* a size exceeds a capacity fixed at creation */
+    K3DOM_ERR_NOT_READY = 5,        /* call order: e.g. stage before first frame */
+    K3DOM_ERR_TIMEOUT = 6,          /* a bounded device wait gave up */
+    K3DOM_ERR_IO = 7,               /* file could not be read */
+    K3DOM_ERR_INVALID_INPUT = 8,    /* non-finite point coordinates */
+    K3DOM_ERR_NO_DEVICE = 9
+} k3dom_status;
+
+typedef enum k3dom_variant {
+    K3DOM_VARIANT_K3DOM = 0,    /* Dirichlet masses + BGKI (src/k3dom) */
+    K3DOM_VARIANT_DSPHDMIB = 1  /* Dempster-Shafer masses + inverse sensor model (src/dsphdmib) */
+} k3dom_variant;
+
+typedef enum k3dom_mem { K3DOM_MEM_HOST = 0, K3DOM_MEM_DEVICE = 1 } k3dom_mem;
+
+/* Mirrors dom::DOM_c::Params (include/common/dom.h:19-52) field for field, in index
+ * units after the node's conversions (k3dom_node.cpp:344-368). The three trailing fields
+ * are additions of this library. */
+typedef struct k3dom_params {
+    float size;
+    float size_z;
+    float mass_scale;
+    float resolution;
+    int32_t particle_count;
+    int32_t new_born_particle_count;
+    float persistence_prob;
+    float stddev_process_noise_position;
+    float stddev_process_noise_velocity;
+    float birth_prob;
+    float stddev_velocity;
+    float init_max_velocity;
+    float particle_min_vel;
+    float sensor_off_x;
+    float sensor_off_y;
+    float sensor_off_z;
+    int32_t map_shift_thresh;
+    float prior_free;
+    float prior_static;
+    float prior_dynamic;
+    float prior_occ;
+    float sigma;           /* K3DOM: sigma_0 of the sparse kernel */
+    float ls;              /* K3DOM: kernel length scale [m] */
+    float gamma;           /* K3DOM: mass decay per second */
+    float max_range;       /* DS-PHD/MIB: inverse sensor model range [m] */
+    float meas_occ_stddev; /* DS-PHD/MIB: occupied evidence stddev [m] */
+    /* additions */
+    uint64_t seed;         /* Philox key of every random draw */
+    int32_t max_points;    /* capacity of points per frame (grows on demand, 0 = 131072) */
+    int32_t reserved;
+} k3dom_params;
+
+typedef struct k3dom_handle k3dom_handle;
+
+/* Node defaults of k3dom_node.cpp:219-258 (K3DOM) or dsphdmib_node.cpp:205-247 (DS),
+ * converted to index units exactly as the node does. */
+k3dom_status k3dom_params_default(k3dom_variant variant, k3dom_params* out);
+
+/* Reads the flat `key: value` YAML subset of config/<method>.yaml and config/<dataset>.yaml
+ * (either path may be NULL), applies them over the node defaults and converts units as
+ * k3dom_node.cpp:344-368 / dsphdmib_node.cpp:330-356 do, quirks included (DS reads
+ * occupied_thresh into valid_thresh; DS max_range fixed at 50). */
+k3dom_status k3dom_params_from_yaml(k3dom_variant variant, const char* method_yaml,
+                                    const char* dataset_yaml, k3dom_params* out);
+
+/* Optional: YAML keys that are node-level, not DOM params (thresholds, publishing). */
+typedef struct k3dom_node_config {
+    float occupied_thresh, valid_thresh, free_thresh, min_z, max_z, min_var, max_var;
+    float ds_resolution, imu_pose_offset;
+    int32_t map_pub_freq, map_vis_mode, do_eval;
+} k3dom_node_config;
+k3dom_status k3dom_node_config_from_yaml(k3dom_variant variant, const char* method_yaml,
+                                         const char* dataset_yaml, k3dom_node_config* out);
+
+/* DOM_c::DOM_c + DOM::DOM (src/common/dom.cu:29-66, src/k3dom/dom.cu:21-23,
+ * src/dsphdmib/dom.cu:21-25). Allocates all device state once on `device`. */
+k3dom_status k3dom_create(const k3dom_params* params, k3dom_variant variant, int device,
+                          k3dom_handle** out);
+k3dom_status k3dom_destroy(k3dom_handle* h);
+
+/* DOM_c::updatePose (src/common/dom.cu:111-158). The map shift runs on the device with no
+ * allocation; the particle part of the shift is folded into the next prediction. */
+k3dom_status k3dom_update_pose(k3dom_handle* h, float x, float y, float z);
+
+/* DOM::updateGrid (src/k3dom/dom.cu:29-50, src/dsphdmib/dom.cu:32-53). xs/ys/zs are n
+ * point coordinates; ys/zs may be NULL when xs holds n interleaved xyz triples. */
+k3dom_status k3dom_update_grid(k3dom_handle* h, float t, const float* xs, const float* ys,
+                               const float* zs, int32_t n, k3dom_mem mem);
+k3dom_status k3dom_update_grid_async(k3dom_handle* h, float t, const float* xs,
+                                     const float* ys, const float* zs, int32_t n,
+                                     k3dom_mem mem);
+k3dom_status k3dom_synchronize(k3dom_handle* h);
+/* The cudaStream_t the handle enqueues on (as void*). */
+k3dom_status k3dom_get_stream(k3dom_handle* h, void** stream);
+/* Capture the steady-state frame in a CUDA graph (default on). */
+k3dom_status k3dom_set_graph_mode(k3dom_handle* h, int enabled);
+
+/* ---- stage calls: the public stage methods of DOM_c / DOM (include/common/dom.h:89-94,
+ * include/k3dom/dom.h:23-29, include/dsphdmib/dom.h:23-32). Each runs the same kernels
+ * as k3dom_update_grid and synchronises. ---- */
+k3dom_status k3dom_particle_prediction(k3dom_handle* h, float dt);
+k3dom_status k3dom_particle_assignment(k3dom_handle* h);
+/* K3DOM: DOM::gridCellOccupancyUpdate(dt, xs, ys, zs); DS: dt is ignored. */
+k3dom_status k3dom_grid_cell_occupancy_update(k3dom_handle* h, float dt, const float* xs,
+                                              const float* ys, const float* zs, int32_t n,
+                                              k3dom_mem mem);
+k3dom_status k3dom_update_persistent_particles(k3dom_handle* h);
+k3dom_status k3dom_initialize_new_particles(k3dom_handle* h);
+/* Per-cell mean velocities are produced inside the occupancy update; this call exists
+ * for call-sequence compatibility and does no GPU work. */
+k3dom_status k3dom_statistical_moments(k3dom_handle* h);
+k3dom_status k3dom_resampling(k3dom_handle* h);
+/* DOM::initializeParticles (first frame, src/k3dom/dom.cu:52-77). */
+k3dom_status k3dom_initialize_particles(k3dom_handle* h, const float* xs, const float* ys,
+                                        const float* zs, int32_t n, k3dom_mem mem);
+/* Copies the resampled set into the persistent set (the deep copy at src/k3dom/dom.cu:43
+ * is a buffer flip here) and advances time like updateGrid's tail. */
+k3dom_status k3dom_finish_frame(k3dom_handle* h, float t);
+
+/* ---- geometry and scalar getters (include/common/dom.h:59-83) ---- */
+typedef struct k3dom_info {
+    int32_t grid_size, grid_size_z, grid_cell_count, particle_count,
+        new_born_particle_count, iteration, variant, initialized;
+    float resolution, center_x, center_y, center_z, sensor_x, sensor_y, sensor_z,
+        updated_time;
+    int32_t max_points, frame_index;
+} k3dom_info;
+k3dom_status k3dom_get_info(k3dom_handle* h, k3dom_info* out);
+k3dom_status k3dom_index_to_coord(k3dom_handle* h, int32_t idx, float* x, float* y,
+                                  float* z);
+
+/* ---- readback (the node's cudaMemcpy of grid_cell_array, k3dom_node.cpp:131-132) ---- */
+typedef enum k3dom_cell_field {
+    K3DOM_CELL_FREE_MASS = 0,
+    K3DOM_CELL_STATIC_MASS = 1,
+    K3DOM_CELL_DYNAMIC_MASS = 2,
+    K3DOM_CELL_OCC_MASS = 3,
+    K3DOM_CELL_PERS_MASS = 4,
+    K3DOM_CELL_PRED_MASS = 5,
+    K3DOM_CELL_BORN_MASS = 6,
+    K3DOM_CELL_MEAN_X_VEL = 7,
+    K3DOM_CELL_MEAN_Y_VEL = 8,
+    K3DOM_CELL_MEAN_Z_VEL = 9,
+    K3DOM_CELL_MU_A = 10,
+    K3DOM_CELL_MU_UA = 11,
+    K3DOM_CELL_W_A = 12,
+    K3DOM_CELL_W_UA = 13,
+    K3DOM_CELL_LIKELIHOOD = 14,
+    K3DOM_CELL_P_A = 15,
+    K3DOM_CELL_OCC_MEAN = 16,   /* GridCell::occ_mean (dom_types.h:48) */
+    K3DOM_CELL_DYN_MEAN = 17,   /* GridCell::dyn_mean (dom_types.h:49) */
+    K3DOM_CELL_TOTAL_MASS = 18, /* GridCell::total_mass (dom_types.h:47) */
+    K3DOM_CELL_OCC_PROB = 19,   /* GridCell::occ_prob (dom_types.h:61) */
+    K3DOM_CELL_VAR = 20,        /* GridCell::calcVar (dom_types.h:50-58) */
+    K3DOM_CELL_MEAS_OCC = 21,   /* DS: MeasurementCell::occ_mass */
+    K3DOM_CELL_MEAS_FREE = 22,  /* DS: MeasurementCell::free_mass */
+    K3DOM_CELL_DEL_OCC = 23,    /* K3DOM: last BGKI occupied evidence */
+    K3DOM_CELL_DEL_FREE = 24,   /* K3DOM: last BGKI free evidence */
+    K3DOM_CELL_FIELD_COUNT = 25
+} k3dom_cell_field;
+k3dom_status k3dom_get_cell_field(k3dom_handle* h, k3dom_cell_field field, float* dst,
+                                  k3dom_mem mem);
+/* start_idx / end_idx per cell (-1 when empty), as particleToGridKernel leaves them. */
+k3dom_status k3dom_get_cell_ranges(k3dom_handle* h, int32_t* start, int32_t* end,
+                                   k3dom_mem mem);
+/* The reference's 68-byte dom::GridCell array (include/common/dom_types.h:12-65). */
+#define K3DOM_GRIDCELL_BYTES 68
+k3dom_status k3dom_get_gridcell_aos(k3dom_handle* h, void* dst, k3dom_mem mem);
+/* The /map_data evaluation cloud of k3dom_node.cpp:161-184: per cell 10 floats
+ * x, y, z, v_x, v_y, v_z (m/s), occ_val, dyn_val, eval_aug, dyn_aug (MapPoint,
+ * include/common/mappoint.h:5-28, without PCL's padding). */
+#define K3DOM_MAPPOINT_FLOATS 10
+k3dom_status k3dom_get_mappoints(k3dom_handle* h, float* dst, k3dom_mem mem);
+
+/* Overwrites cell state (masses) -- checkpoint restore and parity tests. Any pointer may
+ * be NULL to leave that field alone. */
+k3dom_status k3dom_set_cell_masses(k3dom_handle* h, const float* free_mass,
+                                   const float* static_mass, const float* dynamic_mass,
+                                   const float* occ_mass, k3dom_mem mem);
+
+/* ---- particles (ParticlesSoA, include/common/dom_types.h:76-167) ---- */
+typedef enum k3dom_particle_set {
+    K3DOM_PARTICLES_PERSISTENT = 0, /* particle_array (current) */
+    K3DOM_PARTICLES_SORTED = 1,     /* particle_array after assignment (sorted by cell) */
+    K3DOM_PARTICLES_BIRTH = 2       /* birth_particle_array */
+} k3dom_particle_set;
+/* Any output may be NULL. pos/vel are n*3 interleaved floats. */
+k3dom_status k3dom_get_particles(k3dom_handle* h, k3dom_particle_set set, float* pos,
+                                 float* vel, float* weight, int32_t* cell_idx,
+                                 uint8_t* associated, k3dom_mem mem);
+k3dom_status k3dom_set_particles(k3dom_handle* h, k3dom_particle_set set, const float* pos,
+                                 const float* vel, const float* weight,
+                                 const int32_t* cell_idx, const uint8_t* associated,
+                                 k3dom_mem mem);
+/* Debug / parity hooks. */
+/* The permutation of the last assignment: sorted slot i holds the particle that was at
+ * index perm[i] before the sort. */
+k3dom_status k3dom_get_sort_permutation(k3dom_handle* h, int32_t* perm, k3dom_mem mem);
+/* Ancestor index of every resampled particle (0..P+B-1; >= P means birth slot - P). */
+k3dom_status k3dom_get_ancestors(k3dom_handle* h, int32_t* anc, k3dom_mem mem);
+/* Joint cumulative weights (P+B floats), born-mass cumulative (C floats), joint max. */
+k3dom_status k3dom_get_resampling_state(k3dom_handle* h, float* joint_cum,
+                                        float* born_cum, float* joint_max, k3dom_mem mem);
+/* The draws the library uses: stage 1 = prediction normals (6 per item), 2 = first-frame
+ * velocities (3 uniforms, (0,1]), 3 = birth velocities (3 uniforms), 4 = resampling (1
+ * uniform). Writes count*per_item floats for items [first, first+count) of frame `frame`. */
+k3dom_status k3dom_debug_draws(uint64_t seed, int32_t frame, int32_t stage, int64_t first,
+                               int64_t count, float* dst, k3dom_mem mem);
+/* Sets the frame counter used to key the draws (tests align it with a reference run). */
+k3dom_status k3dom_set_frame_index(k3dom_handle* h, int32_t frame);
+
+/* Per-stage device time of the last frame in milliseconds (CUDA events). */
+typedef struct k3dom_stage_times {
+    float predict_ms, assign_ms, occupancy_ms, persistent_ms, births_ms, resample_ms,
+        total_ms;
+} k3dom_stage_times;
+k3dom_status k3dom_get_stage_times(k3dom_handle* h, k3dom_stage_times* out);
+k3dom_status k3dom_set_timing(k3dom_handle* h, int enabled);
+
+/* Diagnostics collected on the device: points skipped as non-finite, list overflow. */
+typedef struct k3dom_diagnostics {
+    int64_t nonfinite_points, ray_list_entries, ray_list_capacity, work_items;
+    int32_t overflow;
+} k3dom_diagnostics;
+k3dom_status k3dom_get_diagnostics(k3dom_handle* h, k3dom_diagnostics* out);
+
+const char* k3dom_status_string(k3dom_status s);
+int32_t k3dom_abi_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* K3DOM_B200_H */

@@ -1,0 +1,1019 @@
+// evidence.cu -- measurement evidence and the per-cell mass update.
+//
+// K3DOM: Bayesian kernel inference (BGKI, src/k3dom/kernel/mass_update.cu:32-77) followed by
+// predict_mass / update_mass / separate_newborn_part (:79-150), with the per-cell parts of
+// updatePersistentParticlesKernel2 (update_persistent_particles.cu:28-44) and
+// statisticalMomentsKernel2 (statistical_moments.cu:36-63) fused into the same pass.
+// DS-PHD/MIB: calcMeasurementGridKernel (src/dsphdmib/kernel/measurement_grid.cu:64-162)
+// followed by gridCellPredictionUpdateKernel (src/dsphdmib/kernel/mass_update.cu:46-87).
+//
+// The reference evaluates every (cell, point) pair: C x N (2.5e11 at 2.1M cells / 120k
+// points). Both evidence models have compact support -- the sparse kernel is zero beyond
+// ls, the DS window is 0.866 res wide -- so each ray is binned to the tiles of cells its
+// support can reach (segment sensor->point with radius ls for K3DOM, the half-line through
+// the point with the window radius for DS). A tile's list keeps rays in input order (stable
+// sort by tile). One CTA takes one (tile, chunk of <= kChunk rays) work item from a device
+// work counter: it stages the chunk's ray data in shared memory; each warp owns 4x4x2-cell
+// sub-blocks and culls 32 rays at a time with one ballot; every lane then evaluates the
+// surviving rays for its own cell. K3DOM evidence is accumulated in FP64 registers; chunks of
+// one tile are combined through 64-bit fixed-point atomics (integer addition is associative,
+// so the result does not depend on the order in which chunks finish) and the last chunk to
+// finish runs the cell update. No block ever waits on another.
+#include <cuda_runtime.h>
+#include <math.h>
+
+#include <algorithm>
+#include <cstddef>
+
+#include "common.cuh"
+#include "internal.h"
+#include "scan.cuh"
+
+namespace k3dom {
+
+constexpr int kChunk = 1024;
+constexpr int kEvThreads = 256;
+constexpr int kEvWarps = kEvThreads / 32;
+constexpr int kDsMaxNeighbors = 100;  // measurement_grid.cu:87
+
+// ================================================================ binning
+struct BinGeom {
+    float ax, ay, az;  // sensor in cell-index space (cell centre ix sits at u = ix)
+    float R;           // support radius in cells
+    int G, Gz, tx, ty, tz, ntx, nty, ntz;
+};
+
+__device__ __forceinline__ bool seg_box(const float a[3], const float d[3], const float l[3], const float h[3],
+                                        float t0, float t1) {
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        if (d[k] == 0.0f) {
+            if (a[k] < l[k] || a[k] > h[k]) return false;
+        } else {
+            const float inv = 1.0f / d[k];
+            const float e0 = (l[k] - a[k]) * inv, e1 = (h[k] - a[k]) * inv;
+            t0 = fmaxf(t0, fminf(e0, e1));
+            t1 = fminf(t1, fmaxf(e0, e1));
+        }
+    }
+    return t0 <= t1;
+}
+
+// Visit every tile whose cell-centre box, grown by R, meets the segment a -> b.
+template <typename F>
+__device__ __forceinline__ void for_each_tile(const BinGeom& g, float bx, float by, float bz, F f) {
+    const float a[3] = {g.ax, g.ay, g.az};
+    const float d[3] = {bx - g.ax, by - g.ay, bz - g.az};
+    const float glo[3] = {-g.R, -g.R, -g.R};
+    const float ghi[3] = {(float)(g.G - 1) + g.R, (float)(g.G - 1) + g.R, (float)(g.Gz - 1) + g.R};
+    float t0 = 0.0f, t1 = 1.0f;
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        if (d[k] == 0.0f) {
+            if (a[k] < glo[k] || a[k] > ghi[k]) return;
+        } else {
+            const float inv = 1.0f / d[k];
+            const float e0 = (glo[k] - a[k]) * inv, e1 = (ghi[k] - a[k]) * inv;
+            t0 = fmaxf(t0, fminf(e0, e1));
+            t1 = fminf(t1, fmaxf(e0, e1));
+        }
+    }
+    if (t0 > t1) return;
+    int A = 0;
+    if (fabsf(d[1]) > fabsf(d[A])) A = 1;
+    if (fabsf(d[2]) > fabsf(d[A])) A = 2;
+    const int Bx = (A + 1) % 3, Cx = (A + 2) % 3;
+    const int ts[3] = {g.tx, g.ty, g.tz}, nt[3] = {g.ntx, g.nty, g.ntz};
+    const float pa0 = a[A] + d[A] * t0, pa1 = a[A] + d[A] * t1;
+    int ta0 = (int)floorf((fminf(pa0, pa1) - g.R) / (float)ts[A]);
+    int ta1 = (int)floorf((fmaxf(pa0, pa1) + g.R) / (float)ts[A]);
+    ta0 = max(ta0, 0);
+    ta1 = min(ta1, nt[A] - 1);
+    for (int ta = ta0; ta <= ta1; ++ta) {
+        const float slo = (float)(ta * ts[A]) - g.R, shi = (float)(ta * ts[A] + ts[A] - 1) + g.R;
+        float s0 = t0, s1 = t1;
+        if (d[A] != 0.0f) {
+            const float inv = 1.0f / d[A];
+            const float e0 = (slo - a[A]) * inv, e1 = (shi - a[A]) * inv;
+            s0 = fmaxf(s0, fminf(e0, e1));
+            s1 = fminf(s1, fmaxf(e0, e1));
+        } else if (a[A] < slo || a[A] > shi) {
+            continue;
+        }
+        if (s0 > s1) continue;
+        const float b0 = a[Bx] + d[Bx] * s0, b1 = a[Bx] + d[Bx] * s1;
+        const float c0 = a[Cx] + d[Cx] * s0, c1 = a[Cx] + d[Cx] * s1;
+        int tb0 = max((int)floorf((fminf(b0, b1) - g.R) / (float)ts[Bx]), 0);
+        int tb1 = min((int)floorf((fmaxf(b0, b1) + g.R) / (float)ts[Bx]), nt[Bx] - 1);
+        int tc0 = max((int)floorf((fminf(c0, c1) - g.R) / (float)ts[Cx]), 0);
+        int tc1 = min((int)floorf((fmaxf(c0, c1) + g.R) / (float)ts[Cx]), nt[Cx] - 1);
+        for (int tb = tb0; tb <= tb1; ++tb) {
+            for (int tc = tc0; tc <= tc1; ++tc) {
+                int t3[3];
+                t3[A] = ta;
+                t3[Bx] = tb;
+                t3[Cx] = tc;
+                float l[3], h[3];
+#pragma unroll
+                for (int k = 0; k < 3; ++k) {
+                    l[k] = (float)(t3[k] * ts[k]) - g.R;
+                    h[k] = (float)(t3[k] * ts[k] + ts[k] - 1) + g.R;
+                }
+                if (seg_box(a, d, l, h, t0, t1)) f(t3[0] + g.ntx * (t3[1] + g.nty * t3[2]));
+            }
+        }
+    }
+}
+
+// The sensor's place in cell-index space comes from the frame scalars in device memory, so a
+// captured graph stays valid while the sensor moves.
+__device__ __forceinline__ void place_sensor(BinGeom& g, const DevParams& p, const FrameParams& f) {
+    const float hg = (float)p.G / 2.0f, hz = (float)p.Gz / 2.0f;
+    // a point q (metres, sensor frame) sits at u = (q + s)/res + G/2 - 0.5
+    g.ax = f.sensor_x / p.res + hg - 0.5f;
+    g.ay = f.sensor_y / p.res + hg - 0.5f;
+    g.az = f.sensor_z / p.res + hz - 0.5f;
+}
+
+struct RayPrep {
+    bool ok;
+    float bx, by, bz;  // far end of the binned segment (cell-index space)
+};
+
+// Per-ray constants. K3DOM: (m, d_m) and (m/d_m, margin), d_m and margin as the reference
+// forms them (mass_update.cu:29-31,55). DS: (m, |m|^2) as measurement_grid.cu:90.
+__device__ __forceinline__ RayPrep prep_ray(const DevParams& p, const BinGeom& g, float mx, float my, float mz,
+                                           bool ds, float4* ra, float4* rb, double4* rc) {
+    RayPrep r;
+    r.ok = isfinite(mx) && isfinite(my) && isfinite(mz);
+    r.bx = r.by = r.bz = 0.0f;
+    *ra = make_float4(0.f, 0.f, 0.f, 0.f);
+    *rb = make_float4(0.f, 0.f, 0.f, 0.f);
+    *rc = make_double4(0.0, 0.0, 0.0, 0.0);
+    if (!r.ok) return r;
+    const float sq = __fadd_rn(__fadd_rn(__fmul_rn(mx, mx), __fmul_rn(my, my)), __fmul_rn(mz, mz));
+    if (!ds) {
+        // d_m and the margin point (mass_update.cu:29-31,55) in FP64; a zero-length ray gets
+        // 1/d_m = 0, which turns its free evidence off as the reference's NaN comparisons do
+        const double dmd = sqrt((double)mx * mx + (double)my * my + (double)mz * mz);
+        const double margd = fmax(0.9 * dmd, dmd - 2.0 * (double)p.res);
+        const double inv = dmd > 0.0 ? 1.0 / dmd : 0.0;
+        const float dm = (float)dmd;
+        *ra = make_float4(mx, my, mz, dm);
+        *rb = make_float4((float)(mx * inv), (float)(my * inv), (float)(mz * inv), (float)margd);
+        *rc = make_double4(dmd, margd, inv, 0.0);
+        r.bx = g.ax + mx / p.res;
+        r.by = g.ay + my / p.res;
+        r.bz = g.az + mz / p.res;
+    } else {
+        *ra = make_float4(mx, my, mz, sq);
+        const float len = sqrtf(sq);
+        if (!(len > 0.0f)) {
+            r.ok = false;  // |m| = 0: inner product 0, never a neighbour (measurement_grid.cu:92)
+            return r;
+        }
+        const float L = sqrtf((float)(2 * g.G * g.G + g.Gz * g.Gz)) + 2.0f * g.R + 4.0f;  // cells
+        const float sc = L / (len / p.res);
+        r.bx = g.ax + mx / p.res * sc;
+        r.by = g.ay + my / p.res * sc;
+        r.bz = g.az + mz / p.res * sc;
+    }
+    return r;
+}
+
+__global__ void k_ray_count(DevParams p, const FrameParams* __restrict__ fpp, BinGeom g,
+                            const float* __restrict__ xs, const float* __restrict__ ys,
+                            const float* __restrict__ zs, int ds, float4* __restrict__ ra,
+                            float4* __restrict__ rb, double4* __restrict__ rc, uint32_t* __restrict__ counts,
+                            DevStatus* status) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const FrameParams f = *fpp;
+    const int n = f.n_points;
+    if (i >= n) return;
+    place_sensor(g, p, f);
+    const float mx = xs[i], my = ys[i], mz = zs[i];
+    float4 a, b;
+    double4 cc;
+    const RayPrep r = prep_ray(p, g, mx, my, mz, ds != 0, &a, &b, &cc);
+    ra[i] = a;
+    rb[i] = b;
+    rc[i] = cc;
+    uint32_t c = 0;
+    if (r.ok) {
+        for_each_tile(g, r.bx, r.by, r.bz, [&](int) { ++c; });
+    } else if (!(isfinite(mx) && isfinite(my) && isfinite(mz))) {
+        atomicAdd(&status->nonfinite_points, 1ull);
+    }
+    counts[i] = c;
+}
+
+__global__ void k_ray_emit(DevParams p, const FrameParams* __restrict__ fpp, BinGeom g,
+                           const float* __restrict__ xs, const float* __restrict__ ys,
+                           const float* __restrict__ zs, int ds, const uint32_t* __restrict__ offsets,
+                           uint32_t* __restrict__ total, long capacity, uint32_t* __restrict__ ekeys,
+                           uint32_t* __restrict__ evals, DevStatus* status) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const FrameParams f = *fpp;
+    const int n = f.n_points;
+    place_sensor(g, p, f);
+    const bool over = (long)total[0] > capacity;
+    if (i == 0) {
+        total[2] = over ? 0u : total[0];  // live entry count for the sort
+        if (over) atomicOr(&status->overflow, 1u);
+    }
+    if (i >= n || over) return;
+    const float mx = xs[i], my = ys[i], mz = zs[i];
+    float4 a, b;
+    double4 c;
+    const RayPrep r = prep_ray(p, g, mx, my, mz, ds != 0, &a, &b, &c);
+    if (!r.ok) return;
+    // never write more entries than were counted: the count pass sized this ray's range
+    const uint32_t o0 = offsets[i];
+    const uint32_t cnt = (i + 1 < n) ? offsets[i + 1] - o0 : total[0] - o0;
+    uint32_t o = o0;
+    for_each_tile(g, r.bx, r.by, r.bz, [&](int t) {
+        if (o - o0 < cnt) {
+            ekeys[o] = (uint32_t)t;
+            evals[o] = (uint32_t)i;
+            ++o;
+        }
+    });
+    for (; o - o0 < cnt; ++o) {  // pad with a key past the last tile (sorted last, ignored)
+        ekeys[o] = (uint32_t)g.ntx * g.nty * g.ntz;
+        evals[o] = (uint32_t)i;
+    }
+}
+
+// tile_start[t] = first sorted entry of tile t, for t in [0, T].
+__global__ void k_tile_start(const uint32_t* __restrict__ skeys, const uint32_t* __restrict__ total, int T,
+                             uint32_t* __restrict__ tile_start) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t > T) return;
+    const long n = (long)total[2];
+    long lo = 0, hi = n;
+    while (lo < hi) {
+        const long mid = (lo + hi) >> 1;
+        if (skeys[mid] < (uint32_t)t) lo = mid + 1; else hi = mid;
+    }
+    tile_start[t] = (uint32_t)lo;
+}
+
+__global__ void k_tile_items(const uint32_t* __restrict__ tile_start, int T, uint32_t* __restrict__ items) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= T) return;
+    const uint32_t len = tile_start[t + 1] - tile_start[t];
+    items[t] = len == 0 ? 1u : (len + kChunk - 1) / kChunk;
+}
+
+__global__ void k_finish_lists(const uint32_t* __restrict__ item_off, int T, DevStatus* status,
+                               const uint32_t* __restrict__ total) {
+    status->work_items = item_off[T];
+    status->ray_entries = total[0];
+    status->work_counter = 0;
+    status->work_counter2 = 0;
+}
+
+// Largest |c| of a cell centre seen from a sensor inside or near the grid [m].
+static float max_extent(const DevParams& p) { return 2.0f * ((float)p.G * p.res * 1.7320508f + p.size_z); }
+
+static BinGeom make_bingeom(const DevParams& p, const RayBuffers& rb, bool ds) {
+    BinGeom g;
+    g.ax = g.ay = g.az = 0.0f;  // placed on the device from the frame scalars
+    if (!ds) {
+        g.R = p.ls / p.res * (1.0f + 1e-4f) + 1e-3f;
+    } else {
+        // window radius plus the FP32 rounding slack of |c|^2 - (c.m)^2/|m|^2
+        const float ext = max_extent(p);
+        const float slack = 64.0f * 5.96e-8f * ext * ext;
+        g.R = sqrtf(p.window_radius * p.window_radius + slack) / p.res + 1e-3f;
+    }
+    g.G = p.G;
+    g.Gz = p.Gz;
+    g.tx = rb.tx; g.ty = rb.ty; g.tz = rb.tz;
+    g.ntx = rb.ntx; g.nty = rb.nty; g.ntz = rb.ntz;
+    return g;
+}
+
+long ray_entries_bound(const DevParams& p, const EvidenceConfig& ec, int max_points) {
+    const int ntx = (p.G + ec.tile_x - 1) / ec.tile_x, nty = (p.G + ec.tile_y - 1) / ec.tile_y,
+              ntz = (p.Gz + ec.tile_z - 1) / ec.tile_z;
+    const double R = std::max((double)p.ls, (double)p.window_radius * 1.5 + 0.05) / p.res + 2.0;
+    const int ts[3] = {ec.tile_x, ec.tile_y, ec.tile_z}, nt[3] = {ntx, nty, ntz};
+    long worst = 0;
+    for (int A = 0; A < 3; ++A) {
+        long per_slab = 1;
+        for (int k = 1; k <= 2; ++k) {
+            const int o = (A + k) % 3;
+            const long n = (long)std::ceil((ts[A] + 4.0 * R + 2.0) / ts[o]) + 2;
+            per_slab *= std::min<long>(n, nt[o]);
+        }
+        worst = std::max(worst, per_slab * nt[A]);
+    }
+    worst = std::min<long>(worst, (long)ntx * nty * ntz);
+    return worst * (long)max_points;
+}
+
+cudaError_t build_ray_lists(const DevParams& p, const FrameParams* fp, const float* xs, const float* ys,
+                            const float* zs, RayBuffers& rb, bool ds, DevStatus* status, cudaStream_t st) {
+    const BinGeom g = make_bingeom(p, rb, ds);
+    const int nmax = rb.max_points;
+    const int T = rb.tiles;
+    const uint32_t* dn_points =
+        reinterpret_cast<const uint32_t*>(reinterpret_cast<const char*>(fp) + offsetof(FrameParams, n_points));
+    k_ray_count<<<div_up(nmax, kBlock), kBlock, 0, st>>>(p, fp, g, xs, ys, zs, ds ? 1 : 0, rb.ray_a, rb.ray_b,
+                                                         rb.ray_c, rb.counts, status);
+    cudaError_t e = scan_u32_exclusive_dn(rb.counts, rb.offsets, nmax, dn_points, rb.scan_tmp, rb.total, st);
+    if (e != cudaSuccess) return e;
+    k_ray_emit<<<div_up(nmax, kBlock), kBlock, 0, st>>>(p, fp, g, xs, ys, zs, ds ? 1 : 0, rb.offsets, rb.total,
+                                                        rb.capacity, rb.ekeys, rb.evals, status);
+    int bits = 1;
+    while ((1 << bits) < T + 1) ++bits;
+    e = radix_sort_pairs_dn(rb.ekeys, rb.evals, rb.ekeys2, rb.evals2, rb.ekeys_alt, rb.evals_alt, rb.capacity,
+                            rb.total + 2, bits, rb.hist, rb.scan_tmp, st);
+    if (e != cudaSuccess) return e;
+    k_tile_start<<<div_up(T + 1, kBlock), kBlock, 0, st>>>(rb.ekeys2, rb.total, T, rb.tile_start);
+    k_tile_items<<<div_up(T, kBlock), kBlock, 0, st>>>(rb.tile_start, T, rb.tile_items);
+    e = scan_u32_exclusive(rb.tile_items, rb.item_off, T, rb.scan_tmp, rb.item_off + T, st);
+    if (e != cudaSuccess) return e;
+    k_finish_lists<<<1, 1, 0, st>>>(rb.item_off, T, status, rb.total);
+    return cudaGetLastError();
+}
+
+// ================================================================ shared kernel machinery
+struct TileShape {
+    int tx, ty, tz, ntx, nty, nsbx, nsby;
+};
+
+__device__ __forceinline__ int find_tile(const uint32_t* __restrict__ item_off, int T, uint32_t item) {
+    // last t with item_off[t] <= item
+    int lo = 0, hi = T;  // answer in [0, T)
+    while (hi - lo > 1) {
+        const int mid = (lo + hi) >> 1;
+        if (item_off[mid] <= item) lo = mid; else hi = mid;
+    }
+    return lo;
+}
+
+struct CellLoc {
+    int c;          // cell index, -1 when outside the grid
+    int local;      // cell index within the tile
+    float x, y, z;  // cell centre relative to the sensor [m], reference FP32 operation order
+    float ox, oy, oz;  // anchor: centre of the sub-block's cell (2, 2, 1), same formula
+};
+
+// Cell centre of index triple (ix, iy, iz), the expression of mass_update.cu:92-99 /
+// measurement_grid.cu:77-84 evaluated in FP32 in the reference's order.
+__device__ __forceinline__ void centre_xyz(int ix, int iy, int iz, const DevParams& p, float sx, float sy, float sz,
+                                           float* x, float* y, float* z) {
+    const float hg = __fdiv_rn((float)p.G, 2.0f), hz = __fdiv_rn((float)p.Gz, 2.0f);
+    *x = __fsub_rn(__fmul_rn(__fsub_rn(__fadd_rn((float)ix, 0.5f), hg), p.res), sx);
+    *y = __fsub_rn(__fmul_rn(__fsub_rn(__fadd_rn((float)iy, 0.5f), hg), p.res), sy);
+    *z = __fsub_rn(__fmul_rn(__fsub_rn(__fadd_rn((float)iz, 0.5f), hz), p.res), sz);
+}
+
+__device__ __forceinline__ CellLoc locate(const DevParams& p, const TileShape& ts, int t, int sb, int lane,
+                                          float sx, float sy, float sz) {
+    const int tx = t % ts.ntx, ty = (t / ts.ntx) % ts.nty, tz = t / (ts.ntx * ts.nty);
+    const int sbx = sb % ts.nsbx, sby = (sb / ts.nsbx) % ts.nsby, sbz = sb / (ts.nsbx * ts.nsby);
+    const int lx = sbx * 4 + (lane & 3), ly = sby * 4 + ((lane >> 2) & 3), lz = sbz * 2 + (lane >> 4);
+    const int ix = tx * ts.tx + lx, iy = ty * ts.ty + ly, iz = tz * ts.tz + lz;
+    CellLoc L;
+    L.local = lx + ts.tx * (ly + ts.ty * lz);
+    const bool in = ix < p.G && iy < p.G && iz < p.Gz;
+    L.c = in ? ix + p.G * iy + p.G * p.G * iz : -1;
+    centre_xyz(ix, iy, iz, p, sx, sy, sz, &L.x, &L.y, &L.z);
+    centre_xyz(tx * ts.tx + sbx * 4 + 2, ty * ts.ty + sby * 4 + 2, tz * ts.tz + sbz * 2 + 1, p, sx, sy, sz, &L.ox,
+               &L.oy, &L.oz);
+    return L;
+}
+
+// ================================================================ K3DOM
+__device__ __forceinline__ float kernel_func(float d, float inv_ls, float sigma) {
+    // mass_update.cu:24-26 (note the reference's 3.141592 in the sine term)
+    const float x = d * inv_ls;
+    float s, c;
+    sincospif(2.0f * x, &s, &c);
+    const float v = sigma * ((2.0f + c) * (1.0f - x) * (1.0f / 3.0f) + s * (1.0f / (2.0f * 3.141592f)));
+    return fmaxf(0.0f, v);
+}
+
+__device__ __forceinline__ float calc_credit(float mass, float mass_scale) {
+    // mass_update.cu:12-14
+    return 1.0f - 2.0f / (1.0f + expf(2.0f * mass / mass_scale));
+}
+__device__ __forceinline__ float positive_diff(float a, float b) { return fmaxf(0.0f, a - b); }
+__device__ __forceinline__ float calc_ratio(float numerator, float rest) {
+    return (numerator <= 0.0f || rest < 0.0f) ? 0.0f : (1.0f / (1.0f + rest / numerator));
+}
+__device__ __forceinline__ float calc_norm(float weight_sum, float rho_p) {
+    return weight_sum > 0.0f ? rho_p / weight_sum : 0.0f;
+}
+
+// gridCellPredictionUpdateKernel's per-cell body (mass_update.cu:163-181) plus the per-cell
+// updates of the persistent-particle and moment stages.
+__device__ void k3dom_cell_update(const DevParams& p, float dt, int c, float del_occ, float del_free,
+                                  CellState cs, CellWork cw, bool first_frame) {
+    float m_f = cs.free_m[c], m_s = cs.static_m[c], m_d = cs.dyn_m[c];
+    const int start = first_frame ? -1 : cw.start[c];
+    const bool has = start >= 0;
+    const float dyn_pred = has ? cw.sum_w[c] : 0.0f;
+    const float g = powf(p.gamma, dt);
+    const float pred_total = (m_f + m_d) * g;
+    // predict_mass (:79-84)
+    m_s *= g;
+    m_d = fminf(dyn_pred, fmaxf(0.0f, pred_total - m_s));
+    m_f = pred_total - m_d;
+    // update_mass (:86-139)
+    if (del_free > 0.0f || del_occ > 0.0f) {
+        const float del_sigma = del_free + del_occ;
+        const float prime_sigma = m_f + m_s + m_d;
+        float l_DtoF = 0.0f, l_StoFD = 0.0f, l_FtoD = 0.0f;
+        if (prime_sigma > 0.0f) {
+            const float credit = calc_credit(sqrtf(del_sigma * prime_sigma), p.mass_scale);
+            const float base_f = credit * positive_diff(del_free, del_occ) / del_sigma;
+            const float base_o = credit * positive_diff(del_occ, del_free) / del_sigma;
+            l_DtoF = base_f * m_d / prime_sigma;
+            l_StoFD = base_f * positive_diff(m_s + m_d, m_f) / prime_sigma;
+            l_FtoD = base_o * positive_diff(m_f, m_s + m_d) / prime_sigma;
+        }
+        const float diff_f = l_StoFD / 2.0f * m_s + l_DtoF * m_d - l_FtoD * m_f;
+        const float diff_s = -l_StoFD * m_s;
+        const float diff_d = l_FtoD * m_f + l_StoFD / 2.0f * m_s - l_DtoF * m_d;
+        m_f += diff_f;
+        m_s += diff_s;
+        m_d += diff_d;
+        const float credit2 = calc_credit(m_s + m_d, p.mass_scale);
+        const float beta = (1.0f - credit2) + credit2 * calc_ratio(m_s, m_d);
+        m_s = m_s + beta * del_occ;
+        m_d = m_d + (1.0f - beta) * del_occ;
+        m_f = m_f + del_free;
+    }
+    // separate_newborn_part (:141-150)
+    float born;
+    if (dyn_pred <= 0.0f) born = m_d;
+    else if (pred_total <= dyn_pred) born = 0.0f;
+    else born = (m_d * p.p_B * (pred_total - dyn_pred)) / (dyn_pred + p.p_B * (pred_total - dyn_pred));
+    const float pers = m_d - born;
+    cs.free_m[c] = m_f;
+    cs.static_m[c] = m_s;
+    cs.dyn_m[c] = m_d;
+    cs.born_m[c] = born;
+    cs.pers_m[c] = pers;
+    cs.pred_m[c] = dyn_pred;
+    cw.del_occ[c] = del_occ;
+    cw.del_free[c] = del_free;
+    if (first_frame) return;
+    // updatePersistentParticlesKernel2: mu_UA = pers / pred (p_A = 0 -> the only factor)
+    const float mu_UA = has ? calc_norm(dyn_pred, pers) : 0.0f;
+    cw.factor[c] = mu_UA;
+    // statisticalMomentsKernel2 with sum(w' v) = mu_UA * sum(w v)
+    float vx = 0.0f, vy = 0.0f, vz = 0.0f;
+    if (has && pers > 0.0f) {
+        vx = (mu_UA * cw.sum_wvx[c]) / pers;
+        vy = (mu_UA * cw.sum_wvy[c]) / pers;
+        vz = (mu_UA * cw.sum_wvz[c]) / pers;
+    }
+    cs.mvx[c] = vx;
+    cs.mvy[c] = vy;
+    cs.mvz[c] = vz;
+}
+
+struct EvArgs {
+    DevParams p;
+    const FrameParams* fp;
+    TileShape ts;
+    int T;
+    const uint32_t* item_off;
+    const uint32_t* tile_start;
+    const uint32_t* evals;
+    const float4* ray_a;
+    const float4* ray_b;
+    const double4* ray_c;
+    uint32_t* tile_done;
+    unsigned long long* acc;
+    uint8_t* ds_counts;
+    long ds_count_capacity;
+    CellState cs;
+    CellWork cw;
+    DevStatus* status;
+    int first_frame;
+    double fx_scale, fx_inv;  // fixed-point scale of the K3DOM evidence
+    float wr2;                // DS window radius squared
+    float cull_r2;            // squared cull radius around a sub-block anchor [m^2]
+};
+
+// Shared memory of k_bgki: one chunk of rays plus a per-warp staging area for the FP64
+// (sub-block, ray) constants.
+struct BgkiSmem {
+    float4 a[kChunk];            // m
+    float4 u[kChunk];            // unit direction (FP32)
+    double4 c[kChunk];           // d_m, margin, 1/d_m
+    float4 stage[kEvWarps][32][3];
+};
+
+// Pair geometry. For the anchor o of a sub-block and a ray m (FP64, once per lane-ray):
+//   par0 = o.u, perp0 = o - par0 u, occ0 = o - m, and par0 - margin, par0 - d_m.
+// For a cell c = o + delta (delta small and exact), with dpar = delta.u:
+//   projection d_proj = par0 + dpar; perpendicular offset perp0 + delta - dpar u;
+//   distance to the free segment [0, margin u] (the three branches of mass_update.cu:57-65)
+//   = |perp|^2 + (min(d_proj, 0) + max(d_proj - margin, 0))^2, valid while d_proj < d_m;
+//   distance to the point = |occ0 + delta|.
+// Every FP32 quantity is O(ls), so the FP32 evaluation keeps ~1e-7 relative accuracy at any
+// distance from the sensor (the direct |c|^2 - d_proj^2 form of :60 loses ~1e-5 at 20 m).
+template <int NSBW>
+__global__ void __launch_bounds__(kEvThreads) k_bgki(EvArgs A) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    BgkiSmem& S = *reinterpret_cast<BgkiSmem*>(smem_raw);
+    __shared__ uint32_t s_item;
+    __shared__ int s_last;
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    const DevParams& p = A.p;
+    const FrameParams fp = *A.fp;
+    const uint32_t total_items = A.item_off[A.T];
+    const float ls2 = p.ls * p.ls;
+    const float inv_ls = 1.0f / p.ls;
+    const int n_points = fp.n_points;
+
+    for (;;) {
+        if (threadIdx.x == 0) s_item = atomicAdd(&A.status->work_counter, 1u);
+        __syncthreads();
+        const uint32_t item = s_item;
+        __syncthreads();
+        if (item >= total_items) break;
+        const int t = find_tile(A.item_off, A.T, item);
+        const uint32_t k = item - A.item_off[t];
+        const uint32_t n_items = A.item_off[t + 1] - A.item_off[t];
+        const uint32_t e0 = A.tile_start[t] + k * kChunk;
+        const uint32_t e1 = min(A.tile_start[t + 1], e0 + (uint32_t)kChunk);
+        const int nr = (int)(e1 > e0 ? e1 - e0 : 0);
+        for (int r = threadIdx.x; r < nr; r += kEvThreads) {
+            uint32_t rid = A.evals[e0 + r];
+            if (rid >= (uint32_t)n_points) rid = 0;  // defensive: never read past the ray arrays
+            S.a[r] = A.ray_a[rid];
+            S.u[r] = A.ray_b[rid];
+            S.c[r] = A.ray_c[rid];
+        }
+        __syncthreads();
+        double acc_o[NSBW], acc_f[NSBW];
+        int cell[NSBW];
+#pragma unroll
+        for (int q = 0; q < NSBW; ++q) {
+            const int sbi = wid + q * kEvWarps;
+            const CellLoc L = locate(p, A.ts, t, sbi, lane, fp.sensor_x, fp.sensor_y, fp.sensor_z);
+            cell[q] = L.c;
+            const float dx = L.x - L.ox, dy = L.y - L.oy, dz = L.z - L.oz;  // exact (nearby floats)
+            const double ox = L.ox, oy = L.oy, oz = L.oz;
+            double ao = 0.0, af = 0.0;
+            for (int g0 = 0; g0 < nr; g0 += 32) {
+                const int r = g0 + lane;
+                bool hit = false;
+                if (r < nr) {
+                    const float4 a = S.a[r];
+                    const double4 cd = S.c[r];
+                    const double par0 = (ox * a.x + oy * a.y + oz * a.z) * cd.z;
+                    const double sc = par0 * cd.z;
+                    const double px = ox - sc * a.x, py = oy - sc * a.y, pz = oz - sc * a.z;
+                    const double along = fmin(par0, 0.0) + fmax(par0 - cd.x, 0.0);
+                    const float d2 = (float)(px * px + py * py + pz * pz + along * along);
+                    hit = d2 < A.cull_r2;
+                    if (hit) {
+                        S.stage[wid][lane][0] = make_float4((float)par0, (float)(par0 - cd.y), (float)(par0 - cd.x), 0.f);
+                        S.stage[wid][lane][1] = make_float4((float)px, (float)py, (float)pz, 0.f);
+                        S.stage[wid][lane][2] =
+                            make_float4((float)(ox - a.x), (float)(oy - a.y), (float)(oz - a.z), 0.f);
+                    }
+                }
+                unsigned mask = __ballot_sync(0xffffffffu, hit);
+                __syncwarp();
+                while (mask) {
+                    const int j = __ffs(mask) - 1;
+                    mask &= mask - 1;
+                    const float4 s0 = S.stage[wid][j][0], s1 = S.stage[wid][j][1], s2 = S.stage[wid][j][2];
+                    const float4 u = S.u[g0 + j];
+                    // occupied evidence (mass_update.cu:48-52)
+                    const float vx = s2.x + dx, vy = s2.y + dy, vz = s2.z + dz;
+                    const float d2o = vx * vx + vy * vy + vz * vz;
+                    if (d2o < ls2) ao += (double)kernel_func(sqrtf(d2o), inv_ls, p.sigma);
+                    // free evidence (:54-71)
+                    const float dpar = dx * u.x + dy * u.y + dz * u.z;
+                    if (s0.z + dpar < 0.0f) {  // d_proj < d_m
+                        const float qx = s1.x + dx - dpar * u.x, qy = s1.y + dy - dpar * u.y,
+                                    qz = s1.z + dz - dpar * u.z;
+                        const float al = fminf(s0.x + dpar, 0.0f) + fmaxf(s0.y + dpar, 0.0f);
+                        const float d2f = qx * qx + qy * qy + qz * qz + al * al;
+                        if (d2f < ls2) af += (double)kernel_func(sqrtf(d2f), inv_ls, p.sigma);
+                    }
+                }
+                __syncwarp();
+            }
+            acc_o[q] = ao;
+            acc_f[q] = af;
+        }
+        // fixed-point quantisation: identical whether a tile has one chunk or many
+        long long fo[NSBW], ff[NSBW];
+#pragma unroll
+        for (int q = 0; q < NSBW; ++q) {
+            fo[q] = __double2ll_rn(acc_o[q] * A.fx_scale);
+            ff[q] = __double2ll_rn(acc_f[q] * A.fx_scale);
+        }
+        bool run_update = true;
+        if (n_items > 1) {
+#pragma unroll
+            for (int q = 0; q < NSBW; ++q) {
+                if (cell[q] >= 0) {
+                    if (fo[q]) atomicAdd(&A.acc[2 * (long)cell[q]], (unsigned long long)fo[q]);
+                    if (ff[q]) atomicAdd(&A.acc[2 * (long)cell[q] + 1], (unsigned long long)ff[q]);
+                }
+            }
+            __threadfence();
+            __syncthreads();
+            if (threadIdx.x == 0) s_last = (atomicAdd(&A.tile_done[t], 1u) == n_items - 1) ? 1 : 0;
+            __syncthreads();
+            run_update = s_last != 0;
+            if (run_update) {
+                __threadfence();
+#pragma unroll
+                for (int q = 0; q < NSBW; ++q) {
+                    if (cell[q] >= 0) {
+                        fo[q] = (long long)atomicExch(&A.acc[2 * (long)cell[q]], 0ull);
+                        ff[q] = (long long)atomicExch(&A.acc[2 * (long)cell[q] + 1], 0ull);
+                    }
+                }
+                if (threadIdx.x == 0) A.tile_done[t] = 0;
+            }
+        }
+        if (run_update) {
+#pragma unroll
+            for (int q = 0; q < NSBW; ++q) {
+                if (cell[q] >= 0) {
+                    const float dlo = (float)((double)fo[q] * A.fx_inv);
+                    const float dlf = (float)((double)ff[q] * A.fx_inv);
+                    k3dom_cell_update(p, fp.dt, cell[q], dlo, dlf, A.cs, A.cw, A.first_frame != 0);
+                }
+            }
+        }
+        __syncthreads();
+    }
+}
+
+// ================================================================ DS-PHD/MIB
+struct DsMeas {
+    float occ, free_m;
+};
+
+// The measurement masses of measurement_grid.cu:98-157 from the neighbour summary.
+__device__ __forceinline__ DsMeas ds_meas_from(const DevParams& p, float acs, int nb, bool all_farther,
+                                               float max_occ) {
+    DsMeas m;
+    if (nb == 0) {
+        m.occ = 0.0f;
+        m.free_m = 0.0f;
+        return m;
+    }
+    float mo, mf;
+    if (all_farther) {
+        // pFree (:41-50): p_min + r / max_range * (p_max - p_min)
+        const float r = sqrtf(acs);
+        const float unc = __fadd_rn(0.15f, __fmul_rn(__fdiv_rn(r, p.max_range), __fsub_rn(1.0f, 0.15f)));
+        if (max_occ > unc) {
+            mo = max_occ;
+            mf = 0.0f;
+        } else {
+            mo = 0.0f;
+            mf = __fsub_rn(1.0f, unc);
+        }
+    } else {
+        mo = max_occ > 0.5f ? max_occ : 0.0f;
+        mf = 0.0f;
+    }
+    const float eps = 0.00001f;
+    m.occ = fmaxf(eps, fminf(__fsub_rn(1.0f, eps), mo));
+    m.free_m = fmaxf(eps, fminf(__fsub_rn(1.0f, eps), mf));
+    return m;
+}
+
+// update_masses (src/dsphdmib/kernel/mass_update.cu:17-30) keeping its double promotions.
+__device__ __forceinline__ void ds_update_masses(float mop, float mfp, DsMeas mc, float* occ, float* fr) {
+    const float unknown_pred = (float)(1.0 - (double)mop - (double)mfp);
+    const float meas_unknown = (float)(1.0 - (double)mc.free_m - (double)mc.occ);
+    const float K = __fadd_rn(__fmul_rn(mfp, mc.occ), __fmul_rn(mop, mc.free_m));
+    const float no = __fadd_rn(__fadd_rn(__fmul_rn(mop, meas_unknown), __fmul_rn(unknown_pred, mc.occ)),
+                               __fmul_rn(mop, mc.occ));
+    const float nf = __fadd_rn(__fadd_rn(__fmul_rn(mfp, meas_unknown), __fmul_rn(unknown_pred, mc.free_m)),
+                               __fmul_rn(mfp, mc.free_m));
+    const double den = 1.0 - (double)K;
+    *occ = (float)((double)no / den);
+    *fr = (float)((double)nf / den);
+}
+
+__device__ void ds_cell_update(const DevParams& p, int c, DsMeas mc, CellState cs, CellWork cw, bool first_frame) {
+    cw.meas_occ[c] = mc.occ;
+    cw.meas_free[c] = mc.free_m;
+    if (first_frame) {
+        cs.born_m[c] = mc.occ;  // copyMassesKernel (measurement_grid.cu:55-62)
+        return;
+    }
+    const int start = cw.start[c];
+    const bool has = start >= 0;
+    const float free0 = cs.free_m[c];
+    float occ_up, free_up, rho_b = 0.0f, mop = 0.0f, divisor = 0.0f;
+    if (has) {
+        mop = cw.sum_w[c];
+        if (mop > 1.0f) {
+            divisor = mop;  // normalize_weights (:37-44), applied in the reweight kernel
+            mop = 1.0f;
+        }
+        const float mfp = fminf(__fmul_rn(0.9f, free0), __fsub_rn(1.0f, mop));
+        ds_update_masses(mop, mfp, mc, &occ_up, &free_up);
+        // separate_newborn_part (:32-35) with its double promotions
+        const double om = 1.0 - (double)mop;
+        rho_b = (float)(((double)__fmul_rn(occ_up, p.p_B) * om) / ((double)mop + (double)p.p_B * om));
+    } else {
+        const float m_occ = cs.occ_m[c];
+        const float m_free = fminf(__fmul_rn(0.9f, free0), __fsub_rn(1.0f, m_occ));
+        ds_update_masses(m_occ, m_free, mc, &occ_up, &free_up);
+    }
+    const float pers = __fsub_rn(occ_up, rho_b);
+    cs.born_m[c] = rho_b;
+    cs.pers_m[c] = pers;
+    cs.free_m[c] = free_up;
+    cs.occ_m[c] = occ_up;
+    cs.pred_m[c] = mop;
+    const float mu_UA = has ? calc_norm(mop, pers) : 0.0f;
+    cw.factor[c] = mu_UA;
+    cw.divisor[c] = divisor;
+    float vx = 0.0f, vy = 0.0f, vz = 0.0f;
+    if (has && pers > 0.0f) {
+        float sx = cw.sum_wvx[c], sy = cw.sum_wvy[c], sz = cw.sum_wvz[c];
+        if (divisor > 0.0f) {
+            sx /= divisor;
+            sy /= divisor;
+            sz /= divisor;
+        }
+        vx = (mu_UA * sx) / pers;
+        vy = (mu_UA * sy) / pers;
+        vz = (mu_UA * sz) / pers;
+    }
+    cs.mvx[c] = vx;
+    cs.mvy[c] = vy;
+    cs.mvz[c] = vz;
+}
+
+// Neighbour test of measurement_grid.cu:88-99 in the reference's FP32 operation order.
+__device__ __forceinline__ bool ds_is_neighbor(float x, float y, float z, float acs, float4 m, float wr2) {
+    const float ip = __fadd_rn(__fadd_rn(__fmul_rn(x, m.x), __fmul_rn(y, m.y)), __fmul_rn(z, m.z));
+    return ip > 0.0f && __fsub_rn(acs, __fdiv_rn(__fmul_rn(ip, ip), m.w)) < wr2;
+}
+
+// pOcc (measurement_grid.cu:28-39)
+__device__ __forceinline__ float ds_pocc(float x, float y, float z, float4 m, float delta) {
+    const float dx = __fsub_rn(x, m.x), dy = __fsub_rn(y, m.y), dz = __fsub_rn(z, m.z);
+    const float r_sqr = __fadd_rn(__fadd_rn(__fmul_rn(dx, dx), __fmul_rn(dy, dy)), __fmul_rn(dz, dz));
+    const float delta_sqr = __fmul_rn(delta, delta);
+    return __fmul_rn(0.95f, expf(__fdiv_rn(__fmul_rn(-0.5f, r_sqr), delta_sqr)));
+}
+
+// COUNT: pass 1, count neighbours per cell in chunks 0..n-2 of multi-chunk tiles.
+// !COUNT: pass 2, take each cell's first (100 - earlier count) neighbours of the chunk.
+template <int NSBW, bool COUNT>
+__global__ void __launch_bounds__(kEvThreads) k_dsgrid(EvArgs A) {
+    __shared__ float4 sa[kChunk];
+    __shared__ uint32_t s_item;
+    __shared__ int s_last;
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    const DevParams& p = A.p;
+    const FrameParams fp = *A.fp;
+    const uint32_t total_items = A.item_off[A.T];
+    const int n_points = fp.n_points;
+    const int tile_cells = A.ts.tx * A.ts.ty * A.ts.tz;
+    unsigned int* counter = COUNT ? &A.status->work_counter2 : &A.status->work_counter;
+    uint32_t* part_max = reinterpret_cast<uint32_t*>(A.acc);
+    uint32_t* part_flags = part_max + p.C;
+
+    for (;;) {
+        if (threadIdx.x == 0) s_item = atomicAdd(counter, 1u);
+        __syncthreads();
+        const uint32_t item = s_item;
+        __syncthreads();
+        if (item >= total_items) break;
+        const int t = find_tile(A.item_off, A.T, item);
+        const uint32_t k = item - A.item_off[t];
+        const uint32_t n_items = A.item_off[t + 1] - A.item_off[t];
+        if (COUNT && (n_items == 1 || k == n_items - 1)) continue;  // uniform across the block
+        const uint32_t e0 = A.tile_start[t] + k * kChunk;
+        const uint32_t e1 = min(A.tile_start[t + 1], e0 + (uint32_t)kChunk);
+        const int nr = (int)(e1 > e0 ? e1 - e0 : 0);
+        for (int r = threadIdx.x; r < nr; r += kEvThreads) {
+            uint32_t rid = A.evals[e0 + r];
+            if (rid >= (uint32_t)n_points) rid = 0;
+            sa[r] = A.ray_a[rid];
+        }
+        __syncthreads();
+        int cell[NSBW], nbq[NSBW];
+        bool farq[NSBW];
+        float maxq[NSBW], acsq[NSBW];
+#pragma unroll
+        for (int q = 0; q < NSBW; ++q) {
+            const int sbi = wid + q * kEvWarps;
+            const CellLoc L = locate(p, A.ts, t, sbi, lane, fp.sensor_x, fp.sensor_y, fp.sensor_z);
+            cell[q] = L.c;
+            const float acs = __fadd_rn(__fadd_rn(__fmul_rn(L.x, L.x), __fmul_rn(L.y, L.y)), __fmul_rn(L.z, L.z));
+            acsq[q] = acs;
+            int quota = kDsMaxNeighbors;
+            if (!COUNT && n_items > 1) {
+                int pre = 0;
+                const long base = (long)A.item_off[t] * tile_cells;
+                for (uint32_t kk = 0; kk < k; ++kk) {
+                    const long idx = base + (long)kk * tile_cells + L.local;
+                    pre += (idx < A.ds_count_capacity) ? (int)A.ds_counts[idx] : 0;
+                }
+                quota = max(0, kDsMaxNeighbors - pre);
+            }
+            if (L.c < 0) quota = 0;
+            int nb = 0;
+            bool all_far = true;
+            float mx = 0.0f;
+            if (__any_sync(0xffffffffu, quota > 0)) {
+                for (int g0 = 0; g0 < nr; g0 += 32) {
+                    const int r = g0 + lane;
+                    bool hit = false;
+                    if (r < nr) {
+                        const float4 a = sa[r];
+                        // distance of the sub-block centre to the half-line through m
+                        const float len = sqrtf(a.w);
+                        const float qx = L.ox - 0.5f * p.res, qy = L.oy - 0.5f * p.res, qz = L.oz - 0.5f * p.res;
+                        const float tproj = fmaxf((qx * a.x + qy * a.y + qz * a.z) / len, 0.0f);
+                        const float ex = qx - tproj * a.x / len, ey = qy - tproj * a.y / len,
+                                    ez = qz - tproj * a.z / len;
+                        hit = ex * ex + ey * ey + ez * ez < A.cull_r2;
+                    }
+                    unsigned mask = __ballot_sync(0xffffffffu, hit);
+                    while (mask) {
+                        const int j = __ffs(mask) - 1;
+                        mask &= mask - 1;
+                        const float4 a = sa[g0 + j];
+                        if (nb < quota && ds_is_neighbor(L.x, L.y, L.z, acs, a, A.wr2)) {
+                            ++nb;
+                            if (!COUNT) {
+                                if (acs > a.w) all_far = false;
+                                const float o = ds_pocc(L.x, L.y, L.z, a, p.meas_occ_stddev);
+                                if (o > mx) mx = o;
+                            }
+                        }
+                    }
+                    if (!__any_sync(0xffffffffu, nb < quota)) break;
+                }
+            }
+            nbq[q] = nb;
+            farq[q] = all_far;
+            maxq[q] = mx;
+            if (COUNT && L.c >= 0) {
+                const long idx = (long)item * tile_cells + L.local;
+                if (idx < A.ds_count_capacity) A.ds_counts[idx] = (uint8_t)nb;
+            }
+        }
+        if (COUNT) {
+            __syncthreads();
+            continue;
+        }
+        bool run_update = true;
+        if (n_items > 1) {
+#pragma unroll
+            for (int q = 0; q < NSBW; ++q) {
+                if (cell[q] >= 0 && nbq[q] > 0) {
+                    atomicMax(&part_max[cell[q]], __float_as_uint(maxq[q]));
+                    atomicOr(&part_flags[cell[q]], 1u | (farq[q] ? 0u : 2u));
+                }
+            }
+            __threadfence();
+            __syncthreads();
+            if (threadIdx.x == 0) s_last = (atomicAdd(&A.tile_done[t], 1u) == n_items - 1) ? 1 : 0;
+            __syncthreads();
+            run_update = s_last != 0;
+            if (run_update) {
+                __threadfence();
+#pragma unroll
+                for (int q = 0; q < NSBW; ++q) {
+                    if (cell[q] >= 0) {
+                        const uint32_t m = atomicExch(&part_max[cell[q]], 0u);
+                        const uint32_t f = atomicExch(&part_flags[cell[q]], 0u);
+                        nbq[q] = (f & 1u) ? 1 : 0;
+                        farq[q] = (f & 2u) == 0;
+                        maxq[q] = __uint_as_float(m);
+                    }
+                }
+                if (threadIdx.x == 0) A.tile_done[t] = 0;
+            }
+        }
+        if (run_update) {
+#pragma unroll
+            for (int q = 0; q < NSBW; ++q) {
+                if (cell[q] >= 0) {
+                    const DsMeas mc = ds_meas_from(p, acsq[q], nbq[q], farq[q], maxq[q]);
+                    ds_cell_update(p, cell[q], mc, A.cs, A.cw, A.first_frame != 0);
+                }
+            }
+        }
+        __syncthreads();
+    }
+}
+
+// ================================================================ launchers
+static EvArgs make_args(const DevParams& p, const FrameParams* fp, RayBuffers& rb, CellState cs, CellWork cw,
+                        bool first_frame, DevStatus* status, bool ds) {
+    EvArgs A;
+    A.p = p;
+    A.fp = fp;
+    A.ts.tx = rb.tx; A.ts.ty = rb.ty; A.ts.tz = rb.tz;
+    A.ts.ntx = rb.ntx; A.ts.nty = rb.nty;
+    A.ts.nsbx = rb.tx / 4; A.ts.nsby = rb.ty / 4;
+    A.T = rb.tiles;
+    A.item_off = rb.item_off;
+    A.tile_start = rb.tile_start;
+    A.evals = rb.evals2;
+    A.ray_a = rb.ray_a;
+    A.ray_b = rb.ray_b;
+    A.ray_c = rb.ray_c;
+    A.tile_done = rb.tile_done;
+    A.acc = rb.acc;
+    A.ds_counts = rb.ds_counts;
+    A.ds_count_capacity = rb.ds_count_capacity;
+    A.cs = cs;
+    A.cw = cw;
+    A.status = status;
+    A.first_frame = first_frame ? 1 : 0;
+    // fixed point: one term is at most sigma; 2^40 / sigma leaves 2^23 terms of headroom
+    const double sig = std::max((double)p.sigma, 1e-30);
+    const int sh = 40 - (int)std::ceil(std::log2(sig));
+    A.fx_scale = std::ldexp(1.0, sh);
+    A.fx_inv = std::ldexp(1.0, -sh);
+    A.wr2 = p.window_radius * p.window_radius;
+    // K3DOM culls around the anchor cell (2,2,1) of a sub-block: the farthest cell centre is
+    // 3 res away. DS culls around the sub-block centre: half diagonal sqrt(1.5^2+1.5^2+0.5^2) res.
+    const float rsb = ds ? 2.1794495f * p.res : 3.0f * p.res;
+    float rsup;
+    if (!ds) {
+        rsup = p.ls * (1.0f + 1e-4f) + rsb + 1e-3f * p.res;
+    } else {
+        const float ext = max_extent(p);
+        const float slack = 64.0f * 5.96e-8f * ext * ext;
+        rsup = sqrtf(p.window_radius * p.window_radius + slack) + rsb + 1e-3f * p.res;
+    }
+    A.cull_r2 = rsup * rsup;
+    return A;
+}
+
+static int nsbw_of(const RayBuffers& rb) { return (rb.tx / 4) * (rb.ty / 4) * (rb.tz / 2) / kEvWarps; }
+
+cudaError_t launch_k3dom_evidence(const DevParams& p, const FrameParams* fp, RayBuffers& rb, CellState cs,
+                                  CellWork cw, bool first_frame, DevStatus* status, int num_sms, cudaStream_t st) {
+    EvArgs A = make_args(p, fp, rb, cs, cw, first_frame, status, false);
+    const int grid = num_sms * 2;
+    const size_t sm = sizeof(BgkiSmem);
+    switch (nsbw_of(rb)) {
+        case 1: k_bgki<1><<<grid, kEvThreads, sm, st>>>(A); break;
+        case 2: k_bgki<2><<<grid, kEvThreads, sm, st>>>(A); break;
+        case 4: k_bgki<4><<<grid, kEvThreads, sm, st>>>(A); break;
+        case 8: k_bgki<8><<<grid, kEvThreads, sm, st>>>(A); break;
+        default: return cudaErrorInvalidValue;
+    }
+    return cudaGetLastError();
+}
+
+cudaError_t launch_ds_evidence(const DevParams& p, const FrameParams* fp, RayBuffers& rb, CellState cs, CellWork cw,
+                               bool first_frame, DevStatus* status, int num_sms, cudaStream_t st) {
+    EvArgs A = make_args(p, fp, rb, cs, cw, first_frame, status, true);
+    const int grid = num_sms * 4;
+    switch (nsbw_of(rb)) {
+        case 1:
+            k_dsgrid<1, true><<<grid, kEvThreads, 0, st>>>(A);
+            k_dsgrid<1, false><<<grid, kEvThreads, 0, st>>>(A);
+            break;
+        case 2:
+            k_dsgrid<2, true><<<grid, kEvThreads, 0, st>>>(A);
+            k_dsgrid<2, false><<<grid, kEvThreads, 0, st>>>(A);
+            break;
+        case 4:
+            k_dsgrid<4, true><<<grid, kEvThreads, 0, st>>>(A);
+            k_dsgrid<4, false><<<grid, kEvThreads, 0, st>>>(A);
+            break;
+        case 8:
+            k_dsgrid<8, true><<<grid, kEvThreads, 0, st>>>(A);
+            k_dsgrid<8, false><<<grid, kEvThreads, 0, st>>>(A);
+            break;
+        default:
+            return cudaErrorInvalidValue;
+    }
+    return cudaGetLastError();
+}
+
+cudaError_t evidence_init() {
+    cudaError_t e;
+    const int sm = (int)sizeof(BgkiSmem);
+    if ((e = cudaFuncSetAttribute(k_bgki<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm))) return e;
+    if ((e = cudaFuncSetAttribute(k_bgki<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm))) return e;
+    if ((e = cudaFuncSetAttribute(k_bgki<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm))) return e;
+    return cudaFuncSetAttribute(k_bgki<8>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
+}
+
+}  // namespace k3dom

@@ -1,0 +1,135 @@
+// exactscan.cu -- inclusive prefix sums of non-negative floats that are exact and
+// order-independent.
+//
+// The reference forms these sums with thrust::inclusive_scan in FP32
+// (include/common/common.h:7-18, called at src/common/dom.cu:215-217 for born masses and
+// :268-273 for the joint weights). Their rounding depends on CUB's tiling, and the integer
+// results derived from them (birth slot boundaries, init_new_particles.cu:14-27; ancestor
+// indices, resampling.cu:55-68) inherit that dependence. Here every element is converted
+// exactly to a 128-bit fixed-point integer with 2^-80 resolution, the integers are summed
+// (associative), and each prefix is rounded once to the nearest float. The result is the
+// correctly rounded exact prefix, independent of the launch shape, so a CPU oracle
+// reproduces it bit for bit.
+#include <cuda_runtime.h>
+
+#include "common.cuh"
+#include "internal.h"
+#include "scan.cuh"
+
+namespace k3dom {
+
+constexpr int kExThreads = 256;
+constexpr int kExItems = 8;
+constexpr int kExTile = kExThreads * kExItems;
+constexpr int kFracBits = 80;
+
+// float (>= 0) -> fixed point with kFracBits fractional bits. Negative or non-finite
+// inputs contribute 0 (they cannot occur for weights and born masses).
+__device__ __forceinline__ u128 to_fixed(float f) {
+    uint32_t b = __float_as_uint(f);
+    if (b & 0x80000000u) return 0;
+    uint32_t e = b >> 23, frac = b & 0x7FFFFFu;
+    if (e == 0xFFu) return 0;
+    uint32_t m = e ? (frac | 0x800000u) : frac;
+    int sh = (e ? (int)e : 1) - 150 + kFracBits;  // value = m * 2^(e-150)
+    if (sh >= 0) {
+        if (sh > 127 - 24) return 0;  // out of range (>= 2^47); never reached by masses
+        return (u128)m << sh;
+    }
+    if (sh <= -32) return 0;
+    return (u128)(m >> (-sh));
+}
+
+// Round-to-nearest-even float of v * 2^-kFracBits.
+__device__ __forceinline__ float from_fixed(u128 v) {
+    if (v == 0) return 0.0f;
+    uint64_t hi = (uint64_t)(v >> 64), lo = (uint64_t)v;
+    int lz = hi ? __clzll((long long)hi) : 64 + __clzll((long long)lo);
+    u128 n = v << lz;
+    uint64_t top = (uint64_t)(n >> 64);
+    if ((uint64_t)n != 0) top |= 1ull;  // sticky
+    float f = __ull2float_rn(top);
+    return ldexpf(f, 64 - lz - kFracBits);
+}
+
+struct TwoSeg {
+    const float* a;
+    long na;
+    const float* b;
+    __device__ __forceinline__ float operator()(long i) const { return i < na ? a[i] : b[i - na]; }
+};
+
+__global__ void exact_tile_sums(TwoSeg in, long n, u128* __restrict__ tile_sums) {
+    __shared__ u128 sm[kExThreads / 32 + 1];
+    const long base = (long)blockIdx.x * kExTile;
+    u128 s = 0;
+#pragma unroll
+    for (int j = 0; j < kExItems; ++j) {
+        long i = base + (long)j * kExThreads + threadIdx.x;
+        if (i < n) s += to_fixed(in(i));
+    }
+    u128 tot;
+    block_exclusive_scan<u128, kExThreads>(s, sm, &tot);
+    if (threadIdx.x == 0) tile_sums[blockIdx.x] = tot;
+}
+
+__global__ void exact_tile_offsets(u128* __restrict__ tile_sums, int ntiles) {
+    __shared__ u128 sm[kExThreads / 32 + 1];
+    u128 carry = 0;
+    for (int b = 0; b < ntiles; b += kExThreads) {
+        int i = b + threadIdx.x;
+        u128 v = (i < ntiles) ? tile_sums[i] : (u128)0;
+        u128 tot;
+        u128 ex = block_exclusive_scan<u128, kExThreads>(v, sm, &tot);
+        if (i < ntiles) tile_sums[i] = carry + ex;
+        carry += tot;
+    }
+}
+
+__global__ void exact_apply(TwoSeg in, long n, const u128* __restrict__ tile_off,
+                            float* __restrict__ out) {
+    __shared__ u128 sm[kExThreads / 32 + 1];
+    const long base = (long)blockIdx.x * kExTile + (long)threadIdx.x * kExItems;
+    u128 v[kExItems];
+    u128 s = 0;
+#pragma unroll
+    for (int j = 0; j < kExItems; ++j) {
+        long i = base + j;
+        v[j] = (i < n) ? to_fixed(in(i)) : (u128)0;
+        s += v[j];
+    }
+    u128 tot;
+    u128 run = tile_off[blockIdx.x] + block_exclusive_scan<u128, kExThreads>(s, sm, &tot);
+#pragma unroll
+    for (int j = 0; j < kExItems; ++j) {
+        long i = base + j;
+        run += v[j];
+        if (i < n) out[i] = from_fixed(run);
+    }
+}
+
+int exact_scan_tiles(long n) { return div_up(n, kExTile); }
+size_t exact_scan_scratch_bytes(long n) { return (size_t)(exact_scan_tiles(n) + 1) * sizeof(u128); }
+
+static cudaError_t exact_scan_impl(TwoSeg in, long n, float* out, void* scratch, cudaStream_t st) {
+    if (n <= 0) return cudaSuccess;
+    int nt = exact_scan_tiles(n);
+    u128* ts = reinterpret_cast<u128*>(scratch);
+    exact_tile_sums<<<nt, kExThreads, 0, st>>>(in, n, ts);
+    exact_tile_offsets<<<1, kExThreads, 0, st>>>(ts, nt);
+    exact_apply<<<nt, kExThreads, 0, st>>>(in, n, ts, out);
+    return cudaGetLastError();
+}
+
+cudaError_t exact_scan_float(const float* in, float* out, long n, void* scratch, cudaStream_t st) {
+    TwoSeg s{in, n, in};
+    return exact_scan_impl(s, n, out, scratch, st);
+}
+
+cudaError_t exact_scan_float2(const float* a, long na, const float* b, long nb, float* out,
+                              void* scratch, cudaStream_t st) {
+    TwoSeg s{a, na, b};
+    return exact_scan_impl(s, na + nb, out, scratch, st);
+}
+
+}  // namespace k3dom

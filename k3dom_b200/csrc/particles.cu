@@ -1,0 +1,516 @@
+// particles.cu -- particle-side kernels of the K3DOM frame: prediction (with the ego-motion
+// particle shift folded in), the post-sort gather with per-cell segmented sums, the
+// persistent reweight, first-frame initialisation, births and resampling.
+//
+// All float arithmetic that decides an integer result (positions -> voxel indices, velocity
+// draws, birth slot and ancestor searches) is written with _rn intrinsics in the operation
+// order of the reference, so it is not contracted into FMAs and reproduces the reference
+// built with -fmad=false bit for bit.
+#include <cuda_runtime.h>
+
+#include "common.cuh"
+#include "internal.h"
+
+namespace k3dom {
+
+using namespace k3dom_draws;
+
+// ---------------------------------------------------------------- prediction
+// predictKernel (src/common/kernel/predict.cu:12-59), preceded by moveParticlesKernel
+// (src/common/kernel/ego_motion_compensation.cu:12-18) when a map shift is pending.
+__global__ void __launch_bounds__(kBlock) k_predict(DevParams p, const FrameParams* __restrict__ fpp,
+                                                    Particles a) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= p.P) return;
+    const FrameParams fp = *fpp;
+    float px = a.px[i], py = a.py[i], pz = a.pz[i];
+    float vx = a.vx[i], vy = a.vy[i], vz = a.vz[i];
+    float w = a.w[i];
+    if (fp.shift_pending) {
+        px = __fsub_rn(px, (float)fp.shift_x);
+        py = __fsub_rn(py, (float)fp.shift_y);
+        pz = __fsub_rn(pz, (float)fp.shift_z);
+    }
+    float n[6];
+    predict_normals(fp.seed, fp.frame, (uint64_t)i, n);
+    // curand_normal(state, 0, s) = z * s + 0 (include/common/cuda_utils.h:33-35)
+    const float npx = __fadd_rn(__fmul_rn(n[0], p.noise_pos), 0.0f);
+    const float npy = __fadd_rn(__fmul_rn(n[1], p.noise_pos), 0.0f);
+    const float npz = __fadd_rn(__fmul_rn(n[2], p.noise_pos), 0.0f);
+    const float nvx = __fadd_rn(__fmul_rn(n[3], p.noise_vel), 0.0f);
+    const float nvy = __fadd_rn(__fmul_rn(n[4], p.noise_vel), 0.0f);
+    const float nvz = __fadd_rn(__fmul_rn(n[5], p.noise_vel), 0.0f);
+    // pos += vel * dt + noise  (old velocity)
+    px = __fadd_rn(px, __fadd_rn(__fmul_rn(vx, fp.dt), npx));
+    py = __fadd_rn(py, __fadd_rn(__fmul_rn(vy, fp.dt), npy));
+    pz = __fadd_rn(pz, __fadd_rn(__fmul_rn(vz, fp.dt), npz));
+    vx = __fadd_rn(vx, nvx);
+    vy = __fadd_rn(vy, nvy);
+    vz = __fadd_rn(vz, nvz);
+    w = __fmul_rn(w, p.p_S);
+    const float lim = __fmul_rn(5.0f, p.init_max_vel);
+    const float nlim = __fmul_rn(-5.0f, p.init_max_vel);
+    vx = clampv(vx, nlim, lim);
+    vy = clampv(vy, nlim, lim);
+    vz = clampv(vz, nlim, lim);
+    const float G = (float)p.G, Gz = (float)p.Gz;
+    if ((px >= G || px < 0.0f) || (py >= G || py < 0.0f) || (pz >= Gz || pz < 0.0f)) w = 0.0f;
+    const int ix = clampv(f2i_trunc(px), 0, p.G - 1);
+    const int iy = clampv(f2i_trunc(py), 0, p.G - 1);
+    const int iz = clampv(f2i_trunc(pz), 0, p.Gz - 1);
+    a.px[i] = px; a.py[i] = py; a.pz[i] = pz;
+    a.vx[i] = vx; a.vy[i] = vy; a.vz[i] = vz;
+    a.w[i] = w;
+    a.cell[i] = ix + p.G * iy + p.G * p.G * iz;
+}
+
+void launch_predict(const DevParams& p, const FrameParams* fp, Particles a, cudaStream_t st) {
+    if (p.P <= 0) return;
+    k_predict<<<div_up(p.P, kBlock), kBlock, 0, st>>>(p, fp, a);
+}
+
+__global__ void k_shift_particles(int n, Particles a, int mx, int my, int mz) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    a.px[i] = __fsub_rn(a.px[i], (float)mx);
+    a.py[i] = __fsub_rn(a.py[i], (float)my);
+    a.pz[i] = __fsub_rn(a.pz[i], (float)mz);
+}
+
+void launch_shift_particles(const DevParams& p, Particles a, int mx, int my, int mz, cudaStream_t st) {
+    if (p.P <= 0) return;
+    k_shift_particles<<<div_up(p.P, kBlock), kBlock, 0, st>>>(p.P, a, mx, my, mz);
+}
+
+// ---------------------------------------------------------------- gather + segmented sums
+// After the sort: sorted slot i takes particle perm[i] (the payload permutation of
+// thrust::sort_by_key, src/common/dom.cu:175-183). In the same pass each warp forms the
+// per-cell sums over its sorted range -- the serial weight loop of
+// gridCellPredictionUpdateKernel (src/k3dom/kernel/mass_update.cu:168-174) and the
+// w*v sums behind statisticalMomentsKernel1/2 (statistical_moments.cu:22-63) -- and the
+// start/end ranges of particleToGridKernel (particle_to_grid.cu:23-39). A cell's sum is
+// formed by exactly one warp (the one holding its first particle) in a fixed order, so it
+// is deterministic. The penalty of penalizeStaticParticlesKernel (resampling.cu:13-36) is
+// recorded as the sign bit of the sorted weight and applied at resampling.
+constexpr int kSegItems = 8;                       // 32-wide chunks per warp range
+constexpr int kSegRange = 32 * kSegItems;          // 256 sorted particles per warp
+constexpr int kSegWarps = kBlock / 32;
+
+struct SegVal {
+    double w, x, y, z;
+};
+
+__device__ __forceinline__ SegVal shfl_up_seg(const SegVal& v, int d) {
+    SegVal o;
+    o.w = __shfl_up_sync(0xffffffffu, v.w, d);
+    o.x = __shfl_up_sync(0xffffffffu, v.x, d);
+    o.y = __shfl_up_sync(0xffffffffu, v.y, d);
+    o.z = __shfl_up_sync(0xffffffffu, v.z, d);
+    return o;
+}
+
+__global__ void __launch_bounds__(kBlock)
+k_gather_segsum(DevParams p, Particles a, Particles s, const uint32_t* __restrict__ keys,
+                const uint32_t* __restrict__ perm, CellWork cw) {
+    const int lane = threadIdx.x & 31;
+    const long warp_global = (long)blockIdx.x * kSegWarps + (threadIdx.x >> 5);
+    const long r0 = warp_global * kSegRange;
+    const long P = p.P;
+    if (r0 >= P) return;
+    const long r1 = min(r0 + (long)kSegRange, P);
+    const float min_sq = __fmul_rn(p.min_vel, p.min_vel);
+
+    // carried state of the open segment (ends of the previous chunk)
+    SegVal carry = {0.0, 0.0, 0.0, 0.0};
+    long carry_head = -1;  // head position of the open segment if this warp owns it
+    uint32_t prev_key = (r0 > 0) ? keys[r0 - 1] : 0xFFFFFFFFu;
+    bool done = false;
+
+    for (long c0 = r0; !done; c0 += 32) {
+        const bool in_range_chunk = c0 < r1;
+        const long pos = c0 + lane;
+        const bool valid = pos < P;
+        const bool mine = pos < r1;  // this warp writes the sorted slot
+        uint32_t key = valid ? keys[pos] : 0xFFFFFFFEu;
+        uint32_t next_key = (pos + 1 < P) ? keys[pos + 1] : 0xFFFFFFFDu;
+        uint32_t kprev = __shfl_up_sync(0xffffffffu, key, 1);
+        if (lane == 0) kprev = prev_key;
+        prev_key = __shfl_sync(0xffffffffu, key, 31);
+        const bool head = valid && (pos == 0 || key != kprev);
+        const bool tail = valid && (key != next_key);
+
+        SegVal v = {0.0, 0.0, 0.0, 0.0};
+        if (valid) {
+            const uint32_t src = perm[pos];
+            const float vx = a.vx[src], vy = a.vy[src], vz = a.vz[src];
+            const float w = a.w[src];
+            if (mine) {
+                const float sp = __fadd_rn(__fadd_rn(__fmul_rn(vx, vx), __fmul_rn(vy, vy)),
+                                           __fmul_rn(vz, vz));
+                const bool slow = sp < min_sq;
+                s.px[pos] = a.px[src];
+                s.py[pos] = a.py[src];
+                s.pz[pos] = a.pz[src];
+                s.vx[pos] = vx;
+                s.vy[pos] = vy;
+                s.vz[pos] = vz;
+                s.w[pos] = slow ? -w : w;  // sign bit = penalised at resampling
+                s.assoc[pos] = a.assoc[src];
+                s.cell[pos] = (int)key;
+            }
+            v.w = (double)w;
+            v.x = (double)__fmul_rn(w, vx);
+            v.y = (double)__fmul_rn(w, vy);
+            v.z = (double)__fmul_rn(w, vz);
+        }
+        // segmented inclusive scan with head flags
+        bool hf = head;
+        long hpos = head ? pos : -1;
+#pragma unroll
+        for (int d = 1; d < 32; d <<= 1) {
+            SegVal o = shfl_up_seg(v, d);
+            bool ohf = __shfl_up_sync(0xffffffffu, hf, d);
+            long oh = __shfl_up_sync(0xffffffffu, hpos, d);
+            if (lane >= d) {
+                if (!hf) { v.w += o.w; v.x += o.x; v.y += o.y; v.z += o.z; }
+                hf = hf || ohf;
+                hpos = max(hpos, oh);
+            }
+        }
+        if (!hf) {
+            v.w += carry.w; v.x += carry.x; v.y += carry.y; v.z += carry.z;
+            hpos = carry_head;
+        }
+        // a segment is owned by the warp whose range holds its head
+        const bool owned = hpos >= r0 && hpos < r1;
+        if (tail && owned) {
+            cw.sum_w[key] = (float)v.w;
+            cw.sum_wvx[key] = (float)v.x;
+            cw.sum_wvy[key] = (float)v.y;
+            cw.sum_wvz[key] = (float)v.z;
+            cw.start[key] = (int)hpos;
+            cw.end[key] = (int)pos;
+        }
+        carry.w = __shfl_sync(0xffffffffu, v.w, 31);
+        carry.x = __shfl_sync(0xffffffffu, v.x, 31);
+        carry.y = __shfl_sync(0xffffffffu, v.y, 31);
+        carry.z = __shfl_sync(0xffffffffu, v.z, 31);
+        carry_head = __shfl_sync(0xffffffffu, hpos, 31);
+        const bool last_tail = __shfl_sync(0xffffffffu, tail, 31);
+        const bool any_valid_after = (c0 + 32) < P;
+        if (!in_range_chunk || (c0 + 32 >= r1)) {
+            // past (or at the end of) the range: continue only for an owned open segment
+            const bool open_owned = !last_tail && carry_head >= r0 && carry_head < r1;
+            done = !open_owned || !any_valid_after;
+        }
+    }
+}
+
+void launch_gather_segsum(const DevParams& p, Particles a, Particles s, const uint32_t* sorted_keys,
+                          const uint32_t* perm, CellWork cw, cudaStream_t st) {
+    if (p.P <= 0) return;
+    const long warps = div_up(p.P, kSegRange);
+    k_gather_segsum<<<div_up(warps, kSegWarps), kBlock, 0, st>>>(p, a, s, sorted_keys, perm, cw);
+}
+
+// ---------------------------------------------------------------- persistent reweight
+// updatePersistentParticlesKernel3 (update_persistent_particles.cu:46-55) with p_A = 0:
+// w = mu_UA * w. For DS-PHD/MIB the in-place normalisation of
+// src/dsphdmib/kernel/mass_update.cu:37-44,64-68 (w /= occ_pred when the cell's weight
+// sum exceeds 1) is applied first. The penalty flag (sign bit) is kept.
+__global__ void __launch_bounds__(kBlock)
+k_reweight(DevParams p, Particles s, const uint32_t* __restrict__ keys, CellWork cw) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= p.P) return;
+    const uint32_t c = keys[i];
+    const float wv = s.w[i];
+    const bool flag = signbit(wv);
+    float w = fabsf(wv);
+    if (p.variant == 1) {
+        const float d = cw.divisor[c];
+        if (d > 0.0f) w = __fdiv_rn(w, d);
+    }
+    // p_A * mu_A * post_w + (1 - p_A) * mu_UA * w with p_A = 0, likelihood = 1
+    const float f = cw.factor[c];
+    w = __fadd_rn(0.0f, __fmul_rn(f, w));
+    s.w[i] = flag ? -w : w;
+}
+
+void launch_reweight(const DevParams& p, Particles s, const uint32_t* sorted_keys, CellWork cw,
+                     cudaStream_t st) {
+    if (p.P <= 0) return;
+    k_reweight<<<div_up(p.P, kBlock), kBlock, 0, st>>>(p, s, sorted_keys, cw);
+}
+
+// ---------------------------------------------------------------- slot ownership
+// Slot ranges of init_new_particles.cu:14-27: cell j owns slots
+// [int(acc[j-1]*k), int(acc[j]*k) - 1] with k = v / acc[C-1] (normalize_particle_orders,
+// :44-52). bound(j) = int(acc[j] * k) is monotone in j.
+struct SlotMap {
+    const float* cum;
+    int C;
+    float k;
+    __device__ __forceinline__ int bound(int j) const { return f2i_trunc(__fmul_rn(cum[j], k)); }
+    // first j with bound(j) > s, or C when none
+    __device__ __forceinline__ int owner(int s) const {
+        int lo = 0, hi = C;
+        while (lo < hi) {
+            int mid = (lo + hi) >> 1;
+            if (bound(mid) > s) hi = mid; else lo = mid + 1;
+        }
+        return lo;
+    }
+    __device__ __forceinline__ int start(int j) const { return j == 0 ? 0 : bound(j - 1); }
+    __device__ __forceinline__ int count(int j) const {
+        int st = start(j), en = bound(j) - 1;
+        return st <= en ? en - st + 1 : 0;
+    }
+};
+
+__device__ __forceinline__ SlotMap make_slotmap(const float* cum, int C, int v) {
+    SlotMap m;
+    m.cum = cum;
+    m.C = C;
+    const float mx = cum[C - 1];
+    m.k = __fdiv_rn((float)v, mx);  // v_B / max
+    return m;
+}
+
+// Uniform velocity in [-vmax, vmax) with the minimum-speed rescale
+// (init_new_particles.cu:77-87, 147-167).
+__device__ __forceinline__ void birth_velocity(float u0, float u1, float u2, float vmax, float min_vel,
+                                               float* vx, float* vy, float* vz) {
+    const float lo = -vmax, hi = vmax;
+    const float span = __fsub_rn(hi, lo);
+    float x = __fadd_rn(lo, __fmul_rn(span, __fsub_rn(1.0f, u0)));
+    float y = __fadd_rn(lo, __fmul_rn(span, __fsub_rn(1.0f, u1)));
+    float z = __fadd_rn(lo, __fmul_rn(span, __fsub_rn(1.0f, u2)));
+    const float vsq = __fadd_rn(__fadd_rn(__fmul_rn(x, x), __fmul_rn(y, y)), __fmul_rn(z, z));
+    if (vsq < __fmul_rn(min_vel, min_vel) && vsq != 0.0f) {
+        const float rate = __fdiv_rn(min_vel, __fsqrt_rn(vsq));
+        x = __fmul_rn(x, rate);
+        y = __fmul_rn(y, rate);
+        z = __fmul_rn(z, rate);
+    }
+    *vx = x; *vy = y; *vz = z;
+}
+
+__device__ __forceinline__ void cell_centre_idx(int c, int G, float* x, float* y, float* z) {
+    int ix, iy, iz;
+    cell_xyz(c, G, &ix, &iy, &iz);
+    *x = __fadd_rn((float)ix, 0.5f);
+    *y = __fadd_rn((float)iy, 0.5f);
+    *z = __fadd_rn((float)iz, 0.5f);
+}
+
+// ---------------------------------------------------------------- births
+// initNewParticlesKernel1/2 (init_new_particles.cu:106-183). One thread per birth slot
+// finds its cell by binary search instead of each cell looping over its slots. Slots
+// beyond the last cell's range keep the previous frame's cell and association, exactly as
+// the reference leaves them unwritten. The penalty of penalizeStaticParticlesKernel
+// (resampling.cu:35-42) is recorded in the sign bit of the weight.
+__global__ void __launch_bounds__(kBlock)
+k_births(DevParams p, const FrameParams* __restrict__ fpp, const float* __restrict__ born,
+         const float* __restrict__ cum, Particles b) {
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= p.B) return;
+    const FrameParams fp = *fpp;
+    const SlotMap m = make_slotmap(cum, p.C, p.B);
+    int j = m.owner(s);
+    bool assoc;
+    int n, st;
+    if (j < p.C) {
+        st = m.start(j);
+        n = m.bound(j) - 1 - st + 1;
+        const int nu_A0 = (int)roundf(__fmul_rn((float)n, p.p_A));
+        assoc = s < st + nu_A0;
+        b.cell[s] = j;
+        b.assoc[s] = assoc ? 1 : 0;
+    } else {
+        j = b.cell[s];
+        j = clampv(j, 0, p.C - 1);
+        assoc = b.assoc[s] != 0;
+        n = m.count(j);
+    }
+    const int nu_A = (int)roundf(__fmul_rn((float)n, p.p_A));
+    const int nu_UA = n - nu_A;
+    const float bm = born[j];
+    float w;
+    if (assoc) {
+        w = nu_A > 0 ? __fdiv_rn(__fmul_rn(p.p_A, bm), (float)nu_A) : 0.0f;
+    } else {
+        w = nu_UA > 0 ? (float)((1.0 - (double)p.p_A) * (double)bm / (double)nu_UA) : 0.0f;
+    }
+    float x, y, z, vx, vy, vz;
+    cell_centre_idx(j, p.G, &x, &y, &z);
+    const U4 r = block(fp.seed, fp.frame, kBirthVel, (uint64_t)s, 0);
+    birth_velocity(u01(r.x), u01(r.y), u01(r.z), p.init_max_vel, p.min_vel, &vx, &vy, &vz);
+    const float sp = __fadd_rn(__fadd_rn(__fmul_rn(vx, vx), __fmul_rn(vy, vy)), __fmul_rn(vz, vz));
+    const bool slow = sp < __fmul_rn(p.min_vel, p.min_vel);
+    b.px[s] = x; b.py[s] = y; b.pz[s] = z;
+    b.vx[s] = vx; b.vy[s] = vy; b.vz[s] = vz;
+    b.w[s] = slow ? -w : w;
+}
+
+void launch_births(const DevParams& p, const FrameParams* fp, const float* born, const float* born_cum,
+                   Particles b, cudaStream_t st) {
+    if (p.B <= 0) return;
+    k_births<<<div_up(p.B, kBlock), kBlock, 0, st>>>(p, fp, born, born_cum, b);
+}
+
+// ---------------------------------------------------------------- first frame
+// initParticlesKernel1/2 (init_new_particles.cu:54-104) driven by the born-mass prefix
+// normalised to P (src/k3dom/dom.cu:60-76, src/dsphdmib/dom.cu:65-81).
+__global__ void __launch_bounds__(kBlock)
+k_init_particles(DevParams p, const FrameParams* __restrict__ fpp, const float* __restrict__ cum,
+                 Particles a) {
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= p.P) return;
+    const FrameParams fp = *fpp;
+    const SlotMap m = make_slotmap(cum, p.C, p.P);
+    int j = m.owner(s);
+    if (j < p.C) {
+        a.cell[s] = j;
+    } else {
+        j = clampv(a.cell[s], 0, p.C - 1);
+    }
+    float x, y, z, vx, vy, vz;
+    cell_centre_idx(j, p.G, &x, &y, &z);
+    const U4 r = block(fp.seed, fp.frame, kInitVel, (uint64_t)s, 0);
+    birth_velocity(u01(r.x), u01(r.y), u01(r.z), p.init_max_vel, p.min_vel, &vx, &vy, &vz);
+    a.px[s] = x; a.py[s] = y; a.pz[s] = z;
+    a.vx[s] = vx; a.vy[s] = vy; a.vz[s] = vz;
+    a.w[s] = __fdiv_rn(1.0f, (float)p.P);
+}
+
+void launch_init_particles(const DevParams& p, const FrameParams* fp, const float* born_cum,
+                           Particles a, cudaStream_t st) {
+    if (p.P <= 0) return;
+    k_init_particles<<<div_up(p.P, kBlock), kBlock, 0, st>>>(p, fp, born_cum, a);
+}
+
+// ---------------------------------------------------------------- resampling
+// Penalty (resampling.cu:13-36): weights flagged slow become 0, in place, as the reference
+// leaves them; the flags are cleared.
+__global__ void k_joint_prepare(int P, int B, Particles s, Particles b) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < P) {
+        const float w = s.w[i];
+        s.w[i] = signbit(w) ? 0.0f : w;
+    } else if (i < P + B) {
+        const float w = b.w[i - P];
+        b.w[i - P] = signbit(w) ? 0.0f : w;
+    }
+}
+
+void launch_joint_prepare(const DevParams& p, Particles s, Particles b, float* joint_w, cudaStream_t st) {
+    (void)joint_w;
+    if (p.P + p.B <= 0) return;
+    k_joint_prepare<<<div_up(p.P + p.B, kBlock), kBlock, 0, st>>>(p.P, p.B, s, b);
+}
+
+// Resampling draws as 24-bit keys of 1 - u: sorting the keys ascending orders the draws
+// u * joint_max ascending for any joint_max >= 0, so the draws can be sorted before the
+// weights exist (resamplingGenerateRandomNumbersKernel + thrust::sort, resampling.cu:38-53,
+// src/common/dom.cu:277-285).
+__global__ void k_draw_keys(int P, const FrameParams* __restrict__ fpp, uint32_t* keys) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= P) return;
+    const FrameParams fp = *fpp;
+    keys[i] = one_minus_u01_key(resample_word(fp.seed, fp.frame, (uint64_t)i));
+}
+
+void launch_draw_keys(const DevParams& p, const FrameParams* fp, uint32_t* keys, cudaStream_t st) {
+    if (p.P <= 0) return;
+    k_draw_keys<<<div_up(p.P, kBlock), kBlock, 0, st>>>(p.P, fp, keys);
+}
+
+constexpr int kResThreads = 256;
+
+// calc_resampled_indices + resamplingKernel (resampling.cu:55-89): ancestor =
+// lower_bound(acc, u) where acc's last element is replaced by the largest draw when they
+// differ; the resampled particle is gathered from the sorted persistent set or the birth
+// set with weight joint_max / P.
+__global__ void __launch_bounds__(kResThreads)
+k_resample(DevParams p, const float* __restrict__ cum, const uint32_t* __restrict__ dkeys,
+           Particles s, Particles b, Particles out, int* __restrict__ anc_out,
+           float* __restrict__ joint_max_out) {
+    __shared__ int s_lo, s_hi;
+    const int P = p.P, n = p.P + p.B;
+    const float jmax = cum[n - 1];
+    const float om_max = (float)dkeys[P - 1] * 5.9604644775390625e-08f;
+    const float rmax = __fadd_rn(0.0f, __fmul_rn(jmax, om_max));
+    const int k0 = blockIdx.x * kResThreads;
+    const int k1 = min(k0 + kResThreads, P) - 1;
+    auto acc = [&](int j) -> float { return j == n - 1 ? rmax : cum[j]; };
+    auto lower = [&](float u, int lo, int hi) -> int {  // first j in [lo, hi) with acc[j] >= u
+        while (lo < hi) {
+            int mid = (lo + hi) >> 1;
+            if (acc(mid) < u) lo = mid + 1; else hi = mid;
+        }
+        return lo;
+    };
+    auto draw = [&](int k) -> float {
+        const float om = (float)dkeys[k] * 5.9604644775390625e-08f;
+        return __fadd_rn(0.0f, __fmul_rn(jmax, om));
+    };
+    if (threadIdx.x == 0) s_lo = lower(draw(k0), 0, n);
+    if (threadIdx.x == 32) s_hi = lower(draw(k1), 0, n);
+    __syncthreads();
+    const int k = k0 + threadIdx.x;
+    if (k >= P) return;
+    int a = lower(draw(k), s_lo, min(s_hi + 1, n));
+    if (a > n - 1) a = n - 1;
+    const float new_w = __fdiv_rn(jmax, (float)P);
+    if (a < P) {
+        out.px[k] = s.px[a]; out.py[k] = s.py[a]; out.pz[k] = s.pz[a];
+        out.vx[k] = s.vx[a]; out.vy[k] = s.vy[a]; out.vz[k] = s.vz[a];
+        out.cell[k] = s.cell[a];
+        out.assoc[k] = s.assoc[a];
+    } else {
+        const int q = a - P;
+        out.px[k] = b.px[q]; out.py[k] = b.py[q]; out.pz[k] = b.pz[q];
+        out.vx[k] = b.vx[q]; out.vy[k] = b.vy[q]; out.vz[k] = b.vz[q];
+        out.cell[k] = b.cell[q];
+        out.assoc[k] = b.assoc[q];
+    }
+    out.w[k] = new_w;
+    anc_out[k] = a;
+    if (k == 0 && joint_max_out) *joint_max_out = jmax;
+}
+
+void launch_resample(const DevParams& p, const float* joint_cum, const uint32_t* sorted_draws,
+                     Particles s, const uint32_t* sorted_keys, Particles b, Particles out,
+                     int* ancestors, float* joint_max_out, cudaStream_t st) {
+    (void)sorted_keys;
+    if (p.P <= 0) return;
+    k_resample<<<div_up(p.P, kResThreads), kResThreads, 0, st>>>(p, joint_cum, sorted_draws, s, b, out,
+                                                                 ancestors, joint_max_out);
+}
+
+// ---------------------------------------------------------------- debug draws
+__global__ void k_debug_draws(uint64_t seed, int frame, int stage, long first, long count, float* dst) {
+    const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= count) return;
+    const uint64_t item = (uint64_t)(first + t);
+    if (stage == kPredict) {
+        float n[6];
+        predict_normals(seed, (uint32_t)frame, item, n);
+        for (int k = 0; k < 6; ++k) dst[t * 6 + k] = n[k];
+    } else if (stage == kInitVel || stage == kBirthVel) {
+        const U4 r = block(seed, (uint32_t)frame, (uint32_t)stage, item, 0);
+        dst[t * 3 + 0] = u01(r.x);
+        dst[t * 3 + 1] = u01(r.y);
+        dst[t * 3 + 2] = u01(r.z);
+    } else {
+        dst[t] = u01(resample_word(seed, (uint32_t)frame, item));
+    }
+}
+
+void launch_debug_draws(uint64_t seed, int frame, int stage, long first, long count, float* dst,
+                        cudaStream_t st) {
+    if (count <= 0) return;
+    k_debug_draws<<<div_up(count, kBlock), kBlock, 0, st>>>(seed, frame, stage, first, count, dst);
+}
+
+}  // namespace k3dom

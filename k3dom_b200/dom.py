@@ -1,0 +1,326 @@
+"""Python mirror of the reference's update API (dom::DOM_c / dom::DOM).
+
+Method names follow include/common/dom.h:54-94, include/k3dom/dom.h:19-29 and
+include/dsphdmib/dom.h:19-32 so code written against the reference reads the same; every
+call goes through the C ABI of libk3dom_b200.so (include/k3dom_b200.h).
+
+    p = params_from_yaml("k3dom", "config/k3dom.yaml", "config/complex.yaml")
+    dom = DOM(p, "k3dom")
+    dom.updatePose(x, y, z)
+    dom.updateGrid(t, xs, ys, zs)
+    occ = dom.get_cell_field("occ_mean")
+"""
+from __future__ import annotations
+
+import ctypes as C
+from typing import Optional
+
+import numpy as np
+
+from . import _native as N
+
+GRIDCELL_DTYPE = np.dtype([
+    ("start_idx", "<i4"), ("end_idx", "<i4"), ("mu_A", "<f4"), ("mu_UA", "<f4"), ("w_A", "<f4"),
+    ("w_UA", "<f4"), ("mean_x_vel", "<f4"), ("mean_y_vel", "<f4"), ("mean_z_vel", "<f4"),
+    ("likelihood", "<f4"), ("p_A", "<f4"), ("free_mass", "<f4"), ("static_mass", "<f4"),
+    ("dynamic_mass", "<f4"), ("occ_mass", "<f4"), ("pers_mass", "<f4"), ("pred_mass", "<f4"),
+])
+assert GRIDCELL_DTYPE.itemsize == 68
+
+MAPPOINT_DTYPE = np.dtype([(n, "<f4") for n in (
+    "x", "y", "z", "v_x", "v_y", "v_z", "occ_val", "dyn_val", "eval_aug", "dyn_aug")])
+
+_VARIANTS = {"k3dom": N.VARIANT_K3DOM, "dsphdmib": N.VARIANT_DSPHDMIB,
+             N.VARIANT_K3DOM: N.VARIANT_K3DOM, N.VARIANT_DSPHDMIB: N.VARIANT_DSPHDMIB}
+_SETS = {"persistent": N.PARTICLES_PERSISTENT, "sorted": N.PARTICLES_SORTED, "birth": N.PARTICLES_BIRTH}
+
+
+def _variant(v) -> int:
+    try:
+        return _VARIANTS[v]
+    except KeyError:
+        raise ValueError(f"unknown variant {v!r} (k3dom | dsphdmib)") from None
+
+
+def params_default(variant="k3dom") -> N.Params:
+    lib = N.load()
+    p = N.Params()
+    N.check(lib.k3dom_params_default(_variant(variant), C.byref(p)), "k3dom_params_default")
+    return p
+
+
+def params_from_yaml(variant, method_yaml: Optional[str], dataset_yaml: Optional[str] = None) -> N.Params:
+    lib = N.load()
+    p = N.Params()
+    enc = lambda s: s.encode() if s else None  # noqa: E731
+    N.check(lib.k3dom_params_from_yaml(_variant(variant), enc(method_yaml), enc(dataset_yaml), C.byref(p)),
+            "k3dom_params_from_yaml")
+    return p
+
+
+def node_config_from_yaml(variant, method_yaml, dataset_yaml=None) -> N.NodeConfig:
+    lib = N.load()
+    c = N.NodeConfig()
+    enc = lambda s: s.encode() if s else None  # noqa: E731
+    N.check(lib.k3dom_node_config_from_yaml(_variant(variant), enc(method_yaml), enc(dataset_yaml), C.byref(c)),
+            "k3dom_node_config_from_yaml")
+    return c
+
+
+def make_params(variant="k3dom", **kw) -> N.Params:
+    p = params_default(variant)
+    for k, v in kw.items():
+        if not hasattr(p, k):
+            raise AttributeError(f"k3dom_params has no field {k!r}")
+        setattr(p, k, v)
+    return p
+
+
+def _f32(a) -> np.ndarray:
+    return np.ascontiguousarray(np.asarray(a, dtype=np.float32))
+
+
+def _ptr(a) -> int:
+    return a.ctypes.data if a is not None else None
+
+
+def _is_cuda_tensor(x) -> bool:
+    return hasattr(x, "is_cuda") and getattr(x, "is_cuda") and hasattr(x, "data_ptr")
+
+
+class DOM:
+    """The K3DOM / DS-PHD/MIB grid (dom::DOM), on one GPU."""
+
+    def __init__(self, params: N.Params, variant="k3dom", device: int = 0):
+        self._lib = N.load()
+        self.variant = _variant(variant)
+        self.params = params
+        h = C.c_void_p()
+        N.check(self._lib.k3dom_create(C.byref(params), self.variant, int(device), C.byref(h)), "k3dom_create")
+        self._h = h
+        info = self.info()
+        self.grid_size = info.grid_size
+        self.grid_size_z = info.grid_size_z
+        self.grid_cell_count = info.grid_cell_count
+        self.particle_count = info.particle_count
+        self.new_born_particle_count = info.new_born_particle_count
+
+    # -- lifetime
+    def close(self) -> None:
+        if getattr(self, "_h", None):
+            self._lib.k3dom_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    # -- points
+    def _points(self, xs, ys=None, zs=None):
+        """Returns (px, py, pz, n, mem, keepalive)."""
+        if _is_cuda_tensor(xs):
+            import torch
+            if ys is None:
+                t = xs.to(torch.float32).contiguous()
+                assert t.dim() == 2 and t.shape[1] == 3
+                return t.data_ptr(), None, None, int(t.shape[0]), N.MEM_DEVICE, (t,)
+            tx, ty, tz = (v.to(torch.float32).contiguous() for v in (xs, ys, zs))
+            if not (tx.numel() == ty.numel() == tz.numel()):
+                raise ValueError("xs, ys, zs differ in length")
+            return tx.data_ptr(), ty.data_ptr(), tz.data_ptr(), int(tx.numel()), N.MEM_DEVICE, (tx, ty, tz)
+        if ys is None:
+            a = _f32(xs).reshape(-1, 3)
+            return _ptr(a), None, None, int(a.shape[0]), N.MEM_HOST, (a,)
+        x, y, z = _f32(xs), _f32(ys), _f32(zs)
+        if not (x.size == y.size == z.size):  # src/k3dom/dom.cu:83 asserts equal lengths
+            raise ValueError("xs, ys, zs differ in length")
+        return _ptr(x), _ptr(y), _ptr(z), int(x.size), N.MEM_HOST, (x, y, z)
+
+    # -- DOM_c interface (include/common/dom.h:57-94)
+    def updatePose(self, x: float, y: float, z: float) -> None:
+        N.check(self._lib.k3dom_update_pose(self._h, float(x), float(y), float(z)), "k3dom_update_pose")
+
+    def updateGrid(self, t: float, xs, ys=None, zs=None) -> None:
+        px, py, pz, n, mem, _keep = self._points(xs, ys, zs)
+        N.check(self._lib.k3dom_update_grid(self._h, float(t), px, py, pz, n, mem), "k3dom_update_grid")
+
+    def updateGridAsync(self, t: float, xs, ys=None, zs=None) -> None:
+        px, py, pz, n, mem, keep = self._points(xs, ys, zs)
+        self._keep = keep
+        N.check(self._lib.k3dom_update_grid_async(self._h, float(t), px, py, pz, n, mem), "k3dom_update_grid_async")
+
+    def synchronize(self) -> None:
+        N.check(self._lib.k3dom_synchronize(self._h), "k3dom_synchronize")
+
+    update_pose = updatePose
+    update_grid = updateGrid
+
+    def particlePrediction(self, dt: float) -> None:
+        N.check(self._lib.k3dom_particle_prediction(self._h, float(dt)), "particlePrediction")
+
+    def particleAssignment(self) -> None:
+        N.check(self._lib.k3dom_particle_assignment(self._h), "particleAssignment")
+
+    def gridCellOccupancyUpdate(self, dt: float, xs, ys=None, zs=None) -> None:
+        px, py, pz, n, mem, _keep = self._points(xs, ys, zs)
+        N.check(self._lib.k3dom_grid_cell_occupancy_update(self._h, float(dt), px, py, pz, n, mem),
+                "gridCellOccupancyUpdate")
+
+    def updatePersistentParticles(self) -> None:
+        N.check(self._lib.k3dom_update_persistent_particles(self._h), "updatePersistentParticles")
+
+    def initializeNewParticles(self) -> None:
+        N.check(self._lib.k3dom_initialize_new_particles(self._h), "initializeNewParticles")
+
+    def statisticalMoments(self) -> None:
+        N.check(self._lib.k3dom_statistical_moments(self._h), "statisticalMoments")
+
+    def resampling(self) -> None:
+        N.check(self._lib.k3dom_resampling(self._h), "resampling")
+
+    def initializeParticles(self, xs, ys=None, zs=None) -> None:
+        px, py, pz, n, mem, _keep = self._points(xs, ys, zs)
+        N.check(self._lib.k3dom_initialize_particles(self._h, px, py, pz, n, mem), "initializeParticles")
+
+    def finishFrame(self, t: float) -> None:
+        N.check(self._lib.k3dom_finish_frame(self._h, float(t)), "finishFrame")
+
+    def setFrameIndex(self, frame: int) -> None:
+        N.check(self._lib.k3dom_set_frame_index(self._h, int(frame)), "setFrameIndex")
+
+    # -- getters (include/common/dom.h:59-83)
+    def info(self) -> N.Info:
+        i = N.Info()
+        N.check(self._lib.k3dom_get_info(self._h, C.byref(i)), "k3dom_get_info")
+        return i
+
+    def getGridSize(self) -> int:
+        return self.grid_size
+
+    def getResolution(self) -> float:
+        return float(self.params.resolution)
+
+    def getCenterPositionX(self) -> float: return self.info().center_x
+    def getCenterPositionY(self) -> float: return self.info().center_y
+    def getCenterPositionZ(self) -> float: return self.info().center_z
+    def getSensorPositionX(self) -> float: return self.info().sensor_x
+    def getSensorPositionY(self) -> float: return self.info().sensor_y
+    def getSensorPositionZ(self) -> float: return self.info().sensor_z
+    def getIteration(self) -> int: return self.info().iteration
+
+    def indexToCoord(self, i: int):
+        x, y, z = C.c_float(), C.c_float(), C.c_float()
+        N.check(self._lib.k3dom_index_to_coord(self._h, int(i), C.byref(x), C.byref(y), C.byref(z)), "indexToCoord")
+        return x.value, y.value, z.value
+
+    def indexToCoordX(self, i: int) -> float: return self.indexToCoord(i)[0]
+    def indexToCoordY(self, i: int) -> float: return self.indexToCoord(i)[1]
+    def indexToCoordZ(self, i: int) -> float: return self.indexToCoord(i)[2]
+
+    # -- readback
+    def get_cell_field(self, name: str) -> np.ndarray:
+        out = np.empty(self.grid_cell_count, np.float32)
+        N.check(self._lib.k3dom_get_cell_field(self._h, N.CELL_FIELDS[name], _ptr(out), N.MEM_HOST), name)
+        return out
+
+    def get_cell_ranges(self):
+        s = np.empty(self.grid_cell_count, np.int32)
+        e = np.empty(self.grid_cell_count, np.int32)
+        N.check(self._lib.k3dom_get_cell_ranges(self._h, _ptr(s), _ptr(e), N.MEM_HOST), "cell_ranges")
+        return s, e
+
+    def get_gridcells(self) -> np.ndarray:
+        """The 68-byte dom::GridCell array the ROS node copies back (k3dom_node.cpp:131-132)."""
+        out = np.empty(self.grid_cell_count, GRIDCELL_DTYPE)
+        N.check(self._lib.k3dom_get_gridcell_aos(self._h, _ptr(out), N.MEM_HOST), "gridcell_aos")
+        return out
+
+    def get_mappoints(self) -> np.ndarray:
+        out = np.empty(self.grid_cell_count, MAPPOINT_DTYPE)
+        N.check(self._lib.k3dom_get_mappoints(self._h, _ptr(out), N.MEM_HOST), "mappoints")
+        return out
+
+    def set_cell_masses(self, free=None, static=None, dynamic=None, occ=None) -> None:
+        arrs = [None if a is None else _f32(a) for a in (free, static, dynamic, occ)]
+        for a in arrs:
+            if a is not None and a.size != self.grid_cell_count:
+                raise ValueError("cell array size mismatch")
+        N.check(self._lib.k3dom_set_cell_masses(self._h, *[_ptr(a) for a in arrs], N.MEM_HOST), "set_cell_masses")
+
+    def get_particles(self, which: str = "persistent") -> dict:
+        n = self.new_born_particle_count if which == "birth" else self.particle_count
+        pos = np.empty((n, 3), np.float32)
+        vel = np.empty((n, 3), np.float32)
+        w = np.empty(n, np.float32)
+        cell = np.empty(n, np.int32)
+        assoc = np.empty(n, np.uint8)
+        N.check(self._lib.k3dom_get_particles(self._h, _SETS[which], _ptr(pos), _ptr(vel), _ptr(w), _ptr(cell),
+                                              _ptr(assoc), N.MEM_HOST), "get_particles")
+        return {"pos": pos, "vel": vel, "weight": w, "cell": cell, "associated": assoc}
+
+    def set_particles(self, which: str, pos=None, vel=None, weight=None, cell=None, associated=None) -> None:
+        n = self.new_born_particle_count if which == "birth" else self.particle_count
+        pos = None if pos is None else _f32(pos).reshape(n, 3)
+        vel = None if vel is None else _f32(vel).reshape(n, 3)
+        weight = None if weight is None else _f32(weight).reshape(n)
+        cell = None if cell is None else np.ascontiguousarray(cell, np.int32).reshape(n)
+        associated = None if associated is None else np.ascontiguousarray(associated, np.uint8).reshape(n)
+        N.check(self._lib.k3dom_set_particles(self._h, _SETS[which], _ptr(pos), _ptr(vel), _ptr(weight), _ptr(cell),
+                                              _ptr(associated), N.MEM_HOST), "set_particles")
+
+    def sort_permutation(self) -> np.ndarray:
+        out = np.empty(self.particle_count, np.int32)
+        N.check(self._lib.k3dom_get_sort_permutation(self._h, _ptr(out), N.MEM_HOST), "sort_permutation")
+        return out
+
+    def ancestors(self) -> np.ndarray:
+        out = np.empty(self.particle_count, np.int32)
+        N.check(self._lib.k3dom_get_ancestors(self._h, _ptr(out), N.MEM_HOST), "ancestors")
+        return out
+
+    def resampling_state(self):
+        jc = np.empty(self.particle_count + self.new_born_particle_count, np.float32)
+        bc = np.empty(self.grid_cell_count, np.float32)
+        jm = np.empty(1, np.float32)
+        N.check(self._lib.k3dom_get_resampling_state(self._h, _ptr(jc), _ptr(bc), _ptr(jm), N.MEM_HOST),
+                "resampling_state")
+        return jc, bc, float(jm[0])
+
+    def stage_times(self) -> dict:
+        t = N.StageTimes()
+        N.check(self._lib.k3dom_get_stage_times(self._h, C.byref(t)), "stage_times")
+        return {k: getattr(t, k) for k, _ in t._fields_}
+
+    def set_timing(self, on: bool) -> None:
+        N.check(self._lib.k3dom_set_timing(self._h, 1 if on else 0), "set_timing")
+
+    def set_graph_mode(self, on: bool) -> None:
+        N.check(self._lib.k3dom_set_graph_mode(self._h, 1 if on else 0), "set_graph_mode")
+
+    def diagnostics(self) -> dict:
+        d = N.Diagnostics()
+        N.check(self._lib.k3dom_get_diagnostics(self._h, C.byref(d)), "diagnostics")
+        return {k: getattr(d, k) for k, _ in d._fields_}
+
+    def stream(self) -> int:
+        s = C.c_void_p()
+        N.check(self._lib.k3dom_get_stream(self._h, C.byref(s)), "get_stream")
+        return s.value or 0
+
+
+def debug_draws(seed: int, frame: int, stage: int, first: int, count: int) -> np.ndarray:
+    """The library's random draws (stage 1: 6 normals per item, 2/3: 3 uniforms, 4: 1 uniform)."""
+    lib = N.load()
+    per = 6 if stage == 1 else (1 if stage == 4 else 3)
+    out = np.empty(count * per, np.float32)
+    N.check(lib.k3dom_debug_draws(int(seed), int(frame), int(stage), int(first), int(count), _ptr(out), N.MEM_HOST),
+            "k3dom_debug_draws")
+    return out.reshape(count, per) if per > 1 else out

@@ -1,0 +1,155 @@
+"""Seeded synthetic LiDAR scenes that stand in for the reference's rosbags (data/*.bag are
+not in the reference checkout).
+
+A scene is a ground plane, static and moving axis-aligned cuboids, and an enclosing
+cylindrical wall at the sensor's maximum range (so every beam returns, as a bag replayed into
+the node would deliver a fixed-size cloud). A multi-beam LiDAR with uniform azimuth steps
+and evenly spread elevations casts rays from the sensor; ranges get Gaussian noise. Points
+are returned sensor-centred and map-axis aligned, the frame DOM::updateGrid expects
+(k3dom_node.cpp:73-85).
+
+The named configurations mirror the benchmark configurations of this project:
+  config0: 64x64x16 @ 0.2 m, P=262144, B=65536, one 32-beam scan of 30000 returns.
+  config1: 256x256x32 @ 0.1 m, P=4194304, B=1048576, 64-beam scans of 120000 returns,
+           ego motion 0-2 m/s, 20 static + 20 moving cuboids at 0-3 m/s, 10 Hz.
+  config2: config1's shape with the DS-PHD/MIB variant.
+"""
+from __future__ import annotations
+
+import dataclasses
+import math
+
+import numpy as np
+
+
+@dataclasses.dataclass
+class Box:
+    center: np.ndarray  # (3,) at t = 0, world frame [m]
+    half: np.ndarray    # (3,)
+    vel: np.ndarray     # (3,) [m/s]
+
+
+class Scene:
+    def __init__(self, seed: int = 0, n_static: int = 2, n_moving: int = 0, side=(1.0, 2.0), speed=(0.5, 1.5),
+                 ego_speed=(0.0, 0.0), extent: float = 6.0, ground_z: float = -1.5, max_range: float = 12.8,
+                 beams: int = 32, elev_deg=(-25.0, 15.0), range_noise: float = 0.02):
+        rng = np.random.Generator(np.random.PCG64(seed))
+        self.seed = seed
+        self.ground_z = ground_z
+        self.max_range = max_range
+        self.beams = beams
+        self.elev = np.deg2rad(np.linspace(elev_deg[0], elev_deg[1], beams))
+        self.range_noise = range_noise
+        self.boxes: list[Box] = []
+        for k in range(n_static + n_moving):
+            moving = k >= n_static
+            h = rng.uniform(side[0], side[1], size=3) / 2.0
+            # keep boxes out of a 1.5 m radius around the start position
+            while True:
+                c = rng.uniform(-extent, extent, size=2)
+                if np.hypot(*c) > 1.5 + h[:2].max():
+                    break
+            center = np.array([c[0], c[1], ground_z + h[2]])
+            v = np.zeros(3)
+            if moving:
+                sp = rng.uniform(speed[0], speed[1])
+                hd = rng.uniform(0.0, 2.0 * math.pi)
+                v = np.array([sp * math.cos(hd), sp * math.sin(hd), 0.0])
+            self.boxes.append(Box(center, h, v))
+        sp = rng.uniform(ego_speed[0], ego_speed[1])
+        hd = rng.uniform(0.0, 2.0 * math.pi)
+        self.ego_vel = np.array([sp * math.cos(hd), sp * math.sin(hd), 0.0])
+        self._noise_seed = int(rng.integers(0, 2**63 - 1))
+
+    def sensor_pos(self, t: float) -> np.ndarray:
+        return self.ego_vel * t
+
+    def scan(self, frame: int, t: float, n_points: int) -> tuple[np.ndarray, np.ndarray]:
+        """(sensor position in the world [m], points (n, 3) float32 relative to the sensor)."""
+        s = self.sensor_pos(t)
+        n_az = -(-n_points // self.beams)
+        az = np.linspace(0.0, 2.0 * math.pi, n_az, endpoint=False)
+        el = self.elev
+        ce, se = np.cos(el), np.sin(el)
+        d = np.stack([np.outer(ce, np.cos(az)), np.outer(ce, np.sin(az)), np.outer(se, np.ones_like(az))],
+                     axis=-1).reshape(-1, 3)[:n_points]
+        # enclosing wall at max_range (horizontal distance)
+        horiz = np.hypot(d[:, 0], d[:, 1])
+        t_hit = np.where(horiz > 1e-9, self.max_range / np.maximum(horiz, 1e-9), np.inf)
+        # ground
+        with np.errstate(divide="ignore", invalid="ignore"):
+            tg = np.where(d[:, 2] < 0, (self.ground_z - s[2]) / d[:, 2], np.inf)
+        t_hit = np.minimum(t_hit, np.where(tg > 0, tg, np.inf))
+        # cuboids (slab test)
+        for b in self.boxes:
+            c = b.center + b.vel * t
+            lo, hi = c - b.half - s, c + b.half - s
+            with np.errstate(divide="ignore", invalid="ignore"):
+                inv = 1.0 / d
+                t0 = lo * inv
+                t1 = hi * inv
+            tmin = np.nanmax(np.minimum(t0, t1), axis=1)
+            tmax = np.nanmin(np.maximum(t0, t1), axis=1)
+            ok = (tmax >= np.maximum(tmin, 0.0)) & np.isfinite(tmin)
+            t_hit = np.where(ok & (tmin > 0) & (tmin < t_hit), tmin, t_hit)
+        t_hit = np.minimum(t_hit, self.max_range / np.maximum(np.abs(d[:, 2]), 1e-9))
+        rng = np.random.Generator(np.random.PCG64([self._noise_seed, frame]))
+        r = t_hit + rng.normal(0.0, self.range_noise, size=t_hit.shape)
+        pts = (d * r[:, None]).astype(np.float32)
+        return s.astype(np.float32), pts
+
+
+@dataclasses.dataclass
+class Config:
+    name: str
+    variant: str
+    params: dict
+    scene: Scene
+    n_points: int
+    frames: int
+    dt: float
+
+
+def _k3dom_params(size, size_z, res, P, B, ls=0.3, sigma=0.1, variant="k3dom", seed=0, max_points=0):
+    """Parameter values of config/k3dom.yaml (or dsphdmib.yaml) in index units, as the node
+    converts them (k3dom_node.cpp:344-368)."""
+    p = dict(size=size, size_z=size_z, resolution=res, particle_count=P, new_born_particle_count=B,
+             mass_scale=2.5, persistence_prob=0.99, stddev_process_noise_position=0.01 / res,
+             stddev_process_noise_velocity=0.1 / res, birth_prob=0.02, stddev_velocity=4.0 / res,
+             init_max_velocity=5.0 / res, particle_min_vel=0.1 / res, sensor_off_x=0.0, sensor_off_y=0.0,
+             sensor_off_z=0.0, map_shift_thresh=int(np.float32(1.0) / np.float32(res)), prior_free=0.001,
+             prior_static=0.001, prior_dynamic=0.001, prior_occ=0.0, sigma=sigma, ls=ls, gamma=0.99,
+             max_range=50.0, meas_occ_stddev=0.1, seed=seed, max_points=max_points)
+    if variant == "dsphdmib":
+        p.update(particle_min_vel=0.0, prior_free=0.0, prior_static=0.0, prior_dynamic=0.0, prior_occ=0.0)
+    return p
+
+
+def config0(seed: int = 0) -> Config:
+    scene = Scene(seed=seed, n_static=0, n_moving=2, side=(1.0, 2.0), speed=(0.5, 1.5), extent=5.0,
+                  ground_z=-1.5, max_range=12.8, beams=32, range_noise=0.02)
+    return Config("config0", "k3dom", _k3dom_params(12.8, 3.2, 0.2, 262144, 65536, max_points=30000),
+                  scene, 30000, 2, 0.1)
+
+
+def config1(seed: int = 0, variant: str = "k3dom") -> Config:
+    scene = Scene(seed=seed, n_static=20, n_moving=20, side=(1.0, 2.0), speed=(0.0, 3.0), ego_speed=(0.0, 2.0),
+                  extent=11.0, ground_z=-1.5, max_range=25.6, beams=64, range_noise=0.02)
+    return Config("config1" if variant == "k3dom" else "config2", variant,
+                  _k3dom_params(25.6, 3.2, 0.1, 4194304, 1048576, variant=variant, max_points=120000),
+                  scene, 120000, 100, 0.1)
+
+
+def config2(seed: int = 0) -> Config:
+    return config1(seed, "dsphdmib")
+
+
+def small(seed: int = 0, variant: str = "k3dom", G: int = 32, Gz: int = 8, res: float = 0.2, P: int = 16384,
+          B: int = 4096, n_points: int = 2000, n_moving: int = 2, ego: float = 0.0) -> Config:
+    """A small scene for parity tests (the CPU oracle finishes in well under a second)."""
+    size, size_z = G * res, Gz * res
+    scene = Scene(seed=seed, n_static=1, n_moving=n_moving, side=(0.6, 1.2), speed=(0.5, 1.5),
+                  ego_speed=(ego, ego), extent=size / 2 - 0.5, ground_z=-0.6, max_range=size / 2 + 1.0,
+                  beams=16, elev_deg=(-30.0, 10.0), range_noise=0.02)
+    p = _k3dom_params(size, size_z, res, P, B, variant=variant, max_points=n_points)
+    return Config(f"small{G}", variant, p, scene, n_points, 4, 0.1)
