@@ -54,6 +54,16 @@ static U4 draw_block(uint64_t seed, uint32_t frame, uint32_t stage, uint64_t ite
 static float u01(uint32_t r) { return (float)((r >> 8) + 1u) * 5.9604644775390625e-08f; }
 static uint32_t pick(U4 v, int i) { return i == 0 ? v.x : (i == 1 ? v.y : (i == 2 ? v.z : v.w)); }
 
+/* Raw Philox4x32-10 block (for the published known-answer vectors). */
+void orc_philox_raw(const uint32_t* ctr, const uint32_t* key, uint32_t* out) {
+    U4 c = {ctr[0], ctr[1], ctr[2], ctr[3]};
+    U4 r = philox(c, key[0], key[1]);
+    out[0] = r.x;
+    out[1] = r.y;
+    out[2] = r.z;
+    out[3] = r.w;
+}
+
 /* Uniform draws: stage 2/3 -> 3 per item, stage 4 -> 1 per item. */
 void orc_uniforms(uint64_t seed, uint32_t frame, uint32_t stage, int64_t first, int64_t count, float* out) {
     for (int64_t t = 0; t < count; ++t) {
@@ -379,6 +389,145 @@ void orc_k3dom_update(int C, double dt, double gamma, double p_B, double mass_sc
         } else {
             o_mvx[c] = o_mvy[c] = o_mvz[c] = 0.0;
         }
+    }
+}
+
+/* ------------------------------------------------------------------ FP32 mirror of the reference */
+/* The reference's own FP32 expressions (mass_update.cu:12-150), brute force over every
+ * (cell, point) pair in input order, for pinning against the reference on small grids.
+ * cospif/sinpif/expf/powf come from libm in double and are rounded to float (within an ulp
+ * of CUDA's). nan_drop counts pairs whose radicand d_c^2 - d_proj^2 (:60) rounds negative in
+ * FP32 -- sqrtf gives NaN and the reference silently drops a term that FP64 keeps. */
+static float kernel_f(float d, float ls, float sigma) {
+    float a = 2.0f * d;
+    a = a / ls;
+    float c = (float)cos(M_PI * (double)a), s = (float)sin(M_PI * (double)a);
+    float t = 1.0f - d / ls;
+    float v = (2.0f + c) * t;
+    v = v / 3.0f;
+    v = v + s / (2.0f * 3.141592f);
+    v = sigma * v;
+    return v > 0.0f ? v : 0.0f;
+}
+
+void orc_bgki_ref32(const orc_grid* g, float ls, float sigma, int n, const float* xs, const float* ys, const float* zs,
+                    float* del_occ, float* del_free, int32_t* nan_drop) {
+    const int G = g->G, Gz = g->Gz;
+    const int64_t C = (int64_t)G * G * Gz;
+    const float res = g->res;
+#pragma omp parallel for schedule(dynamic, 64)
+    for (int64_t c = 0; c < C; ++c) {
+        int ix = (int)(c % G), iy = (int)((c % ((int64_t)G * G)) / G), iz = (int)(c / ((int64_t)G * G));
+        float x, y, z;
+        centre_f(g, ix, iy, iz, &x, &y, &z);
+        float occ = 0.0f, fr = 0.0f;
+        int drops = 0;
+        float dc = x * x;
+        dc = dc + y * y;
+        dc = dc + z * z;
+        dc = sqrtf(dc);
+        for (int i = 0; i < n; ++i) {
+            float xm = xs[i], ym = ys[i], zm = zs[i];
+            float a = (x - xm) * (x - xm);
+            a = a + (y - ym) * (y - ym);
+            a = a + (z - zm) * (z - zm);
+            float d = sqrtf(a);
+            if (d < ls) occ += kernel_f(d, ls, sigma);
+            float dm = xm * xm;
+            dm = dm + ym * ym;
+            dm = dm + zm * zm;
+            dm = sqrtf(dm);
+            float dp = x * xm;
+            dp = dp + y * ym;
+            dp = dp + z * zm;
+            dp = dp / dm;
+            float marg = fmaxf(0.9f * dm, dm - 2.0f * res);
+            if (dp <= 0.0f) {
+                d = dc;
+            } else if (dp < marg) {
+                float q = dc * dc - dp * dp;
+                if (q < 0.0f) drops++;
+                d = sqrtf(q);
+            } else if (dp < dm) {
+                float r = marg / dm;
+                float ex = (x - r * xm) * (x - r * xm);
+                ex = ex + (y - r * ym) * (y - r * ym);
+                ex = ex + (z - r * zm) * (z - r * zm);
+                d = sqrtf(ex);
+            } else {
+                d = ls + 1.0f;
+            }
+            if (d < ls) fr += kernel_f(d, ls, sigma);
+        }
+        del_occ[c] = occ;
+        del_free[c] = fr;
+        nan_drop[c] = drops;
+    }
+}
+
+/* gridCellPredictionUpdateKernel's per-cell body in FP32 (mass_update.cu:79-150, 163-181). */
+void orc_k3dom_update_ref32(int C, float dt, float gamma, float p_B, float mass_scale, const float* del_occ,
+                            const float* del_free, const float* free_in, const float* static_in, const float* dyn_in,
+                            const float* dyn_pred, float* o_free, float* o_static, float* o_dyn, float* o_born,
+                            float* o_pers) {
+    const float g = (float)pow((double)gamma, (double)dt);
+    for (int c = 0; c < C; ++c) {
+        float mf = free_in[c], ms = static_in[c], md = dyn_in[c], dp = dyn_pred[c];
+        float pt = (mf + md) * g;
+        ms = ms * g;
+        md = fminf(dp, fmaxf(0.0f, pt - ms));
+        mf = pt - md;
+        float dlf = del_free[c], dlo = del_occ[c];
+        if (dlf > 0.0f || dlo > 0.0f) {
+            float ds = dlf + dlo;
+            float ps = mf + ms;
+            ps = ps + md;
+            float cr = 1.0f - 2.0f / (1.0f + (float)exp((double)(2.0f * sqrtf(ds * ps) / mass_scale)));
+            float pdf = fmaxf(0.0f, dlf - dlo), pdo = fmaxf(0.0f, dlo - dlf);
+            float lD = cr * pdf;
+            lD = lD / ds;
+            lD = lD * md;
+            lD = lD / ps;
+            float lS = cr * pdf;
+            lS = lS / ds;
+            lS = lS * fmaxf(0.0f, (ms + md) - mf);
+            lS = lS / ps;
+            float lF = cr * pdo;
+            lF = lF / ds;
+            lF = lF * fmaxf(0.0f, mf - (ms + md));
+            lF = lF / ps;
+            float df = (lS / 2.0f) * ms;
+            df = df + lD * md;
+            df = df - lF * mf;
+            float dsm = -lS * ms;
+            float dd = lF * mf;
+            dd = dd + (lS / 2.0f) * ms;
+            dd = dd - lD * md;
+            mf = mf + df;
+            ms = ms + dsm;
+            md = md + dd;
+            float cr2 = 1.0f - 2.0f / (1.0f + (float)exp((double)(2.0f * (ms + md) / mass_scale)));
+            float ratio = (ms <= 0.0f || md < 0.0f) ? 0.0f : 1.0f / (1.0f + md / ms);
+            float beta = (1.0f - cr2) + cr2 * ratio;
+            ms = ms + beta * dlo;
+            md = md + (1.0f - beta) * dlo;
+            mf = mf + dlf;
+        }
+        float born;
+        if (dp <= 0.0f) born = md;
+        else if (pt <= dp) born = 0.0f;
+        else {
+            float a = md * p_B;
+            a = a * (pt - dp);
+            float b = p_B * (pt - dp);
+            b = dp + b;
+            born = a / b;
+        }
+        o_free[c] = mf;
+        o_static[c] = ms;
+        o_dyn[c] = md;
+        o_born[c] = born;
+        o_pers[c] = md - born;
     }
 }
 
