@@ -250,6 +250,8 @@ k3dom_status k3dom_set_frame_index(k3dom_handle* h, int32_t frame);
 typedef struct k3dom_stage_times {
     float predict_ms, assign_ms, occupancy_ms, persistent_ms, births_ms, resample_ms,
         total_ms;
+    float binning_ms;  /* part of occupancy_ms: ray lists */
+    float evidence_ms; /* part of occupancy_ms: evidence + cell update kernel(s) */
 } k3dom_stage_times;
 k3dom_status k3dom_get_stage_times(k3dom_handle* h, k3dom_stage_times* out);
 k3dom_status k3dom_set_timing(k3dom_handle* h, int enabled);
@@ -258,6 +260,7 @@ k3dom_status k3dom_set_timing(k3dom_handle* h, int enabled);
 typedef struct k3dom_diagnostics {
     int64_t nonfinite_points, ray_list_entries, ray_list_capacity, work_items;
     int32_t overflow;
+    int32_t kernel_launches_per_frame; /* kernels a steady-state frame enqueues */
 } k3dom_diagnostics;
 k3dom_status k3dom_get_diagnostics(k3dom_handle* h, k3dom_diagnostics* out);
 

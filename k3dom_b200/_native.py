@@ -92,13 +92,14 @@ class Info(C.Structure):
 class StageTimes(C.Structure):
     _fields_ = [(n, C.c_float) for n in (
         "predict_ms", "assign_ms", "occupancy_ms", "persistent_ms", "births_ms", "resample_ms",
-        "total_ms")]
+        "total_ms", "binning_ms", "evidence_ms")]
 
 
 class Diagnostics(C.Structure):
     _fields_ = [
         ("nonfinite_points", C.c_int64), ("ray_list_entries", C.c_int64),
         ("ray_list_capacity", C.c_int64), ("work_items", C.c_int64), ("overflow", C.c_int32),
+        ("kernel_launches_per_frame", C.c_int32),
     ]
 
 

@@ -19,6 +19,7 @@ __global__ void k_cells_init(DevParams p, CellState cs, CellWork cw) {
 }
 
 void launch_cells_init(const DevParams& p, CellState cs, CellWork cw, cudaStream_t st) {
+    ++g_launches;
     k_cells_init<<<div_up(p.C, kBlock), kBlock, 0, st>>>(p, cs, cw);
 }
 
@@ -64,17 +65,13 @@ __global__ void k_map_shift(DevParams p, CellState src, CellState dst, const int
 void launch_map_shift_full(const DevParams& p, CellState src, CellState dst, const int* s_start,
                            const int* s_end, int* d_start, int* d_end, int mx, int my, int mz,
                            cudaStream_t st) {
+    ++g_launches;
     k_map_shift<<<div_up(p.C, kBlock), kBlock, 0, st>>>(p, src, dst, s_start, s_end, d_start, d_end,
                                                          mx, my, mz);
 }
 
 
 // ---------------------------------------------------------------- readback
-__device__ __forceinline__ float calc_norm(float weight_sum, float rho_p) {
-    // update_persistent_particles.cu:12-15
-    return weight_sum > 0.0f ? __fdiv_rn(rho_p, weight_sum) : 0.0f;
-}
-
 struct CellView {
     float f, s, d, o, pers, pred, born, mvx, mvy, mvz, mu_A, mu_UA, w_A, w_UA, mocc, mfree, dlo, dlf;
     int start, end;
@@ -87,7 +84,8 @@ __device__ __forceinline__ void view_cell(const DevParams& p, int c, CellState c
     v.mvx = cs.mvx[c]; v.mvy = cs.mvy[c]; v.mvz = cs.mvz[c];
     v.start = cw.start[c]; v.end = cw.end[c];
     if (v.start >= 0) {
-        v.mu_UA = calc_norm(v.pred, v.pers);
+        // the factor the reweight applies: pers / pred (p_A = 0, so mu_A only multiplies 0)
+        v.mu_UA = cw.factor[c];
         v.mu_A = v.mu_UA;
     } else {
         v.mu_A = v.mu_UA = 0.0f;
@@ -160,6 +158,7 @@ __global__ void k_export_field(DevParams p, int field, CellState cs, CellWork cw
 
 void launch_export_field(const DevParams& p, int field, CellState cs, CellWork cw, const float* born_cum,
                          float* dst, cudaStream_t st) {
+    ++g_launches;
     k_export_field<<<div_up(p.C, kBlock), kBlock, 0, st>>>(p, field, cs, cw, born_cum, dst);
 }
 
@@ -189,6 +188,7 @@ __global__ void k_export_gridcell(DevParams p, CellState cs, CellWork cw, const 
 
 void launch_export_gridcell(const DevParams& p, CellState cs, CellWork cw, const float* born_cum, void* dst,
                             cudaStream_t st) {
+    ++g_launches;
     k_export_gridcell<<<div_up(p.C, kBlock), kBlock, 0, st>>>(p, cs, cw, born_cum,
                                                                reinterpret_cast<GridCellAoS*>(dst));
 }
@@ -218,6 +218,7 @@ __global__ void k_export_mappoints(DevParams p, float cx, float cy, float cz, Ce
 
 void launch_export_mappoints(const DevParams& p, float cx, float cy, float cz, CellState cs, CellWork cw,
                              float* dst, cudaStream_t st) {
+    ++g_launches;
     k_export_mappoints<<<div_up(p.C, kBlock), kBlock, 0, st>>>(p, cx, cy, cz, cs, cw, dst);
 }
 

@@ -83,6 +83,7 @@ struct k3dom_handle {
     bool shift_pending = false;
     int pending_shift[3] = {0, 0, 0};
     bool births_done = false;
+    int launches_per_frame = 0;
     bool initialized = false;
 
     // graph of the steady-state frame
@@ -384,6 +385,7 @@ cudaError_t enq_occupancy(k3dom_handle* h, bool first_frame) {
     cudaError_t e = build_ray_lists(p, h->fp_dev, h->pts, h->pts + M, h->pts + 2 * (size_t)M, h->rb, ds,
                                     h->status, h->st);
     if (e != cudaSuccess) return e;
+    rec(h, 7);
     if (ds)
         e = launch_ds_evidence(p, h->fp_dev, h->rb, h->cells(), h->cw, first_frame, h->status, h->num_sms, h->st);
     else
@@ -435,6 +437,7 @@ cudaError_t enq_init_particles(k3dom_handle* h) {
 // The steady-state frame (DOM::updateGrid's branch for updated_time > 0).
 cudaError_t enq_frame(k3dom_handle* h) {
     cudaError_t e;
+    const long l0 = g_launches;
     // resampling draws depend only on (seed, frame): produce them beside the frame
     if ((e = cudaEventRecord(h->ev_fork, h->st))) return e;
     if ((e = cudaStreamWaitEvent(h->st2, h->ev_fork, 0))) return e;
@@ -454,6 +457,7 @@ cudaError_t enq_frame(k3dom_handle* h) {
     if ((e = cudaStreamWaitEvent(h->st, h->ev_join, 0))) return e;
     if ((e = enq_resample(h, true))) return e;
     rec(h, 6);
+    h->launches_per_frame = (int)(g_launches - l0);
     return cudaSuccess;
 }
 
@@ -468,6 +472,8 @@ void read_times(k3dom_handle* h) {
     h->times.births_ms = t[4];
     h->times.resample_ms = t[5];
     cudaEventElapsedTime(&h->times.total_ms, h->ev_t[0], h->ev_t[6]);
+    cudaEventElapsedTime(&h->times.binning_ms, h->ev_t[2], h->ev_t[7]);
+    cudaEventElapsedTime(&h->times.evidence_ms, h->ev_t[7], h->ev_t[3]);
 }
 
 }  // namespace
@@ -1033,6 +1039,7 @@ k3dom_status k3dom_get_particles(k3dom_handle* h, k3dom_particle_set set, float*
     if (weight) {
         k3dom_status s = ensure_export(h, sizeof(float) * (size_t)n);
         if (s != K3DOM_OK) return s;
+        ++g_launches;
         k_abs_copy<<<div_up(n, 256), 256, 0, h->st>>>(q->w, (float*)h->export_buf, n);
         if ((e = cudaMemcpyAsync(weight, h->export_buf, sizeof(float) * (size_t)n, k, h->st))) return h->fail(e);
     }
@@ -1073,6 +1080,7 @@ k3dom_status k3dom_set_particles(k3dom_handle* h, k3dom_particle_set set, const 
         // a sorted set defines the cell ranges and sums: rebuild them from it in place
         if ((e = cudaMemcpyAsync(h->sorted_keys, q->cell, sizeof(int) * (size_t)n, cudaMemcpyDeviceToDevice, h->st)))
             return h->fail(e);
+        ++g_launches;
         k_iota<<<div_up(n, 256), 256, 0, h->st>>>(h->perm, n);
         if ((e = cudaMemsetAsync(h->cw.start, 0xFF, sizeof(int) * (size_t)h->dp.C, h->st))) return h->fail(e);
         if ((e = cudaMemsetAsync(h->cw.end, 0xFF, sizeof(int) * (size_t)h->dp.C, h->st))) return h->fail(e);
@@ -1135,6 +1143,7 @@ k3dom_status k3dom_get_diagnostics(k3dom_handle* h, k3dom_diagnostics* out) {
     out->ray_list_capacity = h->rb.capacity;
     out->work_items = (int64_t)st.work_items;
     out->overflow = (int32_t)st.overflow;
+    out->kernel_launches_per_frame = h->launches_per_frame;
     return K3DOM_OK;
 }
 

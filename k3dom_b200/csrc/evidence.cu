@@ -320,10 +320,12 @@ cudaError_t build_ray_lists(const DevParams& p, const FrameParams* fp, const flo
     const int T = rb.tiles;
     const uint32_t* dn_points =
         reinterpret_cast<const uint32_t*>(reinterpret_cast<const char*>(fp) + offsetof(FrameParams, n_points));
+    ++g_launches;
     k_ray_count<<<div_up(nmax, kBlock), kBlock, 0, st>>>(p, fp, g, xs, ys, zs, ds ? 1 : 0, rb.ray_a, rb.ray_b,
                                                          rb.ray_c, rb.counts, status);
     cudaError_t e = scan_u32_exclusive_dn(rb.counts, rb.offsets, nmax, dn_points, rb.scan_tmp, rb.total, st);
     if (e != cudaSuccess) return e;
+    ++g_launches;
     k_ray_emit<<<div_up(nmax, kBlock), kBlock, 0, st>>>(p, fp, g, xs, ys, zs, ds ? 1 : 0, rb.offsets, rb.total,
                                                         rb.capacity, rb.ekeys, rb.evals, status);
     int bits = 1;
@@ -331,10 +333,13 @@ cudaError_t build_ray_lists(const DevParams& p, const FrameParams* fp, const flo
     e = radix_sort_pairs_dn(rb.ekeys, rb.evals, rb.ekeys2, rb.evals2, rb.ekeys_alt, rb.evals_alt, rb.capacity,
                             rb.total + 2, bits, rb.hist, rb.scan_tmp, st);
     if (e != cudaSuccess) return e;
+    ++g_launches;
     k_tile_start<<<div_up(T + 1, kBlock), kBlock, 0, st>>>(rb.ekeys2, rb.total, T, rb.tile_start);
+    ++g_launches;
     k_tile_items<<<div_up(T, kBlock), kBlock, 0, st>>>(rb.tile_start, T, rb.tile_items);
     e = scan_u32_exclusive(rb.tile_items, rb.item_off, T, rb.scan_tmp, rb.item_off + T, st);
     if (e != cudaSuccess) return e;
+    ++g_launches;
     k_finish_lists<<<1, 1, 0, st>>>(rb.item_off, T, status, rb.total);
     return cudaGetLastError();
 }
@@ -388,94 +393,105 @@ __device__ __forceinline__ CellLoc locate(const DevParams& p, const TileShape& t
 }
 
 // ================================================================ K3DOM
-__device__ __forceinline__ float kernel_func(float d, float inv_ls, float sigma) {
-    // mass_update.cu:24-26 (note the reference's 3.141592 in the sine term)
-    const float x = d * inv_ls;
+// The sparse kernel of mass_update.cu:24-26,
+//   k(d) = max(0, sigma ((2 + cos(2 pi x)) (1 - x) / 3 + sin(2 pi x) / (2 * 3.141592))),  x = d / ls,
+// (the reference's truncated pi in the sine term is kept). Its two terms cancel up to ~16x over
+// the outer half of the support, so the angle 2x is carried in double (hi + lo, the FP32
+// sincospif of hi corrected to first order in lo) and the combination is formed in FP64.
+__device__ __forceinline__ double kernel_func(float d, double inv_ls, double sigma) {
+    const double x = (double)d * inv_ls;
+    const double t = 2.0 * x;
+    const float hi = (float)t;
+    const float lo = (float)(t - (double)hi);
     float s, c;
-    sincospif(2.0f * x, &s, &c);
-    const float v = sigma * ((2.0f + c) * (1.0f - x) * (1.0f / 3.0f) + s * (1.0f / (2.0f * 3.141592f)));
-    return fmaxf(0.0f, v);
+    sincospif(hi, &s, &c);
+    const float plo = 3.14159265358979f * lo;
+    const double cc = (double)c - (double)(plo * s);
+    const double ss = (double)s + (double)(plo * c);
+    const double v = sigma * ((2.0 + cc) * (1.0 - x) * (1.0 / 3.0) + ss * (1.0 / (2.0 * 3.141592)));
+    return v > 0.0 ? v : 0.0;
 }
 
-__device__ __forceinline__ float calc_credit(float mass, float mass_scale) {
+__device__ __forceinline__ double calc_credit(double mass, double mass_scale) {
     // mass_update.cu:12-14
-    return 1.0f - 2.0f / (1.0f + expf(2.0f * mass / mass_scale));
+    return 1.0 - 2.0 / (1.0 + exp(2.0 * mass / mass_scale));
 }
-__device__ __forceinline__ float positive_diff(float a, float b) { return fmaxf(0.0f, a - b); }
-__device__ __forceinline__ float calc_ratio(float numerator, float rest) {
-    return (numerator <= 0.0f || rest < 0.0f) ? 0.0f : (1.0f / (1.0f + rest / numerator));
+__device__ __forceinline__ double positive_diff(double a, double b) { return fmax(0.0, a - b); }
+__device__ __forceinline__ double calc_ratio(double numerator, double rest) {
+    return (numerator <= 0.0 || rest < 0.0) ? 0.0 : (1.0 / (1.0 + rest / numerator));
 }
 __device__ __forceinline__ float calc_norm(float weight_sum, float rho_p) {
     return weight_sum > 0.0f ? rho_p / weight_sum : 0.0f;
 }
 
 // gridCellPredictionUpdateKernel's per-cell body (mass_update.cu:163-181) plus the per-cell
-// updates of the persistent-particle and moment stages.
-__device__ void k3dom_cell_update(const DevParams& p, float dt, int c, float del_occ, float del_free,
+// updates of the persistent-particle and moment stages. Masses are stored in FP32; the update
+// is evaluated in FP64 (it has several cancelling differences) and rounded once.
+__device__ void k3dom_cell_update(const DevParams& p, float dt, int c, double del_occ, double del_free,
                                   CellState cs, CellWork cw, bool first_frame) {
-    float m_f = cs.free_m[c], m_s = cs.static_m[c], m_d = cs.dyn_m[c];
+    double m_f = cs.free_m[c], m_s = cs.static_m[c], m_d = cs.dyn_m[c];
     const int start = first_frame ? -1 : cw.start[c];
     const bool has = start >= 0;
-    const float dyn_pred = has ? cw.sum_w[c] : 0.0f;
-    const float g = powf(p.gamma, dt);
-    const float pred_total = (m_f + m_d) * g;
+    const double dyn_pred = has ? (double)cw.sum_w[c] : 0.0;
+    const double g = pow((double)p.gamma, (double)dt);
+    const double pred_total = (m_f + m_d) * g;
     // predict_mass (:79-84)
     m_s *= g;
-    m_d = fminf(dyn_pred, fmaxf(0.0f, pred_total - m_s));
+    m_d = fmin(dyn_pred, fmax(0.0, pred_total - m_s));
     m_f = pred_total - m_d;
     // update_mass (:86-139)
-    if (del_free > 0.0f || del_occ > 0.0f) {
-        const float del_sigma = del_free + del_occ;
-        const float prime_sigma = m_f + m_s + m_d;
-        float l_DtoF = 0.0f, l_StoFD = 0.0f, l_FtoD = 0.0f;
-        if (prime_sigma > 0.0f) {
-            const float credit = calc_credit(sqrtf(del_sigma * prime_sigma), p.mass_scale);
-            const float base_f = credit * positive_diff(del_free, del_occ) / del_sigma;
-            const float base_o = credit * positive_diff(del_occ, del_free) / del_sigma;
+    if (del_free > 0.0 || del_occ > 0.0) {
+        const double del_sigma = del_free + del_occ;
+        const double prime_sigma = m_f + m_s + m_d;
+        double l_DtoF = 0.0, l_StoFD = 0.0, l_FtoD = 0.0;
+        if (prime_sigma > 0.0) {
+            const double credit = calc_credit(sqrt(del_sigma * prime_sigma), p.mass_scale);
+            const double base_f = credit * positive_diff(del_free, del_occ) / del_sigma;
+            const double base_o = credit * positive_diff(del_occ, del_free) / del_sigma;
             l_DtoF = base_f * m_d / prime_sigma;
             l_StoFD = base_f * positive_diff(m_s + m_d, m_f) / prime_sigma;
             l_FtoD = base_o * positive_diff(m_f, m_s + m_d) / prime_sigma;
         }
-        const float diff_f = l_StoFD / 2.0f * m_s + l_DtoF * m_d - l_FtoD * m_f;
-        const float diff_s = -l_StoFD * m_s;
-        const float diff_d = l_FtoD * m_f + l_StoFD / 2.0f * m_s - l_DtoF * m_d;
+        const double diff_f = l_StoFD / 2.0 * m_s + l_DtoF * m_d - l_FtoD * m_f;
+        const double diff_s = -l_StoFD * m_s;
+        const double diff_d = l_FtoD * m_f + l_StoFD / 2.0 * m_s - l_DtoF * m_d;
         m_f += diff_f;
         m_s += diff_s;
         m_d += diff_d;
-        const float credit2 = calc_credit(m_s + m_d, p.mass_scale);
-        const float beta = (1.0f - credit2) + credit2 * calc_ratio(m_s, m_d);
+        const double credit2 = calc_credit(m_s + m_d, p.mass_scale);
+        const double beta = (1.0 - credit2) + credit2 * calc_ratio(m_s, m_d);
         m_s = m_s + beta * del_occ;
-        m_d = m_d + (1.0f - beta) * del_occ;
+        m_d = m_d + (1.0 - beta) * del_occ;
         m_f = m_f + del_free;
     }
     // separate_newborn_part (:141-150)
-    float born;
-    if (dyn_pred <= 0.0f) born = m_d;
-    else if (pred_total <= dyn_pred) born = 0.0f;
+    double born;
+    if (dyn_pred <= 0.0) born = m_d;
+    else if (pred_total <= dyn_pred) born = 0.0;
     else born = (m_d * p.p_B * (pred_total - dyn_pred)) / (dyn_pred + p.p_B * (pred_total - dyn_pred));
-    const float pers = m_d - born;
-    cs.free_m[c] = m_f;
-    cs.static_m[c] = m_s;
-    cs.dyn_m[c] = m_d;
-    cs.born_m[c] = born;
-    cs.pers_m[c] = pers;
-    cs.pred_m[c] = dyn_pred;
-    cw.del_occ[c] = del_occ;
-    cw.del_free[c] = del_free;
+    const double pers = m_d - born;
+    cs.free_m[c] = (float)m_f;
+    cs.static_m[c] = (float)m_s;
+    cs.dyn_m[c] = (float)m_d;
+    cs.born_m[c] = (float)born;
+    cs.pers_m[c] = (float)pers;
+    cs.pred_m[c] = (float)dyn_pred;
+    cw.del_occ[c] = (float)del_occ;
+    cw.del_free[c] = (float)del_free;
     if (first_frame) return;
     // updatePersistentParticlesKernel2: mu_UA = pers / pred (p_A = 0 -> the only factor)
-    const float mu_UA = has ? calc_norm(dyn_pred, pers) : 0.0f;
-    cw.factor[c] = mu_UA;
+    const double mu_UA = (has && dyn_pred > 0.0) ? pers / dyn_pred : 0.0;
+    cw.factor[c] = (float)mu_UA;
     // statisticalMomentsKernel2 with sum(w' v) = mu_UA * sum(w v)
-    float vx = 0.0f, vy = 0.0f, vz = 0.0f;
-    if (has && pers > 0.0f) {
-        vx = (mu_UA * cw.sum_wvx[c]) / pers;
-        vy = (mu_UA * cw.sum_wvy[c]) / pers;
-        vz = (mu_UA * cw.sum_wvz[c]) / pers;
+    double vx = 0.0, vy = 0.0, vz = 0.0;
+    if (has && pers > 0.0) {
+        vx = mu_UA * (double)cw.sum_wvx[c] / pers;
+        vy = mu_UA * (double)cw.sum_wvy[c] / pers;
+        vz = mu_UA * (double)cw.sum_wvz[c] / pers;
     }
-    cs.mvx[c] = vx;
-    cs.mvy[c] = vy;
-    cs.mvz[c] = vz;
+    cs.mvx[c] = (float)vx;
+    cs.mvy[c] = (float)vy;
+    cs.mvz[c] = (float)vz;
 }
 
 struct EvArgs {
@@ -531,7 +547,8 @@ __global__ void __launch_bounds__(kEvThreads) k_bgki(EvArgs A) {
     const FrameParams fp = *A.fp;
     const uint32_t total_items = A.item_off[A.T];
     const float ls2 = p.ls * p.ls;
-    const float inv_ls = 1.0f / p.ls;
+    const double inv_ls = 1.0 / (double)p.ls;
+    const double sigma = p.sigma;
     const int n_points = fp.n_points;
 
     for (;;) {
@@ -593,7 +610,7 @@ __global__ void __launch_bounds__(kEvThreads) k_bgki(EvArgs A) {
                     // occupied evidence (mass_update.cu:48-52)
                     const float vx = s2.x + dx, vy = s2.y + dy, vz = s2.z + dz;
                     const float d2o = vx * vx + vy * vy + vz * vz;
-                    if (d2o < ls2) ao += (double)kernel_func(sqrtf(d2o), inv_ls, p.sigma);
+                    if (d2o < ls2) ao += kernel_func(sqrtf(d2o), inv_ls, sigma);
                     // free evidence (:54-71)
                     const float dpar = dx * u.x + dy * u.y + dz * u.z;
                     if (s0.z + dpar < 0.0f) {  // d_proj < d_m
@@ -601,7 +618,7 @@ __global__ void __launch_bounds__(kEvThreads) k_bgki(EvArgs A) {
                                     qz = s1.z + dz - dpar * u.z;
                         const float al = fminf(s0.x + dpar, 0.0f) + fmaxf(s0.y + dpar, 0.0f);
                         const float d2f = qx * qx + qy * qy + qz * qz + al * al;
-                        if (d2f < ls2) af += (double)kernel_func(sqrtf(d2f), inv_ls, p.sigma);
+                        if (d2f < ls2) af += kernel_func(sqrtf(d2f), inv_ls, sigma);
                     }
                 }
                 __syncwarp();
@@ -646,8 +663,8 @@ __global__ void __launch_bounds__(kEvThreads) k_bgki(EvArgs A) {
 #pragma unroll
             for (int q = 0; q < NSBW; ++q) {
                 if (cell[q] >= 0) {
-                    const float dlo = (float)((double)fo[q] * A.fx_inv);
-                    const float dlf = (float)((double)ff[q] * A.fx_inv);
+                    const double dlo = (double)fo[q] * A.fx_inv;
+                    const double dlf = (double)ff[q] * A.fx_inv;
                     k3dom_cell_update(p, fp.dt, cell[q], dlo, dlf, A.cs, A.cw, A.first_frame != 0);
                 }
             }
@@ -971,10 +988,10 @@ cudaError_t launch_k3dom_evidence(const DevParams& p, const FrameParams* fp, Ray
     const int grid = num_sms * 2;
     const size_t sm = sizeof(BgkiSmem);
     switch (nsbw_of(rb)) {
-        case 1: k_bgki<1><<<grid, kEvThreads, sm, st>>>(A); break;
-        case 2: k_bgki<2><<<grid, kEvThreads, sm, st>>>(A); break;
-        case 4: k_bgki<4><<<grid, kEvThreads, sm, st>>>(A); break;
-        case 8: k_bgki<8><<<grid, kEvThreads, sm, st>>>(A); break;
+        case 1: ++g_launches; k_bgki<1><<<grid, kEvThreads, sm, st>>>(A); break;
+        case 2: ++g_launches; k_bgki<2><<<grid, kEvThreads, sm, st>>>(A); break;
+        case 4: ++g_launches; k_bgki<4><<<grid, kEvThreads, sm, st>>>(A); break;
+        case 8: ++g_launches; k_bgki<8><<<grid, kEvThreads, sm, st>>>(A); break;
         default: return cudaErrorInvalidValue;
     }
     return cudaGetLastError();
@@ -986,19 +1003,27 @@ cudaError_t launch_ds_evidence(const DevParams& p, const FrameParams* fp, RayBuf
     const int grid = num_sms * 4;
     switch (nsbw_of(rb)) {
         case 1:
+            ++g_launches;
             k_dsgrid<1, true><<<grid, kEvThreads, 0, st>>>(A);
+            ++g_launches;
             k_dsgrid<1, false><<<grid, kEvThreads, 0, st>>>(A);
             break;
         case 2:
+            ++g_launches;
             k_dsgrid<2, true><<<grid, kEvThreads, 0, st>>>(A);
+            ++g_launches;
             k_dsgrid<2, false><<<grid, kEvThreads, 0, st>>>(A);
             break;
         case 4:
+            ++g_launches;
             k_dsgrid<4, true><<<grid, kEvThreads, 0, st>>>(A);
+            ++g_launches;
             k_dsgrid<4, false><<<grid, kEvThreads, 0, st>>>(A);
             break;
         case 8:
+            ++g_launches;
             k_dsgrid<8, true><<<grid, kEvThreads, 0, st>>>(A);
+            ++g_launches;
             k_dsgrid<8, false><<<grid, kEvThreads, 0, st>>>(A);
             break;
         default:

@@ -115,8 +115,11 @@ static cudaError_t exact_scan_impl(TwoSeg in, long n, float* out, void* scratch,
     if (n <= 0) return cudaSuccess;
     int nt = exact_scan_tiles(n);
     u128* ts = reinterpret_cast<u128*>(scratch);
+    ++g_launches;
     exact_tile_sums<<<nt, kExThreads, 0, st>>>(in, n, ts);
+    ++g_launches;
     exact_tile_offsets<<<1, kExThreads, 0, st>>>(ts, nt);
+    ++g_launches;
     exact_apply<<<nt, kExThreads, 0, st>>>(in, n, ts, out);
     return cudaGetLastError();
 }

@@ -7,6 +7,10 @@
 
 namespace k3dom {
 
+// Kernel launches enqueued by this library (host counter; a frame's count is the difference
+// across it). Handles are single-threaded, as the reference's DOM is.
+extern long g_launches;
+
 // sort.cu
 int scan_u32_tiles(long n);
 cudaError_t scan_u32_exclusive(const uint32_t* in, uint32_t* out, long n, uint32_t* tmp,

@@ -66,6 +66,7 @@ __global__ void __launch_bounds__(kBlock) k_predict(DevParams p, const FramePara
 
 void launch_predict(const DevParams& p, const FrameParams* fp, Particles a, cudaStream_t st) {
     if (p.P <= 0) return;
+    ++g_launches;
     k_predict<<<div_up(p.P, kBlock), kBlock, 0, st>>>(p, fp, a);
 }
 
@@ -79,6 +80,7 @@ __global__ void k_shift_particles(int n, Particles a, int mx, int my, int mz) {
 
 void launch_shift_particles(const DevParams& p, Particles a, int mx, int my, int mz, cudaStream_t st) {
     if (p.P <= 0) return;
+    ++g_launches;
     k_shift_particles<<<div_up(p.P, kBlock), kBlock, 0, st>>>(p.P, a, mx, my, mz);
 }
 
@@ -210,6 +212,7 @@ void launch_gather_segsum(const DevParams& p, Particles a, Particles s, const ui
                           const uint32_t* perm, CellWork cw, cudaStream_t st) {
     if (p.P <= 0) return;
     const long warps = div_up(p.P, kSegRange);
+    ++g_launches;
     k_gather_segsum<<<div_up(warps, kSegWarps), kBlock, 0, st>>>(p, a, s, sorted_keys, perm, cw);
 }
 
@@ -239,6 +242,7 @@ k_reweight(DevParams p, Particles s, const uint32_t* __restrict__ keys, CellWork
 void launch_reweight(const DevParams& p, Particles s, const uint32_t* sorted_keys, CellWork cw,
                      cudaStream_t st) {
     if (p.P <= 0) return;
+    ++g_launches;
     k_reweight<<<div_up(p.P, kBlock), kBlock, 0, st>>>(p, s, sorted_keys, cw);
 }
 
@@ -355,6 +359,7 @@ k_births(DevParams p, const FrameParams* __restrict__ fpp, const float* __restri
 void launch_births(const DevParams& p, const FrameParams* fp, const float* born, const float* born_cum,
                    Particles b, cudaStream_t st) {
     if (p.B <= 0) return;
+    ++g_launches;
     k_births<<<div_up(p.B, kBlock), kBlock, 0, st>>>(p, fp, born, born_cum, b);
 }
 
@@ -386,6 +391,7 @@ k_init_particles(DevParams p, const FrameParams* __restrict__ fpp, const float* 
 void launch_init_particles(const DevParams& p, const FrameParams* fp, const float* born_cum,
                            Particles a, cudaStream_t st) {
     if (p.P <= 0) return;
+    ++g_launches;
     k_init_particles<<<div_up(p.P, kBlock), kBlock, 0, st>>>(p, fp, born_cum, a);
 }
 
@@ -406,6 +412,7 @@ __global__ void k_joint_prepare(int P, int B, Particles s, Particles b) {
 void launch_joint_prepare(const DevParams& p, Particles s, Particles b, float* joint_w, cudaStream_t st) {
     (void)joint_w;
     if (p.P + p.B <= 0) return;
+    ++g_launches;
     k_joint_prepare<<<div_up(p.P + p.B, kBlock), kBlock, 0, st>>>(p.P, p.B, s, b);
 }
 
@@ -422,6 +429,7 @@ __global__ void k_draw_keys(int P, const FrameParams* __restrict__ fpp, uint32_t
 
 void launch_draw_keys(const DevParams& p, const FrameParams* fp, uint32_t* keys, cudaStream_t st) {
     if (p.P <= 0) return;
+    ++g_launches;
     k_draw_keys<<<div_up(p.P, kBlock), kBlock, 0, st>>>(p.P, fp, keys);
 }
 
@@ -484,6 +492,7 @@ void launch_resample(const DevParams& p, const float* joint_cum, const uint32_t*
                      int* ancestors, float* joint_max_out, cudaStream_t st) {
     (void)sorted_keys;
     if (p.P <= 0) return;
+    ++g_launches;
     k_resample<<<div_up(p.P, kResThreads), kResThreads, 0, st>>>(p, joint_cum, sorted_draws, s, b, out,
                                                                  ancestors, joint_max_out);
 }
@@ -510,6 +519,7 @@ __global__ void k_debug_draws(uint64_t seed, int frame, int stage, long first, l
 void launch_debug_draws(uint64_t seed, int frame, int stage, long first, long count, float* dst,
                         cudaStream_t st) {
     if (count <= 0) return;
+    ++g_launches;
     k_debug_draws<<<div_up(count, kBlock), kBlock, 0, st>>>(seed, frame, stage, first, count, dst);
 }
 

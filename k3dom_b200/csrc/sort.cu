@@ -17,6 +17,8 @@
 
 namespace k3dom {
 
+long g_launches = 0;
+
 constexpr int kSortThreads = 256;
 constexpr int kSortItems = 16;
 constexpr int kSortTile = kSortThreads * kSortItems;  // 4096
@@ -104,8 +106,11 @@ cudaError_t scan_u32_exclusive_dn(const uint32_t* in, uint32_t* out, long nmax, 
                                   uint32_t* tmp, uint32_t* total, cudaStream_t st) {
     if (nmax <= 0) return cudaSuccess;
     int nt = scan_u32_tiles(nmax);
+    ++g_launches;
     scan_u32_tile_sums<<<grid_for(nt), kScanThreads, 0, st>>>(in, nmax, dn, tmp);
+    ++g_launches;
     scan_u32_tile_offsets<<<1, kScanThreads, 0, st>>>(tmp, nmax, dn, total);
+    ++g_launches;
     scan_u32_apply<<<grid_for(nt), kScanThreads, 0, st>>>(in, nmax, dn, tmp, out);
     return cudaGetLastError();
 }
@@ -262,9 +267,11 @@ static cudaError_t radix_pass(const uint32_t* kin, const uint32_t* vin, uint32_t
     const long hn = (long)nt << BITS;
     // the last word of hist holds the live histogram length (device count case)
     uint32_t* hist_len = hist + hn;
+    ++g_launches;
     radix_upsweep<BITS><<<grid_for(nt), kSortThreads, 0, st>>>(kin, nmax, dn, shift, hist, dn ? hist_len : nullptr);
     cudaError_t e = scan_u32_exclusive_dn(hist, hist, hn, dn ? hist_len : nullptr, scan_tmp, nullptr, st);
     if (e != cudaSuccess) return e;
+    ++g_launches;
     radix_downsweep<BITS><<<grid_for(nt), kSortThreads, sizeof(RadixSmem<BITS>), st>>>(kin, vin, nmax, dn, shift,
                                                                                        hist, kout, vout);
     return cudaGetLastError();
