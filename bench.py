@@ -1,0 +1,458 @@
+#!/usr/bin/env python
+"""Benchmark: K3DOM update frames/s on B200 at 2.1M voxels / 4.2M particles / 120k points.
+
+Workload (one step = one steady-state frame of the K3DOM 10 Hz sequence): 256x256x32 grid at
+0.1 m (2,097,152 voxels), 4,194,304 persistent + 1,048,576 new-born particles, 64-beam scans of
+120,000 returns, ego motion 0-2 m/s, 20 static + 20 moving cuboids (k3dom_b200.scene.config1).
+Seeded synthetic scans stand in for the reference's rosbags (not in its checkout).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference|reference-gpu]
+                    [--variant k3dom|dsphdmib]
+
+ours           the library through its C ABI: `value` is device-timed frames/s with the scans
+               resident in HBM (graph-captured frames); `e2e` is frames/s through
+               k3dom_update_grid with the scan in pinned host memory and the per-voxel occupancy
+               read back to pinned host memory every frame (wall clock).
+reference      the CPU baseline of the path: the reference has no CPU implementation, so its
+               restatement (oracle/, FP64, OpenMP over all host threads) runs the same frames.
+reference-gpu  the reference's own CUDA update (oracle/_ref, built from its sources), frames/s
+               on this GPU (not used by the driver; reported in the design notes).
+
+Multi-GPU: the single-scene update does not shard (replicas only); with torchrun every rank
+runs an independent scene (weak scaling), timed on the device, max over ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+METRIC = "update frames/s @2.1M voxels,4M particles; batched vs plain; grad-step ms"
+UNIT = "frames/s"
+PEAKS_FILE = ROOT / "MEASURED_PEAKS.json"
+FALLBACK_HBM_GBS = 6650.0
+NOMINAL_FP32_TFLOPS = 148 * 128 * 2 * 1.965e9 / 1e12  # 74.4: no measured FP32 peak exists
+FLOP_PER_EVAL = 20  # distance (8 + sqrt) + sparse kernel (2x/ls, cospi, sinpi, 7 arithmetic)
+
+
+def log(*a):
+    print(*a, file=sys.stderr, flush=True)
+
+
+# ------------------------------------------------------------------ clocks
+class ClockSampler:
+    """nvidia-smi samples during the timed region (clocks, power, throttle reasons)."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_id: str):
+        self.gpu = gpu_id
+        self.proc = None
+        self.lines: list[str] = []
+        self.t = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "100"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except (FileNotFoundError, OSError):
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self) -> dict:
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        self.t.join(timeout=2)
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [x.strip() for x in ln.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                mx.append(float(parts[2]))
+            except ValueError:
+                continue
+            for nm, v in zip(names, parts[5:9]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+# ------------------------------------------------------------------ distributed plumbing
+def dist_setup(gpus: int):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
+                                device_id=torch.device("cuda", local))
+        return rank, world, local, dist
+    return 0, 1, local, None
+
+
+def barrier(dist):
+    if dist is not None:
+        dist.barrier()
+
+
+def max_over_ranks(x: float, dist) -> float:
+    if dist is None:
+        return x
+    import torch
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def sum_over_ranks(x: float, dist) -> float:
+    if dist is None:
+        return x
+    import torch
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.SUM)
+    return float(t.item())
+
+
+def read_peaks() -> tuple[float, str]:
+    try:
+        d = json.loads(PEAKS_FILE.read_text())
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return FALLBACK_HBM_GBS, "fallback"
+
+
+def hbm_bytes_particle_stages(P: int, B: int, C: int, N: int) -> float:
+    """Algorithmic bytes of the HBM-bound stages per frame (minimal FP32 SoA)."""
+    return (60 * P + 52 * P + 56 * P + 4 * P + 8 * C + 36 * C + 4 * P + 12 * N + 12 * P + 4 * C + 16 * P + 12 * C
+            + 8 * C + 36 * B + 12 * (P + B) + 32 * P + 60 * P)
+
+
+# ------------------------------------------------------------------ frames
+def make_frames(cfg, n_frames: int):
+    frames = []
+    for f in range(n_frames):
+        t = 0.1 + f * cfg.dt
+        s, pts = cfg.scene.scan(f, t, cfg.n_points)
+        frames.append((t, s, np.ascontiguousarray(pts)))
+    return frames
+
+
+def cpu_oracle_frames(cfg, variant: str, frames, steps: int, warmup: int, budget_s: float):
+    """Time steady-state frames of the CPU oracle. Returns (frames/s, sample note, threads)."""
+    from oracle import binding as O
+    from oracle.frame import OracleDOM
+    dom = OracleDOM(_params_struct(variant, dict(cfg.params)), variant)
+    t, s, pts = frames[0]
+    dom.update_pose(*s)
+    dom.update_grid(t, pts)
+    idx = 1
+    for _ in range(warmup):
+        t, s, pts = frames[idx]
+        idx += 1
+        dom.update_pose(*s)
+        t0 = time.perf_counter()
+        dom.update_grid(t, pts)
+    times = []
+    t_start = time.perf_counter()
+    for _ in range(steps):
+        t, s, pts = frames[idx]
+        idx += 1
+        dom.update_pose(*s)
+        t0 = time.perf_counter()
+        dom.update_grid(t, pts)
+        times.append(time.perf_counter() - t0)
+        if time.perf_counter() - t_start > budget_s:
+            break
+    fps = len(times) / sum(times)
+    note = (f"{len(times)} full steady-state frame(s) of the {cfg.name} sequence on the CPU oracle "
+            f"(FP64 continuous math, all stages), {O.oracle().orc_num_threads()} OpenMP threads")
+    return fps, note, int(O.oracle().orc_num_threads()), len(times)
+
+
+def _params_struct(variant, params):
+    from k3dom_b200 import _native as N
+    p = N.Params()
+    # defaults without the library (the CPU arm must not need a GPU)
+    for k, v in params.items():
+        setattr(p, k, v)
+    return p
+
+
+def scene_cfg(variant: str, rank: int):
+    from k3dom_b200 import scene
+    cfg = scene.config1(seed=1000 + rank, variant=variant)
+    cfg.params["seed"] = 20240 + rank
+    return cfg
+
+
+# ------------------------------------------------------------------ arms
+def run_ours(args):
+    import torch
+
+    import k3dom_b200 as K
+    rank, world, local, dist = dist_setup(args.gpus)
+    torch.cuda.set_device(local)
+    cfg = scene_cfg(args.variant, rank)
+    W, Kst = args.warmup, args.steps
+    n_frames = 1 + W + Kst + 2 + Kst + 1 + Kst
+    log(f"[rank {rank}] generating {n_frames} scans of {cfg.n_points} points")
+    frames = make_frames(cfg, n_frames)
+    p = K.make_params(args.variant, **cfg.params)
+    dom = K.DOM(p, args.variant, device=local)
+    C_, P, B = dom.grid_cell_count, dom.particle_count, dom.new_born_particle_count
+    # scans resident in HBM for the device-timed run
+    dev_pts = [torch.from_numpy(f[2]).to(f"cuda:{local}") for f in frames]
+    torch.cuda.synchronize()
+    idx = 0
+
+    def step_device(i):
+        t, s, _ = frames[i]
+        dom.updatePose(*s)
+        dom.updateGridAsync(t, dev_pts[i])
+
+    # first frame (initialisation) + warm-up, graph captured on the first steady frame
+    dom.set_graph_mode(True)
+    dom.updatePose(*frames[0][1])
+    dom.updateGrid(frames[0][0], dev_pts[0])
+    idx = 1
+    for _ in range(W):
+        step_device(idx)
+        idx += 1
+    dom.synchronize()
+    stream = torch.cuda.ExternalStream(dom.stream())
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    props = torch.cuda.get_device_properties(local)
+    uuid = getattr(props, "uuid", None)
+    gpu_id = f"GPU-{uuid}" if uuid is not None else str(local)
+    sampler = ClockSampler(gpu_id) if rank == 0 else None
+    barrier(dist)
+    torch.cuda.synchronize()
+    if sampler:
+        sampler.start()
+        time.sleep(0.3)
+    ev0.record(stream)
+    for _ in range(Kst):
+        step_device(idx)
+        idx += 1
+    ev1.record(stream)
+    dom.synchronize()
+    torch.cuda.synchronize()
+    barrier(dist)
+    clocks = sampler.stop() if sampler else None
+    ms = ev0.elapsed_time(ev1) / Kst
+    ms_max = max_over_ranks(ms, dist)
+    diag = dom.diagnostics()
+    launches = int(diag["kernel_launches_per_frame"])
+
+    # per-stage device times and the evidence kernel's work (events on the handle's stream)
+    dom.set_timing(True)
+    st_acc, evals = [], []
+    for _ in range(2):
+        step_device(idx)
+        idx += 1
+        dom.synchronize()
+    for _ in range(min(Kst, 10)):
+        step_device(idx)
+        idx += 1
+        dom.synchronize()
+        st_acc.append(dom.stage_times())
+        evals.append(dom.diagnostics()["kernel_evaluations"])
+    dom.set_timing(False)
+    stage = {k: float(np.mean([s[k] for s in st_acc])) for k in st_acc[0]}
+
+    # end to end through the C ABI: pinned host scan in, per-voxel occupancy out, every frame
+    host_pts = [torch.from_numpy(f[2]).pin_memory() for f in frames]
+    occ_out = torch.empty(C_, dtype=torch.float32).pin_memory()
+    occ_ptr = occ_out.data_ptr()
+    lib = dom._lib
+    from k3dom_b200 import _native as N
+    field = N.CELL_FIELDS["occ_mean" if args.variant == "k3dom" else "occ_prob"]
+    barrier(dist)
+    t0 = time.perf_counter()
+    n_e2e = 0
+    while n_e2e < Kst and idx < len(frames):
+        t, s, _ = frames[idx]
+        hp = host_pts[idx].numpy()
+        dom.updatePose(*s)
+        N.check(lib.k3dom_update_grid(dom._h, float(t), hp.ctypes.data, None, None, hp.shape[0], N.MEM_HOST),
+                "update_grid")
+        N.check(lib.k3dom_get_cell_field(dom._h, field, occ_ptr, N.MEM_HOST), "get_cell_field")
+        idx += 1
+        n_e2e += 1
+    e2e_s = time.perf_counter() - t0
+    e2e_s = max_over_ranks(e2e_s, dist)
+    e2e_fps = world * n_e2e / e2e_s
+
+    value = world * 1000.0 / ms_max
+    out = None
+    if rank == 0:
+        hbm_peak, peak_src = read_peaks()
+        ev_ms = stage["evidence_ms"]
+        n_evals = float(np.mean(evals))
+        achieved_tflops = n_evals * FLOP_PER_EVAL / (ev_ms * 1e-3) / 1e12
+        part_ms = stage["predict_ms"] + stage["assign_ms"] + stage["persistent_ms"] + stage["births_ms"] + \
+            stage["resample_ms"]
+        part_bytes = hbm_bytes_particle_stages(P, B, C_, cfg.n_points)
+        traffic = None
+        tr_file = ROOT / "profiles" / "bgki_traffic.json"
+        if tr_file.exists():
+            try:
+                traffic = json.loads(tr_file.read_text()).get("dram_bytes_per_launch")
+            except Exception:
+                traffic = None
+        out = {
+            "metric": METRIC, "value": round(value, 3), "unit": UNIT, "n_gpus": world, "steps": Kst,
+            "warmup": W, "ms_per_step": round(ms_max, 4), "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32 (f64 accumulation)", "data": "synthetic (seeded LiDAR scans)",
+            "config": {
+                "workload": f"{cfg.name}: {args.variant} steady-state frame, 256x256x32 voxels @0.1 m, "
+                            f"P={P}, B={B}, {cfg.n_points} points/scan, ego motion, 10 Hz",
+                "voxels": C_, "particles": P, "new_born": B, "points_per_frame": cfg.n_points,
+                "parallelism": f"replicas x{world} (independent scenes)",
+                "l2": "state > L2 (about 1 GB of particle/cell arrays touched per frame)",
+                "graph": True,
+            },
+            "e2e": {"value": round(e2e_fps, 3), "unit": UNIT, "h2d_bytes_per_step": int(cfg.n_points * 12),
+                    "d2h_bytes_per_step": int(C_ * 4)},
+            "gpu_launches": launches * Kst,
+            "clocks": clocks,
+            "roofline": {
+                "kernel": "k_bgki (sparse BGKI evidence + fused cell update)",
+                "bound": "fp32", "achieved": round(achieved_tflops, 3), "peak": round(NOMINAL_FP32_TFLOPS, 1),
+                "unit": "TFLOP/s", "frac": round(achieved_tflops / NOMINAL_FP32_TFLOPS, 4), "traffic": traffic,
+                "peak_source": "nominal FP32 (148 SMs x 128 lanes x 2 x 1.965 GHz); no measured FP32 peak",
+                "work": f"{n_evals:.4g} in-support kernel evaluations x {FLOP_PER_EVAL} FLOP per frame",
+                "launch_ms": round(ev_ms, 4),
+            },
+            "roofline_hbm": {
+                "kernels": "particle stages (predict, sort, gather+sums, reweight, births, resampling)",
+                "bound": "hbm", "achieved": round(part_bytes / (part_ms * 1e-3) / 1e9, 1), "peak": hbm_peak,
+                "unit": "GB/s", "frac": round(part_bytes / (part_ms * 1e-3) / 1e9 / hbm_peak, 4),
+                "peak_source": peak_src, "algorithmic_bytes": int(part_bytes), "time_ms": round(part_ms, 4),
+            },
+            "stage_ms": {k: round(v, 4) for k, v in stage.items()},
+        }
+        if world == 1 and not args.no_cpu_baseline:
+            fps, note, cores, n = cpu_oracle_frames(cfg, args.variant, frames, 1, 0, budget_s=60.0)
+            out["cpu_baseline"] = {"value": round(fps, 5), "unit": UNIT, "cores": cores, "kind": "port",
+                                   "sample": note}
+    dom.close()
+    if dist is not None:
+        dist.destroy_process_group()
+    if out is not None:
+        print(json.dumps(out), flush=True)
+
+
+def run_reference_cpu(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    cfg = scene_cfg(args.variant, 0)
+    W = min(args.warmup, 1)
+    frames = make_frames(cfg, 1 + W + args.steps)
+    fps, note, cores, n = cpu_oracle_frames(cfg, args.variant, frames, args.steps, W, budget_s=240.0)
+    out = {
+        "impl": "reference", "metric": METRIC, "value": round(fps, 5), "unit": UNIT, "n_gpus": args.gpus,
+        "steps": n, "warmup": W, "ms_per_step": round(1000.0 / fps, 2), "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded LiDAR scans)",
+        "config": {"workload": f"{cfg.name}: {args.variant} steady-state frame, 256x256x32 voxels @0.1 m, "
+                               f"P={cfg.params['particle_count']}, B={cfg.params['new_born_particle_count']}, "
+                               f"{cfg.n_points} points/scan", "parallelism": "CPU"},
+        "cpu_baseline": {"value": round(fps, 5), "unit": UNIT, "cores": cores, "kind": "port",
+                         "sample": note + "; the reference has no CPU implementation of the update"},
+        "e2e": {"value": round(fps, 5), "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(out), flush=True)
+
+
+def run_reference_gpu(args):
+    """The reference's own CUDA update (unmodified sources behind oracle/ref_harness.cu)."""
+    import torch
+
+    import k3dom_b200 as K
+    from oracle.binding import Reference
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    cfg = scene_cfg(args.variant, 0)
+    frames = make_frames(cfg, 1 + args.warmup + args.steps)
+    p = K.make_params(args.variant, **cfg.params)
+    ref = Reference(p, args.variant)
+    t, s, pts = frames[0]
+    ref.update_pose(*s)
+    ref.update_grid(t, pts)
+    for i in range(1, 1 + args.warmup):
+        t, s, pts = frames[i]
+        ref.update_pose(*s)
+        ref.update_grid(t, pts)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for i in range(1 + args.warmup, len(frames)):
+        t, s, pts = frames[i]
+        ref.update_pose(*s)
+        ref.update_grid(t, pts)  # ends with cudaDeviceSynchronize (src/k3dom/dom.cu:47)
+    wall = time.perf_counter() - t0
+    ref.close()
+    fps = args.steps / wall
+    print(json.dumps({"impl": "reference-gpu", "metric": METRIC, "value": round(fps, 4), "unit": UNIT,
+                      "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+                      "ms_per_step": round(1000 / fps, 3), "higher_is_better": True,
+                      "config": {"workload": f"{cfg.name}: {args.variant} steady-state frame, reference CUDA "
+                                             "(its own updateGrid, host vectors in, synchronising)"}}), flush=True)
+
+
+def main(argv=None):
+    ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", choices=["ours", "reference", "reference-gpu"], default="ours")
+    ap.add_argument("--variant", choices=["k3dom", "dsphdmib"], default="k3dom")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args(argv)
+    if args.warmup < 3 and args.impl == "ours":
+        log("warmup < 3 raised to 3")
+        args.warmup = 3
+    if args.impl == "ours":
+        run_ours(args)
+    elif args.impl == "reference":
+        run_reference_cpu(args)
+    else:
+        run_reference_gpu(args)
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

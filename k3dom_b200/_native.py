@@ -99,7 +99,7 @@ class Diagnostics(C.Structure):
     _fields_ = [
         ("nonfinite_points", C.c_int64), ("ray_list_entries", C.c_int64),
         ("ray_list_capacity", C.c_int64), ("work_items", C.c_int64), ("overflow", C.c_int32),
-        ("kernel_launches_per_frame", C.c_int32),
+        ("kernel_launches_per_frame", C.c_int32), ("kernel_evaluations", C.c_int64),
     ]
 
 

@@ -44,6 +44,7 @@ struct DevStatus {
     unsigned int work_counter;  // dynamic work queue of the evidence kernels
     unsigned int work_counter2;
     unsigned int pad;
+    unsigned long long kernel_evals;  // in-support sparse-kernel evaluations of the last frame
 };
 
 // Particle set, SoA (ParticlesSoA, include/common/dom_types.h:76-167; post_weight is

@@ -192,8 +192,14 @@ cudaError_t alloc_ray_buffers(k3dom_handle* h, int max_points) {
         (e = h->alloc(&rb.ekeys2, cap, false)) || (e = h->alloc(&rb.evals2, cap, false)) ||
         (e = h->alloc(&rb.tile_start, rb.tiles + 1)) || (e = h->alloc(&rb.tile_items, rb.tiles)) ||
         (e = h->alloc(&rb.item_off, rb.tiles + 1)) || (e = h->alloc(&rb.tile_done, rb.tiles)) ||
-        (e = h->alloc(&rb.acc, 2 * (size_t)h->dp.C)) || (e = h->alloc(&rb.total, 4)))
+        (e = h->alloc(&rb.acc, 2 * (size_t)h->dp.C)) || (e = h->alloc(&rb.total, 4)) ||
+        (e = h->alloc(&rb.ktab, kKernelTableSize)))
         return e;
+    {
+        std::vector<float4> tab(kKernelTableSize);
+        build_kernel_table(h->dp.sigma, tab.data());
+        if ((e = cudaMemcpy(rb.ktab, tab.data(), sizeof(float4) * tab.size(), cudaMemcpyHostToDevice))) return e;
+    }
     int bits = 1;
     while ((1 << bits) < rb.tiles + 1) ++bits;
     int pb[4];
@@ -281,6 +287,7 @@ k3dom_status grow_points(k3dom_handle* h, int n) {
     for (void* p : {(void*)rb.ray_a, (void*)rb.ray_b, (void*)rb.ray_c, (void*)rb.counts, (void*)rb.offsets, (void*)rb.ekeys,
                     (void*)rb.evals, (void*)rb.ekeys2, (void*)rb.evals2, (void*)rb.tile_start, (void*)rb.tile_items,
                     (void*)rb.item_off, (void*)rb.tile_done, (void*)rb.acc, (void*)rb.total, (void*)rb.ds_counts,
+                    (void*)rb.ktab,
                     (void*)h->pts})
         drop(p);
     if (rb.ekeys_alt != rb.ekeys) { drop(rb.ekeys_alt); drop(rb.evals_alt); }
@@ -1144,6 +1151,7 @@ k3dom_status k3dom_get_diagnostics(k3dom_handle* h, k3dom_diagnostics* out) {
     out->work_items = (int64_t)st.work_items;
     out->overflow = (int32_t)st.overflow;
     out->kernel_launches_per_frame = h->launches_per_frame;
+    out->kernel_evaluations = (int64_t)st.kernel_evals;
     return K3DOM_OK;
 }
 

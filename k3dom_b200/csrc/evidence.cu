@@ -23,6 +23,7 @@
 #include <math.h>
 
 #include <algorithm>
+#include <cmath>
 #include <cstddef>
 
 #include "common.cuh"
@@ -32,6 +33,7 @@
 namespace k3dom {
 
 constexpr int kChunk = 1024;
+constexpr int kKernelTab = 512;  // intervals of the sparse-kernel table over u = d^2 / ls^2
 constexpr int kEvThreads = 256;
 constexpr int kEvWarps = kEvThreads / 32;
 constexpr int kDsMaxNeighbors = 100;  // measurement_grid.cu:87
@@ -271,6 +273,7 @@ __global__ void k_finish_lists(const uint32_t* __restrict__ item_off, int T, Dev
     status->ray_entries = total[0];
     status->work_counter = 0;
     status->work_counter2 = 0;
+    status->kernel_evals = 0;
 }
 
 // Largest |c| of a cell centre seen from a sensor inside or near the grid [m].
@@ -395,21 +398,38 @@ __device__ __forceinline__ CellLoc locate(const DevParams& p, const TileShape& t
 // ================================================================ K3DOM
 // The sparse kernel of mass_update.cu:24-26,
 //   k(d) = max(0, sigma ((2 + cos(2 pi x)) (1 - x) / 3 + sin(2 pi x) / (2 * 3.141592))),  x = d / ls,
-// (the reference's truncated pi in the sine term is kept). Its two terms cancel up to ~16x over
-// the outer half of the support, so the angle 2x is carried in double (hi + lo, the FP32
-// sincospif of hi corrected to first order in lo) and the combination is formed in FP64.
-__device__ __forceinline__ double kernel_func(float d, double inv_ls, double sigma) {
-    const double x = (double)d * inv_ls;
-    const double t = 2.0 * x;
-    const float hi = (float)t;
-    const float lo = (float)(t - (double)hi);
-    float s, c;
-    sincospif(hi, &s, &c);
-    const float plo = 3.14159265358979f * lo;
-    const double cc = (double)c - (double)(plo * s);
-    const double ss = (double)s + (double)(plo * c);
-    const double v = sigma * ((2.0 + cc) * (1.0 - x) * (1.0 / 3.0) + ss * (1.0 / (2.0 * 3.141592)));
+// (the reference's truncated pi in the sine term is kept) is tabulated as a function of
+// u = d^2 / ls^2 (no square root in the hot loop): kKernelTab intervals, on each a cubic in the
+// local coordinate through four FP64 samples (f = 0, 1/3, 2/3, 1). Evaluated in FP32 by Horner,
+// it is within 1.2e-7 relative of the FP64 kernel wherever k > 1e-3 sigma and within 8e-8 sigma
+// absolute everywhere; the direct FP32 formula loses up to ~1e-5 to cancellation between its two
+// terms over the outer half of the support.
+static double kernel_ref(double u, double sigma) {
+    const double x = std::sqrt(u);
+    const double v = sigma * ((2.0 + std::cos(M_PI * 2.0 * x)) * (1.0 - x) / 3.0 +
+                              std::sin(M_PI * 2.0 * x) / (2.0 * 3.141592));
     return v > 0.0 ? v : 0.0;
+}
+
+void build_kernel_table(float sigma, float4* out) {
+    for (int i = 0; i < kKernelTab; ++i) {
+        double y[4];
+        for (int j = 0; j < 4; ++j) y[j] = kernel_ref(std::min(1.0, (i + j / 3.0) / kKernelTab), sigma);
+        // inverse Vandermonde of the nodes 0, 1/3, 2/3, 1
+        const double c0 = y[0];
+        const double c1 = -5.5 * y[0] + 9.0 * y[1] - 4.5 * y[2] + y[3];
+        const double c2 = 9.0 * y[0] - 22.5 * y[1] + 18.0 * y[2] - 4.5 * y[3];
+        const double c3 = -4.5 * y[0] + 13.5 * y[1] - 13.5 * y[2] + 4.5 * y[3];
+        out[i] = make_float4((float)c0, (float)c1, (float)c2, (float)c3);
+    }
+}
+
+__device__ __forceinline__ float kernel_tab(const float4* __restrict__ tab, float u) {
+    const float t = u * (float)kKernelTab;
+    const int i = min((int)t, kKernelTab - 1);
+    const float f = t - (float)i;
+    const float4 c = tab[i];
+    return fmaf(f, fmaf(f, fmaf(f, c.w, c.z), c.y), c.x);
 }
 
 __device__ __forceinline__ double calc_credit(double mass, double mass_scale) {
@@ -505,6 +525,7 @@ struct EvArgs {
     const float4* ray_a;
     const float4* ray_b;
     const double4* ray_c;
+    const float4* ktab;
     uint32_t* tile_done;
     unsigned long long* acc;
     uint8_t* ds_counts;
@@ -521,6 +542,7 @@ struct EvArgs {
 // Shared memory of k_bgki: one chunk of rays plus a per-warp staging area for the FP64
 // (sub-block, ray) constants.
 struct BgkiSmem {
+    float4 ktab[kKernelTab];     // sparse-kernel table (sigma folded in)
     float4 a[kChunk];            // m
     float4 u[kChunk];            // unit direction (FP32)
     double4 c[kChunk];           // d_m, margin, 1/d_m
@@ -547,9 +569,9 @@ __global__ void __launch_bounds__(kEvThreads) k_bgki(EvArgs A) {
     const FrameParams fp = *A.fp;
     const uint32_t total_items = A.item_off[A.T];
     const float ls2 = p.ls * p.ls;
-    const double inv_ls = 1.0 / (double)p.ls;
-    const double sigma = p.sigma;
+    const float inv_ls2 = 1.0f / ls2;
     const int n_points = fp.n_points;
+    for (int i = threadIdx.x; i < kKernelTab; i += kEvThreads) S.ktab[i] = A.ktab[i];
 
     for (;;) {
         if (threadIdx.x == 0) s_item = atomicAdd(&A.status->work_counter, 1u);
@@ -573,6 +595,7 @@ __global__ void __launch_bounds__(kEvThreads) k_bgki(EvArgs A) {
         __syncthreads();
         double acc_o[NSBW], acc_f[NSBW];
         int cell[NSBW];
+        unsigned nev = 0;  // in-support evaluations of this lane (the roofline's work count)
 #pragma unroll
         for (int q = 0; q < NSBW; ++q) {
             const int sbi = wid + q * kEvWarps;
@@ -610,7 +633,10 @@ __global__ void __launch_bounds__(kEvThreads) k_bgki(EvArgs A) {
                     // occupied evidence (mass_update.cu:48-52)
                     const float vx = s2.x + dx, vy = s2.y + dy, vz = s2.z + dz;
                     const float d2o = vx * vx + vy * vy + vz * vz;
-                    if (d2o < ls2) ao += kernel_func(sqrtf(d2o), inv_ls, sigma);
+                    if (d2o < ls2 && L.c >= 0) {
+                        ao += (double)kernel_tab(S.ktab, d2o * inv_ls2);
+                        ++nev;
+                    }
                     // free evidence (:54-71)
                     const float dpar = dx * u.x + dy * u.y + dz * u.z;
                     if (s0.z + dpar < 0.0f) {  // d_proj < d_m
@@ -618,7 +644,10 @@ __global__ void __launch_bounds__(kEvThreads) k_bgki(EvArgs A) {
                                     qz = s1.z + dz - dpar * u.z;
                         const float al = fminf(s0.x + dpar, 0.0f) + fmaxf(s0.y + dpar, 0.0f);
                         const float d2f = qx * qx + qy * qy + qz * qz + al * al;
-                        if (d2f < ls2) af += kernel_func(sqrtf(d2f), inv_ls, sigma);
+                        if (d2f < ls2 && L.c >= 0) {
+                            af += (double)kernel_tab(S.ktab, d2f * inv_ls2);
+                            ++nev;
+                        }
                     }
                 }
                 __syncwarp();
@@ -626,6 +655,9 @@ __global__ void __launch_bounds__(kEvThreads) k_bgki(EvArgs A) {
             acc_o[q] = ao;
             acc_f[q] = af;
         }
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) nev += __shfl_xor_sync(0xffffffffu, nev, o);
+        if (lane == 0 && nev) atomicAdd(&A.status->kernel_evals, (unsigned long long)nev);
         // fixed-point quantisation: identical whether a tile has one chunk or many
         long long fo[NSBW], ff[NSBW];
 #pragma unroll
@@ -951,6 +983,7 @@ static EvArgs make_args(const DevParams& p, const FrameParams* fp, RayBuffers& r
     A.ray_a = rb.ray_a;
     A.ray_b = rb.ray_b;
     A.ray_c = rb.ray_c;
+    A.ktab = rb.ktab;
     A.tile_done = rb.tile_done;
     A.acc = rb.acc;
     A.ds_counts = rb.ds_counts;

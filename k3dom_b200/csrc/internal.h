@@ -80,6 +80,7 @@ struct RayBuffers {
     float4* ray_a;         // m.x, m.y, m.z, d_m (K3DOM) | |m|^2 (DS)
     float4* ray_b;         // u.x, u.y, u.z, margin (FP32 unit direction)
     double4* ray_c;        // d_m, margin, 1/d_m, 0 in FP64 (K3DOM)
+    float4* ktab;          // sparse-kernel table (build_kernel_table)
     uint32_t* counts;      // per ray: number of tiles touched
     uint32_t* offsets;     // exclusive scan of counts
     uint32_t* ekeys;       // entries: tile id
@@ -118,5 +119,8 @@ cudaError_t launch_ds_evidence(const DevParams& p, const FrameParams* fp, RayBuf
                                CellState cs, CellWork cw, bool first_frame, DevStatus* status,
                                int num_sms, cudaStream_t st);
 cudaError_t evidence_init();
+// Host: the sparse-kernel table (512 float4) for sigma, uploaded once per handle.
+void build_kernel_table(float sigma, float4* out);
+constexpr int kKernelTableSize = 512;
 
 }  // namespace k3dom

@@ -80,18 +80,22 @@ class Scene:
         with np.errstate(divide="ignore", invalid="ignore"):
             tg = np.where(d[:, 2] < 0, (self.ground_z - s[2]) / d[:, 2], np.inf)
         t_hit = np.minimum(t_hit, np.where(tg > 0, tg, np.inf))
-        # cuboids (slab test)
+        # cuboids (slab test); fmin/fmax ignore the NaN of 0 * inf on axis-parallel rays
+        d32 = d.astype(np.float32)
+        with np.errstate(divide="ignore", invalid="ignore"):
+            inv = (1.0 / d32).astype(np.float32)
         for b in self.boxes:
-            c = b.center + b.vel * t
-            lo, hi = c - b.half - s, c + b.half - s
-            with np.errstate(divide="ignore", invalid="ignore"):
-                inv = 1.0 / d
-                t0 = lo * inv
-                t1 = hi * inv
-            tmin = np.nanmax(np.minimum(t0, t1), axis=1)
-            tmax = np.nanmin(np.maximum(t0, t1), axis=1)
-            ok = (tmax >= np.maximum(tmin, 0.0)) & np.isfinite(tmin)
-            t_hit = np.where(ok & (tmin > 0) & (tmin < t_hit), tmin, t_hit)
+            c = (b.center + b.vel * t - s).astype(np.float32)
+            h = b.half.astype(np.float32)
+            with np.errstate(invalid="ignore"):
+                t0 = (c - h) * inv
+                t1 = (c + h) * inv
+            lo = np.fmin(t0, t1)
+            hi = np.fmax(t0, t1)
+            tmin = np.fmax(np.fmax(lo[:, 0], lo[:, 1]), lo[:, 2])
+            tmax = np.fmin(np.fmin(hi[:, 0], hi[:, 1]), hi[:, 2])
+            ok = (tmax >= tmin) & (tmin > 0) & (tmin < t_hit)
+            t_hit = np.where(ok, tmin, t_hit)
         t_hit = np.minimum(t_hit, self.max_range / np.maximum(np.abs(d[:, 2]), 1e-9))
         rng = np.random.Generator(np.random.PCG64([self._noise_seed, frame]))
         r = t_hit + rng.normal(0.0, self.range_noise, size=t_hit.shape)
