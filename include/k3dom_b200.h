@@ -265,6 +265,15 @@ typedef struct k3dom_diagnostics {
 } k3dom_diagnostics;
 k3dom_status k3dom_get_diagnostics(k3dom_handle* h, k3dom_diagnostics* out);
 
+/* Exact inclusive prefix sum of n non-negative floats (device pointers in/out, enqueued on
+ * `stream`, a cudaStream_t or NULL) that allocates no memory: its scratch is a fixed 256 KiB
+ * array inside the library on each GPU. For callers that may not allocate device memory at
+ * run time. The sum is the one the update uses for birth slots and ancestors: each prefix is
+ * the correctly rounded exact sum. n <= 33,554,432 (else K3DOM_ERR_CAPACITY). Calls share the
+ * scratch: calls that overlap on the GPU race. The first call on a device looks up the
+ * scratch address; make it before any stream capture. No counterpart in the reference. */
+k3dom_status k3dom_exact_prefix_sum_noalloc(const float* in, float* out, int64_t n, void* stream);
+
 const char* k3dom_status_string(k3dom_status s);
 int32_t k3dom_abi_version(void);
 

@@ -148,6 +148,7 @@ SIGNATURES = {
     "k3dom_get_stage_times": (_ST, [_P, C.POINTER(StageTimes)]),
     "k3dom_set_timing": (_ST, [_P, C.c_int]),
     "k3dom_get_diagnostics": (_ST, [_P, C.POINTER(Diagnostics)]),
+    "k3dom_exact_prefix_sum_noalloc": (_ST, [_P, _P, C.c_int64, _P]),
     "k3dom_status_string": (C.c_char_p, [C.c_int]),
     "k3dom_abi_version": (C.c_int32, []),
 }
