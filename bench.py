@@ -433,6 +433,26 @@ def run_reference_gpu(args):
                                              "(its own updateGrid, host vectors in, synchronising)"}}), flush=True)
 
 
+def run_profile_case(args):
+    """A mid-size scene for ncu captures (state > L2, well under a few GB): 128x128x32 voxels at
+    0.1 m, P=1,048,576, B=262,144, 60,000 points; the first frame plus `--steps` frames."""
+    import k3dom_b200 as K
+    from k3dom_b200 import scene
+    cfg = scene.config1(seed=5, variant=args.variant)
+    cfg.params.update(size=12.8, particle_count=1 << 20, new_born_particle_count=1 << 18, max_points=60000)
+    cfg.n_points = 60000
+    cfg.scene.max_range = 12.8
+    p = K.make_params(args.variant, **cfg.params)
+    dom = K.DOM(p, args.variant)
+    for f in range(1 + args.steps):
+        t = 0.1 + f * cfg.dt
+        s, pts = cfg.scene.scan(f, t, cfg.n_points)
+        dom.updatePose(*s)
+        dom.updateGrid(t, pts)
+    log("profile case done", dom.diagnostics())
+    dom.close()
+
+
 def main(argv=None):
     ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
     ap.add_argument("--gpus", type=int, default=1)
@@ -441,11 +461,15 @@ def main(argv=None):
     ap.add_argument("--impl", choices=["ours", "reference", "reference-gpu"], default="ours")
     ap.add_argument("--variant", choices=["k3dom", "dsphdmib"], default="k3dom")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--profile-case", choices=["medium"], default=None,
+                    help="run a mid-size scene for profiler captures instead of the benchmark")
     args = ap.parse_args(argv)
     if args.warmup < 3 and args.impl == "ours":
         log("warmup < 3 raised to 3")
         args.warmup = 3
-    if args.impl == "ours":
+    if args.profile_case:
+        run_profile_case(args)
+    elif args.impl == "ours":
         run_ours(args)
     elif args.impl == "reference":
         run_reference_cpu(args)

@@ -539,13 +539,12 @@ struct EvArgs {
     float cull_r2;            // squared cull radius around a sub-block anchor [m^2]
 };
 
-// Shared memory of k_bgki: one chunk of rays plus a per-warp staging area for the FP64
-// (sub-block, ray) constants.
+// Shared memory of k_bgki: the kernel table, one chunk of rays, and a per-warp staging area for
+// the FP64 (sub-block, ray) constants of the rays that pass the cull.
 struct BgkiSmem {
-    float4 ktab[kKernelTab];     // sparse-kernel table (sigma folded in)
-    float4 a[kChunk];            // m
-    float4 u[kChunk];            // unit direction (FP32)
-    double4 c[kChunk];           // d_m, margin, 1/d_m
+    float4 ktab[kKernelTab];      // sparse-kernel table (sigma folded in)
+    float4 a[kChunk];             // m.x, m.y, m.z, d_m
+    double4 c[kChunk];            // d_m, margin, 1/d_m
     float4 stage[kEvWarps][32][3];
 };
 
@@ -558,12 +557,20 @@ struct BgkiSmem {
 //   distance to the point = |occ0 + delta|.
 // Every FP32 quantity is O(ls), so the FP32 evaluation keeps ~1e-7 relative accuracy at any
 // distance from the sensor (the direct |c|^2 - d_proj^2 form of :60 loses ~1e-5 at 20 m).
-template <int NSBW>
+//
+// Work: a CTA takes one (tile, chunk) item and stages its rays; its warps then pull the tile's
+// 4x4x2 sub-blocks from a block-local counter (so a warp that meets few rays takes more
+// sub-blocks), test 32 rays per ballot against the sub-block's bounding sphere, and evaluate
+// the surviving rays for their own cells. Each warp adds its sub-block's evidence to per-cell
+// 64-bit fixed-point accumulators in global memory (integer addition: the total does not depend
+// on the order of chunks or warps); the last CTA to finish a tile's chunks runs the cell update
+// for the whole tile and clears the accumulators.
+template <int UNUSED>
 __global__ void __launch_bounds__(kEvThreads) k_bgki(EvArgs A) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     BgkiSmem& S = *reinterpret_cast<BgkiSmem*>(smem_raw);
     __shared__ uint32_t s_item;
-    __shared__ int s_last;
+    __shared__ int s_next_sb, s_last;
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
     const DevParams& p = A.p;
     const FrameParams fp = *A.fp;
@@ -571,13 +578,19 @@ __global__ void __launch_bounds__(kEvThreads) k_bgki(EvArgs A) {
     const float ls2 = p.ls * p.ls;
     const float inv_ls2 = 1.0f / ls2;
     const int n_points = fp.n_points;
+    const int nsb = A.ts.nsbx * A.ts.nsby * (A.ts.tz / 2);
+    const int tile_cells = A.ts.tx * A.ts.ty * A.ts.tz;
+    const float hres = 0.5f * p.res;
     for (int i = threadIdx.x; i < kKernelTab; i += kEvThreads) S.ktab[i] = A.ktab[i];
+    unsigned nev = 0;  // in-support evaluations of this lane (the roofline's work count)
 
     for (;;) {
-        if (threadIdx.x == 0) s_item = atomicAdd(&A.status->work_counter, 1u);
+        if (threadIdx.x == 0) {
+            s_item = atomicAdd(&A.status->work_counter, 1u);
+            s_next_sb = 0;
+        }
         __syncthreads();
         const uint32_t item = s_item;
-        __syncthreads();
         if (item >= total_items) break;
         const int t = find_tile(A.item_off, A.T, item);
         const uint32_t k = item - A.item_off[t];
@@ -589,18 +602,15 @@ __global__ void __launch_bounds__(kEvThreads) k_bgki(EvArgs A) {
             uint32_t rid = A.evals[e0 + r];
             if (rid >= (uint32_t)n_points) rid = 0;  // defensive: never read past the ray arrays
             S.a[r] = A.ray_a[rid];
-            S.u[r] = A.ray_b[rid];
             S.c[r] = A.ray_c[rid];
         }
         __syncthreads();
-        double acc_o[NSBW], acc_f[NSBW];
-        int cell[NSBW];
-        unsigned nev = 0;  // in-support evaluations of this lane (the roofline's work count)
-#pragma unroll
-        for (int q = 0; q < NSBW; ++q) {
-            const int sbi = wid + q * kEvWarps;
-            const CellLoc L = locate(p, A.ts, t, sbi, lane, fp.sensor_x, fp.sensor_y, fp.sensor_z);
-            cell[q] = L.c;
+        for (;;) {
+            int sb = 0;
+            if (lane == 0) sb = atomicAdd(&s_next_sb, 1);
+            sb = __shfl_sync(0xffffffffu, sb, 0);
+            if (sb >= nsb) break;
+            const CellLoc L = locate(p, A.ts, t, sb, lane, fp.sensor_x, fp.sensor_y, fp.sensor_z);
             const float dx = L.x - L.ox, dy = L.y - L.oy, dz = L.z - L.oz;  // exact (nearby floats)
             const double ox = L.ox, oy = L.oy, oz = L.oz;
             double ao = 0.0, af = 0.0;
@@ -613,14 +623,19 @@ __global__ void __launch_bounds__(kEvThreads) k_bgki(EvArgs A) {
                     const double par0 = (ox * a.x + oy * a.y + oz * a.z) * cd.z;
                     const double sc = par0 * cd.z;
                     const double px = ox - sc * a.x, py = oy - sc * a.y, pz = oz - sc * a.z;
-                    const double along = fmin(par0, 0.0) + fmax(par0 - cd.x, 0.0);
-                    const float d2 = (float)(px * px + py * py + pz * pz + along * along);
-                    hit = d2 < A.cull_r2;
+                    const float ux = (float)(a.x * cd.z), uy = (float)(a.y * cd.z), uz = (float)(a.z * cd.z);
+                    // cull on the sub-block centroid (anchor - res/2 on each axis), in FP32
+                    const float qd = -hres * (ux + uy + uz);
+                    const float qpar = (float)par0 + qd;
+                    const float qx = (float)px - hres - qd * ux, qy = (float)py - hres - qd * uy,
+                                qz = (float)pz - hres - qd * uz;
+                    const float qal = fminf(qpar, 0.0f) + fmaxf(qpar - a.w, 0.0f);
+                    hit = qx * qx + qy * qy + qz * qz + qal * qal < A.cull_r2;
                     if (hit) {
-                        S.stage[wid][lane][0] = make_float4((float)par0, (float)(par0 - cd.y), (float)(par0 - cd.x), 0.f);
-                        S.stage[wid][lane][1] = make_float4((float)px, (float)py, (float)pz, 0.f);
+                        S.stage[wid][lane][0] = make_float4((float)par0, (float)(par0 - cd.y), (float)(par0 - cd.x), ux);
+                        S.stage[wid][lane][1] = make_float4((float)px, (float)py, (float)pz, uy);
                         S.stage[wid][lane][2] =
-                            make_float4((float)(ox - a.x), (float)(oy - a.y), (float)(oz - a.z), 0.f);
+                            make_float4((float)(ox - a.x), (float)(oy - a.y), (float)(oz - a.z), uz);
                     }
                 }
                 unsigned mask = __ballot_sync(0xffffffffu, hit);
@@ -629,7 +644,6 @@ __global__ void __launch_bounds__(kEvThreads) k_bgki(EvArgs A) {
                     const int j = __ffs(mask) - 1;
                     mask &= mask - 1;
                     const float4 s0 = S.stage[wid][j][0], s1 = S.stage[wid][j][1], s2 = S.stage[wid][j][2];
-                    const float4 u = S.u[g0 + j];
                     // occupied evidence (mass_update.cu:48-52)
                     const float vx = s2.x + dx, vy = s2.y + dy, vz = s2.z + dz;
                     const float d2o = vx * vx + vy * vy + vz * vz;
@@ -638,10 +652,10 @@ __global__ void __launch_bounds__(kEvThreads) k_bgki(EvArgs A) {
                         ++nev;
                     }
                     // free evidence (:54-71)
-                    const float dpar = dx * u.x + dy * u.y + dz * u.z;
+                    const float dpar = dx * s0.w + dy * s1.w + dz * s2.w;
                     if (s0.z + dpar < 0.0f) {  // d_proj < d_m
-                        const float qx = s1.x + dx - dpar * u.x, qy = s1.y + dy - dpar * u.y,
-                                    qz = s1.z + dz - dpar * u.z;
+                        const float qx = s1.x + dx - dpar * s0.w, qy = s1.y + dy - dpar * s1.w,
+                                    qz = s1.z + dz - dpar * s2.w;
                         const float al = fminf(s0.x + dpar, 0.0f) + fmaxf(s0.y + dpar, 0.0f);
                         const float d2f = qx * qx + qy * qy + qz * qz + al * al;
                         if (d2f < ls2 && L.c >= 0) {
@@ -652,57 +666,43 @@ __global__ void __launch_bounds__(kEvThreads) k_bgki(EvArgs A) {
                 }
                 __syncwarp();
             }
-            acc_o[q] = ao;
-            acc_f[q] = af;
-        }
-#pragma unroll
-        for (int o = 16; o > 0; o >>= 1) nev += __shfl_xor_sync(0xffffffffu, nev, o);
-        if (lane == 0 && nev) atomicAdd(&A.status->kernel_evals, (unsigned long long)nev);
-        // fixed-point quantisation: identical whether a tile has one chunk or many
-        long long fo[NSBW], ff[NSBW];
-#pragma unroll
-        for (int q = 0; q < NSBW; ++q) {
-            fo[q] = __double2ll_rn(acc_o[q] * A.fx_scale);
-            ff[q] = __double2ll_rn(acc_f[q] * A.fx_scale);
-        }
-        bool run_update = true;
-        if (n_items > 1) {
-#pragma unroll
-            for (int q = 0; q < NSBW; ++q) {
-                if (cell[q] >= 0) {
-                    if (fo[q]) atomicAdd(&A.acc[2 * (long)cell[q]], (unsigned long long)fo[q]);
-                    if (ff[q]) atomicAdd(&A.acc[2 * (long)cell[q] + 1], (unsigned long long)ff[q]);
-                }
+            // fixed-point quantisation and accumulation (associative)
+            if (L.c >= 0) {
+                const long long fo = __double2ll_rn(ao * A.fx_scale);
+                const long long ff = __double2ll_rn(af * A.fx_scale);
+                if (fo) atomicAdd(&A.acc[2 * (long)L.c], (unsigned long long)fo);
+                if (ff) atomicAdd(&A.acc[2 * (long)L.c + 1], (unsigned long long)ff);
             }
+        }
+        __threadfence();
+        __syncthreads();
+        if (threadIdx.x == 0) s_last = (atomicAdd(&A.tile_done[t], 1u) == n_items - 1) ? 1 : 0;
+        __syncthreads();
+        if (s_last) {
             __threadfence();
-            __syncthreads();
-            if (threadIdx.x == 0) s_last = (atomicAdd(&A.tile_done[t], 1u) == n_items - 1) ? 1 : 0;
-            __syncthreads();
-            run_update = s_last != 0;
-            if (run_update) {
-                __threadfence();
-#pragma unroll
-                for (int q = 0; q < NSBW; ++q) {
-                    if (cell[q] >= 0) {
-                        fo[q] = (long long)atomicExch(&A.acc[2 * (long)cell[q]], 0ull);
-                        ff[q] = (long long)atomicExch(&A.acc[2 * (long)cell[q] + 1], 0ull);
-                    }
-                }
-                if (threadIdx.x == 0) A.tile_done[t] = 0;
+            const int tx = t % A.ts.ntx, ty = (t / A.ts.ntx) % A.ts.nty, tz = t / (A.ts.ntx * A.ts.nty);
+            for (int li = threadIdx.x; li < tile_cells; li += kEvThreads) {
+                const int lx = li % A.ts.tx, ly = (li / A.ts.tx) % A.ts.ty, lz = li / (A.ts.tx * A.ts.ty);
+                const int ix = tx * A.ts.tx + lx, iy = ty * A.ts.ty + ly, iz = tz * A.ts.tz + lz;
+                if (ix >= p.G || iy >= p.G || iz >= p.Gz) continue;
+                const int c = ix + p.G * iy + p.G * p.G * iz;
+                // every chunk of the tile has added its share (fence + tile counter above); read
+                // the totals from L2 and clear only what was written
+                unsigned long long* ac = A.acc + 2 * (long)c;
+                const long long fo = (long long)__ldcg(ac);
+                const long long ff = (long long)__ldcg(ac + 1);
+                if (fo) __stcg(ac, 0ull);
+                if (ff) __stcg(ac + 1, 0ull);
+                k3dom_cell_update(p, fp.dt, c, (double)fo * A.fx_inv, (double)ff * A.fx_inv, A.cs, A.cw,
+                                  A.first_frame != 0);
             }
-        }
-        if (run_update) {
-#pragma unroll
-            for (int q = 0; q < NSBW; ++q) {
-                if (cell[q] >= 0) {
-                    const double dlo = (double)fo[q] * A.fx_inv;
-                    const double dlf = (double)ff[q] * A.fx_inv;
-                    k3dom_cell_update(p, fp.dt, cell[q], dlo, dlf, A.cs, A.cw, A.first_frame != 0);
-                }
-            }
+            if (threadIdx.x == 0) A.tile_done[t] = 0;
         }
         __syncthreads();
     }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) nev += __shfl_xor_sync(0xffffffffu, nev, o);
+    if (lane == 0 && nev) atomicAdd(&A.status->kernel_evals, (unsigned long long)nev);
 }
 
 // ================================================================ DS-PHD/MIB
@@ -998,9 +998,8 @@ static EvArgs make_args(const DevParams& p, const FrameParams* fp, RayBuffers& r
     A.fx_scale = std::ldexp(1.0, sh);
     A.fx_inv = std::ldexp(1.0, -sh);
     A.wr2 = p.window_radius * p.window_radius;
-    // K3DOM culls around the anchor cell (2,2,1) of a sub-block: the farthest cell centre is
-    // 3 res away. DS culls around the sub-block centre: half diagonal sqrt(1.5^2+1.5^2+0.5^2) res.
-    const float rsb = ds ? 2.1794495f * p.res : 3.0f * p.res;
+    // both variants cull around the sub-block centroid: half diagonal sqrt(1.5^2+1.5^2+0.5^2) res
+    const float rsb = 2.1794495f * p.res;
     float rsup;
     if (!ds) {
         rsup = p.ls * (1.0f + 1e-4f) + rsb + 1e-3f * p.res;
@@ -1018,15 +1017,12 @@ static int nsbw_of(const RayBuffers& rb) { return (rb.tx / 4) * (rb.ty / 4) * (r
 cudaError_t launch_k3dom_evidence(const DevParams& p, const FrameParams* fp, RayBuffers& rb, CellState cs,
                                   CellWork cw, bool first_frame, DevStatus* status, int num_sms, cudaStream_t st) {
     EvArgs A = make_args(p, fp, rb, cs, cw, first_frame, status, false);
-    const int grid = num_sms * 2;
     const size_t sm = sizeof(BgkiSmem);
-    switch (nsbw_of(rb)) {
-        case 1: ++g_launches; k_bgki<1><<<grid, kEvThreads, sm, st>>>(A); break;
-        case 2: ++g_launches; k_bgki<2><<<grid, kEvThreads, sm, st>>>(A); break;
-        case 4: ++g_launches; k_bgki<4><<<grid, kEvThreads, sm, st>>>(A); break;
-        case 8: ++g_launches; k_bgki<8><<<grid, kEvThreads, sm, st>>>(A); break;
-        default: return cudaErrorInvalidValue;
-    }
+    int per_sm = 1;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_bgki<0>, kEvThreads, sm);
+    const int grid = num_sms * std::max(1, per_sm);
+    ++g_launches;
+    k_bgki<0><<<grid, kEvThreads, sm, st>>>(A);
     return cudaGetLastError();
 }
 
@@ -1068,10 +1064,7 @@ cudaError_t launch_ds_evidence(const DevParams& p, const FrameParams* fp, RayBuf
 cudaError_t evidence_init() {
     cudaError_t e;
     const int sm = (int)sizeof(BgkiSmem);
-    if ((e = cudaFuncSetAttribute(k_bgki<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm))) return e;
-    if ((e = cudaFuncSetAttribute(k_bgki<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm))) return e;
-    if ((e = cudaFuncSetAttribute(k_bgki<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm))) return e;
-    return cudaFuncSetAttribute(k_bgki<8>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
+    return cudaFuncSetAttribute(k_bgki<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
 }
 
 }  // namespace k3dom
