@@ -29,7 +29,7 @@
 extern "C" {
 #endif
 
-#define K3DOM_B200_ABI_VERSION 1
+#define K3DOM_B200_ABI_VERSION 2
 
 typedef enum k3dom_status {
     K3DOM_OK = 0,
@@ -264,6 +264,44 @@ typedef struct k3dom_diagnostics {
     int64_t kernel_evaluations;        /* K3DOM: in-support sparse-kernel evaluations, last frame */
 } k3dom_diagnostics;
 k3dom_status k3dom_get_diagnostics(k3dom_handle* h, k3dom_diagnostics* out);
+
+/* ---- batches: S independent scenes updated together, one launch per stage ----
+ * No counterpart in the reference, whose DOM holds one scene. Each scene keeps its own
+ * parameters, pose, clock and draw stream, and a scene updated in a batch produces exactly the
+ * results of the same scene in a handle of its own. A plain handle is a batch of one; the
+ * per-scene getters and setters above (info, cell fields, ranges, GridCell / MapPoint export,
+ * particles, permutation, ancestors, resampling state, cell masses, update_pose) address the
+ * scene chosen with k3dom_select_scene (scene 0 by default). At most 64 scenes. */
+k3dom_status k3dom_batch_create(const k3dom_params* params, int32_t n_scenes, k3dom_variant variant,
+                                int device, k3dom_handle** out);
+k3dom_status k3dom_batch_size(k3dom_handle* h, int32_t* n_scenes);
+k3dom_status k3dom_select_scene(k3dom_handle* h, int32_t scene);
+k3dom_status k3dom_batch_update_pose(k3dom_handle* h, int32_t scene, float x, float y, float z);
+/* One frame of every scene: scene s gets time t[s] and points xs[s], ys[s], zs[s] (n[s] of
+ * them; ys/zs may be NULL, or ys[s]/zs[s] NULL, for interleaved xyz in xs[s]). All scenes are
+ * in the same phase: the first call initialises every scene. */
+k3dom_status k3dom_batch_update(k3dom_handle* h, const float* t, const float* const* xs,
+                                const float* const* ys, const float* const* zs, const int32_t* n,
+                                k3dom_mem mem);
+k3dom_status k3dom_batch_update_async(k3dom_handle* h, const float* t, const float* const* xs,
+                                      const float* const* ys, const float* const* zs,
+                                      const int32_t* n, k3dom_mem mem);
+
+/* ---- evidence tuning ----
+ * The evidence stage's tile shape (rule 0: 16x16x8 cells for grids of >= 2^20 cells, else
+ * 8x8x4; 1: 8x8x4; 2: 16x16x4; 3: 16x16x8) and rays per work item (chunk) change its speed,
+ * never its results. k3dom_autotune(h, 1) measures every (rule, chunk in {512, 1024})
+ * candidate on the next steady frames, one candidate per frame (those frames are run without
+ * the graph), then keeps the fastest. */
+#define K3DOM_TUNE_MAX_CANDIDATES 16
+typedef struct k3dom_tuning {
+    int32_t tile_rule, chunk, tuned, tuning, candidates, evidence_blocks;
+    float best_ms;
+    float candidate_ms[K3DOM_TUNE_MAX_CANDIDATES]; /* evidence stage time of each candidate */
+} k3dom_tuning;
+k3dom_status k3dom_autotune(k3dom_handle* h, int enabled);
+k3dom_status k3dom_get_tuning(k3dom_handle* h, k3dom_tuning* out);
+k3dom_status k3dom_set_tuning(k3dom_handle* h, int32_t tile_rule, int32_t chunk);
 
 /* Exact inclusive prefix sum of n non-negative floats (device pointers in/out, enqueued on
  * `stream`, a cudaStream_t or NULL) that allocates no memory: its scratch is a fixed 256 KiB

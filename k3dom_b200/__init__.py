@@ -5,8 +5,8 @@ The compute path is libk3dom_b200.so (hand-written sm_100a CUDA, built with
 update API (dom.py), the ctypes binding (_native.py) and the synthetic scene generator
 (scene.py).
 """
-from .dom import (DOM, GRIDCELL_DTYPE, MAPPOINT_DTYPE, debug_draws, make_params, node_config_from_yaml,  # noqa: F401
+from .dom import (DOM, GRIDCELL_DTYPE, BatchDOM, MAPPOINT_DTYPE, debug_draws, make_params, node_config_from_yaml,  # noqa: F401
                   params_default, params_from_yaml)
 
-__all__ = ["DOM", "GRIDCELL_DTYPE", "MAPPOINT_DTYPE", "debug_draws", "make_params", "node_config_from_yaml",
+__all__ = ["BatchDOM", "DOM", "GRIDCELL_DTYPE", "MAPPOINT_DTYPE", "debug_draws", "make_params", "node_config_from_yaml",
            "params_default", "params_from_yaml"]

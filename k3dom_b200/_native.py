@@ -103,6 +103,14 @@ class Diagnostics(C.Structure):
     ]
 
 
+class Tuning(C.Structure):
+    _fields_ = [
+        ("tile_rule", C.c_int32), ("chunk", C.c_int32), ("tuned", C.c_int32), ("tuning", C.c_int32),
+        ("candidates", C.c_int32), ("evidence_blocks", C.c_int32), ("best_ms", C.c_float),
+        ("candidate_ms", C.c_float * 16),
+    ]
+
+
 _P = C.c_void_p
 _F = C.POINTER(C.c_float)
 _I = C.POINTER(C.c_int32)
@@ -149,6 +157,15 @@ SIGNATURES = {
     "k3dom_set_timing": (_ST, [_P, C.c_int]),
     "k3dom_get_diagnostics": (_ST, [_P, C.POINTER(Diagnostics)]),
     "k3dom_exact_prefix_sum_noalloc": (_ST, [_P, _P, C.c_int64, _P]),
+    "k3dom_batch_create": (_ST, [C.POINTER(Params), C.c_int32, C.c_int, C.c_int, C.POINTER(_P)]),
+    "k3dom_batch_size": (_ST, [_P, C.POINTER(C.c_int32)]),
+    "k3dom_select_scene": (_ST, [_P, C.c_int32]),
+    "k3dom_batch_update_pose": (_ST, [_P, C.c_int32, C.c_float, C.c_float, C.c_float]),
+    "k3dom_batch_update": (_ST, [_P, _F, C.POINTER(_P), C.POINTER(_P), C.POINTER(_P), _I, C.c_int]),
+    "k3dom_batch_update_async": (_ST, [_P, _F, C.POINTER(_P), C.POINTER(_P), C.POINTER(_P), _I, C.c_int]),
+    "k3dom_autotune": (_ST, [_P, C.c_int]),
+    "k3dom_get_tuning": (_ST, [_P, C.POINTER(Tuning)]),
+    "k3dom_set_tuning": (_ST, [_P, C.c_int32, C.c_int32]),
     "k3dom_status_string": (C.c_char_p, [C.c_int]),
     "k3dom_abi_version": (C.c_int32, []),
 }

@@ -6,21 +6,22 @@
 
 namespace k3dom {
 
-// initGridCellsKernel (src/common/kernel/init.cu:20-35): priors, empty ranges.
-__global__ void k_cells_init(DevParams p, CellState cs, CellWork cw) {
-    const int c = blockIdx.x * blockDim.x + threadIdx.x;
-    if (c >= p.C) return;
-    cs.free_m[c] = p.prior_free;
-    cs.static_m[c] = p.prior_static;
-    cs.dyn_m[c] = p.prior_dynamic;
-    cs.occ_m[c] = p.prior_occ;
-    cw.start[c] = -1;
-    cw.end[c] = -1;
+// initGridCellsKernel (src/common/kernel/init.cu:20-35): priors, empty ranges; every scene.
+__global__ void k_cells_init(Batch bt, CellState cs, CellWork cw) {
+    for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < bt.C; c += gridDim.x * blockDim.x) {
+        const DevParams& p = bt.sc[scene_of(bt.off->cell, bt.S, c)].p;
+        cs.free_m[c] = p.prior_free;
+        cs.static_m[c] = p.prior_static;
+        cs.dyn_m[c] = p.prior_dynamic;
+        cs.occ_m[c] = p.prior_occ;
+        cw.start[c] = -1;
+        cw.end[c] = -1;
+    }
 }
 
-void launch_cells_init(const DevParams& p, CellState cs, CellWork cw, cudaStream_t st) {
+void launch_cells_init(const Batch& bt, CellState cs, CellWork cw, cudaStream_t st) {
     ++g_launches;
-    k_cells_init<<<div_up(p.C, kBlock), kBlock, 0, st>>>(p, cs, cw);
+    k_cells_init<<<grid_for(bt.C), kBlock, 0, st>>>(bt, cs, cw);
 }
 
 // The map part of DOM_c::updatePose (src/common/dom.cu:130-156): cells re-initialised to the
@@ -77,12 +78,16 @@ struct CellView {
     int start, end;
 };
 
+// Pointers are the scene's own ranges; range_base is the scene's first sorted particle, so the
+// exported start/end are indices within the scene.
 __device__ __forceinline__ void view_cell(const DevParams& p, int c, CellState cs, CellWork cw,
-                                          const float* born_cum, CellView& v) {
+                                          const float* born_cum, int range_base, CellView& v) {
     v.f = cs.free_m[c]; v.s = cs.static_m[c]; v.d = cs.dyn_m[c]; v.o = cs.occ_m[c];
     v.pers = cs.pers_m[c]; v.pred = cs.pred_m[c]; v.born = cs.born_m[c];
     v.mvx = cs.mvx[c]; v.mvy = cs.mvy[c]; v.mvz = cs.mvz[c];
     v.start = cw.start[c]; v.end = cw.end[c];
+    if (v.start >= 0) v.start -= range_base;
+    if (v.end >= 0) v.end -= range_base;
     if (v.start >= 0) {
         // the factor the reweight applies: pers / pred (p_A = 0, so mu_A only multiplies 0)
         v.mu_UA = cw.factor[c];
@@ -112,11 +117,11 @@ __device__ __forceinline__ void view_cell(const DevParams& p, int c, CellState c
 __device__ __forceinline__ float total_mass(const CellView& v) { return __fadd_rn(__fadd_rn(v.f, v.s), v.d); }
 
 __global__ void k_export_field(DevParams p, int field, CellState cs, CellWork cw, const float* born_cum,
-                               float* dst) {
+                               int range_base, float* dst) {
     const int c = blockIdx.x * blockDim.x + threadIdx.x;
     if (c >= p.C) return;
     CellView v;
-    view_cell(p, c, cs, cw, born_cum, v);
+    view_cell(p, c, cs, cw, born_cum, range_base, v);
     float r = 0.0f;
     const float tm = total_mass(v);
     switch (field) {
@@ -157,9 +162,9 @@ __global__ void k_export_field(DevParams p, int field, CellState cs, CellWork cw
 }
 
 void launch_export_field(const DevParams& p, int field, CellState cs, CellWork cw, const float* born_cum,
-                         float* dst, cudaStream_t st) {
+                         int range_base, float* dst, cudaStream_t st) {
     ++g_launches;
-    k_export_field<<<div_up(p.C, kBlock), kBlock, 0, st>>>(p, field, cs, cw, born_cum, dst);
+    k_export_field<<<div_up(p.C, kBlock), kBlock, 0, st>>>(p, field, cs, cw, born_cum, range_base, dst);
 }
 
 // dom::GridCell, include/common/dom_types.h:12-45 (68 bytes).
@@ -171,11 +176,11 @@ struct GridCellAoS {
 static_assert(sizeof(GridCellAoS) == 68, "GridCell layout");
 
 __global__ void k_export_gridcell(DevParams p, CellState cs, CellWork cw, const float* born_cum,
-                                  GridCellAoS* dst) {
+                                  int range_base, GridCellAoS* dst) {
     const int c = blockIdx.x * blockDim.x + threadIdx.x;
     if (c >= p.C) return;
     CellView v;
-    view_cell(p, c, cs, cw, born_cum, v);
+    view_cell(p, c, cs, cw, born_cum, range_base, v);
     GridCellAoS g;
     g.start_idx = v.start; g.end_idx = v.end;
     g.mu_A = v.mu_A; g.mu_UA = v.mu_UA; g.w_A = v.w_A; g.w_UA = v.w_UA;
@@ -186,10 +191,10 @@ __global__ void k_export_gridcell(DevParams p, CellState cs, CellWork cw, const 
     dst[c] = g;
 }
 
-void launch_export_gridcell(const DevParams& p, CellState cs, CellWork cw, const float* born_cum, void* dst,
-                            cudaStream_t st) {
+void launch_export_gridcell(const DevParams& p, CellState cs, CellWork cw, const float* born_cum,
+                            int range_base, void* dst, cudaStream_t st) {
     ++g_launches;
-    k_export_gridcell<<<div_up(p.C, kBlock), kBlock, 0, st>>>(p, cs, cw, born_cum,
+    k_export_gridcell<<<div_up(p.C, kBlock), kBlock, 0, st>>>(p, cs, cw, born_cum, range_base,
                                                                reinterpret_cast<GridCellAoS*>(dst));
 }
 

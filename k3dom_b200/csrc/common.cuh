@@ -24,6 +24,38 @@ struct DevParams {
     int variant;            // 0 = K3DOM, 1 = DS-PHD/MIB
 };
 
+constexpr int kMaxScenes = 64;
+
+// Evidence tiling of one scene: tiles of tx x ty x tz cells (multiples of 4, 4, 2), each cut
+// into 4x4x2-cell sub-blocks.
+struct TileShape {
+    int tx, ty, tz, ntx, nty, ntz, nsbx, nsby;
+};
+
+// Per-scene constants in device memory. Every scene of a batch owns contiguous ranges of the
+// concatenated cell, particle, birth, joint-weight, point and tile arrays.
+struct SceneDev {
+    DevParams p;
+    TileShape ts;
+    int cell_off, part_off, birth_off, joint_off, point_off, tile_off;
+    int n_tiles, max_points;
+    float bin_R;    // ray-binning support radius [cells]
+    float cull_r2;  // squared cull radius around a sub-block centroid [m^2]
+    float wr2;      // DS window radius squared [m^2]
+    float pad;
+    double fx_inv;  // K3DOM evidence: value = fixed-point integer * fx_inv
+};
+
+// Range starts of every scene, entry S = the total (device memory).
+struct SceneOffsets {
+    int part[kMaxScenes + 1];
+    int birth[kMaxScenes + 1];
+    int joint[kMaxScenes + 1];
+    int cell[kMaxScenes + 1];
+    int point[kMaxScenes + 1];
+    int tile[kMaxScenes + 1];
+};
+
 // Per-frame scalars, resident in device memory so a captured graph can be replayed.
 struct FrameParams {
     float dt;
@@ -34,6 +66,25 @@ struct FrameParams {
     int shift_pending;
     uint64_t seed;
 };
+
+// The batch as the kernels see it: S scenes, their totals and per-scene tables.
+struct Batch {
+    int S, variant;
+    int P, B, C, N, T;  // total particles, births, cells, point slots, tiles
+    const SceneDev* sc;
+    const FrameParams* fp;
+    const SceneOffsets* off;
+};
+
+// Scene owning element i of a concatenated range: the last s with off[s] <= i.
+__device__ __forceinline__ int scene_of(const int* off, int S, int i) {
+    int lo = 0, hi = S;
+    while (hi - lo > 1) {
+        const int mid = (lo + hi) >> 1;
+        if (off[mid] <= i) lo = mid; else hi = mid;
+    }
+    return lo;
+}
 
 // Per-handle device status words.
 struct DevStatus {
@@ -109,5 +160,12 @@ __device__ __forceinline__ T clampv(T a, T lo, T hi) {
 }
 
 inline int div_up(long long a, long long b) { return (int)((a + b - 1) / b); }
+
+// Grid of a grid-stride kernel over n elements: at most kGridStrideCap blocks of kBlock.
+constexpr int kGridStrideCap = 148 * 8;
+inline int grid_for(long long n) {
+    const int g = div_up(n, kBlock);
+    return g < 1 ? 1 : (g > kGridStrideCap ? kGridStrideCap : g);
+}
 
 }  // namespace k3dom

@@ -1,16 +1,25 @@
 // dom.cu -- host orchestration behind the C ABI: the B200 counterpart of dom::DOM_c and the
 // two dom::DOM variants (src/common/dom.cu, src/k3dom/dom.cu, src/dsphdmib/dom.cu).
 //
+// A handle holds S >= 1 independent scenes (a plain handle is a batch of one). Every scene
+// owns contiguous ranges of one set of concatenated arrays (cells, particles, births, points,
+// evidence tiles), and every stage is ONE launch over all scenes, so a batched frame costs the
+// same number of launches as a single one and fills the GPU with the union of the scenes' work.
+// Each scene keeps its own parameters, pose, clock and Philox stream (keyed by its own particle
+// indices), so a scene updated in a batch gives the same bits as the same scene updated alone.
+//
 // Differences in structure from the reference, by design:
 //  * every buffer is allocated once at creation (the reference allocates measurement arrays,
 //    Thrust temporaries and a map copy on every frame);
 //  * no host synchronisation inside a frame (the reference reads scalars back at
 //    init_new_particles.cu:49, src/common/dom.cu:275 and resampling.cu:58), so the
-//    steady-state frame can be captured in a CUDA graph and replayed;
+//    steady-state frame is captured in a CUDA graph and replayed;
 //  * particles are double-buffered by role (current / sorted / birth) instead of the deep
 //    copy particle_array = particle_array_next (src/k3dom/dom.cu:43);
 //  * resampling draws are generated and sorted on a second stream while the evidence
-//    kernel runs.
+//    kernel runs;
+//  * evidence tile shapes and work-item sizes are picked by measuring candidates on live
+//    frames (the results do not depend on them).
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -26,54 +35,36 @@
 
 using namespace k3dom;
 
-namespace k3dom {
-cudaError_t exact_scan_float2(const float* a, long na, const float* b, long nb, float* out, void* scratch,
-                              cudaStream_t st);
+namespace {
+
+// Evidence tiling rules the autotuner chooses from.
+enum TileRule { kRuleBySize = 0, kRuleSmall = 1, kRuleFlat = 2, kRuleLarge = 3, kRuleCount = 4 };
+
+TileShape tile_shape(const DevParams& p, int rule) {
+    int tx = 8, ty = 8, tz = 4;
+    const bool large = (long)p.C >= (1L << 20) && p.Gz >= 8;
+    switch (rule) {
+        case kRuleBySize: if (large) { tx = 16; ty = 16; tz = 8; } break;
+        case kRuleSmall: break;
+        case kRuleFlat: tx = 16; ty = 16; tz = 4; break;
+        case kRuleLarge: tx = 16; ty = 16; tz = p.Gz >= 8 ? 8 : 4; break;
+        default: break;
+    }
+    TileShape t;
+    t.tx = tx; t.ty = ty; t.tz = tz;
+    t.ntx = (p.G + tx - 1) / tx;
+    t.nty = (p.G + ty - 1) / ty;
+    t.ntz = (p.Gz + tz - 1) / tz;
+    t.nsbx = tx / 4;
+    t.nsby = ty / 4;
+    return t;
 }
 
-#define CK(x)                                  \
-    do {                                       \
-        cudaError_t e_ = (x);                  \
-        if (e_ != cudaSuccess) return fail(e_); \
-    } while (0)
-
-struct k3dom_handle {
-    int device = 0;
-    int num_sms = 148;
-    k3dom_variant variant = K3DOM_VARIANT_K3DOM;
+struct SceneHost {
     k3dom_params params{};
     DevParams dp{};
-    EvidenceConfig ec{};
-    cudaStream_t st = nullptr, st2 = nullptr;
-    cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
-    cudaEvent_t ev_t[8] = {};
-    bool timing = false;
-    k3dom_stage_times times{};
-
-    FrameParams* fp_dev = nullptr;
-    FrameParams* fp_host = nullptr;  // pinned
-    DevStatus* status = nullptr;
-
-    Particles A{}, S{}, Bp{};
-    uint32_t *sorted_keys = nullptr, *perm = nullptr, *alt_k = nullptr, *alt_v = nullptr;
-    uint32_t *hist = nullptr, *scan_tmp = nullptr;
-    long hist_words = 0, scan_tmp_words = 0;
-    CellState cs[2]{};  // cs[0] live, cs[1] spare for the map shift
-    int *start2 = nullptr, *end2 = nullptr;
-    CellWork cw{};
-    float *born_cum = nullptr, *joint_cum = nullptr, *joint_max = nullptr;
-    void* exact_scratch = nullptr;
-    uint32_t *draw_keys = nullptr, *draw_sorted = nullptr, *draw_alt = nullptr;
-    uint32_t *hist_draw = nullptr, *scan_tmp_draw = nullptr;
-    cudaEvent_t ev_staged = nullptr;  // host staging (frame scalars, points) consumed
-    int* ancestors = nullptr;
-    float *pts = nullptr;       // device x | y | z (3 * max_points)
-    float* pts_pinned = nullptr;
-    RayBuffers rb{};
-    void* export_buf = nullptr;
-    size_t export_bytes = 0;
-    std::vector<void*> allocs;
-
+    TileShape ts{};
+    int max_points = 0;
     // DOM_c host state (include/common/dom.h:135-147)
     bool first_pose_received = false;
     float sensor_pos[3] = {0, 0, 0}, center_pos[3] = {0, 0, 0};
@@ -82,15 +73,79 @@ struct k3dom_handle {
     uint32_t frame = 0;
     bool shift_pending = false;
     int pending_shift[3] = {0, 0, 0};
+    bool initialized = false;
+};
+
+int key_bits_for(long n) {
+    int b = 1;
+    while (b < 31 && (1L << b) < n) ++b;
+    return b;
+}
+
+}  // namespace
+
+struct k3dom_handle {
+    int device = 0;
+    int num_sms = 148;
+    k3dom_variant variant = K3DOM_VARIANT_K3DOM;
+    int S = 1;
+    int cur = 0;  // scene the per-scene getters and setters address
+    std::vector<SceneHost> sc;
+    SceneOffsets off{};
+    int P = 0, B = 0, C = 0, N = 0, T = 0;
+
+    cudaStream_t st = nullptr, st2 = nullptr;
+    cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
+    cudaEvent_t ev_t[8] = {};
+    bool timing = false;
+    k3dom_stage_times times{};
+
+    SceneDev* sc_dev = nullptr;
+    SceneOffsets* off_dev = nullptr;
+    FrameParams* fp_dev = nullptr;
+    FrameParams* fp_host = nullptr;  // pinned, S entries
+    DevStatus* status = nullptr;
+
+    Particles A{}, Ss{}, Bp{};
+    uint32_t *sorted_keys = nullptr, *perm = nullptr, *alt_k = nullptr, *alt_v = nullptr;
+    uint32_t *hist = nullptr, *scan_tmp = nullptr;
+    long hist_words = 0, scan_tmp_words = 0;
+    CellState cs[2]{};  // cs[0] live, cs[1] spare for the map shift
+    int *start2 = nullptr, *end2 = nullptr;
+    CellWork cw{};
+    float *born_cum = nullptr, *joint_cum = nullptr, *joint_max = nullptr;
+    void* exact_scratch = nullptr;
+    ExactTile *plan_born = nullptr, *plan_joint = nullptr;
+    int plan_born_n = 0, plan_joint_n = 0;
+    uint32_t *draw_keys = nullptr, *draw_sorted = nullptr, *draw_alt = nullptr;
+    uint32_t *hist_draw = nullptr, *scan_tmp_draw = nullptr;
+    cudaEvent_t ev_staged = nullptr;  // host staging (frame scalars, points) consumed
+    int* ancestors = nullptr;
+    float* pts = nullptr;  // device x | y | z, N slots each
+    float* pts_pinned = nullptr;
+    RayBuffers rb{};
+    std::vector<void*> ray_allocs;  // buffers sized by points and tiles (re-made on growth)
+    void* export_buf = nullptr;
+    size_t export_bytes = 0;
+    std::vector<void*> allocs;
+
     bool births_done = false;
     int launches_per_frame = 0;
-    bool initialized = false;
+    int bgki_grid = 0, ds_grid = 0;
+    int ds_sized_chunk = 0;  // chunk the DS count buffer was sized for
+
+    // evidence tuning
+    int tile_rule = kRuleBySize;
+    int chunk = 1024;
+    int tune_next = -1;  // next candidate to measure, -1 when not tuning
+    float tune_best_ms = 0.0f;
+    int tune_best = 0, tuned = 0;
+    std::vector<float> tune_ms;
 
     // graph of the steady-state frame
     bool graph_mode = true;
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t graph_exec = nullptr;
-    int graph_npts = -1;
 
     cudaError_t last_error = cudaSuccess;
     k3dom_status fail(cudaError_t e) {
@@ -99,12 +154,12 @@ struct k3dom_handle {
     }
 
     template <typename T>
-    cudaError_t alloc(T** p, size_t count, bool zero = true) {
+    cudaError_t alloc(T** p, size_t count, bool zero = true, std::vector<void*>* list = nullptr) {
         *p = nullptr;
         if (count == 0) count = 1;
         cudaError_t e = cudaMalloc((void**)p, count * sizeof(T));
         if (e != cudaSuccess) return e;
-        allocs.push_back((void*)*p);
+        (list ? list : &allocs)->push_back((void*)*p);
         if (zero) e = cudaMemset(*p, 0, count * sizeof(T));
         return e;
     }
@@ -125,15 +180,24 @@ struct k3dom_handle {
             return e;
         return cudaSuccess;
     }
-    void release() {
+    void drop_graph() {
         if (graph_exec) cudaGraphExecDestroy(graph_exec);
         if (graph) cudaGraphDestroy(graph);
         graph_exec = nullptr;
         graph = nullptr;
+    }
+    void free_ray_buffers() {
+        for (void* p : ray_allocs) cudaFree(p);
+        ray_allocs.clear();
+        if (pts_pinned) cudaFreeHost(pts_pinned);
+        pts_pinned = nullptr;
+    }
+    void release() {
+        drop_graph();
+        free_ray_buffers();
         for (void* p : allocs) cudaFree(p);
         allocs.clear();
         if (fp_host) cudaFreeHost(fp_host);
-        if (pts_pinned) cudaFreeHost(pts_pinned);
         if (export_buf) cudaFree(export_buf);
         for (auto& e : ev_t)
             if (e) cudaEventDestroy(e);
@@ -144,14 +208,34 @@ struct k3dom_handle {
         if (st2) cudaStreamDestroy(st2);
     }
     CellState cells() const { return cs[0]; }
+    Batch batch() const {
+        Batch b;
+        b.S = S;
+        b.variant = (int)variant;
+        b.P = P; b.B = B; b.C = C; b.N = N; b.T = T;
+        b.sc = sc_dev;
+        b.fp = fp_dev;
+        b.off = off_dev;
+        return b;
+    }
+    bool ds() const { return variant == K3DOM_VARIANT_DSPHDMIB; }
 };
 
 namespace {
 
-int key_bits_for(long n) {
-    int b = 1;
-    while (b < 31 && (1L << b) < n) ++b;
-    return b;
+CellState offset_cells(CellState c, long o) {
+    c.free_m += o; c.static_m += o; c.dyn_m += o; c.occ_m += o; c.pers_m += o; c.pred_m += o; c.born_m += o;
+    c.mvx += o; c.mvy += o; c.mvz += o;
+    return c;
+}
+CellWork offset_work(CellWork w, long o) {
+    w.start += o; w.end += o; w.sum_w += o; w.sum_wvx += o; w.sum_wvy += o; w.sum_wvz += o; w.factor += o;
+    w.divisor += o; w.meas_occ += o; w.meas_free += o; w.del_occ += o; w.del_free += o;
+    return w;
+}
+Particles offset_particles(Particles q, long o) {
+    q.px += o; q.py += o; q.pz += o; q.vx += o; q.vy += o; q.vz += o; q.w += o; q.cell += o; q.assoc += o;
+    return q;
 }
 
 k3dom_status validate(const k3dom_params* p, k3dom_variant v) {
@@ -171,79 +255,134 @@ k3dom_status validate(const k3dom_params* p, k3dom_variant v) {
     return K3DOM_OK;
 }
 
-cudaError_t alloc_ray_buffers(k3dom_handle* h, int max_points) {
-    RayBuffers& rb = h->rb;
-    rb.max_points = max_points;
-    rb.tx = h->ec.tile_x;
-    rb.ty = h->ec.tile_y;
-    rb.tz = h->ec.tile_z;
-    rb.ntx = (h->dp.G + rb.tx - 1) / rb.tx;
-    rb.nty = (h->dp.G + rb.ty - 1) / rb.ty;
-    rb.ntz = (h->dp.Gz + rb.tz - 1) / rb.tz;
-    rb.tiles = rb.ntx * rb.nty * rb.ntz;
-    long cap = ray_entries_bound(h->dp, h->ec, max_points);
-    cap = std::max(cap, 4096L);
-    rb.capacity = cap;
-    cudaError_t e;
-    if ((e = h->alloc(&rb.ray_a, max_points)) || (e = h->alloc(&rb.ray_b, max_points)) ||
-        (e = h->alloc(&rb.ray_c, max_points)) ||
-        (e = h->alloc(&rb.counts, max_points)) || (e = h->alloc(&rb.offsets, max_points)) ||
-        (e = h->alloc(&rb.ekeys, cap, false)) || (e = h->alloc(&rb.evals, cap, false)) ||
-        (e = h->alloc(&rb.ekeys2, cap, false)) || (e = h->alloc(&rb.evals2, cap, false)) ||
-        (e = h->alloc(&rb.tile_start, rb.tiles + 1)) || (e = h->alloc(&rb.tile_items, rb.tiles)) ||
-        (e = h->alloc(&rb.item_off, rb.tiles + 1)) || (e = h->alloc(&rb.tile_done, rb.tiles)) ||
-        (e = h->alloc(&rb.acc, 2 * (size_t)h->dp.C)) || (e = h->alloc(&rb.total, 4)) ||
-        (e = h->alloc(&rb.ktab, kKernelTableSize)))
-        return e;
-    {
-        std::vector<float4> tab(kKernelTableSize);
-        build_kernel_table(h->dp.sigma, tab.data());
-        if ((e = cudaMemcpy(rb.ktab, tab.data(), sizeof(float4) * tab.size(), cudaMemcpyHostToDevice))) return e;
+DevParams dev_params(const k3dom_params& p, k3dom_variant variant) {
+    DevParams d{};
+    d.G = static_cast<int>(p.size / p.resolution);  // src/common/dom.cu:30
+    d.Gz = static_cast<int>(p.size_z / p.resolution);
+    d.C = d.G * d.G * d.Gz;
+    d.P = p.particle_count;
+    d.B = p.new_born_particle_count;
+    d.res = p.resolution;
+    d.size = p.size;
+    d.size_z = p.size_z;
+    d.mass_scale = p.mass_scale;
+    d.p_S = p.persistence_prob;
+    d.noise_pos = p.stddev_process_noise_position;
+    d.noise_vel = p.stddev_process_noise_velocity;
+    d.p_B = p.birth_prob;
+    d.stddev_vel = p.stddev_velocity;
+    d.init_max_vel = p.init_max_velocity;
+    d.min_vel = p.particle_min_vel;
+    d.prior_free = p.prior_free;
+    d.prior_static = p.prior_static;
+    d.prior_dynamic = p.prior_dynamic;
+    d.prior_occ = p.prior_occ;
+    d.sigma = p.sigma;
+    d.ls = p.ls;
+    d.gamma = p.gamma;
+    d.max_range = p.max_range;
+    d.meas_occ_stddev = p.meas_occ_stddev;
+    d.window_radius = p.resolution * 0.866f;  // src/dsphdmib/dom.cu:22
+    d.p_A = 0.0f;
+    d.likelihood = 1.0f;
+    d.seed = p.seed;
+    d.variant = (int)variant;
+    return d;
+}
+
+// Point slots and evidence tiles of every scene; uploads the scene table and kernel tables.
+cudaError_t layout_points_tiles(k3dom_handle* h) {
+    int pt = 0, tl = 0;
+    for (int s = 0; s < h->S; ++s) {
+        SceneHost& x = h->sc[s];
+        x.ts = tile_shape(x.dp, h->tile_rule);
+        h->off.point[s] = pt;
+        h->off.tile[s] = tl;
+        pt += x.max_points;
+        tl += x.ts.ntx * x.ts.nty * x.ts.ntz;
     }
+    h->off.point[h->S] = pt;
+    h->off.tile[h->S] = tl;
+    h->N = pt;
+    h->T = tl;
+    std::vector<SceneDev> sd(h->S);
+    std::vector<float4> tabs((size_t)h->S * kKernelTableSize);
+    for (int s = 0; s < h->S; ++s) {
+        const SceneHost& x = h->sc[s];
+        SceneDev& d = sd[s];
+        std::memset(&d, 0, sizeof(d));
+        d.p = x.dp;
+        d.ts = x.ts;
+        d.cell_off = h->off.cell[s];
+        d.part_off = h->off.part[s];
+        d.birth_off = h->off.birth[s];
+        d.joint_off = h->off.joint[s];
+        d.point_off = h->off.point[s];
+        d.tile_off = h->off.tile[s];
+        d.n_tiles = h->off.tile[s + 1] - h->off.tile[s];
+        d.max_points = x.max_points;
+        fill_scene_evidence(d, h->ds(), tabs.data() + (size_t)s * kKernelTableSize);
+    }
+    cudaError_t e;
+    if ((e = cudaMemcpy(h->sc_dev, sd.data(), sizeof(SceneDev) * sd.size(), cudaMemcpyHostToDevice))) return e;
+    if ((e = cudaMemcpy(h->off_dev, &h->off, sizeof(SceneOffsets), cudaMemcpyHostToDevice))) return e;
+    if (h->rb.ktab)
+        e = cudaMemcpy(h->rb.ktab, tabs.data(), sizeof(float4) * tabs.size(), cudaMemcpyHostToDevice);
+    return e;
+}
+
+// Buffers sized by the point slots and tiles: ray data, entry lists, tile lists, points.
+cudaError_t alloc_ray_buffers(k3dom_handle* h) {
+    h->drop_graph();
+    h->free_ray_buffers();
+    RayBuffers& rb = h->rb;
+    rb = RayBuffers{};
+    std::vector<void*>* L = &h->ray_allocs;
+    cudaError_t e;
+    if ((e = h->alloc(&rb.ktab, (size_t)h->S * kKernelTableSize, true, L))) return e;
+    if ((e = layout_points_tiles(h))) return e;
+    long cap = 0;
+    for (int s = 0; s < h->S; ++s) cap += ray_entries_bound(h->sc[s].dp, h->sc[s].ts, h->sc[s].max_points);
+    cap = std::max(cap, 4096L);
+    if (cap > 0xFFFFFFF0L) cap = 0xFFFFFFF0L;
+    rb.capacity = cap;
+    rb.chunk = h->chunk;
+    const int N = h->N, T = h->T;
+    if ((e = h->alloc(&rb.ray_a, N, true, L)) || (e = h->alloc(&rb.ray_c, N, true, L)) ||
+        (e = h->alloc(&rb.counts, N, true, L)) || (e = h->alloc(&rb.offsets, N, true, L)) ||
+        (e = h->alloc(&rb.ekeys, cap, false, L)) || (e = h->alloc(&rb.evals, cap, false, L)) ||
+        (e = h->alloc(&rb.ekeys2, cap, false, L)) || (e = h->alloc(&rb.evals2, cap, false, L)) ||
+        (e = h->alloc(&rb.tile_start, T + 1, true, L)) || (e = h->alloc(&rb.tile_items, T, true, L)) ||
+        (e = h->alloc(&rb.item_off, T + 1, true, L)) || (e = h->alloc(&rb.tile_done, T, true, L)) ||
+        (e = h->alloc(&rb.acc, 2 * (size_t)h->C, true, L)) || (e = h->alloc(&rb.total, 4, true, L)))
+        return e;
     int bits = 1;
-    while ((1 << bits) < rb.tiles + 1) ++bits;
+    while ((1 << bits) < T + 1) ++bits;
     int pb[4];
     if (radix_plan(bits, pb) > 1) {
-        if ((e = h->alloc(&rb.ekeys_alt, cap, false)) || (e = h->alloc(&rb.evals_alt, cap, false))) return e;
+        if ((e = h->alloc(&rb.ekeys_alt, cap, false, L)) || (e = h->alloc(&rb.evals_alt, cap, false, L))) return e;
     } else {
         rb.ekeys_alt = rb.ekeys;
         rb.evals_alt = rb.evals;
     }
-    const long items_max = rb.tiles + cap / 1024 + 2;
-    const long tile_cells = (long)rb.tx * rb.ty * rb.tz;
-    if (h->variant == K3DOM_VARIANT_DSPHDMIB) {
-        rb.ds_count_capacity = items_max * tile_cells;
-        if ((e = h->alloc(&rb.ds_counts, rb.ds_count_capacity))) return e;
-    } else {
-        rb.ds_count_capacity = 0;
+    if (h->ds()) {
+        h->ds_sized_chunk = std::max(32, h->chunk);
+        const long items_max = T + cap / h->ds_sized_chunk + 2;
+        rb.ds_count_capacity = ds_count_bytes(items_max);
+        if ((e = h->alloc(&rb.ds_counts, rb.ds_count_capacity, true, L))) return e;
     }
     // shared sort/scan scratch sized for the largest user
-    const long hw = std::max({radix_hist_words(h->dp.P, 11), radix_hist_words(cap, 11), 1L});
-    if (hw > h->hist_words) {
-        if ((e = h->alloc(&h->hist, hw))) return e;
-        h->hist_words = hw;
-    }
-    const long sw = scan_u32_tiles(std::max({hw, (long)max_points, (long)rb.tiles + 1})) + 16;
-    if (sw > h->scan_tmp_words) {
-        if ((e = h->alloc(&h->scan_tmp, sw))) return e;
-        h->scan_tmp_words = sw;
-    }
+    const long hw = std::max({radix_hist_words(h->P, 11), radix_hist_words(cap, 11), 1L});
+    if ((e = h->alloc(&h->hist, hw, true, L))) return e;
+    h->hist_words = hw;
+    const long sw = scan_u32_tiles(std::max({hw, (long)N, (long)T + 1})) + 16;
+    if ((e = h->alloc(&h->scan_tmp, sw, true, L))) return e;
+    h->scan_tmp_words = sw;
     rb.hist = h->hist;
     rb.scan_tmp = h->scan_tmp;
-    if ((e = h->alloc(&h->pts, 3 * (size_t)max_points))) return e;
-    if (h->pts_pinned) cudaFreeHost(h->pts_pinned);
-    if ((e = cudaMallocHost((void**)&h->pts_pinned, 3 * (size_t)max_points * sizeof(float)))) return e;
+    if ((e = h->alloc(&h->pts, 3 * (size_t)N, true, L))) return e;
+    if ((e = cudaMallocHost((void**)&h->pts_pinned, 3 * (size_t)N * sizeof(float)))) return e;
     return cudaSuccess;
-}
-
-void choose_tiles(k3dom_handle* h) {
-    // 16x16x8-cell tiles for large grids, 8x8x4 for small ones
-    if ((long)h->dp.C >= (1L << 20) && h->dp.Gz >= 8) {
-        h->ec.tile_x = 16; h->ec.tile_y = 16; h->ec.tile_z = 8;
-    } else {
-        h->ec.tile_x = 8; h->ec.tile_y = 8; h->ec.tile_z = 4;
-    }
-    h->ec.chunk = 1024;
 }
 
 }  // namespace
@@ -251,73 +390,86 @@ void choose_tiles(k3dom_handle* h) {
 // ===================================================================== frame pieces
 namespace {
 
-k3dom_status set_frame_params(k3dom_handle* h, float dt, int n_points) {
-    // the pinned staging (frame scalars and points) may still be read by an earlier copy
+// Frame scalars of every scene (dt[s], n[s]); waits until the previous staging was consumed.
+k3dom_status set_frame_params(k3dom_handle* h, const float* dt, const int* n_points) {
     cudaError_t e = cudaEventSynchronize(h->ev_staged);
     if (e != cudaSuccess) return h->fail(e);
-    FrameParams& f = *h->fp_host;
-    f.dt = dt;
-    f.sensor_x = h->sensor_pos[0] - h->center_pos[0];
-    f.sensor_y = h->sensor_pos[1] - h->center_pos[1];
-    f.sensor_z = h->sensor_pos[2] - h->center_pos[2];
-    f.n_points = n_points;
-    f.frame = h->frame;
-    f.shift_x = h->pending_shift[0];
-    f.shift_y = h->pending_shift[1];
-    f.shift_z = h->pending_shift[2];
-    f.shift_pending = h->shift_pending ? 1 : 0;
-    f.seed = h->params.seed;
-    e = cudaMemcpyAsync(h->fp_dev, h->fp_host, sizeof(FrameParams), cudaMemcpyHostToDevice, h->st);
+    for (int s = 0; s < h->S; ++s) {
+        const SceneHost& x = h->sc[s];
+        FrameParams& f = h->fp_host[s];
+        f.dt = dt[s];
+        f.sensor_x = x.sensor_pos[0] - x.center_pos[0];
+        f.sensor_y = x.sensor_pos[1] - x.center_pos[1];
+        f.sensor_z = x.sensor_pos[2] - x.center_pos[2];
+        f.n_points = n_points[s];
+        f.frame = x.frame;
+        f.shift_x = x.pending_shift[0];
+        f.shift_y = x.pending_shift[1];
+        f.shift_z = x.pending_shift[2];
+        f.shift_pending = x.shift_pending ? 1 : 0;
+        f.seed = x.params.seed;
+    }
+    e = cudaMemcpyAsync(h->fp_dev, h->fp_host, sizeof(FrameParams) * h->S, cudaMemcpyHostToDevice, h->st);
     if (e != cudaSuccess) return h->fail(e);
     e = cudaEventRecord(h->ev_staged, h->st);
     return e == cudaSuccess ? K3DOM_OK : h->fail(e);
 }
 
-k3dom_status grow_points(k3dom_handle* h, int n) {
-    if (n <= h->rb.max_points) return K3DOM_OK;
-    // capacity grows (allocation happens only here, outside the steady state)
-    cudaError_t e = cudaStreamSynchronize(h->st);
-    if (e != cudaSuccess) return h->fail(e);
-    auto drop = [&](void* p) {
-        if (!p) return;
-        auto it = std::find(h->allocs.begin(), h->allocs.end(), p);
-        if (it != h->allocs.end()) { cudaFree(p); h->allocs.erase(it); }
-    };
-    RayBuffers& rb = h->rb;
-    for (void* p : {(void*)rb.ray_a, (void*)rb.ray_b, (void*)rb.ray_c, (void*)rb.counts, (void*)rb.offsets, (void*)rb.ekeys,
-                    (void*)rb.evals, (void*)rb.ekeys2, (void*)rb.evals2, (void*)rb.tile_start, (void*)rb.tile_items,
-                    (void*)rb.item_off, (void*)rb.tile_done, (void*)rb.acc, (void*)rb.total, (void*)rb.ds_counts,
-                    (void*)rb.ktab,
-                    (void*)h->pts})
-        drop(p);
-    if (rb.ekeys_alt != rb.ekeys) { drop(rb.ekeys_alt); drop(rb.evals_alt); }
-    int np = std::max(n, (int)(rb.max_points * 1.25));
-    e = alloc_ray_buffers(h, np);
-    if (e != cudaSuccess) return h->fail(e);
-    if (h->graph_exec) { cudaGraphExecDestroy(h->graph_exec); h->graph_exec = nullptr; }
-    if (h->graph) { cudaGraphDestroy(h->graph); h->graph = nullptr; }
-    h->params.max_points = np;
-    return K3DOM_OK;
+// Same dt and point count for every scene (the stage calls).
+k3dom_status set_frame_params_all(k3dom_handle* h, float dt, int n) {
+    std::vector<float> d(h->S, dt);
+    std::vector<int> m(h->S, n);
+    return set_frame_params(h, d.data(), m.data());
 }
 
-// Points -> device SoA. Host input is staged through pinned memory.
-k3dom_status upload_points(k3dom_handle* h, const float* xs, const float* ys, const float* zs, int n, k3dom_mem mem) {
-    if (n < 0) return K3DOM_ERR_INVALID_ARGUMENT;
-    if (n > 0 && !xs) return K3DOM_ERR_INVALID_ARGUMENT;
-    k3dom_status s = grow_points(h, n);
-    if (s != K3DOM_OK) return s;
-    const int M = h->rb.max_points;
-    float* dx = h->pts;
-    float* dy = h->pts + M;
-    float* dz = h->pts + 2 * (size_t)M;
+// Point capacities grow (allocation happens only here, outside the steady state).
+k3dom_status grow_points(k3dom_handle* h, const int32_t* n) {
+    bool grow = false;
+    for (int s = 0; s < h->S; ++s) grow = grow || n[s] > h->sc[s].max_points;
+    if (!grow) return K3DOM_OK;
+    cudaError_t e = cudaStreamSynchronize(h->st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(h->st2);
+    if (e != cudaSuccess) return h->fail(e);
+    for (int s = 0; s < h->S; ++s) {
+        SceneHost& x = h->sc[s];
+        if (n[s] > x.max_points) x.max_points = std::max(n[s], (int)(x.max_points * 1.25));
+        x.params.max_points = x.max_points;
+    }
+    long slots = 0;
+    for (int s = 0; s < h->S; ++s) slots += h->sc[s].max_points;
+    if (slots > (1L << 30)) return K3DOM_ERR_CAPACITY;
+    e = alloc_ray_buffers(h);
+    if (e != cudaSuccess) return h->fail(e);
+    e = cudaEventRecord(h->ev_staged, h->st);
+    return e == cudaSuccess ? K3DOM_OK : h->fail(e);
+}
+
+bool has_nonfinite_host(const float* xs, const float* ys, const float* zs, int n) {
+    const bool inter = (ys == nullptr || zs == nullptr);
+    const long m = inter ? 3L * n : n;
+    for (long i = 0; i < m; ++i)
+        if (!std::isfinite(xs[i])) return true;
+    if (!inter)
+        for (int i = 0; i < n; ++i)
+            if (!std::isfinite(ys[i]) || !std::isfinite(zs[i])) return true;
+    return false;
+}
+
+// Points of scene s -> device SoA slots of the scene. Host input is staged through pinned
+// memory (the previous frame's copies have completed: set_frame_params waited on them).
+k3dom_status upload_points(k3dom_handle* h, int s, const float* xs, const float* ys, const float* zs, int n,
+                           k3dom_mem mem) {
     if (n == 0) return K3DOM_OK;
+    const long N = h->N, o = h->off.point[s];
+    float* dx = h->pts + o;
+    float* dy = h->pts + N + o;
+    float* dz = h->pts + 2 * N + o;
     const bool interleaved = (ys == nullptr || zs == nullptr);
     cudaError_t e;
     if (mem == K3DOM_MEM_HOST) {
-        // stage in pinned memory (previous frame's copies completed: set_frame_params synced)
-        float* hx = h->pts_pinned;
-        float* hy = hx + M;
-        float* hz = hx + 2 * (size_t)M;
+        float* hx = h->pts_pinned + o;
+        float* hy = h->pts_pinned + N + o;
+        float* hz = h->pts_pinned + 2 * N + o;
         if (interleaved) {
             for (int i = 0; i < n; ++i) {
                 hx[i] = xs[3 * i];
@@ -353,15 +505,10 @@ k3dom_status upload_points(k3dom_handle* h, const float* xs, const float* ys, co
     return K3DOM_OK;
 }
 
-bool has_nonfinite_host(const float* xs, const float* ys, const float* zs, int n) {
-    const bool inter = (ys == nullptr || zs == nullptr);
-    const long m = inter ? 3L * n : n;
-    for (long i = 0; i < m; ++i)
-        if (!std::isfinite(xs[i])) return true;
-    if (!inter)
-        for (int i = 0; i < n; ++i)
-            if (!std::isfinite(ys[i]) || !std::isfinite(zs[i])) return true;
-    return false;
+k3dom_status check_points(const float* xs, const float* ys, const float* zs, int n, k3dom_mem mem) {
+    if (n < 0 || (n > 0 && !xs)) return K3DOM_ERR_INVALID_ARGUMENT;
+    if (mem == K3DOM_MEM_HOST && n > 0 && has_nonfinite_host(xs, ys, zs, n)) return K3DOM_ERR_INVALID_INPUT;
+    return K3DOM_OK;
 }
 
 void rec(k3dom_handle* h, int i) {
@@ -370,78 +517,69 @@ void rec(k3dom_handle* h, int i) {
 
 // --- enqueue helpers (no synchronisation) ---
 cudaError_t enq_predict(k3dom_handle* h) {
-    launch_predict(h->dp, h->fp_dev, h->A, h->st);
+    launch_predict(h->batch(), h->A, h->st);
     return cudaGetLastError();
 }
 
 cudaError_t enq_assign(k3dom_handle* h) {
-    const DevParams& p = h->dp;
     cudaError_t e = radix_sort_pairs(reinterpret_cast<const uint32_t*>(h->A.cell), nullptr, h->sorted_keys, h->perm,
-                                     h->alt_k, h->alt_v, p.P, key_bits_for(p.C), h->hist, h->scan_tmp, h->st);
+                                     h->alt_k, h->alt_v, h->P, key_bits_for(h->C), h->hist, h->scan_tmp, h->st);
     if (e != cudaSuccess) return e;
-    if ((e = cudaMemsetAsync(h->cw.start, 0xFF, sizeof(int) * (size_t)p.C, h->st))) return e;
-    if ((e = cudaMemsetAsync(h->cw.end, 0xFF, sizeof(int) * (size_t)p.C, h->st))) return e;
-    launch_gather_segsum(p, h->A, h->S, h->sorted_keys, h->perm, h->cw, h->st);
+    if ((e = cudaMemsetAsync(h->cw.start, 0xFF, sizeof(int) * (size_t)h->C, h->st))) return e;
+    if ((e = cudaMemsetAsync(h->cw.end, 0xFF, sizeof(int) * (size_t)h->C, h->st))) return e;
+    launch_gather_segsum(h->batch(), h->A, h->Ss, h->sorted_keys, h->perm, h->cw, h->st);
     return cudaGetLastError();
 }
 
 cudaError_t enq_occupancy(k3dom_handle* h, bool first_frame) {
-    const DevParams& p = h->dp;
-    const int M = h->rb.max_points;
-    const bool ds = h->variant == K3DOM_VARIANT_DSPHDMIB;
-    cudaError_t e = build_ray_lists(p, h->fp_dev, h->pts, h->pts + M, h->pts + 2 * (size_t)M, h->rb, ds,
-                                    h->status, h->st);
+    const Batch bt = h->batch();
+    const long N = h->N;
+    cudaError_t e = build_ray_lists(bt, h->pts, h->pts + N, h->pts + 2 * N, h->rb, h->ds(), h->status, h->st);
     if (e != cudaSuccess) return e;
     rec(h, 7);
-    if (ds)
-        e = launch_ds_evidence(p, h->fp_dev, h->rb, h->cells(), h->cw, first_frame, h->status, h->num_sms, h->st);
-    else
-        e = launch_k3dom_evidence(p, h->fp_dev, h->rb, h->cells(), h->cw, first_frame, h->status, h->num_sms, h->st);
-    return e;
+    if (h->ds())
+        return launch_ds_evidence(bt, h->rb, h->cells(), h->cw, first_frame, h->status, h->ds_grid, h->st);
+    return launch_k3dom_evidence(bt, h->rb, h->cells(), h->cw, first_frame, h->status, h->bgki_grid, h->st);
 }
 
 cudaError_t enq_persistent(k3dom_handle* h) {
-    launch_reweight(h->dp, h->S, h->sorted_keys, h->cw, h->st);
+    launch_reweight(h->batch(), h->Ss, h->sorted_keys, h->cw, h->st);
     return cudaGetLastError();
 }
 
 cudaError_t enq_births(k3dom_handle* h) {
-    const DevParams& p = h->dp;
-    cudaError_t e = exact_scan_float(h->cells().born_m, h->born_cum, p.C, h->exact_scratch, h->st);
+    cudaError_t e = exact_scan_plan(h->plan_born, h->plan_born_n, h->exact_scratch, h->st);
     if (e != cudaSuccess) return e;
-    launch_births(p, h->fp_dev, h->cells().born_m, h->born_cum, h->Bp, h->st);
+    launch_births(h->batch(), h->cells().born_m, h->born_cum, h->Bp, h->st);
     return cudaGetLastError();
 }
 
 cudaError_t enq_draws(k3dom_handle* h, cudaStream_t s) {
-    const DevParams& p = h->dp;
-    launch_draw_keys(p, h->fp_dev, h->draw_keys, s);
-    return radix_sort_pairs(h->draw_keys, nullptr, h->draw_sorted, nullptr, h->draw_alt, nullptr, p.P, 24,
-                            h->hist_draw, h->scan_tmp_draw, s);
+    launch_draw_keys(h->batch(), h->draw_keys, s);
+    return radix_sort_pairs(h->draw_keys, nullptr, h->draw_sorted, nullptr, h->draw_alt, nullptr, h->P,
+                            draw_key_bits(h->S), h->hist_draw, h->scan_tmp_draw, s);
 }
 
 cudaError_t enq_resample(k3dom_handle* h, bool draws_ready) {
-    const DevParams& p = h->dp;
     cudaError_t e;
     if (!draws_ready) {
         if ((e = enq_draws(h, h->st))) return e;
     }
-    launch_joint_prepare(p, h->S, h->Bp, nullptr, h->st);
-    if ((e = exact_scan_float2(h->S.w, p.P, h->Bp.w, p.B, h->joint_cum, h->exact_scratch, h->st))) return e;
-    launch_resample(p, h->joint_cum, h->draw_sorted, h->S, h->sorted_keys, h->Bp, h->A, h->ancestors, h->joint_max,
+    launch_joint_prepare(h->batch(), h->Ss, h->Bp, h->st);
+    if ((e = exact_scan_plan(h->plan_joint, h->plan_joint_n, h->exact_scratch, h->st))) return e;
+    launch_resample(h->batch(), h->joint_cum, h->draw_sorted, h->Ss, h->Bp, h->A, h->ancestors, h->joint_max,
                     h->st);
     return cudaGetLastError();
 }
 
 cudaError_t enq_init_particles(k3dom_handle* h) {
-    const DevParams& p = h->dp;
-    cudaError_t e = exact_scan_float(h->cells().born_m, h->born_cum, p.C, h->exact_scratch, h->st);
+    cudaError_t e = exact_scan_plan(h->plan_born, h->plan_born_n, h->exact_scratch, h->st);
     if (e != cudaSuccess) return e;
-    launch_init_particles(p, h->fp_dev, h->born_cum, h->A, h->st);
+    launch_init_particles(h->batch(), h->born_cum, h->A, h->st);
     return cudaGetLastError();
 }
 
-// The steady-state frame (DOM::updateGrid's branch for updated_time > 0).
+// The steady-state frame (DOM::updateGrid's branch for updated_time > 0), all scenes.
 cudaError_t enq_frame(k3dom_handle* h) {
     cudaError_t e;
     const long l0 = g_launches;
@@ -469,7 +607,6 @@ cudaError_t enq_frame(k3dom_handle* h) {
 }
 
 void read_times(k3dom_handle* h) {
-    if (!h->timing) return;
     float t[7] = {0};
     for (int i = 0; i < 6; ++i) cudaEventElapsedTime(&t[i], h->ev_t[i], h->ev_t[i + 1]);
     h->times.predict_ms = t[0];
@@ -483,12 +620,35 @@ void read_times(k3dom_handle* h) {
     cudaEventElapsedTime(&h->times.evidence_ms, h->ev_t[7], h->ev_t[3]);
 }
 
+// Evidence tuning: candidates are (tile rule, chunk) pairs measured one per steady frame.
+constexpr int kTuneChunks[2] = {512, 1024};
+constexpr int kTuneCount = kRuleCount * 2;
+
+cudaError_t apply_tuning(k3dom_handle* h, int rule, int chunk) {
+    if (rule == h->tile_rule && chunk == h->chunk) return cudaSuccess;
+    cudaError_t e = cudaStreamSynchronize(h->st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(h->st2);
+    if (e != cudaSuccess) return e;
+    // a smaller chunk makes more work items than the DS count buffer was sized for
+    const bool relayout = rule != h->tile_rule || (h->ds() && chunk < h->ds_sized_chunk);
+    h->tile_rule = rule;
+    h->chunk = chunk;
+    h->drop_graph();
+    if (relayout) {
+        e = alloc_ray_buffers(h);
+        if (e == cudaSuccess) e = cudaEventRecord(h->ev_staged, h->st);
+        return e;
+    }
+    h->rb.chunk = chunk;
+    return cudaSuccess;
+}
+
 }  // namespace
 
 // ===================================================================== C ABI
 extern "C" {
 
-static cudaError_t copy_cells_back(k3dom_handle* h);
+static cudaError_t copy_cells_back(k3dom_handle* h, int s);
 
 const char* k3dom_status_string(k3dom_status s) {
     switch (s) {
@@ -508,11 +668,22 @@ const char* k3dom_status_string(k3dom_status s) {
 
 int32_t k3dom_abi_version(void) { return K3DOM_B200_ABI_VERSION; }
 
-k3dom_status k3dom_create(const k3dom_params* params, k3dom_variant variant, int device, k3dom_handle** out) {
+k3dom_status k3dom_batch_create(const k3dom_params* params, int32_t n_scenes, k3dom_variant variant, int device,
+                                k3dom_handle** out) {
     if (!out) return K3DOM_ERR_INVALID_ARGUMENT;
     *out = nullptr;
-    k3dom_status s = validate(params, variant);
-    if (s != K3DOM_OK) return s;
+    if (!params || n_scenes < 1) return K3DOM_ERR_INVALID_ARGUMENT;
+    if (n_scenes > kMaxScenes) return K3DOM_ERR_CAPACITY;
+    long tp = 0, tb = 0, tc = 0;
+    for (int s = 0; s < n_scenes; ++s) {
+        k3dom_status v = validate(&params[s], variant);
+        if (v != K3DOM_OK) return v;
+        const DevParams d = dev_params(params[s], variant);
+        tp += d.P;
+        tb += d.B;
+        tc += d.C;
+    }
+    if (tp + tb > (1L << 30) || tc > (1L << 30)) return K3DOM_ERR_CAPACITY;
     int ndev = 0;
     if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) return K3DOM_ERR_NO_DEVICE;
     if (device < 0 || device >= ndev) return K3DOM_ERR_INVALID_ARGUMENT;
@@ -520,8 +691,8 @@ k3dom_status k3dom_create(const k3dom_params* params, k3dom_variant variant, int
     if (!h) return K3DOM_ERR_OUT_OF_MEMORY;
     h->device = device;
     h->variant = variant;
-    h->params = *params;
-    if (h->params.max_points <= 0) h->params.max_points = 131072;
+    h->S = n_scenes;
+    h->sc.resize(n_scenes);
     auto bail = [&](cudaError_t e) {
         k3dom_status r = h->fail(e);
         h->release();
@@ -534,40 +705,32 @@ k3dom_status k3dom_create(const k3dom_params* params, k3dom_variant variant, int
     if ((e = cudaGetDeviceProperties(&prop, device))) return bail(e);
     h->num_sms = prop.multiProcessorCount;
     if ((e = sort_init()) || (e = evidence_init())) return bail(e);
+    h->bgki_grid = h->num_sms * bgki_blocks_per_sm();
+    h->ds_grid = h->num_sms * 4;
 
-    DevParams& d = h->dp;
-    const k3dom_params& p = h->params;
-    d.G = static_cast<int>(p.size / p.resolution);          // src/common/dom.cu:30
-    d.Gz = static_cast<int>(p.size_z / p.resolution);
-    d.C = d.G * d.G * d.Gz;
-    d.P = p.particle_count;
-    d.B = p.new_born_particle_count;
-    d.res = p.resolution;
-    d.size = p.size;
-    d.size_z = p.size_z;
-    d.mass_scale = p.mass_scale;
-    d.p_S = p.persistence_prob;
-    d.noise_pos = p.stddev_process_noise_position;
-    d.noise_vel = p.stddev_process_noise_velocity;
-    d.p_B = p.birth_prob;
-    d.stddev_vel = p.stddev_velocity;
-    d.init_max_vel = p.init_max_velocity;
-    d.min_vel = p.particle_min_vel;
-    d.prior_free = p.prior_free;
-    d.prior_static = p.prior_static;
-    d.prior_dynamic = p.prior_dynamic;
-    d.prior_occ = p.prior_occ;
-    d.sigma = p.sigma;
-    d.ls = p.ls;
-    d.gamma = p.gamma;
-    d.max_range = p.max_range;
-    d.meas_occ_stddev = p.meas_occ_stddev;
-    d.window_radius = p.resolution * 0.866f;  // src/dsphdmib/dom.cu:22
-    d.p_A = 0.0f;
-    d.likelihood = 1.0f;
-    d.seed = p.seed;
-    d.variant = (int)variant;
-    choose_tiles(h);
+    // scene ranges
+    int P = 0, B = 0, C = 0;
+    for (int s = 0; s < n_scenes; ++s) {
+        SceneHost& x = h->sc[s];
+        x.params = params[s];
+        if (x.params.max_points <= 0) x.params.max_points = 131072;
+        x.max_points = x.params.max_points;
+        x.dp = dev_params(x.params, variant);
+        h->off.part[s] = P;
+        h->off.birth[s] = B;
+        h->off.joint[s] = P + B;
+        h->off.cell[s] = C;
+        P += x.dp.P;
+        B += x.dp.B;
+        C += x.dp.C;
+    }
+    h->off.part[n_scenes] = P;
+    h->off.birth[n_scenes] = B;
+    h->off.joint[n_scenes] = P + B;
+    h->off.cell[n_scenes] = C;
+    h->P = P;
+    h->B = B;
+    h->C = C;
 
     if ((e = cudaStreamCreateWithFlags(&h->st, cudaStreamNonBlocking))) return bail(e);
     if ((e = cudaStreamCreateWithFlags(&h->st2, cudaStreamNonBlocking))) return bail(e);
@@ -577,48 +740,70 @@ k3dom_status k3dom_create(const k3dom_params* params, k3dom_variant variant, int
     if ((e = cudaEventRecord(h->ev_staged, h->st))) return bail(e);
     for (auto& ev : h->ev_t)
         if ((e = cudaEventCreate(&ev))) return bail(e);
-    if ((e = cudaMallocHost((void**)&h->fp_host, sizeof(FrameParams)))) return bail(e);
-    std::memset(h->fp_host, 0, sizeof(FrameParams));
-    if ((e = h->alloc(&h->fp_dev, 1)) || (e = h->alloc(&h->status, 1))) return bail(e);
-    if ((e = h->alloc_particles(&h->A, d.P)) || (e = h->alloc_particles(&h->S, d.P)) ||
-        (e = h->alloc_particles(&h->Bp, d.B)))
+    if ((e = cudaMallocHost((void**)&h->fp_host, sizeof(FrameParams) * n_scenes))) return bail(e);
+    std::memset(h->fp_host, 0, sizeof(FrameParams) * n_scenes);
+    if ((e = h->alloc(&h->fp_dev, n_scenes)) || (e = h->alloc(&h->status, 1)) ||
+        (e = h->alloc(&h->sc_dev, n_scenes)) || (e = h->alloc(&h->off_dev, 1)))
         return bail(e);
-    if ((e = h->alloc(&h->sorted_keys, d.P)) || (e = h->alloc(&h->perm, d.P)) || (e = h->alloc(&h->alt_k, d.P)) ||
-        (e = h->alloc(&h->alt_v, d.P)))
+    if ((e = h->alloc_particles(&h->A, P)) || (e = h->alloc_particles(&h->Ss, P)) ||
+        (e = h->alloc_particles(&h->Bp, B)))
         return bail(e);
-    if ((e = h->alloc_cells(&h->cs[0], d.C)) || (e = h->alloc_cells(&h->cs[1], d.C))) return bail(e);
+    if ((e = h->alloc(&h->sorted_keys, P)) || (e = h->alloc(&h->perm, P)) || (e = h->alloc(&h->alt_k, P)) ||
+        (e = h->alloc(&h->alt_v, P)))
+        return bail(e);
+    if ((e = h->alloc_cells(&h->cs[0], C)) || (e = h->alloc_cells(&h->cs[1], C))) return bail(e);
     CellWork& cw = h->cw;
-    if ((e = h->alloc(&cw.start, d.C)) || (e = h->alloc(&cw.end, d.C)) || (e = h->alloc(&h->start2, d.C)) ||
-        (e = h->alloc(&h->end2, d.C)) || (e = h->alloc(&cw.sum_w, d.C)) || (e = h->alloc(&cw.sum_wvx, d.C)) ||
-        (e = h->alloc(&cw.sum_wvy, d.C)) || (e = h->alloc(&cw.sum_wvz, d.C)) || (e = h->alloc(&cw.factor, d.C)) ||
-        (e = h->alloc(&cw.divisor, d.C)) || (e = h->alloc(&cw.meas_occ, d.C)) || (e = h->alloc(&cw.meas_free, d.C)) ||
-        (e = h->alloc(&cw.del_occ, d.C)) || (e = h->alloc(&cw.del_free, d.C)))
+    if ((e = h->alloc(&cw.start, C)) || (e = h->alloc(&cw.end, C)) || (e = h->alloc(&h->start2, C)) ||
+        (e = h->alloc(&h->end2, C)) || (e = h->alloc(&cw.sum_w, C)) || (e = h->alloc(&cw.sum_wvx, C)) ||
+        (e = h->alloc(&cw.sum_wvy, C)) || (e = h->alloc(&cw.sum_wvz, C)) || (e = h->alloc(&cw.factor, C)) ||
+        (e = h->alloc(&cw.divisor, C)) || (e = h->alloc(&cw.meas_occ, C)) || (e = h->alloc(&cw.meas_free, C)) ||
+        (e = h->alloc(&cw.del_occ, C)) || (e = h->alloc(&cw.del_free, C)))
         return bail(e);
-    if ((e = h->alloc(&h->born_cum, d.C)) || (e = h->alloc(&h->joint_cum, (size_t)d.P + d.B)) ||
-        (e = h->alloc(&h->joint_max, 1)) || (e = h->alloc(&h->ancestors, d.P)))
+    if ((e = h->alloc(&h->born_cum, C)) || (e = h->alloc(&h->joint_cum, (size_t)P + B)) ||
+        (e = h->alloc(&h->joint_max, n_scenes)) || (e = h->alloc(&h->ancestors, P)))
         return bail(e);
+    // exact-scan plans: born masses per scene; joint weights (persistent ++ births) per scene
     {
-        const size_t sb = std::max(exact_scan_scratch_bytes((long)d.P + d.B), exact_scan_scratch_bytes(d.C));
+        std::vector<ExactTile> pb, pj;
+        for (int s = 0; s < n_scenes; ++s) {
+            const SceneHost& x = h->sc[s];
+            const float* in1[1] = {h->cs[0].born_m + h->off.cell[s]};
+            const long n1[1] = {x.dp.C};
+            exact_plan_add(pb, in1, n1, 1, h->born_cum + h->off.cell[s]);
+            const float* in2[2] = {h->Ss.w + h->off.part[s], h->Bp.w + h->off.birth[s]};
+            const long n2[2] = {x.dp.P, x.dp.B};
+            exact_plan_add(pj, in2, n2, 2, h->joint_cum + h->off.joint[s]);
+        }
+        h->plan_born_n = (int)pb.size();
+        h->plan_joint_n = (int)pj.size();
+        if ((e = h->alloc(&h->plan_born, pb.size())) || (e = h->alloc(&h->plan_joint, pj.size()))) return bail(e);
+        if ((e = cudaMemcpy(h->plan_born, pb.data(), sizeof(ExactTile) * pb.size(), cudaMemcpyHostToDevice)) ||
+            (e = cudaMemcpy(h->plan_joint, pj.data(), sizeof(ExactTile) * pj.size(), cudaMemcpyHostToDevice)))
+            return bail(e);
+        const size_t sb = exact_plan_scratch_bytes(std::max(h->plan_born_n, h->plan_joint_n));
         unsigned char* es = nullptr;
         if ((e = h->alloc(&es, sb))) return bail(e);
         h->exact_scratch = es;
     }
-    if ((e = h->alloc(&h->draw_keys, d.P)) || (e = h->alloc(&h->draw_sorted, d.P)) ||
-        (e = h->alloc(&h->draw_alt, d.P)))
+    if ((e = h->alloc(&h->draw_keys, P)) || (e = h->alloc(&h->draw_sorted, P)) || (e = h->alloc(&h->draw_alt, P)))
         return bail(e);
     // separate sort scratch for the draw sort (it runs concurrently on the second stream)
     {
-        const long hw = radix_hist_words(d.P, 8);
+        const long hw = radix_hist_words(P, 8);
         if ((e = h->alloc(&h->hist_draw, hw))) return bail(e);
         if ((e = h->alloc(&h->scan_tmp_draw, scan_u32_tiles(hw) + 16))) return bail(e);
     }
-    if ((e = alloc_ray_buffers(h, h->params.max_points))) return bail(e);
+    if ((e = alloc_ray_buffers(h))) return bail(e);
     // DOM_c::initialize (src/common/dom.cu:90-109): cells to priors
-    launch_cells_init(d, h->cs[0], h->cw, h->st);
-    launch_cells_init(d, h->cs[1], h->cw, h->st);
+    launch_cells_init(h->batch(), h->cs[0], h->cw, h->st);
+    launch_cells_init(h->batch(), h->cs[1], h->cw, h->st);
     if ((e = cudaGetLastError()) || (e = cudaStreamSynchronize(h->st))) return bail(e);
     *out = h;
     return K3DOM_OK;
+}
+
+k3dom_status k3dom_create(const k3dom_params* params, k3dom_variant variant, int device, k3dom_handle** out) {
+    return k3dom_batch_create(params, 1, variant, device, out);
 }
 
 k3dom_status k3dom_destroy(k3dom_handle* h) {
@@ -631,59 +816,82 @@ k3dom_status k3dom_destroy(k3dom_handle* h) {
     return K3DOM_OK;
 }
 
-k3dom_status k3dom_update_pose(k3dom_handle* h, float x, float y, float z) {
-    if (!h) return K3DOM_ERR_INVALID_ARGUMENT;
+k3dom_status k3dom_batch_size(k3dom_handle* h, int32_t* n_scenes) {
+    if (!h || !n_scenes) return K3DOM_ERR_INVALID_ARGUMENT;
+    *n_scenes = h->S;
+    return K3DOM_OK;
+}
+
+k3dom_status k3dom_select_scene(k3dom_handle* h, int32_t scene) {
+    if (!h || scene < 0 || scene >= h->S) return K3DOM_ERR_INVALID_ARGUMENT;
+    h->cur = scene;
+    return K3DOM_OK;
+}
+
+k3dom_status k3dom_batch_update_pose(k3dom_handle* h, int32_t scene, float x, float y, float z) {
+    if (!h || scene < 0 || scene >= h->S) return K3DOM_ERR_INVALID_ARGUMENT;
     cudaSetDevice(h->device);
-    const k3dom_params& p = h->params;
-    h->sensor_pos[0] = x;
-    h->sensor_pos[1] = y;
-    h->sensor_pos[2] = z;
-    if (!h->first_pose_received) {
-        h->first_pose_received = true;
-        h->center_pos[0] = x - p.sensor_off_x;
-        h->center_pos[1] = y - p.sensor_off_y;
-        h->center_pos[2] = z - p.sensor_off_z;
+    SceneHost& sh = h->sc[scene];
+    const k3dom_params& p = sh.params;
+    sh.sensor_pos[0] = x;
+    sh.sensor_pos[1] = y;
+    sh.sensor_pos[2] = z;
+    if (!sh.first_pose_received) {
+        sh.first_pose_received = true;
+        sh.center_pos[0] = x - p.sensor_off_x;
+        sh.center_pos[1] = y - p.sensor_off_y;
+        sh.center_pos[2] = z - p.sensor_off_z;
         return K3DOM_OK;
     }
-    const int mx = static_cast<int>((x - h->center_pos[0] - p.sensor_off_x) / p.resolution);
-    const int my = static_cast<int>((y - h->center_pos[1] - p.sensor_off_y) / p.resolution);
-    const int mz = static_cast<int>((z - h->center_pos[2] - p.sensor_off_z) / p.resolution);
+    const int mx = static_cast<int>((x - sh.center_pos[0] - p.sensor_off_x) / p.resolution);
+    const int my = static_cast<int>((y - sh.center_pos[1] - p.sensor_off_y) / p.resolution);
+    const int mz = static_cast<int>((z - sh.center_pos[2] - p.sensor_off_z) / p.resolution);
     if (std::abs(mx) >= p.map_shift_thresh || std::abs(my) >= p.map_shift_thresh ||
         std::abs(mz) >= p.map_shift_thresh) {
         cudaError_t e;
-        if (h->shift_pending) {
+        const long co = h->off.cell[scene];
+        if (sh.shift_pending) {
             // a second shift before any prediction: apply the first to the particles now so
             // each subtraction rounds exactly as moveParticlesKernel's would
-            launch_shift_particles(h->dp, h->A, h->pending_shift[0], h->pending_shift[1], h->pending_shift[2], h->st);
+            launch_shift_particles(sh.dp.P, offset_particles(h->A, h->off.part[scene]), sh.pending_shift[0],
+                                   sh.pending_shift[1], sh.pending_shift[2], h->st);
         }
         // shift into the spare buffers, then copy back so every captured pointer stays valid
-        launch_map_shift_full(h->dp, h->cs[0], h->cs[1], h->cw.start, h->cw.end, h->start2, h->end2, mx, my, mz,
-                              h->st);
-        if ((e = copy_cells_back(h))) return h->fail(e);
-        h->shift_pending = true;
-        h->pending_shift[0] = mx;
-        h->pending_shift[1] = my;
-        h->pending_shift[2] = mz;
+        launch_map_shift_full(sh.dp, offset_cells(h->cs[0], co), offset_cells(h->cs[1], co), h->cw.start + co,
+                              h->cw.end + co, h->start2 + co, h->end2 + co, mx, my, mz, h->st);
+        if ((e = copy_cells_back(h, scene))) return h->fail(e);
+        sh.shift_pending = true;
+        sh.pending_shift[0] = mx;
+        sh.pending_shift[1] = my;
+        sh.pending_shift[2] = mz;
         if ((e = cudaGetLastError())) return h->fail(e);
-        h->center_pos[0] += mx * p.resolution;
-        h->center_pos[1] += my * p.resolution;
-        h->center_pos[2] += mz * p.resolution;
+        sh.center_pos[0] += mx * p.resolution;
+        sh.center_pos[1] += my * p.resolution;
+        sh.center_pos[2] += mz * p.resolution;
     }
     return K3DOM_OK;
 }
 
-static cudaError_t copy_cells_back(k3dom_handle* h) {
-    const size_t b = sizeof(float) * (size_t)h->dp.C;
-    const CellState& s = h->cs[1];
-    const CellState& d = h->cs[0];
-    const float* src[] = {s.free_m, s.static_m, s.dyn_m, s.occ_m, s.pers_m, s.pred_m, s.born_m, s.mvx, s.mvy, s.mvz};
-    float* dst[] = {d.free_m, d.static_m, d.dyn_m, d.occ_m, d.pers_m, d.pred_m, d.born_m, d.mvx, d.mvy, d.mvz};
+k3dom_status k3dom_update_pose(k3dom_handle* h, float x, float y, float z) {
+    if (!h) return K3DOM_ERR_INVALID_ARGUMENT;
+    return k3dom_batch_update_pose(h, h->cur, x, y, z);
+}
+
+static cudaError_t copy_cells_back(k3dom_handle* h, int s) {
+    const long co = h->off.cell[s];
+    const size_t b = sizeof(float) * (size_t)h->sc[s].dp.C;
+    const CellState src = offset_cells(h->cs[1], co);
+    const CellState dst = offset_cells(h->cs[0], co);
+    const float* from[] = {src.free_m, src.static_m, src.dyn_m, src.occ_m, src.pers_m,
+                           src.pred_m, src.born_m,   src.mvx,   src.mvy,   src.mvz};
+    float* to[] = {dst.free_m, dst.static_m, dst.dyn_m, dst.occ_m, dst.pers_m,
+                   dst.pred_m, dst.born_m,   dst.mvx,   dst.mvy,   dst.mvz};
     cudaError_t e;
     for (int i = 0; i < 10; ++i)
-        if ((e = cudaMemcpyAsync(dst[i], src[i], b, cudaMemcpyDeviceToDevice, h->st))) return e;
-    if ((e = cudaMemcpyAsync(h->cw.start, h->start2, sizeof(int) * (size_t)h->dp.C, cudaMemcpyDeviceToDevice, h->st)))
-        return e;
-    return cudaMemcpyAsync(h->cw.end, h->end2, sizeof(int) * (size_t)h->dp.C, cudaMemcpyDeviceToDevice, h->st);
+        if ((e = cudaMemcpyAsync(to[i], from[i], b, cudaMemcpyDeviceToDevice, h->st))) return e;
+    const size_t bi = sizeof(int) * (size_t)h->sc[s].dp.C;
+    if ((e = cudaMemcpyAsync(h->cw.start + co, h->start2 + co, bi, cudaMemcpyDeviceToDevice, h->st))) return e;
+    return cudaMemcpyAsync(h->cw.end + co, h->end2 + co, bi, cudaMemcpyDeviceToDevice, h->st);
 }
 
 static k3dom_status finish_sync(k3dom_handle* h) {
@@ -698,28 +906,65 @@ static k3dom_status finish_sync(k3dom_handle* h) {
     return K3DOM_OK;
 }
 
-static k3dom_status update_grid_impl(k3dom_handle* h, float t, const float* xs, const float* ys, const float* zs,
-                                     int32_t n, k3dom_mem mem, bool sync) {
-    if (!h) return K3DOM_ERR_INVALID_ARGUMENT;
-    if (n < 0 || (n > 0 && !xs)) return K3DOM_ERR_INVALID_ARGUMENT;
-    if (mem == K3DOM_MEM_HOST && n > 0 && has_nonfinite_host(xs, ys, zs, n)) return K3DOM_ERR_INVALID_INPUT;
+// One frame of every scene: t[s], points (xs[s], ys[s], zs[s], n[s]).
+static k3dom_status update_impl(k3dom_handle* h, const float* t, const float* const* xs, const float* const* ys,
+                                const float* const* zs, const int32_t* n, k3dom_mem mem, bool sync) {
+    if (!h || !t || !n || !xs) return K3DOM_ERR_INVALID_ARGUMENT;
+    const int S = h->S;
+    for (int s = 0; s < S; ++s) {
+        k3dom_status c = check_points(xs[s], ys ? ys[s] : nullptr, zs ? zs[s] : nullptr, n[s], mem);
+        if (c != K3DOM_OK) return c;
+    }
+    // scenes step together: the first frame initialises every scene (src/k3dom/dom.cu:32)
+    const bool steady = h->sc[0].updated_time > 0.0f;
+    for (int s = 1; s < S; ++s)
+        if ((h->sc[s].updated_time > 0.0f) != steady) return K3DOM_ERR_NOT_READY;
     cudaSetDevice(h->device);
-    const bool steady = h->updated_time > 0.0f;  // src/k3dom/dom.cu:32
-    const float dt = steady ? t - h->updated_time : 0.0f;
-    k3dom_status s = set_frame_params(h, dt, n);
-    if (s != K3DOM_OK) return s;
-    if ((s = upload_points(h, xs, ys, zs, n, mem)) != K3DOM_OK) return s;
+    k3dom_status st = grow_points(h, n);
+    if (st != K3DOM_OK) return st;
+    std::vector<float> dt(S);
+    std::vector<int> np(S);
+    for (int s = 0; s < S; ++s) {
+        dt[s] = steady ? t[s] - h->sc[s].updated_time : 0.0f;
+        np[s] = n[s];
+    }
+    if ((st = set_frame_params(h, dt.data(), np.data())) != K3DOM_OK) return st;
+    for (int s = 0; s < S; ++s) {
+        st = upload_points(h, s, xs[s], ys ? ys[s] : nullptr, zs ? zs[s] : nullptr, n[s], mem);
+        if (st != K3DOM_OK) return st;
+    }
     cudaError_t e;
+    bool timed = false;
     if (steady) {
-        if (h->timing || !h->graph_mode) {
-            if ((e = enq_frame(h))) return h->fail(e);
+        const bool tuning = h->tune_next >= 0;
+        if (tuning) {
+            const int k = h->tune_next;
+            if ((e = apply_tuning(h, k % kRuleCount, kTuneChunks[k / kRuleCount]))) return h->fail(e);
+            // the candidate's upload of this frame's points happened before any re-layout
+            // changed the point slots: stage them again
+            if ((st = set_frame_params(h, dt.data(), np.data())) != K3DOM_OK) return st;
+            for (int s = 0; s < S; ++s) {
+                st = upload_points(h, s, xs[s], ys ? ys[s] : nullptr, zs ? zs[s] : nullptr, n[s], mem);
+                if (st != K3DOM_OK) return st;
+            }
+        }
+        if (h->timing || !h->graph_mode || tuning) {
+            const bool was = h->timing;
+            h->timing = true;
+            e = enq_frame(h);
+            h->timing = was;
+            if (e) return h->fail(e);
+            timed = true;
         } else {
             if (!h->graph_exec) {
                 if ((e = cudaStreamBeginCapture(h->st, cudaStreamCaptureModeThreadLocal))) return h->fail(e);
                 cudaError_t ce = enq_frame(h);
                 cudaGraph_t g = nullptr;
                 e = cudaStreamEndCapture(h->st, &g);
-                if (ce != cudaSuccess) { if (g) cudaGraphDestroy(g); return h->fail(ce); }
+                if (ce != cudaSuccess) {
+                    if (g) cudaGraphDestroy(g);
+                    return h->fail(ce);
+                }
                 if (e != cudaSuccess) return h->fail(e);
                 h->graph = g;
                 if ((e = cudaGraphInstantiate(&h->graph_exec, g, 0))) return h->fail(e);
@@ -732,33 +977,68 @@ static k3dom_status update_grid_impl(k3dom_handle* h, float t, const float* xs, 
         if ((e = enq_occupancy(h, true))) return h->fail(e);
         if ((e = enq_init_particles(h))) return h->fail(e);
     }
-    h->shift_pending = false;
-    h->pending_shift[0] = h->pending_shift[1] = h->pending_shift[2] = 0;
-    h->updated_time = t;
-    h->frame += 1;
-    if (h->variant == K3DOM_VARIANT_DSPHDMIB) h->iteration += 1;  // src/dsphdmib/dom.cu:52
-    h->initialized = true;
-    if (!sync) return K3DOM_OK;
-    s = finish_sync(h);
-    if (s == K3DOM_OK && steady) read_times(h);
-    return s;
+    for (int s = 0; s < S; ++s) {
+        SceneHost& x = h->sc[s];
+        x.shift_pending = false;
+        x.pending_shift[0] = x.pending_shift[1] = x.pending_shift[2] = 0;
+        x.updated_time = t[s];
+        x.frame += 1;
+        if (h->ds()) x.iteration += 1;  // src/dsphdmib/dom.cu:52
+        x.initialized = true;
+    }
+    if (!sync && !timed) return K3DOM_OK;
+    st = finish_sync(h);
+    if (st != K3DOM_OK || !timed) return st;
+    read_times(h);
+    if (h->tune_next >= 0) {
+        // the evidence stage (ray lists + evidence kernels) decides between candidates
+        const float ms = h->times.occupancy_ms;
+        h->tune_ms[h->tune_next] = ms;
+        if (h->tune_next == 0 || ms < h->tune_best_ms) {
+            h->tune_best_ms = ms;
+            h->tune_best = h->tune_next;
+        }
+        h->tune_next += 1;
+        if (h->tune_next >= kTuneCount) {
+            h->tune_next = -1;
+            h->tuned = 1;
+            if ((e = apply_tuning(h, h->tune_best % kRuleCount, kTuneChunks[h->tune_best / kRuleCount])))
+                return h->fail(e);
+        }
+    }
+    return K3DOM_OK;
+}
+
+k3dom_status k3dom_batch_update(k3dom_handle* h, const float* t, const float* const* xs, const float* const* ys,
+                                const float* const* zs, const int32_t* n, k3dom_mem mem) {
+    return update_impl(h, t, xs, ys, zs, n, mem, true);
+}
+
+k3dom_status k3dom_batch_update_async(k3dom_handle* h, const float* t, const float* const* xs,
+                                      const float* const* ys, const float* const* zs, const int32_t* n,
+                                      k3dom_mem mem) {
+    return update_impl(h, t, xs, ys, zs, n, mem, false);
 }
 
 k3dom_status k3dom_update_grid(k3dom_handle* h, float t, const float* xs, const float* ys, const float* zs, int32_t n,
                                k3dom_mem mem) {
-    return update_grid_impl(h, t, xs, ys, zs, n, mem, true);
+    if (!h) return K3DOM_ERR_INVALID_ARGUMENT;
+    if (h->S != 1) return K3DOM_ERR_INVALID_ARGUMENT;
+    return update_impl(h, &t, &xs, &ys, &zs, &n, mem, true);
 }
 
 k3dom_status k3dom_update_grid_async(k3dom_handle* h, float t, const float* xs, const float* ys, const float* zs,
                                      int32_t n, k3dom_mem mem) {
-    return update_grid_impl(h, t, xs, ys, zs, n, mem, false);
+    if (!h) return K3DOM_ERR_INVALID_ARGUMENT;
+    if (h->S != 1) return K3DOM_ERR_INVALID_ARGUMENT;
+    return update_impl(h, &t, &xs, &ys, &zs, &n, mem, false);
 }
 
 k3dom_status k3dom_synchronize(k3dom_handle* h) {
     if (!h) return K3DOM_ERR_INVALID_ARGUMENT;
     cudaSetDevice(h->device);
     k3dom_status s = finish_sync(h);
-    if (s == K3DOM_OK) read_times(h);
+    if (s == K3DOM_OK && h->timing) read_times(h);
     return s;
 }
 
@@ -786,19 +1066,61 @@ k3dom_status k3dom_get_stage_times(k3dom_handle* h, k3dom_stage_times* out) {
     return K3DOM_OK;
 }
 
-// ---- stage calls
+// ---- evidence tuning
+k3dom_status k3dom_autotune(k3dom_handle* h, int enabled) {
+    if (!h) return K3DOM_ERR_INVALID_ARGUMENT;
+    if (enabled) {
+        h->tune_next = 0;
+        h->tuned = 0;
+        h->tune_ms.assign(kTuneCount, 0.0f);
+    } else {
+        h->tune_next = -1;
+    }
+    return K3DOM_OK;
+}
+
+k3dom_status k3dom_get_tuning(k3dom_handle* h, k3dom_tuning* out) {
+    if (!h || !out) return K3DOM_ERR_INVALID_ARGUMENT;
+    std::memset(out, 0, sizeof(*out));
+    out->tile_rule = h->tile_rule;
+    out->chunk = h->chunk;
+    out->tuned = h->tuned;
+    out->tuning = h->tune_next >= 0 ? 1 : 0;
+    out->candidates = kTuneCount;
+    out->best_ms = h->tune_best_ms;
+    for (int k = 0; k < kTuneCount && k < (int)h->tune_ms.size() && k < K3DOM_TUNE_MAX_CANDIDATES; ++k)
+        out->candidate_ms[k] = h->tune_ms[k];
+    out->evidence_blocks = h->ds() ? h->ds_grid : h->bgki_grid;
+    return K3DOM_OK;
+}
+
+k3dom_status k3dom_set_tuning(k3dom_handle* h, int32_t tile_rule, int32_t chunk) {
+    if (!h || tile_rule < 0 || tile_rule >= kRuleCount || chunk < 32 || chunk > 1024) return K3DOM_ERR_INVALID_ARGUMENT;
+    cudaSetDevice(h->device);
+    h->tune_next = -1;
+    cudaError_t e = apply_tuning(h, tile_rule, chunk);
+    return e == cudaSuccess ? K3DOM_OK : h->fail(e);
+}
+
+// ---- stage calls (all scenes; the point-taking calls need a single scene)
 #define STAGE_BEGIN                          \
     if (!h) return K3DOM_ERR_INVALID_ARGUMENT; \
     cudaSetDevice(h->device);                \
     cudaError_t e;
 
+static void clear_shifts(k3dom_handle* h) {
+    for (auto& x : h->sc) {
+        x.shift_pending = false;
+        x.pending_shift[0] = x.pending_shift[1] = x.pending_shift[2] = 0;
+    }
+}
+
 k3dom_status k3dom_particle_prediction(k3dom_handle* h, float dt) {
     STAGE_BEGIN
-    k3dom_status s = set_frame_params(h, dt, 0);
+    k3dom_status s = set_frame_params_all(h, dt, 0);
     if (s != K3DOM_OK) return s;
     if ((e = enq_predict(h))) return h->fail(e);
-    h->shift_pending = false;
-    h->pending_shift[0] = h->pending_shift[1] = h->pending_shift[2] = 0;
+    clear_shifts(h);
     return finish_sync(h);
 }
 
@@ -811,11 +1133,12 @@ k3dom_status k3dom_particle_assignment(k3dom_handle* h) {
 k3dom_status k3dom_grid_cell_occupancy_update(k3dom_handle* h, float dt, const float* xs, const float* ys,
                                               const float* zs, int32_t n, k3dom_mem mem) {
     STAGE_BEGIN
-    if (n < 0 || (n > 0 && !xs)) return K3DOM_ERR_INVALID_ARGUMENT;
-    if (mem == K3DOM_MEM_HOST && n > 0 && has_nonfinite_host(xs, ys, zs, n)) return K3DOM_ERR_INVALID_INPUT;
-    k3dom_status s = set_frame_params(h, dt, n);
+    if (h->S != 1) return K3DOM_ERR_INVALID_ARGUMENT;
+    k3dom_status s = check_points(xs, ys, zs, n, mem);
     if (s != K3DOM_OK) return s;
-    if ((s = upload_points(h, xs, ys, zs, n, mem)) != K3DOM_OK) return s;
+    if ((s = grow_points(h, &n)) != K3DOM_OK) return s;
+    if ((s = set_frame_params_all(h, dt, n)) != K3DOM_OK) return s;
+    if ((s = upload_points(h, 0, xs, ys, zs, n, mem)) != K3DOM_OK) return s;
     if ((e = enq_occupancy(h, false))) return h->fail(e);
     return finish_sync(h);
 }
@@ -828,7 +1151,7 @@ k3dom_status k3dom_update_persistent_particles(k3dom_handle* h) {
 
 k3dom_status k3dom_initialize_new_particles(k3dom_handle* h) {
     STAGE_BEGIN
-    k3dom_status s = set_frame_params(h, h->fp_host->dt, h->fp_host->n_points);
+    k3dom_status s = set_frame_params_all(h, h->fp_host[0].dt, h->fp_host[0].n_points);
     if (s != K3DOM_OK) return s;
     if ((e = enq_births(h))) return h->fail(e);
     h->births_done = true;
@@ -842,7 +1165,7 @@ k3dom_status k3dom_statistical_moments(k3dom_handle* h) {
 
 k3dom_status k3dom_resampling(k3dom_handle* h) {
     STAGE_BEGIN
-    k3dom_status s = set_frame_params(h, h->fp_host->dt, h->fp_host->n_points);
+    k3dom_status s = set_frame_params_all(h, h->fp_host[0].dt, h->fp_host[0].n_points);
     if (s != K3DOM_OK) return s;
     if ((e = enq_resample(h, false))) return h->fail(e);
     return finish_sync(h);
@@ -851,11 +1174,12 @@ k3dom_status k3dom_resampling(k3dom_handle* h) {
 k3dom_status k3dom_initialize_particles(k3dom_handle* h, const float* xs, const float* ys, const float* zs, int32_t n,
                                         k3dom_mem mem) {
     STAGE_BEGIN
-    if (n < 0 || (n > 0 && !xs)) return K3DOM_ERR_INVALID_ARGUMENT;
-    if (mem == K3DOM_MEM_HOST && n > 0 && has_nonfinite_host(xs, ys, zs, n)) return K3DOM_ERR_INVALID_INPUT;
-    k3dom_status s = set_frame_params(h, 0.0f, n);
+    if (h->S != 1) return K3DOM_ERR_INVALID_ARGUMENT;
+    k3dom_status s = check_points(xs, ys, zs, n, mem);
     if (s != K3DOM_OK) return s;
-    if ((s = upload_points(h, xs, ys, zs, n, mem)) != K3DOM_OK) return s;
+    if ((s = grow_points(h, &n)) != K3DOM_OK) return s;
+    if ((s = set_frame_params_all(h, 0.0f, n)) != K3DOM_OK) return s;
+    if ((s = upload_points(h, 0, xs, ys, zs, n, mem)) != K3DOM_OK) return s;
     if ((e = enq_occupancy(h, true))) return h->fail(e);
     if ((e = enq_init_particles(h))) return h->fail(e);
     return finish_sync(h);
@@ -863,55 +1187,60 @@ k3dom_status k3dom_initialize_particles(k3dom_handle* h, const float* xs, const 
 
 k3dom_status k3dom_finish_frame(k3dom_handle* h, float t) {
     if (!h) return K3DOM_ERR_INVALID_ARGUMENT;
-    h->updated_time = t;
-    h->frame += 1;
-    if (h->variant == K3DOM_VARIANT_DSPHDMIB) h->iteration += 1;
-    h->initialized = true;
+    for (auto& x : h->sc) {
+        x.updated_time = t;
+        x.frame += 1;
+        if (h->ds()) x.iteration += 1;
+        x.initialized = true;
+    }
     return K3DOM_OK;
 }
 
 k3dom_status k3dom_set_frame_index(k3dom_handle* h, int32_t frame) {
     if (!h || frame < 0) return K3DOM_ERR_INVALID_ARGUMENT;
-    h->frame = (uint32_t)frame;
+    for (auto& x : h->sc) x.frame = (uint32_t)frame;
     return K3DOM_OK;
 }
 
-// ---- info
+// ---- info (selected scene)
 k3dom_status k3dom_get_info(k3dom_handle* h, k3dom_info* o) {
     if (!h || !o) return K3DOM_ERR_INVALID_ARGUMENT;
-    o->grid_size = h->dp.G;
-    o->grid_size_z = h->dp.Gz;
-    o->grid_cell_count = h->dp.C;
-    o->particle_count = h->dp.P;
-    o->new_born_particle_count = h->dp.B;
-    o->iteration = h->iteration;
+    const SceneHost& x = h->sc[h->cur];
+    o->grid_size = x.dp.G;
+    o->grid_size_z = x.dp.Gz;
+    o->grid_cell_count = x.dp.C;
+    o->particle_count = x.dp.P;
+    o->new_born_particle_count = x.dp.B;
+    o->iteration = x.iteration;
     o->variant = (int)h->variant;
-    o->initialized = h->initialized ? 1 : 0;
-    o->resolution = h->params.resolution;
-    o->center_x = h->center_pos[0];
-    o->center_y = h->center_pos[1];
-    o->center_z = h->center_pos[2];
-    o->sensor_x = h->sensor_pos[0];
-    o->sensor_y = h->sensor_pos[1];
-    o->sensor_z = h->sensor_pos[2];
-    o->updated_time = h->updated_time;
-    o->max_points = h->rb.max_points;
-    o->frame_index = (int32_t)h->frame;
+    o->initialized = x.initialized ? 1 : 0;
+    o->resolution = x.params.resolution;
+    o->center_x = x.center_pos[0];
+    o->center_y = x.center_pos[1];
+    o->center_z = x.center_pos[2];
+    o->sensor_x = x.sensor_pos[0];
+    o->sensor_y = x.sensor_pos[1];
+    o->sensor_z = x.sensor_pos[2];
+    o->updated_time = x.updated_time;
+    o->max_points = x.max_points;
+    o->frame_index = (int32_t)x.frame;
     return K3DOM_OK;
 }
 
 k3dom_status k3dom_index_to_coord(k3dom_handle* h, int32_t i, float* x, float* y, float* z) {
     // DOM_c::indexToCoordX/Y/Z (include/common/dom.h:70-81)
-    if (!h || i < 0 || i >= h->dp.C) return K3DOM_ERR_INVALID_ARGUMENT;
-    const int G = h->dp.G;
-    const float r = h->params.resolution;
-    if (x) *x = (i % G + 0.5f) * r - h->params.size / 2.0f + h->center_pos[0];
-    if (y) *y = ((i % (G * G)) / G + 0.5f) * r - h->params.size / 2.0f + h->center_pos[1];
-    if (z) *z = (i / (G * G) + 0.5f) * r - h->params.size_z / 2.0f + h->center_pos[2];
+    if (!h) return K3DOM_ERR_INVALID_ARGUMENT;
+    const SceneHost& s = h->sc[h->cur];
+    if (i < 0 || i >= s.dp.C) return K3DOM_ERR_INVALID_ARGUMENT;
+    const int G = s.dp.G;
+    const float r = s.params.resolution;
+    if (x) *x = (i % G + 0.5f) * r - s.params.size / 2.0f + s.center_pos[0];
+    if (y) *y = ((i % (G * G)) / G + 0.5f) * r - s.params.size / 2.0f + s.center_pos[1];
+    if (z) *z = (i / (G * G) + 0.5f) * r - s.params.size_z / 2.0f + s.center_pos[2];
     return K3DOM_OK;
 }
 
-// ---- readback
+// ---- readback (selected scene)
 static k3dom_status ensure_export(k3dom_handle* h, size_t bytes) {
     if (h->export_bytes >= bytes) return K3DOM_OK;
     if (h->export_buf) cudaFree(h->export_buf);
@@ -931,17 +1260,46 @@ static k3dom_status deliver(k3dom_handle* h, void* dst, const void* dev_src, siz
     return e == cudaSuccess ? K3DOM_OK : h->fail(e);
 }
 
+// dst[i] = src[i] - base where src[i] >= 0 (global -> scene-local indices); weights: |w|.
+__global__ void k_rebase(const int* __restrict__ src, int* __restrict__ dst, int n, int base, int keep_neg) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const int v = src[i];
+    dst[i] = (keep_neg && v < 0) ? v : v - base;
+}
+
+// strips the penalty flag (sign bit) kept in the sorted and birth weights between stages
+__global__ void k_abs_copy(const float* __restrict__ src, float* __restrict__ dst, int n) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) dst[i] = fabsf(src[i]);
+}
+
+static k3dom_status deliver_rebased(k3dom_handle* h, int32_t* dst, const int* src, int n, int base, bool keep_neg,
+                                    k3dom_mem mem) {
+    k3dom_status s = ensure_export(h, sizeof(int) * (size_t)std::max(n, 1));
+    if (s != K3DOM_OK) return s;
+    ++g_launches;
+    k_rebase<<<div_up(std::max(n, 1), 256), 256, 0, h->st>>>(src, (int*)h->export_buf, n, base, keep_neg ? 1 : 0);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return h->fail(e);
+    return deliver(h, dst, h->export_buf, sizeof(int) * (size_t)n, mem);
+}
+
 k3dom_status k3dom_get_cell_field(k3dom_handle* h, k3dom_cell_field field, float* dst, k3dom_mem mem) {
     if (!h || !dst || (int)field < 0 || field >= K3DOM_CELL_FIELD_COUNT) return K3DOM_ERR_INVALID_ARGUMENT;
     cudaSetDevice(h->device);
-    const size_t bytes = sizeof(float) * (size_t)h->dp.C;
+    const int s = h->cur;
+    const SceneHost& x = h->sc[s];
+    const long co = h->off.cell[s];
+    const size_t bytes = sizeof(float) * (size_t)x.dp.C;
     float* out = dst;
     if (mem == K3DOM_MEM_HOST) {
-        k3dom_status s = ensure_export(h, bytes);
-        if (s != K3DOM_OK) return s;
+        k3dom_status r = ensure_export(h, bytes);
+        if (r != K3DOM_OK) return r;
         out = (float*)h->export_buf;
     }
-    launch_export_field(h->dp, (int)field, h->cells(), h->cw, h->births_done ? h->born_cum : nullptr, out, h->st);
+    launch_export_field(x.dp, (int)field, offset_cells(h->cells(), co), offset_work(h->cw, co),
+                        h->births_done ? h->born_cum + co : nullptr, h->off.part[s], out, h->st);
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return h->fail(e);
     if (mem == K3DOM_MEM_HOST) return deliver(h, dst, out, bytes, mem);
@@ -952,24 +1310,30 @@ k3dom_status k3dom_get_cell_field(k3dom_handle* h, k3dom_cell_field field, float
 k3dom_status k3dom_get_cell_ranges(k3dom_handle* h, int32_t* start, int32_t* end, k3dom_mem mem) {
     if (!h) return K3DOM_ERR_INVALID_ARGUMENT;
     cudaSetDevice(h->device);
-    const size_t bytes = sizeof(int) * (size_t)h->dp.C;
-    k3dom_status s = K3DOM_OK;
-    if (start) s = deliver(h, start, h->cw.start, bytes, mem);
-    if (s == K3DOM_OK && end) s = deliver(h, end, h->cw.end, bytes, mem);
-    return s;
+    const int s = h->cur;
+    const long co = h->off.cell[s];
+    const int C = h->sc[s].dp.C, base = h->off.part[s];
+    k3dom_status r = K3DOM_OK;
+    if (start) r = deliver_rebased(h, start, h->cw.start + co, C, base, true, mem);
+    if (r == K3DOM_OK && end) r = deliver_rebased(h, end, h->cw.end + co, C, base, true, mem);
+    return r;
 }
 
 k3dom_status k3dom_get_gridcell_aos(k3dom_handle* h, void* dst, k3dom_mem mem) {
     if (!h || !dst) return K3DOM_ERR_INVALID_ARGUMENT;
     cudaSetDevice(h->device);
-    const size_t bytes = (size_t)K3DOM_GRIDCELL_BYTES * h->dp.C;
+    const int s = h->cur;
+    const SceneHost& x = h->sc[s];
+    const long co = h->off.cell[s];
+    const size_t bytes = (size_t)K3DOM_GRIDCELL_BYTES * x.dp.C;
     void* out = dst;
     if (mem == K3DOM_MEM_HOST) {
-        k3dom_status s = ensure_export(h, bytes);
-        if (s != K3DOM_OK) return s;
+        k3dom_status r = ensure_export(h, bytes);
+        if (r != K3DOM_OK) return r;
         out = h->export_buf;
     }
-    launch_export_gridcell(h->dp, h->cells(), h->cw, h->births_done ? h->born_cum : nullptr, out, h->st);
+    launch_export_gridcell(x.dp, offset_cells(h->cells(), co), offset_work(h->cw, co),
+                           h->births_done ? h->born_cum + co : nullptr, h->off.part[s], out, h->st);
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return h->fail(e);
     if (mem == K3DOM_MEM_HOST) return deliver(h, dst, out, bytes, mem);
@@ -980,14 +1344,18 @@ k3dom_status k3dom_get_gridcell_aos(k3dom_handle* h, void* dst, k3dom_mem mem) {
 k3dom_status k3dom_get_mappoints(k3dom_handle* h, float* dst, k3dom_mem mem) {
     if (!h || !dst) return K3DOM_ERR_INVALID_ARGUMENT;
     cudaSetDevice(h->device);
-    const size_t bytes = sizeof(float) * K3DOM_MAPPOINT_FLOATS * (size_t)h->dp.C;
+    const int s = h->cur;
+    const SceneHost& x = h->sc[s];
+    const long co = h->off.cell[s];
+    const size_t bytes = sizeof(float) * K3DOM_MAPPOINT_FLOATS * (size_t)x.dp.C;
     float* out = dst;
     if (mem == K3DOM_MEM_HOST) {
-        k3dom_status s = ensure_export(h, bytes);
-        if (s != K3DOM_OK) return s;
+        k3dom_status r = ensure_export(h, bytes);
+        if (r != K3DOM_OK) return r;
         out = (float*)h->export_buf;
     }
-    launch_export_mappoints(h->dp, h->center_pos[0], h->center_pos[1], h->center_pos[2], h->cells(), h->cw, out, h->st);
+    launch_export_mappoints(x.dp, x.center_pos[0], x.center_pos[1], x.center_pos[2], offset_cells(h->cells(), co),
+                            offset_work(h->cw, co), out, h->st);
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return h->fail(e);
     if (mem == K3DOM_MEM_HOST) return deliver(h, dst, out, bytes, mem);
@@ -999,9 +1367,10 @@ k3dom_status k3dom_set_cell_masses(k3dom_handle* h, const float* f, const float*
                                    k3dom_mem mem) {
     if (!h) return K3DOM_ERR_INVALID_ARGUMENT;
     cudaSetDevice(h->device);
-    const size_t bytes = sizeof(float) * (size_t)h->dp.C;
+    const long co = h->off.cell[h->cur];
+    const size_t bytes = sizeof(float) * (size_t)h->sc[h->cur].dp.C;
     const cudaMemcpyKind k = mem == K3DOM_MEM_HOST ? cudaMemcpyHostToDevice : cudaMemcpyDeviceToDevice;
-    CellState c = h->cells();
+    const CellState c = offset_cells(h->cells(), co);
     cudaError_t e;
     if (f && (e = cudaMemcpyAsync(c.free_m, f, bytes, k, h->st))) return h->fail(e);
     if (s && (e = cudaMemcpyAsync(c.static_m, s, bytes, k, h->st))) return h->fail(e);
@@ -1011,19 +1380,14 @@ k3dom_status k3dom_set_cell_masses(k3dom_handle* h, const float* f, const float*
     return e == cudaSuccess ? K3DOM_OK : h->fail(e);
 }
 
-static Particles* pick_set(k3dom_handle* h, k3dom_particle_set set, int* n) {
+static bool pick_set(k3dom_handle* h, k3dom_particle_set set, Particles* q, int* n) {
+    const int s = h->cur;
     switch (set) {
-        case K3DOM_PARTICLES_PERSISTENT: *n = h->dp.P; return &h->A;
-        case K3DOM_PARTICLES_SORTED: *n = h->dp.P; return &h->S;
-        case K3DOM_PARTICLES_BIRTH: *n = h->dp.B; return &h->Bp;
+        case K3DOM_PARTICLES_PERSISTENT: *n = h->sc[s].dp.P; *q = offset_particles(h->A, h->off.part[s]); return true;
+        case K3DOM_PARTICLES_SORTED: *n = h->sc[s].dp.P; *q = offset_particles(h->Ss, h->off.part[s]); return true;
+        case K3DOM_PARTICLES_BIRTH: *n = h->sc[s].dp.B; *q = offset_particles(h->Bp, h->off.birth[s]); return true;
     }
-    return nullptr;
-}
-
-// strips the penalty flag (sign bit) kept in the sorted and birth weights between stages
-__global__ void k_abs_copy(const float* __restrict__ src, float* __restrict__ dst, int n) {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i < n) dst[i] = fabsf(src[i]);
+    return false;
 }
 
 k3dom_status k3dom_get_particles(k3dom_handle* h, k3dom_particle_set set, float* pos, float* vel, float* weight,
@@ -1031,8 +1395,8 @@ k3dom_status k3dom_get_particles(k3dom_handle* h, k3dom_particle_set set, float*
     if (!h) return K3DOM_ERR_INVALID_ARGUMENT;
     cudaSetDevice(h->device);
     int n = 0;
-    Particles* q = pick_set(h, set, &n);
-    if (!q) return K3DOM_ERR_INVALID_ARGUMENT;
+    Particles q;
+    if (!pick_set(h, set, &q, &n)) return K3DOM_ERR_INVALID_ARGUMENT;
     const cudaMemcpyKind k = mem == K3DOM_MEM_HOST ? cudaMemcpyDeviceToHost : cudaMemcpyDeviceToDevice;
     cudaError_t e;
     auto strided = [&](float* dst, const float* a, const float* b, const float* c) -> cudaError_t {
@@ -1041,17 +1405,21 @@ k3dom_status k3dom_get_particles(k3dom_handle* h, k3dom_particle_set set, float*
         if ((r = cudaMemcpy2DAsync(dst + 1, 3 * sizeof(float), b, sizeof(float), sizeof(float), n, k, h->st))) return r;
         return cudaMemcpy2DAsync(dst + 2, 3 * sizeof(float), c, sizeof(float), sizeof(float), n, k, h->st);
     };
-    if (pos && (e = strided(pos, q->px, q->py, q->pz))) return h->fail(e);
-    if (vel && (e = strided(vel, q->vx, q->vy, q->vz))) return h->fail(e);
+    if (pos && (e = strided(pos, q.px, q.py, q.pz))) return h->fail(e);
+    if (vel && (e = strided(vel, q.vx, q.vy, q.vz))) return h->fail(e);
     if (weight) {
         k3dom_status s = ensure_export(h, sizeof(float) * (size_t)n);
         if (s != K3DOM_OK) return s;
         ++g_launches;
-        k_abs_copy<<<div_up(n, 256), 256, 0, h->st>>>(q->w, (float*)h->export_buf, n);
+        k_abs_copy<<<div_up(n, 256), 256, 0, h->st>>>(q.w, (float*)h->export_buf, n);
         if ((e = cudaMemcpyAsync(weight, h->export_buf, sizeof(float) * (size_t)n, k, h->st))) return h->fail(e);
+        if ((e = cudaStreamSynchronize(h->st))) return h->fail(e);
     }
-    if (cell_idx && (e = cudaMemcpyAsync(cell_idx, q->cell, sizeof(int) * (size_t)n, k, h->st))) return h->fail(e);
-    if (associated && (e = cudaMemcpyAsync(associated, q->assoc, (size_t)n, k, h->st))) return h->fail(e);
+    if (cell_idx) {
+        k3dom_status s = deliver_rebased(h, cell_idx, q.cell, n, h->off.cell[h->cur], false, mem);
+        if (s != K3DOM_OK) return s;
+    }
+    if (associated && (e = cudaMemcpyAsync(associated, q.assoc, (size_t)n, k, h->st))) return h->fail(e);
     e = cudaStreamSynchronize(h->st);
     return e == cudaSuccess ? K3DOM_OK : h->fail(e);
 }
@@ -1061,15 +1429,20 @@ __global__ void k_iota(uint32_t* a, int n) {
     if (i < n) a[i] = (uint32_t)i;
 }
 
+__global__ void k_add_base(int* a, int n, int base) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) a[i] += base;
+}
+
 k3dom_status k3dom_set_particles(k3dom_handle* h, k3dom_particle_set set, const float* pos, const float* vel,
                                  const float* weight, const int32_t* cell_idx, const uint8_t* associated,
                                  k3dom_mem mem) {
     if (!h) return K3DOM_ERR_INVALID_ARGUMENT;
     cudaSetDevice(h->device);
     int n = 0;
-    Particles* q = pick_set(h, set, &n);
-    if (!q) return K3DOM_ERR_INVALID_ARGUMENT;
-    if (set == K3DOM_PARTICLES_SORTED && !cell_idx) return K3DOM_ERR_INVALID_ARGUMENT;
+    Particles q;
+    if (!pick_set(h, set, &q, &n)) return K3DOM_ERR_INVALID_ARGUMENT;
+    if (set == K3DOM_PARTICLES_SORTED && (!cell_idx || h->S != 1)) return K3DOM_ERR_INVALID_ARGUMENT;
     const cudaMemcpyKind k = mem == K3DOM_MEM_HOST ? cudaMemcpyHostToDevice : cudaMemcpyDeviceToDevice;
     cudaError_t e;
     auto strided = [&](const float* src, float* a, float* b, float* c) -> cudaError_t {
@@ -1078,20 +1451,27 @@ k3dom_status k3dom_set_particles(k3dom_handle* h, k3dom_particle_set set, const 
         if ((r = cudaMemcpy2DAsync(b, sizeof(float), src + 1, 3 * sizeof(float), sizeof(float), n, k, h->st))) return r;
         return cudaMemcpy2DAsync(c, sizeof(float), src + 2, 3 * sizeof(float), sizeof(float), n, k, h->st);
     };
-    if (pos && (e = strided(pos, q->px, q->py, q->pz))) return h->fail(e);
-    if (vel && (e = strided(vel, q->vx, q->vy, q->vz))) return h->fail(e);
-    if (weight && (e = cudaMemcpyAsync(q->w, weight, sizeof(float) * (size_t)n, k, h->st))) return h->fail(e);
-    if (cell_idx && (e = cudaMemcpyAsync(q->cell, cell_idx, sizeof(int) * (size_t)n, k, h->st))) return h->fail(e);
-    if (associated && (e = cudaMemcpyAsync(q->assoc, associated, (size_t)n, k, h->st))) return h->fail(e);
+    if (pos && (e = strided(pos, q.px, q.py, q.pz))) return h->fail(e);
+    if (vel && (e = strided(vel, q.vx, q.vy, q.vz))) return h->fail(e);
+    if (weight && (e = cudaMemcpyAsync(q.w, weight, sizeof(float) * (size_t)n, k, h->st))) return h->fail(e);
+    if (cell_idx) {
+        if ((e = cudaMemcpyAsync(q.cell, cell_idx, sizeof(int) * (size_t)n, k, h->st))) return h->fail(e);
+        const int base = h->off.cell[h->cur];
+        if (base != 0) {
+            ++g_launches;
+            k_add_base<<<div_up(n, 256), 256, 0, h->st>>>(q.cell, n, base);
+        }
+    }
+    if (associated && (e = cudaMemcpyAsync(q.assoc, associated, (size_t)n, k, h->st))) return h->fail(e);
     if (set == K3DOM_PARTICLES_SORTED) {
         // a sorted set defines the cell ranges and sums: rebuild them from it in place
-        if ((e = cudaMemcpyAsync(h->sorted_keys, q->cell, sizeof(int) * (size_t)n, cudaMemcpyDeviceToDevice, h->st)))
+        if ((e = cudaMemcpyAsync(h->sorted_keys, q.cell, sizeof(int) * (size_t)n, cudaMemcpyDeviceToDevice, h->st)))
             return h->fail(e);
         ++g_launches;
         k_iota<<<div_up(n, 256), 256, 0, h->st>>>(h->perm, n);
-        if ((e = cudaMemsetAsync(h->cw.start, 0xFF, sizeof(int) * (size_t)h->dp.C, h->st))) return h->fail(e);
-        if ((e = cudaMemsetAsync(h->cw.end, 0xFF, sizeof(int) * (size_t)h->dp.C, h->st))) return h->fail(e);
-        launch_gather_segsum(h->dp, h->S, h->S, h->sorted_keys, h->perm, h->cw, h->st);
+        if ((e = cudaMemsetAsync(h->cw.start, 0xFF, sizeof(int) * (size_t)h->C, h->st))) return h->fail(e);
+        if ((e = cudaMemsetAsync(h->cw.end, 0xFF, sizeof(int) * (size_t)h->C, h->st))) return h->fail(e);
+        launch_gather_segsum(h->batch(), h->Ss, h->Ss, h->sorted_keys, h->perm, h->cw, h->st);
     }
     e = cudaStreamSynchronize(h->st);
     return e == cudaSuccess ? K3DOM_OK : h->fail(e);
@@ -1100,24 +1480,31 @@ k3dom_status k3dom_set_particles(k3dom_handle* h, k3dom_particle_set set, const 
 k3dom_status k3dom_get_sort_permutation(k3dom_handle* h, int32_t* perm, k3dom_mem mem) {
     if (!h || !perm) return K3DOM_ERR_INVALID_ARGUMENT;
     cudaSetDevice(h->device);
-    return deliver(h, perm, h->perm, sizeof(int) * (size_t)h->dp.P, mem);
+    const int s = h->cur;
+    return deliver_rebased(h, perm, reinterpret_cast<const int*>(h->perm) + h->off.part[s], h->sc[s].dp.P,
+                           h->off.part[s], false, mem);
 }
 
 k3dom_status k3dom_get_ancestors(k3dom_handle* h, int32_t* anc, k3dom_mem mem) {
     if (!h || !anc) return K3DOM_ERR_INVALID_ARGUMENT;
     cudaSetDevice(h->device);
-    return deliver(h, anc, h->ancestors, sizeof(int) * (size_t)h->dp.P, mem);
+    const int s = h->cur;
+    return deliver(h, anc, h->ancestors + h->off.part[s], sizeof(int) * (size_t)h->sc[s].dp.P, mem);
 }
 
 k3dom_status k3dom_get_resampling_state(k3dom_handle* h, float* joint_cum, float* born_cum, float* joint_max,
                                         k3dom_mem mem) {
     if (!h) return K3DOM_ERR_INVALID_ARGUMENT;
     cudaSetDevice(h->device);
-    k3dom_status s = K3DOM_OK;
-    if (joint_cum) s = deliver(h, joint_cum, h->joint_cum, sizeof(float) * ((size_t)h->dp.P + h->dp.B), mem);
-    if (s == K3DOM_OK && born_cum) s = deliver(h, born_cum, h->born_cum, sizeof(float) * (size_t)h->dp.C, mem);
-    if (s == K3DOM_OK && joint_max) s = deliver(h, joint_max, h->joint_max, sizeof(float), mem);
-    return s;
+    const int s = h->cur;
+    const SceneHost& x = h->sc[s];
+    k3dom_status r = K3DOM_OK;
+    if (joint_cum)
+        r = deliver(h, joint_cum, h->joint_cum + h->off.joint[s], sizeof(float) * ((size_t)x.dp.P + x.dp.B), mem);
+    if (r == K3DOM_OK && born_cum)
+        r = deliver(h, born_cum, h->born_cum + h->off.cell[s], sizeof(float) * (size_t)x.dp.C, mem);
+    if (r == K3DOM_OK && joint_max) r = deliver(h, joint_max, h->joint_max + s, sizeof(float), mem);
+    return r;
 }
 
 k3dom_status k3dom_debug_draws(uint64_t seed, int32_t frame, int32_t stage, int64_t first, int64_t count, float* dst,
@@ -1128,7 +1515,8 @@ k3dom_status k3dom_debug_draws(uint64_t seed, int32_t frame, int32_t stage, int6
     float* out = dst;
     cudaError_t e;
     if (mem == K3DOM_MEM_HOST) {
-        if ((e = cudaMalloc((void**)&out, std::max<size_t>(bytes, 4)))) return e == cudaErrorMemoryAllocation ? K3DOM_ERR_OUT_OF_MEMORY : K3DOM_ERR_CUDA;
+        if ((e = cudaMalloc((void**)&out, std::max<size_t>(bytes, 4))))
+            return e == cudaErrorMemoryAllocation ? K3DOM_ERR_OUT_OF_MEMORY : K3DOM_ERR_CUDA;
     }
     launch_debug_draws(seed, frame, stage, first, count, out, 0);
     e = cudaGetLastError();

@@ -1,4 +1,5 @@
-// evidence.cu -- measurement evidence and the per-cell mass update.
+// evidence.cu -- measurement evidence and the per-cell mass update, for every scene of a batch
+// in one launch per kernel.
 //
 // K3DOM: Bayesian kernel inference (BGKI, src/k3dom/kernel/mass_update.cu:32-77) followed by
 // predict_mass / update_mass / separate_newborn_part (:79-150), with the per-cell parts of
@@ -11,14 +12,19 @@
 // points). Both evidence models have compact support -- the sparse kernel is zero beyond
 // ls, the DS window is 0.866 res wide -- so each ray is binned to the tiles of cells its
 // support can reach (segment sensor->point with radius ls for K3DOM, the half-line through
-// the point with the window radius for DS). A tile's list keeps rays in input order (stable
-// sort by tile). One CTA takes one (tile, chunk of <= kChunk rays) work item from a device
-// work counter: it stages the chunk's ray data in shared memory; each warp owns 4x4x2-cell
-// sub-blocks and culls 32 rays at a time with one ballot; every lane then evaluates the
-// surviving rays for its own cell. K3DOM evidence is accumulated in FP64 registers; chunks of
-// one tile are combined through 64-bit fixed-point atomics (integer addition is associative,
-// so the result does not depend on the order in which chunks finish) and the last chunk to
-// finish runs the cell update. No block ever waits on another.
+// the point with the window radius for DS). Tiles of all scenes share one global numbering
+// (scene tile offset + local tile), so one sort builds every scene's lists. A tile's list keeps
+// rays in input order (stable sort by tile). One CTA takes one (tile, chunk of rays) work item
+// from a device work counter and stages the chunk's rays in shared memory; its warps pull the
+// tile's 4x4x2-cell sub-blocks from a block-local counter, cull 32 rays at a time with one
+// ballot, and every lane evaluates the surviving rays for its own cell.
+//
+// K3DOM evidence is summed in fixed point: each kernel value is rounded once to an integer
+// number of units of 2^-k sigma (the table carries the scale), summed exactly (FP64 within a
+// chunk, 64-bit integer atomics across chunks), so a cell's evidence is the same for any
+// tiling, chunking or scheduling. The
+// last CTA to finish a tile's chunks runs the cell update for the whole tile. No block ever
+// waits on another.
 #include <cuda_runtime.h>
 #include <math.h>
 
@@ -32,7 +38,7 @@
 
 namespace k3dom {
 
-constexpr int kChunk = 1024;
+constexpr int kChunk = 1024;      // largest number of rays per work item
 constexpr int kKernelTab = 512;  // intervals of the sparse-kernel table over u = d^2 / ls^2
 constexpr int kEvThreads = 256;
 constexpr int kEvWarps = kEvThreads / 32;
@@ -145,12 +151,11 @@ struct RayPrep {
 // Per-ray constants. K3DOM: (m, d_m) and (m/d_m, margin), d_m and margin as the reference
 // forms them (mass_update.cu:29-31,55). DS: (m, |m|^2) as measurement_grid.cu:90.
 __device__ __forceinline__ RayPrep prep_ray(const DevParams& p, const BinGeom& g, float mx, float my, float mz,
-                                           bool ds, float4* ra, float4* rb, double4* rc) {
+                                           bool ds, float4* ra, double4* rc) {
     RayPrep r;
     r.ok = isfinite(mx) && isfinite(my) && isfinite(mz);
     r.bx = r.by = r.bz = 0.0f;
     *ra = make_float4(0.f, 0.f, 0.f, 0.f);
-    *rb = make_float4(0.f, 0.f, 0.f, 0.f);
     *rc = make_double4(0.0, 0.0, 0.0, 0.0);
     if (!r.ok) return r;
     const float sq = __fadd_rn(__fadd_rn(__fmul_rn(mx, mx), __fmul_rn(my, my)), __fmul_rn(mz, mz));
@@ -162,7 +167,6 @@ __device__ __forceinline__ RayPrep prep_ray(const DevParams& p, const BinGeom& g
         const double inv = dmd > 0.0 ? 1.0 / dmd : 0.0;
         const float dm = (float)dmd;
         *ra = make_float4(mx, my, mz, dm);
-        *rb = make_float4((float)(mx * inv), (float)(my * inv), (float)(mz * inv), (float)margd);
         *rc = make_double4(dmd, margd, inv, 0.0);
         r.bx = g.ax + mx / p.res;
         r.by = g.ay + my / p.res;
@@ -183,66 +187,86 @@ __device__ __forceinline__ RayPrep prep_ray(const DevParams& p, const BinGeom& g
     return r;
 }
 
-__global__ void k_ray_count(DevParams p, const FrameParams* __restrict__ fpp, BinGeom g,
-                            const float* __restrict__ xs, const float* __restrict__ ys,
-                            const float* __restrict__ zs, int ds, float4* __restrict__ ra,
-                            float4* __restrict__ rb, double4* __restrict__ rc, uint32_t* __restrict__ counts,
-                            DevStatus* status) {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    const FrameParams f = *fpp;
-    const int n = f.n_points;
-    if (i >= n) return;
-    place_sensor(g, p, f);
-    const float mx = xs[i], my = ys[i], mz = zs[i];
-    float4 a, b;
-    double4 cc;
-    const RayPrep r = prep_ray(p, g, mx, my, mz, ds != 0, &a, &b, &cc);
-    ra[i] = a;
-    rb[i] = b;
-    rc[i] = cc;
-    uint32_t c = 0;
-    if (r.ok) {
-        for_each_tile(g, r.bx, r.by, r.bz, [&](int) { ++c; });
-    } else if (!(isfinite(mx) && isfinite(my) && isfinite(mz))) {
-        atomicAdd(&status->nonfinite_points, 1ull);
-    }
-    counts[i] = c;
+
+__device__ __forceinline__ BinGeom scene_geom(const SceneDev& sd, const FrameParams& f) {
+    BinGeom g;
+    g.R = sd.bin_R;
+    g.G = sd.p.G;
+    g.Gz = sd.p.Gz;
+    g.tx = sd.ts.tx; g.ty = sd.ts.ty; g.tz = sd.ts.tz;
+    g.ntx = sd.ts.ntx; g.nty = sd.ts.nty; g.ntz = sd.ts.ntz;
+    place_sensor(g, sd.p, f);
+    return g;
 }
 
-__global__ void k_ray_emit(DevParams p, const FrameParams* __restrict__ fpp, BinGeom g,
-                           const float* __restrict__ xs, const float* __restrict__ ys,
+// Pass 1 over every point slot of every scene: per-ray constants and the number of tiles the
+// ray's support reaches (0 for slots past the scene's point count).
+__global__ void k_ray_count(Batch bt, const float* __restrict__ xs, const float* __restrict__ ys,
+                            const float* __restrict__ zs, int ds, float4* __restrict__ ra,
+                            double4* __restrict__ rc, uint32_t* __restrict__ counts, DevStatus* status) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < bt.N; i += gridDim.x * blockDim.x) {
+        const int sc = scene_of(bt.off->point, bt.S, i);
+        const FrameParams f = bt.fp[sc];
+        if (i - bt.off->point[sc] >= f.n_points) {
+            counts[i] = 0;
+            continue;
+        }
+        const SceneDev& sd = bt.sc[sc];
+        const BinGeom g = scene_geom(sd, f);
+        const float mx = xs[i], my = ys[i], mz = zs[i];
+        float4 a;
+        double4 cc;
+        const RayPrep r = prep_ray(sd.p, g, mx, my, mz, ds != 0, &a, &cc);
+        ra[i] = a;
+        rc[i] = cc;
+        uint32_t c = 0;
+        if (r.ok) {
+            for_each_tile(g, r.bx, r.by, r.bz, [&](int) { ++c; });
+        } else if (!(isfinite(mx) && isfinite(my) && isfinite(mz))) {
+            atomicAdd(&status->nonfinite_points, 1ull);
+        }
+        counts[i] = c;
+    }
+}
+
+// Pass 2: (global tile, ray) entries at the ray's scanned offset.
+__global__ void k_ray_emit(Batch bt, const float* __restrict__ xs, const float* __restrict__ ys,
                            const float* __restrict__ zs, int ds, const uint32_t* __restrict__ offsets,
                            uint32_t* __restrict__ total, long capacity, uint32_t* __restrict__ ekeys,
                            uint32_t* __restrict__ evals, DevStatus* status) {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    const FrameParams f = *fpp;
-    const int n = f.n_points;
-    place_sensor(g, p, f);
     const bool over = (long)total[0] > capacity;
-    if (i == 0) {
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
         total[2] = over ? 0u : total[0];  // live entry count for the sort
         if (over) atomicOr(&status->overflow, 1u);
     }
-    if (i >= n || over) return;
-    const float mx = xs[i], my = ys[i], mz = zs[i];
-    float4 a, b;
-    double4 c;
-    const RayPrep r = prep_ray(p, g, mx, my, mz, ds != 0, &a, &b, &c);
-    if (!r.ok) return;
-    // never write more entries than were counted: the count pass sized this ray's range
-    const uint32_t o0 = offsets[i];
-    const uint32_t cnt = (i + 1 < n) ? offsets[i + 1] - o0 : total[0] - o0;
-    uint32_t o = o0;
-    for_each_tile(g, r.bx, r.by, r.bz, [&](int t) {
-        if (o - o0 < cnt) {
-            ekeys[o] = (uint32_t)t;
+    if (over) return;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < bt.N; i += gridDim.x * blockDim.x) {
+        const int sc = scene_of(bt.off->point, bt.S, i);
+        const FrameParams f = bt.fp[sc];
+        if (i - bt.off->point[sc] >= f.n_points) continue;
+        const SceneDev& sd = bt.sc[sc];
+        const BinGeom g = scene_geom(sd, f);
+        const float mx = xs[i], my = ys[i], mz = zs[i];
+        float4 a;
+        double4 c;
+        const RayPrep r = prep_ray(sd.p, g, mx, my, mz, ds != 0, &a, &c);
+        if (!r.ok) continue;
+        // never write more entries than were counted: the count pass sized this ray's range
+        const uint32_t o0 = offsets[i];
+        const uint32_t cnt = (i + 1 < bt.N) ? offsets[i + 1] - o0 : total[0] - o0;
+        const uint32_t toff = (uint32_t)bt.off->tile[sc];
+        uint32_t o = o0;
+        for_each_tile(g, r.bx, r.by, r.bz, [&](int t) {
+            if (o - o0 < cnt) {
+                ekeys[o] = toff + (uint32_t)t;
+                evals[o] = (uint32_t)i;
+                ++o;
+            }
+        });
+        for (; o - o0 < cnt; ++o) {  // pad with a key past the last tile (sorted last, ignored)
+            ekeys[o] = (uint32_t)bt.T;
             evals[o] = (uint32_t)i;
-            ++o;
         }
-    });
-    for (; o - o0 < cnt; ++o) {  // pad with a key past the last tile (sorted last, ignored)
-        ekeys[o] = (uint32_t)g.ntx * g.nty * g.ntz;
-        evals[o] = (uint32_t)i;
     }
 }
 
@@ -260,11 +284,11 @@ __global__ void k_tile_start(const uint32_t* __restrict__ skeys, const uint32_t*
     tile_start[t] = (uint32_t)lo;
 }
 
-__global__ void k_tile_items(const uint32_t* __restrict__ tile_start, int T, uint32_t* __restrict__ items) {
+__global__ void k_tile_items(const uint32_t* __restrict__ tile_start, int T, int chunk, uint32_t* __restrict__ items) {
     const int t = blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= T) return;
     const uint32_t len = tile_start[t + 1] - tile_start[t];
-    items[t] = len == 0 ? 1u : (len + kChunk - 1) / kChunk;
+    items[t] = len == 0 ? 1u : (len + chunk - 1) / chunk;
 }
 
 __global__ void k_finish_lists(const uint32_t* __restrict__ item_off, int T, DevStatus* status,
@@ -279,58 +303,64 @@ __global__ void k_finish_lists(const uint32_t* __restrict__ item_off, int T, Dev
 // Largest |c| of a cell centre seen from a sensor inside or near the grid [m].
 static float max_extent(const DevParams& p) { return 2.0f * ((float)p.G * p.res * 1.7320508f + p.size_z); }
 
-static BinGeom make_bingeom(const DevParams& p, const RayBuffers& rb, bool ds) {
-    BinGeom g;
-    g.ax = g.ay = g.az = 0.0f;  // placed on the device from the frame scalars
+void fill_scene_evidence(SceneDev& sd, bool ds, float4* ktab) {
+    const DevParams& p = sd.p;
     if (!ds) {
-        g.R = p.ls / p.res * (1.0f + 1e-4f) + 1e-3f;
+        sd.bin_R = p.ls / p.res * (1.0f + 1e-4f) + 1e-3f;
     } else {
         // window radius plus the FP32 rounding slack of |c|^2 - (c.m)^2/|m|^2
         const float ext = max_extent(p);
         const float slack = 64.0f * 5.96e-8f * ext * ext;
-        g.R = sqrtf(p.window_radius * p.window_radius + slack) / p.res + 1e-3f;
+        sd.bin_R = sqrtf(p.window_radius * p.window_radius + slack) / p.res + 1e-3f;
     }
-    g.G = p.G;
-    g.Gz = p.Gz;
-    g.tx = rb.tx; g.ty = rb.ty; g.tz = rb.tz;
-    g.ntx = rb.ntx; g.nty = rb.nty; g.ntz = rb.ntz;
-    return g;
+    sd.wr2 = p.window_radius * p.window_radius;
+    // cull around the sub-block centroid: half diagonal sqrt(1.5^2+1.5^2+0.5^2) res
+    const float rsb = 2.1794495f * p.res;
+    float rsup;
+    if (!ds) {
+        rsup = p.ls * (1.0f + 1e-4f) + rsb + 1e-3f * p.res;
+    } else {
+        const float ext = max_extent(p);
+        const float slack = 64.0f * 5.96e-8f * ext * ext;
+        rsup = sqrtf(p.window_radius * p.window_radius + slack) + rsb + 1e-3f * p.res;
+    }
+    sd.cull_r2 = rsup * rsup;
+    // fixed point: one kernel value is at most sigma -> at most 2^40 units, leaving 2^23 terms
+    // of headroom in a signed 64-bit sum
+    const double sig = std::max((double)p.sigma, 1e-30);
+    const int sh = 40 - (int)std::ceil(std::log2(sig));
+    sd.fx_inv = std::ldexp(1.0, -sh);
+    if (ktab) build_kernel_table(p.sigma, std::ldexp(1.0, sh), ktab);
 }
 
-long ray_entries_bound(const DevParams& p, const EvidenceConfig& ec, int max_points) {
-    const int ntx = (p.G + ec.tile_x - 1) / ec.tile_x, nty = (p.G + ec.tile_y - 1) / ec.tile_y,
-              ntz = (p.Gz + ec.tile_z - 1) / ec.tile_z;
+long ray_entries_bound(const DevParams& p, const TileShape& ts, int max_points) {
     const double R = std::max((double)p.ls, (double)p.window_radius * 1.5 + 0.05) / p.res + 2.0;
-    const int ts[3] = {ec.tile_x, ec.tile_y, ec.tile_z}, nt[3] = {ntx, nty, ntz};
+    const int tsz[3] = {ts.tx, ts.ty, ts.tz}, nt[3] = {ts.ntx, ts.nty, ts.ntz};
     long worst = 0;
     for (int A = 0; A < 3; ++A) {
         long per_slab = 1;
         for (int k = 1; k <= 2; ++k) {
             const int o = (A + k) % 3;
-            const long n = (long)std::ceil((ts[A] + 4.0 * R + 2.0) / ts[o]) + 2;
+            const long n = (long)std::ceil((tsz[A] + 4.0 * R + 2.0) / tsz[o]) + 2;
             per_slab *= std::min<long>(n, nt[o]);
         }
         worst = std::max(worst, per_slab * nt[A]);
     }
-    worst = std::min<long>(worst, (long)ntx * nty * ntz);
+    worst = std::min<long>(worst, (long)ts.ntx * ts.nty * ts.ntz);
     return worst * (long)max_points;
 }
 
-cudaError_t build_ray_lists(const DevParams& p, const FrameParams* fp, const float* xs, const float* ys,
-                            const float* zs, RayBuffers& rb, bool ds, DevStatus* status, cudaStream_t st) {
-    const BinGeom g = make_bingeom(p, rb, ds);
-    const int nmax = rb.max_points;
-    const int T = rb.tiles;
-    const uint32_t* dn_points =
-        reinterpret_cast<const uint32_t*>(reinterpret_cast<const char*>(fp) + offsetof(FrameParams, n_points));
+cudaError_t build_ray_lists(const Batch& bt, const float* xs, const float* ys, const float* zs, RayBuffers& rb,
+                            bool ds, DevStatus* status, cudaStream_t st) {
+    const int N = bt.N;
+    const int T = bt.T;
     ++g_launches;
-    k_ray_count<<<div_up(nmax, kBlock), kBlock, 0, st>>>(p, fp, g, xs, ys, zs, ds ? 1 : 0, rb.ray_a, rb.ray_b,
-                                                         rb.ray_c, rb.counts, status);
-    cudaError_t e = scan_u32_exclusive_dn(rb.counts, rb.offsets, nmax, dn_points, rb.scan_tmp, rb.total, st);
+    k_ray_count<<<grid_for(N), kBlock, 0, st>>>(bt, xs, ys, zs, ds ? 1 : 0, rb.ray_a, rb.ray_c, rb.counts, status);
+    cudaError_t e = scan_u32_exclusive(rb.counts, rb.offsets, N, rb.scan_tmp, rb.total, st);
     if (e != cudaSuccess) return e;
     ++g_launches;
-    k_ray_emit<<<div_up(nmax, kBlock), kBlock, 0, st>>>(p, fp, g, xs, ys, zs, ds ? 1 : 0, rb.offsets, rb.total,
-                                                        rb.capacity, rb.ekeys, rb.evals, status);
+    k_ray_emit<<<grid_for(N), kBlock, 0, st>>>(bt, xs, ys, zs, ds ? 1 : 0, rb.offsets, rb.total, rb.capacity,
+                                               rb.ekeys, rb.evals, status);
     int bits = 1;
     while ((1 << bits) < T + 1) ++bits;
     e = radix_sort_pairs_dn(rb.ekeys, rb.evals, rb.ekeys2, rb.evals2, rb.ekeys_alt, rb.evals_alt, rb.capacity,
@@ -339,7 +369,7 @@ cudaError_t build_ray_lists(const DevParams& p, const FrameParams* fp, const flo
     ++g_launches;
     k_tile_start<<<div_up(T + 1, kBlock), kBlock, 0, st>>>(rb.ekeys2, rb.total, T, rb.tile_start);
     ++g_launches;
-    k_tile_items<<<div_up(T, kBlock), kBlock, 0, st>>>(rb.tile_start, T, rb.tile_items);
+    k_tile_items<<<div_up(T, kBlock), kBlock, 0, st>>>(rb.tile_start, T, rb.chunk, rb.tile_items);
     e = scan_u32_exclusive(rb.tile_items, rb.item_off, T, rb.scan_tmp, rb.item_off + T, st);
     if (e != cudaSuccess) return e;
     ++g_launches;
@@ -348,10 +378,6 @@ cudaError_t build_ray_lists(const DevParams& p, const FrameParams* fp, const flo
 }
 
 // ================================================================ shared kernel machinery
-struct TileShape {
-    int tx, ty, tz, ntx, nty, nsbx, nsby;
-};
-
 __device__ __forceinline__ int find_tile(const uint32_t* __restrict__ item_off, int T, uint32_t item) {
     // last t with item_off[t] <= item
     int lo = 0, hi = T;  // answer in [0, T)
@@ -363,7 +389,7 @@ __device__ __forceinline__ int find_tile(const uint32_t* __restrict__ item_off, 
 }
 
 struct CellLoc {
-    int c;          // cell index, -1 when outside the grid
+    int c;          // cell index within the scene, -1 when outside the grid
     int local;      // cell index within the tile
     float x, y, z;  // cell centre relative to the sensor [m], reference FP32 operation order
     float ox, oy, oz;  // anchor: centre of the sub-block's cell (2, 2, 1), same formula
@@ -395,6 +421,46 @@ __device__ __forceinline__ CellLoc locate(const DevParams& p, const TileShape& t
     return L;
 }
 
+// The work item a CTA holds: its tile (global and scene-local), scene and ray range.
+struct Item {
+    int t, lt, sc;
+    uint32_t k, n_items, e0;
+    int nr;
+};
+
+__device__ __forceinline__ Item item_of(const Batch& bt, const uint32_t* item_off, const uint32_t* tile_start,
+                                        uint32_t item, int chunk) {
+    Item it;
+    it.t = find_tile(item_off, bt.T, item);
+    it.sc = scene_of(bt.off->tile, bt.S, it.t);
+    it.lt = it.t - bt.off->tile[it.sc];
+    it.k = item - item_off[it.t];
+    it.n_items = item_off[it.t + 1] - item_off[it.t];
+    it.e0 = tile_start[it.t] + it.k * (uint32_t)chunk;
+    const uint32_t e1 = min(tile_start[it.t + 1], it.e0 + (uint32_t)chunk);
+    it.nr = (int)(e1 > it.e0 ? e1 - it.e0 : 0);
+    return it;
+}
+
+struct EvArgs {
+    Batch bt;
+    const uint32_t* item_off;
+    const uint32_t* tile_start;
+    const uint32_t* evals;
+    const float4* ray_a;
+    const double4* ray_c;
+    const float4* ktab;  // S tables of kKernelTab entries, fixed-point scale folded in
+    uint32_t* tile_done;
+    unsigned long long* acc;
+    uint8_t* ds_counts;
+    long ds_count_capacity;
+    CellState cs;
+    CellWork cw;
+    DevStatus* status;
+    int first_frame;
+    int chunk;  // rays per work item (<= kChunk)
+};
+
 // ================================================================ K3DOM
 // The sparse kernel of mass_update.cu:24-26,
 //   k(d) = max(0, sigma ((2 + cos(2 pi x)) (1 - x) / 3 + sin(2 pi x) / (2 * 3.141592))),  x = d / ls,
@@ -411,10 +477,10 @@ static double kernel_ref(double u, double sigma) {
     return v > 0.0 ? v : 0.0;
 }
 
-void build_kernel_table(float sigma, float4* out) {
+void build_kernel_table(float sigma, double scale, float4* out) {
     for (int i = 0; i < kKernelTab; ++i) {
         double y[4];
-        for (int j = 0; j < 4; ++j) y[j] = kernel_ref(std::min(1.0, (i + j / 3.0) / kKernelTab), sigma);
+        for (int j = 0; j < 4; ++j) y[j] = scale * kernel_ref(std::min(1.0, (i + j / 3.0) / kKernelTab), sigma);
         // inverse Vandermonde of the nodes 0, 1/3, 2/3, 1
         const double c0 = y[0];
         const double c1 = -5.5 * y[0] + 9.0 * y[1] - 4.5 * y[2] + y[3];
@@ -430,6 +496,18 @@ __device__ __forceinline__ float kernel_tab(const float4* __restrict__ tab, floa
     const float f = t - (float)i;
     const float4 c = tab[i];
     return fmaf(f, fmaf(f, fmaf(f, c.w, c.z), c.y), c.x);
+}
+
+// Kernel value rounded to an integer number of fixed-point units (the table is pre-scaled, so
+// one unit is 2^-k sigma), clamped at 0 as k(d) = max(0, ...) is. For 0 <= v < 2^23 adding 2^23
+// lands in [2^23, 2^24), where the float spacing is 1, so the add rounds v to the nearest
+// integer and the subtraction is exact; larger floats are integers already. Sums of such
+// integers below 2^53 are exact in FP64, so the FP64 accumulation is exact and its result does
+// not depend on the order of the terms.
+__device__ __forceinline__ double kernel_units(float v) {
+    v = fmaxf(v, 0.0f);
+    const float r = __fsub_rn(__fadd_rn(v, 8388608.0f), 8388608.0f);
+    return (double)(v < 8388608.0f ? r : v);
 }
 
 __device__ __forceinline__ double calc_credit(double mass, double mass_scale) {
@@ -514,35 +592,10 @@ __device__ void k3dom_cell_update(const DevParams& p, float dt, int c, double de
     cs.mvz[c] = (float)vz;
 }
 
-struct EvArgs {
-    DevParams p;
-    const FrameParams* fp;
-    TileShape ts;
-    int T;
-    const uint32_t* item_off;
-    const uint32_t* tile_start;
-    const uint32_t* evals;
-    const float4* ray_a;
-    const float4* ray_b;
-    const double4* ray_c;
-    const float4* ktab;
-    uint32_t* tile_done;
-    unsigned long long* acc;
-    uint8_t* ds_counts;
-    long ds_count_capacity;
-    CellState cs;
-    CellWork cw;
-    DevStatus* status;
-    int first_frame;
-    double fx_scale, fx_inv;  // fixed-point scale of the K3DOM evidence
-    float wr2;                // DS window radius squared
-    float cull_r2;            // squared cull radius around a sub-block anchor [m^2]
-};
-
 // Shared memory of k_bgki: the kernel table, one chunk of rays, and a per-warp staging area for
 // the FP64 (sub-block, ray) constants of the rays that pass the cull.
 struct BgkiSmem {
-    float4 ktab[kKernelTab];      // sparse-kernel table (sigma folded in)
+    float4 ktab[kKernelTab];      // sparse-kernel table of the current scene
     float4 a[kChunk];             // m.x, m.y, m.z, d_m
     double4 c[kChunk];            // d_m, margin, 1/d_m
     float4 stage[kEvWarps][32][3];
@@ -557,32 +610,16 @@ struct BgkiSmem {
 //   distance to the point = |occ0 + delta|.
 // Every FP32 quantity is O(ls), so the FP32 evaluation keeps ~1e-7 relative accuracy at any
 // distance from the sensor (the direct |c|^2 - d_proj^2 form of :60 loses ~1e-5 at 20 m).
-//
-// Work: a CTA takes one (tile, chunk) item and stages its rays; its warps then pull the tile's
-// 4x4x2 sub-blocks from a block-local counter (so a warp that meets few rays takes more
-// sub-blocks), test 32 rays per ballot against the sub-block's bounding sphere, and evaluate
-// the surviving rays for their own cells. Each warp adds its sub-block's evidence to per-cell
-// 64-bit fixed-point accumulators in global memory (integer addition: the total does not depend
-// on the order of chunks or warps); the last CTA to finish a tile's chunks runs the cell update
-// for the whole tile and clears the accumulators.
-template <int UNUSED>
-__global__ void __launch_bounds__(kEvThreads) k_bgki(EvArgs A) {
+__global__ void __launch_bounds__(kEvThreads, 3) k_bgki(EvArgs A) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     BgkiSmem& S = *reinterpret_cast<BgkiSmem*>(smem_raw);
     __shared__ uint32_t s_item;
     __shared__ int s_next_sb, s_last;
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-    const DevParams& p = A.p;
-    const FrameParams fp = *A.fp;
-    const uint32_t total_items = A.item_off[A.T];
-    const float ls2 = p.ls * p.ls;
-    const float inv_ls2 = 1.0f / ls2;
-    const int n_points = fp.n_points;
-    const int nsb = A.ts.nsbx * A.ts.nsby * (A.ts.tz / 2);
-    const int tile_cells = A.ts.tx * A.ts.ty * A.ts.tz;
-    const float hres = 0.5f * p.res;
-    for (int i = threadIdx.x; i < kKernelTab; i += kEvThreads) S.ktab[i] = A.ktab[i];
-    unsigned nev = 0;  // in-support evaluations of this lane (the roofline's work count)
+    const Batch& bt = A.bt;
+    const uint32_t total_items = A.item_off[bt.T];
+    int table_scene = -1;  // scene whose kernel table is in shared memory
+    unsigned nev = 0;      // in-support evaluations of this lane (the roofline's work count)
 
     for (;;) {
         if (threadIdx.x == 0) {
@@ -592,28 +629,38 @@ __global__ void __launch_bounds__(kEvThreads) k_bgki(EvArgs A) {
         __syncthreads();
         const uint32_t item = s_item;
         if (item >= total_items) break;
-        const int t = find_tile(A.item_off, A.T, item);
-        const uint32_t k = item - A.item_off[t];
-        const uint32_t n_items = A.item_off[t + 1] - A.item_off[t];
-        const uint32_t e0 = A.tile_start[t] + k * kChunk;
-        const uint32_t e1 = min(A.tile_start[t + 1], e0 + (uint32_t)kChunk);
-        const int nr = (int)(e1 > e0 ? e1 - e0 : 0);
-        for (int r = threadIdx.x; r < nr; r += kEvThreads) {
-            uint32_t rid = A.evals[e0 + r];
-            if (rid >= (uint32_t)n_points) rid = 0;  // defensive: never read past the ray arrays
+        const Item it = item_of(bt, A.item_off, A.tile_start, item, A.chunk);
+        const SceneDev& sd = bt.sc[it.sc];
+        const DevParams& p = sd.p;
+        const TileShape ts = sd.ts;
+        const FrameParams fp = bt.fp[it.sc];
+        const int coff = bt.off->cell[it.sc];
+        const float ls2 = p.ls * p.ls;
+        const float inv_ls2 = 1.0f / ls2;
+        const float hres = 0.5f * p.res;
+        const float cull_r2 = sd.cull_r2;
+        const int nsb = ts.nsbx * ts.nsby * (ts.tz / 2);
+        if (it.sc != table_scene) {
+            for (int i = threadIdx.x; i < kKernelTab; i += kEvThreads) S.ktab[i] = A.ktab[it.sc * kKernelTab + i];
+            table_scene = it.sc;
+        }
+        for (int r = threadIdx.x; r < it.nr; r += kEvThreads) {
+            uint32_t rid = A.evals[it.e0 + r];
+            if (rid >= (uint32_t)bt.N) rid = 0;  // defensive: never read past the ray arrays
             S.a[r] = A.ray_a[rid];
             S.c[r] = A.ray_c[rid];
         }
         __syncthreads();
+        const int nr = it.nr;
         for (;;) {
             int sb = 0;
             if (lane == 0) sb = atomicAdd(&s_next_sb, 1);
             sb = __shfl_sync(0xffffffffu, sb, 0);
             if (sb >= nsb) break;
-            const CellLoc L = locate(p, A.ts, t, sb, lane, fp.sensor_x, fp.sensor_y, fp.sensor_z);
+            const CellLoc L = locate(p, ts, it.lt, sb, lane, fp.sensor_x, fp.sensor_y, fp.sensor_z);
             const float dx = L.x - L.ox, dy = L.y - L.oy, dz = L.z - L.oz;  // exact (nearby floats)
             const double ox = L.ox, oy = L.oy, oz = L.oz;
-            double ao = 0.0, af = 0.0;
+            double ao = 0.0, af = 0.0;  // exact sums of integer units (< 2^52 per chunk)
             for (int g0 = 0; g0 < nr; g0 += 32) {
                 const int r = g0 + lane;
                 bool hit = false;
@@ -630,7 +677,7 @@ __global__ void __launch_bounds__(kEvThreads) k_bgki(EvArgs A) {
                     const float qx = (float)px - hres - qd * ux, qy = (float)py - hres - qd * uy,
                                 qz = (float)pz - hres - qd * uz;
                     const float qal = fminf(qpar, 0.0f) + fmaxf(qpar - a.w, 0.0f);
-                    hit = qx * qx + qy * qy + qz * qz + qal * qal < A.cull_r2;
+                    hit = qx * qx + qy * qy + qz * qz + qal * qal < cull_r2;
                     if (hit) {
                         S.stage[wid][lane][0] = make_float4((float)par0, (float)(par0 - cd.y), (float)(par0 - cd.x), ux);
                         S.stage[wid][lane][1] = make_float4((float)px, (float)py, (float)pz, uy);
@@ -648,7 +695,7 @@ __global__ void __launch_bounds__(kEvThreads) k_bgki(EvArgs A) {
                     const float vx = s2.x + dx, vy = s2.y + dy, vz = s2.z + dz;
                     const float d2o = vx * vx + vy * vy + vz * vz;
                     if (d2o < ls2 && L.c >= 0) {
-                        ao += (double)kernel_tab(S.ktab, d2o * inv_ls2);
+                        ao += kernel_units(kernel_tab(S.ktab, d2o * inv_ls2));
                         ++nev;
                     }
                     // free evidence (:54-71)
@@ -659,33 +706,33 @@ __global__ void __launch_bounds__(kEvThreads) k_bgki(EvArgs A) {
                         const float al = fminf(s0.x + dpar, 0.0f) + fmaxf(s0.y + dpar, 0.0f);
                         const float d2f = qx * qx + qy * qy + qz * qz + al * al;
                         if (d2f < ls2 && L.c >= 0) {
-                            af += (double)kernel_tab(S.ktab, d2f * inv_ls2);
+                            af += kernel_units(kernel_tab(S.ktab, d2f * inv_ls2));
                             ++nev;
                         }
                     }
                 }
                 __syncwarp();
             }
-            // fixed-point quantisation and accumulation (associative)
             if (L.c >= 0) {
-                const long long fo = __double2ll_rn(ao * A.fx_scale);
-                const long long ff = __double2ll_rn(af * A.fx_scale);
-                if (fo) atomicAdd(&A.acc[2 * (long)L.c], (unsigned long long)fo);
-                if (ff) atomicAdd(&A.acc[2 * (long)L.c + 1], (unsigned long long)ff);
+                unsigned long long* ac = A.acc + 2 * (long)(coff + L.c);
+                const long long io = __double2ll_rn(ao), jf = __double2ll_rn(af);  // exact
+                if (io) atomicAdd(ac, (unsigned long long)io);
+                if (jf) atomicAdd(ac + 1, (unsigned long long)jf);
             }
         }
         __threadfence();
         __syncthreads();
-        if (threadIdx.x == 0) s_last = (atomicAdd(&A.tile_done[t], 1u) == n_items - 1) ? 1 : 0;
+        if (threadIdx.x == 0) s_last = (atomicAdd(&A.tile_done[it.t], 1u) == it.n_items - 1) ? 1 : 0;
         __syncthreads();
         if (s_last) {
             __threadfence();
-            const int tx = t % A.ts.ntx, ty = (t / A.ts.ntx) % A.ts.nty, tz = t / (A.ts.ntx * A.ts.nty);
+            const int tx = it.lt % ts.ntx, ty = (it.lt / ts.ntx) % ts.nty, tz = it.lt / (ts.ntx * ts.nty);
+            const int tile_cells = ts.tx * ts.ty * ts.tz;
             for (int li = threadIdx.x; li < tile_cells; li += kEvThreads) {
-                const int lx = li % A.ts.tx, ly = (li / A.ts.tx) % A.ts.ty, lz = li / (A.ts.tx * A.ts.ty);
-                const int ix = tx * A.ts.tx + lx, iy = ty * A.ts.ty + ly, iz = tz * A.ts.tz + lz;
+                const int lx = li % ts.tx, ly = (li / ts.tx) % ts.ty, lz = li / (ts.tx * ts.ty);
+                const int ix = tx * ts.tx + lx, iy = ty * ts.ty + ly, iz = tz * ts.tz + lz;
                 if (ix >= p.G || iy >= p.G || iz >= p.Gz) continue;
-                const int c = ix + p.G * iy + p.G * p.G * iz;
+                const int c = coff + ix + p.G * iy + p.G * p.G * iz;
                 // every chunk of the tile has added its share (fence + tile counter above); read
                 // the totals from L2 and clear only what was written
                 unsigned long long* ac = A.acc + 2 * (long)c;
@@ -693,10 +740,10 @@ __global__ void __launch_bounds__(kEvThreads) k_bgki(EvArgs A) {
                 const long long ff = (long long)__ldcg(ac + 1);
                 if (fo) __stcg(ac, 0ull);
                 if (ff) __stcg(ac + 1, 0ull);
-                k3dom_cell_update(p, fp.dt, c, (double)fo * A.fx_inv, (double)ff * A.fx_inv, A.cs, A.cw,
+                k3dom_cell_update(p, fp.dt, c, (double)fo * sd.fx_inv, (double)ff * sd.fx_inv, A.cs, A.cw,
                                   A.first_frame != 0);
             }
-            if (threadIdx.x == 0) A.tile_done[t] = 0;
+            if (threadIdx.x == 0) A.tile_done[it.t] = 0;
         }
         __syncthreads();
     }
@@ -822,58 +869,66 @@ __device__ __forceinline__ float ds_pocc(float x, float y, float z, float4 m, fl
     return __fmul_rn(0.95f, expf(__fdiv_rn(__fmul_rn(-0.5f, r_sqr), delta_sqr)));
 }
 
-// COUNT: pass 1, count neighbours per cell in chunks 0..n-2 of multi-chunk tiles.
-// !COUNT: pass 2, take each cell's first (100 - earlier count) neighbours of the chunk.
-template <int NSBW, bool COUNT>
+// Pass COUNT (multi-chunk tiles, every chunk but the last): per (item, cell) number of
+// neighbours. Pass !COUNT: each cell takes its first (100 - neighbours in earlier chunks)
+// neighbours of the chunk, in list order, so the kept set is the reference's first 100 rays in
+// input order (measurement_grid.cu:86-97). Per-chunk summaries (any neighbour, all farther,
+// largest pOcc) are combined per cell with integer atomics; the last CTA of a tile runs the
+// measurement-to-mass step for the whole tile.
+constexpr int kMaxTileCells = 16 * 16 * 8;
+
+template <bool COUNT>
 __global__ void __launch_bounds__(kEvThreads) k_dsgrid(EvArgs A) {
     __shared__ float4 sa[kChunk];
     __shared__ uint32_t s_item;
-    __shared__ int s_last;
-    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-    const DevParams& p = A.p;
-    const FrameParams fp = *A.fp;
-    const uint32_t total_items = A.item_off[A.T];
-    const int n_points = fp.n_points;
-    const int tile_cells = A.ts.tx * A.ts.ty * A.ts.tz;
+    __shared__ int s_next_sb, s_last;
+    const int lane = threadIdx.x & 31;
+    const Batch& bt = A.bt;
+    const uint32_t total_items = A.item_off[bt.T];
     unsigned int* counter = COUNT ? &A.status->work_counter2 : &A.status->work_counter;
     uint32_t* part_max = reinterpret_cast<uint32_t*>(A.acc);
-    uint32_t* part_flags = part_max + p.C;
+    uint32_t* part_flags = part_max + bt.C;
 
     for (;;) {
-        if (threadIdx.x == 0) s_item = atomicAdd(counter, 1u);
+        if (threadIdx.x == 0) {
+            s_item = atomicAdd(counter, 1u);
+            s_next_sb = 0;
+        }
         __syncthreads();
         const uint32_t item = s_item;
-        __syncthreads();
         if (item >= total_items) break;
-        const int t = find_tile(A.item_off, A.T, item);
-        const uint32_t k = item - A.item_off[t];
-        const uint32_t n_items = A.item_off[t + 1] - A.item_off[t];
-        if (COUNT && (n_items == 1 || k == n_items - 1)) continue;  // uniform across the block
-        const uint32_t e0 = A.tile_start[t] + k * kChunk;
-        const uint32_t e1 = min(A.tile_start[t + 1], e0 + (uint32_t)kChunk);
-        const int nr = (int)(e1 > e0 ? e1 - e0 : 0);
-        for (int r = threadIdx.x; r < nr; r += kEvThreads) {
-            uint32_t rid = A.evals[e0 + r];
-            if (rid >= (uint32_t)n_points) rid = 0;
+        const Item it = item_of(bt, A.item_off, A.tile_start, item, A.chunk);
+        if (COUNT && (it.n_items == 1 || it.k == it.n_items - 1)) {  // uniform across the block
+            __syncthreads();
+            continue;
+        }
+        const SceneDev& sd = bt.sc[it.sc];
+        const DevParams& p = sd.p;
+        const TileShape ts = sd.ts;
+        const FrameParams fp = bt.fp[it.sc];
+        const int coff = bt.off->cell[it.sc];
+        const int nsb = ts.nsbx * ts.nsby * (ts.tz / 2);
+        const float hres = 0.5f * p.res;
+        for (int r = threadIdx.x; r < it.nr; r += kEvThreads) {
+            uint32_t rid = A.evals[it.e0 + r];
+            if (rid >= (uint32_t)bt.N) rid = 0;
             sa[r] = A.ray_a[rid];
         }
         __syncthreads();
-        int cell[NSBW], nbq[NSBW];
-        bool farq[NSBW];
-        float maxq[NSBW], acsq[NSBW];
-#pragma unroll
-        for (int q = 0; q < NSBW; ++q) {
-            const int sbi = wid + q * kEvWarps;
-            const CellLoc L = locate(p, A.ts, t, sbi, lane, fp.sensor_x, fp.sensor_y, fp.sensor_z);
-            cell[q] = L.c;
+        const int nr = it.nr;
+        for (;;) {
+            int sb = 0;
+            if (lane == 0) sb = atomicAdd(&s_next_sb, 1);
+            sb = __shfl_sync(0xffffffffu, sb, 0);
+            if (sb >= nsb) break;
+            const CellLoc L = locate(p, ts, it.lt, sb, lane, fp.sensor_x, fp.sensor_y, fp.sensor_z);
             const float acs = __fadd_rn(__fadd_rn(__fmul_rn(L.x, L.x), __fmul_rn(L.y, L.y)), __fmul_rn(L.z, L.z));
-            acsq[q] = acs;
             int quota = kDsMaxNeighbors;
-            if (!COUNT && n_items > 1) {
+            if (!COUNT && it.n_items > 1) {
                 int pre = 0;
-                const long base = (long)A.item_off[t] * tile_cells;
-                for (uint32_t kk = 0; kk < k; ++kk) {
-                    const long idx = base + (long)kk * tile_cells + L.local;
+                const long base = (long)A.item_off[it.t] * kMaxTileCells;
+                for (uint32_t kk = 0; kk < it.k; ++kk) {
+                    const long idx = base + (long)kk * kMaxTileCells + L.local;
                     pre += (idx < A.ds_count_capacity) ? (int)A.ds_counts[idx] : 0;
                 }
                 quota = max(0, kDsMaxNeighbors - pre);
@@ -890,18 +945,18 @@ __global__ void __launch_bounds__(kEvThreads) k_dsgrid(EvArgs A) {
                         const float4 a = sa[r];
                         // distance of the sub-block centre to the half-line through m
                         const float len = sqrtf(a.w);
-                        const float qx = L.ox - 0.5f * p.res, qy = L.oy - 0.5f * p.res, qz = L.oz - 0.5f * p.res;
+                        const float qx = L.ox - hres, qy = L.oy - hres, qz = L.oz - hres;
                         const float tproj = fmaxf((qx * a.x + qy * a.y + qz * a.z) / len, 0.0f);
                         const float ex = qx - tproj * a.x / len, ey = qy - tproj * a.y / len,
                                     ez = qz - tproj * a.z / len;
-                        hit = ex * ex + ey * ey + ez * ez < A.cull_r2;
+                        hit = ex * ex + ey * ey + ez * ez < sd.cull_r2;
                     }
                     unsigned mask = __ballot_sync(0xffffffffu, hit);
                     while (mask) {
                         const int j = __ffs(mask) - 1;
                         mask &= mask - 1;
                         const float4 a = sa[g0 + j];
-                        if (nb < quota && ds_is_neighbor(L.x, L.y, L.z, acs, a, A.wr2)) {
+                        if (nb < quota && ds_is_neighbor(L.x, L.y, L.z, acs, a, sd.wr2)) {
                             ++nb;
                             if (!COUNT) {
                                 if (acs > a.w) all_far = false;
@@ -913,75 +968,59 @@ __global__ void __launch_bounds__(kEvThreads) k_dsgrid(EvArgs A) {
                     if (!__any_sync(0xffffffffu, nb < quota)) break;
                 }
             }
-            nbq[q] = nb;
-            farq[q] = all_far;
-            maxq[q] = mx;
-            if (COUNT && L.c >= 0) {
-                const long idx = (long)item * tile_cells + L.local;
-                if (idx < A.ds_count_capacity) A.ds_counts[idx] = (uint8_t)nb;
+            if (COUNT) {
+                if (L.c >= 0) {
+                    const long idx = (long)item * kMaxTileCells + L.local;
+                    if (idx < A.ds_count_capacity) A.ds_counts[idx] = (uint8_t)nb;
+                }
+            } else if (L.c >= 0 && nb > 0) {
+                const int c = coff + L.c;
+                atomicMax(&part_max[c], __float_as_uint(mx));
+                atomicOr(&part_flags[c], 1u | (all_far ? 0u : 2u));
             }
         }
         if (COUNT) {
             __syncthreads();
             continue;
         }
-        bool run_update = true;
-        if (n_items > 1) {
-#pragma unroll
-            for (int q = 0; q < NSBW; ++q) {
-                if (cell[q] >= 0 && nbq[q] > 0) {
-                    atomicMax(&part_max[cell[q]], __float_as_uint(maxq[q]));
-                    atomicOr(&part_flags[cell[q]], 1u | (farq[q] ? 0u : 2u));
-                }
-            }
+        __threadfence();
+        __syncthreads();
+        if (threadIdx.x == 0) s_last = (atomicAdd(&A.tile_done[it.t], 1u) == it.n_items - 1) ? 1 : 0;
+        __syncthreads();
+        if (s_last) {
             __threadfence();
-            __syncthreads();
-            if (threadIdx.x == 0) s_last = (atomicAdd(&A.tile_done[t], 1u) == n_items - 1) ? 1 : 0;
-            __syncthreads();
-            run_update = s_last != 0;
-            if (run_update) {
-                __threadfence();
-#pragma unroll
-                for (int q = 0; q < NSBW; ++q) {
-                    if (cell[q] >= 0) {
-                        const uint32_t m = atomicExch(&part_max[cell[q]], 0u);
-                        const uint32_t f = atomicExch(&part_flags[cell[q]], 0u);
-                        nbq[q] = (f & 1u) ? 1 : 0;
-                        farq[q] = (f & 2u) == 0;
-                        maxq[q] = __uint_as_float(m);
-                    }
-                }
-                if (threadIdx.x == 0) A.tile_done[t] = 0;
+            const int tx = it.lt % ts.ntx, ty = (it.lt / ts.ntx) % ts.nty, tz = it.lt / (ts.ntx * ts.nty);
+            const int tile_cells = ts.tx * ts.ty * ts.tz;
+            for (int li = threadIdx.x; li < tile_cells; li += kEvThreads) {
+                const int lx = li % ts.tx, ly = (li / ts.tx) % ts.ty, lz = li / (ts.tx * ts.ty);
+                const int ix = tx * ts.tx + lx, iy = ty * ts.ty + ly, iz = tz * ts.tz + lz;
+                if (ix >= p.G || iy >= p.G || iz >= p.Gz) continue;
+                const int c = coff + ix + p.G * iy + p.G * p.G * iz;
+                const uint32_t m = __ldcg(&part_max[c]);
+                const uint32_t f = __ldcg(&part_flags[c]);
+                if (m) __stcg(&part_max[c], 0u);
+                if (f) __stcg(&part_flags[c], 0u);
+                float x, y, z;
+                centre_xyz(ix, iy, iz, p, fp.sensor_x, fp.sensor_y, fp.sensor_z, &x, &y, &z);
+                const float acs = __fadd_rn(__fadd_rn(__fmul_rn(x, x), __fmul_rn(y, y)), __fmul_rn(z, z));
+                const DsMeas mc = ds_meas_from(p, acs, (f & 1u) ? 1 : 0, (f & 2u) == 0, __uint_as_float(m));
+                ds_cell_update(p, c, mc, A.cs, A.cw, A.first_frame != 0);
             }
-        }
-        if (run_update) {
-#pragma unroll
-            for (int q = 0; q < NSBW; ++q) {
-                if (cell[q] >= 0) {
-                    const DsMeas mc = ds_meas_from(p, acsq[q], nbq[q], farq[q], maxq[q]);
-                    ds_cell_update(p, cell[q], mc, A.cs, A.cw, A.first_frame != 0);
-                }
-            }
+            if (threadIdx.x == 0) A.tile_done[it.t] = 0;
         }
         __syncthreads();
     }
 }
 
 // ================================================================ launchers
-static EvArgs make_args(const DevParams& p, const FrameParams* fp, RayBuffers& rb, CellState cs, CellWork cw,
-                        bool first_frame, DevStatus* status, bool ds) {
+static EvArgs make_args(const Batch& bt, RayBuffers& rb, CellState cs, CellWork cw, bool first_frame,
+                        DevStatus* status) {
     EvArgs A;
-    A.p = p;
-    A.fp = fp;
-    A.ts.tx = rb.tx; A.ts.ty = rb.ty; A.ts.tz = rb.tz;
-    A.ts.ntx = rb.ntx; A.ts.nty = rb.nty;
-    A.ts.nsbx = rb.tx / 4; A.ts.nsby = rb.ty / 4;
-    A.T = rb.tiles;
+    A.bt = bt;
     A.item_off = rb.item_off;
     A.tile_start = rb.tile_start;
     A.evals = rb.evals2;
     A.ray_a = rb.ray_a;
-    A.ray_b = rb.ray_b;
     A.ray_c = rb.ray_c;
     A.ktab = rb.ktab;
     A.tile_done = rb.tile_done;
@@ -992,79 +1031,40 @@ static EvArgs make_args(const DevParams& p, const FrameParams* fp, RayBuffers& r
     A.cw = cw;
     A.status = status;
     A.first_frame = first_frame ? 1 : 0;
-    // fixed point: one term is at most sigma; 2^40 / sigma leaves 2^23 terms of headroom
-    const double sig = std::max((double)p.sigma, 1e-30);
-    const int sh = 40 - (int)std::ceil(std::log2(sig));
-    A.fx_scale = std::ldexp(1.0, sh);
-    A.fx_inv = std::ldexp(1.0, -sh);
-    A.wr2 = p.window_radius * p.window_radius;
-    // both variants cull around the sub-block centroid: half diagonal sqrt(1.5^2+1.5^2+0.5^2) res
-    const float rsb = 2.1794495f * p.res;
-    float rsup;
-    if (!ds) {
-        rsup = p.ls * (1.0f + 1e-4f) + rsb + 1e-3f * p.res;
-    } else {
-        const float ext = max_extent(p);
-        const float slack = 64.0f * 5.96e-8f * ext * ext;
-        rsup = sqrtf(p.window_radius * p.window_radius + slack) + rsb + 1e-3f * p.res;
-    }
-    A.cull_r2 = rsup * rsup;
+    A.chunk = rb.chunk;
     return A;
 }
 
-static int nsbw_of(const RayBuffers& rb) { return (rb.tx / 4) * (rb.ty / 4) * (rb.tz / 2) / kEvWarps; }
-
-cudaError_t launch_k3dom_evidence(const DevParams& p, const FrameParams* fp, RayBuffers& rb, CellState cs,
-                                  CellWork cw, bool first_frame, DevStatus* status, int num_sms, cudaStream_t st) {
-    EvArgs A = make_args(p, fp, rb, cs, cw, first_frame, status, false);
-    const size_t sm = sizeof(BgkiSmem);
+int bgki_blocks_per_sm() {
     int per_sm = 1;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_bgki<0>, kEvThreads, sm);
-    const int grid = num_sms * std::max(1, per_sm);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_bgki, kEvThreads, sizeof(BgkiSmem));
+    return std::max(1, per_sm);
+}
+
+cudaError_t launch_k3dom_evidence(const Batch& bt, RayBuffers& rb, CellState cs, CellWork cw, bool first_frame,
+                                  DevStatus* status, int grid, cudaStream_t st) {
+    if (rb.chunk < 32 || rb.chunk > kChunk) return cudaErrorInvalidValue;
+    EvArgs A = make_args(bt, rb, cs, cw, first_frame, status);
     ++g_launches;
-    k_bgki<0><<<grid, kEvThreads, sm, st>>>(A);
+    k_bgki<<<grid, kEvThreads, sizeof(BgkiSmem), st>>>(A);
     return cudaGetLastError();
 }
 
-cudaError_t launch_ds_evidence(const DevParams& p, const FrameParams* fp, RayBuffers& rb, CellState cs, CellWork cw,
-                               bool first_frame, DevStatus* status, int num_sms, cudaStream_t st) {
-    EvArgs A = make_args(p, fp, rb, cs, cw, first_frame, status, true);
-    const int grid = num_sms * 4;
-    switch (nsbw_of(rb)) {
-        case 1:
-            ++g_launches;
-            k_dsgrid<1, true><<<grid, kEvThreads, 0, st>>>(A);
-            ++g_launches;
-            k_dsgrid<1, false><<<grid, kEvThreads, 0, st>>>(A);
-            break;
-        case 2:
-            ++g_launches;
-            k_dsgrid<2, true><<<grid, kEvThreads, 0, st>>>(A);
-            ++g_launches;
-            k_dsgrid<2, false><<<grid, kEvThreads, 0, st>>>(A);
-            break;
-        case 4:
-            ++g_launches;
-            k_dsgrid<4, true><<<grid, kEvThreads, 0, st>>>(A);
-            ++g_launches;
-            k_dsgrid<4, false><<<grid, kEvThreads, 0, st>>>(A);
-            break;
-        case 8:
-            ++g_launches;
-            k_dsgrid<8, true><<<grid, kEvThreads, 0, st>>>(A);
-            ++g_launches;
-            k_dsgrid<8, false><<<grid, kEvThreads, 0, st>>>(A);
-            break;
-        default:
-            return cudaErrorInvalidValue;
-    }
+cudaError_t launch_ds_evidence(const Batch& bt, RayBuffers& rb, CellState cs, CellWork cw, bool first_frame,
+                               DevStatus* status, int grid, cudaStream_t st) {
+    if (rb.chunk < 32 || rb.chunk > kChunk) return cudaErrorInvalidValue;
+    EvArgs A = make_args(bt, rb, cs, cw, first_frame, status);
+    ++g_launches;
+    k_dsgrid<true><<<grid, kEvThreads, 0, st>>>(A);
+    ++g_launches;
+    k_dsgrid<false><<<grid, kEvThreads, 0, st>>>(A);
     return cudaGetLastError();
 }
+
+long ds_count_bytes(long items) { return items * (long)kMaxTileCells; }
 
 cudaError_t evidence_init() {
-    cudaError_t e;
-    const int sm = (int)sizeof(BgkiSmem);
-    return cudaFuncSetAttribute(k_bgki<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
+    return cudaFuncSetAttribute(k_bgki, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(BgkiSmem));
 }
 
 }  // namespace k3dom

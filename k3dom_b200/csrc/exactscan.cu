@@ -16,6 +16,9 @@
 #include "internal.h"
 #include "scan.cuh"
 
+#include <algorithm>
+#include <vector>
+
 namespace k3dom {
 
 constexpr int kExThreads = 256;
@@ -106,6 +109,128 @@ __global__ void exact_apply(TwoSeg in, long n, const u128* __restrict__ tile_off
         run += v[j];
         if (i < n) out[i] = from_fixed(run);
     }
+}
+
+// ---------------------------------------------------------------- segmented, table driven
+// A scan plan lists tiles of at most kExTile elements; each tile reads one contiguous input
+// range and writes one contiguous output range, and names the first tile of its segment.
+// Output = exact prefix within the segment, rounded once: the global prefix in 128-bit fixed
+// point minus the global prefix at the segment's first tile, both exact.
+constexpr int kExGroup = kExThreads * kExItems;  // tiles per group of the offset pass
+
+__global__ void exact_tab_sums(const ExactTile* __restrict__ tiles, int nt, u128* __restrict__ tsum) {
+    __shared__ u128 sm[kExThreads / 32 + 1];
+    const int b = blockIdx.x;
+    if (b >= nt) return;
+    const ExactTile t = tiles[b];
+    u128 s = 0;
+#pragma unroll
+    for (int j = 0; j < kExItems; ++j) {
+        const int i = j * kExThreads + threadIdx.x;
+        if (i < t.n) s += to_fixed(t.in[i]);
+    }
+    u128 tot;
+    block_exclusive_scan<u128, kExThreads>(s, sm, &tot);
+    if (threadIdx.x == 0) tsum[b] = tot;
+}
+
+// Within each group of kExGroup tiles: tile sums -> exclusive prefixes; group totals out.
+__global__ void exact_tab_groups(u128* __restrict__ tsum, int nt, u128* __restrict__ gsum) {
+    __shared__ u128 sm[kExThreads / 32 + 1];
+    const int base = blockIdx.x * kExGroup + threadIdx.x * kExItems;
+    u128 v[kExItems];
+    u128 s = 0;
+#pragma unroll
+    for (int j = 0; j < kExItems; ++j) {
+        v[j] = (base + j < nt) ? tsum[base + j] : (u128)0;
+        s += v[j];
+    }
+    u128 tot;
+    u128 run = block_exclusive_scan<u128, kExThreads>(s, sm, &tot);
+#pragma unroll
+    for (int j = 0; j < kExItems; ++j) {
+        if (base + j < nt) tsum[base + j] = run;
+        run += v[j];
+    }
+    if (threadIdx.x == 0) gsum[blockIdx.x] = tot;
+}
+
+__device__ __forceinline__ u128 group_prefix(const u128* __restrict__ gsum, int g) {
+    // sum of gsum[0..g): warp 0 reduces, result broadcast through shared memory
+    __shared__ u128 s_r;
+    if (threadIdx.x < 32) {
+        u128 a = 0;
+        for (int i = threadIdx.x; i < g; i += 32) a += gsum[i];
+        a = warp_inclusive_scan<u128>(a);
+        if (threadIdx.x == 31) s_r = a;
+    }
+    __syncthreads();
+    const u128 r = s_r;
+    __syncthreads();
+    return r;
+}
+
+__global__ void exact_tab_apply(const ExactTile* __restrict__ tiles, int nt, const u128* __restrict__ tsum,
+                                const u128* __restrict__ gsum) {
+    __shared__ u128 sm[kExThreads / 32 + 1];
+    const int b = blockIdx.x;
+    const ExactTile t = tiles[b];
+    const u128 pre_b = group_prefix(gsum, b / kExGroup) + tsum[b];
+    const int f = t.seg_first;
+    const u128 pre_f = group_prefix(gsum, f / kExGroup) + tsum[f];
+    const int base = threadIdx.x * kExItems;
+    u128 v[kExItems];
+    u128 s = 0;
+#pragma unroll
+    for (int j = 0; j < kExItems; ++j) {
+        const int i = base + j;
+        v[j] = (i < t.n) ? to_fixed(t.in[i]) : (u128)0;
+        s += v[j];
+    }
+    u128 tot;
+    u128 run = (pre_b - pre_f) + block_exclusive_scan<u128, kExThreads>(s, sm, &tot);
+#pragma unroll
+    for (int j = 0; j < kExItems; ++j) {
+        const int i = base + j;
+        run += v[j];
+        if (i < t.n) t.out[i] = from_fixed(run);
+    }
+}
+
+int exact_plan_tiles(long n) { return div_up(n, kExTile); }
+
+void exact_plan_add(std::vector<ExactTile>& plan, const float* const* in, const long* n, int pieces, float* out) {
+    const int first = (int)plan.size();
+    long o = 0;
+    for (int k = 0; k < pieces; ++k) {
+        for (long i = 0; i < n[k]; i += kExTile) {
+            ExactTile t;
+            t.in = in[k] + i;
+            t.out = out + o + i;
+            t.n = (int)std::min<long>(kExTile, n[k] - i);
+            t.seg_first = first;
+            plan.push_back(t);
+        }
+        o += n[k];
+    }
+}
+
+size_t exact_plan_scratch_bytes(int ntiles) {
+    return ((size_t)ntiles + (size_t)div_up(ntiles, kExGroup) + 2) * sizeof(u128);
+}
+
+cudaError_t exact_scan_plan(const ExactTile* tiles, int nt, void* scratch, cudaStream_t st) {
+    if (nt <= 0) return cudaSuccess;
+    u128* tsum = reinterpret_cast<u128*>(scratch);
+    u128* gsum = tsum + nt;
+    const int ng = div_up(nt, kExGroup);
+    ++g_launches;
+    exact_tab_sums<<<nt, kExThreads, 0, st>>>(tiles, nt, tsum);
+    ++g_launches;
+    exact_tab_groups<<<ng, kExThreads, 0, st>>>(tsum, nt, gsum);
+    ++g_launches;
+    exact_tab_apply<<<nt, kExThreads, 0, st>>>(tiles, nt, tsum, gsum);
+    return cudaGetLastError();
 }
 
 int exact_scan_tiles(long n) { return div_up(n, kExTile); }

@@ -3,6 +3,8 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <vector>
+
 #include "common.cuh"
 
 namespace k3dom {
@@ -40,51 +42,58 @@ cudaError_t exact_scan_float(const float* in, float* out, long n, void* scratch,
 cudaError_t exact_scan_float2(const float* a, long na, const float* b, long nb, float* out,
                               void* scratch, cudaStream_t st);
 
+// Segmented exact scan driven by a plan of tiles (each <= 2048 elements, one contiguous input
+// and output range, and the index of its segment's first tile).
+struct ExactTile {
+    const float* in;
+    float* out;
+    int n;
+    int seg_first;
+};
+// Appends one segment made of `pieces` input ranges, written contiguously from `out`.
+void exact_plan_add(std::vector<ExactTile>& plan, const float* const* in, const long* n, int pieces, float* out);
+size_t exact_plan_scratch_bytes(int ntiles);
+cudaError_t exact_scan_plan(const ExactTile* tiles, int nt, void* scratch, cudaStream_t st);
+
 // particles.cu
-void launch_predict(const DevParams& p, const FrameParams* fp, Particles a, cudaStream_t st);
-void launch_shift_particles(const DevParams& p, Particles a, int mx, int my, int mz,
-                            cudaStream_t st);
-void launch_gather_segsum(const DevParams& p, Particles a, Particles s,
-                          const uint32_t* sorted_keys, const uint32_t* perm, CellWork cw,
-                          cudaStream_t st);
-void launch_reweight(const DevParams& p, Particles s, const uint32_t* sorted_keys, CellWork cw,
-                     cudaStream_t st);
-void launch_births(const DevParams& p, const FrameParams* fp, const float* born,
-                   const float* born_cum, Particles b, cudaStream_t st);
-void launch_init_particles(const DevParams& p, const FrameParams* fp, const float* born_cum,
-                           Particles a, cudaStream_t st);
-void launch_joint_prepare(const DevParams& p, Particles s, Particles b, float* joint_w,
-                          cudaStream_t st);
-void launch_draw_keys(const DevParams& p, const FrameParams* fp, uint32_t* keys,
-                      cudaStream_t st);
-void launch_resample(const DevParams& p, const float* joint_cum, const uint32_t* sorted_draws,
-                     Particles s, const uint32_t* sorted_keys, Particles b, Particles out,
-                     int* ancestors, float* joint_max_out, cudaStream_t st);
+void launch_predict(const Batch& bt, Particles a, cudaStream_t st);
+void launch_shift_particles(int n, Particles a, int mx, int my, int mz, cudaStream_t st);
+void launch_gather_segsum(const Batch& bt, Particles a, Particles s, const uint32_t* sorted_keys,
+                          const uint32_t* perm, CellWork cw, cudaStream_t st);
+void launch_reweight(const Batch& bt, Particles s, const uint32_t* sorted_keys, CellWork cw, cudaStream_t st);
+void launch_births(const Batch& bt, const float* born, const float* born_cum, Particles b, cudaStream_t st);
+void launch_init_particles(const Batch& bt, const float* born_cum, Particles a, cudaStream_t st);
+void launch_joint_prepare(const Batch& bt, Particles s, Particles b, cudaStream_t st);
+int draw_key_bits(int S);
+void launch_draw_keys(const Batch& bt, uint32_t* keys, cudaStream_t st);
+void launch_resample(const Batch& bt, const float* joint_cum, const uint32_t* sorted_draws, Particles s,
+                     Particles b, Particles out, int* ancestors, float* joint_max_out, cudaStream_t st);
 void launch_debug_draws(uint64_t seed, int frame, int stage, long first, long count, float* dst,
                         cudaStream_t st);
 
 // cells.cu
-void launch_cells_init(const DevParams& p, CellState cs, CellWork cw, cudaStream_t st);
+void launch_cells_init(const Batch& bt, CellState cs, CellWork cw, cudaStream_t st);
 void launch_map_shift_full(const DevParams& p, CellState src, CellState dst, const int* s_start,
                            const int* s_end, int* d_start, int* d_end, int mx, int my, int mz,
                            cudaStream_t st);
+// Exports take the scene's own ranges (pointers offset by its cell range); range_base is the
+// scene's first sorted particle.
 void launch_export_field(const DevParams& p, int field, CellState cs, CellWork cw,
-                         const float* born_cum, float* dst, cudaStream_t st);
+                         const float* born_cum, int range_base, float* dst, cudaStream_t st);
 void launch_export_gridcell(const DevParams& p, CellState cs, CellWork cw, const float* born_cum,
-                            void* dst, cudaStream_t st);
+                            int range_base, void* dst, cudaStream_t st);
 void launch_export_mappoints(const DevParams& p, float cx, float cy, float cz, CellState cs,
                              CellWork cw, float* dst, cudaStream_t st);
 
 // evidence.cu
 struct RayBuffers {
     float4* ray_a;         // m.x, m.y, m.z, d_m (K3DOM) | |m|^2 (DS)
-    float4* ray_b;         // u.x, u.y, u.z, margin (FP32 unit direction)
     double4* ray_c;        // d_m, margin, 1/d_m, 0 in FP64 (K3DOM)
-    float4* ktab;          // sparse-kernel table (build_kernel_table)
-    uint32_t* counts;      // per ray: number of tiles touched
+    float4* ktab;          // per scene: sparse-kernel table with the fixed-point scale folded in
+    uint32_t* counts;      // per point slot: number of tiles touched
     uint32_t* offsets;     // exclusive scan of counts
-    uint32_t* ekeys;       // entries: tile id
-    uint32_t* evals;       // entries: ray id
+    uint32_t* ekeys;       // entries: global tile id
+    uint32_t* evals;       // entries: point slot
     uint32_t* ekeys2;      // sorted
     uint32_t* evals2;
     uint32_t* ekeys_alt;
@@ -94,33 +103,29 @@ struct RayBuffers {
     uint32_t* item_off;    // T+1 work-item offsets per tile
     uint32_t* tile_done;   // T
     unsigned long long* acc;  // 2*C fixed-point accumulators (K3DOM) / DS partials
-    uint8_t* ds_counts;    // DS: per (item, cell) hit counts of pass 1
-    uint32_t* ds_quota_base;  // DS: item index of a tile's first item
+    uint8_t* ds_counts;    // DS: per (item, cell) neighbour counts of pass 1
     uint32_t* hist;
     uint32_t* scan_tmp;
     uint32_t* total;       // [0] = entries, [2] = entries kept (0 on overflow)
     long capacity;         // entries
     long ds_count_capacity;
-    int max_points;
-    int tiles, tx, ty, tz, ntx, nty, ntz;
+    int chunk;             // rays per work item
 };
-struct EvidenceConfig {
-    int tile_x, tile_y, tile_z;  // cells per tile (multiples of 4, 4, 2)
-    int chunk;                   // rays per work item
-};
-long ray_entries_bound(const DevParams& p, const EvidenceConfig& ec, int max_points);
-cudaError_t build_ray_lists(const DevParams& p, const FrameParams* fp, const float* xs,
-                            const float* ys, const float* zs, RayBuffers& rb, bool ds,
-                            DevStatus* status, cudaStream_t st);
-cudaError_t launch_k3dom_evidence(const DevParams& p, const FrameParams* fp, RayBuffers& rb,
-                                  CellState cs, CellWork cw, bool first_frame,
-                                  DevStatus* status, int num_sms, cudaStream_t st);
-cudaError_t launch_ds_evidence(const DevParams& p, const FrameParams* fp, RayBuffers& rb,
-                               CellState cs, CellWork cw, bool first_frame, DevStatus* status,
-                               int num_sms, cudaStream_t st);
+long ray_entries_bound(const DevParams& p, const TileShape& ts, int max_points);
+// Per-scene evidence constants (binning radius, cull radius, fixed-point scale); writes the
+// scene's kernel table when ktab is not null.
+void fill_scene_evidence(SceneDev& sd, bool ds, float4* ktab);
+cudaError_t build_ray_lists(const Batch& bt, const float* xs, const float* ys, const float* zs, RayBuffers& rb,
+                            bool ds, DevStatus* status, cudaStream_t st);
+cudaError_t launch_k3dom_evidence(const Batch& bt, RayBuffers& rb, CellState cs, CellWork cw, bool first_frame,
+                                  DevStatus* status, int grid, cudaStream_t st);
+cudaError_t launch_ds_evidence(const Batch& bt, RayBuffers& rb, CellState cs, CellWork cw, bool first_frame,
+                               DevStatus* status, int grid, cudaStream_t st);
+int bgki_blocks_per_sm();
+long ds_count_bytes(long items);
 cudaError_t evidence_init();
-// Host: the sparse-kernel table (512 float4) for sigma, uploaded once per handle.
-void build_kernel_table(float sigma, float4* out);
+// Host: the sparse-kernel table (512 float4) for sigma, every value multiplied by scale.
+void build_kernel_table(float sigma, double scale, float4* out);
 constexpr int kKernelTableSize = 512;
 
 }  // namespace k3dom

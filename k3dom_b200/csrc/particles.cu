@@ -17,57 +17,63 @@ using namespace k3dom_draws;
 
 // ---------------------------------------------------------------- prediction
 // predictKernel (src/common/kernel/predict.cu:12-59), preceded by moveParticlesKernel
-// (src/common/kernel/ego_motion_compensation.cu:12-18) when a map shift is pending.
-__global__ void __launch_bounds__(kBlock) k_predict(DevParams p, const FrameParams* __restrict__ fpp,
-                                                    Particles a) {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= p.P) return;
-    const FrameParams fp = *fpp;
-    float px = a.px[i], py = a.py[i], pz = a.pz[i];
-    float vx = a.vx[i], vy = a.vy[i], vz = a.vz[i];
-    float w = a.w[i];
-    if (fp.shift_pending) {
-        px = __fsub_rn(px, (float)fp.shift_x);
-        py = __fsub_rn(py, (float)fp.shift_y);
-        pz = __fsub_rn(pz, (float)fp.shift_z);
+// (src/common/kernel/ego_motion_compensation.cu:12-18) when a map shift is pending. Over all
+// scenes of the batch; the Philox item is the particle's index within its scene and the
+// stored cell index is the global one (scene cell offset + x + G y + G^2 z).
+__global__ void __launch_bounds__(kBlock) k_predict(Batch bt, Particles a) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < bt.P; i += gridDim.x * blockDim.x) {
+        const int sc = scene_of(bt.off->part, bt.S, i);
+        const DevParams& p = bt.sc[sc].p;
+        const FrameParams fp = bt.fp[sc];
+        const int local = i - bt.off->part[sc];
+        float px = a.px[i], py = a.py[i], pz = a.pz[i];
+        float vx = a.vx[i], vy = a.vy[i], vz = a.vz[i];
+        float w = a.w[i];
+        if (fp.shift_pending) {
+            px = __fsub_rn(px, (float)fp.shift_x);
+            py = __fsub_rn(py, (float)fp.shift_y);
+            pz = __fsub_rn(pz, (float)fp.shift_z);
+        }
+        float n[6];
+        predict_normals(fp.seed, fp.frame, (uint64_t)local, n);
+        const float noise_pos = p.noise_pos, noise_vel = p.noise_vel;
+        // curand_normal(state, 0, s) = z * s + 0 (include/common/cuda_utils.h:33-35)
+        const float npx = __fadd_rn(__fmul_rn(n[0], noise_pos), 0.0f);
+        const float npy = __fadd_rn(__fmul_rn(n[1], noise_pos), 0.0f);
+        const float npz = __fadd_rn(__fmul_rn(n[2], noise_pos), 0.0f);
+        const float nvx = __fadd_rn(__fmul_rn(n[3], noise_vel), 0.0f);
+        const float nvy = __fadd_rn(__fmul_rn(n[4], noise_vel), 0.0f);
+        const float nvz = __fadd_rn(__fmul_rn(n[5], noise_vel), 0.0f);
+        // pos += vel * dt + noise  (old velocity)
+        px = __fadd_rn(px, __fadd_rn(__fmul_rn(vx, fp.dt), npx));
+        py = __fadd_rn(py, __fadd_rn(__fmul_rn(vy, fp.dt), npy));
+        pz = __fadd_rn(pz, __fadd_rn(__fmul_rn(vz, fp.dt), npz));
+        vx = __fadd_rn(vx, nvx);
+        vy = __fadd_rn(vy, nvy);
+        vz = __fadd_rn(vz, nvz);
+        w = __fmul_rn(w, p.p_S);
+        const float lim = __fmul_rn(5.0f, p.init_max_vel);
+        const float nlim = __fmul_rn(-5.0f, p.init_max_vel);
+        vx = clampv(vx, nlim, lim);
+        vy = clampv(vy, nlim, lim);
+        vz = clampv(vz, nlim, lim);
+        const int Gi = p.G, Gzi = p.Gz;
+        const float G = (float)Gi, Gz = (float)Gzi;
+        if ((px >= G || px < 0.0f) || (py >= G || py < 0.0f) || (pz >= Gz || pz < 0.0f)) w = 0.0f;
+        const int ix = clampv(f2i_trunc(px), 0, Gi - 1);
+        const int iy = clampv(f2i_trunc(py), 0, Gi - 1);
+        const int iz = clampv(f2i_trunc(pz), 0, Gzi - 1);
+        a.px[i] = px; a.py[i] = py; a.pz[i] = pz;
+        a.vx[i] = vx; a.vy[i] = vy; a.vz[i] = vz;
+        a.w[i] = w;
+        a.cell[i] = bt.off->cell[sc] + ix + Gi * iy + Gi * Gi * iz;
     }
-    float n[6];
-    predict_normals(fp.seed, fp.frame, (uint64_t)i, n);
-    // curand_normal(state, 0, s) = z * s + 0 (include/common/cuda_utils.h:33-35)
-    const float npx = __fadd_rn(__fmul_rn(n[0], p.noise_pos), 0.0f);
-    const float npy = __fadd_rn(__fmul_rn(n[1], p.noise_pos), 0.0f);
-    const float npz = __fadd_rn(__fmul_rn(n[2], p.noise_pos), 0.0f);
-    const float nvx = __fadd_rn(__fmul_rn(n[3], p.noise_vel), 0.0f);
-    const float nvy = __fadd_rn(__fmul_rn(n[4], p.noise_vel), 0.0f);
-    const float nvz = __fadd_rn(__fmul_rn(n[5], p.noise_vel), 0.0f);
-    // pos += vel * dt + noise  (old velocity)
-    px = __fadd_rn(px, __fadd_rn(__fmul_rn(vx, fp.dt), npx));
-    py = __fadd_rn(py, __fadd_rn(__fmul_rn(vy, fp.dt), npy));
-    pz = __fadd_rn(pz, __fadd_rn(__fmul_rn(vz, fp.dt), npz));
-    vx = __fadd_rn(vx, nvx);
-    vy = __fadd_rn(vy, nvy);
-    vz = __fadd_rn(vz, nvz);
-    w = __fmul_rn(w, p.p_S);
-    const float lim = __fmul_rn(5.0f, p.init_max_vel);
-    const float nlim = __fmul_rn(-5.0f, p.init_max_vel);
-    vx = clampv(vx, nlim, lim);
-    vy = clampv(vy, nlim, lim);
-    vz = clampv(vz, nlim, lim);
-    const float G = (float)p.G, Gz = (float)p.Gz;
-    if ((px >= G || px < 0.0f) || (py >= G || py < 0.0f) || (pz >= Gz || pz < 0.0f)) w = 0.0f;
-    const int ix = clampv(f2i_trunc(px), 0, p.G - 1);
-    const int iy = clampv(f2i_trunc(py), 0, p.G - 1);
-    const int iz = clampv(f2i_trunc(pz), 0, p.Gz - 1);
-    a.px[i] = px; a.py[i] = py; a.pz[i] = pz;
-    a.vx[i] = vx; a.vy[i] = vy; a.vz[i] = vz;
-    a.w[i] = w;
-    a.cell[i] = ix + p.G * iy + p.G * p.G * iz;
 }
 
-void launch_predict(const DevParams& p, const FrameParams* fp, Particles a, cudaStream_t st) {
-    if (p.P <= 0) return;
+void launch_predict(const Batch& bt, Particles a, cudaStream_t st) {
+    if (bt.P <= 0) return;
     ++g_launches;
-    k_predict<<<div_up(p.P, kBlock), kBlock, 0, st>>>(p, fp, a);
+    k_predict<<<grid_for(bt.P), kBlock, 0, st>>>(bt, a);
 }
 
 __global__ void k_shift_particles(int n, Particles a, int mx, int my, int mz) {
@@ -78,10 +84,10 @@ __global__ void k_shift_particles(int n, Particles a, int mx, int my, int mz) {
     a.pz[i] = __fsub_rn(a.pz[i], (float)mz);
 }
 
-void launch_shift_particles(const DevParams& p, Particles a, int mx, int my, int mz, cudaStream_t st) {
-    if (p.P <= 0) return;
+void launch_shift_particles(int n, Particles a, int mx, int my, int mz, cudaStream_t st) {
+    if (n <= 0) return;
     ++g_launches;
-    k_shift_particles<<<div_up(p.P, kBlock), kBlock, 0, st>>>(p.P, a, mx, my, mz);
+    k_shift_particles<<<div_up(n, kBlock), kBlock, 0, st>>>(n, a, mx, my, mz);
 }
 
 // ---------------------------------------------------------------- gather + segmented sums
@@ -112,15 +118,14 @@ __device__ __forceinline__ SegVal shfl_up_seg(const SegVal& v, int d) {
 }
 
 __global__ void __launch_bounds__(kBlock)
-k_gather_segsum(DevParams p, Particles a, Particles s, const uint32_t* __restrict__ keys,
+k_gather_segsum(Batch bt, Particles a, Particles s, const uint32_t* __restrict__ keys,
                 const uint32_t* __restrict__ perm, CellWork cw) {
     const int lane = threadIdx.x & 31;
     const long warp_global = (long)blockIdx.x * kSegWarps + (threadIdx.x >> 5);
     const long r0 = warp_global * kSegRange;
-    const long P = p.P;
+    const long P = bt.P;
     if (r0 >= P) return;
     const long r1 = min(r0 + (long)kSegRange, P);
-    const float min_sq = __fmul_rn(p.min_vel, p.min_vel);
 
     // carried state of the open segment (ends of the previous chunk)
     SegVal carry = {0.0, 0.0, 0.0, 0.0};
@@ -147,9 +152,11 @@ k_gather_segsum(DevParams p, Particles a, Particles s, const uint32_t* __restric
             const float vx = a.vx[src], vy = a.vy[src], vz = a.vz[src];
             const float w = a.w[src];
             if (mine) {
+                // sorted slots of a scene lie in its particle range (cells are scene-major)
+                const float mv = bt.sc[scene_of(bt.off->part, bt.S, (int)pos)].p.min_vel;
                 const float sp = __fadd_rn(__fadd_rn(__fmul_rn(vx, vx), __fmul_rn(vy, vy)),
                                            __fmul_rn(vz, vz));
-                const bool slow = sp < min_sq;
+                const bool slow = sp < __fmul_rn(mv, mv);
                 s.px[pos] = a.px[src];
                 s.py[pos] = a.py[src];
                 s.pz[pos] = a.pz[src];
@@ -208,12 +215,12 @@ k_gather_segsum(DevParams p, Particles a, Particles s, const uint32_t* __restric
     }
 }
 
-void launch_gather_segsum(const DevParams& p, Particles a, Particles s, const uint32_t* sorted_keys,
+void launch_gather_segsum(const Batch& bt, Particles a, Particles s, const uint32_t* sorted_keys,
                           const uint32_t* perm, CellWork cw, cudaStream_t st) {
-    if (p.P <= 0) return;
-    const long warps = div_up(p.P, kSegRange);
+    if (bt.P <= 0) return;
+    const long warps = div_up(bt.P, kSegRange);
     ++g_launches;
-    k_gather_segsum<<<div_up(warps, kSegWarps), kBlock, 0, st>>>(p, a, s, sorted_keys, perm, cw);
+    k_gather_segsum<<<div_up(warps, kSegWarps), kBlock, 0, st>>>(bt, a, s, sorted_keys, perm, cw);
 }
 
 // ---------------------------------------------------------------- persistent reweight
@@ -222,14 +229,13 @@ void launch_gather_segsum(const DevParams& p, Particles a, Particles s, const ui
 // src/dsphdmib/kernel/mass_update.cu:37-44,64-68 (w /= occ_pred when the cell's weight
 // sum exceeds 1) is applied first. The penalty flag (sign bit) is kept.
 __global__ void __launch_bounds__(kBlock)
-k_reweight(DevParams p, Particles s, const uint32_t* __restrict__ keys, CellWork cw) {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= p.P) return;
+k_reweight(int P, int variant, Particles s, const uint32_t* __restrict__ keys, CellWork cw) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < P; i += gridDim.x * blockDim.x) {
     const uint32_t c = keys[i];
     const float wv = s.w[i];
     const bool flag = signbit(wv);
     float w = fabsf(wv);
-    if (p.variant == 1) {
+    if (variant == 1) {
         const float d = cw.divisor[c];
         if (d > 0.0f) w = __fdiv_rn(w, d);
     }
@@ -237,13 +243,14 @@ k_reweight(DevParams p, Particles s, const uint32_t* __restrict__ keys, CellWork
     const float f = cw.factor[c];
     w = __fadd_rn(0.0f, __fmul_rn(f, w));
     s.w[i] = flag ? -w : w;
+  }
 }
 
-void launch_reweight(const DevParams& p, Particles s, const uint32_t* sorted_keys, CellWork cw,
+void launch_reweight(const Batch& bt, Particles s, const uint32_t* sorted_keys, CellWork cw,
                      cudaStream_t st) {
-    if (p.P <= 0) return;
+    if (bt.P <= 0) return;
     ++g_launches;
-    k_reweight<<<div_up(p.P, kBlock), kBlock, 0, st>>>(p, s, sorted_keys, cw);
+    k_reweight<<<grid_for(bt.P), kBlock, 0, st>>>(bt.P, bt.variant, s, sorted_keys, cw);
 }
 
 // ---------------------------------------------------------------- slot ownership
@@ -314,123 +321,139 @@ __device__ __forceinline__ void cell_centre_idx(int c, int G, float* x, float* y
 // the reference leaves them unwritten. The penalty of penalizeStaticParticlesKernel
 // (resampling.cu:35-42) is recorded in the sign bit of the weight.
 __global__ void __launch_bounds__(kBlock)
-k_births(DevParams p, const FrameParams* __restrict__ fpp, const float* __restrict__ born,
-         const float* __restrict__ cum, Particles b) {
-    const int s = blockIdx.x * blockDim.x + threadIdx.x;
-    if (s >= p.B) return;
-    const FrameParams fp = *fpp;
-    const SlotMap m = make_slotmap(cum, p.C, p.B);
-    int j = m.owner(s);
-    bool assoc;
-    int n, st;
-    if (j < p.C) {
-        st = m.start(j);
-        n = m.bound(j) - 1 - st + 1;
-        const int nu_A0 = (int)roundf(__fmul_rn((float)n, p.p_A));
-        assoc = s < st + nu_A0;
-        b.cell[s] = j;
-        b.assoc[s] = assoc ? 1 : 0;
-    } else {
-        j = b.cell[s];
-        j = clampv(j, 0, p.C - 1);
-        assoc = b.assoc[s] != 0;
-        n = m.count(j);
+k_births(Batch bt, const float* __restrict__ born, const float* __restrict__ cum, Particles b) {
+    for (int g = blockIdx.x * blockDim.x + threadIdx.x; g < bt.B; g += gridDim.x * blockDim.x) {
+        const int sc = scene_of(bt.off->birth, bt.S, g);
+        const DevParams& p = bt.sc[sc].p;
+        const FrameParams& fp = bt.fp[sc];
+        const int s = g - bt.off->birth[sc];  // slot within the scene
+        const int coff = bt.off->cell[sc];
+        const int C = p.C;
+        const float p_A = p.p_A;
+        const SlotMap m = make_slotmap(cum + coff, C, p.B);
+        int j = m.owner(s);
+        bool assoc;
+        int n, st;
+        if (j < C) {
+            st = m.start(j);
+            n = m.bound(j) - 1 - st + 1;
+            const int nu_A0 = (int)roundf(__fmul_rn((float)n, p_A));
+            assoc = s < st + nu_A0;
+            b.cell[g] = coff + j;
+            b.assoc[g] = assoc ? 1 : 0;
+        } else {
+            j = clampv(b.cell[g] - coff, 0, C - 1);
+            assoc = b.assoc[g] != 0;
+            n = m.count(j);
+        }
+        const int nu_A = (int)roundf(__fmul_rn((float)n, p_A));
+        const int nu_UA = n - nu_A;
+        const float bm = born[coff + j];
+        float w;
+        if (assoc) {
+            w = nu_A > 0 ? __fdiv_rn(__fmul_rn(p_A, bm), (float)nu_A) : 0.0f;
+        } else {
+            w = nu_UA > 0 ? (float)((1.0 - (double)p_A) * (double)bm / (double)nu_UA) : 0.0f;
+        }
+        float x, y, z, vx, vy, vz;
+        cell_centre_idx(j, p.G, &x, &y, &z);
+        const U4 r = block(fp.seed, fp.frame, kBirthVel, (uint64_t)s, 0);
+        const float min_vel = p.min_vel;
+        birth_velocity(u01(r.x), u01(r.y), u01(r.z), p.init_max_vel, min_vel, &vx, &vy, &vz);
+        const float sp = __fadd_rn(__fadd_rn(__fmul_rn(vx, vx), __fmul_rn(vy, vy)), __fmul_rn(vz, vz));
+        const bool slow = sp < __fmul_rn(min_vel, min_vel);
+        b.px[g] = x; b.py[g] = y; b.pz[g] = z;
+        b.vx[g] = vx; b.vy[g] = vy; b.vz[g] = vz;
+        b.w[g] = slow ? -w : w;
     }
-    const int nu_A = (int)roundf(__fmul_rn((float)n, p.p_A));
-    const int nu_UA = n - nu_A;
-    const float bm = born[j];
-    float w;
-    if (assoc) {
-        w = nu_A > 0 ? __fdiv_rn(__fmul_rn(p.p_A, bm), (float)nu_A) : 0.0f;
-    } else {
-        w = nu_UA > 0 ? (float)((1.0 - (double)p.p_A) * (double)bm / (double)nu_UA) : 0.0f;
-    }
-    float x, y, z, vx, vy, vz;
-    cell_centre_idx(j, p.G, &x, &y, &z);
-    const U4 r = block(fp.seed, fp.frame, kBirthVel, (uint64_t)s, 0);
-    birth_velocity(u01(r.x), u01(r.y), u01(r.z), p.init_max_vel, p.min_vel, &vx, &vy, &vz);
-    const float sp = __fadd_rn(__fadd_rn(__fmul_rn(vx, vx), __fmul_rn(vy, vy)), __fmul_rn(vz, vz));
-    const bool slow = sp < __fmul_rn(p.min_vel, p.min_vel);
-    b.px[s] = x; b.py[s] = y; b.pz[s] = z;
-    b.vx[s] = vx; b.vy[s] = vy; b.vz[s] = vz;
-    b.w[s] = slow ? -w : w;
 }
 
-void launch_births(const DevParams& p, const FrameParams* fp, const float* born, const float* born_cum,
-                   Particles b, cudaStream_t st) {
-    if (p.B <= 0) return;
+void launch_births(const Batch& bt, const float* born, const float* born_cum, Particles b, cudaStream_t st) {
+    if (bt.B <= 0) return;
     ++g_launches;
-    k_births<<<div_up(p.B, kBlock), kBlock, 0, st>>>(p, fp, born, born_cum, b);
+    k_births<<<grid_for(bt.B), kBlock, 0, st>>>(bt, born, born_cum, b);
 }
 
 // ---------------------------------------------------------------- first frame
 // initParticlesKernel1/2 (init_new_particles.cu:54-104) driven by the born-mass prefix
 // normalised to P (src/k3dom/dom.cu:60-76, src/dsphdmib/dom.cu:65-81).
 __global__ void __launch_bounds__(kBlock)
-k_init_particles(DevParams p, const FrameParams* __restrict__ fpp, const float* __restrict__ cum,
-                 Particles a) {
-    const int s = blockIdx.x * blockDim.x + threadIdx.x;
-    if (s >= p.P) return;
-    const FrameParams fp = *fpp;
-    const SlotMap m = make_slotmap(cum, p.C, p.P);
-    int j = m.owner(s);
-    if (j < p.C) {
-        a.cell[s] = j;
-    } else {
-        j = clampv(a.cell[s], 0, p.C - 1);
+k_init_particles(Batch bt, const float* __restrict__ cum, Particles a) {
+    for (int g = blockIdx.x * blockDim.x + threadIdx.x; g < bt.P; g += gridDim.x * blockDim.x) {
+        const int sc = scene_of(bt.off->part, bt.S, g);
+        const DevParams& p = bt.sc[sc].p;
+        const FrameParams& fp = bt.fp[sc];
+        const int s = g - bt.off->part[sc];
+        const int coff = bt.off->cell[sc];
+        const int C = p.C, P = p.P;
+        const SlotMap m = make_slotmap(cum + coff, C, P);
+        int j = m.owner(s);
+        if (j < C) {
+            a.cell[g] = coff + j;
+        } else {
+            j = clampv(a.cell[g] - coff, 0, C - 1);
+        }
+        float x, y, z, vx, vy, vz;
+        cell_centre_idx(j, p.G, &x, &y, &z);
+        const U4 r = block(fp.seed, fp.frame, kInitVel, (uint64_t)s, 0);
+        birth_velocity(u01(r.x), u01(r.y), u01(r.z), p.init_max_vel, p.min_vel, &vx, &vy, &vz);
+        a.px[g] = x; a.py[g] = y; a.pz[g] = z;
+        a.vx[g] = vx; a.vy[g] = vy; a.vz[g] = vz;
+        a.w[g] = __fdiv_rn(1.0f, (float)P);
     }
-    float x, y, z, vx, vy, vz;
-    cell_centre_idx(j, p.G, &x, &y, &z);
-    const U4 r = block(fp.seed, fp.frame, kInitVel, (uint64_t)s, 0);
-    birth_velocity(u01(r.x), u01(r.y), u01(r.z), p.init_max_vel, p.min_vel, &vx, &vy, &vz);
-    a.px[s] = x; a.py[s] = y; a.pz[s] = z;
-    a.vx[s] = vx; a.vy[s] = vy; a.vz[s] = vz;
-    a.w[s] = __fdiv_rn(1.0f, (float)p.P);
 }
 
-void launch_init_particles(const DevParams& p, const FrameParams* fp, const float* born_cum,
-                           Particles a, cudaStream_t st) {
-    if (p.P <= 0) return;
+void launch_init_particles(const Batch& bt, const float* born_cum, Particles a, cudaStream_t st) {
+    if (bt.P <= 0) return;
     ++g_launches;
-    k_init_particles<<<div_up(p.P, kBlock), kBlock, 0, st>>>(p, fp, born_cum, a);
+    k_init_particles<<<grid_for(bt.P), kBlock, 0, st>>>(bt, born_cum, a);
 }
 
 // ---------------------------------------------------------------- resampling
 // Penalty (resampling.cu:13-36): weights flagged slow become 0, in place, as the reference
 // leaves them; the flags are cleared.
 __global__ void k_joint_prepare(int P, int B, Particles s, Particles b) {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i < P) {
-        const float w = s.w[i];
-        s.w[i] = signbit(w) ? 0.0f : w;
-    } else if (i < P + B) {
-        const float w = b.w[i - P];
-        b.w[i - P] = signbit(w) ? 0.0f : w;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < P + B; i += gridDim.x * blockDim.x) {
+        if (i < P) {
+            const float w = s.w[i];
+            s.w[i] = signbit(w) ? 0.0f : w;
+        } else {
+            const float w = b.w[i - P];
+            b.w[i - P] = signbit(w) ? 0.0f : w;
+        }
     }
 }
 
-void launch_joint_prepare(const DevParams& p, Particles s, Particles b, float* joint_w, cudaStream_t st) {
-    (void)joint_w;
-    if (p.P + p.B <= 0) return;
+void launch_joint_prepare(const Batch& bt, Particles s, Particles b, cudaStream_t st) {
+    if (bt.P + bt.B <= 0) return;
     ++g_launches;
-    k_joint_prepare<<<div_up(p.P + p.B, kBlock), kBlock, 0, st>>>(p.P, p.B, s, b);
+    k_joint_prepare<<<grid_for((long)bt.P + bt.B), kBlock, 0, st>>>(bt.P, bt.B, s, b);
 }
 
 // Resampling draws as 24-bit keys of 1 - u: sorting the keys ascending orders the draws
 // u * joint_max ascending for any joint_max >= 0, so the draws can be sorted before the
 // weights exist (resamplingGenerateRandomNumbersKernel + thrust::sort, resampling.cu:38-53,
-// src/common/dom.cu:277-285).
-__global__ void k_draw_keys(int P, const FrameParams* __restrict__ fpp, uint32_t* keys) {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= P) return;
-    const FrameParams fp = *fpp;
-    keys[i] = one_minus_u01_key(resample_word(fp.seed, fp.frame, (uint64_t)i));
+// src/common/dom.cu:277-285). The scene index sits above the 24 key bits, so one sort orders
+// every scene's draws within the scene's own particle range.
+__global__ void k_draw_keys(Batch bt, uint32_t* keys) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < bt.P; i += gridDim.x * blockDim.x) {
+        const int sc = scene_of(bt.off->part, bt.S, i);
+        const FrameParams& fp = bt.fp[sc];
+        const int local = i - bt.off->part[sc];
+        keys[i] = ((uint32_t)sc << 24) | one_minus_u01_key(resample_word(fp.seed, fp.frame, (uint64_t)local));
+    }
 }
 
-void launch_draw_keys(const DevParams& p, const FrameParams* fp, uint32_t* keys, cudaStream_t st) {
-    if (p.P <= 0) return;
+int draw_key_bits(int S) {
+    int b = 0;
+    while ((1 << b) < S) ++b;
+    return 24 + b;
+}
+
+void launch_draw_keys(const Batch& bt, uint32_t* keys, cudaStream_t st) {
+    if (bt.P <= 0) return;
     ++g_launches;
-    k_draw_keys<<<div_up(p.P, kBlock), kBlock, 0, st>>>(p.P, fp, keys);
+    k_draw_keys<<<grid_for(bt.P), kBlock, 0, st>>>(bt, keys);
 }
 
 constexpr int kResThreads = 256;
@@ -438,45 +461,71 @@ constexpr int kResThreads = 256;
 // calc_resampled_indices + resamplingKernel (resampling.cu:55-89): ancestor =
 // lower_bound(acc, u) where acc's last element is replaced by the largest draw when they
 // differ; the resampled particle is gathered from the sorted persistent set or the birth
-// set with weight joint_max / P.
-__global__ void __launch_bounds__(kResThreads)
-k_resample(DevParams p, const float* __restrict__ cum, const uint32_t* __restrict__ dkeys,
-           Particles s, Particles b, Particles out, int* __restrict__ anc_out,
-           float* __restrict__ joint_max_out) {
-    __shared__ int s_lo, s_hi;
-    const int P = p.P, n = p.P + p.B;
-    const float jmax = cum[n - 1];
-    const float om_max = (float)dkeys[P - 1] * 5.9604644775390625e-08f;
-    const float rmax = __fadd_rn(0.0f, __fmul_rn(jmax, om_max));
-    const int k0 = blockIdx.x * kResThreads;
-    const int k1 = min(k0 + kResThreads, P) - 1;
-    auto acc = [&](int j) -> float { return j == n - 1 ? rmax : cum[j]; };
-    auto lower = [&](float u, int lo, int hi) -> int {  // first j in [lo, hi) with acc[j] >= u
+// set with weight joint_max / P. Ancestors are scene-local indices into [persistent, births).
+struct ResScene {
+    const float* cum;
+    int n, P;
+    float jmax, rmax;
+    const uint32_t* dk;  // the scene's sorted draw keys
+    __device__ __forceinline__ float acc(int j) const { return j == n - 1 ? rmax : cum[j]; }
+    __device__ __forceinline__ int lower(float u, int lo, int hi) const {  // first j in [lo, hi) with acc[j] >= u
         while (lo < hi) {
-            int mid = (lo + hi) >> 1;
+            const int mid = (lo + hi) >> 1;
             if (acc(mid) < u) lo = mid + 1; else hi = mid;
         }
         return lo;
-    };
-    auto draw = [&](int k) -> float {
-        const float om = (float)dkeys[k] * 5.9604644775390625e-08f;
+    }
+    __device__ __forceinline__ float draw(int k) const {  // k local
+        const float om = (float)(dk[k] & 0xFFFFFFu) * 5.9604644775390625e-08f;
         return __fadd_rn(0.0f, __fmul_rn(jmax, om));
-    };
-    if (threadIdx.x == 0) s_lo = lower(draw(k0), 0, n);
-    if (threadIdx.x == 32) s_hi = lower(draw(k1), 0, n);
+    }
+};
+
+__device__ __forceinline__ ResScene res_scene(const Batch& bt, const float* joint_cum, const uint32_t* dkeys, int sc) {
+    ResScene r;
+    const DevParams& p = bt.sc[sc].p;
+    r.P = p.P;
+    r.n = p.P + p.B;
+    r.cum = joint_cum + bt.off->joint[sc];
+    r.dk = dkeys + bt.off->part[sc];
+    r.jmax = r.cum[r.n - 1];
+    const float om_max = (float)(r.dk[r.P - 1] & 0xFFFFFFu) * 5.9604644775390625e-08f;
+    r.rmax = __fadd_rn(0.0f, __fmul_rn(r.jmax, om_max));
+    return r;
+}
+
+__global__ void __launch_bounds__(kResThreads)
+k_resample(Batch bt, const float* __restrict__ joint_cum, const uint32_t* __restrict__ dkeys, Particles s,
+           Particles b, Particles out, int* __restrict__ anc_out, float* __restrict__ joint_max_out) {
+    __shared__ int s_lo, s_hi;
+    const int k0 = blockIdx.x * kResThreads;
+    const int k1 = min(k0 + kResThreads, bt.P) - 1;
+    const int sc0 = scene_of(bt.off->part, bt.S, k0);
+    const bool one_scene = scene_of(bt.off->part, bt.S, k1) == sc0;
+    if (one_scene) {
+        // the block's draws are sorted: bracket their search by the first and last
+        const ResScene r = res_scene(bt, joint_cum, dkeys, sc0);
+        const int base = bt.off->part[sc0];
+        if (threadIdx.x == 0) s_lo = r.lower(r.draw(k0 - base), 0, r.n);
+        if (threadIdx.x == 32) s_hi = r.lower(r.draw(k1 - base), 0, r.n);
+    }
     __syncthreads();
     const int k = k0 + threadIdx.x;
-    if (k >= P) return;
-    int a = lower(draw(k), s_lo, min(s_hi + 1, n));
-    if (a > n - 1) a = n - 1;
-    const float new_w = __fdiv_rn(jmax, (float)P);
-    if (a < P) {
-        out.px[k] = s.px[a]; out.py[k] = s.py[a]; out.pz[k] = s.pz[a];
-        out.vx[k] = s.vx[a]; out.vy[k] = s.vy[a]; out.vz[k] = s.vz[a];
-        out.cell[k] = s.cell[a];
-        out.assoc[k] = s.assoc[a];
+    if (k >= bt.P) return;
+    const int sc = one_scene ? sc0 : scene_of(bt.off->part, bt.S, k);
+    const ResScene r = res_scene(bt, joint_cum, dkeys, sc);
+    const int kl = k - bt.off->part[sc];
+    int a = one_scene ? r.lower(r.draw(kl), s_lo, min(s_hi + 1, r.n)) : r.lower(r.draw(kl), 0, r.n);
+    if (a > r.n - 1) a = r.n - 1;
+    const float new_w = __fdiv_rn(r.jmax, (float)r.P);
+    if (a < r.P) {
+        const int q = bt.off->part[sc] + a;
+        out.px[k] = s.px[q]; out.py[k] = s.py[q]; out.pz[k] = s.pz[q];
+        out.vx[k] = s.vx[q]; out.vy[k] = s.vy[q]; out.vz[k] = s.vz[q];
+        out.cell[k] = s.cell[q];
+        out.assoc[k] = s.assoc[q];
     } else {
-        const int q = a - P;
+        const int q = bt.off->birth[sc] + a - r.P;
         out.px[k] = b.px[q]; out.py[k] = b.py[q]; out.pz[k] = b.pz[q];
         out.vx[k] = b.vx[q]; out.vy[k] = b.vy[q]; out.vz[k] = b.vz[q];
         out.cell[k] = b.cell[q];
@@ -484,17 +533,15 @@ k_resample(DevParams p, const float* __restrict__ cum, const uint32_t* __restric
     }
     out.w[k] = new_w;
     anc_out[k] = a;
-    if (k == 0 && joint_max_out) *joint_max_out = jmax;
+    if (kl == 0 && joint_max_out) joint_max_out[sc] = r.jmax;
 }
 
-void launch_resample(const DevParams& p, const float* joint_cum, const uint32_t* sorted_draws,
-                     Particles s, const uint32_t* sorted_keys, Particles b, Particles out,
-                     int* ancestors, float* joint_max_out, cudaStream_t st) {
-    (void)sorted_keys;
-    if (p.P <= 0) return;
+void launch_resample(const Batch& bt, const float* joint_cum, const uint32_t* sorted_draws, Particles s,
+                     Particles b, Particles out, int* ancestors, float* joint_max_out, cudaStream_t st) {
+    if (bt.P <= 0) return;
     ++g_launches;
-    k_resample<<<div_up(p.P, kResThreads), kResThreads, 0, st>>>(p, joint_cum, sorted_draws, s, b, out,
-                                                                 ancestors, joint_max_out);
+    k_resample<<<div_up(bt.P, kResThreads), kResThreads, 0, st>>>(bt, joint_cum, sorted_draws, s, b, out,
+                                                                   ancestors, joint_max_out);
 }
 
 // ---------------------------------------------------------------- debug draws

@@ -98,7 +98,7 @@ __global__ void scan_u32_apply(const uint32_t* __restrict__ in, long nmax, const
 
 int scan_u32_tiles(long n) { return div_up(n, kScanTile); }
 
-static int grid_for(long tiles) { return (int)std::max(1L, std::min(tiles, (long)kGridCap)); }
+static int tile_grid(long tiles) { return (int)std::max(1L, std::min(tiles, (long)kGridCap)); }
 
 // Exclusive scan of n u32 values (in may alias out); n = min(*dn, nmax) when dn is given.
 // tmp needs scan_u32_tiles(nmax) words. total (optional, device) receives the sum.
@@ -107,11 +107,11 @@ cudaError_t scan_u32_exclusive_dn(const uint32_t* in, uint32_t* out, long nmax, 
     if (nmax <= 0) return cudaSuccess;
     int nt = scan_u32_tiles(nmax);
     ++g_launches;
-    scan_u32_tile_sums<<<grid_for(nt), kScanThreads, 0, st>>>(in, nmax, dn, tmp);
+    scan_u32_tile_sums<<<tile_grid(nt), kScanThreads, 0, st>>>(in, nmax, dn, tmp);
     ++g_launches;
     scan_u32_tile_offsets<<<1, kScanThreads, 0, st>>>(tmp, nmax, dn, total);
     ++g_launches;
-    scan_u32_apply<<<grid_for(nt), kScanThreads, 0, st>>>(in, nmax, dn, tmp, out);
+    scan_u32_apply<<<tile_grid(nt), kScanThreads, 0, st>>>(in, nmax, dn, tmp, out);
     return cudaGetLastError();
 }
 
@@ -268,11 +268,11 @@ static cudaError_t radix_pass(const uint32_t* kin, const uint32_t* vin, uint32_t
     // the last word of hist holds the live histogram length (device count case)
     uint32_t* hist_len = hist + hn;
     ++g_launches;
-    radix_upsweep<BITS><<<grid_for(nt), kSortThreads, 0, st>>>(kin, nmax, dn, shift, hist, dn ? hist_len : nullptr);
+    radix_upsweep<BITS><<<tile_grid(nt), kSortThreads, 0, st>>>(kin, nmax, dn, shift, hist, dn ? hist_len : nullptr);
     cudaError_t e = scan_u32_exclusive_dn(hist, hist, hn, dn ? hist_len : nullptr, scan_tmp, nullptr, st);
     if (e != cudaSuccess) return e;
     ++g_launches;
-    radix_downsweep<BITS><<<grid_for(nt), kSortThreads, sizeof(RadixSmem<BITS>), st>>>(kin, vin, nmax, dn, shift,
+    radix_downsweep<BITS><<<tile_grid(nt), kSortThreads, sizeof(RadixSmem<BITS>), st>>>(kin, vin, nmax, dn, shift,
                                                                                        hist, kout, vout);
     return cudaGetLastError();
 }

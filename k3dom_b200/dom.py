@@ -89,15 +89,23 @@ def _is_cuda_tensor(x) -> bool:
 
 
 class DOM:
-    """The K3DOM / DS-PHD/MIB grid (dom::DOM), on one GPU."""
+    """The K3DOM / DS-PHD/MIB grid (dom::DOM), on one GPU.
 
-    def __init__(self, params: N.Params, variant="k3dom", device: int = 0):
+    A DOM either owns a single-scene handle or is a view of one scene of a BatchDOM
+    (BatchDOM.scene(s)); per-scene calls select that scene first."""
+
+    def __init__(self, params: N.Params, variant="k3dom", device: int = 0, _handle=None, _scene: int = 0):
         self._lib = N.load()
         self.variant = _variant(variant)
         self.params = params
-        h = C.c_void_p()
-        N.check(self._lib.k3dom_create(C.byref(params), self.variant, int(device), C.byref(h)), "k3dom_create")
-        self._h = h
+        self._scene = int(_scene)
+        self._owner = _handle is None
+        if _handle is None:
+            h = C.c_void_p()
+            N.check(self._lib.k3dom_create(C.byref(params), self.variant, int(device), C.byref(h)), "k3dom_create")
+            self._h = h
+        else:
+            self._h = _handle
         info = self.info()
         self.grid_size = info.grid_size
         self.grid_size_z = info.grid_size_z
@@ -108,8 +116,13 @@ class DOM:
     # -- lifetime
     def close(self) -> None:
         if getattr(self, "_h", None):
-            self._lib.k3dom_destroy(self._h)
+            if self._owner:
+                self._lib.k3dom_destroy(self._h)
             self._h = None
+
+    def _sel(self):
+        N.check(self._lib.k3dom_select_scene(self._h, self._scene), "k3dom_select_scene")
+        return self._h
 
     def __del__(self):
         try:
@@ -146,7 +159,7 @@ class DOM:
 
     # -- DOM_c interface (include/common/dom.h:57-94)
     def updatePose(self, x: float, y: float, z: float) -> None:
-        N.check(self._lib.k3dom_update_pose(self._h, float(x), float(y), float(z)), "k3dom_update_pose")
+        N.check(self._lib.k3dom_update_pose(self._sel(), float(x), float(y), float(z)), "k3dom_update_pose")
 
     def updateGrid(self, t: float, xs, ys=None, zs=None) -> None:
         px, py, pz, n, mem, _keep = self._points(xs, ys, zs)
@@ -199,7 +212,7 @@ class DOM:
     # -- getters (include/common/dom.h:59-83)
     def info(self) -> N.Info:
         i = N.Info()
-        N.check(self._lib.k3dom_get_info(self._h, C.byref(i)), "k3dom_get_info")
+        N.check(self._lib.k3dom_get_info(self._sel(), C.byref(i)), "k3dom_get_info")
         return i
 
     def getGridSize(self) -> int:
@@ -218,7 +231,7 @@ class DOM:
 
     def indexToCoord(self, i: int):
         x, y, z = C.c_float(), C.c_float(), C.c_float()
-        N.check(self._lib.k3dom_index_to_coord(self._h, int(i), C.byref(x), C.byref(y), C.byref(z)), "indexToCoord")
+        N.check(self._lib.k3dom_index_to_coord(self._sel(), int(i), C.byref(x), C.byref(y), C.byref(z)), "indexToCoord")
         return x.value, y.value, z.value
 
     def indexToCoordX(self, i: int) -> float: return self.indexToCoord(i)[0]
@@ -228,24 +241,24 @@ class DOM:
     # -- readback
     def get_cell_field(self, name: str) -> np.ndarray:
         out = np.empty(self.grid_cell_count, np.float32)
-        N.check(self._lib.k3dom_get_cell_field(self._h, N.CELL_FIELDS[name], _ptr(out), N.MEM_HOST), name)
+        N.check(self._lib.k3dom_get_cell_field(self._sel(), N.CELL_FIELDS[name], _ptr(out), N.MEM_HOST), name)
         return out
 
     def get_cell_ranges(self):
         s = np.empty(self.grid_cell_count, np.int32)
         e = np.empty(self.grid_cell_count, np.int32)
-        N.check(self._lib.k3dom_get_cell_ranges(self._h, _ptr(s), _ptr(e), N.MEM_HOST), "cell_ranges")
+        N.check(self._lib.k3dom_get_cell_ranges(self._sel(), _ptr(s), _ptr(e), N.MEM_HOST), "cell_ranges")
         return s, e
 
     def get_gridcells(self) -> np.ndarray:
         """The 68-byte dom::GridCell array the ROS node copies back (k3dom_node.cpp:131-132)."""
         out = np.empty(self.grid_cell_count, GRIDCELL_DTYPE)
-        N.check(self._lib.k3dom_get_gridcell_aos(self._h, _ptr(out), N.MEM_HOST), "gridcell_aos")
+        N.check(self._lib.k3dom_get_gridcell_aos(self._sel(), _ptr(out), N.MEM_HOST), "gridcell_aos")
         return out
 
     def get_mappoints(self) -> np.ndarray:
         out = np.empty(self.grid_cell_count, MAPPOINT_DTYPE)
-        N.check(self._lib.k3dom_get_mappoints(self._h, _ptr(out), N.MEM_HOST), "mappoints")
+        N.check(self._lib.k3dom_get_mappoints(self._sel(), _ptr(out), N.MEM_HOST), "mappoints")
         return out
 
     def set_cell_masses(self, free=None, static=None, dynamic=None, occ=None) -> None:
@@ -253,7 +266,7 @@ class DOM:
         for a in arrs:
             if a is not None and a.size != self.grid_cell_count:
                 raise ValueError("cell array size mismatch")
-        N.check(self._lib.k3dom_set_cell_masses(self._h, *[_ptr(a) for a in arrs], N.MEM_HOST), "set_cell_masses")
+        N.check(self._lib.k3dom_set_cell_masses(self._sel(), *[_ptr(a) for a in arrs], N.MEM_HOST), "set_cell_masses")
 
     def get_particles(self, which: str = "persistent") -> dict:
         n = self.new_born_particle_count if which == "birth" else self.particle_count
@@ -262,7 +275,7 @@ class DOM:
         w = np.empty(n, np.float32)
         cell = np.empty(n, np.int32)
         assoc = np.empty(n, np.uint8)
-        N.check(self._lib.k3dom_get_particles(self._h, _SETS[which], _ptr(pos), _ptr(vel), _ptr(w), _ptr(cell),
+        N.check(self._lib.k3dom_get_particles(self._sel(), _SETS[which], _ptr(pos), _ptr(vel), _ptr(w), _ptr(cell),
                                               _ptr(assoc), N.MEM_HOST), "get_particles")
         return {"pos": pos, "vel": vel, "weight": w, "cell": cell, "associated": assoc}
 
@@ -273,24 +286,24 @@ class DOM:
         weight = None if weight is None else _f32(weight).reshape(n)
         cell = None if cell is None else np.ascontiguousarray(cell, np.int32).reshape(n)
         associated = None if associated is None else np.ascontiguousarray(associated, np.uint8).reshape(n)
-        N.check(self._lib.k3dom_set_particles(self._h, _SETS[which], _ptr(pos), _ptr(vel), _ptr(weight), _ptr(cell),
+        N.check(self._lib.k3dom_set_particles(self._sel(), _SETS[which], _ptr(pos), _ptr(vel), _ptr(weight), _ptr(cell),
                                               _ptr(associated), N.MEM_HOST), "set_particles")
 
     def sort_permutation(self) -> np.ndarray:
         out = np.empty(self.particle_count, np.int32)
-        N.check(self._lib.k3dom_get_sort_permutation(self._h, _ptr(out), N.MEM_HOST), "sort_permutation")
+        N.check(self._lib.k3dom_get_sort_permutation(self._sel(), _ptr(out), N.MEM_HOST), "sort_permutation")
         return out
 
     def ancestors(self) -> np.ndarray:
         out = np.empty(self.particle_count, np.int32)
-        N.check(self._lib.k3dom_get_ancestors(self._h, _ptr(out), N.MEM_HOST), "ancestors")
+        N.check(self._lib.k3dom_get_ancestors(self._sel(), _ptr(out), N.MEM_HOST), "ancestors")
         return out
 
     def resampling_state(self):
         jc = np.empty(self.particle_count + self.new_born_particle_count, np.float32)
         bc = np.empty(self.grid_cell_count, np.float32)
         jm = np.empty(1, np.float32)
-        N.check(self._lib.k3dom_get_resampling_state(self._h, _ptr(jc), _ptr(bc), _ptr(jm), N.MEM_HOST),
+        N.check(self._lib.k3dom_get_resampling_state(self._sel(), _ptr(jc), _ptr(bc), _ptr(jm), N.MEM_HOST),
                 "resampling_state")
         return jc, bc, float(jm[0])
 
@@ -310,10 +323,137 @@ class DOM:
         N.check(self._lib.k3dom_get_diagnostics(self._h, C.byref(d)), "diagnostics")
         return {k: getattr(d, k) for k, _ in d._fields_}
 
+    def autotune(self, on: bool = True) -> None:
+        N.check(self._lib.k3dom_autotune(self._h, 1 if on else 0), "k3dom_autotune")
+
+    def tuning(self) -> dict:
+        t = N.Tuning()
+        N.check(self._lib.k3dom_get_tuning(self._h, C.byref(t)), "k3dom_get_tuning")
+        d = {k: getattr(t, k) for k, _ in t._fields_ if k != "candidate_ms"}
+        d["candidate_ms"] = list(t.candidate_ms)[: t.candidates]
+        return d
+
+    def set_tuning(self, tile_rule: int, chunk: int) -> None:
+        N.check(self._lib.k3dom_set_tuning(self._h, int(tile_rule), int(chunk)), "k3dom_set_tuning")
+
     def stream(self) -> int:
         s = C.c_void_p()
         N.check(self._lib.k3dom_get_stream(self._h, C.byref(s)), "get_stream")
         return s.value or 0
+
+
+def _points_of(item):
+    """(xs, ys, zs) of one scene's points: an (n, 3) array/tensor or an (xs, ys, zs) tuple."""
+    if isinstance(item, (tuple, list)) and len(item) == 3:
+        return item[0], item[1], item[2]
+    return item, None, None
+
+
+class BatchDOM:
+    """S independent scenes updated together (k3dom_batch_*): one launch per stage for all
+    scenes, each scene bit-identical to the same scene in a DOM of its own."""
+
+    def __init__(self, params_list, variant="k3dom", device: int = 0):
+        self._lib = N.load()
+        self.variant = _variant(variant)
+        self.params = list(params_list)
+        arr = (N.Params * len(self.params))(*self.params)
+        h = C.c_void_p()
+        N.check(self._lib.k3dom_batch_create(arr, len(self.params), self.variant, int(device), C.byref(h)),
+                "k3dom_batch_create")
+        self._h = h
+        self.scenes = [DOM(p, variant, _handle=h, _scene=s) for s, p in enumerate(self.params)]
+
+    def __len__(self):
+        return len(self.scenes)
+
+    def scene(self, s: int) -> DOM:
+        return self.scenes[s]
+
+    def close(self) -> None:
+        if getattr(self, "_h", None):
+            for v in self.scenes:
+                v._h = None
+            self._lib.k3dom_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def updatePose(self, scene: int, x: float, y: float, z: float) -> None:
+        N.check(self._lib.k3dom_batch_update_pose(self._h, int(scene), float(x), float(y), float(z)),
+                "k3dom_batch_update_pose")
+
+    def _pack(self, points):
+        S = len(self.scenes)
+        if len(points) != S:
+            raise ValueError(f"expected points for {S} scenes, got {len(points)}")
+        xs, ys, zs, ns, keep, mems = [], [], [], [], [], set()
+        for s in range(S):
+            px, py, pz, n, mem, k = self.scenes[s]._points(*_points_of(points[s]))
+            xs.append(px)
+            ys.append(py)
+            zs.append(pz)
+            ns.append(n)
+            keep.append(k)
+            mems.add(mem)
+        if len(mems) != 1:
+            raise ValueError("all scenes' points must be host arrays, or all CUDA tensors")
+        PA = C.c_void_p * S
+        return (PA(*xs), PA(*ys), PA(*zs), (C.c_int32 * S)(*ns), mems.pop(), keep)
+
+    def update(self, t, points) -> None:
+        """One frame of every scene: t[s] and points[s] ((n, 3) or (xs, ys, zs))."""
+        xs, ys, zs, ns, mem, _keep = self._pack(points)
+        tt = (C.c_float * len(self.scenes))(*[float(v) for v in t])
+        N.check(self._lib.k3dom_batch_update(self._h, tt, xs, ys, zs, ns, mem), "k3dom_batch_update")
+
+    def update_async(self, t, points) -> None:
+        xs, ys, zs, ns, mem, keep = self._pack(points)
+        self._keep = (keep, xs, ys, zs, ns)
+        tt = (C.c_float * len(self.scenes))(*[float(v) for v in t])
+        self._keep_t = tt
+        N.check(self._lib.k3dom_batch_update_async(self._h, tt, xs, ys, zs, ns, mem), "k3dom_batch_update_async")
+
+    def synchronize(self) -> None:
+        N.check(self._lib.k3dom_synchronize(self._h), "k3dom_synchronize")
+
+    def autotune(self, on: bool = True) -> None:
+        N.check(self._lib.k3dom_autotune(self._h, 1 if on else 0), "k3dom_autotune")
+
+    def tuning(self) -> dict:
+        t = N.Tuning()
+        N.check(self._lib.k3dom_get_tuning(self._h, C.byref(t)), "k3dom_get_tuning")
+        d = {k: getattr(t, k) for k, _ in t._fields_ if k != "candidate_ms"}
+        d["candidate_ms"] = list(t.candidate_ms)[: t.candidates]
+        return d
+
+    def set_tuning(self, tile_rule: int, chunk: int) -> None:
+        N.check(self._lib.k3dom_set_tuning(self._h, int(tile_rule), int(chunk)), "k3dom_set_tuning")
+
+    def set_timing(self, on: bool) -> None:
+        N.check(self._lib.k3dom_set_timing(self._h, 1 if on else 0), "set_timing")
+
+    def set_graph_mode(self, on: bool) -> None:
+        N.check(self._lib.k3dom_set_graph_mode(self._h, 1 if on else 0), "set_graph_mode")
+
+    def stage_times(self) -> dict:
+        return self.scenes[0].stage_times()
+
+    def diagnostics(self) -> dict:
+        return self.scenes[0].diagnostics()
+
+    def stream(self) -> int:
+        return self.scenes[0].stream()
 
 
 def debug_draws(seed: int, frame: int, stage: int, first: int, count: int) -> np.ndarray:

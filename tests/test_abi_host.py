@@ -35,7 +35,7 @@ def test_library_exports_every_declared_symbol():
 
 def test_abi_version_and_status_strings():
     lib = N.load()
-    assert lib.k3dom_abi_version() == 1
+    assert lib.k3dom_abi_version() == 2
     assert lib.k3dom_status_string(0) == b"ok"
     assert lib.k3dom_status_string(8) == b"non-finite input"
 
