@@ -364,6 +364,8 @@ def run_ours(args):
             },
             "stage_ms": {k: round(v, 4) for k, v in stage.items()},
         }
+        if world == 1 and not args.no_batch:
+            out["batched"] = run_batch(args, local)
         if world == 1 and not args.no_cpu_baseline:
             fps, note, cores, n = cpu_oracle_frames(cfg, args.variant, frames, 1, 0, budget_s=60.0)
             out["cpu_baseline"] = {"value": round(fps, 5), "unit": UNIT, "cores": cores, "kind": "port",
@@ -433,6 +435,122 @@ def run_reference_gpu(args):
                                              "(its own updateGrid, host vectors in, synchronising)"}}), flush=True)
 
 
+def run_batch(args, local: int = 0) -> dict:
+    """Batched form: 16 independent scenes (k3dom_b200.scene.config3) updated together by one
+    BatchDOM (one launch per stage, graph-replayed, evidence tiling autotuned on live frames)
+    against the plain form looping over the same 16 scenes with one DOM each. Aggregate frames/s
+    = scenes x frames / time. Both arms take the same host scans and run synchronous calls (the
+    reference's updateGrid synchronises, src/k3dom/dom.cu:47); time = host clock around the
+    timed frames. The device-resident rows feed the scans from HBM instead."""
+    import torch
+
+    import k3dom_b200 as K
+    from k3dom_b200 import scene
+    cfgs = scene.config3(seed=args.batch_seed, n_scenes=args.scenes, variant=args.variant)
+    S = len(cfgs)
+    W, Kst = 2, args.batch_steps
+    n_frames = 1 + W + Kst
+    log(f"batch: generating {S} x {n_frames} scans ({sum(c.n_points for c in cfgs)} points per frame)")
+    frames = [make_frames(c, n_frames) for c in cfgs]  # frames[s][f] = (t, sensor, pts)
+    params = [K.make_params(args.variant, **c.params) for c in cfgs]
+    dev = f"cuda:{local}"
+    dev_pts = [[torch.from_numpy(fr[2]).to(dev) for fr in frames[s]] for s in range(S)]
+    torch.cuda.synchronize()
+
+    def plain_arm(device_resident: bool) -> float:
+        doms = [K.DOM(p, args.variant, device=local) for p in params]
+        try:
+            def frame(f):
+                for s, d in enumerate(doms):
+                    t, pose, pts = frames[s][f]
+                    d.updatePose(*pose)
+                    if device_resident:
+                        d.updateGridAsync(t, dev_pts[s][f])
+                        d.synchronize()
+                    else:
+                        d.updateGrid(t, pts)
+            for f in range(1 + W):
+                frame(f)
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            for f in range(1 + W, n_frames):
+                frame(f)
+            torch.cuda.synchronize()
+            return S * Kst / (time.perf_counter() - t0)
+        finally:
+            for d in doms:
+                d.close()
+
+    def batch_arm(device_resident: bool):
+        b = K.BatchDOM(params, args.variant, device=local)
+        try:
+            def frame(f, g=None):
+                g = f if g is None else g
+                for s in range(S):
+                    b.updatePose(s, *frames[s][f][1])
+                ts = [frames[s][f][0] for s in range(S)]
+                if device_resident:
+                    b.update_async(ts, [dev_pts[s][g] for s in range(S)])
+                    b.synchronize()
+                else:
+                    b.update(ts, [frames[s][g][2] for s in range(S)])
+            frame(0)
+            # autotune on live frames (replaying frame 1's scans as the clock advances)
+            b.autotune(True)
+            tune_frames = b.tuning()["candidates"]
+            for k in range(tune_frames):
+                for s in range(S):
+                    b.updatePose(s, *frames[s][1][1])
+                ts = [frames[s][1][0] + 0.1 * k for s in range(S)]
+                b.update(ts, [frames[s][1][2] for s in range(S)])
+            tuning = b.tuning()
+            t_shift = 0.1 * tune_frames
+            def timed_frame(f):
+                for s in range(S):
+                    b.updatePose(s, *frames[s][f][1])
+                ts = [frames[s][f][0] + t_shift for s in range(S)]
+                if device_resident:
+                    b.update_async(ts, [dev_pts[s][f] for s in range(S)])
+                    b.synchronize()
+                else:
+                    b.update(ts, [frames[s][f][2] for s in range(S)])
+            for f in range(1, 1 + W):
+                timed_frame(f)
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            for f in range(1 + W, n_frames):
+                timed_frame(f)
+            torch.cuda.synchronize()
+            fps = S * Kst / (time.perf_counter() - t0)
+            launches = b.diagnostics()["kernel_launches_per_frame"]
+            return fps, tuning, launches
+        finally:
+            b.close()
+
+    plain_host = plain_arm(False)
+    plain_dev = plain_arm(True)
+    batch_host, tuning, launches = batch_arm(False)
+    batch_dev, _, _ = batch_arm(True)
+    rules = ["by-size", "8x8x4", "16x16x4", "16x16x8"]
+    return {
+        "workload": f"config3: {S} independent {args.variant} scenes, G 64-256, Gz 16-32, P 2^18-2^22, "
+                    f"B=P/4, 10k-200k points; {Kst} timed frames after {W} warm-up",
+        "scenes": S, "frames": Kst, "unit": "aggregate frames/s",
+        "voxels_total": int(sum(int(np.float32(c.params["size"]) / np.float32(0.1)) ** 2 *
+                                int(np.float32(c.params["size_z"]) / np.float32(0.1)) for c in cfgs)),
+        "particles_total": int(sum(c.params["particle_count"] for c in cfgs)),
+        "points_per_frame_total": int(sum(c.n_points for c in cfgs)),
+        "plain_loop": round(plain_host, 2), "batched": round(batch_host, 2),
+        "speedup": round(batch_host / plain_host, 3),
+        "plain_loop_device_resident": round(plain_dev, 2), "batched_device_resident": round(batch_dev, 2),
+        "speedup_device_resident": round(batch_dev / plain_dev, 3),
+        "batched_launches_per_frame": int(launches),
+        "tuning": {"tile_rule": rules[tuning["tile_rule"]], "chunk": tuning["chunk"],
+                   "candidate_ms": [round(x, 3) for x in tuning["candidate_ms"]]},
+        "timing": "host clock around synchronous calls (both arms), host scans unless device_resident",
+    }
+
+
 def run_profile_case(args):
     """A mid-size scene for ncu captures (state > L2, well under a few GB): 128x128x32 voxels at
     0.1 m, P=1,048,576, B=262,144, 60,000 points; the first frame plus `--steps` frames."""
@@ -463,12 +581,22 @@ def main(argv=None):
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--profile-case", choices=["medium"], default=None,
                     help="run a mid-size scene for profiler captures instead of the benchmark")
+    ap.add_argument("--workload", choices=["frame", "batch"], default="frame",
+                    help="batch: print only the batched-vs-plain line (16 scenes)")
+    ap.add_argument("--no-batch", action="store_true", help="skip the batched-vs-plain measurement")
+    ap.add_argument("--scenes", type=int, default=16)
+    ap.add_argument("--batch-steps", type=int, default=5)
+    ap.add_argument("--batch-seed", type=int, default=0)
     args = ap.parse_args(argv)
     if args.warmup < 3 and args.impl == "ours":
         log("warmup < 3 raised to 3")
         args.warmup = 3
     if args.profile_case:
         run_profile_case(args)
+    elif args.workload == "batch":
+        import torch
+        torch.cuda.set_device(0)
+        print(json.dumps({"metric": "batched vs plain aggregate frames/s", **run_batch(args)}), flush=True)
     elif args.impl == "ours":
         run_ours(args)
     elif args.impl == "reference":

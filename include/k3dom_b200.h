@@ -313,6 +313,9 @@ k3dom_status k3dom_set_tuning(k3dom_handle* h, int32_t tile_rule, int32_t chunk)
 k3dom_status k3dom_exact_prefix_sum_noalloc(const float* in, float* out, int64_t n, void* stream);
 
 const char* k3dom_status_string(k3dom_status s);
+/* The CUDA runtime's message for the last CUDA error a call on this handle met
+ * ("no error" when none). */
+const char* k3dom_last_cuda_error(k3dom_handle* h);
 int32_t k3dom_abi_version(void);
 
 #ifdef __cplusplus

@@ -167,6 +167,7 @@ SIGNATURES = {
     "k3dom_get_tuning": (_ST, [_P, C.POINTER(Tuning)]),
     "k3dom_set_tuning": (_ST, [_P, C.c_int32, C.c_int32]),
     "k3dom_status_string": (C.c_char_p, [C.c_int]),
+    "k3dom_last_cuda_error": (C.c_char_p, [_P]),
     "k3dom_abi_version": (C.c_int32, []),
 }
 
@@ -191,6 +192,8 @@ def load() -> C.CDLL:
     return lib
 
 
-def check(status: int, where: str) -> None:
+def check(status: int, where: str, handle=None) -> None:
     if status != K3DOM_OK:
+        if handle is not None and status == 2:
+            where = f"{where} ({load().k3dom_last_cuda_error(handle).decode()})"
         raise K3domError(status, where)

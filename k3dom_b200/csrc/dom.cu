@@ -64,6 +64,7 @@ struct SceneHost {
     k3dom_params params{};
     DevParams dp{};
     TileShape ts{};
+    float bin_R = 0.0f;
     int max_points = 0;
     // DOM_c host state (include/common/dom.h:135-147)
     bool first_pose_received = false;
@@ -119,6 +120,7 @@ struct k3dom_handle {
     int plan_born_n = 0, plan_joint_n = 0;
     uint32_t *draw_keys = nullptr, *draw_sorted = nullptr, *draw_alt = nullptr;
     uint32_t *hist_draw = nullptr, *scan_tmp_draw = nullptr;
+    long hist_draw_words = 0, scan_draw_words = 0;
     cudaEvent_t ev_staged = nullptr;  // host staging (frame scalars, points) consumed
     int* ancestors = nullptr;
     float* pts = nullptr;  // device x | y | z, N slots each
@@ -308,7 +310,7 @@ cudaError_t layout_points_tiles(k3dom_handle* h) {
     std::vector<SceneDev> sd(h->S);
     std::vector<float4> tabs((size_t)h->S * kKernelTableSize);
     for (int s = 0; s < h->S; ++s) {
-        const SceneHost& x = h->sc[s];
+        SceneHost& x = h->sc[s];
         SceneDev& d = sd[s];
         std::memset(&d, 0, sizeof(d));
         d.p = x.dp;
@@ -322,6 +324,7 @@ cudaError_t layout_points_tiles(k3dom_handle* h) {
         d.n_tiles = h->off.tile[s + 1] - h->off.tile[s];
         d.max_points = x.max_points;
         fill_scene_evidence(d, h->ds(), tabs.data() + (size_t)s * kKernelTableSize);
+        x.bin_R = d.bin_R;
     }
     cudaError_t e;
     if ((e = cudaMemcpy(h->sc_dev, sd.data(), sizeof(SceneDev) * sd.size(), cudaMemcpyHostToDevice))) return e;
@@ -342,7 +345,8 @@ cudaError_t alloc_ray_buffers(k3dom_handle* h) {
     if ((e = h->alloc(&rb.ktab, (size_t)h->S * kKernelTableSize, true, L))) return e;
     if ((e = layout_points_tiles(h))) return e;
     long cap = 0;
-    for (int s = 0; s < h->S; ++s) cap += ray_entries_bound(h->sc[s].dp, h->sc[s].ts, h->sc[s].max_points);
+    for (int s = 0; s < h->S; ++s)
+        cap += ray_entries_bound(h->sc[s].dp, h->sc[s].ts, h->sc[s].max_points, h->sc[s].bin_R);
     cap = std::max(cap, 4096L);
     if (cap > 0xFFFFFFF0L) cap = 0xFFFFFFF0L;
     rb.capacity = cap;
@@ -380,6 +384,8 @@ cudaError_t alloc_ray_buffers(k3dom_handle* h) {
     h->scan_tmp_words = sw;
     rb.hist = h->hist;
     rb.scan_tmp = h->scan_tmp;
+    rb.hist_words = h->hist_words;
+    rb.scan_words = h->scan_tmp_words;
     if ((e = h->alloc(&h->pts, 3 * (size_t)N, true, L))) return e;
     if ((e = cudaMallocHost((void**)&h->pts_pinned, 3 * (size_t)N * sizeof(float)))) return e;
     return cudaSuccess;
@@ -523,7 +529,8 @@ cudaError_t enq_predict(k3dom_handle* h) {
 
 cudaError_t enq_assign(k3dom_handle* h) {
     cudaError_t e = radix_sort_pairs(reinterpret_cast<const uint32_t*>(h->A.cell), nullptr, h->sorted_keys, h->perm,
-                                     h->alt_k, h->alt_v, h->P, key_bits_for(h->C), h->hist, h->scan_tmp, h->st);
+                                     h->alt_k, h->alt_v, h->P, key_bits_for(h->C), h->hist, h->hist_words,
+                                     h->scan_tmp, h->scan_tmp_words, h->st);
     if (e != cudaSuccess) return e;
     if ((e = cudaMemsetAsync(h->cw.start, 0xFF, sizeof(int) * (size_t)h->C, h->st))) return e;
     if ((e = cudaMemsetAsync(h->cw.end, 0xFF, sizeof(int) * (size_t)h->C, h->st))) return e;
@@ -557,7 +564,8 @@ cudaError_t enq_births(k3dom_handle* h) {
 cudaError_t enq_draws(k3dom_handle* h, cudaStream_t s) {
     launch_draw_keys(h->batch(), h->draw_keys, s);
     return radix_sort_pairs(h->draw_keys, nullptr, h->draw_sorted, nullptr, h->draw_alt, nullptr, h->P,
-                            draw_key_bits(h->S), h->hist_draw, h->scan_tmp_draw, s);
+                            draw_key_bits(h->S), h->hist_draw, h->hist_draw_words, h->scan_tmp_draw,
+                            h->scan_draw_words, s);
 }
 
 cudaError_t enq_resample(k3dom_handle* h, bool draws_ready) {
@@ -667,6 +675,11 @@ const char* k3dom_status_string(k3dom_status s) {
 }
 
 int32_t k3dom_abi_version(void) { return K3DOM_B200_ABI_VERSION; }
+
+const char* k3dom_last_cuda_error(k3dom_handle* h) {
+    if (!h) return "no handle";
+    return cudaGetErrorString(h->last_error);
+}
 
 k3dom_status k3dom_batch_create(const k3dom_params* params, int32_t n_scenes, k3dom_variant variant, int device,
                                 k3dom_handle** out) {
@@ -787,11 +800,14 @@ k3dom_status k3dom_batch_create(const k3dom_params* params, int32_t n_scenes, k3
     }
     if ((e = h->alloc(&h->draw_keys, P)) || (e = h->alloc(&h->draw_sorted, P)) || (e = h->alloc(&h->draw_alt, P)))
         return bail(e);
-    // separate sort scratch for the draw sort (it runs concurrently on the second stream)
+    // separate sort scratch for the draw sort (it runs concurrently on the second stream); the
+    // draw keys carry the scene index above 24 bits, so passes may be up to 11 bits wide
     {
-        const long hw = radix_hist_words(P, 8);
+        const long hw = radix_hist_words(P, 11);
+        h->hist_draw_words = hw;
+        h->scan_draw_words = scan_u32_tiles(hw) + 16;
         if ((e = h->alloc(&h->hist_draw, hw))) return bail(e);
-        if ((e = h->alloc(&h->scan_tmp_draw, scan_u32_tiles(hw) + 16))) return bail(e);
+        if ((e = h->alloc(&h->scan_tmp_draw, h->scan_draw_words))) return bail(e);
     }
     if ((e = alloc_ray_buffers(h))) return bail(e);
     // DOM_c::initialize (src/common/dom.cu:90-109): cells to priors

@@ -333,15 +333,19 @@ void fill_scene_evidence(SceneDev& sd, bool ds, float4* ktab) {
     if (ktab) build_kernel_table(p.sigma, std::ldexp(1.0, sh), ktab);
 }
 
-long ray_entries_bound(const DevParams& p, const TileShape& ts, int max_points) {
-    const double R = std::max((double)p.ls, (double)p.window_radius * 1.5 + 0.05) / p.res + 2.0;
+// Worst case of tiles one ray can reach: for each slab of tiles along the ray's dominant axis A,
+// the segment clipped to the slab grown by R spans at most ts[A] - 1 + 2R cells along every
+// axis (|d_o| <= |d_A|), and the tiles within R of it along axis o number at most
+// ceil((ts[A] + 4R) / ts[o]) + 1. Times the slabs, for the worst axis.
+long ray_entries_bound(const DevParams& p, const TileShape& ts, int max_points, float bin_R) {
+    const double R = (double)bin_R + 0.01;
     const int tsz[3] = {ts.tx, ts.ty, ts.tz}, nt[3] = {ts.ntx, ts.nty, ts.ntz};
     long worst = 0;
     for (int A = 0; A < 3; ++A) {
         long per_slab = 1;
         for (int k = 1; k <= 2; ++k) {
             const int o = (A + k) % 3;
-            const long n = (long)std::ceil((tsz[A] + 4.0 * R + 2.0) / tsz[o]) + 2;
+            const long n = (long)std::ceil((tsz[A] + 4.0 * R) / tsz[o]) + 1;
             per_slab *= std::min<long>(n, nt[o]);
         }
         worst = std::max(worst, per_slab * nt[A]);
@@ -364,7 +368,7 @@ cudaError_t build_ray_lists(const Batch& bt, const float* xs, const float* ys, c
     int bits = 1;
     while ((1 << bits) < T + 1) ++bits;
     e = radix_sort_pairs_dn(rb.ekeys, rb.evals, rb.ekeys2, rb.evals2, rb.ekeys_alt, rb.evals_alt, rb.capacity,
-                            rb.total + 2, bits, rb.hist, rb.scan_tmp, st);
+                            rb.total + 2, bits, rb.hist, rb.hist_words, rb.scan_tmp, rb.scan_words, st);
     if (e != cudaSuccess) return e;
     ++g_launches;
     k_tile_start<<<div_up(T + 1, kBlock), kBlock, 0, st>>>(rb.ekeys2, rb.total, T, rb.tile_start);

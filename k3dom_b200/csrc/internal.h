@@ -23,13 +23,16 @@ cudaError_t scan_u32_exclusive_dn(const uint32_t* in, uint32_t* out, long nmax, 
 int radix_tiles(long n);
 long radix_hist_words(long n, int max_bits);
 int radix_plan(int key_bits, int* pass_bits);
+// hist_words / scan_words are the capacities of hist and scan_tmp (radix_hist_words(n, 11) and
+// scan_u32_tiles of it suffice for any key width); too small a buffer is refused.
 cudaError_t radix_sort_pairs(const uint32_t* keys, const uint32_t* vals, uint32_t* keys_out,
                              uint32_t* vals_out, uint32_t* alt_k, uint32_t* alt_v, long n,
-                             int key_bits, uint32_t* hist, uint32_t* scan_tmp, cudaStream_t st);
+                             int key_bits, uint32_t* hist, long hist_words, uint32_t* scan_tmp,
+                             long scan_words, cudaStream_t st);
 cudaError_t radix_sort_pairs_dn(const uint32_t* keys, const uint32_t* vals, uint32_t* keys_out,
                                 uint32_t* vals_out, uint32_t* alt_k, uint32_t* alt_v, long nmax,
-                                const uint32_t* dn, int key_bits, uint32_t* hist,
-                                uint32_t* scan_tmp, cudaStream_t st);
+                                const uint32_t* dn, int key_bits, uint32_t* hist, long hist_words,
+                                uint32_t* scan_tmp, long scan_words, cudaStream_t st);
 cudaError_t sort_init();
 
 // exactscan.cu: inclusive prefix sums of non-negative floats, exact in 128-bit fixed
@@ -106,12 +109,13 @@ struct RayBuffers {
     uint8_t* ds_counts;    // DS: per (item, cell) neighbour counts of pass 1
     uint32_t* hist;
     uint32_t* scan_tmp;
+    long hist_words, scan_words;
     uint32_t* total;       // [0] = entries, [2] = entries kept (0 on overflow)
     long capacity;         // entries
     long ds_count_capacity;
     int chunk;             // rays per work item
 };
-long ray_entries_bound(const DevParams& p, const TileShape& ts, int max_points);
+long ray_entries_bound(const DevParams& p, const TileShape& ts, int max_points, float bin_R);
 // Per-scene evidence constants (binning radius, cull radius, fixed-point scale); writes the
 // scene's kernel table when ktab is not null.
 void fill_scene_evidence(SceneDev& sd, bool ds, float4* ktab);

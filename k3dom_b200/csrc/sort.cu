@@ -310,13 +310,20 @@ int radix_plan(int key_bits, int* pass_bits) {
 // Stable sort by the low key_bits bits. The result lands in keys_out / vals_out; alt_k /
 // alt_v are ping-pong buffers (unused for a single pass). vals == nullptr sorts an
 // identity payload (argsort); vals_out == nullptr sorts keys only.
+// hist_words / scan_words: capacity of hist and scan_tmp; a call whose passes would need more
+// is refused (cudaErrorInvalidValue) before anything is launched.
 cudaError_t radix_sort_pairs_dn(const uint32_t* keys, const uint32_t* vals, uint32_t* keys_out,
                                 uint32_t* vals_out, uint32_t* alt_k, uint32_t* alt_v, long nmax,
-                                const uint32_t* dn, int key_bits, uint32_t* hist, uint32_t* scan_tmp,
-                                cudaStream_t st) {
+                                const uint32_t* dn, int key_bits, uint32_t* hist, long hist_words,
+                                uint32_t* scan_tmp, long scan_words, cudaStream_t st) {
     if (nmax <= 0) return cudaSuccess;
     int pb[4];
     const int np = radix_plan(key_bits, pb);
+    for (int p = 0; p < np; ++p) {
+        const int tb = pb[p] <= 8 ? 8 : (pb[p] <= 10 ? 10 : 11);  // template width of the pass
+        const long hn = (long)radix_tiles(nmax) << tb;
+        if (hn + 1 > hist_words || scan_u32_tiles(hn) > scan_words) return cudaErrorInvalidValue;
+    }
     const uint32_t* ck = keys;
     const uint32_t* cv = vals;
     int shift = 0;
@@ -335,9 +342,9 @@ cudaError_t radix_sort_pairs_dn(const uint32_t* keys, const uint32_t* vals, uint
 
 cudaError_t radix_sort_pairs(const uint32_t* keys, const uint32_t* vals, uint32_t* keys_out, uint32_t* vals_out,
                              uint32_t* alt_k, uint32_t* alt_v, long n, int key_bits, uint32_t* hist,
-                             uint32_t* scan_tmp, cudaStream_t st) {
-    return radix_sort_pairs_dn(keys, vals, keys_out, vals_out, alt_k, alt_v, n, nullptr, key_bits, hist, scan_tmp,
-                               st);
+                             long hist_words, uint32_t* scan_tmp, long scan_words, cudaStream_t st) {
+    return radix_sort_pairs_dn(keys, vals, keys_out, vals_out, alt_k, alt_v, n, nullptr, key_bits, hist, hist_words,
+                               scan_tmp, scan_words, st);
 }
 
 }  // namespace k3dom

@@ -163,15 +163,16 @@ class DOM:
 
     def updateGrid(self, t: float, xs, ys=None, zs=None) -> None:
         px, py, pz, n, mem, _keep = self._points(xs, ys, zs)
-        N.check(self._lib.k3dom_update_grid(self._h, float(t), px, py, pz, n, mem), "k3dom_update_grid")
+        N.check(self._lib.k3dom_update_grid(self._h, float(t), px, py, pz, n, mem), "k3dom_update_grid", self._h)
 
     def updateGridAsync(self, t: float, xs, ys=None, zs=None) -> None:
         px, py, pz, n, mem, keep = self._points(xs, ys, zs)
         self._keep = keep
-        N.check(self._lib.k3dom_update_grid_async(self._h, float(t), px, py, pz, n, mem), "k3dom_update_grid_async")
+        N.check(self._lib.k3dom_update_grid_async(self._h, float(t), px, py, pz, n, mem), "k3dom_update_grid_async",
+                self._h)
 
     def synchronize(self) -> None:
-        N.check(self._lib.k3dom_synchronize(self._h), "k3dom_synchronize")
+        N.check(self._lib.k3dom_synchronize(self._h), "k3dom_synchronize", self._h)
 
     update_pose = updatePose
     update_grid = updateGrid
@@ -415,17 +416,18 @@ class BatchDOM:
         """One frame of every scene: t[s] and points[s] ((n, 3) or (xs, ys, zs))."""
         xs, ys, zs, ns, mem, _keep = self._pack(points)
         tt = (C.c_float * len(self.scenes))(*[float(v) for v in t])
-        N.check(self._lib.k3dom_batch_update(self._h, tt, xs, ys, zs, ns, mem), "k3dom_batch_update")
+        N.check(self._lib.k3dom_batch_update(self._h, tt, xs, ys, zs, ns, mem), "k3dom_batch_update", self._h)
 
     def update_async(self, t, points) -> None:
         xs, ys, zs, ns, mem, keep = self._pack(points)
         self._keep = (keep, xs, ys, zs, ns)
         tt = (C.c_float * len(self.scenes))(*[float(v) for v in t])
         self._keep_t = tt
-        N.check(self._lib.k3dom_batch_update_async(self._h, tt, xs, ys, zs, ns, mem), "k3dom_batch_update_async")
+        N.check(self._lib.k3dom_batch_update_async(self._h, tt, xs, ys, zs, ns, mem), "k3dom_batch_update_async",
+                self._h)
 
     def synchronize(self) -> None:
-        N.check(self._lib.k3dom_synchronize(self._h), "k3dom_synchronize")
+        N.check(self._lib.k3dom_synchronize(self._h), "k3dom_synchronize", self._h)
 
     def autotune(self, on: bool = True) -> None:
         N.check(self._lib.k3dom_autotune(self._h, 1 if on else 0), "k3dom_autotune")

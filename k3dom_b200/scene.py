@@ -13,6 +13,10 @@ The named configurations mirror the benchmark configurations of this project:
   config1: 256x256x32 @ 0.1 m, P=4194304, B=1048576, 64-beam scans of 120000 returns,
            ego motion 0-2 m/s, 20 static + 20 moving cuboids at 0-3 m/s, 10 Hz.
   config2: config1's shape with the DS-PHD/MIB variant.
+  config3: 16 independent scenes for the batched update, per-scene seeds: grids G x G x Gz at
+           0.1 m with G uniform in 64..256 and Gz in 16..32, P = 2^u with u uniform in [18, 22],
+           B = P / 4, 10,000-200,000 points per scan; contents as config1 (20 static + 20 moving
+           cuboids, ego motion 0-2 m/s) scaled to each grid.
 """
 from __future__ import annotations
 
@@ -146,6 +150,25 @@ def config1(seed: int = 0, variant: str = "k3dom") -> Config:
 
 def config2(seed: int = 0) -> Config:
     return config1(seed, "dsphdmib")
+
+
+def config3(seed: int = 0, n_scenes: int = 16, variant: str = "k3dom") -> list:
+    rng = np.random.Generator(np.random.PCG64([seed, 3]))
+    out = []
+    for k in range(n_scenes):
+        G = int(rng.integers(64, 257))
+        Gz = int(rng.integers(16, 33))
+        P = int(round(2.0 ** rng.uniform(18.0, 22.0)))
+        B = max(1, P // 4)
+        n = int(rng.integers(10000, 200001))
+        res = 0.1
+        size, size_z = G * res, Gz * res
+        sc = Scene(seed=seed * 1000 + k, n_static=20, n_moving=20, side=(1.0, 2.0), speed=(0.0, 3.0),
+                   ego_speed=(0.0, 2.0), extent=max(2.0, size / 2 - 1.5), ground_z=-1.5, max_range=size,
+                   beams=64, range_noise=0.02)
+        params = _k3dom_params(size, size_z, res, P, B, variant=variant, seed=5000 + k, max_points=n)
+        out.append(Config(f"config3[{k}]", variant, params, sc, n, 100, 0.1))
+    return out
 
 
 def small(seed: int = 0, variant: str = "k3dom", G: int = 32, Gz: int = 8, res: float = 0.2, P: int = 16384,
