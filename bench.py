@@ -366,6 +366,8 @@ def run_ours(args):
         }
         if world == 1 and not args.no_batch:
             out["batched"] = run_batch(args, local)
+        if world == 1 and not args.no_grad:
+            out["grad_step"] = run_grad_step(args, local, frame_ms=ms_max)
         if world == 1 and not args.no_cpu_baseline:
             fps, note, cores, n = cpu_oracle_frames(cfg, args.variant, frames, 1, 0, budget_s=60.0)
             out["cpu_baseline"] = {"value": round(fps, 5), "unit": UNIT, "cores": cores, "kind": "port",
@@ -551,6 +553,57 @@ def run_batch(args, local: int = 0) -> dict:
     }
 
 
+def run_grad_step(args, local: int = 0, frame_ms: float | None = None) -> dict:
+    """Differentiable update (config4 scaled to config1's grid): one gradient step is
+    k3dom_bgki_backward (kernel and derivative sums of both training frames, the mass recursion,
+    the loss and its hand-written adjoint); the forward is k3dom_bgki_forward. The length-scale
+    changes every call, so the sums are recomputed each time, as in a calibration loop. Device
+    time between CUDA events on the problem's stream (the calls synchronise inside)."""
+    import torch
+
+    from k3dom_b200 import calib, scene
+    cfg = scene.config4(seed=0, scale="config1")
+    pr = calib.build_problem(cfg, device=local)
+    try:
+        stream = torch.cuda.ExternalStream(pr.calib.stream())
+        th = np.array(pr.theta0, np.float64)
+
+        def timed(fn, n):
+            ms = []
+            for i in range(n):
+                t = th.copy()
+                t[0] = th[0] * (1.0 + 1e-4 * (i % 7 + 1))
+                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                e0.record(stream)
+                fn(t)
+                e1.record(stream)
+                e1.synchronize()
+                ms.append(e0.elapsed_time(e1))
+            return float(np.median(ms))
+        for _ in range(3):
+            pr.calib.loss_and_grad(th)
+        fwd = timed(pr.calib.loss, 10)
+        step = timed(pr.calib.loss_and_grad, 10)
+        loss, g = pr.calib.loss_and_grad(th)
+        n0, n1 = pr.calib.label_counts()
+        out = {
+            "workload": "config4 scaled to config1: 256x256x32 grid @0.1 m, 2 training frames of 120,000 points "
+                        "(initialisation + one update with the particle filter's weights), 10 held-out scans "
+                        "of 120,000 points; theta = (ls 0.3 m, sigma 1.0, gamma 0.1, occupied prior 0.01, free "
+                        "prior 0.01)",
+            "forward_ms": round(fwd, 3), "grad_step_ms": round(step, 3),
+            "step_over_forward": round(step / fwd, 3),
+            "label_instances": int(n0.sum() + n1.sum()), "loss": round(float(loss), 6),
+            "grad": [float(f"{v:.6g}") for v in g],
+            "timing": "CUDA events on the problem's stream, median of 10, ls perturbed every call",
+        }
+        if frame_ms:
+            out["step_over_plain_frame"] = round(step / frame_ms, 3)
+        return out
+    finally:
+        pr.close()
+
+
 def run_profile_case(args):
     """A mid-size scene for ncu captures (state > L2, well under a few GB): 128x128x32 voxels at
     0.1 m, P=1,048,576, B=262,144, 60,000 points; the first frame plus `--steps` frames."""
@@ -581,9 +634,10 @@ def main(argv=None):
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--profile-case", choices=["medium"], default=None,
                     help="run a mid-size scene for profiler captures instead of the benchmark")
-    ap.add_argument("--workload", choices=["frame", "batch"], default="frame",
-                    help="batch: print only the batched-vs-plain line (16 scenes)")
+    ap.add_argument("--workload", choices=["frame", "batch", "grad"], default="frame",
+                    help="batch: only the batched-vs-plain line (16 scenes); grad: only the gradient step")
     ap.add_argument("--no-batch", action="store_true", help="skip the batched-vs-plain measurement")
+    ap.add_argument("--no-grad", action="store_true", help="skip the gradient-step measurement")
     ap.add_argument("--scenes", type=int, default=16)
     ap.add_argument("--batch-steps", type=int, default=5)
     ap.add_argument("--batch-seed", type=int, default=0)
@@ -597,6 +651,10 @@ def main(argv=None):
         import torch
         torch.cuda.set_device(0)
         print(json.dumps({"metric": "batched vs plain aggregate frames/s", **run_batch(args)}), flush=True)
+    elif args.workload == "grad":
+        import torch
+        torch.cuda.set_device(0)
+        print(json.dumps({"metric": "gradient step ms", **run_grad_step(args)}), flush=True)
     elif args.impl == "ours":
         run_ours(args)
     elif args.impl == "reference":

@@ -303,6 +303,43 @@ k3dom_status k3dom_autotune(k3dom_handle* h, int enabled);
 k3dom_status k3dom_get_tuning(k3dom_handle* h, k3dom_tuning* out);
 k3dom_status k3dom_set_tuning(k3dom_handle* h, int32_t tile_rule, int32_t chunk);
 
+/* ---- the differentiable kernel-inference update (calibration) ----
+ * No counterpart in the reference. A calibration problem holds a grid (from `base`), training
+ * frames (points, sensor pose, dt; frame 0 initialises with dt = 0, later frames may carry the
+ * particle weight sum of every cell, which is treated as data: sort and resampling are not
+ * differentiated) and held-out scans, whose rays are traversed by 3-D DDA into per-cell label
+ * counts (hit voxel: label 1; voxels traversed before it: label 0).
+ * theta[5] = { kernel length-scale ls [m], kernel amplitude sigma, free-space decay gamma
+ * (pred_total = (free + dynamic) * gamma^dt, mass_update.cu:166), occupied prior mass (split
+ * evenly into the static and dynamic priors), free prior mass }.
+ * Loss = mean binary cross-entropy between the occupancy (static + dynamic) / total after the
+ * last frame (clamped to [1e-7, 1 - 1e-7]) and the labels, over all label instances.
+ * Points are sensor-relative xyz triples (n x 3, interleaved); the sensor position is relative
+ * to the grid centre. */
+typedef struct k3dom_calib k3dom_calib;
+k3dom_status k3dom_calib_create(const k3dom_params* base, int device, k3dom_calib** out);
+k3dom_status k3dom_calib_destroy(k3dom_calib* c);
+/* dyn_pred: grid_cell_count floats (NULL: no particles); ignored for frame 0. */
+k3dom_status k3dom_calib_add_frame(k3dom_calib* c, float dt, float sensor_x, float sensor_y,
+                                   float sensor_z, const float* xyz, int32_t n,
+                                   const float* dyn_pred, k3dom_mem mem);
+k3dom_status k3dom_calib_add_heldout_scan(k3dom_calib* c, float sensor_x, float sensor_y,
+                                          float sensor_z, const float* xyz, int32_t n,
+                                          k3dom_mem mem);
+k3dom_status k3dom_calib_label_counts(k3dom_calib* c, uint32_t* n0, uint32_t* n1, k3dom_mem mem);
+/* Per-cell sums of frame `frame` at length-scale ls: 4 x grid_cell_count doubles
+ * (sum f occupied, sum f free, sum -x f'(x) occupied, sum -x f'(x) free; x = d / ls). */
+k3dom_status k3dom_calib_get_sums(k3dom_calib* c, float ls, int32_t frame, double* out, k3dom_mem mem);
+k3dom_status k3dom_calib_info(k3dom_calib* c, int32_t* cells, int32_t* frames,
+                              double* label_instances);
+k3dom_status k3dom_calib_get_stream(k3dom_calib* c, void** stream);
+/* Loss at theta; occupancy (grid_cell_count floats, may be NULL) receives p(c). */
+k3dom_status k3dom_bgki_forward(k3dom_calib* c, const float* theta, float* loss, float* occupancy,
+                                k3dom_mem mem);
+/* grad_theta[i] = grad_loss * dLoss/dtheta[i] by the hand-written adjoint; loss may be NULL. */
+k3dom_status k3dom_bgki_backward(k3dom_calib* c, const float* theta, float grad_loss,
+                                 float* grad_theta, float* loss);
+
 /* Exact inclusive prefix sum of n non-negative floats (device pointers in/out, enqueued on
  * `stream`, a cudaStream_t or NULL) that allocates no memory: its scratch is a fixed 256 KiB
  * array inside the library on each GPU. For callers that may not allocate device memory at

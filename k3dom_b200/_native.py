@@ -166,6 +166,16 @@ SIGNATURES = {
     "k3dom_autotune": (_ST, [_P, C.c_int]),
     "k3dom_get_tuning": (_ST, [_P, C.POINTER(Tuning)]),
     "k3dom_set_tuning": (_ST, [_P, C.c_int32, C.c_int32]),
+    "k3dom_calib_create": (_ST, [C.POINTER(Params), C.c_int, C.POINTER(_P)]),
+    "k3dom_calib_destroy": (_ST, [_P]),
+    "k3dom_calib_add_frame": (_ST, [_P, C.c_float, C.c_float, C.c_float, C.c_float, _P, C.c_int32, _P, C.c_int]),
+    "k3dom_calib_add_heldout_scan": (_ST, [_P, C.c_float, C.c_float, C.c_float, _P, C.c_int32, C.c_int]),
+    "k3dom_calib_label_counts": (_ST, [_P, _P, _P, C.c_int]),
+    "k3dom_calib_get_sums": (_ST, [_P, C.c_float, C.c_int32, _P, C.c_int]),
+    "k3dom_calib_info": (_ST, [_P, C.POINTER(C.c_int32), C.POINTER(C.c_int32), C.POINTER(C.c_double)]),
+    "k3dom_calib_get_stream": (_ST, [_P, C.POINTER(_P)]),
+    "k3dom_bgki_forward": (_ST, [_P, _F, _F, _P, C.c_int]),
+    "k3dom_bgki_backward": (_ST, [_P, _F, C.c_float, _F, _F]),
     "k3dom_status_string": (C.c_char_p, [C.c_int]),
     "k3dom_last_cuda_error": (C.c_char_p, [_P]),
     "k3dom_abi_version": (C.c_int32, []),

@@ -1,0 +1,835 @@
+// calib.cu -- the differentiable kernel-inference update: a calibration loss over held-out rays
+// and its hand-written adjoint with respect to the kernel length-scale, the kernel amplitude,
+// the free-space decay and the prior masses.
+//
+// Forward, per cell c (the K3DOM cell update of src/k3dom/kernel/mass_update.cu:79-183, in FP64):
+//   frame 0: masses start at the priors (free = theta_free, static = dynamic = theta_occ / 2), are
+//            predicted with dt = 0 and no particles, and updated with the BGKI evidence
+//            E = sigma * sum f(d / ls) of the frame's scan (occupied and free parts);
+//   frame k: predicted with gamma^dt_k and the frame's particle weight sum (given, not
+//            differentiated: sort and resampling are not differentiable), then updated;
+//   p(c) = (static + dynamic) / (free + static + dynamic) after the last frame.
+// Loss = mean over held-out label instances of the binary cross-entropy of p(c) (p clamped to
+// [1e-7, 1 - 1e-7]); labels come from 3-D DDA along each held-out ray: 1 for the voxel holding
+// the hit, 0 for the voxels traversed before it.
+//
+// The free-space decay of the calibration is the reference's gamma (the only decay on free mass,
+// pred_total = (free + dynamic) gamma^dt, mass_update.cu:166). The occupied prior is split
+// evenly between the static and dynamic prior masses.
+//
+// Gradient: the evidence enters only through per-cell sums F = sum f(x) and H = sum -x f'(x)
+// (x = d / ls), formed by one BGKI pass per frame (k_bgki_sums, exact fixed point, no per-pair
+// storage): dE/dsigma = F, dE/dls = sigma H / ls. The backward recomputes each cell's mass
+// recursion and runs it in reverse (frame_adjoint), then reduces sum_c dL/dE * dE/dtheta over the
+// cells; nothing per point and nothing per frame intermediate is kept between the passes.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <new>
+#include <vector>
+
+#include "../../include/k3dom_b200.h"
+#include "common.cuh"
+#include "internal.h"
+
+using namespace k3dom;
+
+namespace {
+
+constexpr int kMaxCalibFrames = 16;
+constexpr double kPClamp = 1e-7;
+
+// ---------------------------------------------------------------- per-cell mass recursion
+__host__ __device__ inline double credit(double x, double ms) { return 1.0 - 2.0 / (1.0 + exp(2.0 * x / ms)); }
+// d credit / dx = (4 / ms) e / (1 + e)^2 with e = exp(2x / ms), written with t = exp(-|2x / ms|)
+// (the same value, e / (1 + e)^2 = t / (1 + t)^2) so that it cannot overflow to inf / inf.
+__host__ __device__ inline double credit_d(double x, double ms) {
+    const double t = exp(-fabs(2.0 * x / ms));
+    return (4.0 / ms) * t / ((1.0 + t) * (1.0 + t));
+}
+
+struct FrameIn {
+    double mf, ms, md;  // masses entering the frame (before prediction)
+    double g;           // gamma^dt
+    double dyn;         // particle weight sum of the cell (0 without particles)
+    double Eo, Ef;      // evidence
+};
+
+// The frame's prediction and update (mass_update.cu:79-139), FP64.
+__device__ inline void frame_forward(const FrameIn& in, double mass_scale, double* f3, double* s3, double* d3) {
+    const double P = (in.mf + in.md) * in.g;
+    const double s1 = in.ms * in.g;
+    const double d1 = fmin(in.dyn, fmax(0.0, P - s1));
+    const double f1 = P - d1;
+    if (!(in.Ef > 0.0 || in.Eo > 0.0)) {
+        *f3 = f1; *s3 = s1; *d3 = d1;
+        return;
+    }
+    const double Sd = in.Ef + in.Eo;
+    const double Sp = f1 + s1 + d1;
+    double lDF = 0.0, lSFD = 0.0, lFD = 0.0;
+    if (Sp > 0.0) {
+        const double cr = credit(sqrt(Sd * Sp), mass_scale);
+        const double bf = cr * fmax(0.0, in.Ef - in.Eo) / Sd;
+        const double bo = cr * fmax(0.0, in.Eo - in.Ef) / Sd;
+        lDF = bf * d1 / Sp;
+        lSFD = bf * fmax(0.0, s1 + d1 - f1) / Sp;
+        lFD = bo * fmax(0.0, f1 - s1 - d1) / Sp;
+    }
+    const double f2 = f1 + lSFD / 2.0 * s1 + lDF * d1 - lFD * f1;
+    const double s2 = s1 - lSFD * s1;
+    const double d2 = d1 + lFD * f1 + lSFD / 2.0 * s1 - lDF * d1;
+    const double cr2 = credit(s2 + d2, mass_scale);
+    const double r = (s2 <= 0.0 || d2 < 0.0) ? 0.0 : 1.0 / (1.0 + d2 / s2);
+    const double beta = (1.0 - cr2) + cr2 * r;
+    *s3 = s2 + beta * in.Eo;
+    *d3 = d2 + (1.0 - beta) * in.Eo;
+    *f3 = f2 + in.Ef;
+}
+
+struct FrameBar {
+    double mf, ms, md, g, Eo, Ef;
+};
+
+// Reverse mode of frame_forward: adjoints of the outputs (F3, S3, D3) -> adjoints of the inputs.
+// Piecewise branches (min, max, the update condition, the ratio's guard) take the derivative of
+// the branch the forward took.
+__device__ inline FrameBar frame_adjoint(const FrameIn& in, double mass_scale, double F3, double S3, double D3) {
+    FrameBar b = {0, 0, 0, 0, 0, 0};
+    // forward recomputation
+    const double P = (in.mf + in.md) * in.g;
+    const double s1 = in.ms * in.g;
+    const double t = P - s1;
+    const double u = fmax(0.0, t);
+    const bool d_is_dyn = in.dyn < u;
+    const double d1 = d_is_dyn ? in.dyn : u;
+    const double f1 = P - d1;
+    double f1b = 0.0, s1b = 0.0, d1b = 0.0;
+    if (!(in.Ef > 0.0 || in.Eo > 0.0)) {
+        f1b = F3; s1b = S3; d1b = D3;
+    } else {
+        const double Sd = in.Ef + in.Eo;
+        const double Sp = f1 + s1 + d1;
+        double lDF = 0.0, lSFD = 0.0, lFD = 0.0, cr = 0.0, bf = 0.0, bo = 0.0, X = 0.0;
+        const double pf = fmax(0.0, in.Ef - in.Eo), po = fmax(0.0, in.Eo - in.Ef);
+        const double q1 = fmax(0.0, s1 + d1 - f1), q2 = fmax(0.0, f1 - s1 - d1);
+        if (Sp > 0.0) {
+            X = sqrt(Sd * Sp);
+            cr = credit(X, mass_scale);
+            bf = cr * pf / Sd;
+            bo = cr * po / Sd;
+            lDF = bf * d1 / Sp;
+            lSFD = bf * q1 / Sp;
+            lFD = bo * q2 / Sp;
+        }
+        const double f2 = f1 + lSFD / 2.0 * s1 + lDF * d1 - lFD * f1;
+        const double s2 = s1 - lSFD * s1;
+        const double d2 = d1 + lFD * f1 + lSFD / 2.0 * s1 - lDF * d1;
+        (void)f2;
+        const double y = s2 + d2;
+        const double cr2 = credit(y, mass_scale);
+        const bool r_on = !(s2 <= 0.0 || d2 < 0.0);
+        const double r = r_on ? 1.0 / (1.0 + d2 / s2) : 0.0;
+        const double beta = (1.0 - cr2) + cr2 * r;
+        // reverse
+        double f2b = F3, s2b = S3, d2b = D3;
+        b.Ef += F3;
+        const double betab = in.Eo * (S3 - D3);
+        b.Eo += S3 * beta + D3 * (1.0 - beta);
+        const double cr2b = betab * (r - 1.0);
+        const double rb = betab * cr2;
+        const double yb = cr2b * credit_d(y, mass_scale);
+        s2b += yb;
+        d2b += yb;
+        if (r_on) {
+            const double den = (s2 + d2) * (s2 + d2);
+            s2b += rb * d2 / den;
+            d2b += -rb * s2 / den;
+        }
+        double lSFDb = 0.0, lDFb = 0.0, lFDb = 0.0;
+        // f2 = f1 + lSFD/2 s1 + lDF d1 - lFD f1
+        f1b += f2b * (1.0 - lFD);
+        s1b += f2b * lSFD / 2.0;
+        d1b += f2b * lDF;
+        lSFDb += f2b * s1 / 2.0;
+        lDFb += f2b * d1;
+        lFDb += -f2b * f1;
+        // s2 = s1 - lSFD s1
+        s1b += s2b * (1.0 - lSFD);
+        lSFDb += -s2b * s1;
+        // d2 = d1 + lFD f1 + lSFD/2 s1 - lDF d1
+        d1b += d2b * (1.0 - lDF);
+        f1b += d2b * lFD;
+        s1b += d2b * lSFD / 2.0;
+        lFDb += d2b * f1;
+        lSFDb += d2b * s1 / 2.0;
+        lDFb += -d2b * d1;
+        if (Sp > 0.0) {
+            double bfb = 0.0, bob = 0.0, Spb = 0.0, Sdb = 0.0, q1b = 0.0, q2b = 0.0;
+            bfb += lDFb * d1 / Sp;
+            d1b += lDFb * bf / Sp;
+            Spb += -lDFb * bf * d1 / (Sp * Sp);
+            bfb += lSFDb * q1 / Sp;
+            q1b += lSFDb * bf / Sp;
+            Spb += -lSFDb * bf * q1 / (Sp * Sp);
+            bob += lFDb * q2 / Sp;
+            q2b += lFDb * bo / Sp;
+            Spb += -lFDb * bo * q2 / (Sp * Sp);
+            if (s1 + d1 - f1 > 0.0) { s1b += q1b; d1b += q1b; f1b -= q1b; }
+            if (f1 - s1 - d1 > 0.0) { f1b += q2b; s1b -= q2b; d1b -= q2b; }
+            double crb = bfb * pf / Sd + bob * po / Sd;
+            const double pfb = bfb * cr / Sd, pob = bob * cr / Sd;
+            Sdb += -(bfb * cr * pf + bob * cr * po) / (Sd * Sd);
+            if (in.Ef - in.Eo > 0.0) { b.Ef += pfb; b.Eo -= pfb; }
+            if (in.Eo - in.Ef > 0.0) { b.Eo += pob; b.Ef -= pob; }
+            const double Xb = crb * credit_d(X, mass_scale);
+            if (X > 0.0) {
+                Sdb += Xb * Sp / (2.0 * X);
+                Spb += Xb * Sd / (2.0 * X);
+            }
+            f1b += Spb; s1b += Spb; d1b += Spb;
+            b.Ef += Sdb; b.Eo += Sdb;
+        }
+    }
+    // prediction reverse: f1 = P - d1; d1 = min(dyn, u); u = max(0, t); t = P - s1
+    double Pb = f1b;
+    d1b -= f1b;
+    if (!d_is_dyn) {
+        const double ub = d1b;
+        if (t > 0.0) {
+            Pb += ub;
+            s1b -= ub;
+        }
+    }
+    b.ms += s1b * in.g;
+    b.g += s1b * in.ms + Pb * (in.mf + in.md);
+    b.mf += Pb * in.g;
+    b.md += Pb * in.g;
+    return b;
+}
+
+struct CalibCellArgs {
+    int C, F;
+    double ls, sigma, gamma, prior_occ, prior_free;
+    double mass_scale;
+    double inv_n;  // 1 / number of label instances
+    float dt[kMaxCalibFrames];
+    const float* dyn[kMaxCalibFrames];  // per frame: particle weight sums (nullptr = none)
+    const double* sums;                 // F x 4 x C: f occ, f free, -x f' occ, -x f' free
+    const uint32_t* n0;
+    const uint32_t* n1;
+    float* occ_out;  // optional
+    double* red;     // [0] loss, [1..5] gradient of (ls, sigma, gamma, prior_occ, prior_free)
+    int want_grad;
+};
+
+__device__ inline double block_sum(double v, double* sm) {
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    __syncthreads();
+    if (lane == 0) sm[w] = v;
+    __syncthreads();
+    double r = 0.0;
+    if (threadIdx.x == 0)
+        for (int i = 0; i < (int)(blockDim.x >> 5); ++i) r += sm[i];
+    return r;  // valid in thread 0
+}
+
+__global__ void __launch_bounds__(256) k_calib_cells(CalibCellArgs a) {
+    __shared__ double sm[8];
+    double loss = 0.0, g_ls = 0.0, g_sig = 0.0, g_gam = 0.0, g_po = 0.0, g_pf = 0.0;
+    const long C = a.C;
+    for (long c = blockIdx.x * (long)blockDim.x + threadIdx.x; c < C; c += (long)gridDim.x * blockDim.x) {
+        const uint32_t n0 = a.n0[c], n1 = a.n1[c];
+        const bool labelled = (n0 | n1) != 0;
+        if (!labelled && !a.occ_out) continue;
+        FrameIn in[kMaxCalibFrames];
+        double mf = a.prior_free, ms = a.prior_occ / 2.0, md = a.prior_occ / 2.0;
+        for (int k = 0; k < a.F; ++k) {
+            const double* s = a.sums + (long)k * 4 * C;
+            FrameIn& x = in[k];
+            x.mf = mf; x.ms = ms; x.md = md;
+            x.g = k == 0 ? 1.0 : pow(a.gamma, (double)a.dt[k]);
+            x.dyn = (k == 0 || !a.dyn[k]) ? 0.0 : (double)a.dyn[k][c];
+            x.Eo = a.sigma * s[c];
+            x.Ef = a.sigma * s[C + c];
+            frame_forward(x, a.mass_scale, &mf, &ms, &md);
+        }
+        const double T = mf + ms + md;
+        const double p = T > 0.0 ? (ms + md) / T : 0.5;
+        if (a.occ_out) a.occ_out[c] = (float)p;
+        if (!labelled) continue;
+        const double pc = fmin(fmax(p, kPClamp), 1.0 - kPClamp);
+        loss += -(double)n1 * log(pc) - (double)n0 * log(1.0 - pc);
+        if (!a.want_grad) continue;
+        double pb = (p > kPClamp && p < 1.0 - kPClamp) ? (-(double)n1 / pc + (double)n0 / (1.0 - pc)) : 0.0;
+        pb *= a.inv_n;
+        double Fb = 0.0, Sb = 0.0, Db = 0.0;
+        if (T > 0.0) {
+            Fb = -pb * (ms + md) / (T * T);
+            Sb = pb * mf / (T * T);
+            Db = Sb;
+        }
+        for (int k = a.F - 1; k >= 0; --k) {
+            const FrameBar b = frame_adjoint(in[k], a.mass_scale, Fb, Sb, Db);
+            const double* s = a.sums + (long)k * 4 * C;
+            // E = sigma F: dE/dsigma = F, dE/dls = sigma H / ls
+            g_sig += b.Eo * s[c] + b.Ef * s[C + c];
+            g_ls += (b.Eo * s[2 * C + c] + b.Ef * s[3 * C + c]) * a.sigma / a.ls;
+            if (k > 0 && a.dt[k] > 0.0f) g_gam += b.g * (double)a.dt[k] * pow(a.gamma, (double)a.dt[k] - 1.0);
+            Fb = b.mf; Sb = b.ms; Db = b.md;
+        }
+        g_pf += Fb;
+        g_po += (Sb + Db) / 2.0;
+    }
+    double r;
+    r = block_sum(loss * a.inv_n, sm);
+    if (threadIdx.x == 0 && r != 0.0) atomicAdd(&a.red[0], r);
+    if (!a.want_grad) return;
+    r = block_sum(g_ls, sm);
+    if (threadIdx.x == 0 && r != 0.0) atomicAdd(&a.red[1], r);
+    r = block_sum(g_sig, sm);
+    if (threadIdx.x == 0 && r != 0.0) atomicAdd(&a.red[2], r);
+    r = block_sum(g_gam, sm);
+    if (threadIdx.x == 0 && r != 0.0) atomicAdd(&a.red[3], r);
+    r = block_sum(g_po, sm);
+    if (threadIdx.x == 0 && r != 0.0) atomicAdd(&a.red[4], r);
+    r = block_sum(g_pf, sm);
+    if (threadIdx.x == 0 && r != 0.0) atomicAdd(&a.red[5], r);
+}
+
+// acc4 (units of 2^-40) -> sums (FP64); clears acc4.
+__global__ void k_take_sums(unsigned long long* __restrict__ acc4, long C, double* __restrict__ sums) {
+    const double inv = 1.0 / (double)(1ull << kCalibShift);
+    for (long c = blockIdx.x * (long)blockDim.x + threadIdx.x; c < C; c += (long)gridDim.x * blockDim.x) {
+        for (int q = 0; q < 4; ++q) {
+            const long long v = (long long)acc4[4 * c + q];
+            sums[q * C + c] = (double)v * inv;
+            acc4[4 * c + q] = 0ull;
+        }
+    }
+}
+
+// ---------------------------------------------------------------- held-out labels (3-D DDA)
+// Ray from the sensor s to the hit s + m, in continuous index space X = x / res + G / 2
+// (cell i spans [i, i + 1)); Amanatides-Woo traversal in FP64 with the operations written out
+// (no contraction), ties broken x before y before z. Every voxel before the hit voxel counts a
+// free label (n0), the hit voxel a hit label (n1); voxels outside the grid are skipped.
+struct DdaGrid {
+    int G, Gz;
+    double res;
+};
+
+__device__ inline void dda_ray(const DdaGrid& g, double sx, double sy, double sz, double mx, double my, double mz,
+                               uint32_t* n0, uint32_t* n1) {
+    const double half[3] = {g.G / 2.0, g.G / 2.0, g.Gz / 2.0};
+    const int dims[3] = {g.G, g.G, g.Gz};
+    const double a[3] = {__dadd_rn(__ddiv_rn(sx, g.res), half[0]), __dadd_rn(__ddiv_rn(sy, g.res), half[1]),
+                         __dadd_rn(__ddiv_rn(sz, g.res), half[2])};
+    const double b[3] = {__dadd_rn(__ddiv_rn(__dadd_rn(sx, mx), g.res), half[0]),
+                         __dadd_rn(__ddiv_rn(__dadd_rn(sy, my), g.res), half[1]),
+                         __dadd_rn(__ddiv_rn(__dadd_rn(sz, mz), g.res), half[2])};
+    int v[3], e[3], step[3];
+    double tmax[3], tdel[3];
+    long budget = 1;
+    for (int k = 0; k < 3; ++k) {
+        v[k] = (int)floor(a[k]);
+        e[k] = (int)floor(b[k]);
+        const double d = __dsub_rn(b[k], a[k]);
+        budget += abs(e[k] - v[k]);
+        if (d > 0.0) {
+            step[k] = 1;
+            tdel[k] = __ddiv_rn(1.0, d);
+            tmax[k] = __dmul_rn(__dsub_rn((double)(v[k] + 1), a[k]), tdel[k]);
+        } else if (d < 0.0) {
+            step[k] = -1;
+            tdel[k] = __ddiv_rn(-1.0, d);
+            tmax[k] = __dmul_rn(__dsub_rn(a[k], (double)v[k]), tdel[k]);
+        } else {
+            step[k] = 0;
+            tdel[k] = INFINITY;
+            tmax[k] = INFINITY;
+        }
+    }
+    for (long it = 0; it < budget; ++it) {
+        if (v[0] == e[0] && v[1] == e[1] && v[2] == e[2]) break;
+        if (v[0] >= 0 && v[0] < dims[0] && v[1] >= 0 && v[1] < dims[1] && v[2] >= 0 && v[2] < dims[2])
+            atomicAdd(&n0[v[0] + (long)g.G * v[1] + (long)g.G * g.G * v[2]], 1u);
+        int k = 0;
+        if (tmax[1] < tmax[k]) k = 1;
+        if (tmax[2] < tmax[k]) k = 2;
+        v[k] += step[k];
+        tmax[k] = __dadd_rn(tmax[k], tdel[k]);
+    }
+    if (e[0] >= 0 && e[0] < dims[0] && e[1] >= 0 && e[1] < dims[1] && e[2] >= 0 && e[2] < dims[2])
+        atomicAdd(&n1[e[0] + (long)g.G * e[1] + (long)g.G * g.G * e[2]], 1u);
+}
+
+__global__ void k_dda_labels(DdaGrid g, float sx, float sy, float sz, const float* __restrict__ xyz, int n,
+                             uint32_t* n0, uint32_t* n1) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const float mx = xyz[3 * i], my = xyz[3 * i + 1], mz = xyz[3 * i + 2];
+        if (!(isfinite(mx) && isfinite(my) && isfinite(mz))) continue;
+        dda_ray(g, sx, sy, sz, mx, my, mz, n0, n1);
+    }
+}
+
+// xyz interleaved -> SoA
+__global__ void k_split_xyz(const float* __restrict__ xyz, int n, float* x, float* y, float* z) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        x[i] = xyz[3 * i];
+        y[i] = xyz[3 * i + 1];
+        z[i] = xyz[3 * i + 2];
+    }
+}
+
+struct CalibFrame {
+    float dt;
+    float sensor[3];
+    int n;
+    float* pts;  // device x | y | z
+    float* dyn;  // device, C floats, or nullptr
+};
+
+}  // namespace
+
+struct k3dom_calib {
+    int device = 0, num_sms = 148;
+    k3dom_params base{};
+    DevParams dp{};
+    cudaStream_t st = nullptr;
+    std::vector<CalibFrame> frames;
+    std::vector<void*> allocs, ray_allocs;
+    uint32_t *n0 = nullptr, *n1 = nullptr;
+    double n_labels = 0.0;
+    SceneDev* sc_dev = nullptr;
+    SceneOffsets* off_dev = nullptr;
+    FrameParams* fp_dev = nullptr;  // one per frame
+    DevStatus* status = nullptr;
+    RayBuffers rb{};
+    int ray_points = 0;
+    float ray_ls = 0.0f;  // length-scale the list capacity was sized for
+    float4 *ftab = nullptr, *htab = nullptr;
+    unsigned long long* acc4 = nullptr;
+    double* sums = nullptr;  // F x 4 x C
+    int sums_frames = 0;
+    double* red = nullptr;
+    double red_host[6] = {0};
+    float sums_ls = -1.0f;  // ls of the sums currently held
+    cudaError_t last = cudaSuccess;
+
+    k3dom_status fail(cudaError_t e) {
+        last = e;
+        return e == cudaErrorMemoryAllocation ? K3DOM_ERR_OUT_OF_MEMORY : K3DOM_ERR_CUDA;
+    }
+    template <typename T>
+    cudaError_t alloc(T** p, size_t count, std::vector<void*>* list = nullptr) {
+        *p = nullptr;
+        cudaError_t e = cudaMalloc((void**)p, std::max<size_t>(count, 1) * sizeof(T));
+        if (e != cudaSuccess) return e;
+        (list ? list : &allocs)->push_back((void*)*p);
+        return cudaMemset(*p, 0, std::max<size_t>(count, 1) * sizeof(T));
+    }
+    void release() {
+        for (void* p : ray_allocs) cudaFree(p);
+        for (void* p : allocs) cudaFree(p);
+        ray_allocs.clear();
+        allocs.clear();
+        if (st) cudaStreamDestroy(st);
+    }
+};
+
+namespace {
+
+TileShape calib_tiles(const DevParams& p) {
+    TileShape t;
+    const bool large = (long)p.C >= (1L << 20) && p.Gz >= 8;
+    t.tx = large ? 16 : 8;
+    t.ty = large ? 16 : 8;
+    t.tz = large ? 8 : 4;
+    t.ntx = (p.G + t.tx - 1) / t.tx;
+    t.nty = (p.G + t.ty - 1) / t.ty;
+    t.ntz = (p.Gz + t.tz - 1) / t.tz;
+    t.nsbx = t.tx / 4;
+    t.nsby = t.ty / 4;
+    return t;
+}
+
+// Ray buffers for the largest frame at length-scale ls (re-made when either grows).
+cudaError_t ensure_ray_buffers(k3dom_calib* c, int max_points, float ls, const SceneDev& sd) {
+    if (max_points <= c->ray_points && ls <= c->ray_ls && c->rb.ekeys) return cudaSuccess;
+    for (void* p : c->ray_allocs) cudaFree(p);
+    c->ray_allocs.clear();
+    RayBuffers& rb = c->rb;
+    rb = RayBuffers{};
+    const int N = std::max(max_points, 1);
+    const int T = sd.ts.ntx * sd.ts.nty * sd.ts.ntz;
+    long cap = std::max(ray_entries_bound(sd.p, sd.ts, N, sd.bin_R), 4096L);
+    if (cap > 0xFFFFFFF0L) cap = 0xFFFFFFF0L;
+    rb.capacity = cap;
+    rb.chunk = 1024;
+    std::vector<void*>* L = &c->ray_allocs;
+    cudaError_t e;
+    if ((e = c->alloc(&rb.ray_a, N, L)) || (e = c->alloc(&rb.ray_c, N, L)) || (e = c->alloc(&rb.counts, N, L)) ||
+        (e = c->alloc(&rb.offsets, N, L)) || (e = c->alloc(&rb.ekeys, cap, L)) || (e = c->alloc(&rb.evals, cap, L)) ||
+        (e = c->alloc(&rb.ekeys2, cap, L)) || (e = c->alloc(&rb.evals2, cap, L)) ||
+        (e = c->alloc(&rb.tile_start, T + 1, L)) || (e = c->alloc(&rb.tile_items, T, L)) ||
+        (e = c->alloc(&rb.item_off, T + 1, L)) || (e = c->alloc(&rb.tile_done, T, L)) ||
+        (e = c->alloc(&rb.total, 4, L)))
+        return e;
+    int bits = 1;
+    while ((1 << bits) < T + 1) ++bits;
+    int pb[4];
+    if (radix_plan(bits, pb) > 1) {
+        if ((e = c->alloc(&rb.ekeys_alt, cap, L)) || (e = c->alloc(&rb.evals_alt, cap, L))) return e;
+    } else {
+        rb.ekeys_alt = rb.ekeys;
+        rb.evals_alt = rb.evals;
+    }
+    rb.hist_words = std::max(radix_hist_words(cap, 11), 1L);
+    rb.scan_words = scan_u32_tiles(std::max({rb.hist_words, (long)N, (long)T + 1})) + 16;
+    if ((e = c->alloc(&rb.hist, rb.hist_words, L)) || (e = c->alloc(&rb.scan_tmp, rb.scan_words, L))) return e;
+    c->ray_points = N;
+    c->ray_ls = ls;
+    return cudaSuccess;
+}
+
+// The per-frame kernel and derivative sums at length-scale ls (kept until ls changes).
+k3dom_status compute_sums(k3dom_calib* c, float ls) {
+    const int F = (int)c->frames.size();
+    if (F == 0) return K3DOM_ERR_NOT_READY;
+    if (ls == c->sums_ls && c->sums_frames == F) return K3DOM_OK;
+    cudaError_t e;
+    const long C = c->dp.C;
+    if (c->sums_frames != F) {
+        if (c->sums) {
+            auto it = std::find(c->allocs.begin(), c->allocs.end(), (void*)c->sums);
+            if (it != c->allocs.end()) c->allocs.erase(it);
+            cudaFree(c->sums);
+            c->sums = nullptr;
+        }
+        if ((e = c->alloc(&c->sums, (size_t)F * 4 * C))) return c->fail(e);
+        c->sums_frames = F;
+    }
+    SceneDev sd;
+    std::memset(&sd, 0, sizeof(sd));
+    sd.p = c->dp;
+    sd.p.ls = ls;
+    sd.p.sigma = 1.0f;
+    sd.ts = calib_tiles(sd.p);
+    sd.n_tiles = sd.ts.ntx * sd.ts.nty * sd.ts.ntz;
+    fill_scene_evidence(sd, false, nullptr);
+    int maxn = 0;
+    for (auto& f : c->frames) maxn = std::max(maxn, f.n);
+    if ((e = ensure_ray_buffers(c, maxn, ls, sd))) return c->fail(e);
+    sd.max_points = c->ray_points;
+    if ((e = cudaMemcpyAsync(c->sc_dev, &sd, sizeof(sd), cudaMemcpyHostToDevice, c->st))) return c->fail(e);
+    for (int k = 0; k < F; ++k) {
+        const CalibFrame& f = c->frames[k];
+        SceneOffsets off;
+        std::memset(&off, 0, sizeof(off));
+        off.point[1] = f.n;
+        off.tile[1] = sd.n_tiles;
+        off.cell[1] = (int)C;
+        off.part[1] = c->dp.P;
+        off.birth[1] = c->dp.B;
+        off.joint[1] = c->dp.P + c->dp.B;
+        FrameParams fp;
+        std::memset(&fp, 0, sizeof(fp));
+        fp.dt = f.dt;
+        fp.sensor_x = f.sensor[0];
+        fp.sensor_y = f.sensor[1];
+        fp.sensor_z = f.sensor[2];
+        fp.n_points = f.n;
+        if ((e = cudaMemcpyAsync(c->off_dev + k, &off, sizeof(off), cudaMemcpyHostToDevice, c->st)) ||
+            (e = cudaMemcpyAsync(c->fp_dev + k, &fp, sizeof(fp), cudaMemcpyHostToDevice, c->st)))
+            return c->fail(e);
+        Batch bt;
+        bt.S = 1;
+        bt.variant = 0;
+        bt.P = c->dp.P;
+        bt.B = c->dp.B;
+        bt.C = (int)C;
+        bt.N = f.n;
+        bt.T = sd.n_tiles;
+        bt.sc = c->sc_dev;
+        bt.fp = c->fp_dev + k;
+        bt.off = c->off_dev + k;
+        if (f.n > 0) {
+            if ((e = build_ray_lists(bt, f.pts, f.pts + f.n, f.pts + 2 * (long)f.n, c->rb, false, c->status, c->st)))
+                return c->fail(e);
+            if ((e = launch_bgki_sums(bt, c->rb, c->ftab, c->htab, c->acc4, c->status, c->num_sms, c->st)))
+                return c->fail(e);
+        }
+        ++g_launches;
+        k_take_sums<<<grid_for(C), kBlock, 0, c->st>>>(c->acc4, C, c->sums + (long)k * 4 * C);
+        if ((e = cudaGetLastError())) return c->fail(e);
+    }
+    DevStatus dst;
+    if ((e = cudaMemcpyAsync(&dst, c->status, sizeof(dst), cudaMemcpyDeviceToHost, c->st)) ||
+        (e = cudaStreamSynchronize(c->st)))
+        return c->fail(e);
+    if (dst.overflow) return K3DOM_ERR_CAPACITY;
+    c->sums_ls = ls;
+    return K3DOM_OK;
+}
+
+k3dom_status run_cells(k3dom_calib* c, const float theta[5], bool grad, float* occ_out) {
+    if (!(theta[0] > 0.0f) || !(theta[2] > 0.0f)) return K3DOM_ERR_INVALID_ARGUMENT;
+    if (c->n_labels <= 0.0 && !occ_out) return K3DOM_ERR_NOT_READY;
+    k3dom_status s = compute_sums(c, theta[0]);
+    if (s != K3DOM_OK) return s;
+    CalibCellArgs a;
+    std::memset(&a, 0, sizeof(a));
+    a.C = c->dp.C;
+    a.F = (int)c->frames.size();
+    a.ls = theta[0];
+    a.sigma = theta[1];
+    a.gamma = theta[2];
+    a.prior_occ = theta[3];
+    a.prior_free = theta[4];
+    a.mass_scale = c->dp.mass_scale;
+    a.inv_n = c->n_labels > 0.0 ? 1.0 / c->n_labels : 0.0;
+    for (int k = 0; k < a.F; ++k) {
+        a.dt[k] = c->frames[k].dt;
+        a.dyn[k] = c->frames[k].dyn;
+    }
+    a.sums = c->sums;
+    a.n0 = c->n0;
+    a.n1 = c->n1;
+    a.occ_out = occ_out;
+    a.red = c->red;
+    a.want_grad = grad ? 1 : 0;
+    cudaError_t e;
+    if ((e = cudaMemsetAsync(c->red, 0, 6 * sizeof(double), c->st))) return c->fail(e);
+    ++g_launches;
+    k_calib_cells<<<grid_for(a.C), 256, 0, c->st>>>(a);
+    if ((e = cudaGetLastError()) || (e = cudaMemcpyAsync(c->red_host, c->red, 6 * sizeof(double),
+                                                         cudaMemcpyDeviceToHost, c->st)) ||
+        (e = cudaStreamSynchronize(c->st)))
+        return c->fail(e);
+    return K3DOM_OK;
+}
+
+cudaError_t to_device_copy(k3dom_calib* c, float** dst, const float* src, size_t count, k3dom_mem mem) {
+    cudaError_t e = c->alloc(dst, count);
+    if (e != cudaSuccess) return e;
+    return cudaMemcpyAsync(*dst, src, count * sizeof(float),
+                           mem == K3DOM_MEM_HOST ? cudaMemcpyHostToDevice : cudaMemcpyDeviceToDevice, c->st);
+}
+
+}  // namespace
+
+extern "C" {
+
+k3dom_status k3dom_calib_create(const k3dom_params* base, int device, k3dom_calib** out) {
+    if (!out || !base) return K3DOM_ERR_INVALID_ARGUMENT;
+    *out = nullptr;
+    if (!(base->resolution > 0.0f) || !(base->size > 0.0f) || !(base->size_z > 0.0f) || !(base->mass_scale != 0.0f))
+        return K3DOM_ERR_INVALID_ARGUMENT;
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) return K3DOM_ERR_NO_DEVICE;
+    if (device < 0 || device >= ndev) return K3DOM_ERR_INVALID_ARGUMENT;
+    k3dom_calib* c = new (std::nothrow) k3dom_calib();
+    if (!c) return K3DOM_ERR_OUT_OF_MEMORY;
+    auto bail = [&](cudaError_t e) {
+        k3dom_status r = c->fail(e);
+        c->release();
+        delete c;
+        return r;
+    };
+    c->device = device;
+    c->base = *base;
+    cudaError_t e = cudaSetDevice(device);
+    if (e != cudaSuccess) return bail(e);
+    cudaDeviceProp prop;
+    if ((e = cudaGetDeviceProperties(&prop, device))) return bail(e);
+    c->num_sms = prop.multiProcessorCount;
+    if ((e = sort_init()) || (e = evidence_init())) return bail(e);
+    DevParams& d = c->dp;
+    d.G = static_cast<int>(base->size / base->resolution);
+    d.Gz = static_cast<int>(base->size_z / base->resolution);
+    if (d.G < 1 || d.Gz < 1 || (double)d.G * d.G * d.Gz > 2147483647.0 / 4) return bail(cudaErrorInvalidValue);
+    d.C = d.G * d.G * d.Gz;
+    d.P = 1;
+    d.B = 1;
+    d.res = base->resolution;
+    d.size = base->size;
+    d.size_z = base->size_z;
+    d.mass_scale = base->mass_scale;
+    d.ls = base->ls;
+    d.sigma = 1.0f;
+    d.window_radius = base->resolution * 0.866f;
+    if ((e = cudaStreamCreateWithFlags(&c->st, cudaStreamNonBlocking))) return bail(e);
+    if ((e = c->alloc(&c->n0, d.C)) || (e = c->alloc(&c->n1, d.C)) || (e = c->alloc(&c->sc_dev, 1)) ||
+        (e = c->alloc(&c->off_dev, kMaxCalibFrames)) || (e = c->alloc(&c->fp_dev, kMaxCalibFrames)) ||
+        (e = c->alloc(&c->status, 1)) || (e = c->alloc(&c->ftab, kKernelTableSize)) ||
+        (e = c->alloc(&c->htab, kKernelTableSize)) || (e = c->alloc(&c->acc4, 4 * (size_t)d.C)) ||
+        (e = c->alloc(&c->red, 6)))
+        return bail(e);
+    std::vector<float4> ft(kKernelTableSize), ht(kKernelTableSize);
+    build_calib_tables(ft.data(), ht.data());
+    if ((e = cudaMemcpy(c->ftab, ft.data(), sizeof(float4) * ft.size(), cudaMemcpyHostToDevice)) ||
+        (e = cudaMemcpy(c->htab, ht.data(), sizeof(float4) * ht.size(), cudaMemcpyHostToDevice)))
+        return bail(e);
+    *out = c;
+    return K3DOM_OK;
+}
+
+k3dom_status k3dom_calib_destroy(k3dom_calib* c) {
+    if (!c) return K3DOM_ERR_INVALID_ARGUMENT;
+    cudaSetDevice(c->device);
+    cudaStreamSynchronize(c->st);
+    c->release();
+    delete c;
+    return K3DOM_OK;
+}
+
+k3dom_status k3dom_calib_add_frame(k3dom_calib* c, float dt, float sx, float sy, float sz, const float* xyz,
+                                   int32_t n, const float* dyn_pred, k3dom_mem mem) {
+    if (!c || n < 0 || (n > 0 && !xyz) || !(dt >= 0.0f)) return K3DOM_ERR_INVALID_ARGUMENT;
+    if ((int)c->frames.size() >= kMaxCalibFrames) return K3DOM_ERR_CAPACITY;
+    if (c->frames.empty() && dt != 0.0f) return K3DOM_ERR_INVALID_ARGUMENT;  // frame 0 initialises
+    if (mem == K3DOM_MEM_HOST)
+        for (long i = 0; i < 3L * n; ++i)
+            if (!std::isfinite(xyz[i])) return K3DOM_ERR_INVALID_INPUT;
+    cudaSetDevice(c->device);
+    CalibFrame f;
+    f.dt = dt;
+    f.sensor[0] = sx;
+    f.sensor[1] = sy;
+    f.sensor[2] = sz;
+    f.n = n;
+    f.pts = nullptr;
+    f.dyn = nullptr;
+    cudaError_t e;
+    float* tmp = nullptr;
+    if ((e = c->alloc(&f.pts, 3 * (size_t)std::max(n, 1)))) return c->fail(e);
+    if (n > 0) {
+        if ((e = to_device_copy(c, &tmp, xyz, 3 * (size_t)n, mem))) return c->fail(e);
+        ++g_launches;
+        k_split_xyz<<<grid_for(n), kBlock, 0, c->st>>>(tmp, n, f.pts, f.pts + n, f.pts + 2 * (long)n);
+        if ((e = cudaGetLastError())) return c->fail(e);
+    }
+    if (dyn_pred && (e = to_device_copy(c, &f.dyn, dyn_pred, (size_t)c->dp.C, mem))) return c->fail(e);
+    if ((e = cudaStreamSynchronize(c->st))) return c->fail(e);
+    if (tmp) {
+        auto it = std::find(c->allocs.begin(), c->allocs.end(), (void*)tmp);
+        if (it != c->allocs.end()) c->allocs.erase(it);
+        cudaFree(tmp);
+    }
+    c->frames.push_back(f);
+    c->sums_ls = -1.0f;
+    return K3DOM_OK;
+}
+
+k3dom_status k3dom_calib_add_heldout_scan(k3dom_calib* c, float sx, float sy, float sz, const float* xyz, int32_t n,
+                                          k3dom_mem mem) {
+    if (!c || n < 0 || (n > 0 && !xyz)) return K3DOM_ERR_INVALID_ARGUMENT;
+    if (n == 0) return K3DOM_OK;
+    cudaSetDevice(c->device);
+    cudaError_t e;
+    float* tmp = nullptr;
+    const float* src = xyz;
+    if (mem == K3DOM_MEM_HOST) {
+        if ((e = to_device_copy(c, &tmp, xyz, 3 * (size_t)n, mem))) return c->fail(e);
+        src = tmp;
+    }
+    DdaGrid g;
+    g.G = c->dp.G;
+    g.Gz = c->dp.Gz;
+    g.res = c->dp.res;
+    ++g_launches;
+    k_dda_labels<<<grid_for(n), kBlock, 0, c->st>>>(g, sx, sy, sz, src, n, c->n0, c->n1);
+    if ((e = cudaGetLastError()) || (e = cudaStreamSynchronize(c->st))) return c->fail(e);
+    if (tmp) {
+        auto it = std::find(c->allocs.begin(), c->allocs.end(), (void*)tmp);
+        if (it != c->allocs.end()) c->allocs.erase(it);
+        cudaFree(tmp);
+    }
+    // total label instances
+    std::vector<uint32_t> h0(c->dp.C), h1(c->dp.C);
+    if ((e = cudaMemcpy(h0.data(), c->n0, sizeof(uint32_t) * h0.size(), cudaMemcpyDeviceToHost)) ||
+        (e = cudaMemcpy(h1.data(), c->n1, sizeof(uint32_t) * h1.size(), cudaMemcpyDeviceToHost)))
+        return c->fail(e);
+    double tot = 0.0;
+    for (size_t i = 0; i < h0.size(); ++i) tot += (double)h0[i] + (double)h1[i];
+    c->n_labels = tot;
+    return K3DOM_OK;
+}
+
+k3dom_status k3dom_calib_label_counts(k3dom_calib* c, uint32_t* n0, uint32_t* n1, k3dom_mem mem) {
+    if (!c) return K3DOM_ERR_INVALID_ARGUMENT;
+    cudaSetDevice(c->device);
+    const cudaMemcpyKind k = mem == K3DOM_MEM_HOST ? cudaMemcpyDeviceToHost : cudaMemcpyDeviceToDevice;
+    cudaError_t e = cudaSuccess;
+    if (n0) e = cudaMemcpy(n0, c->n0, sizeof(uint32_t) * (size_t)c->dp.C, k);
+    if (e == cudaSuccess && n1) e = cudaMemcpy(n1, c->n1, sizeof(uint32_t) * (size_t)c->dp.C, k);
+    return e == cudaSuccess ? K3DOM_OK : c->fail(e);
+}
+
+k3dom_status k3dom_calib_get_sums(k3dom_calib* c, float ls, int32_t frame, double* out, k3dom_mem mem) {
+    if (!c || !out || frame < 0 || frame >= (int)c->frames.size() || !(ls > 0.0f)) return K3DOM_ERR_INVALID_ARGUMENT;
+    cudaSetDevice(c->device);
+    k3dom_status s = compute_sums(c, ls);
+    if (s != K3DOM_OK) return s;
+    const size_t C = (size_t)c->dp.C;
+    cudaError_t e = cudaMemcpy(out, c->sums + (size_t)frame * 4 * C, sizeof(double) * 4 * C,
+                               mem == K3DOM_MEM_HOST ? cudaMemcpyDeviceToHost : cudaMemcpyDeviceToDevice);
+    return e == cudaSuccess ? K3DOM_OK : c->fail(e);
+}
+
+k3dom_status k3dom_bgki_forward(k3dom_calib* c, const float* theta, float* loss, float* occupancy, k3dom_mem mem) {
+    if (!c || !theta) return K3DOM_ERR_INVALID_ARGUMENT;
+    cudaSetDevice(c->device);
+    float* occ_dev = nullptr;
+    cudaError_t e;
+    if (occupancy) {
+        if (mem == K3DOM_MEM_DEVICE) {
+            occ_dev = occupancy;
+        } else if ((e = c->alloc(&occ_dev, (size_t)c->dp.C))) {
+            return c->fail(e);
+        }
+    }
+    k3dom_status s = run_cells(c, theta, false, occ_dev);
+    if (s == K3DOM_OK && occupancy && mem == K3DOM_MEM_HOST) {
+        e = cudaMemcpy(occupancy, occ_dev, sizeof(float) * (size_t)c->dp.C, cudaMemcpyDeviceToHost);
+        if (e != cudaSuccess) s = c->fail(e);
+    }
+    if (occupancy && mem == K3DOM_MEM_HOST && occ_dev) {
+        auto it = std::find(c->allocs.begin(), c->allocs.end(), (void*)occ_dev);
+        if (it != c->allocs.end()) c->allocs.erase(it);
+        cudaFree(occ_dev);
+    }
+    if (s == K3DOM_OK && loss) *loss = (float)c->red_host[0];
+    return s;
+}
+
+k3dom_status k3dom_bgki_backward(k3dom_calib* c, const float* theta, float grad_loss, float* grad_theta,
+                                 float* loss) {
+    if (!c || !theta || !grad_theta) return K3DOM_ERR_INVALID_ARGUMENT;
+    cudaSetDevice(c->device);
+    k3dom_status s = run_cells(c, theta, true, nullptr);
+    if (s != K3DOM_OK) return s;
+    for (int i = 0; i < 5; ++i) grad_theta[i] = (float)(grad_loss * c->red_host[1 + i]);
+    if (loss) *loss = (float)c->red_host[0];
+    return K3DOM_OK;
+}
+
+k3dom_status k3dom_calib_info(k3dom_calib* c, int32_t* cells, int32_t* frames, double* label_instances) {
+    if (!c) return K3DOM_ERR_INVALID_ARGUMENT;
+    if (cells) *cells = c->dp.C;
+    if (frames) *frames = (int32_t)c->frames.size();
+    if (label_instances) *label_instances = c->n_labels;
+    return K3DOM_OK;
+}
+
+k3dom_status k3dom_calib_get_stream(k3dom_calib* c, void** stream) {
+    if (!c || !stream) return K3DOM_ERR_INVALID_ARGUMENT;
+    *stream = (void*)c->st;
+    return K3DOM_OK;
+}
+
+}  // extern "C"

@@ -204,6 +204,7 @@ __device__ __forceinline__ BinGeom scene_geom(const SceneDev& sd, const FramePar
 __global__ void k_ray_count(Batch bt, const float* __restrict__ xs, const float* __restrict__ ys,
                             const float* __restrict__ zs, int ds, float4* __restrict__ ra,
                             double4* __restrict__ rc, uint32_t* __restrict__ counts, DevStatus* status) {
+    if (blockIdx.x == 0 && threadIdx.x == 0) status->overflow = 0u;  // per-frame flag (set by k_ray_emit)
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < bt.N; i += gridDim.x * blockDim.x) {
         const int sc = scene_of(bt.off->point, bt.S, i);
         const FrameParams f = bt.fp[sc];
@@ -1039,6 +1040,187 @@ static EvArgs make_args(const Batch& bt, RayBuffers& rb, CellState cs, CellWork 
     return A;
 }
 
+// ================================================================ calibration sums
+// For the differentiable update: per cell and frame, the sums of the unit-amplitude sparse
+// kernel f(d/ls) over the occupied and free pairs, and of d f(d/ls) / d ls (times ls, i.e.
+// -x f'(x)), from the same tiles, culls and pair geometry as k_bgki. Both are summed exactly
+// in fixed point (units of 2^-40), so the loss and its gradient are deterministic. No per-pair
+// value is stored: the derivative is formed in the same pass as the value.
+//
+// f(x) = max(0, (2 + cos 2 pi x)(1 - x) / 3 + sin(2 pi x) / (2 * 3.141592)), mass_update.cu:24-26.
+static double unit_kernel(double x) {
+    const double v = (2.0 + std::cos(M_PI * 2.0 * x)) * (1.0 - x) / 3.0 + std::sin(M_PI * 2.0 * x) / (2.0 * 3.141592);
+    return v > 0.0 ? v : 0.0;
+}
+// -x f'(x) where f > 0 (0 where the clamp is active)
+static double unit_kernel_dls(double x) {
+    const double v = (2.0 + std::cos(M_PI * 2.0 * x)) * (1.0 - x) / 3.0 + std::sin(M_PI * 2.0 * x) / (2.0 * 3.141592);
+    if (!(v > 0.0)) return 0.0;
+    const double fp = (-2.0 * M_PI * std::sin(M_PI * 2.0 * x) * (1.0 - x) - (2.0 + std::cos(M_PI * 2.0 * x))) / 3.0 +
+                      2.0 * M_PI * std::cos(M_PI * 2.0 * x) / (2.0 * 3.141592);
+    return -x * fp;
+}
+
+static void build_table(double (*fn)(double), double scale, float4* out) {
+    for (int i = 0; i < kKernelTab; ++i) {
+        double y[4];
+        for (int j = 0; j < 4; ++j) y[j] = scale * fn(std::sqrt(std::min(1.0, (i + j / 3.0) / kKernelTab)));
+        const double c0 = y[0];
+        const double c1 = -5.5 * y[0] + 9.0 * y[1] - 4.5 * y[2] + y[3];
+        const double c2 = 9.0 * y[0] - 22.5 * y[1] + 18.0 * y[2] - 4.5 * y[3];
+        const double c3 = -4.5 * y[0] + 13.5 * y[1] - 13.5 * y[2] + 4.5 * y[3];
+        out[i] = make_float4((float)c0, (float)c1, (float)c2, (float)c3);
+    }
+}
+
+void build_calib_tables(float4* f_tab, float4* dls_tab) {
+    build_table(unit_kernel, std::ldexp(1.0, kCalibShift), f_tab);
+    build_table(unit_kernel_dls, std::ldexp(1.0, kCalibShift), dls_tab);
+}
+
+// Signed rounding to the nearest integer (|v| < 2^23 by the magic add, larger floats are
+// integers already).
+__device__ __forceinline__ double signed_units(float v) {
+    const float a = fabsf(v);
+    const float r = a < 8388608.0f ? __fsub_rn(__fadd_rn(a, 8388608.0f), 8388608.0f) : a;
+    return (double)copysignf(r, v);
+}
+
+struct CalibSmem {
+    float4 ftab[kKernelTab];
+    float4 htab[kKernelTab];
+    float4 a[kChunk];
+    double4 c[kChunk];
+    float4 stage[kEvWarps][32][3];
+};
+
+// acc4: 4 signed 64-bit sums per cell (f occ, f free, -x f' occ, -x f' free), in units.
+__global__ void __launch_bounds__(kEvThreads, 2) k_bgki_sums(EvArgs A, const float4* __restrict__ htab,
+                                                            unsigned long long* __restrict__ acc4) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    CalibSmem& S = *reinterpret_cast<CalibSmem*>(smem_raw);
+    __shared__ uint32_t s_item;
+    __shared__ int s_next_sb;
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    const Batch& bt = A.bt;
+    const uint32_t total_items = A.item_off[bt.T];
+    for (int i = threadIdx.x; i < kKernelTab; i += kEvThreads) {
+        S.ftab[i] = A.ktab[i];
+        S.htab[i] = htab[i];
+    }
+    for (;;) {
+        if (threadIdx.x == 0) {
+            s_item = atomicAdd(&A.status->work_counter, 1u);
+            s_next_sb = 0;
+        }
+        __syncthreads();
+        const uint32_t item = s_item;
+        if (item >= total_items) break;
+        const Item it = item_of(bt, A.item_off, A.tile_start, item, A.chunk);
+        const SceneDev& sd = bt.sc[it.sc];
+        const DevParams& p = sd.p;
+        const TileShape ts = sd.ts;
+        const FrameParams fp = bt.fp[it.sc];
+        const int coff = bt.off->cell[it.sc];
+        const float ls2 = p.ls * p.ls;
+        const float inv_ls2 = 1.0f / ls2;
+        const float hres = 0.5f * p.res;
+        const float cull_r2 = sd.cull_r2;
+        const int nsb = ts.nsbx * ts.nsby * (ts.tz / 2);
+        for (int r = threadIdx.x; r < it.nr; r += kEvThreads) {
+            uint32_t rid = A.evals[it.e0 + r];
+            if (rid >= (uint32_t)bt.N) rid = 0;
+            S.a[r] = A.ray_a[rid];
+            S.c[r] = A.ray_c[rid];
+        }
+        __syncthreads();
+        const int nr = it.nr;
+        for (;;) {
+            int sb = 0;
+            if (lane == 0) sb = atomicAdd(&s_next_sb, 1);
+            sb = __shfl_sync(0xffffffffu, sb, 0);
+            if (sb >= nsb) break;
+            const CellLoc L = locate(p, ts, it.lt, sb, lane, fp.sensor_x, fp.sensor_y, fp.sensor_z);
+            const float dx = L.x - L.ox, dy = L.y - L.oy, dz = L.z - L.oz;
+            const double ox = L.ox, oy = L.oy, oz = L.oz;
+            double fo = 0.0, ff = 0.0, ho = 0.0, hf = 0.0;  // exact sums of integer units
+            for (int g0 = 0; g0 < nr; g0 += 32) {
+                const int r = g0 + lane;
+                bool hit = false;
+                if (r < nr) {
+                    const float4 a = S.a[r];
+                    const double4 cd = S.c[r];
+                    const double par0 = (ox * a.x + oy * a.y + oz * a.z) * cd.z;
+                    const double sc = par0 * cd.z;
+                    const double px = ox - sc * a.x, py = oy - sc * a.y, pz = oz - sc * a.z;
+                    const float ux = (float)(a.x * cd.z), uy = (float)(a.y * cd.z), uz = (float)(a.z * cd.z);
+                    const float qd = -hres * (ux + uy + uz);
+                    const float qpar = (float)par0 + qd;
+                    const float qx = (float)px - hres - qd * ux, qy = (float)py - hres - qd * uy,
+                                qz = (float)pz - hres - qd * uz;
+                    const float qal = fminf(qpar, 0.0f) + fmaxf(qpar - a.w, 0.0f);
+                    hit = qx * qx + qy * qy + qz * qz + qal * qal < cull_r2;
+                    if (hit) {
+                        S.stage[wid][lane][0] = make_float4((float)par0, (float)(par0 - cd.y), (float)(par0 - cd.x), ux);
+                        S.stage[wid][lane][1] = make_float4((float)px, (float)py, (float)pz, uy);
+                        S.stage[wid][lane][2] =
+                            make_float4((float)(ox - a.x), (float)(oy - a.y), (float)(oz - a.z), uz);
+                    }
+                }
+                unsigned mask = __ballot_sync(0xffffffffu, hit);
+                __syncwarp();
+                while (mask) {
+                    const int j = __ffs(mask) - 1;
+                    mask &= mask - 1;
+                    const float4 s0 = S.stage[wid][j][0], s1 = S.stage[wid][j][1], s2 = S.stage[wid][j][2];
+                    const float vx = s2.x + dx, vy = s2.y + dy, vz = s2.z + dz;
+                    const float d2o = vx * vx + vy * vy + vz * vz;
+                    if (d2o < ls2 && L.c >= 0) {
+                        const float u = d2o * inv_ls2;
+                        fo += kernel_units(kernel_tab(S.ftab, u));
+                        ho += signed_units(kernel_tab(S.htab, u));
+                    }
+                    const float dpar = dx * s0.w + dy * s1.w + dz * s2.w;
+                    if (s0.z + dpar < 0.0f) {
+                        const float qx = s1.x + dx - dpar * s0.w, qy = s1.y + dy - dpar * s1.w,
+                                    qz = s1.z + dz - dpar * s2.w;
+                        const float al = fminf(s0.x + dpar, 0.0f) + fmaxf(s0.y + dpar, 0.0f);
+                        const float d2f = qx * qx + qy * qy + qz * qz + al * al;
+                        if (d2f < ls2 && L.c >= 0) {
+                            const float u = d2f * inv_ls2;
+                            ff += kernel_units(kernel_tab(S.ftab, u));
+                            hf += signed_units(kernel_tab(S.htab, u));
+                        }
+                    }
+                }
+                __syncwarp();
+            }
+            if (L.c >= 0) {
+                unsigned long long* ac = acc4 + 4 * (long)(coff + L.c);
+                const long long v0 = __double2ll_rn(fo), v1 = __double2ll_rn(ff), v2 = __double2ll_rn(ho),
+                                v3 = __double2ll_rn(hf);
+                if (v0) atomicAdd(ac, (unsigned long long)v0);
+                if (v1) atomicAdd(ac + 1, (unsigned long long)v1);
+                if (v2) atomicAdd(ac + 2, (unsigned long long)v2);
+                if (v3) atomicAdd(ac + 3, (unsigned long long)v3);
+            }
+        }
+        __syncthreads();
+    }
+}
+
+cudaError_t launch_bgki_sums(const Batch& bt, RayBuffers& rb, const float4* f_tab, const float4* dls_tab,
+                             unsigned long long* acc4, DevStatus* status, int num_sms, cudaStream_t st) {
+    if (rb.chunk < 32 || rb.chunk > kChunk) return cudaErrorInvalidValue;
+    EvArgs A = make_args(bt, rb, CellState{}, CellWork{}, false, status);
+    A.ktab = f_tab;
+    int per_sm = 1;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_bgki_sums, kEvThreads, sizeof(CalibSmem));
+    ++g_launches;
+    k_bgki_sums<<<num_sms * std::max(1, per_sm), kEvThreads, sizeof(CalibSmem), st>>>(A, dls_tab, acc4);
+    return cudaGetLastError();
+}
+
 int bgki_blocks_per_sm() {
     int per_sm = 1;
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_bgki, kEvThreads, sizeof(BgkiSmem));
@@ -1068,7 +1250,9 @@ cudaError_t launch_ds_evidence(const Batch& bt, RayBuffers& rb, CellState cs, Ce
 long ds_count_bytes(long items) { return items * (long)kMaxTileCells; }
 
 cudaError_t evidence_init() {
-    return cudaFuncSetAttribute(k_bgki, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(BgkiSmem));
+    cudaError_t e = cudaFuncSetAttribute(k_bgki, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(BgkiSmem));
+    if (e != cudaSuccess) return e;
+    return cudaFuncSetAttribute(k_bgki_sums, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(CalibSmem));
 }
 
 }  // namespace k3dom

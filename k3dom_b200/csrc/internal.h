@@ -131,5 +131,10 @@ cudaError_t evidence_init();
 // Host: the sparse-kernel table (512 float4) for sigma, every value multiplied by scale.
 void build_kernel_table(float sigma, double scale, float4* out);
 constexpr int kKernelTableSize = 512;
+// Calibration: unit-amplitude kernel and -x f'(x) tables scaled to units of 2^-kCalibShift.
+constexpr int kCalibShift = 40;
+void build_calib_tables(float4* f_tab, float4* dls_tab);
+cudaError_t launch_bgki_sums(const Batch& bt, RayBuffers& rb, const float4* f_tab, const float4* dls_tab,
+                             unsigned long long* acc4, DevStatus* status, int num_sms, cudaStream_t st);
 
 }  // namespace k3dom

@@ -68,11 +68,15 @@ class Scene:
     def sensor_pos(self, t: float) -> np.ndarray:
         return self.ego_vel * t
 
-    def scan(self, frame: int, t: float, n_points: int) -> tuple[np.ndarray, np.ndarray]:
-        """(sensor position in the world [m], points (n, 3) float32 relative to the sensor)."""
+    def scan(self, frame: int, t: float, n_points: int, sensor_offset=None,
+             az_offset: float = 0.0) -> tuple[np.ndarray, np.ndarray]:
+        """(sensor position in the world [m], points (n, 3) float32 relative to the sensor).
+        sensor_offset moves the sensor off its trajectory; az_offset rotates the beam pattern."""
         s = self.sensor_pos(t)
+        if sensor_offset is not None:
+            s = s + np.asarray(sensor_offset, np.float64)
         n_az = -(-n_points // self.beams)
-        az = np.linspace(0.0, 2.0 * math.pi, n_az, endpoint=False)
+        az = np.linspace(0.0, 2.0 * math.pi, n_az, endpoint=False) + az_offset
         el = self.elev
         ce, se = np.cos(el), np.sin(el)
         d = np.stack([np.outer(ce, np.cos(az)), np.outer(ce, np.sin(az)), np.outer(se, np.ones_like(az))],
@@ -169,6 +173,43 @@ def config3(seed: int = 0, n_scenes: int = 16, variant: str = "k3dom") -> list:
         params = _k3dom_params(size, size_z, res, P, B, variant=variant, seed=5000 + k, max_points=n)
         out.append(Config(f"config3[{k}]", variant, params, sc, n, 100, 0.1))
     return out
+
+
+@dataclasses.dataclass
+class CalibConfig:
+    """The differentiable update's calibration problem: training frames (t, sensor, points) and
+    held-out scans (sensor, points), all sensor positions in the world frame."""
+    name: str
+    params: dict
+    train: list
+    heldout: list
+    theta0: tuple
+
+
+def config4(seed: int = 0, scale: str = "config0", n_heldout: int = 10) -> CalibConfig:
+    """config0's grid and scans (initialisation + one update) and 10 held-out 30,000-point scans
+    of the scene at the last training time from sensors displaced by up to 0.5 m, with rotated
+    beam patterns; theta0 = (ls 0.3 m, sigma 1.0, gamma 0.1, occupied prior 0.01, free prior 0.01).
+    scale="config1" uses config1's grid, particle counts and 120,000-point scans instead."""
+    base = config0(seed) if scale == "config0" else config1(seed)
+    rng = np.random.Generator(np.random.PCG64([seed, 4]))
+    params = dict(base.params)
+    theta0 = (0.3, 1.0, 0.1, 0.01, 0.01)
+    params.update(ls=theta0[0], sigma=theta0[1], gamma=theta0[2], prior_static=theta0[3] / 2,
+                  prior_dynamic=theta0[3] / 2, prior_free=theta0[4])
+    train = []
+    for f in range(2):
+        t = 0.1 + f * base.dt
+        s, pts = base.scene.scan(f, t, base.n_points)
+        train.append((t, s, pts))
+    t_last = train[-1][0]
+    heldout = []
+    for k in range(n_heldout):
+        off = rng.uniform(-0.5, 0.5, 3) * np.array([1.0, 1.0, 0.2])
+        s, pts = base.scene.scan(100 + k, t_last, 30000 if scale == "config0" else base.n_points,
+                                 sensor_offset=off, az_offset=float(rng.uniform(0, 2 * math.pi)))
+        heldout.append((s, pts))
+    return CalibConfig(f"config4[{scale}]", params, train, heldout, theta0)
 
 
 def small(seed: int = 0, variant: str = "k3dom", G: int = 32, Gz: int = 8, res: float = 0.2, P: int = 16384,

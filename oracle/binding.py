@@ -28,7 +28,8 @@ class OrcGrid(C.Structure):
 
 
 def build_oracle() -> Path:
-    if not ORACLE_SO.exists() or ORACLE_SO.stat().st_mtime < (HERE / "k3dom_oracle.c").stat().st_mtime:
+    srcs = [HERE / "k3dom_oracle.c", HERE / "k3dom_calib_oracle.c"]
+    if not ORACLE_SO.exists() or ORACLE_SO.stat().st_mtime < max(p.stat().st_mtime for p in srcs):
         subprocess.run(["make", "-C", str(HERE), "-s"], check=True)
     return ORACLE_SO
 
@@ -69,6 +70,12 @@ def oracle() -> C.CDLL:
         "orc_bgki_ref32": (None, [C.POINTER(OrcGrid), C.c_float, C.c_float, C.c_int, _F, _F, _F, _F, _F, _I]),
         "orc_k3dom_update_ref32": (None, [C.c_int, C.c_float, C.c_float, C.c_float, C.c_float, _F, _F, _F, _F, _F,
                                           _F, _F, _F, _F, _F, _F]),
+        "orc_bgki_sums": (None, [C.POINTER(OrcGrid), C.c_double, C.c_int, _F, _F, _F, _D, _D, _D, _D]),
+        "orc_calib_loss_grad": (C.c_double, [C.c_int64, C.c_int, _D, _F, _F, _I, _U, _U, _D, C.c_double,
+                                             C.c_void_p]),
+        "orc_calib_occupancy": (None, [C.c_int64, C.c_int, _D, _F, _F, _I, _D, C.c_double, _D]),
+        "orc_dda_labels": (None, [C.c_int, C.c_int, C.c_double, C.c_float, C.c_float, C.c_float, C.c_int, _F, _U,
+                                  _U]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)
@@ -433,3 +440,81 @@ class Reference:
         out = np.empty(u.size, np.int32)
         self.lib.ref_thrust_lower_bound(cum, cum.size, u, u.size, out)
         return out
+
+
+# ------------------------------------------------------------------ calibration (differentiable update)
+class OracleCalib:
+    """FP64 reference of the calibration loss (k3dom_bgki_forward/backward): per-cell kernel and
+    derivative sums (orc_bgki_sums), the mass recursion with forward-mode dual numbers
+    (orc_calib_loss_grad) and DDA labels (orc_dda_labels)."""
+
+    def __init__(self, G: int, Gz: int, res: float, mass_scale: float):
+        self.G, self.Gz, self.res, self.mass_scale = int(G), int(Gz), float(res), float(mass_scale)
+        self.C = self.G * self.G * self.Gz
+        self.frames = []  # (dt, sensor_rel (3,), pts (n, 3) float32, dyn (C,) float32 | None)
+        self.n0 = np.zeros(self.C, np.uint32)
+        self.n1 = np.zeros(self.C, np.uint32)
+        self._sums = {}
+
+    def add_frame(self, dt, sensor, pts, dyn=None):
+        self.frames.append((float(dt), np.asarray(sensor, np.float32), np.ascontiguousarray(pts, np.float32),
+                            None if dyn is None else np.ascontiguousarray(dyn, np.float32)))
+        self._sums.clear()
+
+    def add_heldout(self, sensor, pts):
+        pts = np.ascontiguousarray(pts, np.float32).reshape(-1)
+        oracle().orc_dda_labels(self.G, self.Gz, self.res, float(sensor[0]), float(sensor[1]), float(sensor[2]),
+                                pts.size // 3, pts, self.n0, self.n1)
+
+    def sums(self, ls: float) -> np.ndarray:
+        """F x 4 x C: sum f occ, sum f free, sum -x f' occ, sum -x f' free."""
+        key = float(ls)
+        if key in self._sums:
+            return self._sums[key]
+        out = np.zeros((len(self.frames), 4, self.C), np.float64)
+        for k, (dt, s, pts, dyn) in enumerate(self.frames):
+            g = OrcGrid(self.G, self.Gz, self.res, float(s[0]), float(s[1]), float(s[2]))
+            xs = np.ascontiguousarray(pts[:, 0])
+            ys = np.ascontiguousarray(pts[:, 1])
+            zs = np.ascontiguousarray(pts[:, 2])
+            oracle().orc_bgki_sums(C.byref(g), key, xs.size, xs, ys, zs, out[k, 0], out[k, 1], out[k, 2], out[k, 3])
+        self._sums[key] = out
+        return out
+
+    def _frame_arrays(self):
+        F = len(self.frames)
+        dt = np.array([f[0] for f in self.frames], np.float32)
+        present = np.array([0 if f[3] is None else 1 for f in self.frames], np.int32)
+        dyn = np.zeros((F, self.C), np.float32)
+        for k, f in enumerate(self.frames):
+            if f[3] is not None:
+                dyn[k] = f[3]
+        return F, dt, dyn, present
+
+    def loss_grad(self, theta, want_grad=True):
+        th = np.ascontiguousarray(theta, np.float64)
+        s = np.ascontiguousarray(self.sums(th[0]))
+        F, dt, dyn, present = self._frame_arrays()
+        g = np.zeros(5, np.float64)
+        loss = oracle().orc_calib_loss_grad(self.C, F, s, dt, dyn, present, self.n0, self.n1, th, self.mass_scale,
+                                            g.ctypes.data if want_grad else None)
+        return loss, g
+
+    def occupancy(self, theta):
+        th = np.ascontiguousarray(theta, np.float64)
+        s = np.ascontiguousarray(self.sums(th[0]))
+        F, dt, dyn, present = self._frame_arrays()
+        p = np.zeros(self.C, np.float64)
+        oracle().orc_calib_occupancy(self.C, F, s, dt, dyn, present, th, self.mass_scale, p)
+        return p
+
+    def fd_grad(self, theta, h=1e-4):
+        """FP64 central finite differences of the loss, step h in every parameter."""
+        th = np.asarray(theta, np.float64)
+        g = np.zeros(5)
+        for i in range(5):
+            a, b = th.copy(), th.copy()
+            a[i] += h
+            b[i] -= h
+            g[i] = (self.loss_grad(a, False)[0] - self.loss_grad(b, False)[0]) / (2 * h)
+        return g

@@ -324,6 +324,127 @@ void orc_bgki(const orc_grid* g, float ls, float sigma, int n, const float* xs, 
     }
 }
 
+/* ------------------------------------------------------------------ calibration sums (FP64) */
+/* Unit-amplitude kernel f(x) of mass_update.cu:24-26 and -x f'(x), the per-pair quantities of
+ * the calibration loss's evidence and of its length-scale derivative (x = d / ls). */
+static double unit_f(double x) {
+    double v = (2.0 + cos(M_PI * 2.0 * x)) * (1.0 - x) / 3.0 + sin(M_PI * 2.0 * x) / (2.0 * 3.141592);
+    return v > 0.0 ? v : 0.0;
+}
+static double unit_mxfp(double x) {
+    double v = (2.0 + cos(M_PI * 2.0 * x)) * (1.0 - x) / 3.0 + sin(M_PI * 2.0 * x) / (2.0 * 3.141592);
+    if (!(v > 0.0)) return 0.0;
+    double fp = (-2.0 * M_PI * sin(M_PI * 2.0 * x) * (1.0 - x) - (2.0 + cos(M_PI * 2.0 * x))) / 3.0 +
+                2.0 * M_PI * cos(M_PI * 2.0 * x) / (2.0 * 3.141592);
+    return -x * fp;
+}
+
+/* Distances of one (cell, point) pair as BGKI forms them (mass_update.cu:43-71): to the point
+ * (occupied) and to the free segment when d_proj < d_m. */
+static void pair_distances(double cx, double cy, double cz, double mx, double my, double mz, double res,
+                           double* d_occ, double* d_free, int* has_free) {
+    double dx = cx - mx, dy = cy - my, dz = cz - mz;
+    *d_occ = sqrt(dx * dx + dy * dy + dz * dz);
+    *has_free = 0;
+    double dc = sqrt(cx * cx + cy * cy + cz * cz);
+    double dm = sqrt(mx * mx + my * my + mz * mz);
+    if (!(dm > 0.0)) return;
+    double dp = (cx * mx + cy * my + cz * mz) / dm;
+    double marg = fmax(0.9 * dm, dm - 2.0 * res);
+    double df;
+    if (dp <= 0.0) {
+        df = dc;
+    } else if (dp < marg) {
+        double q = dc * dc - dp * dp;
+        df = sqrt(q > 0.0 ? q : 0.0);
+    } else {
+        double r = marg / dm;
+        double ex = cx - r * mx, ey = cy - r * my, ez = cz - r * mz;
+        df = sqrt(ex * ex + ey * ey + ez * ez);
+    }
+    *d_free = df;
+    *has_free = dp < dm;
+}
+
+/* Per cell: sum f(x) and sum -x f'(x) over the occupied pairs (Fo, Ho) and the free pairs
+ * (Ff, Hf) within ls; enumeration as orc_bgki. */
+void orc_bgki_sums(const orc_grid* g, double ls, int n, const float* xs, const float* ys, const float* zs,
+                   double* Fo, double* Ff, double* Ho, double* Hf) {
+    const int G = g->G, Gz = g->Gz;
+    const int64_t C = (int64_t)G * G * Gz;
+    memset(Fo, 0, sizeof(double) * C);
+    memset(Ff, 0, sizeof(double) * C);
+    memset(Ho, 0, sizeof(double) * C);
+    memset(Hf, 0, sizeof(double) * C);
+    const double res = g->res;
+    const double R = ls / res + 1e-6;
+    const double au[3] = {(double)g->sx / res + G / 2.0 - 0.5, (double)g->sy / res + G / 2.0 - 0.5,
+                          (double)g->sz / res + Gz / 2.0 - 0.5};
+    const int dims[3] = {G, G, Gz};
+#pragma omp parallel for schedule(dynamic, 64)
+    for (int i = 0; i < n; ++i) {
+        const double m[3] = {xs[i], ys[i], zs[i]};
+        if (!isfinite(m[0]) || !isfinite(m[1]) || !isfinite(m[2])) continue;
+        const double bu[3] = {au[0] + m[0] / res, au[1] + m[1] / res, au[2] + m[2] / res};
+        const double d[3] = {bu[0] - au[0], bu[1] - au[1], bu[2] - au[2]};
+        int A = 0;
+        if (fabs(d[1]) > fabs(d[A])) A = 1;
+        if (fabs(d[2]) > fabs(d[A])) A = 2;
+        const int Bx = (A + 1) % 3, Cx = (A + 2) % 3;
+        int lo = (int)floor(fmin(au[A], bu[A]) - R), hi = (int)ceil(fmax(au[A], bu[A]) + R);
+        if (lo < 0) lo = 0;
+        if (hi > dims[A] - 1) hi = dims[A] - 1;
+        for (int ia = lo; ia <= hi; ++ia) {
+            double t0 = 0.0, t1 = 1.0;
+            if (d[A] != 0.0) {
+                double e0 = (ia - R - au[A]) / d[A], e1 = (ia + R - au[A]) / d[A];
+                t0 = fmax(t0, fmin(e0, e1));
+                t1 = fmin(t1, fmax(e0, e1));
+                if (t0 > t1) continue;
+            } else if (fabs(ia - au[A]) > R) {
+                continue;
+            }
+            double b0 = au[Bx] + d[Bx] * t0, b1 = au[Bx] + d[Bx] * t1;
+            double c0 = au[Cx] + d[Cx] * t0, c1 = au[Cx] + d[Cx] * t1;
+            int ib0 = (int)floor(fmin(b0, b1) - R), ib1 = (int)ceil(fmax(b0, b1) + R);
+            int ic0 = (int)floor(fmin(c0, c1) - R), ic1 = (int)ceil(fmax(c0, c1) + R);
+            if (ib0 < 0) ib0 = 0;
+            if (ic0 < 0) ic0 = 0;
+            if (ib1 > dims[Bx] - 1) ib1 = dims[Bx] - 1;
+            if (ic1 > dims[Cx] - 1) ic1 = dims[Cx] - 1;
+            for (int ib = ib0; ib <= ib1; ++ib)
+                for (int ic = ic0; ic <= ic1; ++ic) {
+                    int idx3[3];
+                    idx3[A] = ia;
+                    idx3[Bx] = ib;
+                    idx3[Cx] = ic;
+                    float cxf, cyf, czf;
+                    centre_f(g, idx3[0], idx3[1], idx3[2], &cxf, &cyf, &czf);
+                    double dof, dfr;
+                    int hf;
+                    pair_distances(cxf, cyf, czf, m[0], m[1], m[2], res, &dof, &dfr, &hf);
+                    const int occ_in = dof < ls, free_in = hf && dfr < ls;
+                    if (!occ_in && !free_in) continue;
+                    int64_t c = idx3[0] + (int64_t)G * idx3[1] + (int64_t)G * G * idx3[2];
+                    if (occ_in) {
+                        double x = dof / ls, a = unit_f(x), b = unit_mxfp(x);
+#pragma omp atomic
+                        Fo[c] += a;
+#pragma omp atomic
+                        Ho[c] += b;
+                    }
+                    if (free_in) {
+                        double x = dfr / ls, a = unit_f(x), b = unit_mxfp(x);
+#pragma omp atomic
+                        Ff[c] += a;
+#pragma omp atomic
+                        Hf[c] += b;
+                    }
+                }
+        }
+    }
+}
+
 /* ------------------------------------------------------------------ K3DOM cell update (FP64) */
 static double credit_d(double mass, double ms) { return 1.0 - 2.0 / (1.0 + exp(2.0 * mass / ms)); }
 static double pdiff(double a, double b) { return a - b > 0.0 ? a - b : 0.0; }
