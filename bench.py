@@ -316,6 +316,9 @@ def run_ours(args):
     e2e_fps = world * n_e2e / e2e_s
 
     value = world * 1000.0 / ms_max
+    batch_res = None
+    if not args.no_batch:
+        batch_res = run_batch(args, local, rank, world, dist)
     out = None
     if rank == 0:
         hbm_peak, peak_src = read_peaks()
@@ -364,8 +367,8 @@ def run_ours(args):
             },
             "stage_ms": {k: round(v, 4) for k, v in stage.items()},
         }
-        if world == 1 and not args.no_batch:
-            out["batched"] = run_batch(args, local)
+        if batch_res is not None:
+            out["batched"] = batch_res
         if world == 1 and not args.no_grad:
             out["grad_step"] = run_grad_step(args, local, frame_ms=ms_max)
         if world == 1 and not args.no_cpu_baseline:
@@ -437,27 +440,39 @@ def run_reference_gpu(args):
                                              "(its own updateGrid, host vectors in, synchronising)"}}), flush=True)
 
 
-def run_batch(args, local: int = 0) -> dict:
+def run_batch(args, local: int = 0, rank: int = 0, world: int = 1, dist=None) -> dict:
     """Batched form: 16 independent scenes (k3dom_b200.scene.config3) updated together by one
     BatchDOM (one launch per stage, graph-replayed, evidence tiling autotuned on live frames)
     against the plain form looping over the same 16 scenes with one DOM each. Aggregate frames/s
     = scenes x frames / time. Both arms take the same host scans and run synchronous calls (the
     reference's updateGrid synchronises, src/k3dom/dom.cu:47); time = host clock around the
-    timed frames. The device-resident rows feed the scans from HBM instead."""
+    timed frames. The device-resident rows feed the scans from HBM instead. With several ranks
+    the scenes are partitioned by estimated cost (k3dom_b200.shard) and each rank runs its own
+    share; time = max over ranks."""
     import torch
 
     import k3dom_b200 as K
-    from k3dom_b200 import scene
-    cfgs = scene.config3(seed=args.batch_seed, n_scenes=args.scenes, variant=args.variant)
+    from k3dom_b200 import scene, shard
+    all_cfgs = scene.config3(seed=args.batch_seed, n_scenes=args.scenes, variant=args.variant)
+    mine = shard.my_scenes([shard.scene_cost(c.params, c.n_points) for c in all_cfgs], rank, world)
+    cfgs = [all_cfgs[i] for i in mine]
     S = len(cfgs)
     W, Kst = 2, args.batch_steps
     n_frames = 1 + W + Kst
-    log(f"batch: generating {S} x {n_frames} scans ({sum(c.n_points for c in cfgs)} points per frame)")
+    log(f"[rank {rank}] batch: generating {S} x {n_frames} scans")
     frames = [make_frames(c, n_frames) for c in cfgs]  # frames[s][f] = (t, sensor, pts)
     params = [K.make_params(args.variant, **c.params) for c in cfgs]
     dev = f"cuda:{local}"
     dev_pts = [[torch.from_numpy(fr[2]).to(dev) for fr in frames[s]] for s in range(S)]
     torch.cuda.synchronize()
+
+    def timed_region(run_frames) -> float:
+        barrier(dist)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        run_frames()
+        torch.cuda.synchronize()
+        return max_over_ranks(time.perf_counter() - t0, dist)
 
     def plain_arm(device_resident: bool) -> float:
         doms = [K.DOM(p, args.variant, device=local) for p in params]
@@ -473,41 +488,34 @@ def run_batch(args, local: int = 0) -> dict:
                         d.updateGrid(t, pts)
             for f in range(1 + W):
                 frame(f)
-            torch.cuda.synchronize()
-            t0 = time.perf_counter()
-            for f in range(1 + W, n_frames):
-                frame(f)
-            torch.cuda.synchronize()
-            return S * Kst / (time.perf_counter() - t0)
+
+            def timed():
+                for f in range(1 + W, n_frames):
+                    frame(f)
+            return timed_region(timed)
         finally:
             for d in doms:
                 d.close()
 
     def batch_arm(device_resident: bool):
+        if S == 0:
+            return timed_region(lambda: None), None, 0
         b = K.BatchDOM(params, args.variant, device=local)
         try:
-            def frame(f, g=None):
-                g = f if g is None else g
-                for s in range(S):
-                    b.updatePose(s, *frames[s][f][1])
-                ts = [frames[s][f][0] for s in range(S)]
-                if device_resident:
-                    b.update_async(ts, [dev_pts[s][g] for s in range(S)])
-                    b.synchronize()
-                else:
-                    b.update(ts, [frames[s][g][2] for s in range(S)])
-            frame(0)
+            for s in range(S):
+                b.updatePose(s, *frames[s][0][1])
+            b.update([frames[s][0][0] for s in range(S)], [frames[s][0][2] for s in range(S)])
             # autotune on live frames (replaying frame 1's scans as the clock advances)
             b.autotune(True)
             tune_frames = b.tuning()["candidates"]
             for k in range(tune_frames):
                 for s in range(S):
                     b.updatePose(s, *frames[s][1][1])
-                ts = [frames[s][1][0] + 0.1 * k for s in range(S)]
-                b.update(ts, [frames[s][1][2] for s in range(S)])
+                b.update([frames[s][1][0] + 0.1 * k for s in range(S)], [frames[s][1][2] for s in range(S)])
             tuning = b.tuning()
             t_shift = 0.1 * tune_frames
-            def timed_frame(f):
+
+            def frame(f):
                 for s in range(S):
                     b.updatePose(s, *frames[s][f][1])
                 ts = [frames[s][f][0] + t_shift for s in range(S)]
@@ -517,39 +525,43 @@ def run_batch(args, local: int = 0) -> dict:
                 else:
                     b.update(ts, [frames[s][f][2] for s in range(S)])
             for f in range(1, 1 + W):
-                timed_frame(f)
-            torch.cuda.synchronize()
-            t0 = time.perf_counter()
-            for f in range(1 + W, n_frames):
-                timed_frame(f)
-            torch.cuda.synchronize()
-            fps = S * Kst / (time.perf_counter() - t0)
-            launches = b.diagnostics()["kernel_launches_per_frame"]
-            return fps, tuning, launches
+                frame(f)
+
+            def timed():
+                for f in range(1 + W, n_frames):
+                    frame(f)
+            secs = timed_region(timed)
+            return secs, tuning, b.diagnostics()["kernel_launches_per_frame"]
         finally:
             b.close()
 
-    plain_host = plain_arm(False)
-    plain_dev = plain_arm(True)
-    batch_host, tuning, launches = batch_arm(False)
-    batch_dev, _, _ = batch_arm(True)
+    total = len(all_cfgs) * Kst
+    plain_host = total / (plain_arm(False) if S else timed_region(lambda: None))
+    plain_dev = total / (plain_arm(True) if S else timed_region(lambda: None))
+    bh, tuning, launches = batch_arm(False)
+    bd, _, _ = batch_arm(True)
+    batch_host, batch_dev = total / bh, total / bd
     rules = ["by-size", "8x8x4", "16x16x4", "16x16x8"]
     return {
-        "workload": f"config3: {S} independent {args.variant} scenes, G 64-256, Gz 16-32, P 2^18-2^22, "
-                    f"B=P/4, 10k-200k points; {Kst} timed frames after {W} warm-up",
-        "scenes": S, "frames": Kst, "unit": "aggregate frames/s",
+        "workload": f"config3: {len(all_cfgs)} independent {args.variant} scenes, G 64-256, Gz 16-32, "
+                    f"P 2^18-2^22, B=P/4, 10k-200k points; {Kst} timed frames after {W} warm-up",
+        "scenes": len(all_cfgs), "frames": Kst, "unit": "aggregate frames/s", "ranks": world,
+        "scenes_per_rank": [len(p) for p in shard.partition(
+            [shard.scene_cost(c.params, c.n_points) for c in all_cfgs], world)],
         "voxels_total": int(sum(int(np.float32(c.params["size"]) / np.float32(0.1)) ** 2 *
-                                int(np.float32(c.params["size_z"]) / np.float32(0.1)) for c in cfgs)),
-        "particles_total": int(sum(c.params["particle_count"] for c in cfgs)),
-        "points_per_frame_total": int(sum(c.n_points for c in cfgs)),
+                                int(np.float32(c.params["size_z"]) / np.float32(0.1)) for c in all_cfgs)),
+        "particles_total": int(sum(c.params["particle_count"] for c in all_cfgs)),
+        "points_per_frame_total": int(sum(c.n_points for c in all_cfgs)),
         "plain_loop": round(plain_host, 2), "batched": round(batch_host, 2),
         "speedup": round(batch_host / plain_host, 3),
         "plain_loop_device_resident": round(plain_dev, 2), "batched_device_resident": round(batch_dev, 2),
         "speedup_device_resident": round(batch_dev / plain_dev, 3),
         "batched_launches_per_frame": int(launches),
-        "tuning": {"tile_rule": rules[tuning["tile_rule"]], "chunk": tuning["chunk"],
-                   "candidate_ms": [round(x, 3) for x in tuning["candidate_ms"]]},
-        "timing": "host clock around synchronous calls (both arms), host scans unless device_resident",
+        "tuning": None if tuning is None else {
+            "tile_rule": rules[tuning["tile_rule"]], "chunk": tuning["chunk"],
+            "candidate_ms": [round(x, 3) for x in tuning["candidate_ms"]]},
+        "timing": "host clock around synchronous calls (both arms), max over ranks; host scans unless "
+                  "device_resident",
     }
 
 

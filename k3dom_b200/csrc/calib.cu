@@ -457,17 +457,20 @@ TileShape calib_tiles(const DevParams& p) {
     return t;
 }
 
-// Ray buffers for the largest frame at length-scale ls (re-made when either grows).
+// Ray buffers for the largest frame at the scene's length-scale: re-made only when the point
+// count or the worst-case list length outgrows them, then with 25 % headroom, so a calibration
+// loop that moves ls a little does not reallocate.
 cudaError_t ensure_ray_buffers(k3dom_calib* c, int max_points, float ls, const SceneDev& sd) {
-    if (max_points <= c->ray_points && ls <= c->ray_ls && c->rb.ekeys) return cudaSuccess;
+    const int T = sd.ts.ntx * sd.ts.nty * sd.ts.ntz;
+    long need = std::max(ray_entries_bound(sd.p, sd.ts, std::max(max_points, 1), sd.bin_R), 4096L);
+    if (need > 0xFFFFFFF0L) need = 0xFFFFFFF0L;
+    if (max_points <= c->ray_points && need <= c->rb.capacity && c->rb.ekeys) return cudaSuccess;
     for (void* p : c->ray_allocs) cudaFree(p);
     c->ray_allocs.clear();
     RayBuffers& rb = c->rb;
     rb = RayBuffers{};
     const int N = std::max(max_points, 1);
-    const int T = sd.ts.ntx * sd.ts.nty * sd.ts.ntz;
-    long cap = std::max(ray_entries_bound(sd.p, sd.ts, N, sd.bin_R), 4096L);
-    if (cap > 0xFFFFFFF0L) cap = 0xFFFFFFF0L;
+    long cap = std::min(need + need / 4, 0xFFFFFFF0L);
     rb.capacity = cap;
     rb.chunk = 1024;
     std::vector<void*>* L = &c->ray_allocs;
