@@ -226,7 +226,8 @@ def run_ours(args):
     torch.cuda.set_device(local)
     cfg = scene_cfg(args.variant, rank)
     W, Kst = args.warmup, args.steps
-    n_frames = 1 + W + Kst + 2 + Kst + 1 + Kst
+    n_tune = 8  # evidence autotuner: one live frame per candidate (k3dom_autotune)
+    n_frames = 1 + n_tune + W + Kst + 2 + Kst + 1 + Kst
     log(f"[rank {rank}] generating {n_frames} scans of {cfg.n_points} points")
     frames = make_frames(cfg, n_frames)
     p = K.make_params(args.variant, **cfg.params)
@@ -242,11 +243,21 @@ def run_ours(args):
         dom.updatePose(*s)
         dom.updateGridAsync(t, dev_pts[i])
 
-    # first frame (initialisation) + warm-up, graph captured on the first steady frame
+    # first frame (initialisation), the autotuner's frames, then warm-up; the graph is captured on
+    # the first steady frame after tuning
     dom.set_graph_mode(True)
     dom.updatePose(*frames[0][1])
     dom.updateGrid(frames[0][0], dev_pts[0])
     idx = 1
+    if args.tile_rule is None:
+        dom.autotune(True)
+        for _ in range(dom.tuning()["candidates"]):
+            step_device(idx)
+            idx += 1
+    else:
+        dom.set_tuning(args.tile_rule, args.chunk)
+    dom.synchronize()
+    tuning = dom.tuning()
     for _ in range(W):
         step_device(idx)
         idx += 1
@@ -290,6 +301,7 @@ def run_ours(args):
         st_acc.append(dom.stage_times())
         evals.append(dom.diagnostics()["kernel_evaluations"])
     dom.set_timing(False)
+    diag_after = dom.diagnostics()
     stage = {k: float(np.mean([s[k] for s in st_acc])) for k in st_acc[0]}
 
     # end to end through the C ABI: pinned host scan in, per-voxel occupancy out, every frame
@@ -345,7 +357,7 @@ def run_ours(args):
                 "voxels": C_, "particles": P, "new_born": B, "points_per_frame": cfg.n_points,
                 "parallelism": f"replicas x{world} (independent scenes)",
                 "l2": "state > L2 (about 1 GB of particle/cell arrays touched per frame)",
-                "graph": True,
+                "graph": True, "evidence_tiling": "autotuned (k3dom_autotune) during warm-up",
             },
             "e2e": {"value": round(e2e_fps, 3), "unit": UNIT, "h2d_bytes_per_step": int(cfg.n_points * 12),
                     "d2h_bytes_per_step": int(C_ * 4)},
@@ -366,6 +378,10 @@ def run_ours(args):
                 "peak_source": peak_src, "algorithmic_bytes": int(part_bytes), "time_ms": round(part_ms, 4),
             },
             "stage_ms": {k: round(v, 4) for k, v in stage.items()},
+            "evidence_lists": {k: diag_after[k] for k in ("ray_list_entries", "ray_list_capacity", "work_items",
+                                                           "kernel_evaluations")},
+            "tuning": {"tile_rule": ["by-size", "8x8x4", "16x16x4", "16x16x8"][tuning["tile_rule"]],
+                       "chunk": tuning["chunk"], "candidate_ms": [round(x, 3) for x in tuning["candidate_ms"]]},
         }
         if batch_res is not None:
             out["batched"] = batch_res
@@ -627,6 +643,8 @@ def run_profile_case(args):
     cfg.scene.max_range = 12.8
     p = K.make_params(args.variant, **cfg.params)
     dom = K.DOM(p, args.variant)
+    if args.profile_tile_rule is not None:
+        dom.set_tuning(args.profile_tile_rule, 1024)
     for f in range(1 + args.steps):
         t = 0.1 + f * cfg.dt
         s, pts = cfg.scene.scan(f, t, cfg.n_points)
@@ -650,6 +668,11 @@ def main(argv=None):
                     help="batch: only the batched-vs-plain line (16 scenes); grad: only the gradient step")
     ap.add_argument("--no-batch", action="store_true", help="skip the batched-vs-plain measurement")
     ap.add_argument("--no-grad", action="store_true", help="skip the gradient-step measurement")
+    ap.add_argument("--tile-rule", type=int, default=None,
+                    help="fixed evidence tile rule instead of autotuning (0 by size, 1 8x8x4, 2 16x16x4, 3 16x16x8)")
+    ap.add_argument("--chunk", type=int, default=1024, help="rays per evidence work item with --tile-rule")
+    ap.add_argument("--profile-tile-rule", type=int, default=None,
+                    help="profile case: evidence tile rule (0 by size, 1 8x8x4, 2 16x16x4, 3 16x16x8)")
     ap.add_argument("--scenes", type=int, default=16)
     ap.add_argument("--batch-steps", type=int, default=5)
     ap.add_argument("--batch-seed", type=int, default=0)

@@ -430,7 +430,8 @@ struct k3dom_calib {
         cudaError_t e = cudaMalloc((void**)p, std::max<size_t>(count, 1) * sizeof(T));
         if (e != cudaSuccess) return e;
         (list ? list : &allocs)->push_back((void*)*p);
-        return cudaMemset(*p, 0, std::max<size_t>(count, 1) * sizeof(T));
+        // on the problem's (non-blocking) stream, so it is ordered before the work that uses it
+        return cudaMemsetAsync(*p, 0, std::max<size_t>(count, 1) * sizeof(T), st);
     }
     void release() {
         for (void* p : ray_allocs) cudaFree(p);
@@ -674,8 +675,9 @@ k3dom_status k3dom_calib_create(const k3dom_params* base, int device, k3dom_cali
         return bail(e);
     std::vector<float4> ft(kKernelTableSize), ht(kKernelTableSize);
     build_calib_tables(ft.data(), ht.data());
-    if ((e = cudaMemcpy(c->ftab, ft.data(), sizeof(float4) * ft.size(), cudaMemcpyHostToDevice)) ||
-        (e = cudaMemcpy(c->htab, ht.data(), sizeof(float4) * ht.size(), cudaMemcpyHostToDevice)))
+    if ((e = cudaMemcpyAsync(c->ftab, ft.data(), sizeof(float4) * ft.size(), cudaMemcpyHostToDevice, c->st)) ||
+        (e = cudaMemcpyAsync(c->htab, ht.data(), sizeof(float4) * ht.size(), cudaMemcpyHostToDevice, c->st)) ||
+        (e = cudaStreamSynchronize(c->st)))
         return bail(e);
     *out = c;
     return K3DOM_OK;
@@ -754,8 +756,9 @@ k3dom_status k3dom_calib_add_heldout_scan(k3dom_calib* c, float sx, float sy, fl
     }
     // total label instances
     std::vector<uint32_t> h0(c->dp.C), h1(c->dp.C);
-    if ((e = cudaMemcpy(h0.data(), c->n0, sizeof(uint32_t) * h0.size(), cudaMemcpyDeviceToHost)) ||
-        (e = cudaMemcpy(h1.data(), c->n1, sizeof(uint32_t) * h1.size(), cudaMemcpyDeviceToHost)))
+    if ((e = cudaMemcpyAsync(h0.data(), c->n0, sizeof(uint32_t) * h0.size(), cudaMemcpyDeviceToHost, c->st)) ||
+        (e = cudaMemcpyAsync(h1.data(), c->n1, sizeof(uint32_t) * h1.size(), cudaMemcpyDeviceToHost, c->st)) ||
+        (e = cudaStreamSynchronize(c->st)))
         return c->fail(e);
     double tot = 0.0;
     for (size_t i = 0; i < h0.size(); ++i) tot += (double)h0[i] + (double)h1[i];
@@ -768,8 +771,9 @@ k3dom_status k3dom_calib_label_counts(k3dom_calib* c, uint32_t* n0, uint32_t* n1
     cudaSetDevice(c->device);
     const cudaMemcpyKind k = mem == K3DOM_MEM_HOST ? cudaMemcpyDeviceToHost : cudaMemcpyDeviceToDevice;
     cudaError_t e = cudaSuccess;
-    if (n0) e = cudaMemcpy(n0, c->n0, sizeof(uint32_t) * (size_t)c->dp.C, k);
-    if (e == cudaSuccess && n1) e = cudaMemcpy(n1, c->n1, sizeof(uint32_t) * (size_t)c->dp.C, k);
+    if (n0) e = cudaMemcpyAsync(n0, c->n0, sizeof(uint32_t) * (size_t)c->dp.C, k, c->st);
+    if (e == cudaSuccess && n1) e = cudaMemcpyAsync(n1, c->n1, sizeof(uint32_t) * (size_t)c->dp.C, k, c->st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(c->st);
     return e == cudaSuccess ? K3DOM_OK : c->fail(e);
 }
 
@@ -779,8 +783,10 @@ k3dom_status k3dom_calib_get_sums(k3dom_calib* c, float ls, int32_t frame, doubl
     k3dom_status s = compute_sums(c, ls);
     if (s != K3DOM_OK) return s;
     const size_t C = (size_t)c->dp.C;
-    cudaError_t e = cudaMemcpy(out, c->sums + (size_t)frame * 4 * C, sizeof(double) * 4 * C,
-                               mem == K3DOM_MEM_HOST ? cudaMemcpyDeviceToHost : cudaMemcpyDeviceToDevice);
+    cudaError_t e = cudaMemcpyAsync(out, c->sums + (size_t)frame * 4 * C, sizeof(double) * 4 * C,
+                                    mem == K3DOM_MEM_HOST ? cudaMemcpyDeviceToHost : cudaMemcpyDeviceToDevice,
+                                    c->st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(c->st);
     return e == cudaSuccess ? K3DOM_OK : c->fail(e);
 }
 
@@ -798,7 +804,8 @@ k3dom_status k3dom_bgki_forward(k3dom_calib* c, const float* theta, float* loss,
     }
     k3dom_status s = run_cells(c, theta, false, occ_dev);
     if (s == K3DOM_OK && occupancy && mem == K3DOM_MEM_HOST) {
-        e = cudaMemcpy(occupancy, occ_dev, sizeof(float) * (size_t)c->dp.C, cudaMemcpyDeviceToHost);
+        e = cudaMemcpyAsync(occupancy, occ_dev, sizeof(float) * (size_t)c->dp.C, cudaMemcpyDeviceToHost, c->st);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(c->st);
         if (e != cudaSuccess) s = c->fail(e);
     }
     if (occupancy && mem == K3DOM_MEM_HOST && occ_dev) {

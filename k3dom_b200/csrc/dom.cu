@@ -162,7 +162,9 @@ struct k3dom_handle {
         cudaError_t e = cudaMalloc((void**)p, count * sizeof(T));
         if (e != cudaSuccess) return e;
         (list ? list : &allocs)->push_back((void*)*p);
-        if (zero) e = cudaMemset(*p, 0, count * sizeof(T));
+        // zero on the handle's stream: it is non-blocking, so a memset on the legacy default stream
+        // would not be ordered before the handle's own work on the buffer
+        if (zero) e = cudaMemsetAsync(*p, 0, count * sizeof(T), st);
         return e;
     }
     cudaError_t alloc_particles(Particles* q, int n) {
@@ -327,11 +329,14 @@ cudaError_t layout_points_tiles(k3dom_handle* h) {
         x.bin_R = d.bin_R;
     }
     cudaError_t e;
-    if ((e = cudaMemcpy(h->sc_dev, sd.data(), sizeof(SceneDev) * sd.size(), cudaMemcpyHostToDevice))) return e;
-    if ((e = cudaMemcpy(h->off_dev, &h->off, sizeof(SceneOffsets), cudaMemcpyHostToDevice))) return e;
-    if (h->rb.ktab)
-        e = cudaMemcpy(h->rb.ktab, tabs.data(), sizeof(float4) * tabs.size(), cudaMemcpyHostToDevice);
-    return e;
+    // on the handle's stream (ordered before its kernels), then waited for: the sources are locals
+    if ((e = cudaMemcpyAsync(h->sc_dev, sd.data(), sizeof(SceneDev) * sd.size(), cudaMemcpyHostToDevice, h->st)))
+        return e;
+    if ((e = cudaMemcpyAsync(h->off_dev, &h->off, sizeof(SceneOffsets), cudaMemcpyHostToDevice, h->st))) return e;
+    if (h->rb.ktab &&
+        (e = cudaMemcpyAsync(h->rb.ktab, tabs.data(), sizeof(float4) * tabs.size(), cudaMemcpyHostToDevice, h->st)))
+        return e;
+    return cudaStreamSynchronize(h->st);
 }
 
 // Buffers sized by the point slots and tiles: ray data, entry lists, tile lists, points.
@@ -790,8 +795,11 @@ k3dom_status k3dom_batch_create(const k3dom_params* params, int32_t n_scenes, k3
         h->plan_born_n = (int)pb.size();
         h->plan_joint_n = (int)pj.size();
         if ((e = h->alloc(&h->plan_born, pb.size())) || (e = h->alloc(&h->plan_joint, pj.size()))) return bail(e);
-        if ((e = cudaMemcpy(h->plan_born, pb.data(), sizeof(ExactTile) * pb.size(), cudaMemcpyHostToDevice)) ||
-            (e = cudaMemcpy(h->plan_joint, pj.data(), sizeof(ExactTile) * pj.size(), cudaMemcpyHostToDevice)))
+        if ((e = cudaMemcpyAsync(h->plan_born, pb.data(), sizeof(ExactTile) * pb.size(), cudaMemcpyHostToDevice,
+                                 h->st)) ||
+            (e = cudaMemcpyAsync(h->plan_joint, pj.data(), sizeof(ExactTile) * pj.size(), cudaMemcpyHostToDevice,
+                                 h->st)) ||
+            (e = cudaStreamSynchronize(h->st)))
             return bail(e);
         const size_t sb = exact_plan_scratch_bytes(std::max(h->plan_born_n, h->plan_joint_n));
         unsigned char* es = nullptr;

@@ -604,6 +604,7 @@ struct BgkiSmem {
     float4 a[kChunk];             // m.x, m.y, m.z, d_m
     double4 c[kChunk];            // d_m, margin, 1/d_m
     float4 stage[kEvWarps][32][3];
+    float near[kEvWarps][32];     // 1 where the point's sphere can reach the sub-block
 };
 
 // Pair geometry. For the anchor o of a sub-block and a ray m (FP64, once per lane-ray):
@@ -664,6 +665,7 @@ __global__ void __launch_bounds__(kEvThreads, 3) k_bgki(EvArgs A) {
             if (sb >= nsb) break;
             const CellLoc L = locate(p, ts, it.lt, sb, lane, fp.sensor_x, fp.sensor_y, fp.sensor_z);
             const float dx = L.x - L.ox, dy = L.y - L.oy, dz = L.z - L.oz;  // exact (nearby floats)
+            const float ls2c = L.c >= 0 ? ls2 : -1.0f;  // cells outside the grid take no evidence
             const double ox = L.ox, oy = L.oy, oz = L.oz;
             double ao = 0.0, af = 0.0;  // exact sums of integer units (< 2^52 per chunk)
             for (int g0 = 0; g0 < nr; g0 += 32) {
@@ -684,10 +686,14 @@ __global__ void __launch_bounds__(kEvThreads, 3) k_bgki(EvArgs A) {
                     const float qal = fminf(qpar, 0.0f) + fmaxf(qpar - a.w, 0.0f);
                     hit = qx * qx + qy * qy + qz * qz + qal * qal < cull_r2;
                     if (hit) {
+                        const float ex = (float)(ox - a.x), ey = (float)(oy - a.y), ez = (float)(oz - a.z);
+                        // the point's sphere can reach the sub-block only if the point lies within
+                        // the cull radius of the sub-block's centroid
+                        const float cx = ex - hres, cy = ey - hres, cz = ez - hres;
                         S.stage[wid][lane][0] = make_float4((float)par0, (float)(par0 - cd.y), (float)(par0 - cd.x), ux);
                         S.stage[wid][lane][1] = make_float4((float)px, (float)py, (float)pz, uy);
-                        S.stage[wid][lane][2] =
-                            make_float4((float)(ox - a.x), (float)(oy - a.y), (float)(oz - a.z), uz);
+                        S.stage[wid][lane][2] = make_float4(ex, ey, ez, uz);
+                        S.near[wid][lane] = cx * cx + cy * cy + cz * cz < cull_r2 ? 1.0f : 0.0f;
                     }
                 }
                 unsigned mask = __ballot_sync(0xffffffffu, hit);
@@ -696,12 +702,15 @@ __global__ void __launch_bounds__(kEvThreads, 3) k_bgki(EvArgs A) {
                     const int j = __ffs(mask) - 1;
                     mask &= mask - 1;
                     const float4 s0 = S.stage[wid][j][0], s1 = S.stage[wid][j][1], s2 = S.stage[wid][j][2];
-                    // occupied evidence (mass_update.cu:48-52)
-                    const float vx = s2.x + dx, vy = s2.y + dy, vz = s2.z + dz;
-                    const float d2o = vx * vx + vy * vy + vz * vz;
-                    if (d2o < ls2 && L.c >= 0) {
-                        ao += kernel_units(kernel_tab(S.ktab, d2o * inv_ls2));
-                        ++nev;
+                    // occupied evidence (mass_update.cu:48-52), only where the point's sphere can
+                    // reach the sub-block (the same for every lane: j is)
+                    if (S.near[wid][j] != 0.0f) {
+                        const float vx = s2.x + dx, vy = s2.y + dy, vz = s2.z + dz;
+                        const float d2o = vx * vx + vy * vy + vz * vz;
+                        if (d2o < ls2c) {
+                            ao += kernel_units(kernel_tab(S.ktab, d2o * inv_ls2));
+                            ++nev;
+                        }
                     }
                     // free evidence (:54-71)
                     const float dpar = dx * s0.w + dy * s1.w + dz * s2.w;
@@ -710,7 +719,7 @@ __global__ void __launch_bounds__(kEvThreads, 3) k_bgki(EvArgs A) {
                                     qz = s1.z + dz - dpar * s2.w;
                         const float al = fminf(s0.x + dpar, 0.0f) + fmaxf(s0.y + dpar, 0.0f);
                         const float d2f = qx * qx + qy * qy + qz * qz + al * al;
-                        if (d2f < ls2 && L.c >= 0) {
+                        if (d2f < ls2c) {
                             af += kernel_units(kernel_tab(S.ktab, d2f * inv_ls2));
                             ++nev;
                         }

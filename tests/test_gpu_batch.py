@@ -91,9 +91,13 @@ def test_batch_equals_separate_scenes(variant):
             d.close()
 
 
-def test_batch_autotune_keeps_results():
+@pytest.mark.parametrize("device_points", [False, True])
+def test_batch_autotune_keeps_results(device_points):
     """The autotuner measures every (tile rule, chunk) candidate on live frames; the results
-    must equal the untuned single-scene handles frame by frame."""
+    must equal the untuned single-scene handles frame by frame. With scans in device memory the
+    candidates that re-lay out the evidence buffers re-stage the frame's points device to device,
+    which must be ordered after the new buffers' zero-fill."""
+    import torch
     variant = "k3dom"
     cfgs = scenes(variant)
     params = [K.make_params(variant, **c.params) for c in cfgs]
@@ -109,7 +113,10 @@ def test_batch_autotune_keeps_results():
                 d.updatePose(*poses[s])
                 d.updateGrid(t, pts[s])
                 batch.updatePose(s, *poses[s])
-            batch.update([t] * len(cfgs), pts)
+            if device_points:
+                batch.update([t] * len(cfgs), [torch.from_numpy(x).cuda() for x in pts])
+            else:
+                batch.update([t] * len(cfgs), pts)
             for s, d in enumerate(plain):
                 assert_same(snapshot(batch.scene(s)), snapshot(d), f"tuned frame {f} scene {s}")
         tu = batch.tuning()
