@@ -119,6 +119,16 @@ k3dom_status k3dom_destroy(k3dom_handle* h);
  * allocation; the particle part of the shift is folded into the next prediction. */
 k3dom_status k3dom_update_pose(k3dom_handle* h, float x, float y, float z);
 
+/* The node's cloud transform (k3dom_node.cpp:73-83,99-127: pcl_ros::transformPointCloud of the
+ * lidar-frame cloud by tf_lidar2lmap.inverse(), a rotation into the map-aligned frame) done on
+ * the GPU: from the next update on, every point p of `scene` (0 for a plain handle) is used as
+ * R p + t, with R = rotation (9 floats, row-major) and t = translation (3 floats, NULL = 0),
+ * evaluated in FP32 as ((R[0] x + R[1] y) + R[2] z) + t[0] per row without fused multiply-add.
+ * rotation = NULL switches the transform off (points as given). Set it before each update whose
+ * pose changed; it is part of the frame, so a captured steady frame stays valid. */
+k3dom_status k3dom_set_point_transform(k3dom_handle* h, int32_t scene, const float* rotation,
+                                       const float* translation);
+
 /* DOM::updateGrid (src/k3dom/dom.cu:29-50, src/dsphdmib/dom.cu:32-53). xs/ys/zs are n
  * point coordinates; ys/zs may be NULL when xs holds n interleaved xyz triples. */
 k3dom_status k3dom_update_grid(k3dom_handle* h, float t, const float* xs, const float* ys,

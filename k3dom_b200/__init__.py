@@ -6,7 +6,7 @@ update API (dom.py), the ctypes binding (_native.py) and the synthetic scene gen
 (scene.py).
 """
 from .dom import (DOM, GRIDCELL_DTYPE, BatchDOM, MAPPOINT_DTYPE, debug_draws, make_params, node_config_from_yaml,  # noqa: F401
-                  params_default, params_from_yaml)
+                  params_default, params_from_yaml, rotation_from_quaternion)
 
 __all__ = ["BatchDOM", "DOM", "GRIDCELL_DTYPE", "MAPPOINT_DTYPE", "debug_draws", "make_params", "node_config_from_yaml",
-           "params_default", "params_from_yaml"]
+           "params_default", "params_from_yaml", "rotation_from_quaternion"]

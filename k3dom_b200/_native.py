@@ -125,6 +125,7 @@ SIGNATURES = {
     "k3dom_create": (_ST, [C.POINTER(Params), C.c_int, C.c_int, C.POINTER(_P)]),
     "k3dom_destroy": (_ST, [_P]),
     "k3dom_update_pose": (_ST, [_P, C.c_float, C.c_float, C.c_float]),
+    "k3dom_set_point_transform": (_ST, [_P, C.c_int32, _P, _P]),
     "k3dom_update_grid": (_ST, [_P, C.c_float, _P, _P, _P, C.c_int32, C.c_int]),
     "k3dom_update_grid_async": (_ST, [_P, C.c_float, _P, _P, _P, C.c_int32, C.c_int]),
     "k3dom_synchronize": (_ST, [_P]),

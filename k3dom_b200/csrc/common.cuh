@@ -65,7 +65,21 @@ struct FrameParams {
     int shift_x, shift_y, shift_z;       // pending particle shift (voxels), applied in predict
     int shift_pending;
     uint64_t seed;
+    // optional rigid transform of the scene's points into the map-aligned sensor frame
+    // (p' = R p + t), applied where the points are read; has_transform = 0: points as given
+    float rot[9];   // row-major
+    float trans[3];
+    int has_transform;
 };
+
+// R p + t in FP32 in the written order, without contraction (a CPU restatement with the same
+// operation order reproduces it bit for bit).
+__device__ __forceinline__ void apply_transform(const FrameParams& f, float* x, float* y, float* z) {
+    const float a = *x, b = *y, c = *z;
+    *x = __fadd_rn(__fadd_rn(__fadd_rn(__fmul_rn(f.rot[0], a), __fmul_rn(f.rot[1], b)), __fmul_rn(f.rot[2], c)), f.trans[0]);
+    *y = __fadd_rn(__fadd_rn(__fadd_rn(__fmul_rn(f.rot[3], a), __fmul_rn(f.rot[4], b)), __fmul_rn(f.rot[5], c)), f.trans[1]);
+    *z = __fadd_rn(__fadd_rn(__fadd_rn(__fmul_rn(f.rot[6], a), __fmul_rn(f.rot[7], b)), __fmul_rn(f.rot[8], c)), f.trans[2]);
+}
 
 // The batch as the kernels see it: S scenes, their totals and per-scene tables.
 struct Batch {

@@ -75,6 +75,10 @@ struct SceneHost {
     bool shift_pending = false;
     int pending_shift[3] = {0, 0, 0};
     bool initialized = false;
+    // points arrive in the sensor's own frame: rotate (and translate) them on the device
+    bool has_transform = false;
+    float rot[9] = {1, 0, 0, 0, 1, 0, 0, 0, 1};
+    float trans[3] = {0, 0, 0};
 };
 
 int key_bits_for(long n) {
@@ -419,6 +423,9 @@ k3dom_status set_frame_params(k3dom_handle* h, const float* dt, const int* n_poi
         f.shift_z = x.pending_shift[2];
         f.shift_pending = x.shift_pending ? 1 : 0;
         f.seed = x.params.seed;
+        f.has_transform = x.has_transform ? 1 : 0;
+        std::memcpy(f.rot, x.rot, sizeof(f.rot));
+        std::memcpy(f.trans, x.trans, sizeof(f.trans));
     }
     e = cudaMemcpyAsync(h->fp_dev, h->fp_host, sizeof(FrameParams) * h->S, cudaMemcpyHostToDevice, h->st);
     if (e != cudaSuccess) return h->fail(e);
@@ -893,6 +900,24 @@ k3dom_status k3dom_batch_update_pose(k3dom_handle* h, int32_t scene, float x, fl
         sh.center_pos[1] += my * p.resolution;
         sh.center_pos[2] += mz * p.resolution;
     }
+    return K3DOM_OK;
+}
+
+k3dom_status k3dom_set_point_transform(k3dom_handle* h, int32_t scene, const float* rotation, const float* translation) {
+    if (!h || scene < 0 || scene >= h->S) return K3DOM_ERR_INVALID_ARGUMENT;
+    SceneHost& x = h->sc[scene];
+    if (!rotation) {
+        x.has_transform = false;
+        return K3DOM_OK;
+    }
+    for (int i = 0; i < 9; ++i)
+        if (!std::isfinite(rotation[i])) return K3DOM_ERR_INVALID_INPUT;
+    if (translation)
+        for (int i = 0; i < 3; ++i)
+            if (!std::isfinite(translation[i])) return K3DOM_ERR_INVALID_INPUT;
+    std::memcpy(x.rot, rotation, sizeof(x.rot));
+    for (int i = 0; i < 3; ++i) x.trans[i] = translation ? translation[i] : 0.0f;
+    x.has_transform = true;
     return K3DOM_OK;
 }
 

@@ -214,7 +214,8 @@ __global__ void k_ray_count(Batch bt, const float* __restrict__ xs, const float*
         }
         const SceneDev& sd = bt.sc[sc];
         const BinGeom g = scene_geom(sd, f);
-        const float mx = xs[i], my = ys[i], mz = zs[i];
+        float mx = xs[i], my = ys[i], mz = zs[i];
+        if (f.has_transform) apply_transform(f, &mx, &my, &mz);
         float4 a;
         double4 cc;
         const RayPrep r = prep_ray(sd.p, g, mx, my, mz, ds != 0, &a, &cc);
@@ -247,7 +248,8 @@ __global__ void k_ray_emit(Batch bt, const float* __restrict__ xs, const float* 
         if (i - bt.off->point[sc] >= f.n_points) continue;
         const SceneDev& sd = bt.sc[sc];
         const BinGeom g = scene_geom(sd, f);
-        const float mx = xs[i], my = ys[i], mz = zs[i];
+        float mx = xs[i], my = ys[i], mz = zs[i];
+        if (f.has_transform) apply_transform(f, &mx, &my, &mz);
         float4 a;
         double4 c;
         const RayPrep r = prep_ray(sd.p, g, mx, my, mz, ds != 0, &a, &c);

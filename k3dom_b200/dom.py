@@ -13,6 +13,7 @@ call goes through the C ABI of libk3dom_b200.so (include/k3dom_b200.h).
 from __future__ import annotations
 
 import ctypes as C
+import math
 from typing import Optional
 
 import numpy as np
@@ -160,6 +161,14 @@ class DOM:
     # -- DOM_c interface (include/common/dom.h:57-94)
     def updatePose(self, x: float, y: float, z: float) -> None:
         N.check(self._lib.k3dom_update_pose(self._sel(), float(x), float(y), float(z)), "k3dom_update_pose")
+
+    def set_point_transform(self, rotation=None, translation=None) -> None:
+        """Points of the next updates are used as R p + t (the node's lidar-to-map rotation, done
+        on the GPU); rotation=None switches it off."""
+        r = None if rotation is None else np.ascontiguousarray(rotation, np.float32).reshape(9)
+        t = None if translation is None else np.ascontiguousarray(translation, np.float32).reshape(3)
+        N.check(self._lib.k3dom_set_point_transform(self._h, self._scene, _ptr(r), _ptr(t)),
+                "k3dom_set_point_transform")
 
     def updateGrid(self, t: float, xs, ys=None, zs=None) -> None:
         px, py, pz, n, mem, _keep = self._points(xs, ys, zs)
@@ -341,6 +350,16 @@ class DOM:
         s = C.c_void_p()
         N.check(self._lib.k3dom_get_stream(self._h, C.byref(s)), "get_stream")
         return s.value or 0
+
+
+def rotation_from_quaternion(x: float, y: float, z: float, w: float) -> np.ndarray:
+    """Row-major 3x3 rotation of the unit quaternion (x, y, z, w), as float32 for
+    k3dom_set_point_transform (the node's tf rotation of a pose's orientation)."""
+    n = math.sqrt(x * x + y * y + z * z + w * w)
+    x, y, z, w = x / n, y / n, z / n, w / n
+    return np.array([[1 - 2 * (y * y + z * z), 2 * (x * y - z * w), 2 * (x * z + y * w)],
+                     [2 * (x * y + z * w), 1 - 2 * (x * x + z * z), 2 * (y * z - x * w)],
+                     [2 * (x * z - y * w), 2 * (y * z + x * w), 1 - 2 * (x * x + y * y)]], np.float32)
 
 
 def _points_of(item):
