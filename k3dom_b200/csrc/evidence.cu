@@ -601,13 +601,32 @@ __device__ void k3dom_cell_update(const DevParams& p, float dt, int c, double de
 
 // Shared memory of k_bgki: the kernel table, one chunk of rays, and a per-warp staging area for
 // the FP64 (sub-block, ray) constants of the rays that pass the cull.
+// (dynamic, sized by the work item's ray count so that smaller chunks leave room for more CTAs)
 struct BgkiSmem {
-    float4 ktab[kKernelTab];      // sparse-kernel table of the current scene
-    float4 a[kChunk];             // m.x, m.y, m.z, d_m
-    double4 c[kChunk];            // d_m, margin, 1/d_m
-    float4 stage[kEvWarps][32][3];
-    float near[kEvWarps][32];     // 1 where the point's sphere can reach the sub-block
+    float4* ktab;                 // [kKernelTab] sparse-kernel table of the current scene
+    float4 (*stage)[32][3];       // [kEvWarps][32][3]
+    float (*near)[32];            // [kEvWarps][32]: 1 where the point's sphere can reach the sub-block
+    float4* a;                    // [chunk] m.x, m.y, m.z, d_m
+    double4* c;                   // [chunk] d_m, margin, 1/d_m
 };
+
+constexpr size_t kBgkiFixedBytes =
+    sizeof(float4) * kKernelTab + sizeof(float4) * kEvWarps * 32 * 3 + sizeof(float) * kEvWarps * 32;
+
+inline size_t bgki_smem_bytes(int chunk) {
+    return ((kBgkiFixedBytes + 31) & ~(size_t)31) + (size_t)chunk * (sizeof(float4) + sizeof(double4));
+}
+
+__device__ __forceinline__ BgkiSmem bgki_smem(unsigned char* base, int chunk) {
+    BgkiSmem S;
+    S.ktab = reinterpret_cast<float4*>(base);
+    S.stage = reinterpret_cast<float4(*)[32][3]>(base + sizeof(float4) * kKernelTab);
+    S.near = reinterpret_cast<float(*)[32]>(base + sizeof(float4) * kKernelTab + sizeof(float4) * kEvWarps * 32 * 3);
+    const size_t off = (kBgkiFixedBytes + 31) & ~(size_t)31;
+    S.c = reinterpret_cast<double4*>(base + off);  // 32-byte aligned
+    S.a = reinterpret_cast<float4*>(base + off + sizeof(double4) * (size_t)chunk);
+    return S;
+}
 
 // Pair geometry. For the anchor o of a sub-block and a ray m (FP64, once per lane-ray):
 //   par0 = o.u, perp0 = o - par0 u, occ0 = o - m, and par0 - margin, par0 - d_m.
@@ -618,9 +637,10 @@ struct BgkiSmem {
 //   distance to the point = |occ0 + delta|.
 // Every FP32 quantity is O(ls), so the FP32 evaluation keeps ~1e-7 relative accuracy at any
 // distance from the sensor (the direct |c|^2 - d_proj^2 form of :60 loses ~1e-5 at 20 m).
-__global__ void __launch_bounds__(kEvThreads, 3) k_bgki(EvArgs A) {
-    extern __shared__ __align__(16) unsigned char smem_raw[];
-    BgkiSmem& S = *reinterpret_cast<BgkiSmem*>(smem_raw);
+template <int MINB>
+__global__ void __launch_bounds__(kEvThreads, MINB) k_bgki(EvArgs A) {
+    extern __shared__ __align__(32) unsigned char smem_raw[];
+    const BgkiSmem S = bgki_smem(smem_raw, A.chunk);
     __shared__ uint32_t s_item;
     __shared__ int s_next_sb, s_last;
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
@@ -669,7 +689,7 @@ __global__ void __launch_bounds__(kEvThreads, 3) k_bgki(EvArgs A) {
             const float dx = L.x - L.ox, dy = L.y - L.oy, dz = L.z - L.oz;  // exact (nearby floats)
             const float ls2c = L.c >= 0 ? ls2 : -1.0f;  // cells outside the grid take no evidence
             const double ox = L.ox, oy = L.oy, oz = L.oz;
-            double ao = 0.0, af = 0.0;  // exact sums of integer units (< 2^52 per chunk)
+            long long ao = 0, af = 0;  // sums of kernel values rounded to integer units
             for (int g0 = 0; g0 < nr; g0 += 32) {
                 const int r = g0 + lane;
                 bool hit = false;
@@ -710,7 +730,7 @@ __global__ void __launch_bounds__(kEvThreads, 3) k_bgki(EvArgs A) {
                         const float vx = s2.x + dx, vy = s2.y + dy, vz = s2.z + dz;
                         const float d2o = vx * vx + vy * vy + vz * vz;
                         if (d2o < ls2c) {
-                            ao += kernel_units(kernel_tab(S.ktab, d2o * inv_ls2));
+                            ao += __float2ll_rn(fmaxf(kernel_tab(S.ktab, d2o * inv_ls2), 0.0f));
                             ++nev;
                         }
                     }
@@ -722,7 +742,7 @@ __global__ void __launch_bounds__(kEvThreads, 3) k_bgki(EvArgs A) {
                         const float al = fminf(s0.x + dpar, 0.0f) + fmaxf(s0.y + dpar, 0.0f);
                         const float d2f = qx * qx + qy * qy + qz * qz + al * al;
                         if (d2f < ls2c) {
-                            af += kernel_units(kernel_tab(S.ktab, d2f * inv_ls2));
+                            af += __float2ll_rn(fmaxf(kernel_tab(S.ktab, d2f * inv_ls2), 0.0f));
                             ++nev;
                         }
                     }
@@ -731,7 +751,7 @@ __global__ void __launch_bounds__(kEvThreads, 3) k_bgki(EvArgs A) {
             }
             if (L.c >= 0) {
                 unsigned long long* ac = A.acc + 2 * (long)(coff + L.c);
-                const long long io = __double2ll_rn(ao), jf = __double2ll_rn(af);  // exact
+                const long long io = ao, jf = af;
                 if (io) atomicAdd(ac, (unsigned long long)io);
                 if (jf) atomicAdd(ac + 1, (unsigned long long)jf);
             }
@@ -1234,16 +1254,29 @@ cudaError_t launch_bgki_sums(const Batch& bt, RayBuffers& rb, const float4* f_ta
 
 int bgki_blocks_per_sm() {
     int per_sm = 1;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_bgki, kEvThreads, sizeof(BgkiSmem));
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_bgki<3>, kEvThreads, bgki_smem_bytes(kChunk));
     return std::max(1, per_sm);
 }
 
+// Work items of up to 512 rays leave shared memory for a fourth CTA per SM; that build is limited
+// to 64 registers. Both builds compute the same sums (exactly), so the choice is speed only.
 cudaError_t launch_k3dom_evidence(const Batch& bt, RayBuffers& rb, CellState cs, CellWork cw, bool first_frame,
                                   DevStatus* status, int grid, cudaStream_t st) {
     if (rb.chunk < 32 || rb.chunk > kChunk) return cudaErrorInvalidValue;
     EvArgs A = make_args(bt, rb, cs, cw, first_frame, status);
+    const size_t sm = bgki_smem_bytes(rb.chunk);
+    int dev = 0, sms = 148, per_sm = 1;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     ++g_launches;
-    k_bgki<<<grid, kEvThreads, sizeof(BgkiSmem), st>>>(A);
+    if (rb.chunk <= 512) {
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_bgki<4>, kEvThreads, sm);
+        k_bgki<4><<<sms * std::max(1, per_sm), kEvThreads, sm, st>>>(A);
+    } else {
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_bgki<3>, kEvThreads, sm);
+        k_bgki<3><<<sms * std::max(1, per_sm), kEvThreads, sm, st>>>(A);
+    }
+    (void)grid;
     return cudaGetLastError();
 }
 
@@ -1261,8 +1294,12 @@ cudaError_t launch_ds_evidence(const Batch& bt, RayBuffers& rb, CellState cs, Ce
 long ds_count_bytes(long items) { return items * (long)kMaxTileCells; }
 
 cudaError_t evidence_init() {
-    cudaError_t e = cudaFuncSetAttribute(k_bgki, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(BgkiSmem));
+    cudaError_t e = cudaFuncSetAttribute(k_bgki<3>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)bgki_smem_bytes(kChunk));
     if (e != cudaSuccess) return e;
+    if ((e = cudaFuncSetAttribute(k_bgki<4>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)bgki_smem_bytes(kChunk))))
+        return e;
     return cudaFuncSetAttribute(k_bgki_sums, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(CalibSmem));
 }
 
