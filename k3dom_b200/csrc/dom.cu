@@ -99,8 +99,8 @@ struct k3dom_handle {
     SceneOffsets off{};
     int P = 0, B = 0, C = 0, N = 0, T = 0;
 
-    cudaStream_t st = nullptr, st2 = nullptr;
-    cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
+    cudaStream_t st = nullptr, st2 = nullptr, st3 = nullptr;  // frame; resampling draws; ray lists
+    cudaEvent_t ev_fork = nullptr, ev_join = nullptr, ev_bin = nullptr;
     cudaEvent_t ev_t[8] = {};
     bool timing = false;
     k3dom_stage_times times{};
@@ -211,9 +211,11 @@ struct k3dom_handle {
             if (e) cudaEventDestroy(e);
         if (ev_fork) cudaEventDestroy(ev_fork);
         if (ev_join) cudaEventDestroy(ev_join);
+        if (ev_bin) cudaEventDestroy(ev_bin);
         if (ev_staged) cudaEventDestroy(ev_staged);
         if (st) cudaStreamDestroy(st);
         if (st2) cudaStreamDestroy(st2);
+        if (st3) cudaStreamDestroy(st3);
     }
     CellState cells() const { return cs[0]; }
     Batch batch() const {
@@ -384,17 +386,11 @@ cudaError_t alloc_ray_buffers(k3dom_handle* h) {
         rb.ds_count_capacity = ds_count_bytes(items_max);
         if ((e = h->alloc(&rb.ds_counts, rb.ds_count_capacity, true, L))) return e;
     }
-    // shared sort/scan scratch sized for the largest user
-    const long hw = std::max({radix_hist_words(h->P, 11), radix_hist_words(cap, 11), 1L});
-    if ((e = h->alloc(&h->hist, hw, true, L))) return e;
-    h->hist_words = hw;
-    const long sw = scan_u32_tiles(std::max({hw, (long)N, (long)T + 1})) + 16;
-    if ((e = h->alloc(&h->scan_tmp, sw, true, L))) return e;
-    h->scan_tmp_words = sw;
-    rb.hist = h->hist;
-    rb.scan_tmp = h->scan_tmp;
-    rb.hist_words = h->hist_words;
-    rb.scan_words = h->scan_tmp_words;
+    // sort/scan scratch of the ray lists (their own: the lists are built beside the particle sort)
+    rb.hist_words = std::max(radix_hist_words(cap, 11), 1L);
+    rb.scan_words = scan_u32_tiles(std::max({rb.hist_words, (long)N, (long)T + 1})) + 16;
+    if ((e = h->alloc(&rb.hist, rb.hist_words, true, L))) return e;
+    if ((e = h->alloc(&rb.scan_tmp, rb.scan_words, true, L))) return e;
     if ((e = h->alloc(&h->pts, 3 * (size_t)N, true, L))) return e;
     if ((e = cudaMallocHost((void**)&h->pts_pinned, 3 * (size_t)N * sizeof(float)))) return e;
     return cudaSuccess;
@@ -447,6 +443,7 @@ k3dom_status grow_points(k3dom_handle* h, const int32_t* n) {
     if (!grow) return K3DOM_OK;
     cudaError_t e = cudaStreamSynchronize(h->st);
     if (e == cudaSuccess) e = cudaStreamSynchronize(h->st2);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(h->st3);
     if (e != cudaSuccess) return h->fail(e);
     for (int s = 0; s < h->S; ++s) {
         SceneHost& x = h->sc[s];
@@ -550,15 +547,23 @@ cudaError_t enq_assign(k3dom_handle* h) {
     return cudaGetLastError();
 }
 
-cudaError_t enq_occupancy(k3dom_handle* h, bool first_frame) {
-    const Batch bt = h->batch();
+cudaError_t enq_binning(k3dom_handle* h, cudaStream_t s) {
     const long N = h->N;
-    cudaError_t e = build_ray_lists(bt, h->pts, h->pts + N, h->pts + 2 * N, h->rb, h->ds(), h->status, h->st);
-    if (e != cudaSuccess) return e;
-    rec(h, 7);
+    return build_ray_lists(h->batch(), h->pts, h->pts + N, h->pts + 2 * N, h->rb, h->ds(), h->status, s);
+}
+
+cudaError_t enq_evidence(k3dom_handle* h, bool first_frame) {
+    const Batch bt = h->batch();
     if (h->ds())
         return launch_ds_evidence(bt, h->rb, h->cells(), h->cw, first_frame, h->status, h->ds_grid, h->st);
     return launch_k3dom_evidence(bt, h->rb, h->cells(), h->cw, first_frame, h->status, h->bgki_grid, h->st);
+}
+
+cudaError_t enq_occupancy(k3dom_handle* h, bool first_frame) {
+    cudaError_t e = enq_binning(h, h->st);
+    if (e != cudaSuccess) return e;
+    rec(h, 7);
+    return enq_evidence(h, first_frame);
 }
 
 cudaError_t enq_persistent(k3dom_handle* h) {
@@ -608,12 +613,25 @@ cudaError_t enq_frame(k3dom_handle* h) {
     if ((e = cudaStreamWaitEvent(h->st2, h->ev_fork, 0))) return e;
     if ((e = enq_draws(h, h->st2))) return e;
     if ((e = cudaEventRecord(h->ev_join, h->st2))) return e;
+    // the ray lists depend on the points only: built beside prediction and assignment, except
+    // when each stage is timed on its own
+    const bool overlap = !h->timing;
+    if (overlap) {
+        if ((e = cudaStreamWaitEvent(h->st3, h->ev_fork, 0))) return e;
+        if ((e = enq_binning(h, h->st3))) return e;
+        if ((e = cudaEventRecord(h->ev_bin, h->st3))) return e;
+    }
     rec(h, 0);
     if ((e = enq_predict(h))) return e;
     rec(h, 1);
     if ((e = enq_assign(h))) return e;
     rec(h, 2);
-    if ((e = enq_occupancy(h, false))) return e;
+    if (overlap) {
+        if ((e = cudaStreamWaitEvent(h->st, h->ev_bin, 0))) return e;
+        if ((e = enq_evidence(h, false))) return e;
+    } else if ((e = enq_occupancy(h, false))) {
+        return e;
+    }
     rec(h, 3);
     if ((e = enq_persistent(h))) return e;
     rec(h, 4);
@@ -648,6 +666,7 @@ cudaError_t apply_tuning(k3dom_handle* h, int rule, int chunk) {
     if (rule == h->tile_rule && chunk == h->chunk) return cudaSuccess;
     cudaError_t e = cudaStreamSynchronize(h->st);
     if (e == cudaSuccess) e = cudaStreamSynchronize(h->st2);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(h->st3);
     if (e != cudaSuccess) return e;
     // a smaller chunk makes more work items than the DS count buffer was sized for
     const bool relayout = rule != h->tile_rule || (h->ds() && chunk < h->ds_sized_chunk);
@@ -759,6 +778,8 @@ k3dom_status k3dom_batch_create(const k3dom_params* params, int32_t n_scenes, k3
 
     if ((e = cudaStreamCreateWithFlags(&h->st, cudaStreamNonBlocking))) return bail(e);
     if ((e = cudaStreamCreateWithFlags(&h->st2, cudaStreamNonBlocking))) return bail(e);
+    if ((e = cudaStreamCreateWithFlags(&h->st3, cudaStreamNonBlocking))) return bail(e);
+    if ((e = cudaEventCreateWithFlags(&h->ev_bin, cudaEventDisableTiming))) return bail(e);
     if ((e = cudaEventCreateWithFlags(&h->ev_fork, cudaEventDisableTiming))) return bail(e);
     if ((e = cudaEventCreateWithFlags(&h->ev_join, cudaEventDisableTiming))) return bail(e);
     if ((e = cudaEventCreateWithFlags(&h->ev_staged, cudaEventDisableTiming))) return bail(e);
@@ -815,6 +836,10 @@ k3dom_status k3dom_batch_create(const k3dom_params* params, int32_t n_scenes, k3
     }
     if ((e = h->alloc(&h->draw_keys, P)) || (e = h->alloc(&h->draw_sorted, P)) || (e = h->alloc(&h->draw_alt, P)))
         return bail(e);
+    // sort/scan scratch of the particle sort
+    h->hist_words = std::max(radix_hist_words(P, 11), 1L);
+    h->scan_tmp_words = scan_u32_tiles(h->hist_words) + 16;
+    if ((e = h->alloc(&h->hist, h->hist_words)) || (e = h->alloc(&h->scan_tmp, h->scan_tmp_words))) return bail(e);
     // separate sort scratch for the draw sort (it runs concurrently on the second stream); the
     // draw keys carry the scene index above 24 bits, so passes may be up to 11 bits wide
     {
@@ -842,6 +867,7 @@ k3dom_status k3dom_destroy(k3dom_handle* h) {
     cudaSetDevice(h->device);
     cudaStreamSynchronize(h->st);
     cudaStreamSynchronize(h->st2);
+    cudaStreamSynchronize(h->st3);
     h->release();
     delete h;
     return K3DOM_OK;
