@@ -42,12 +42,15 @@ constexpr int kMaxCalibFrames = 16;
 constexpr double kPClamp = 1e-7;
 
 // ---------------------------------------------------------------- per-cell mass recursion
-__host__ __device__ inline double credit(double x, double ms) { return 1.0 - 2.0 / (1.0 + exp(2.0 * x / ms)); }
-// d credit / dx = (4 / ms) e / (1 + e)^2 with e = exp(2x / ms), written with t = exp(-|2x / ms|)
-// (the same value, e / (1 + e)^2 = t / (1 + t)^2) so that it cannot overflow to inf / inf.
-__host__ __device__ inline double credit_d(double x, double ms) {
-    const double t = exp(-fabs(2.0 * x / ms));
-    return (4.0 / ms) * t / ((1.0 + t) * (1.0 + t));
+// k2 = 2 / mass_scale throughout.
+// credit(x) = 1 - 2 / (1 + e), e = exp(2x / mass_scale)
+__device__ inline double credit(double x, double k2) { return 1.0 - 2.0 / (1.0 + exp(x * k2)); }
+// d credit / dx = (4 / ms) e / (1 + e)^2, written with t = exp(-|2x / ms|) (the same value,
+// e / (1 + e)^2 = t / (1 + t)^2) so that it cannot overflow to inf / inf.
+__device__ inline double credit_d(double x, double k2) {
+    const double t = exp(-fabs(x * k2));
+    const double u = 1.0 + t;
+    return (2.0 * k2) * t / (u * u);
 }
 
 struct FrameIn {
@@ -57,8 +60,33 @@ struct FrameIn {
     double Eo, Ef;      // evidence
 };
 
+// The evidence-driven transfers of the update (mass_update.cu:95-118), shared by the forward and
+// the adjoint's recomputation: with Z = Sd Sp, X = sqrt(Z), cr = credit(X) and w = cr / Z,
+// lDF = w (Ef - Eo)+ d1, lSFD = w (Ef - Eo)+ (s1 + d1 - f1)+, lFD = w (Eo - Ef)+ (f1 - s1 - d1)+
+// (the reference's bf d1 / Sp etc. with bf = cr (Ef - Eo)+ / Sd).
+struct Transfers {
+    double iZ, X, cr, w, lDF, lSFD, lFD;
+};
+
+__device__ inline Transfers transfers(double Eo, double Ef, double f1, double s1, double d1, double Sd,
+                                      double Sp, double k2) {
+    Transfers t = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
+    if (Sp > 0.0) {
+        const double Z = Sd * Sp;
+        t.iZ = 1.0 / Z;
+        t.X = sqrt(Z);
+        t.cr = credit(t.X, k2);
+        t.w = t.cr * t.iZ;
+        const double pf = fmax(0.0, Ef - Eo), po = fmax(0.0, Eo - Ef);
+        t.lDF = t.w * pf * d1;
+        t.lSFD = t.w * pf * fmax(0.0, s1 + d1 - f1);
+        t.lFD = t.w * po * fmax(0.0, f1 - s1 - d1);
+    }
+    return t;
+}
+
 // The frame's prediction and update (mass_update.cu:79-139), FP64.
-__device__ inline void frame_forward(const FrameIn& in, double mass_scale, double* f3, double* s3, double* d3) {
+__device__ inline void frame_forward(const FrameIn& in, double k2, double* f3, double* s3, double* d3) {
     const double P = (in.mf + in.md) * in.g;
     const double s1 = in.ms * in.g;
     const double d1 = fmin(in.dyn, fmax(0.0, P - s1));
@@ -67,22 +95,14 @@ __device__ inline void frame_forward(const FrameIn& in, double mass_scale, doubl
         *f3 = f1; *s3 = s1; *d3 = d1;
         return;
     }
-    const double Sd = in.Ef + in.Eo;
-    const double Sp = f1 + s1 + d1;
-    double lDF = 0.0, lSFD = 0.0, lFD = 0.0;
-    if (Sp > 0.0) {
-        const double cr = credit(sqrt(Sd * Sp), mass_scale);
-        const double bf = cr * fmax(0.0, in.Ef - in.Eo) / Sd;
-        const double bo = cr * fmax(0.0, in.Eo - in.Ef) / Sd;
-        lDF = bf * d1 / Sp;
-        lSFD = bf * fmax(0.0, s1 + d1 - f1) / Sp;
-        lFD = bo * fmax(0.0, f1 - s1 - d1) / Sp;
-    }
-    const double f2 = f1 + lSFD / 2.0 * s1 + lDF * d1 - lFD * f1;
-    const double s2 = s1 - lSFD * s1;
-    const double d2 = d1 + lFD * f1 + lSFD / 2.0 * s1 - lDF * d1;
-    const double cr2 = credit(s2 + d2, mass_scale);
-    const double r = (s2 <= 0.0 || d2 < 0.0) ? 0.0 : 1.0 / (1.0 + d2 / s2);
+    const Transfers t = transfers(in.Eo, in.Ef, f1, s1, d1, in.Ef + in.Eo, f1 + s1 + d1, k2);
+    const double f2 = f1 + t.lSFD / 2.0 * s1 + t.lDF * d1 - t.lFD * f1;
+    const double s2 = s1 - t.lSFD * s1;
+    const double d2 = d1 + t.lFD * f1 + t.lSFD / 2.0 * s1 - t.lDF * d1;
+    const double y = s2 + d2;
+    const double cr2 = credit(y, k2);
+    // ratio 1 / (1 + d2 / s2) = s2 / (s2 + d2)
+    const double r = (s2 <= 0.0 || d2 < 0.0) ? 0.0 : s2 / y;
     const double beta = (1.0 - cr2) + cr2 * r;
     *s3 = s2 + beta * in.Eo;
     *d3 = d2 + (1.0 - beta) * in.Eo;
@@ -96,7 +116,7 @@ struct FrameBar {
 // Reverse mode of frame_forward: adjoints of the outputs (F3, S3, D3) -> adjoints of the inputs.
 // Piecewise branches (min, max, the update condition, the ratio's guard) take the derivative of
 // the branch the forward took.
-__device__ inline FrameBar frame_adjoint(const FrameIn& in, double mass_scale, double F3, double S3, double D3) {
+__device__ inline FrameBar frame_adjoint(const FrameIn& in, double k2, double F3, double S3, double D3) {
     FrameBar b = {0, 0, 0, 0, 0, 0};
     // forward recomputation
     const double P = (in.mf + in.md) * in.g;
@@ -112,26 +132,17 @@ __device__ inline FrameBar frame_adjoint(const FrameIn& in, double mass_scale, d
     } else {
         const double Sd = in.Ef + in.Eo;
         const double Sp = f1 + s1 + d1;
-        double lDF = 0.0, lSFD = 0.0, lFD = 0.0, cr = 0.0, bf = 0.0, bo = 0.0, X = 0.0;
         const double pf = fmax(0.0, in.Ef - in.Eo), po = fmax(0.0, in.Eo - in.Ef);
         const double q1 = fmax(0.0, s1 + d1 - f1), q2 = fmax(0.0, f1 - s1 - d1);
-        if (Sp > 0.0) {
-            X = sqrt(Sd * Sp);
-            cr = credit(X, mass_scale);
-            bf = cr * pf / Sd;
-            bo = cr * po / Sd;
-            lDF = bf * d1 / Sp;
-            lSFD = bf * q1 / Sp;
-            lFD = bo * q2 / Sp;
-        }
-        const double f2 = f1 + lSFD / 2.0 * s1 + lDF * d1 - lFD * f1;
+        const Transfers tr = transfers(in.Eo, in.Ef, f1, s1, d1, Sd, Sp, k2);
+        const double lDF = tr.lDF, lSFD = tr.lSFD, lFD = tr.lFD;
         const double s2 = s1 - lSFD * s1;
         const double d2 = d1 + lFD * f1 + lSFD / 2.0 * s1 - lDF * d1;
-        (void)f2;
         const double y = s2 + d2;
-        const double cr2 = credit(y, mass_scale);
+        const double cr2 = credit(y, k2);
         const bool r_on = !(s2 <= 0.0 || d2 < 0.0);
-        const double r = r_on ? 1.0 / (1.0 + d2 / s2) : 0.0;
+        const double iy = r_on ? 1.0 / y : 0.0;
+        const double r = s2 * iy;
         const double beta = (1.0 - cr2) + cr2 * r;
         // reverse
         double f2b = F3, s2b = S3, d2b = D3;
@@ -140,13 +151,14 @@ __device__ inline FrameBar frame_adjoint(const FrameIn& in, double mass_scale, d
         b.Eo += S3 * beta + D3 * (1.0 - beta);
         const double cr2b = betab * (r - 1.0);
         const double rb = betab * cr2;
-        const double yb = cr2b * credit_d(y, mass_scale);
+        const double yb = cr2b * credit_d(y, k2);
         s2b += yb;
         d2b += yb;
         if (r_on) {
-            const double den = (s2 + d2) * (s2 + d2);
-            s2b += rb * d2 / den;
-            d2b += -rb * s2 / den;
+            // r = s2 / (s2 + d2): dr/ds2 = d2 / y^2, dr/dd2 = -s2 / y^2
+            const double riy2 = rb * iy * iy;
+            s2b += riy2 * d2;
+            d2b -= riy2 * s2;
         }
         double lSFDb = 0.0, lDFb = 0.0, lFDb = 0.0;
         // f2 = f1 + lSFD/2 s1 + lDF d1 - lFD f1
@@ -167,28 +179,24 @@ __device__ inline FrameBar frame_adjoint(const FrameIn& in, double mass_scale, d
         lSFDb += d2b * s1 / 2.0;
         lDFb += -d2b * d1;
         if (Sp > 0.0) {
-            double bfb = 0.0, bob = 0.0, Spb = 0.0, Sdb = 0.0, q1b = 0.0, q2b = 0.0;
-            bfb += lDFb * d1 / Sp;
-            d1b += lDFb * bf / Sp;
-            Spb += -lDFb * bf * d1 / (Sp * Sp);
-            bfb += lSFDb * q1 / Sp;
-            q1b += lSFDb * bf / Sp;
-            Spb += -lSFDb * bf * q1 / (Sp * Sp);
-            bob += lFDb * q2 / Sp;
-            q2b += lFDb * bo / Sp;
-            Spb += -lFDb * bo * q2 / (Sp * Sp);
+            // lDF = w pf d1, lSFD = w pf q1, lFD = w po q2, w = cr / (Sd Sp), cr = credit(sqrt(Sd Sp))
+            const double w = tr.w;
+            const double pfb = w * (lDFb * d1 + lSFDb * q1);
+            const double pob = w * lFDb * q2;
+            d1b += lDFb * w * pf;
+            const double q1b = lSFDb * w * pf;
+            const double q2b = lFDb * w * po;
+            const double wb = lDFb * pf * d1 + lSFDb * pf * q1 + lFDb * po * q2;
+            // w = cr / Z, Z = Sd Sp: crb = wb / Z, Zb = -wb w / Z; X = sqrt(Z): Zb += Xb / (2 X)
+            const double crb = wb * tr.iZ;
+            double Zb = -wb * w * tr.iZ;
+            const double Xb = crb * credit_d(tr.X, k2);
+            if (tr.X > 0.0) Zb += Xb / (2.0 * tr.X);
             if (s1 + d1 - f1 > 0.0) { s1b += q1b; d1b += q1b; f1b -= q1b; }
             if (f1 - s1 - d1 > 0.0) { f1b += q2b; s1b -= q2b; d1b -= q2b; }
-            double crb = bfb * pf / Sd + bob * po / Sd;
-            const double pfb = bfb * cr / Sd, pob = bob * cr / Sd;
-            Sdb += -(bfb * cr * pf + bob * cr * po) / (Sd * Sd);
             if (in.Ef - in.Eo > 0.0) { b.Ef += pfb; b.Eo -= pfb; }
             if (in.Eo - in.Ef > 0.0) { b.Eo += pob; b.Ef -= pob; }
-            const double Xb = crb * credit_d(X, mass_scale);
-            if (X > 0.0) {
-                Sdb += Xb * Sp / (2.0 * X);
-                Spb += Xb * Sd / (2.0 * X);
-            }
+            const double Sdb = Zb * Sp, Spb = Zb * Sd;
             f1b += Spb; s1b += Spb; d1b += Spb;
             b.Ef += Sdb; b.Eo += Sdb;
         }
@@ -213,9 +221,10 @@ __device__ inline FrameBar frame_adjoint(const FrameIn& in, double mass_scale, d
 struct CalibCellArgs {
     int C, F;
     double ls, sigma, gamma, prior_occ, prior_free;
-    double mass_scale;
+    double k2;  // 2 / mass_scale
     double inv_n;  // 1 / number of label instances
-    float dt[kMaxCalibFrames];
+    double g[kMaxCalibFrames];   // gamma^dt of each frame (1 for the first)
+    double gd[kMaxCalibFrames];  // d gamma^dt / d gamma (0 for the first frame and for dt = 0)
     const float* dyn[kMaxCalibFrames];  // per frame: particle weight sums (nullptr = none)
     const double* sums;                 // F x 4 x C: f occ, f free, -x f' occ, -x f' free
     const uint32_t* n0;
@@ -237,6 +246,9 @@ __device__ inline double block_sum(double v, double* sm) {
     return r;  // valid in thread 0
 }
 
+// NF: compile-time bound on the frame count. Up to 4 frames the loops unroll and the per-frame
+// inputs stay in registers; the 16-frame form keeps them in local memory.
+template <int NF>
 __global__ void __launch_bounds__(256) k_calib_cells(CalibCellArgs a) {
     __shared__ double sm[8];
     double loss = 0.0, g_ls = 0.0, g_sig = 0.0, g_gam = 0.0, g_po = 0.0, g_pf = 0.0;
@@ -245,20 +257,24 @@ __global__ void __launch_bounds__(256) k_calib_cells(CalibCellArgs a) {
         const uint32_t n0 = a.n0[c], n1 = a.n1[c];
         const bool labelled = (n0 | n1) != 0;
         if (!labelled && !a.occ_out) continue;
-        FrameIn in[kMaxCalibFrames];
+        FrameIn in[NF];
         double mf = a.prior_free, ms = a.prior_occ / 2.0, md = a.prior_occ / 2.0;
-        for (int k = 0; k < a.F; ++k) {
-            const double* s = a.sums + (long)k * 4 * C;
-            FrameIn& x = in[k];
-            x.mf = mf; x.ms = ms; x.md = md;
-            x.g = k == 0 ? 1.0 : pow(a.gamma, (double)a.dt[k]);
-            x.dyn = (k == 0 || !a.dyn[k]) ? 0.0 : (double)a.dyn[k][c];
-            x.Eo = a.sigma * s[c];
-            x.Ef = a.sigma * s[C + c];
-            frame_forward(x, a.mass_scale, &mf, &ms, &md);
+#pragma unroll(NF <= 4 ? NF : 1)
+        for (int k = 0; k < NF; ++k) {
+            if (k < a.F) {
+                const double* s = a.sums + (long)k * 4 * C;
+                FrameIn& x = in[k];
+                x.mf = mf; x.ms = ms; x.md = md;
+                x.g = a.g[k];
+                x.dyn = (k == 0 || !a.dyn[k]) ? 0.0 : (double)a.dyn[k][c];
+                x.Eo = a.sigma * s[c];
+                x.Ef = a.sigma * s[C + c];
+                frame_forward(x, a.k2, &mf, &ms, &md);
+            }
         }
         const double T = mf + ms + md;
-        const double p = T > 0.0 ? (ms + md) / T : 0.5;
+        const double iT = T > 0.0 ? 1.0 / T : 0.0;
+        const double p = T > 0.0 ? (ms + md) * iT : 0.5;
         if (a.occ_out) a.occ_out[c] = (float)p;
         if (!labelled) continue;
         const double pc = fmin(fmax(p, kPClamp), 1.0 - kPClamp);
@@ -268,18 +284,22 @@ __global__ void __launch_bounds__(256) k_calib_cells(CalibCellArgs a) {
         pb *= a.inv_n;
         double Fb = 0.0, Sb = 0.0, Db = 0.0;
         if (T > 0.0) {
-            Fb = -pb * (ms + md) / (T * T);
-            Sb = pb * mf / (T * T);
+            const double pbT2 = pb * iT * iT;
+            Fb = -pbT2 * (ms + md);
+            Sb = pbT2 * mf;
             Db = Sb;
         }
-        for (int k = a.F - 1; k >= 0; --k) {
-            const FrameBar b = frame_adjoint(in[k], a.mass_scale, Fb, Sb, Db);
-            const double* s = a.sums + (long)k * 4 * C;
-            // E = sigma F: dE/dsigma = F, dE/dls = sigma H / ls
-            g_sig += b.Eo * s[c] + b.Ef * s[C + c];
-            g_ls += (b.Eo * s[2 * C + c] + b.Ef * s[3 * C + c]) * a.sigma / a.ls;
-            if (k > 0 && a.dt[k] > 0.0f) g_gam += b.g * (double)a.dt[k] * pow(a.gamma, (double)a.dt[k] - 1.0);
-            Fb = b.mf; Sb = b.ms; Db = b.md;
+#pragma unroll(NF <= 4 ? NF : 1)
+        for (int k = NF - 1; k >= 0; --k) {
+            if (k < a.F) {
+                const FrameBar b = frame_adjoint(in[k], a.k2, Fb, Sb, Db);
+                const double* s = a.sums + (long)k * 4 * C;
+                // E = sigma F: dE/dsigma = F, dE/dls = sigma H / ls
+                g_sig += b.Eo * s[c] + b.Ef * s[C + c];
+                g_ls += (b.Eo * s[2 * C + c] + b.Ef * s[3 * C + c]) * a.sigma / a.ls;
+                g_gam += b.g * a.gd[k];
+                Fb = b.mf; Sb = b.ms; Db = b.md;
+            }
         }
         g_pf += Fb;
         g_po += (Sb + Db) / 2.0;
@@ -449,7 +469,7 @@ TileShape calib_tiles(const DevParams& p) {
     const bool large = (long)p.C >= (1L << 20) && p.Gz >= 8;
     t.tx = large ? 16 : 8;
     t.ty = large ? 16 : 8;
-    t.tz = large ? 8 : 4;
+    t.tz = 4;
     t.ntx = (p.G + t.tx - 1) / t.tx;
     t.nty = (p.G + t.ty - 1) / t.ty;
     t.ntz = (p.Gz + t.tz - 1) / t.tz;
@@ -473,7 +493,7 @@ cudaError_t ensure_ray_buffers(k3dom_calib* c, int max_points, float ls, const S
     const int N = std::max(max_points, 1);
     long cap = std::min(need + need / 4, 0xFFFFFFF0L);
     rb.capacity = cap;
-    rb.chunk = 1024;
+    rb.chunk = 512;
     std::vector<void*>* L = &c->ray_allocs;
     cudaError_t e;
     if ((e = c->alloc(&rb.ray_a, N, L)) || (e = c->alloc(&rb.ray_c, N, L)) || (e = c->alloc(&rb.counts, N, L)) ||
@@ -594,10 +614,12 @@ k3dom_status run_cells(k3dom_calib* c, const float theta[5], bool grad, float* o
     a.gamma = theta[2];
     a.prior_occ = theta[3];
     a.prior_free = theta[4];
-    a.mass_scale = c->dp.mass_scale;
+    a.k2 = 2.0 / (double)c->dp.mass_scale;
     a.inv_n = c->n_labels > 0.0 ? 1.0 / c->n_labels : 0.0;
     for (int k = 0; k < a.F; ++k) {
-        a.dt[k] = c->frames[k].dt;
+        const double dt = c->frames[k].dt;
+        a.g[k] = k == 0 ? 1.0 : std::pow(a.gamma, dt);
+        a.gd[k] = (k > 0 && dt > 0.0) ? dt * std::pow(a.gamma, dt - 1.0) : 0.0;
         a.dyn[k] = c->frames[k].dyn;
     }
     a.sums = c->sums;
@@ -609,7 +631,12 @@ k3dom_status run_cells(k3dom_calib* c, const float theta[5], bool grad, float* o
     cudaError_t e;
     if ((e = cudaMemsetAsync(c->red, 0, 6 * sizeof(double), c->st))) return c->fail(e);
     ++g_launches;
-    k_calib_cells<<<grid_for(a.C), 256, 0, c->st>>>(a);
+    // one wave of resident blocks: each block reduces its partial sums once, at the end
+    auto kern = a.F <= 2 ? k_calib_cells<2> : a.F <= 4 ? k_calib_cells<4> : k_calib_cells<kMaxCalibFrames>;
+    int per_sm = 1;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, 256, 0);
+    const long blocks = std::min<long>((long)c->num_sms * std::max(1, per_sm), (a.C + 255) / 256);
+    kern<<<(unsigned)std::max(1L, blocks), 256, 0, c->st>>>(a);
     if ((e = cudaGetLastError()) || (e = cudaMemcpyAsync(c->red_host, c->red, 6 * sizeof(double),
                                                          cudaMemcpyDeviceToHost, c->st)) ||
         (e = cudaStreamSynchronize(c->st)))

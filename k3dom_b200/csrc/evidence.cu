@@ -505,18 +505,6 @@ __device__ __forceinline__ float kernel_tab(const float4* __restrict__ tab, floa
     return fmaf(f, fmaf(f, fmaf(f, c.w, c.z), c.y), c.x);
 }
 
-// Kernel value rounded to an integer number of fixed-point units (the table is pre-scaled, so
-// one unit is 2^-k sigma), clamped at 0 as k(d) = max(0, ...) is. For 0 <= v < 2^23 adding 2^23
-// lands in [2^23, 2^24), where the float spacing is 1, so the add rounds v to the nearest
-// integer and the subtraction is exact; larger floats are integers already. Sums of such
-// integers below 2^53 are exact in FP64, so the FP64 accumulation is exact and its result does
-// not depend on the order of the terms.
-__device__ __forceinline__ double kernel_units(float v) {
-    v = fmaxf(v, 0.0f);
-    const float r = __fsub_rn(__fadd_rn(v, 8388608.0f), 8388608.0f);
-    return (double)(v < 8388608.0f ? r : v);
-}
-
 __device__ __forceinline__ double calc_credit(double mass, double mass_scale) {
     // mass_update.cu:12-14
     return 1.0 - 2.0 / (1.0 + exp(2.0 * mass / mass_scale));
@@ -1109,27 +1097,43 @@ void build_calib_tables(float4* f_tab, float4* dls_tab) {
     build_table(unit_kernel_dls, std::ldexp(1.0, kCalibShift), dls_tab);
 }
 
-// Signed rounding to the nearest integer (|v| < 2^23 by the magic add, larger floats are
-// integers already).
-__device__ __forceinline__ double signed_units(float v) {
-    const float a = fabsf(v);
-    const float r = a < 8388608.0f ? __fsub_rn(__fadd_rn(a, 8388608.0f), 8388608.0f) : a;
-    return (double)copysignf(r, v);
-}
-
+// Shared memory of k_bgki_sums (dynamic, sized by the work item's ray count).
 struct CalibSmem {
-    float4 ftab[kKernelTab];
-    float4 htab[kKernelTab];
-    float4 a[kChunk];
-    double4 c[kChunk];
-    float4 stage[kEvWarps][32][3];
+    float4* ftab;            // [kKernelTab] unit kernel f, fixed-point scale folded in
+    float4* htab;            // [kKernelTab] -x f'(x), same scale
+    float4 (*stage)[32][3];  // [kEvWarps][32][3]
+    float (*near)[32];       // [kEvWarps][32]
+    float4* a;               // [chunk]
+    double4* c;              // [chunk]
 };
 
-// acc4: 4 signed 64-bit sums per cell (f occ, f free, -x f' occ, -x f' free), in units.
-__global__ void __launch_bounds__(kEvThreads, 2) k_bgki_sums(EvArgs A, const float4* __restrict__ htab,
+constexpr size_t kCalibFixedBytes =
+    2 * sizeof(float4) * kKernelTab + sizeof(float4) * kEvWarps * 32 * 3 + sizeof(float) * kEvWarps * 32;
+
+inline size_t calib_smem_bytes(int chunk) {
+    return ((kCalibFixedBytes + 31) & ~(size_t)31) + (size_t)chunk * (sizeof(float4) + sizeof(double4));
+}
+
+__device__ __forceinline__ CalibSmem calib_smem(unsigned char* base, int chunk) {
+    CalibSmem S;
+    S.ftab = reinterpret_cast<float4*>(base);
+    S.htab = S.ftab + kKernelTab;
+    S.stage = reinterpret_cast<float4(*)[32][3]>(base + 2 * sizeof(float4) * kKernelTab);
+    S.near = reinterpret_cast<float(*)[32]>(base + 2 * sizeof(float4) * kKernelTab +
+                                             sizeof(float4) * kEvWarps * 32 * 3);
+    const size_t off = (kCalibFixedBytes + 31) & ~(size_t)31;
+    S.c = reinterpret_cast<double4*>(base + off);
+    S.a = reinterpret_cast<float4*>(base + off + sizeof(double4) * (size_t)chunk);
+    return S;
+}
+
+// acc4: 4 signed 64-bit sums per cell (f occ, f free, -x f' occ, -x f' free), in units. Same
+// tiles, culls and pair geometry as k_bgki; each value is rounded once to an integer number of
+// units (round to nearest even).
+__global__ void __launch_bounds__(kEvThreads, 3) k_bgki_sums(EvArgs A, const float4* __restrict__ htab,
                                                             unsigned long long* __restrict__ acc4) {
-    extern __shared__ __align__(16) unsigned char smem_raw[];
-    CalibSmem& S = *reinterpret_cast<CalibSmem*>(smem_raw);
+    extern __shared__ __align__(32) unsigned char smem_raw[];
+    const CalibSmem S = calib_smem(smem_raw, A.chunk);
     __shared__ uint32_t s_item;
     __shared__ int s_next_sb;
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
@@ -1173,8 +1177,9 @@ __global__ void __launch_bounds__(kEvThreads, 2) k_bgki_sums(EvArgs A, const flo
             if (sb >= nsb) break;
             const CellLoc L = locate(p, ts, it.lt, sb, lane, fp.sensor_x, fp.sensor_y, fp.sensor_z);
             const float dx = L.x - L.ox, dy = L.y - L.oy, dz = L.z - L.oz;
+            const float ls2c = L.c >= 0 ? ls2 : -1.0f;
             const double ox = L.ox, oy = L.oy, oz = L.oz;
-            double fo = 0.0, ff = 0.0, ho = 0.0, hf = 0.0;  // exact sums of integer units
+            long long fo = 0, ff = 0, ho = 0, hf = 0;
             for (int g0 = 0; g0 < nr; g0 += 32) {
                 const int r = g0 + lane;
                 bool hit = false;
@@ -1192,10 +1197,12 @@ __global__ void __launch_bounds__(kEvThreads, 2) k_bgki_sums(EvArgs A, const flo
                     const float qal = fminf(qpar, 0.0f) + fmaxf(qpar - a.w, 0.0f);
                     hit = qx * qx + qy * qy + qz * qz + qal * qal < cull_r2;
                     if (hit) {
+                        const float ex = (float)(ox - a.x), ey = (float)(oy - a.y), ez = (float)(oz - a.z);
+                        const float cx = ex - hres, cy = ey - hres, cz = ez - hres;
                         S.stage[wid][lane][0] = make_float4((float)par0, (float)(par0 - cd.y), (float)(par0 - cd.x), ux);
                         S.stage[wid][lane][1] = make_float4((float)px, (float)py, (float)pz, uy);
-                        S.stage[wid][lane][2] =
-                            make_float4((float)(ox - a.x), (float)(oy - a.y), (float)(oz - a.z), uz);
+                        S.stage[wid][lane][2] = make_float4(ex, ey, ez, uz);
+                        S.near[wid][lane] = cx * cx + cy * cy + cz * cz < cull_r2 ? 1.0f : 0.0f;
                     }
                 }
                 unsigned mask = __ballot_sync(0xffffffffu, hit);
@@ -1204,12 +1211,14 @@ __global__ void __launch_bounds__(kEvThreads, 2) k_bgki_sums(EvArgs A, const flo
                     const int j = __ffs(mask) - 1;
                     mask &= mask - 1;
                     const float4 s0 = S.stage[wid][j][0], s1 = S.stage[wid][j][1], s2 = S.stage[wid][j][2];
-                    const float vx = s2.x + dx, vy = s2.y + dy, vz = s2.z + dz;
-                    const float d2o = vx * vx + vy * vy + vz * vz;
-                    if (d2o < ls2 && L.c >= 0) {
-                        const float u = d2o * inv_ls2;
-                        fo += kernel_units(kernel_tab(S.ftab, u));
-                        ho += signed_units(kernel_tab(S.htab, u));
+                    if (S.near[wid][j] != 0.0f) {
+                        const float vx = s2.x + dx, vy = s2.y + dy, vz = s2.z + dz;
+                        const float d2o = vx * vx + vy * vy + vz * vz;
+                        if (d2o < ls2c) {
+                            const float u = d2o * inv_ls2;
+                            fo += __float2ll_rn(fmaxf(kernel_tab(S.ftab, u), 0.0f));
+                            ho += __float2ll_rn(kernel_tab(S.htab, u));
+                        }
                     }
                     const float dpar = dx * s0.w + dy * s1.w + dz * s2.w;
                     if (s0.z + dpar < 0.0f) {
@@ -1217,10 +1226,10 @@ __global__ void __launch_bounds__(kEvThreads, 2) k_bgki_sums(EvArgs A, const flo
                                     qz = s1.z + dz - dpar * s2.w;
                         const float al = fminf(s0.x + dpar, 0.0f) + fmaxf(s0.y + dpar, 0.0f);
                         const float d2f = qx * qx + qy * qy + qz * qz + al * al;
-                        if (d2f < ls2 && L.c >= 0) {
+                        if (d2f < ls2c) {
                             const float u = d2f * inv_ls2;
-                            ff += kernel_units(kernel_tab(S.ftab, u));
-                            hf += signed_units(kernel_tab(S.htab, u));
+                            ff += __float2ll_rn(fmaxf(kernel_tab(S.ftab, u), 0.0f));
+                            hf += __float2ll_rn(kernel_tab(S.htab, u));
                         }
                     }
                 }
@@ -1228,12 +1237,10 @@ __global__ void __launch_bounds__(kEvThreads, 2) k_bgki_sums(EvArgs A, const flo
             }
             if (L.c >= 0) {
                 unsigned long long* ac = acc4 + 4 * (long)(coff + L.c);
-                const long long v0 = __double2ll_rn(fo), v1 = __double2ll_rn(ff), v2 = __double2ll_rn(ho),
-                                v3 = __double2ll_rn(hf);
-                if (v0) atomicAdd(ac, (unsigned long long)v0);
-                if (v1) atomicAdd(ac + 1, (unsigned long long)v1);
-                if (v2) atomicAdd(ac + 2, (unsigned long long)v2);
-                if (v3) atomicAdd(ac + 3, (unsigned long long)v3);
+                if (fo) atomicAdd(ac, (unsigned long long)fo);
+                if (ff) atomicAdd(ac + 1, (unsigned long long)ff);
+                if (ho) atomicAdd(ac + 2, (unsigned long long)ho);
+                if (hf) atomicAdd(ac + 3, (unsigned long long)hf);
             }
         }
         __syncthreads();
@@ -1245,10 +1252,11 @@ cudaError_t launch_bgki_sums(const Batch& bt, RayBuffers& rb, const float4* f_ta
     if (rb.chunk < 32 || rb.chunk > kChunk) return cudaErrorInvalidValue;
     EvArgs A = make_args(bt, rb, CellState{}, CellWork{}, false, status);
     A.ktab = f_tab;
+    const size_t sm = calib_smem_bytes(rb.chunk);
     int per_sm = 1;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_bgki_sums, kEvThreads, sizeof(CalibSmem));
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_bgki_sums, kEvThreads, sm);
     ++g_launches;
-    k_bgki_sums<<<num_sms * std::max(1, per_sm), kEvThreads, sizeof(CalibSmem), st>>>(A, dls_tab, acc4);
+    k_bgki_sums<<<num_sms * std::max(1, per_sm), kEvThreads, sm, st>>>(A, dls_tab, acc4);
     return cudaGetLastError();
 }
 
@@ -1300,7 +1308,8 @@ cudaError_t evidence_init() {
     if ((e = cudaFuncSetAttribute(k_bgki<4>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                   (int)bgki_smem_bytes(kChunk))))
         return e;
-    return cudaFuncSetAttribute(k_bgki_sums, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(CalibSmem));
+    return cudaFuncSetAttribute(k_bgki_sums, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)calib_smem_bytes(kChunk));
 }
 
 }  // namespace k3dom
