@@ -59,6 +59,7 @@ struct SceneOffsets {
 // Per-frame scalars, resident in device memory so a captured graph can be replayed.
 struct FrameParams {
     float dt;
+    double gamma_dt;  // gamma^dt of the scene (the prediction's decay), FP64
     float sensor_x, sensor_y, sensor_z;  // sensor position minus map centre [m]
     int n_points;
     uint32_t frame;

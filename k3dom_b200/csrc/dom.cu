@@ -409,6 +409,7 @@ k3dom_status set_frame_params(k3dom_handle* h, const float* dt, const int* n_poi
         const SceneHost& x = h->sc[s];
         FrameParams& f = h->fp_host[s];
         f.dt = dt[s];
+        f.gamma_dt = std::pow((double)x.dp.gamma, (double)dt[s]);
         f.sensor_x = x.sensor_pos[0] - x.center_pos[0];
         f.sensor_y = x.sensor_pos[1] - x.center_pos[1];
         f.sensor_z = x.sensor_pos[2] - x.center_pos[2];

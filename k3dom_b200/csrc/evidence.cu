@@ -505,13 +505,14 @@ __device__ __forceinline__ float kernel_tab(const float4* __restrict__ tab, floa
     return fmaf(f, fmaf(f, fmaf(f, c.w, c.z), c.y), c.x);
 }
 
-__device__ __forceinline__ double calc_credit(double mass, double mass_scale) {
-    // mass_update.cu:12-14
-    return 1.0 - 2.0 / (1.0 + exp(2.0 * mass / mass_scale));
+// mass_update.cu:12-14, 1 - 2 / (1 + exp(2 mass / mass_scale)), with k2 = 2 / mass_scale
+__device__ __forceinline__ double calc_credit(double mass, double k2) {
+    return 1.0 - 2.0 / (1.0 + exp(mass * k2));
 }
 __device__ __forceinline__ double positive_diff(double a, double b) { return fmax(0.0, a - b); }
+// mass_update.cu:16-19, 1 / (1 + rest / numerator), written numerator / (numerator + rest)
 __device__ __forceinline__ double calc_ratio(double numerator, double rest) {
-    return (numerator <= 0.0 || rest < 0.0) ? 0.0 : (1.0 / (1.0 + rest / numerator));
+    return (numerator <= 0.0 || rest < 0.0) ? 0.0 : numerator / (numerator + rest);
 }
 __device__ __forceinline__ float calc_norm(float weight_sum, float rho_p) {
     return weight_sum > 0.0f ? rho_p / weight_sum : 0.0f;
@@ -520,13 +521,14 @@ __device__ __forceinline__ float calc_norm(float weight_sum, float rho_p) {
 // gridCellPredictionUpdateKernel's per-cell body (mass_update.cu:163-181) plus the per-cell
 // updates of the persistent-particle and moment stages. Masses are stored in FP32; the update
 // is evaluated in FP64 (it has several cancelling differences) and rounded once.
-__device__ void k3dom_cell_update(const DevParams& p, float dt, int c, double del_occ, double del_free,
+// g = gamma^dt of the frame.
+__device__ void k3dom_cell_update(const DevParams& p, double g, int c, double del_occ, double del_free,
                                   CellState cs, CellWork cw, bool first_frame) {
     double m_f = cs.free_m[c], m_s = cs.static_m[c], m_d = cs.dyn_m[c];
     const int start = first_frame ? -1 : cw.start[c];
     const bool has = start >= 0;
     const double dyn_pred = has ? (double)cw.sum_w[c] : 0.0;
-    const double g = pow((double)p.gamma, (double)dt);
+    const double k2 = 2.0 / (double)p.mass_scale;
     const double pred_total = (m_f + m_d) * g;
     // predict_mass (:79-84)
     m_s *= g;
@@ -538,12 +540,15 @@ __device__ void k3dom_cell_update(const DevParams& p, float dt, int c, double de
         const double prime_sigma = m_f + m_s + m_d;
         double l_DtoF = 0.0, l_StoFD = 0.0, l_FtoD = 0.0;
         if (prime_sigma > 0.0) {
-            const double credit = calc_credit(sqrt(del_sigma * prime_sigma), p.mass_scale);
-            const double base_f = credit * positive_diff(del_free, del_occ) / del_sigma;
-            const double base_o = credit * positive_diff(del_occ, del_free) / del_sigma;
-            l_DtoF = base_f * m_d / prime_sigma;
-            l_StoFD = base_f * positive_diff(m_s + m_d, m_f) / prime_sigma;
-            l_FtoD = base_o * positive_diff(m_f, m_s + m_d) / prime_sigma;
+            // base_f m / prime_sigma with base_f = credit (del_free - del_occ)+ / del_sigma:
+            // one reciprocal of z = del_sigma prime_sigma serves the three fractions
+            const double z = del_sigma * prime_sigma;
+            const double w = calc_credit(sqrt(z), k2) / z;
+            const double wf = w * positive_diff(del_free, del_occ);
+            const double wo = w * positive_diff(del_occ, del_free);
+            l_DtoF = wf * m_d;
+            l_StoFD = wf * positive_diff(m_s + m_d, m_f);
+            l_FtoD = wo * positive_diff(m_f, m_s + m_d);
         }
         const double diff_f = l_StoFD / 2.0 * m_s + l_DtoF * m_d - l_FtoD * m_f;
         const double diff_s = -l_StoFD * m_s;
@@ -551,7 +556,7 @@ __device__ void k3dom_cell_update(const DevParams& p, float dt, int c, double de
         m_f += diff_f;
         m_s += diff_s;
         m_d += diff_d;
-        const double credit2 = calc_credit(m_s + m_d, p.mass_scale);
+        const double credit2 = calc_credit(m_s + m_d, k2);
         const double beta = (1.0 - credit2) + credit2 * calc_ratio(m_s, m_d);
         m_s = m_s + beta * del_occ;
         m_d = m_d + (1.0 - beta) * del_occ;
@@ -578,9 +583,10 @@ __device__ void k3dom_cell_update(const DevParams& p, float dt, int c, double de
     // statisticalMomentsKernel2 with sum(w' v) = mu_UA * sum(w v)
     double vx = 0.0, vy = 0.0, vz = 0.0;
     if (has && pers > 0.0) {
-        vx = mu_UA * (double)cw.sum_wvx[c] / pers;
-        vy = mu_UA * (double)cw.sum_wvy[c] / pers;
-        vz = mu_UA * (double)cw.sum_wvz[c] / pers;
+        const double q = mu_UA / pers;
+        vx = q * (double)cw.sum_wvx[c];
+        vy = q * (double)cw.sum_wvy[c];
+        vz = q * (double)cw.sum_wvz[c];
     }
     cs.mvx[c] = (float)vx;
     cs.mvy[c] = (float)vy;
@@ -593,13 +599,11 @@ __device__ void k3dom_cell_update(const DevParams& p, float dt, int c, double de
 struct BgkiSmem {
     float4* ktab;                 // [kKernelTab] sparse-kernel table of the current scene
     float4 (*stage)[32][3];       // [kEvWarps][32][3]
-    float (*near)[32];            // [kEvWarps][32]: 1 where the point's sphere can reach the sub-block
     float4* a;                    // [chunk] m.x, m.y, m.z, d_m
     double4* c;                   // [chunk] d_m, margin, 1/d_m
 };
 
-constexpr size_t kBgkiFixedBytes =
-    sizeof(float4) * kKernelTab + sizeof(float4) * kEvWarps * 32 * 3 + sizeof(float) * kEvWarps * 32;
+constexpr size_t kBgkiFixedBytes = sizeof(float4) * kKernelTab + sizeof(float4) * kEvWarps * 32 * 3;
 
 inline size_t bgki_smem_bytes(int chunk) {
     return ((kBgkiFixedBytes + 31) & ~(size_t)31) + (size_t)chunk * (sizeof(float4) + sizeof(double4));
@@ -609,7 +613,6 @@ __device__ __forceinline__ BgkiSmem bgki_smem(unsigned char* base, int chunk) {
     BgkiSmem S;
     S.ktab = reinterpret_cast<float4*>(base);
     S.stage = reinterpret_cast<float4(*)[32][3]>(base + sizeof(float4) * kKernelTab);
-    S.near = reinterpret_cast<float(*)[32]>(base + sizeof(float4) * kKernelTab + sizeof(float4) * kEvWarps * 32 * 3);
     const size_t off = (kBgkiFixedBytes + 31) & ~(size_t)31;
     S.c = reinterpret_cast<double4*>(base + off);  // 32-byte aligned
     S.a = reinterpret_cast<float4*>(base + off + sizeof(double4) * (size_t)chunk);
@@ -680,7 +683,7 @@ __global__ void __launch_bounds__(kEvThreads, MINB) k_bgki(EvArgs A) {
             long long ao = 0, af = 0;  // sums of kernel values rounded to integer units
             for (int g0 = 0; g0 < nr; g0 += 32) {
                 const int r = g0 + lane;
-                bool hit = false;
+                bool hit = false, near = false;
                 if (r < nr) {
                     const float4 a = S.a[r];
                     const double4 cd = S.c[r];
@@ -703,30 +706,19 @@ __global__ void __launch_bounds__(kEvThreads, MINB) k_bgki(EvArgs A) {
                         S.stage[wid][lane][0] = make_float4((float)par0, (float)(par0 - cd.y), (float)(par0 - cd.x), ux);
                         S.stage[wid][lane][1] = make_float4((float)px, (float)py, (float)pz, uy);
                         S.stage[wid][lane][2] = make_float4(ex, ey, ez, uz);
-                        S.near[wid][lane] = cx * cx + cy * cy + cz * cz < cull_r2 ? 1.0f : 0.0f;
+                        near = cx * cx + cy * cy + cz * cz < cull_r2;
                     }
                 }
-                unsigned mask = __ballot_sync(0xffffffffu, hit);
+                const unsigned hits = __ballot_sync(0xffffffffu, hit);
+                unsigned mnear = __ballot_sync(0xffffffffu, near);
+                unsigned mfar = hits & ~mnear;
                 __syncwarp();
-                while (mask) {
-                    const int j = __ffs(mask) - 1;
-                    mask &= mask - 1;
-                    const float4 s0 = S.stage[wid][j][0], s1 = S.stage[wid][j][1], s2 = S.stage[wid][j][2];
-                    // occupied evidence (mass_update.cu:48-52), only where the point's sphere can
-                    // reach the sub-block (the same for every lane: j is)
-                    if (S.near[wid][j] != 0.0f) {
-                        const float vx = s2.x + dx, vy = s2.y + dy, vz = s2.z + dz;
-                        const float d2o = vx * vx + vy * vy + vz * vz;
-                        if (d2o < ls2c) {
-                            ao += __float2ll_rn(fmaxf(kernel_tab(S.ktab, d2o * inv_ls2), 0.0f));
-                            ++nev;
-                        }
-                    }
-                    // free evidence (:54-71)
-                    const float dpar = dx * s0.w + dy * s1.w + dz * s2.w;
+                // free evidence (:54-71) of staged ray j for this lane's cell
+                auto free_term = [&](const float4& s0, const float4& s1, float uz) {
+                    const float dpar = dx * s0.w + dy * s1.w + dz * uz;
                     if (s0.z + dpar < 0.0f) {  // d_proj < d_m
                         const float qx = s1.x + dx - dpar * s0.w, qy = s1.y + dy - dpar * s1.w,
-                                    qz = s1.z + dz - dpar * s2.w;
+                                    qz = s1.z + dz - dpar * uz;
                         const float al = fminf(s0.x + dpar, 0.0f) + fmaxf(s0.y + dpar, 0.0f);
                         const float d2f = qx * qx + qy * qy + qz * qz + al * al;
                         if (d2f < ls2c) {
@@ -734,6 +726,25 @@ __global__ void __launch_bounds__(kEvThreads, MINB) k_bgki(EvArgs A) {
                             ++nev;
                         }
                     }
+                };
+                // rays whose point's sphere can reach the sub-block: occupied (:48-52) and free
+                while (mnear) {
+                    const int j = __ffs(mnear) - 1;
+                    mnear &= mnear - 1;
+                    const float4 s0 = S.stage[wid][j][0], s1 = S.stage[wid][j][1], s2 = S.stage[wid][j][2];
+                    const float vx = s2.x + dx, vy = s2.y + dy, vz = s2.z + dz;
+                    const float d2o = vx * vx + vy * vy + vz * vz;
+                    if (d2o < ls2c) {
+                        ao += __float2ll_rn(fmaxf(kernel_tab(S.ktab, d2o * inv_ls2), 0.0f));
+                        ++nev;
+                    }
+                    free_term(s0, s1, s2.w);
+                }
+                // the other rays: free evidence only
+                while (mfar) {
+                    const int j = __ffs(mfar) - 1;
+                    mfar &= mfar - 1;
+                    free_term(S.stage[wid][j][0], S.stage[wid][j][1], S.stage[wid][j][2].w);
                 }
                 __syncwarp();
             }
@@ -764,7 +775,7 @@ __global__ void __launch_bounds__(kEvThreads, MINB) k_bgki(EvArgs A) {
                 const long long ff = (long long)__ldcg(ac + 1);
                 if (fo) __stcg(ac, 0ull);
                 if (ff) __stcg(ac + 1, 0ull);
-                k3dom_cell_update(p, fp.dt, c, (double)fo * sd.fx_inv, (double)ff * sd.fx_inv, A.cs, A.cw,
+                k3dom_cell_update(p, fp.gamma_dt, c, (double)fo * sd.fx_inv, (double)ff * sd.fx_inv, A.cs, A.cw,
                                   A.first_frame != 0);
             }
             if (threadIdx.x == 0) A.tile_done[it.t] = 0;
@@ -1102,13 +1113,11 @@ struct CalibSmem {
     float4* ftab;            // [kKernelTab] unit kernel f, fixed-point scale folded in
     float4* htab;            // [kKernelTab] -x f'(x), same scale
     float4 (*stage)[32][3];  // [kEvWarps][32][3]
-    float (*near)[32];       // [kEvWarps][32]
     float4* a;               // [chunk]
     double4* c;              // [chunk]
 };
 
-constexpr size_t kCalibFixedBytes =
-    2 * sizeof(float4) * kKernelTab + sizeof(float4) * kEvWarps * 32 * 3 + sizeof(float) * kEvWarps * 32;
+constexpr size_t kCalibFixedBytes = 2 * sizeof(float4) * kKernelTab + sizeof(float4) * kEvWarps * 32 * 3;
 
 inline size_t calib_smem_bytes(int chunk) {
     return ((kCalibFixedBytes + 31) & ~(size_t)31) + (size_t)chunk * (sizeof(float4) + sizeof(double4));
@@ -1119,8 +1128,6 @@ __device__ __forceinline__ CalibSmem calib_smem(unsigned char* base, int chunk) 
     S.ftab = reinterpret_cast<float4*>(base);
     S.htab = S.ftab + kKernelTab;
     S.stage = reinterpret_cast<float4(*)[32][3]>(base + 2 * sizeof(float4) * kKernelTab);
-    S.near = reinterpret_cast<float(*)[32]>(base + 2 * sizeof(float4) * kKernelTab +
-                                             sizeof(float4) * kEvWarps * 32 * 3);
     const size_t off = (kCalibFixedBytes + 31) & ~(size_t)31;
     S.c = reinterpret_cast<double4*>(base + off);
     S.a = reinterpret_cast<float4*>(base + off + sizeof(double4) * (size_t)chunk);
@@ -1130,8 +1137,9 @@ __device__ __forceinline__ CalibSmem calib_smem(unsigned char* base, int chunk) 
 // acc4: 4 signed 64-bit sums per cell (f occ, f free, -x f' occ, -x f' free), in units. Same
 // tiles, culls and pair geometry as k_bgki; each value is rounded once to an integer number of
 // units (round to nearest even).
-__global__ void __launch_bounds__(kEvThreads, 3) k_bgki_sums(EvArgs A, const float4* __restrict__ htab,
-                                                            unsigned long long* __restrict__ acc4) {
+template <int MINB>
+__global__ void __launch_bounds__(kEvThreads, MINB) k_bgki_sums(EvArgs A, const float4* __restrict__ htab,
+                                                               unsigned long long* __restrict__ acc4) {
     extern __shared__ __align__(32) unsigned char smem_raw[];
     const CalibSmem S = calib_smem(smem_raw, A.chunk);
     __shared__ uint32_t s_item;
@@ -1182,7 +1190,7 @@ __global__ void __launch_bounds__(kEvThreads, 3) k_bgki_sums(EvArgs A, const flo
             long long fo = 0, ff = 0, ho = 0, hf = 0;
             for (int g0 = 0; g0 < nr; g0 += 32) {
                 const int r = g0 + lane;
-                bool hit = false;
+                bool hit = false, near = false;
                 if (r < nr) {
                     const float4 a = S.a[r];
                     const double4 cd = S.c[r];
@@ -1202,28 +1210,18 @@ __global__ void __launch_bounds__(kEvThreads, 3) k_bgki_sums(EvArgs A, const flo
                         S.stage[wid][lane][0] = make_float4((float)par0, (float)(par0 - cd.y), (float)(par0 - cd.x), ux);
                         S.stage[wid][lane][1] = make_float4((float)px, (float)py, (float)pz, uy);
                         S.stage[wid][lane][2] = make_float4(ex, ey, ez, uz);
-                        S.near[wid][lane] = cx * cx + cy * cy + cz * cz < cull_r2 ? 1.0f : 0.0f;
+                        near = cx * cx + cy * cy + cz * cz < cull_r2;
                     }
                 }
-                unsigned mask = __ballot_sync(0xffffffffu, hit);
+                const unsigned hits = __ballot_sync(0xffffffffu, hit);
+                unsigned mnear = __ballot_sync(0xffffffffu, near);
+                unsigned mfar = hits & ~mnear;
                 __syncwarp();
-                while (mask) {
-                    const int j = __ffs(mask) - 1;
-                    mask &= mask - 1;
-                    const float4 s0 = S.stage[wid][j][0], s1 = S.stage[wid][j][1], s2 = S.stage[wid][j][2];
-                    if (S.near[wid][j] != 0.0f) {
-                        const float vx = s2.x + dx, vy = s2.y + dy, vz = s2.z + dz;
-                        const float d2o = vx * vx + vy * vy + vz * vz;
-                        if (d2o < ls2c) {
-                            const float u = d2o * inv_ls2;
-                            fo += __float2ll_rn(fmaxf(kernel_tab(S.ftab, u), 0.0f));
-                            ho += __float2ll_rn(kernel_tab(S.htab, u));
-                        }
-                    }
-                    const float dpar = dx * s0.w + dy * s1.w + dz * s2.w;
+                auto free_term = [&](const float4& s0, const float4& s1, float uz) {
+                    const float dpar = dx * s0.w + dy * s1.w + dz * uz;
                     if (s0.z + dpar < 0.0f) {
                         const float qx = s1.x + dx - dpar * s0.w, qy = s1.y + dy - dpar * s1.w,
-                                    qz = s1.z + dz - dpar * s2.w;
+                                    qz = s1.z + dz - dpar * uz;
                         const float al = fminf(s0.x + dpar, 0.0f) + fmaxf(s0.y + dpar, 0.0f);
                         const float d2f = qx * qx + qy * qy + qz * qz + al * al;
                         if (d2f < ls2c) {
@@ -1232,6 +1230,24 @@ __global__ void __launch_bounds__(kEvThreads, 3) k_bgki_sums(EvArgs A, const flo
                             hf += __float2ll_rn(kernel_tab(S.htab, u));
                         }
                     }
+                };
+                while (mnear) {
+                    const int j = __ffs(mnear) - 1;
+                    mnear &= mnear - 1;
+                    const float4 s0 = S.stage[wid][j][0], s1 = S.stage[wid][j][1], s2 = S.stage[wid][j][2];
+                    const float vx = s2.x + dx, vy = s2.y + dy, vz = s2.z + dz;
+                    const float d2o = vx * vx + vy * vy + vz * vz;
+                    if (d2o < ls2c) {
+                        const float u = d2o * inv_ls2;
+                        fo += __float2ll_rn(fmaxf(kernel_tab(S.ftab, u), 0.0f));
+                        ho += __float2ll_rn(kernel_tab(S.htab, u));
+                    }
+                    free_term(s0, s1, s2.w);
+                }
+                while (mfar) {
+                    const int j = __ffs(mfar) - 1;
+                    mfar &= mfar - 1;
+                    free_term(S.stage[wid][j][0], S.stage[wid][j][1], S.stage[wid][j][2].w);
                 }
                 __syncwarp();
             }
@@ -1253,10 +1269,12 @@ cudaError_t launch_bgki_sums(const Batch& bt, RayBuffers& rb, const float4* f_ta
     EvArgs A = make_args(bt, rb, CellState{}, CellWork{}, false, status);
     A.ktab = f_tab;
     const size_t sm = calib_smem_bytes(rb.chunk);
+    // 4 CTAs per SM where a 512-ray chunk leaves the shared memory for them, else 3
+    auto kern = rb.chunk <= 512 ? k_bgki_sums<4> : k_bgki_sums<3>;
     int per_sm = 1;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_bgki_sums, kEvThreads, sm);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kEvThreads, sm);
     ++g_launches;
-    k_bgki_sums<<<num_sms * std::max(1, per_sm), kEvThreads, sm, st>>>(A, dls_tab, acc4);
+    kern<<<num_sms * std::max(1, per_sm), kEvThreads, sm, st>>>(A, dls_tab, acc4);
     return cudaGetLastError();
 }
 
@@ -1308,7 +1326,10 @@ cudaError_t evidence_init() {
     if ((e = cudaFuncSetAttribute(k_bgki<4>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                   (int)bgki_smem_bytes(kChunk))))
         return e;
-    return cudaFuncSetAttribute(k_bgki_sums, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    if ((e = cudaFuncSetAttribute(k_bgki_sums<3>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)calib_smem_bytes(kChunk))))
+        return e;
+    return cudaFuncSetAttribute(k_bgki_sums<4>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                 (int)calib_smem_bytes(kChunk));
 }
 
