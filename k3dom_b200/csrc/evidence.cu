@@ -628,6 +628,49 @@ __device__ __forceinline__ BgkiSmem bgki_smem(unsigned char* base, int chunk) {
 //   distance to the point = |occ0 + delta|.
 // Every FP32 quantity is O(ls), so the FP32 evaluation keeps ~1e-7 relative accuracy at any
 // distance from the sensor (the direct |c|^2 - d_proj^2 form of :60 loses ~1e-5 at 20 m).
+//
+// stage_pair culls the pair on the sub-block centroid and, for a pair that passes, stages three
+// float4: st[0] = (perp0, par0), st[1] = (u, par0 - margin), st[2] = (occ0, par0 - d_m).
+// *near: the point lies within the cull radius of the centroid, i.e. its sphere of radius ls can
+// reach a cell of the sub-block. For the other rays no cell of the sub-block with d_proj >= d_m
+// is within ls of the free segment either (margin <= d_m, so such a cell is at least as far from
+// the segment's end as from the point, and the cull radius exceeds ls + half the sub-block
+// diagonal by 1e-4 ls + 1e-3 res), so their free term needs no d_m test.
+__device__ __forceinline__ bool stage_pair(const float4& a, const double4& cd, double ox, double oy, double oz,
+                                           float hres, float cull_r2, float4* st, bool* near) {
+    const double par0 = (ox * a.x + oy * a.y + oz * a.z) * cd.z;
+    const double sc = par0 * cd.z;
+    const double px = ox - sc * a.x, py = oy - sc * a.y, pz = oz - sc * a.z;
+    const float ux = (float)(a.x * cd.z), uy = (float)(a.y * cd.z), uz = (float)(a.z * cd.z);
+    // cull on the sub-block centroid (anchor - res/2 on each axis), in FP32
+    const float qd = -hres * (ux + uy + uz);
+    const float qpar = (float)par0 + qd;
+    const float qx = (float)px - hres - qd * ux, qy = (float)py - hres - qd * uy, qz = (float)pz - hres - qd * uz;
+    const float qal = fminf(qpar, 0.0f) + fmaxf(qpar - a.w, 0.0f);
+    const bool hit = qx * qx + qy * qy + qz * qz + qal * qal < cull_r2;
+    *near = false;
+    if (hit) {
+        const float ex = (float)(ox - a.x), ey = (float)(oy - a.y), ez = (float)(oz - a.z);
+        const float cx = ex - hres, cy = ey - hres, cz = ez - hres;
+        st[0] = make_float4((float)px, (float)py, (float)pz, (float)par0);
+        st[1] = make_float4(ux, uy, uz, (float)(par0 - cd.y));
+        st[2] = make_float4(ex, ey, ez, (float)(par0 - cd.x));
+        *near = cx * cx + cy * cy + cz * cz < cull_r2;
+    }
+    return hit;
+}
+
+// Squared distance from the cell at offset (dx, dy, dz) from the anchor to the free segment
+// [0, margin u] of a staged ray (st0, st1); *dpar = delta.u.
+__device__ __forceinline__ float free_d2(const float4& st0, const float4& st1, float dx, float dy, float dz,
+                                         float* dpar) {
+    const float dp = dx * st1.x + dy * st1.y + dz * st1.z;
+    const float qx = st0.x + dx - dp * st1.x, qy = st0.y + dy - dp * st1.y, qz = st0.z + dz - dp * st1.z;
+    const float al = fminf(st0.w + dp, 0.0f) + fmaxf(st1.w + dp, 0.0f);
+    *dpar = dp;
+    return qx * qx + qy * qy + qz * qz + al * al;
+}
+
 template <int MINB>
 __global__ void __launch_bounds__(kEvThreads, MINB) k_bgki(EvArgs A) {
     extern __shared__ __align__(32) unsigned char smem_raw[];
@@ -684,50 +727,13 @@ __global__ void __launch_bounds__(kEvThreads, MINB) k_bgki(EvArgs A) {
             for (int g0 = 0; g0 < nr; g0 += 32) {
                 const int r = g0 + lane;
                 bool hit = false, near = false;
-                if (r < nr) {
-                    const float4 a = S.a[r];
-                    const double4 cd = S.c[r];
-                    const double par0 = (ox * a.x + oy * a.y + oz * a.z) * cd.z;
-                    const double sc = par0 * cd.z;
-                    const double px = ox - sc * a.x, py = oy - sc * a.y, pz = oz - sc * a.z;
-                    const float ux = (float)(a.x * cd.z), uy = (float)(a.y * cd.z), uz = (float)(a.z * cd.z);
-                    // cull on the sub-block centroid (anchor - res/2 on each axis), in FP32
-                    const float qd = -hres * (ux + uy + uz);
-                    const float qpar = (float)par0 + qd;
-                    const float qx = (float)px - hres - qd * ux, qy = (float)py - hres - qd * uy,
-                                qz = (float)pz - hres - qd * uz;
-                    const float qal = fminf(qpar, 0.0f) + fmaxf(qpar - a.w, 0.0f);
-                    hit = qx * qx + qy * qy + qz * qz + qal * qal < cull_r2;
-                    if (hit) {
-                        const float ex = (float)(ox - a.x), ey = (float)(oy - a.y), ez = (float)(oz - a.z);
-                        // the point's sphere can reach the sub-block only if the point lies within
-                        // the cull radius of the sub-block's centroid
-                        const float cx = ex - hres, cy = ey - hres, cz = ez - hres;
-                        S.stage[wid][lane][0] = make_float4((float)par0, (float)(par0 - cd.y), (float)(par0 - cd.x), ux);
-                        S.stage[wid][lane][1] = make_float4((float)px, (float)py, (float)pz, uy);
-                        S.stage[wid][lane][2] = make_float4(ex, ey, ez, uz);
-                        near = cx * cx + cy * cy + cz * cz < cull_r2;
-                    }
-                }
+                if (r < nr) hit = stage_pair(S.a[r], S.c[r], ox, oy, oz, hres, cull_r2, S.stage[wid][lane], &near);
                 const unsigned hits = __ballot_sync(0xffffffffu, hit);
                 unsigned mnear = __ballot_sync(0xffffffffu, near);
                 unsigned mfar = hits & ~mnear;
                 __syncwarp();
-                // free evidence (:54-71) of staged ray j for this lane's cell
-                auto free_term = [&](const float4& s0, const float4& s1, float uz) {
-                    const float dpar = dx * s0.w + dy * s1.w + dz * uz;
-                    if (s0.z + dpar < 0.0f) {  // d_proj < d_m
-                        const float qx = s1.x + dx - dpar * s0.w, qy = s1.y + dy - dpar * s1.w,
-                                    qz = s1.z + dz - dpar * uz;
-                        const float al = fminf(s0.x + dpar, 0.0f) + fmaxf(s0.y + dpar, 0.0f);
-                        const float d2f = qx * qx + qy * qy + qz * qz + al * al;
-                        if (d2f < ls2c) {
-                            af += __float2ll_rn(fmaxf(kernel_tab(S.ktab, d2f * inv_ls2), 0.0f));
-                            ++nev;
-                        }
-                    }
-                };
-                // rays whose point's sphere can reach the sub-block: occupied (:48-52) and free
+                // rays whose point's sphere can reach the sub-block: occupied (mass_update.cu:48-52)
+                // and free (:54-71) evidence
                 while (mnear) {
                     const int j = __ffs(mnear) - 1;
                     mnear &= mnear - 1;
@@ -738,13 +744,23 @@ __global__ void __launch_bounds__(kEvThreads, MINB) k_bgki(EvArgs A) {
                         ao += __float2ll_rn(fmaxf(kernel_tab(S.ktab, d2o * inv_ls2), 0.0f));
                         ++nev;
                     }
-                    free_term(s0, s1, s2.w);
+                    float dpar;
+                    const float d2f = free_d2(s0, s1, dx, dy, dz, &dpar);
+                    if (s2.w + dpar < 0.0f && d2f < ls2c) {  // d_proj < d_m
+                        af += __float2ll_rn(fmaxf(kernel_tab(S.ktab, d2f * inv_ls2), 0.0f));
+                        ++nev;
+                    }
                 }
                 // the other rays: free evidence only
                 while (mfar) {
                     const int j = __ffs(mfar) - 1;
                     mfar &= mfar - 1;
-                    free_term(S.stage[wid][j][0], S.stage[wid][j][1], S.stage[wid][j][2].w);
+                    float dpar;
+                    const float d2f = free_d2(S.stage[wid][j][0], S.stage[wid][j][1], dx, dy, dz, &dpar);
+                    if (d2f < ls2c) {
+                        af += __float2ll_rn(fmaxf(kernel_tab(S.ktab, d2f * inv_ls2), 0.0f));
+                        ++nev;
+                    }
                 }
                 __syncwarp();
             }
@@ -1191,46 +1207,11 @@ __global__ void __launch_bounds__(kEvThreads, MINB) k_bgki_sums(EvArgs A, const 
             for (int g0 = 0; g0 < nr; g0 += 32) {
                 const int r = g0 + lane;
                 bool hit = false, near = false;
-                if (r < nr) {
-                    const float4 a = S.a[r];
-                    const double4 cd = S.c[r];
-                    const double par0 = (ox * a.x + oy * a.y + oz * a.z) * cd.z;
-                    const double sc = par0 * cd.z;
-                    const double px = ox - sc * a.x, py = oy - sc * a.y, pz = oz - sc * a.z;
-                    const float ux = (float)(a.x * cd.z), uy = (float)(a.y * cd.z), uz = (float)(a.z * cd.z);
-                    const float qd = -hres * (ux + uy + uz);
-                    const float qpar = (float)par0 + qd;
-                    const float qx = (float)px - hres - qd * ux, qy = (float)py - hres - qd * uy,
-                                qz = (float)pz - hres - qd * uz;
-                    const float qal = fminf(qpar, 0.0f) + fmaxf(qpar - a.w, 0.0f);
-                    hit = qx * qx + qy * qy + qz * qz + qal * qal < cull_r2;
-                    if (hit) {
-                        const float ex = (float)(ox - a.x), ey = (float)(oy - a.y), ez = (float)(oz - a.z);
-                        const float cx = ex - hres, cy = ey - hres, cz = ez - hres;
-                        S.stage[wid][lane][0] = make_float4((float)par0, (float)(par0 - cd.y), (float)(par0 - cd.x), ux);
-                        S.stage[wid][lane][1] = make_float4((float)px, (float)py, (float)pz, uy);
-                        S.stage[wid][lane][2] = make_float4(ex, ey, ez, uz);
-                        near = cx * cx + cy * cy + cz * cz < cull_r2;
-                    }
-                }
+                if (r < nr) hit = stage_pair(S.a[r], S.c[r], ox, oy, oz, hres, cull_r2, S.stage[wid][lane], &near);
                 const unsigned hits = __ballot_sync(0xffffffffu, hit);
                 unsigned mnear = __ballot_sync(0xffffffffu, near);
                 unsigned mfar = hits & ~mnear;
                 __syncwarp();
-                auto free_term = [&](const float4& s0, const float4& s1, float uz) {
-                    const float dpar = dx * s0.w + dy * s1.w + dz * uz;
-                    if (s0.z + dpar < 0.0f) {
-                        const float qx = s1.x + dx - dpar * s0.w, qy = s1.y + dy - dpar * s1.w,
-                                    qz = s1.z + dz - dpar * uz;
-                        const float al = fminf(s0.x + dpar, 0.0f) + fmaxf(s0.y + dpar, 0.0f);
-                        const float d2f = qx * qx + qy * qy + qz * qz + al * al;
-                        if (d2f < ls2c) {
-                            const float u = d2f * inv_ls2;
-                            ff += __float2ll_rn(fmaxf(kernel_tab(S.ftab, u), 0.0f));
-                            hf += __float2ll_rn(kernel_tab(S.htab, u));
-                        }
-                    }
-                };
                 while (mnear) {
                     const int j = __ffs(mnear) - 1;
                     mnear &= mnear - 1;
@@ -1242,12 +1223,24 @@ __global__ void __launch_bounds__(kEvThreads, MINB) k_bgki_sums(EvArgs A, const 
                         fo += __float2ll_rn(fmaxf(kernel_tab(S.ftab, u), 0.0f));
                         ho += __float2ll_rn(kernel_tab(S.htab, u));
                     }
-                    free_term(s0, s1, s2.w);
+                    float dpar;
+                    const float d2f = free_d2(s0, s1, dx, dy, dz, &dpar);
+                    if (s2.w + dpar < 0.0f && d2f < ls2c) {
+                        const float u = d2f * inv_ls2;
+                        ff += __float2ll_rn(fmaxf(kernel_tab(S.ftab, u), 0.0f));
+                        hf += __float2ll_rn(kernel_tab(S.htab, u));
+                    }
                 }
                 while (mfar) {
                     const int j = __ffs(mfar) - 1;
                     mfar &= mfar - 1;
-                    free_term(S.stage[wid][j][0], S.stage[wid][j][1], S.stage[wid][j][2].w);
+                    float dpar;
+                    const float d2f = free_d2(S.stage[wid][j][0], S.stage[wid][j][1], dx, dy, dz, &dpar);
+                    if (d2f < ls2c) {
+                        const float u = d2f * inv_ls2;
+                        ff += __float2ll_rn(fmaxf(kernel_tab(S.ftab, u), 0.0f));
+                        hf += __float2ll_rn(kernel_tab(S.htab, u));
+                    }
                 }
                 __syncwarp();
             }
