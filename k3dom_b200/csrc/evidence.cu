@@ -497,12 +497,27 @@ void build_kernel_table(float sigma, double scale, float4* out) {
     }
 }
 
+// Table position of u = d^2 / ls^2: interval i = floor(t) and offset f = t - i, t = u * kKernelTab
+// clamped below kKernelTab. The floor is taken without conversion instructions: t + 2^23 rounded
+// down is 2^23 + floor(t) exactly for 0 <= t < 2^23, whose low mantissa bits are floor(t).
+struct TabPos {
+    int i;
+    float f;
+};
+__device__ __forceinline__ TabPos tab_pos(float u) {
+    const float t = fminf(u * (float)kKernelTab, (float)kKernelTab - 3.0517578e-05f);
+    const float tr = __fadd_rd(t, 8388608.0f);
+    TabPos q;
+    q.i = __float_as_int(tr) - 0x4B000000;
+    q.f = t - (tr - 8388608.0f);
+    return q;
+}
+__device__ __forceinline__ float tab_eval(const float4* __restrict__ tab, TabPos q) {
+    const float4 c = tab[q.i];
+    return fmaf(q.f, fmaf(q.f, fmaf(q.f, c.w, c.z), c.y), c.x);
+}
 __device__ __forceinline__ float kernel_tab(const float4* __restrict__ tab, float u) {
-    const float t = u * (float)kKernelTab;
-    const int i = min((int)t, kKernelTab - 1);
-    const float f = t - (float)i;
-    const float4 c = tab[i];
-    return fmaf(f, fmaf(f, fmaf(f, c.w, c.z), c.y), c.x);
+    return tab_eval(tab, tab_pos(u));
 }
 
 // mass_update.cu:12-14, 1 - 2 / (1 + exp(2 mass / mass_scale)), with k2 = 2 / mass_scale
@@ -629,7 +644,7 @@ __device__ __forceinline__ BgkiSmem bgki_smem(unsigned char* base, int chunk) {
 // Every FP32 quantity is O(ls), so the FP32 evaluation keeps ~1e-7 relative accuracy at any
 // distance from the sensor (the direct |c|^2 - d_proj^2 form of :60 loses ~1e-5 at 20 m).
 //
-// stage_pair culls the pair on the sub-block centroid and, for a pair that passes, stages three
+// stage_pair culls the pair on the sub-block centroid and, for a pair that passes, forms three
 // float4: st[0] = (perp0, par0), st[1] = (u, par0 - margin), st[2] = (occ0, par0 - d_m).
 // *near: the point lies within the cull radius of the centroid, i.e. its sphere of radius ls can
 // reach a cell of the sub-block. For the other rays no cell of the sub-block with d_proj >= d_m
@@ -637,7 +652,7 @@ __device__ __forceinline__ BgkiSmem bgki_smem(unsigned char* base, int chunk) {
 // the segment's end as from the point, and the cull radius exceeds ls + half the sub-block
 // diagonal by 1e-4 ls + 1e-3 res), so their free term needs no d_m test.
 __device__ __forceinline__ bool stage_pair(const float4& a, const double4& cd, double ox, double oy, double oz,
-                                           float hres, float cull_r2, float4* st, bool* near) {
+                                           float hres, float cull_r2, float4 st[3], bool* near) {
     const double par0 = (ox * a.x + oy * a.y + oz * a.z) * cd.z;
     const double sc = par0 * cd.z;
     const double px = ox - sc * a.x, py = oy - sc * a.y, pz = oz - sc * a.z;
@@ -678,6 +693,7 @@ __global__ void __launch_bounds__(kEvThreads, MINB) k_bgki(EvArgs A) {
     __shared__ uint32_t s_item;
     __shared__ int s_next_sb, s_last;
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    const unsigned lanes_below = (1u << lane) - 1u;
     const Batch& bt = A.bt;
     const uint32_t total_items = A.item_off[bt.T];
     int table_scene = -1;  // scene whose kernel table is in shared memory
@@ -727,16 +743,22 @@ __global__ void __launch_bounds__(kEvThreads, MINB) k_bgki(EvArgs A) {
             for (int g0 = 0; g0 < nr; g0 += 32) {
                 const int r = g0 + lane;
                 bool hit = false, near = false;
-                if (r < nr) hit = stage_pair(S.a[r], S.c[r], ox, oy, oz, hres, cull_r2, S.stage[wid][lane], &near);
-                const unsigned hits = __ballot_sync(0xffffffffu, hit);
-                unsigned mnear = __ballot_sync(0xffffffffu, near);
-                unsigned mfar = hits & ~mnear;
+                float4 st[3];
+                if (r < nr) hit = stage_pair(S.a[r], S.c[r], ox, oy, oz, hres, cull_r2, st, &near);
+                // compact the passing rays into the warp's staging list: near rays first
+                const unsigned mnear = __ballot_sync(0xffffffffu, near);
+                const unsigned mfar = __ballot_sync(0xffffffffu, hit && !near);
+                const int nn = __popc(mnear), nh = nn + __popc(mfar);
+                if (hit) {
+                    float4* dst = S.stage[wid][near ? __popc(mnear & lanes_below) : nn + __popc(mfar & lanes_below)];
+                    dst[0] = st[0];
+                    dst[1] = st[1];
+                    if (near) dst[2] = st[2];
+                }
                 __syncwarp();
                 // rays whose point's sphere can reach the sub-block: occupied (mass_update.cu:48-52)
                 // and free (:54-71) evidence
-                while (mnear) {
-                    const int j = __ffs(mnear) - 1;
-                    mnear &= mnear - 1;
+                for (int j = 0; j < nn; ++j) {
                     const float4 s0 = S.stage[wid][j][0], s1 = S.stage[wid][j][1], s2 = S.stage[wid][j][2];
                     const float vx = s2.x + dx, vy = s2.y + dy, vz = s2.z + dz;
                     const float d2o = vx * vx + vy * vy + vz * vz;
@@ -752,9 +774,7 @@ __global__ void __launch_bounds__(kEvThreads, MINB) k_bgki(EvArgs A) {
                     }
                 }
                 // the other rays: free evidence only
-                while (mfar) {
-                    const int j = __ffs(mfar) - 1;
-                    mfar &= mfar - 1;
+                for (int j = nn; j < nh; ++j) {
                     float dpar;
                     const float d2f = free_d2(S.stage[wid][j][0], S.stage[wid][j][1], dx, dy, dz, &dpar);
                     if (d2f < ls2c) {
@@ -1161,6 +1181,7 @@ __global__ void __launch_bounds__(kEvThreads, MINB) k_bgki_sums(EvArgs A, const 
     __shared__ uint32_t s_item;
     __shared__ int s_next_sb;
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    const unsigned lanes_below = (1u << lane) - 1u;
     const Batch& bt = A.bt;
     const uint32_t total_items = A.item_off[bt.T];
     for (int i = threadIdx.x; i < kKernelTab; i += kEvThreads) {
@@ -1207,39 +1228,42 @@ __global__ void __launch_bounds__(kEvThreads, MINB) k_bgki_sums(EvArgs A, const 
             for (int g0 = 0; g0 < nr; g0 += 32) {
                 const int r = g0 + lane;
                 bool hit = false, near = false;
-                if (r < nr) hit = stage_pair(S.a[r], S.c[r], ox, oy, oz, hres, cull_r2, S.stage[wid][lane], &near);
-                const unsigned hits = __ballot_sync(0xffffffffu, hit);
-                unsigned mnear = __ballot_sync(0xffffffffu, near);
-                unsigned mfar = hits & ~mnear;
+                float4 st[3];
+                if (r < nr) hit = stage_pair(S.a[r], S.c[r], ox, oy, oz, hres, cull_r2, st, &near);
+                const unsigned mnear = __ballot_sync(0xffffffffu, near);
+                const unsigned mfar = __ballot_sync(0xffffffffu, hit && !near);
+                const int nn = __popc(mnear), nh = nn + __popc(mfar);
+                if (hit) {
+                    float4* dst = S.stage[wid][near ? __popc(mnear & lanes_below) : nn + __popc(mfar & lanes_below)];
+                    dst[0] = st[0];
+                    dst[1] = st[1];
+                    if (near) dst[2] = st[2];
+                }
                 __syncwarp();
-                while (mnear) {
-                    const int j = __ffs(mnear) - 1;
-                    mnear &= mnear - 1;
+                for (int j = 0; j < nn; ++j) {
                     const float4 s0 = S.stage[wid][j][0], s1 = S.stage[wid][j][1], s2 = S.stage[wid][j][2];
                     const float vx = s2.x + dx, vy = s2.y + dy, vz = s2.z + dz;
                     const float d2o = vx * vx + vy * vy + vz * vz;
                     if (d2o < ls2c) {
-                        const float u = d2o * inv_ls2;
-                        fo += __float2ll_rn(fmaxf(kernel_tab(S.ftab, u), 0.0f));
-                        ho += __float2ll_rn(kernel_tab(S.htab, u));
+                        const TabPos q = tab_pos(d2o * inv_ls2);
+                        fo += __float2ll_rn(fmaxf(tab_eval(S.ftab, q), 0.0f));
+                        ho += __float2ll_rn(tab_eval(S.htab, q));
                     }
                     float dpar;
                     const float d2f = free_d2(s0, s1, dx, dy, dz, &dpar);
                     if (s2.w + dpar < 0.0f && d2f < ls2c) {
-                        const float u = d2f * inv_ls2;
-                        ff += __float2ll_rn(fmaxf(kernel_tab(S.ftab, u), 0.0f));
-                        hf += __float2ll_rn(kernel_tab(S.htab, u));
+                        const TabPos q = tab_pos(d2f * inv_ls2);
+                        ff += __float2ll_rn(fmaxf(tab_eval(S.ftab, q), 0.0f));
+                        hf += __float2ll_rn(tab_eval(S.htab, q));
                     }
                 }
-                while (mfar) {
-                    const int j = __ffs(mfar) - 1;
-                    mfar &= mfar - 1;
+                for (int j = nn; j < nh; ++j) {
                     float dpar;
                     const float d2f = free_d2(S.stage[wid][j][0], S.stage[wid][j][1], dx, dy, dz, &dpar);
                     if (d2f < ls2c) {
-                        const float u = d2f * inv_ls2;
-                        ff += __float2ll_rn(fmaxf(kernel_tab(S.ftab, u), 0.0f));
-                        hf += __float2ll_rn(kernel_tab(S.htab, u));
+                        const TabPos q = tab_pos(d2f * inv_ls2);
+                        ff += __float2ll_rn(fmaxf(tab_eval(S.ftab, q), 0.0f));
+                        hf += __float2ll_rn(tab_eval(S.htab, q));
                     }
                 }
                 __syncwarp();
