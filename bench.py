@@ -655,7 +655,7 @@ def run_profile_case(args):
     p = K.make_params(args.variant, **cfg.params)
     dom = K.DOM(p, args.variant)
     if args.profile_tile_rule is not None:
-        dom.set_tuning(args.profile_tile_rule, 1024)
+        dom.set_tuning(args.profile_tile_rule, args.chunk)
     for f in range(1 + args.steps):
         t = 0.1 + f * cfg.dt
         s, pts = cfg.scene.scan(f, t, cfg.n_points)
@@ -681,7 +681,8 @@ def main(argv=None):
     ap.add_argument("--no-grad", action="store_true", help="skip the gradient-step measurement")
     ap.add_argument("--tile-rule", type=int, default=None,
                     help="fixed evidence tile rule instead of autotuning (0 by size, 1 8x8x4, 2 16x16x4, 3 16x16x8)")
-    ap.add_argument("--chunk", type=int, default=1024, help="rays per evidence work item with --tile-rule")
+    ap.add_argument("--chunk", type=int, default=1024,
+                    help="rays per evidence work item with --tile-rule or --profile-tile-rule")
     ap.add_argument("--profile-tile-rule", type=int, default=None,
                     help="profile case: evidence tile rule (0 by size, 1 8x8x4, 2 16x16x4, 3 16x16x8)")
     ap.add_argument("--scenes", type=int, default=16)

@@ -40,10 +40,10 @@ struct SceneDev {
     int cell_off, part_off, birth_off, joint_off, point_off, tile_off;
     int n_tiles, max_points;
     float bin_R;    // ray-binning support radius [cells]
-    float cull_r2;  // squared cull radius around a sub-block centroid [m^2]
-    float wr2;      // DS window radius squared [m^2]
-    float pad;
-    double fx_inv;  // K3DOM evidence: value = fixed-point integer * fx_inv
+    float cull_r2;   // DS: squared cull radius around a sub-block centroid [m^2]
+    float wr2;       // DS window radius squared [m^2]
+    float cull_ls2;  // K3DOM: squared support radius of the sub-block cull, ls plus slack [m^2]
+    double fx_inv;   // K3DOM evidence: value = fixed-point integer * fx_inv
 };
 
 // Range starts of every scene, entry S = the total (device memory).

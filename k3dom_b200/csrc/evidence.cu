@@ -328,6 +328,9 @@ void fill_scene_evidence(SceneDev& sd, bool ds, float4* ktab) {
         rsup = sqrtf(p.window_radius * p.window_radius + slack) + rsb + 1e-3f * p.res;
     }
     sd.cull_r2 = rsup * rsup;
+    // K3DOM box cull (stage_pair): the support radius with the same slack as rsup
+    const float rls = p.ls * (1.0f + 1e-4f) + 1e-3f * p.res;
+    sd.cull_ls2 = rls * rls;
     // fixed point: one kernel value is at most sigma -> at most 2^40 units, leaving 2^23 terms
     // of headroom in a signed 64-bit sum
     const double sig = std::max((double)p.sigma, 1e-30);
@@ -644,25 +647,41 @@ __device__ __forceinline__ BgkiSmem bgki_smem(unsigned char* base, int chunk) {
 // Every FP32 quantity is O(ls), so the FP32 evaluation keeps ~1e-7 relative accuracy at any
 // distance from the sensor (the direct |c|^2 - d_proj^2 form of :60 loses ~1e-5 at 20 m).
 //
-// stage_pair culls the pair on the sub-block centroid and, for a pair that passes, forms three
-// float4: st[0] = (perp0, par0), st[1] = (u, par0 - margin), st[2] = (occ0, par0 - d_m).
-// *near: the point lies within the cull radius of the centroid, i.e. its sphere of radius ls can
-// reach a cell of the sub-block. For the other rays no cell of the sub-block with d_proj >= d_m
-// is within ls of the free segment either (margin <= d_m, so such a cell is at least as far from
-// the segment's end as from the point, and the cull radius exceeds ls + half the sub-block
-// diagonal by 1e-4 ls + 1e-3 res), so their free term needs no d_m test.
+// stage_pair culls the pair on the sub-block and, for a pair that passes, forms three float4:
+// st[0] = (perp0, par0), st[1] = (u, par0 - margin), st[2] = (occ0, par0 - d_m).
+//
+// The cull bounds the distance from a convex set K (the segment [0, d_m u], or the point) to the
+// sub-block's cell centres x = c + h, |h_i| <= e_i, e = (1.5, 1.5, 0.5) res around the centroid c.
+// dist(K, .) is convex with gradient D / |D| at c (D = c minus the closest point of K), so
+// dist(K, x) >= |D| - (e . |D|) / |D| for every cell centre, where |D| is taken componentwise in
+// e . |D|. No cell is within rls = ls (1 + 1e-4) + 1e-3 res of K unless |D|^2 - e . |D| < rls |D|
+// (box_reaches). This is tighter than a sphere around c for the flat 4x4x2 sub-block, above all
+// for the near-horizontal rays of a LiDAR scan.
+//
+// *near: the point's sphere of radius ls can reach a cell of the sub-block. For the other rays no
+// cell of the sub-block with d_proj >= d_m is within ls of the free segment either (margin <= d_m,
+// so such a cell is at least as far from the segment's end as from the point, and the bound above
+// keeps 1e-4 ls + 1e-3 res of slack), so their free term needs no d_m test.
+__device__ __forceinline__ bool box_reaches(float Dx, float Dy, float Dz, float D2, float hres, float rls2) {
+    const float s = fmaf(3.0f * hres, fabsf(Dx) + fabsf(Dy), hres * fabsf(Dz));
+    const float t = D2 - s;
+    return t < 0.0f || t * t < rls2 * D2;
+}
+
 __device__ __forceinline__ bool stage_pair(const float4& a, const double4& cd, double ox, double oy, double oz,
-                                           float hres, float cull_r2, float4 st[3], bool* near) {
+                                           float hres, float rls2, float4 st[3], bool* near) {
     const double par0 = (ox * a.x + oy * a.y + oz * a.z) * cd.z;
     const double sc = par0 * cd.z;
     const double px = ox - sc * a.x, py = oy - sc * a.y, pz = oz - sc * a.z;
     const float ux = (float)(a.x * cd.z), uy = (float)(a.y * cd.z), uz = (float)(a.z * cd.z);
-    // cull on the sub-block centroid (anchor - res/2 on each axis), in FP32
+    // centroid = anchor - res/2 on each axis; its perpendicular offset q and its distance qal
+    // along the ray beyond [0, d_m], in FP32
     const float qd = -hres * (ux + uy + uz);
     const float qpar = (float)par0 + qd;
     const float qx = (float)px - hres - qd * ux, qy = (float)py - hres - qd * uy, qz = (float)pz - hres - qd * uz;
     const float qal = fminf(qpar, 0.0f) + fmaxf(qpar - a.w, 0.0f);
-    const bool hit = qx * qx + qy * qy + qz * qz + qal * qal < cull_r2;
+    const bool hit = box_reaches(fmaf(qal, ux, qx), fmaf(qal, uy, qy), fmaf(qal, uz, qz),
+                                 qx * qx + qy * qy + qz * qz + qal * qal, hres, rls2);
     *near = false;
     if (hit) {
         const float ex = (float)(ox - a.x), ey = (float)(oy - a.y), ez = (float)(oz - a.z);
@@ -670,7 +689,7 @@ __device__ __forceinline__ bool stage_pair(const float4& a, const double4& cd, d
         st[0] = make_float4((float)px, (float)py, (float)pz, (float)par0);
         st[1] = make_float4(ux, uy, uz, (float)(par0 - cd.y));
         st[2] = make_float4(ex, ey, ez, (float)(par0 - cd.x));
-        *near = cx * cx + cy * cy + cz * cz < cull_r2;
+        *near = box_reaches(cx, cy, cz, cx * cx + cy * cy + cz * cz, hres, rls2);
     }
     return hit;
 }
@@ -716,7 +735,7 @@ __global__ void __launch_bounds__(kEvThreads, MINB) k_bgki(EvArgs A) {
         const float ls2 = p.ls * p.ls;
         const float inv_ls2 = 1.0f / ls2;
         const float hres = 0.5f * p.res;
-        const float cull_r2 = sd.cull_r2;
+        const float cull_ls2 = sd.cull_ls2;
         const int nsb = ts.nsbx * ts.nsby * (ts.tz / 2);
         if (it.sc != table_scene) {
             for (int i = threadIdx.x; i < kKernelTab; i += kEvThreads) S.ktab[i] = A.ktab[it.sc * kKernelTab + i];
@@ -744,7 +763,7 @@ __global__ void __launch_bounds__(kEvThreads, MINB) k_bgki(EvArgs A) {
                 const int r = g0 + lane;
                 bool hit = false, near = false;
                 float4 st[3];
-                if (r < nr) hit = stage_pair(S.a[r], S.c[r], ox, oy, oz, hres, cull_r2, st, &near);
+                if (r < nr) hit = stage_pair(S.a[r], S.c[r], ox, oy, oz, hres, cull_ls2, st, &near);
                 // compact the passing rays into the warp's staging list: near rays first
                 const unsigned mnear = __ballot_sync(0xffffffffu, near);
                 const unsigned mfar = __ballot_sync(0xffffffffu, hit && !near);
@@ -1205,7 +1224,7 @@ __global__ void __launch_bounds__(kEvThreads, MINB) k_bgki_sums(EvArgs A, const 
         const float ls2 = p.ls * p.ls;
         const float inv_ls2 = 1.0f / ls2;
         const float hres = 0.5f * p.res;
-        const float cull_r2 = sd.cull_r2;
+        const float cull_ls2 = sd.cull_ls2;
         const int nsb = ts.nsbx * ts.nsby * (ts.tz / 2);
         for (int r = threadIdx.x; r < it.nr; r += kEvThreads) {
             uint32_t rid = A.evals[it.e0 + r];
@@ -1229,7 +1248,7 @@ __global__ void __launch_bounds__(kEvThreads, MINB) k_bgki_sums(EvArgs A, const 
                 const int r = g0 + lane;
                 bool hit = false, near = false;
                 float4 st[3];
-                if (r < nr) hit = stage_pair(S.a[r], S.c[r], ox, oy, oz, hres, cull_r2, st, &near);
+                if (r < nr) hit = stage_pair(S.a[r], S.c[r], ox, oy, oz, hres, cull_ls2, st, &near);
                 const unsigned mnear = __ballot_sync(0xffffffffu, near);
                 const unsigned mfar = __ballot_sync(0xffffffffu, hit && !near);
                 const int nn = __popc(mnear), nh = nn + __popc(mfar);
