@@ -113,6 +113,7 @@ struct k3dom_handle {
 
     Particles A{}, Ss{}, Bp{};
     uint32_t *sorted_keys = nullptr, *perm = nullptr, *alt_k = nullptr, *alt_v = nullptr;
+    SegRec* seg_rec = nullptr;  // piece sums of the segmented per-cell sums, one per 256 sorted slots
     uint32_t *hist = nullptr, *scan_tmp = nullptr;
     long hist_words = 0, scan_tmp_words = 0;
     CellState cs[2]{};  // cs[0] live, cs[1] spare for the map shift
@@ -544,7 +545,7 @@ cudaError_t enq_assign(k3dom_handle* h) {
     if (e != cudaSuccess) return e;
     if ((e = cudaMemsetAsync(h->cw.start, 0xFF, sizeof(int) * (size_t)h->C, h->st))) return e;
     if ((e = cudaMemsetAsync(h->cw.end, 0xFF, sizeof(int) * (size_t)h->C, h->st))) return e;
-    launch_gather_segsum(h->batch(), h->A, h->Ss, h->sorted_keys, h->perm, h->cw, h->st);
+    launch_gather_segsum(h->batch(), h->A, h->Ss, h->sorted_keys, h->perm, h->cw, h->seg_rec, h->st);
     return cudaGetLastError();
 }
 
@@ -796,7 +797,7 @@ k3dom_status k3dom_batch_create(const k3dom_params* params, int32_t n_scenes, k3
         (e = h->alloc_particles(&h->Bp, B)))
         return bail(e);
     if ((e = h->alloc(&h->sorted_keys, P)) || (e = h->alloc(&h->perm, P)) || (e = h->alloc(&h->alt_k, P)) ||
-        (e = h->alloc(&h->alt_v, P)))
+        (e = h->alloc(&h->alt_v, P)) || (e = h->alloc(&h->seg_rec, seg_rec_count(P))))
         return bail(e);
     if ((e = h->alloc_cells(&h->cs[0], C)) || (e = h->alloc_cells(&h->cs[1], C))) return bail(e);
     CellWork& cw = h->cw;
@@ -1547,7 +1548,7 @@ k3dom_status k3dom_set_particles(k3dom_handle* h, k3dom_particle_set set, const 
         k_iota<<<div_up(n, 256), 256, 0, h->st>>>(h->perm, n);
         if ((e = cudaMemsetAsync(h->cw.start, 0xFF, sizeof(int) * (size_t)h->C, h->st))) return h->fail(e);
         if ((e = cudaMemsetAsync(h->cw.end, 0xFF, sizeof(int) * (size_t)h->C, h->st))) return h->fail(e);
-        launch_gather_segsum(h->batch(), h->Ss, h->Ss, h->sorted_keys, h->perm, h->cw, h->st);
+        launch_gather_segsum(h->batch(), h->Ss, h->Ss, h->sorted_keys, h->perm, h->cw, h->seg_rec, h->st);
     }
     e = cudaStreamSynchronize(h->st);
     return e == cudaSuccess ? K3DOM_OK : h->fail(e);

@@ -61,8 +61,18 @@ cudaError_t exact_scan_plan(const ExactTile* tiles, int nt, void* scratch, cudaS
 // particles.cu
 void launch_predict(const Batch& bt, Particles a, cudaStream_t st);
 void launch_shift_particles(int n, Particles a, int mx, int my, int mz, cudaStream_t st);
+// Piece sums of one 256-slot range of the sorted particles (gather + segmented sums): the
+// range's first piece when its cell began in an earlier range, and its last piece when its cell
+// continues into the next range.
+struct SegRec {
+    double lead[4];   // sum w, w vx, w vy, w vz of the first piece
+    double trail[4];  // the same of the last piece
+    int lead_end;     // position of the first piece's last particle; -1: it reaches the range's end
+    int trail_head;   // position of the last piece's cell head; -1: no such piece
+};
+long seg_rec_count(long P);
 void launch_gather_segsum(const Batch& bt, Particles a, Particles s, const uint32_t* sorted_keys,
-                          const uint32_t* perm, CellWork cw, cudaStream_t st);
+                          const uint32_t* perm, CellWork cw, SegRec* rec, cudaStream_t st);
 void launch_reweight(const Batch& bt, Particles s, const uint32_t* sorted_keys, CellWork cw, cudaStream_t st);
 void launch_births(const Batch& bt, const float* born, const float* born_cum, Particles b, cudaStream_t st);
 void launch_init_particles(const Batch& bt, const float* born_cum, Particles a, cudaStream_t st);

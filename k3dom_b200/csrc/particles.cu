@@ -92,17 +92,25 @@ void launch_shift_particles(int n, Particles a, int mx, int my, int mz, cudaStre
 
 // ---------------------------------------------------------------- gather + segmented sums
 // After the sort: sorted slot i takes particle perm[i] (the payload permutation of
-// thrust::sort_by_key, src/common/dom.cu:175-183). In the same pass each warp forms the
-// per-cell sums over its sorted range -- the serial weight loop of
-// gridCellPredictionUpdateKernel (src/k3dom/kernel/mass_update.cu:168-174) and the
-// w*v sums behind statisticalMomentsKernel1/2 (statistical_moments.cu:22-63) -- and the
-// start/end ranges of particleToGridKernel (particle_to_grid.cu:23-39). A cell's sum is
-// formed by exactly one warp (the one holding its first particle) in a fixed order, so it
-// is deterministic. The penalty of penalizeStaticParticlesKernel (resampling.cu:13-36) is
-// recorded as the sign bit of the sorted weight and applied at resampling.
+// thrust::sort_by_key, src/common/dom.cu:175-183). In the same pass the per-cell sums over the
+// sorted ranges are formed -- the serial weight loop of gridCellPredictionUpdateKernel
+// (src/k3dom/kernel/mass_update.cu:168-174) and the w*v sums behind statisticalMomentsKernel1/2
+// (statistical_moments.cu:22-63) -- and the start/end ranges of particleToGridKernel
+// (particle_to_grid.cu:23-39). The penalty of penalizeStaticParticlesKernel
+// (resampling.cu:13-36) is recorded as the sign bit of the sorted weight and applied at
+// resampling.
+//
+// Two levels. Each warp takes 256 sorted slots and finishes every cell whose particles lie in
+// its range (FP64 segmented scan over 32-slot chunks). For a cell that crosses range boundaries
+// it records the piece sums: the range's first piece (SegRec.lead) and its last piece
+// (SegRec.trail). k_seg_fixup then adds, for each cell whose head lies in a range, that range's
+// trail and the lead pieces of the following ranges up to the cell's end. Every sum is formed in
+// a fixed order, so it is deterministic, and no warp walks a long cell alone.
 constexpr int kSegItems = 8;                       // 32-wide chunks per warp range
 constexpr int kSegRange = 32 * kSegItems;          // 256 sorted particles per warp
 constexpr int kSegWarps = kBlock / 32;
+
+long seg_rec_count(long P) { return P > 0 ? div_up(P, (long)kSegRange) : 1; }
 
 struct SegVal {
     double w, x, y, z;
@@ -117,9 +125,19 @@ __device__ __forceinline__ SegVal shfl_up_seg(const SegVal& v, int d) {
     return o;
 }
 
+__device__ __forceinline__ void put_sums(CellWork cw, uint32_t key, double w, double x, double y, double z, int start,
+                                         int end) {
+    cw.sum_w[key] = (float)w;
+    cw.sum_wvx[key] = (float)x;
+    cw.sum_wvy[key] = (float)y;
+    cw.sum_wvz[key] = (float)z;
+    cw.start[key] = start;
+    cw.end[key] = end;
+}
+
 __global__ void __launch_bounds__(kBlock)
 k_gather_segsum(Batch bt, Particles a, Particles s, const uint32_t* __restrict__ keys,
-                const uint32_t* __restrict__ perm, CellWork cw) {
+                const uint32_t* __restrict__ perm, CellWork cw, SegRec* __restrict__ rec) {
     const int lane = threadIdx.x & 31;
     const long warp_global = (long)blockIdx.x * kSegWarps + (threadIdx.x >> 5);
     const long r0 = warp_global * kSegRange;
@@ -127,19 +145,22 @@ k_gather_segsum(Batch bt, Particles a, Particles s, const uint32_t* __restrict__
     if (r0 >= P) return;
     const long r1 = min(r0 + (long)kSegRange, P);
 
-    // carried state of the open segment (ends of the previous chunk)
+    // carried state of the open segment (ends of the previous chunk); head -1: the segment
+    // began before this range
     SegVal carry = {0.0, 0.0, 0.0, 0.0};
-    long carry_head = -1;  // head position of the open segment if this warp owns it
+    long carry_head = -1;
     uint32_t prev_key = (r0 > 0) ? keys[r0 - 1] : 0xFFFFFFFFu;
-    bool done = false;
-
-    for (long c0 = r0; !done; c0 += 32) {
-        const bool in_range_chunk = c0 < r1;
+    bool lead_open = true;  // the range's first piece has not ended yet
+    if (lane == 0) {
+        rec[warp_global].lead_end = -1;
+        rec[warp_global].trail_head = -1;
+    }
+    __syncwarp();
+    for (long c0 = r0; c0 < r1; c0 += 32) {
         const long pos = c0 + lane;
-        const bool valid = pos < P;
-        const bool mine = pos < r1;  // this warp writes the sorted slot
-        uint32_t key = valid ? keys[pos] : 0xFFFFFFFEu;
-        uint32_t next_key = (pos + 1 < P) ? keys[pos + 1] : 0xFFFFFFFDu;
+        const bool valid = pos < r1;
+        const uint32_t key = valid ? keys[pos] : 0xFFFFFFFEu;
+        const uint32_t next_key = (pos + 1 < P) ? keys[pos + 1] : 0xFFFFFFFDu;
         uint32_t kprev = __shfl_up_sync(0xffffffffu, key, 1);
         if (lane == 0) kprev = prev_key;
         prev_key = __shfl_sync(0xffffffffu, key, 31);
@@ -151,22 +172,19 @@ k_gather_segsum(Batch bt, Particles a, Particles s, const uint32_t* __restrict__
             const uint32_t src = perm[pos];
             const float vx = a.vx[src], vy = a.vy[src], vz = a.vz[src];
             const float w = a.w[src];
-            if (mine) {
-                // sorted slots of a scene lie in its particle range (cells are scene-major)
-                const float mv = bt.sc[scene_of(bt.off->part, bt.S, (int)pos)].p.min_vel;
-                const float sp = __fadd_rn(__fadd_rn(__fmul_rn(vx, vx), __fmul_rn(vy, vy)),
-                                           __fmul_rn(vz, vz));
-                const bool slow = sp < __fmul_rn(mv, mv);
-                s.px[pos] = a.px[src];
-                s.py[pos] = a.py[src];
-                s.pz[pos] = a.pz[src];
-                s.vx[pos] = vx;
-                s.vy[pos] = vy;
-                s.vz[pos] = vz;
-                s.w[pos] = slow ? -w : w;  // sign bit = penalised at resampling
-                s.assoc[pos] = a.assoc[src];
-                s.cell[pos] = (int)key;
-            }
+            // sorted slots of a scene lie in its particle range (cells are scene-major)
+            const float mv = bt.sc[scene_of(bt.off->part, bt.S, (int)pos)].p.min_vel;
+            const float sp = __fadd_rn(__fadd_rn(__fmul_rn(vx, vx), __fmul_rn(vy, vy)), __fmul_rn(vz, vz));
+            const bool slow = sp < __fmul_rn(mv, mv);
+            s.px[pos] = a.px[src];
+            s.py[pos] = a.py[src];
+            s.pz[pos] = a.pz[src];
+            s.vx[pos] = vx;
+            s.vy[pos] = vy;
+            s.vz[pos] = vz;
+            s.w[pos] = slow ? -w : w;  // sign bit = penalised at resampling
+            s.assoc[pos] = a.assoc[src];
+            s.cell[pos] = (int)key;
             v.w = (double)w;
             v.x = (double)__fmul_rn(w, vx);
             v.y = (double)__fmul_rn(w, vy);
@@ -190,37 +208,68 @@ k_gather_segsum(Batch bt, Particles a, Particles s, const uint32_t* __restrict__
             v.w += carry.w; v.x += carry.x; v.y += carry.y; v.z += carry.z;
             hpos = carry_head;
         }
-        // a segment is owned by the warp whose range holds its head
-        const bool owned = hpos >= r0 && hpos < r1;
-        if (tail && owned) {
-            cw.sum_w[key] = (float)v.w;
-            cw.sum_wvx[key] = (float)v.x;
-            cw.sum_wvy[key] = (float)v.y;
-            cw.sum_wvz[key] = (float)v.z;
-            cw.start[key] = (int)hpos;
-            cw.end[key] = (int)pos;
+        if (tail) {
+            if (hpos >= 0) {
+                put_sums(cw, key, v.w, v.x, v.y, v.z, (int)hpos, (int)pos);
+            } else {
+                // end of the range's first piece, whose cell began in an earlier range
+                SegRec& r = rec[warp_global];
+                r.lead[0] = v.w; r.lead[1] = v.x; r.lead[2] = v.y; r.lead[3] = v.z;
+                r.lead_end = (int)pos;
+            }
         }
-        carry.w = __shfl_sync(0xffffffffu, v.w, 31);
-        carry.x = __shfl_sync(0xffffffffu, v.x, 31);
-        carry.y = __shfl_sync(0xffffffffu, v.y, 31);
-        carry.z = __shfl_sync(0xffffffffu, v.z, 31);
-        carry_head = __shfl_sync(0xffffffffu, hpos, 31);
-        const bool last_tail = __shfl_sync(0xffffffffu, tail, 31);
-        const bool any_valid_after = (c0 + 32) < P;
-        if (!in_range_chunk || (c0 + 32 >= r1)) {
-            // past (or at the end of) the range: continue only for an owned open segment
-            const bool open_owned = !last_tail && carry_head >= r0 && carry_head < r1;
-            done = !open_owned || !any_valid_after;
+        const int last = (int)min(31L, r1 - 1 - c0);  // last valid lane of the chunk
+        carry.w = __shfl_sync(0xffffffffu, v.w, last);
+        carry.x = __shfl_sync(0xffffffffu, v.x, last);
+        carry.y = __shfl_sync(0xffffffffu, v.y, last);
+        carry.z = __shfl_sync(0xffffffffu, v.z, last);
+        carry_head = __shfl_sync(0xffffffffu, hpos, last);
+        const bool last_tail = __shfl_sync(0xffffffffu, tail, last);
+        if (__any_sync(0xffffffffu, tail && hpos < 0)) lead_open = false;
+        if (c0 + 32 >= r1 && !last_tail && lane == last) {
+            // the range's last piece continues into the next range
+            SegRec& r = rec[warp_global];
+            if (carry_head >= 0) {
+                r.trail[0] = v.w; r.trail[1] = v.x; r.trail[2] = v.y; r.trail[3] = v.z;
+                r.trail_head = (int)carry_head;
+            } else if (lead_open) {
+                // the whole range lies inside one cell that began earlier: all of it is lead
+                r.lead[0] = v.w; r.lead[1] = v.x; r.lead[2] = v.y; r.lead[3] = v.z;
+            }
         }
     }
 }
 
+// Cells that cross range boundaries: the range holding the head adds its trail and the
+// following ranges' lead pieces in order until the piece that ends the cell.
+__global__ void __launch_bounds__(kBlock)
+k_seg_fixup(long nrec, const SegRec* __restrict__ rec, const uint32_t* __restrict__ keys, CellWork cw) {
+    const long w = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (w >= nrec) return;
+    const int head = rec[w].trail_head;
+    if (head < 0) return;
+    double sw = rec[w].trail[0], sx = rec[w].trail[1], sy = rec[w].trail[2], sz = rec[w].trail[3];
+    int end = -1;
+    for (long v = w + 1; v < nrec; ++v) {
+        sw += rec[v].lead[0];
+        sx += rec[v].lead[1];
+        sy += rec[v].lead[2];
+        sz += rec[v].lead[3];
+        if (rec[v].lead_end >= 0) {
+            end = rec[v].lead_end;
+            break;
+        }
+    }
+    put_sums(cw, keys[head], sw, sx, sy, sz, head, end);
+}
+
 void launch_gather_segsum(const Batch& bt, Particles a, Particles s, const uint32_t* sorted_keys,
-                          const uint32_t* perm, CellWork cw, cudaStream_t st) {
+                          const uint32_t* perm, CellWork cw, SegRec* rec, cudaStream_t st) {
     if (bt.P <= 0) return;
-    const long warps = div_up(bt.P, kSegRange);
-    ++g_launches;
-    k_gather_segsum<<<div_up(warps, kSegWarps), kBlock, 0, st>>>(bt, a, s, sorted_keys, perm, cw);
+    const long warps = div_up((long)bt.P, (long)kSegRange);
+    g_launches += 2;
+    k_gather_segsum<<<div_up(warps, (long)kSegWarps), kBlock, 0, st>>>(bt, a, s, sorted_keys, perm, cw, rec);
+    k_seg_fixup<<<div_up(warps, (long)kBlock), kBlock, 0, st>>>(warps, rec, sorted_keys, cw);
 }
 
 // ---------------------------------------------------------------- persistent reweight

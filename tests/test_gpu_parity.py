@@ -179,6 +179,7 @@ class Lockstep:
         st, en = lib.get_cell_ranges()
         np.testing.assert_array_equal(st, ost)
         np.testing.assert_array_equal(en, oen)
+        self.last_ranges = (st, en)
         if ref is not None:
             ref.assign()
             r = ref.particles(0)
@@ -326,6 +327,35 @@ def test_lockstep_config0_scale(variant):
         print(variant, ls.report)
     finally:
         ls.close()
+
+
+def test_lockstep_crowded_cells():
+    """Cells holding thousands of particles: their sums span many 256-slot ranges of the sorted
+    set (range pieces combined by the fix-up pass), and ranges that lie wholly inside one cell or
+    end exactly at a cell boundary. The steady frame checks the sorted set and cell ranges bit for
+    bit and the masses built from the sums against the oracle."""
+    cfg = small_cfg("k3dom")
+    run = Lockstep(cfg, with_reference=False)
+    try:
+        run.first_frame()
+        a = run.lib.get_particles("persistent")
+        G = run.G
+        rng = np.random.default_rng(3)
+        pos, vel, cell = a["pos"].copy(), a["vel"].copy(), a["cell"].copy()
+        i = 0
+        for n, (x, y, z) in [(5000, (10, 12, 3)), (1500, (20, 8, 4)), (600, (5, 25, 2)), (257, (14, 14, 1)),
+                             (256, (15, 14, 1)), (255, (16, 14, 1))]:
+            pos[i:i + n] = np.float32([x, y, z]) + rng.uniform(0.3, 0.7, (n, 3)).astype(np.float32)
+            cell[i:i + n] = x + G * y + G * G * z
+            i += n
+        vel[:i] = 0.0
+        run.lib.set_particles("persistent", pos=pos, vel=vel, cell=cell)
+        run.steady_frame(1)
+        st, en = run.last_ranges
+        counts = np.where(st >= 0, en - st + 1, 0)
+        assert counts.max() >= 4000 and (counts > 256).sum() >= 3
+    finally:
+        run.close()
 
 
 def test_draws_equal_oracle():
