@@ -270,7 +270,7 @@ k3dom_status k3dom_set_timing(k3dom_handle* h, int enabled);
 typedef struct k3dom_diagnostics {
     int64_t nonfinite_points, ray_list_entries, ray_list_capacity, work_items;
     int32_t overflow;
-    int32_t kernel_launches_per_frame; /* kernels a steady-state frame enqueues */
+    int32_t kernel_launches_per_frame; /* kernels a steady-state frame enqueues (with its point upload) */
     int64_t kernel_evaluations;        /* K3DOM: in-support sparse-kernel evaluations, last frame */
 } k3dom_diagnostics;
 k3dom_status k3dom_get_diagnostics(k3dom_handle* h, k3dom_diagnostics* out);

@@ -130,6 +130,8 @@ struct k3dom_handle {
     int* ancestors = nullptr;
     float* pts = nullptr;  // device x | y | z, N slots each
     float* pts_pinned = nullptr;
+    float* pts_xyz = nullptr;         // device staging of interleaved scans (3 N floats)
+    float* pts_xyz_pinned = nullptr;  // pinned host staging of interleaved scans (3 N floats)
     RayBuffers rb{};
     std::vector<void*> ray_allocs;  // buffers sized by points and tiles (re-made on growth)
     void* export_buf = nullptr;
@@ -138,6 +140,7 @@ struct k3dom_handle {
 
     bool births_done = false;
     int launches_per_frame = 0;
+    int launches_upload = 0;  // kernels of the last frame's point upload (de-interleaving)
     int bgki_grid = 0, ds_grid = 0;
     int ds_sized_chunk = 0;  // chunk the DS count buffer was sized for
 
@@ -200,6 +203,8 @@ struct k3dom_handle {
         ray_allocs.clear();
         if (pts_pinned) cudaFreeHost(pts_pinned);
         pts_pinned = nullptr;
+        if (pts_xyz_pinned) cudaFreeHost(pts_xyz_pinned);
+        pts_xyz_pinned = nullptr;
     }
     void release() {
         drop_graph();
@@ -393,7 +398,9 @@ cudaError_t alloc_ray_buffers(k3dom_handle* h) {
     if ((e = h->alloc(&rb.hist, rb.hist_words, true, L))) return e;
     if ((e = h->alloc(&rb.scan_tmp, rb.scan_words, true, L))) return e;
     if ((e = h->alloc(&h->pts, 3 * (size_t)N, true, L))) return e;
+    if ((e = h->alloc(&h->pts_xyz, 3 * (size_t)N, true, L))) return e;
     if ((e = cudaMallocHost((void**)&h->pts_pinned, 3 * (size_t)N * sizeof(float)))) return e;
+    if ((e = cudaMallocHost((void**)&h->pts_xyz_pinned, 3 * (size_t)N * sizeof(float)))) return e;
     return cudaSuccess;
 }
 
@@ -461,21 +468,55 @@ k3dom_status grow_points(k3dom_handle* h, const int32_t* n) {
     return e == cudaSuccess ? K3DOM_OK : h->fail(e);
 }
 
+// A float is infinite or NaN exactly when its exponent bits are all ones; the branch-free OR
+// over the bits lets the compiler vectorise the scan.
+static bool nonfinite_any(const float* v, long m) {
+    uint32_t bad = 0;
+    for (long i = 0; i < m; ++i) {
+        uint32_t u;
+        std::memcpy(&u, v + i, sizeof(u));
+        bad |= (uint32_t)((u & 0x7F800000u) == 0x7F800000u);
+    }
+    return bad != 0;
+}
+
 bool has_nonfinite_host(const float* xs, const float* ys, const float* zs, int n) {
     const bool inter = (ys == nullptr || zs == nullptr);
-    const long m = inter ? 3L * n : n;
-    for (long i = 0; i < m; ++i)
-        if (!std::isfinite(xs[i])) return true;
-    if (!inter)
-        for (int i = 0; i < n; ++i)
-            if (!std::isfinite(ys[i]) || !std::isfinite(zs[i])) return true;
-    return false;
+    if (inter) return nonfinite_any(xs, 3L * n);
+    return nonfinite_any(xs, n) || nonfinite_any(ys, n) || nonfinite_any(zs, n);
+}
+
+// (x, y, z) interleaved -> the three point planes
+__global__ void k_deinterleave(const float* __restrict__ xyz, int n, float* __restrict__ x, float* __restrict__ y,
+                               float* __restrict__ z) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    x[i] = xyz[3 * i];
+    y[i] = xyz[3 * i + 1];
+    z[i] = xyz[3 * i + 2];
+}
+
+static cudaError_t deinterleave(k3dom_handle* h, const float* xyz, int n, float* dx, float* dy, float* dz) {
+    ++g_launches;
+    k_deinterleave<<<div_up(n, 256), 256, 0, h->st>>>(xyz, n, dx, dy, dz);
+    return cudaGetLastError();
+}
+
+static bool is_pinned_host(const void* p) {
+    cudaPointerAttributes a;
+    if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+        cudaGetLastError();  // unregistered pageable memory on older drivers
+        return false;
+    }
+    return a.type == cudaMemoryTypeHost;
 }
 
 // Points of scene s -> device SoA slots of the scene. Host input is staged through pinned
-// memory (the previous frame's copies have completed: set_frame_params waited on them).
+// memory (the previous frame's copies have completed: set_frame_params waited on them); an
+// interleaved scan in pinned host memory is read in place when the call waits for the frame
+// (sync), so the caller cannot reuse the buffer while the copy is pending.
 k3dom_status upload_points(k3dom_handle* h, int s, const float* xs, const float* ys, const float* zs, int n,
-                           k3dom_mem mem) {
+                           k3dom_mem mem, bool sync) {
     if (n == 0) return K3DOM_OK;
     const long N = h->N, o = h->off.point[s];
     float* dx = h->pts + o;
@@ -484,34 +525,34 @@ k3dom_status upload_points(k3dom_handle* h, int s, const float* xs, const float*
     const bool interleaved = (ys == nullptr || zs == nullptr);
     cudaError_t e;
     if (mem == K3DOM_MEM_HOST) {
-        float* hx = h->pts_pinned + o;
-        float* hy = h->pts_pinned + N + o;
-        float* hz = h->pts_pinned + 2 * N + o;
         if (interleaved) {
-            for (int i = 0; i < n; ++i) {
-                hx[i] = xs[3 * i];
-                hy[i] = xs[3 * i + 1];
-                hz[i] = xs[3 * i + 2];
+            // one upload of the interleaved scan (straight from the caller's memory when it is
+            // pinned), then the planes on the device
+            const float* src = xs;
+            if (!sync || !is_pinned_host(xs)) {
+                std::memcpy(h->pts_xyz_pinned + 3 * o, xs, 3 * n * sizeof(float));
+                src = h->pts_xyz_pinned + 3 * o;
             }
+            if ((e = cudaMemcpyAsync(h->pts_xyz + 3 * o, src, 3 * n * sizeof(float), cudaMemcpyHostToDevice,
+                                     h->st)) ||
+                (e = deinterleave(h, h->pts_xyz + 3 * o, n, dx, dy, dz)))
+                return h->fail(e);
         } else {
+            float* hx = h->pts_pinned + o;
+            float* hy = h->pts_pinned + N + o;
+            float* hz = h->pts_pinned + 2 * N + o;
             std::memcpy(hx, xs, n * sizeof(float));
             std::memcpy(hy, ys, n * sizeof(float));
             std::memcpy(hz, zs, n * sizeof(float));
+            if ((e = cudaMemcpyAsync(dx, hx, n * sizeof(float), cudaMemcpyHostToDevice, h->st)) ||
+                (e = cudaMemcpyAsync(dy, hy, n * sizeof(float), cudaMemcpyHostToDevice, h->st)) ||
+                (e = cudaMemcpyAsync(dz, hz, n * sizeof(float), cudaMemcpyHostToDevice, h->st)))
+                return h->fail(e);
         }
-        if ((e = cudaMemcpyAsync(dx, hx, n * sizeof(float), cudaMemcpyHostToDevice, h->st)) ||
-            (e = cudaMemcpyAsync(dy, hy, n * sizeof(float), cudaMemcpyHostToDevice, h->st)) ||
-            (e = cudaMemcpyAsync(dz, hz, n * sizeof(float), cudaMemcpyHostToDevice, h->st)))
-            return h->fail(e);
         if ((e = cudaEventRecord(h->ev_staged, h->st))) return h->fail(e);
     } else {
         if (interleaved) {
-            if ((e = cudaMemcpy2DAsync(dx, sizeof(float), xs, 3 * sizeof(float), sizeof(float), n,
-                                       cudaMemcpyDeviceToDevice, h->st)) ||
-                (e = cudaMemcpy2DAsync(dy, sizeof(float), xs + 1, 3 * sizeof(float), sizeof(float), n,
-                                       cudaMemcpyDeviceToDevice, h->st)) ||
-                (e = cudaMemcpy2DAsync(dz, sizeof(float), xs + 2, 3 * sizeof(float), sizeof(float), n,
-                                       cudaMemcpyDeviceToDevice, h->st)))
-                return h->fail(e);
+            if ((e = deinterleave(h, xs, n, dx, dy, dz))) return h->fail(e);
         } else {
             if ((e = cudaMemcpyAsync(dx, xs, n * sizeof(float), cudaMemcpyDeviceToDevice, h->st)) ||
                 (e = cudaMemcpyAsync(dy, ys, n * sizeof(float), cudaMemcpyDeviceToDevice, h->st)) ||
@@ -1006,10 +1047,12 @@ static k3dom_status update_impl(k3dom_handle* h, const float* t, const float* co
         np[s] = n[s];
     }
     if ((st = set_frame_params(h, dt.data(), np.data())) != K3DOM_OK) return st;
+    const long l_up = g_launches;
     for (int s = 0; s < S; ++s) {
-        st = upload_points(h, s, xs[s], ys ? ys[s] : nullptr, zs ? zs[s] : nullptr, n[s], mem);
+        st = upload_points(h, s, xs[s], ys ? ys[s] : nullptr, zs ? zs[s] : nullptr, n[s], mem, sync);
         if (st != K3DOM_OK) return st;
     }
+    h->launches_upload = (int)(g_launches - l_up);
     cudaError_t e;
     bool timed = false;
     if (steady) {
@@ -1021,7 +1064,7 @@ static k3dom_status update_impl(k3dom_handle* h, const float* t, const float* co
             // changed the point slots: stage them again
             if ((st = set_frame_params(h, dt.data(), np.data())) != K3DOM_OK) return st;
             for (int s = 0; s < S; ++s) {
-                st = upload_points(h, s, xs[s], ys ? ys[s] : nullptr, zs ? zs[s] : nullptr, n[s], mem);
+                st = upload_points(h, s, xs[s], ys ? ys[s] : nullptr, zs ? zs[s] : nullptr, n[s], mem, sync);
                 if (st != K3DOM_OK) return st;
             }
         }
@@ -1215,7 +1258,7 @@ k3dom_status k3dom_grid_cell_occupancy_update(k3dom_handle* h, float dt, const f
     if (s != K3DOM_OK) return s;
     if ((s = grow_points(h, &n)) != K3DOM_OK) return s;
     if ((s = set_frame_params_all(h, dt, n)) != K3DOM_OK) return s;
-    if ((s = upload_points(h, 0, xs, ys, zs, n, mem)) != K3DOM_OK) return s;
+    if ((s = upload_points(h, 0, xs, ys, zs, n, mem, false)) != K3DOM_OK) return s;
     if ((e = enq_occupancy(h, false))) return h->fail(e);
     return finish_sync(h);
 }
@@ -1256,7 +1299,7 @@ k3dom_status k3dom_initialize_particles(k3dom_handle* h, const float* xs, const 
     if (s != K3DOM_OK) return s;
     if ((s = grow_points(h, &n)) != K3DOM_OK) return s;
     if ((s = set_frame_params_all(h, 0.0f, n)) != K3DOM_OK) return s;
-    if ((s = upload_points(h, 0, xs, ys, zs, n, mem)) != K3DOM_OK) return s;
+    if ((s = upload_points(h, 0, xs, ys, zs, n, mem, false)) != K3DOM_OK) return s;
     if ((e = enq_occupancy(h, true))) return h->fail(e);
     if ((e = enq_init_particles(h))) return h->fail(e);
     return finish_sync(h);
@@ -1615,7 +1658,7 @@ k3dom_status k3dom_get_diagnostics(k3dom_handle* h, k3dom_diagnostics* out) {
     out->ray_list_capacity = h->rb.capacity;
     out->work_items = (int64_t)st.work_items;
     out->overflow = (int32_t)st.overflow;
-    out->kernel_launches_per_frame = h->launches_per_frame;
+    out->kernel_launches_per_frame = h->launches_per_frame + h->launches_upload;
     out->kernel_evaluations = (int64_t)st.kernel_evals;
     return K3DOM_OK;
 }
