@@ -114,6 +114,7 @@ struct k3dom_handle {
     Particles A{}, Ss{}, Bp{};
     uint32_t *sorted_keys = nullptr, *perm = nullptr, *alt_k = nullptr, *alt_v = nullptr;
     SegRec* seg_rec = nullptr;  // piece sums of the segmented per-cell sums, one per 256 sorted slots
+    int2* res_br = nullptr;     // ancestor brackets of the resampling blocks
     uint32_t *hist = nullptr, *scan_tmp = nullptr;
     long hist_words = 0, scan_tmp_words = 0;
     CellState cs[2]{};  // cs[0] live, cs[1] spare for the map shift
@@ -636,7 +637,7 @@ cudaError_t enq_resample(k3dom_handle* h, bool draws_ready) {
     launch_joint_prepare(h->batch(), h->Ss, h->Bp, h->st);
     if ((e = exact_scan_plan(h->plan_joint, h->plan_joint_n, h->exact_scratch, h->st))) return e;
     launch_resample(h->batch(), h->joint_cum, h->draw_sorted, h->Ss, h->Bp, h->A, h->ancestors, h->joint_max,
-                    h->st);
+                    h->res_br, h->st);
     return cudaGetLastError();
 }
 
@@ -838,7 +839,8 @@ k3dom_status k3dom_batch_create(const k3dom_params* params, int32_t n_scenes, k3
         (e = h->alloc_particles(&h->Bp, B)))
         return bail(e);
     if ((e = h->alloc(&h->sorted_keys, P)) || (e = h->alloc(&h->perm, P)) || (e = h->alloc(&h->alt_k, P)) ||
-        (e = h->alloc(&h->alt_v, P)) || (e = h->alloc(&h->seg_rec, seg_rec_count(P))))
+        (e = h->alloc(&h->alt_v, P)) || (e = h->alloc(&h->seg_rec, seg_rec_count(P))) ||
+        (e = h->alloc(&h->res_br, res_bracket_count(P))))
         return bail(e);
     if ((e = h->alloc_cells(&h->cs[0], C)) || (e = h->alloc_cells(&h->cs[1], C))) return bail(e);
     CellWork& cw = h->cw;

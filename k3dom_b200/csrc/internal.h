@@ -79,8 +79,10 @@ void launch_init_particles(const Batch& bt, const float* born_cum, Particles a, 
 void launch_joint_prepare(const Batch& bt, Particles s, Particles b, cudaStream_t st);
 int draw_key_bits(int S);
 void launch_draw_keys(const Batch& bt, uint32_t* keys, cudaStream_t st);
+long res_bracket_count(long P);
 void launch_resample(const Batch& bt, const float* joint_cum, const uint32_t* sorted_draws, Particles s,
-                     Particles b, Particles out, int* ancestors, float* joint_max_out, cudaStream_t st);
+                     Particles b, Particles out, int* ancestors, float* joint_max_out, int2* brackets,
+                     cudaStream_t st);
 void launch_debug_draws(uint64_t seed, int frame, int stage, long first, long count, float* dst,
                         cudaStream_t st);
 

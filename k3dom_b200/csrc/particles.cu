@@ -543,28 +543,65 @@ __device__ __forceinline__ ResScene res_scene(const Batch& bt, const float* join
     return r;
 }
 
-__global__ void __launch_bounds__(kResThreads)
-k_resample(Batch bt, const float* __restrict__ joint_cum, const uint32_t* __restrict__ dkeys, Particles s,
-           Particles b, Particles out, int* __restrict__ anc_out, float* __restrict__ joint_max_out) {
-    __shared__ int s_lo, s_hi;
-    const int k0 = blockIdx.x * kResThreads;
+long res_bracket_count(long P) { return P > 0 ? div_up(P, (long)kResThreads) : 1; }
+
+// The block's draws are sorted, so its ancestors lie in [lower(first draw), lower(last draw)]:
+// one thread per block of kResThreads draws finds that bracket (all blocks in parallel). A
+// block whose draws span two scenes gets (-1, -1) and searches each draw in full.
+__global__ void k_res_brackets(Batch bt, const float* __restrict__ joint_cum, const uint32_t* __restrict__ dkeys,
+                               int nblocks, int2* __restrict__ br) {
+    const int blk = blockIdx.x * blockDim.x + threadIdx.x;
+    if (blk >= nblocks) return;
+    const int k0 = blk * kResThreads;
     const int k1 = min(k0 + kResThreads, bt.P) - 1;
-    const int sc0 = scene_of(bt.off->part, bt.S, k0);
-    const bool one_scene = scene_of(bt.off->part, bt.S, k1) == sc0;
-    if (one_scene) {
-        // the block's draws are sorted: bracket their search by the first and last
-        const ResScene r = res_scene(bt, joint_cum, dkeys, sc0);
-        const int base = bt.off->part[sc0];
-        if (threadIdx.x == 0) s_lo = r.lower(r.draw(k0 - base), 0, r.n);
-        if (threadIdx.x == 32) s_hi = r.lower(r.draw(k1 - base), 0, r.n);
+    const int sc = scene_of(bt.off->part, bt.S, k0);
+    if (scene_of(bt.off->part, bt.S, k1) != sc) {
+        br[blk] = make_int2(-1, -1);
+        return;
     }
-    __syncthreads();
+    const ResScene r = res_scene(bt, joint_cum, dkeys, sc);
+    const int base = bt.off->part[sc];
+    const int lo = r.lower(r.draw(k0 - base), 0, r.n);
+    const int hi = r.lower(r.draw(k1 - base), lo, r.n);
+    br[blk] = make_int2(lo, hi);
+}
+
+constexpr int kResStage = 2048;  // bracket entries staged in shared memory
+
+__global__ void __launch_bounds__(kResThreads)
+k_resample(Batch bt, const float* __restrict__ joint_cum, const uint32_t* __restrict__ dkeys, const int2* br,
+           Particles s, Particles b, Particles out, int* __restrict__ anc_out, float* __restrict__ joint_max_out) {
+    __shared__ float s_acc[kResStage];
+    const int k0 = blockIdx.x * kResThreads;
     const int k = k0 + threadIdx.x;
-    if (k >= bt.P) return;
-    const int sc = one_scene ? sc0 : scene_of(bt.off->part, bt.S, k);
+    const int2 bk = br[blockIdx.x];
+    const int sc = bk.x >= 0 ? scene_of(bt.off->part, bt.S, k0)
+                             : scene_of(bt.off->part, bt.S, min(k, bt.P - 1));
     const ResScene r = res_scene(bt, joint_cum, dkeys, sc);
     const int kl = k - bt.off->part[sc];
-    int a = one_scene ? r.lower(r.draw(kl), s_lo, min(s_hi + 1, r.n)) : r.lower(r.draw(kl), 0, r.n);
+    int a;
+    if (bk.x >= 0) {
+        // search the bracket [lo, hi]; staged in shared memory when it fits (block-uniform)
+        const int lo = bk.x, hi = min(bk.y + 1, r.n), len = hi - lo;
+        if (len <= kResStage) {
+            for (int i = threadIdx.x; i < len; i += kResThreads) s_acc[i] = r.acc(lo + i);
+            __syncthreads();
+            if (k >= bt.P) return;
+            const float u = r.draw(kl);
+            int l = 0, h = len;  // first j in [0, len) with s_acc[j] >= u
+            while (l < h) {
+                const int mid = (l + h) >> 1;
+                if (s_acc[mid] < u) l = mid + 1; else h = mid;
+            }
+            a = lo + l;
+        } else {
+            if (k >= bt.P) return;
+            a = r.lower(r.draw(kl), lo, hi);
+        }
+    } else {
+        if (k >= bt.P) return;
+        a = r.lower(r.draw(kl), 0, r.n);
+    }
     if (a > r.n - 1) a = r.n - 1;
     const float new_w = __fdiv_rn(r.jmax, (float)r.P);
     if (a < r.P) {
@@ -586,11 +623,14 @@ k_resample(Batch bt, const float* __restrict__ joint_cum, const uint32_t* __rest
 }
 
 void launch_resample(const Batch& bt, const float* joint_cum, const uint32_t* sorted_draws, Particles s,
-                     Particles b, Particles out, int* ancestors, float* joint_max_out, cudaStream_t st) {
+                     Particles b, Particles out, int* ancestors, float* joint_max_out, int2* brackets,
+                     cudaStream_t st) {
     if (bt.P <= 0) return;
-    ++g_launches;
-    k_resample<<<div_up(bt.P, kResThreads), kResThreads, 0, st>>>(bt, joint_cum, sorted_draws, s, b, out,
-                                                                   ancestors, joint_max_out);
+    const int nblk = div_up(bt.P, kResThreads);
+    g_launches += 2;
+    k_res_brackets<<<div_up(nblk, 256), 256, 0, st>>>(bt, joint_cum, sorted_draws, nblk, brackets);
+    k_resample<<<nblk, kResThreads, 0, st>>>(bt, joint_cum, sorted_draws, brackets, s, b, out, ancestors,
+                                             joint_max_out);
 }
 
 // ---------------------------------------------------------------- debug draws
