@@ -156,34 +156,60 @@ k_gather_segsum(Batch bt, Particles a, Particles s, const uint32_t* __restrict__
         rec[warp_global].trail_head = -1;
     }
     __syncwarp();
-    for (long c0 = r0; c0 < r1; c0 += 32) {
+    // the particles of one 32-slot chunk, loaded one chunk ahead of their stores (the next chunk's
+    // loads are in flight while this one is stored and scanned; the slots differ, so this holds
+    // for an in-place gather too)
+    struct Chunk {
+        uint32_t key, next_key;
+        float px, py, pz, vx, vy, vz, w;
+        uint8_t assoc;
+    };
+    auto load_chunk = [&](long c0) {
+        Chunk c;
         const long pos = c0 + lane;
         const bool valid = pos < r1;
-        const uint32_t key = valid ? keys[pos] : 0xFFFFFFFEu;
-        const uint32_t next_key = (pos + 1 < P) ? keys[pos + 1] : 0xFFFFFFFDu;
+        c.key = valid ? keys[pos] : 0xFFFFFFFEu;
+        c.next_key = (pos + 1 < P) ? keys[pos + 1] : 0xFFFFFFFDu;
+        if (valid) {
+            const uint32_t src = perm[pos];
+            c.px = a.px[src]; c.py = a.py[src]; c.pz = a.pz[src];
+            c.vx = a.vx[src]; c.vy = a.vy[src]; c.vz = a.vz[src];
+            c.w = a.w[src];
+            c.assoc = a.assoc[src];
+        }
+        return c;
+    };
+    Chunk nxt = load_chunk(r0);
+#pragma unroll 1
+    for (int it = 0; it < kSegItems; ++it) {
+        const long c0 = r0 + 32L * it;
+        if (c0 >= r1) break;
+        const Chunk cur = nxt;
+        if (c0 + 32 < r1) nxt = load_chunk(c0 + 32);
+        const long pos = c0 + lane;
+        const bool valid = pos < r1;
+        const uint32_t key = cur.key;
         uint32_t kprev = __shfl_up_sync(0xffffffffu, key, 1);
         if (lane == 0) kprev = prev_key;
         prev_key = __shfl_sync(0xffffffffu, key, 31);
         const bool head = valid && (pos == 0 || key != kprev);
-        const bool tail = valid && (key != next_key);
+        const bool tail = valid && (key != cur.next_key);
 
         SegVal v = {0.0, 0.0, 0.0, 0.0};
         if (valid) {
-            const uint32_t src = perm[pos];
-            const float vx = a.vx[src], vy = a.vy[src], vz = a.vz[src];
-            const float w = a.w[src];
+            const float vx = cur.vx, vy = cur.vy, vz = cur.vz, w = cur.w;
             // sorted slots of a scene lie in its particle range (cells are scene-major)
             const float mv = bt.sc[scene_of(bt.off->part, bt.S, (int)pos)].p.min_vel;
             const float sp = __fadd_rn(__fadd_rn(__fmul_rn(vx, vx), __fmul_rn(vy, vy)), __fmul_rn(vz, vz));
             const bool slow = sp < __fmul_rn(mv, mv);
-            s.px[pos] = a.px[src];
-            s.py[pos] = a.py[src];
-            s.pz[pos] = a.pz[src];
+            s.px[pos] = cur.px;
+            s.py[pos] = cur.py;
+            s.pz[pos] = cur.pz;
             s.vx[pos] = vx;
             s.vy[pos] = vy;
             s.vz[pos] = vz;
             s.w[pos] = slow ? -w : w;  // sign bit = penalised at resampling
-            s.assoc[pos] = a.assoc[src];
+            s.assoc[pos] = cur.assoc;
             s.cell[pos] = (int)key;
             v.w = (double)w;
             v.x = (double)__fmul_rn(w, vx);
@@ -543,17 +569,20 @@ __device__ __forceinline__ ResScene res_scene(const Batch& bt, const float* join
     return r;
 }
 
-long res_bracket_count(long P) { return P > 0 ? div_up(P, (long)kResThreads) : 1; }
+constexpr int kResPerThread = 4;
+constexpr int kResBlock = kResThreads * kResPerThread;  // draws per resampling block
+
+long res_bracket_count(long P) { return P > 0 ? div_up(P, (long)kResBlock) : 1; }
 
 // The block's draws are sorted, so its ancestors lie in [lower(first draw), lower(last draw)]:
-// one thread per block of kResThreads draws finds that bracket (all blocks in parallel). A
-// block whose draws span two scenes gets (-1, -1) and searches each draw in full.
+// one thread per block of kResBlock draws finds that bracket (all blocks in parallel). A block
+// whose draws span two scenes gets (-1, -1) and searches each draw in full.
 __global__ void k_res_brackets(Batch bt, const float* __restrict__ joint_cum, const uint32_t* __restrict__ dkeys,
                                int nblocks, int2* __restrict__ br) {
     const int blk = blockIdx.x * blockDim.x + threadIdx.x;
     if (blk >= nblocks) return;
-    const int k0 = blk * kResThreads;
-    const int k1 = min(k0 + kResThreads, bt.P) - 1;
+    const int k0 = blk * kResBlock;
+    const int k1 = min(k0 + kResBlock, bt.P) - 1;
     const int sc = scene_of(bt.off->part, bt.S, k0);
     if (scene_of(bt.off->part, bt.S, k1) != sc) {
         br[blk] = make_int2(-1, -1);
@@ -566,67 +595,106 @@ __global__ void k_res_brackets(Batch bt, const float* __restrict__ joint_cum, co
     br[blk] = make_int2(lo, hi);
 }
 
-constexpr int kResStage = 2048;  // bracket entries staged in shared memory
+constexpr int kResStage = 4096;  // bracket entries staged in shared memory
+
+// One resampled particle: the ancestor's state, gathered before any store so that the loads of
+// a thread's draws are all in flight together.
+struct ResPart {
+    float px, py, pz, vx, vy, vz;
+    int cell;
+    uint8_t assoc;
+};
+
+__device__ __forceinline__ int res_clamp(const ResScene& r, int a) { return a > r.n - 1 ? r.n - 1 : a; }
+
+__device__ __forceinline__ ResPart res_load(const Batch& bt, const ResScene& r, int sc, int a, const Particles& s,
+                                            const Particles& b) {
+    ResPart v;
+    const bool pers = a < r.P;
+    const int q = pers ? bt.off->part[sc] + a : bt.off->birth[sc] + a - r.P;
+    const Particles& src = pers ? s : b;
+    v.px = src.px[q]; v.py = src.py[q]; v.pz = src.pz[q];
+    v.vx = src.vx[q]; v.vy = src.vy[q]; v.vz = src.vz[q];
+    v.cell = src.cell[q];
+    v.assoc = src.assoc[q];
+    return v;
+}
+
+__device__ __forceinline__ void res_store(const ResScene& r, int k, int a, const ResPart& v, Particles& out,
+                                          int* __restrict__ anc_out) {
+    out.px[k] = v.px; out.py[k] = v.py; out.pz[k] = v.pz;
+    out.vx[k] = v.vx; out.vy[k] = v.vy; out.vz[k] = v.vz;
+    out.cell[k] = v.cell;
+    out.assoc[k] = v.assoc;
+    out.w[k] = __fdiv_rn(r.jmax, (float)r.P);
+    anc_out[k] = a;
+}
 
 __global__ void __launch_bounds__(kResThreads)
 k_resample(Batch bt, const float* __restrict__ joint_cum, const uint32_t* __restrict__ dkeys, const int2* br,
            Particles s, Particles b, Particles out, int* __restrict__ anc_out, float* __restrict__ joint_max_out) {
     __shared__ float s_acc[kResStage];
-    const int k0 = blockIdx.x * kResThreads;
-    const int k = k0 + threadIdx.x;
+    const int k0 = blockIdx.x * kResBlock;
     const int2 bk = br[blockIdx.x];
-    const int sc = bk.x >= 0 ? scene_of(bt.off->part, bt.S, k0)
-                             : scene_of(bt.off->part, bt.S, min(k, bt.P - 1));
-    const ResScene r = res_scene(bt, joint_cum, dkeys, sc);
-    const int kl = k - bt.off->part[sc];
-    int a;
     if (bk.x >= 0) {
+        const int sc = scene_of(bt.off->part, bt.S, k0);
+        const ResScene r = res_scene(bt, joint_cum, dkeys, sc);
+        const int base = bt.off->part[sc];
         // search the bracket [lo, hi]; staged in shared memory when it fits (block-uniform)
         const int lo = bk.x, hi = min(bk.y + 1, r.n), len = hi - lo;
-        if (len <= kResStage) {
+        const bool staged = len <= kResStage;
+        if (staged) {
             for (int i = threadIdx.x; i < len; i += kResThreads) s_acc[i] = r.acc(lo + i);
             __syncthreads();
-            if (k >= bt.P) return;
-            const float u = r.draw(kl);
-            int l = 0, h = len;  // first j in [0, len) with s_acc[j] >= u
-            while (l < h) {
-                const int mid = (l + h) >> 1;
-                if (s_acc[mid] < u) l = mid + 1; else h = mid;
+        }
+        int a[kResPerThread];
+#pragma unroll
+        for (int it = 0; it < kResPerThread; ++it) {
+            const int k = k0 + it * kResThreads + threadIdx.x;
+            a[it] = 0;
+            if (k >= bt.P) continue;
+            const float u = r.draw(k - base);
+            if (staged) {
+                int l = 0, h = len;  // first j in [0, len) with s_acc[j] >= u
+                while (l < h) {
+                    const int mid = (l + h) >> 1;
+                    if (s_acc[mid] < u) l = mid + 1; else h = mid;
+                }
+                a[it] = res_clamp(r, lo + l);
+            } else {
+                a[it] = res_clamp(r, r.lower(u, lo, hi));
             }
-            a = lo + l;
-        } else {
-            if (k >= bt.P) return;
-            a = r.lower(r.draw(kl), lo, hi);
+        }
+        ResPart v[kResPerThread];
+#pragma unroll
+        for (int it = 0; it < kResPerThread; ++it)
+            if (k0 + it * kResThreads + (int)threadIdx.x < bt.P) v[it] = res_load(bt, r, sc, a[it], s, b);
+#pragma unroll
+        for (int it = 0; it < kResPerThread; ++it) {
+            const int k = k0 + it * kResThreads + threadIdx.x;
+            if (k >= bt.P) continue;
+            res_store(r, k, a[it], v[it], out, anc_out);
+            if (k == base && joint_max_out) joint_max_out[sc] = r.jmax;
         }
     } else {
-        if (k >= bt.P) return;
-        a = r.lower(r.draw(kl), 0, r.n);
+        for (int it = 0; it < kResPerThread; ++it) {
+            const int k = k0 + it * kResThreads + threadIdx.x;
+            if (k >= bt.P) break;
+            const int sc = scene_of(bt.off->part, bt.S, k);
+            const ResScene r = res_scene(bt, joint_cum, dkeys, sc);
+            const int kl = k - bt.off->part[sc];
+            const int a = res_clamp(r, r.lower(r.draw(kl), 0, r.n));
+            res_store(r, k, a, res_load(bt, r, sc, a, s, b), out, anc_out);
+            if (kl == 0 && joint_max_out) joint_max_out[sc] = r.jmax;
+        }
     }
-    if (a > r.n - 1) a = r.n - 1;
-    const float new_w = __fdiv_rn(r.jmax, (float)r.P);
-    if (a < r.P) {
-        const int q = bt.off->part[sc] + a;
-        out.px[k] = s.px[q]; out.py[k] = s.py[q]; out.pz[k] = s.pz[q];
-        out.vx[k] = s.vx[q]; out.vy[k] = s.vy[q]; out.vz[k] = s.vz[q];
-        out.cell[k] = s.cell[q];
-        out.assoc[k] = s.assoc[q];
-    } else {
-        const int q = bt.off->birth[sc] + a - r.P;
-        out.px[k] = b.px[q]; out.py[k] = b.py[q]; out.pz[k] = b.pz[q];
-        out.vx[k] = b.vx[q]; out.vy[k] = b.vy[q]; out.vz[k] = b.vz[q];
-        out.cell[k] = b.cell[q];
-        out.assoc[k] = b.assoc[q];
-    }
-    out.w[k] = new_w;
-    anc_out[k] = a;
-    if (kl == 0 && joint_max_out) joint_max_out[sc] = r.jmax;
 }
 
 void launch_resample(const Batch& bt, const float* joint_cum, const uint32_t* sorted_draws, Particles s,
                      Particles b, Particles out, int* ancestors, float* joint_max_out, int2* brackets,
                      cudaStream_t st) {
     if (bt.P <= 0) return;
-    const int nblk = div_up(bt.P, kResThreads);
+    const int nblk = div_up(bt.P, kResBlock);
     g_launches += 2;
     k_res_brackets<<<div_up(nblk, 256), 256, 0, st>>>(bt, joint_cum, sorted_draws, nblk, brackets);
     k_resample<<<nblk, kResThreads, 0, st>>>(bt, joint_cum, sorted_draws, brackets, s, b, out, ancestors,
