@@ -355,7 +355,9 @@ def run_ours(args):
             rule_name = "16x16x8"  # the rule's choice for grids of >= 2^20 cells
         if tr_file.exists():
             try:
-                traffic = json.loads(tr_file.read_text())["per_tiling"].get(rule_name, {}).get("dram_bytes_per_launch")
+                per = json.loads(tr_file.read_text())["per_tiling"]
+                hit = per.get(f"{rule_name}@{tuning['chunk']}") or per.get(rule_name) or {}
+                traffic = hit.get("dram_bytes_per_launch")
             except Exception:
                 traffic = None
         out = {

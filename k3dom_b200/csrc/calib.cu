@@ -218,6 +218,15 @@ __device__ inline FrameBar frame_adjoint(const FrameIn& in, double k2, double F3
     return b;
 }
 
+// Frame k's sums of cell c as (F occ, F free, H occ, H free), FP64: the exact 64-bit unit sums
+// times 2^-kCalibShift (a power of two, so the conversion is exact up to 2^53 units).
+__device__ __forceinline__ double4 frame_sums(const long long* __restrict__ acc, long C, int k, long c) {
+    const longlong2* p = reinterpret_cast<const longlong2*>(acc + (((long)k * C + c) << 2));
+    const longlong2 a = p[0], b = p[1];
+    const double u = 1.0 / (double)(1ull << kCalibShift);
+    return make_double4((double)a.x * u, (double)a.y * u, (double)b.x * u, (double)b.y * u);
+}
+
 struct CalibCellArgs {
     int C, F;
     double ls, sigma, gamma, prior_occ, prior_free;
@@ -226,7 +235,7 @@ struct CalibCellArgs {
     double g[kMaxCalibFrames];   // gamma^dt of each frame (1 for the first)
     double gd[kMaxCalibFrames];  // d gamma^dt / d gamma (0 for the first frame and for dt = 0)
     const float* dyn[kMaxCalibFrames];  // per frame: particle weight sums (nullptr = none)
-    const double* sums;                 // F x 4 x C: f occ, f free, -x f' occ, -x f' free
+    const long long* acc;               // F x C x 4 units of 2^-kCalibShift: f occ, f free, -x f' occ, -x f' free
     const uint32_t* n0;
     const uint32_t* n1;
     float* occ_out;  // optional
@@ -262,13 +271,13 @@ __global__ void __launch_bounds__(256) k_calib_cells(CalibCellArgs a) {
 #pragma unroll(NF <= 4 ? NF : 1)
         for (int k = 0; k < NF; ++k) {
             if (k < a.F) {
-                const double* s = a.sums + (long)k * 4 * C;
+                const double4 s = frame_sums(a.acc, C, k, c);
                 FrameIn& x = in[k];
                 x.mf = mf; x.ms = ms; x.md = md;
                 x.g = a.g[k];
                 x.dyn = (k == 0 || !a.dyn[k]) ? 0.0 : (double)a.dyn[k][c];
-                x.Eo = a.sigma * s[c];
-                x.Ef = a.sigma * s[C + c];
+                x.Eo = a.sigma * s.x;
+                x.Ef = a.sigma * s.y;
                 frame_forward(x, a.k2, &mf, &ms, &md);
             }
         }
@@ -293,10 +302,10 @@ __global__ void __launch_bounds__(256) k_calib_cells(CalibCellArgs a) {
         for (int k = NF - 1; k >= 0; --k) {
             if (k < a.F) {
                 const FrameBar b = frame_adjoint(in[k], a.k2, Fb, Sb, Db);
-                const double* s = a.sums + (long)k * 4 * C;
+                const double4 s = frame_sums(a.acc, C, k, c);
                 // E = sigma F: dE/dsigma = F, dE/dls = sigma H / ls
-                g_sig += b.Eo * s[c] + b.Ef * s[C + c];
-                g_ls += (b.Eo * s[2 * C + c] + b.Ef * s[3 * C + c]) * a.sigma / a.ls;
+                g_sig += b.Eo * s.x + b.Ef * s.y;
+                g_ls += (b.Eo * s.z + b.Ef * s.w) * a.sigma / a.ls;
                 g_gam += b.g * a.gd[k];
                 Fb = b.mf; Sb = b.ms; Db = b.md;
             }
@@ -320,15 +329,14 @@ __global__ void __launch_bounds__(256) k_calib_cells(CalibCellArgs a) {
     if (threadIdx.x == 0 && r != 0.0) atomicAdd(&a.red[5], r);
 }
 
-// acc4 (units of 2^-40) -> sums (FP64); clears acc4.
-__global__ void k_take_sums(unsigned long long* __restrict__ acc4, long C, double* __restrict__ sums) {
-    const double inv = 1.0 / (double)(1ull << kCalibShift);
+// One frame's sums as four planes q x C (the layout k3dom_calib_get_sums returns).
+__global__ void k_sums_planes(const long long* __restrict__ acc, long C, int k, double* __restrict__ out) {
     for (long c = blockIdx.x * (long)blockDim.x + threadIdx.x; c < C; c += (long)gridDim.x * blockDim.x) {
-        for (int q = 0; q < 4; ++q) {
-            const long long v = (long long)acc4[4 * c + q];
-            sums[q * C + c] = (double)v * inv;
-            acc4[4 * c + q] = 0ull;
-        }
+        const double4 v = frame_sums(acc, C, k, c);
+        out[c] = v.x;
+        out[C + c] = v.y;
+        out[2 * C + c] = v.z;
+        out[3 * C + c] = v.w;
     }
 }
 
@@ -432,8 +440,8 @@ struct k3dom_calib {
     int ray_points = 0;
     float ray_ls = 0.0f;  // length-scale the list capacity was sized for
     float4 *ftab = nullptr, *htab = nullptr;
-    unsigned long long* acc4 = nullptr;
-    double* sums = nullptr;  // F x 4 x C
+    long long* acc = nullptr;        // F x C x 4 exact unit sums of the frames
+    double* sums_out = nullptr;      // 4 x C staging of k3dom_calib_get_sums
     int sums_frames = 0;
     double* red = nullptr;
     double red_host[6] = {0};
@@ -528,13 +536,13 @@ k3dom_status compute_sums(k3dom_calib* c, float ls) {
     cudaError_t e;
     const long C = c->dp.C;
     if (c->sums_frames != F) {
-        if (c->sums) {
-            auto it = std::find(c->allocs.begin(), c->allocs.end(), (void*)c->sums);
+        if (c->acc) {
+            auto it = std::find(c->allocs.begin(), c->allocs.end(), (void*)c->acc);
             if (it != c->allocs.end()) c->allocs.erase(it);
-            cudaFree(c->sums);
-            c->sums = nullptr;
+            cudaFree(c->acc);
+            c->acc = nullptr;
         }
-        if ((e = c->alloc(&c->sums, (size_t)F * 4 * C))) return c->fail(e);
+        if ((e = c->alloc(&c->acc, (size_t)F * 4 * C))) return c->fail(e);
         c->sums_frames = F;
     }
     SceneDev sd;
@@ -581,15 +589,15 @@ k3dom_status compute_sums(k3dom_calib* c, float ls) {
         bt.sc = c->sc_dev;
         bt.fp = c->fp_dev + k;
         bt.off = c->off_dev + k;
+        long long* acc_k = c->acc + (long)k * 4 * C;
+        if ((e = cudaMemsetAsync(acc_k, 0, sizeof(long long) * 4 * (size_t)C, c->st))) return c->fail(e);
         if (f.n > 0) {
             if ((e = build_ray_lists(bt, f.pts, f.pts + f.n, f.pts + 2 * (long)f.n, c->rb, false, c->status, c->st)))
                 return c->fail(e);
-            if ((e = launch_bgki_sums(bt, c->rb, c->ftab, c->htab, c->acc4, c->status, c->num_sms, c->st)))
+            if ((e = launch_bgki_sums(bt, c->rb, c->ftab, c->htab, reinterpret_cast<unsigned long long*>(acc_k),
+                                      c->status, c->num_sms, c->st)))
                 return c->fail(e);
         }
-        ++g_launches;
-        k_take_sums<<<grid_for(C), kBlock, 0, c->st>>>(c->acc4, C, c->sums + (long)k * 4 * C);
-        if ((e = cudaGetLastError())) return c->fail(e);
     }
     DevStatus dst;
     if ((e = cudaMemcpyAsync(&dst, c->status, sizeof(dst), cudaMemcpyDeviceToHost, c->st)) ||
@@ -622,7 +630,7 @@ k3dom_status run_cells(k3dom_calib* c, const float theta[5], bool grad, float* o
         a.gd[k] = (k > 0 && dt > 0.0) ? dt * std::pow(a.gamma, dt - 1.0) : 0.0;
         a.dyn[k] = c->frames[k].dyn;
     }
-    a.sums = c->sums;
+    a.acc = c->acc;
     a.n0 = c->n0;
     a.n1 = c->n1;
     a.occ_out = occ_out;
@@ -697,7 +705,7 @@ k3dom_status k3dom_calib_create(const k3dom_params* base, int device, k3dom_cali
     if ((e = c->alloc(&c->n0, d.C)) || (e = c->alloc(&c->n1, d.C)) || (e = c->alloc(&c->sc_dev, 1)) ||
         (e = c->alloc(&c->off_dev, kMaxCalibFrames)) || (e = c->alloc(&c->fp_dev, kMaxCalibFrames)) ||
         (e = c->alloc(&c->status, 1)) || (e = c->alloc(&c->ftab, kKernelTableSize)) ||
-        (e = c->alloc(&c->htab, kKernelTableSize)) || (e = c->alloc(&c->acc4, 4 * (size_t)d.C)) ||
+        (e = c->alloc(&c->htab, kKernelTableSize)) || (e = c->alloc(&c->sums_out, 4 * (size_t)d.C)) ||
         (e = c->alloc(&c->red, 6)))
         return bail(e);
     std::vector<float4> ft(kKernelTableSize), ht(kKernelTableSize);
@@ -810,9 +818,12 @@ k3dom_status k3dom_calib_get_sums(k3dom_calib* c, float ls, int32_t frame, doubl
     k3dom_status s = compute_sums(c, ls);
     if (s != K3DOM_OK) return s;
     const size_t C = (size_t)c->dp.C;
-    cudaError_t e = cudaMemcpyAsync(out, c->sums + (size_t)frame * 4 * C, sizeof(double) * 4 * C,
-                                    mem == K3DOM_MEM_HOST ? cudaMemcpyDeviceToHost : cudaMemcpyDeviceToDevice,
-                                    c->st);
+    double* planes = mem == K3DOM_MEM_HOST ? c->sums_out : out;
+    ++g_launches;
+    k_sums_planes<<<grid_for((long)C), kBlock, 0, c->st>>>(c->acc, (long)C, frame, planes);
+    cudaError_t e = cudaGetLastError();
+    if (e == cudaSuccess && mem == K3DOM_MEM_HOST)
+        e = cudaMemcpyAsync(out, planes, sizeof(double) * 4 * C, cudaMemcpyDeviceToHost, c->st);
     if (e == cudaSuccess) e = cudaStreamSynchronize(c->st);
     return e == cudaSuccess ? K3DOM_OK : c->fail(e);
 }
