@@ -159,8 +159,14 @@ struct RadixSmem {
 
 // vals_in == nullptr: the value is the input position (first pass of an argsort).
 // vals_out == nullptr: values are not written (key-only sort).
+// CTAs per SM that the shared memory of a BITS-wide pass allows (RadixSmem: 38, 56, 80 KB)
 template <int BITS>
-__global__ void __launch_bounds__(kSortThreads)
+struct DownsweepMinBlocks {
+    static constexpr int value = BITS <= 8 ? 4 : (BITS <= 10 ? 3 : 2);
+};
+
+template <int BITS>
+__global__ void __launch_bounds__(kSortThreads, DownsweepMinBlocks<BITS>::value)
 radix_downsweep(const uint32_t* __restrict__ keys_in, const uint32_t* __restrict__ vals_in, long nmax,
                 const uint32_t* dn, int shift, const uint32_t* __restrict__ hist_scan,
                 uint32_t* __restrict__ keys_out, uint32_t* __restrict__ vals_out) {
