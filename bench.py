@@ -44,6 +44,7 @@ PEAKS_FILE = ROOT / "MEASURED_PEAKS.json"
 FALLBACK_HBM_GBS = 6650.0
 NOMINAL_FP32_TFLOPS = 148 * 128 * 2 * 1.965e9 / 1e12  # 74.4: no measured FP32 peak exists
 FLOP_PER_EVAL = 20  # distance (8 + sqrt) + sparse kernel (2x/ls, cospi, sinpi, 7 arithmetic)
+FLOP_PER_DS_NEIGHBOUR = 25  # window test (c.m, (c.m)^2/|m|^2, compare: 8) + pOcc (r^2, exp, scale: 17)
 
 
 def log(*a):
@@ -343,7 +344,9 @@ def run_ours(args):
         hbm_peak, peak_src = read_peaks()
         ev_ms = stage["evidence_ms"]
         n_evals = float(np.mean(evals))
-        achieved_tflops = n_evals * FLOP_PER_EVAL / (ev_ms * 1e-3) / 1e12
+        ds = args.variant != "k3dom"
+        flop_per = FLOP_PER_DS_NEIGHBOUR if ds else FLOP_PER_EVAL
+        achieved_tflops = n_evals * flop_per / (ev_ms * 1e-3) / 1e12
         part_ms = stage["predict_ms"] + stage["assign_ms"] + stage["persistent_ms"] + stage["births_ms"] + \
             stage["resample_ms"]
         part_bytes = hbm_bytes_particle_stages(P, B, C_, cfg.n_points)
@@ -353,7 +356,7 @@ def run_ours(args):
         rule_name = ["by-size", "8x8x4", "16x16x4", "16x16x8"][tuning["tile_rule"]]
         if rule_name == "by-size":
             rule_name = "16x16x8"  # the rule's choice for grids of >= 2^20 cells
-        if tr_file.exists():
+        if tr_file.exists() and args.variant == "k3dom":
             try:
                 per = json.loads(tr_file.read_text())["per_tiling"]
                 hit = per.get(f"{rule_name}@{tuning['chunk']}") or per.get(rule_name) or {}
@@ -377,11 +380,13 @@ def run_ours(args):
             "gpu_launches": launches * Kst,
             "clocks": clocks,
             "roofline": {
-                "kernel": "k_bgki (sparse BGKI evidence + fused cell update)",
+                "kernel": ("k_dsgrid (DS measurement grid + fused Dempster update)" if ds else
+                           "k_bgki (sparse BGKI evidence + fused cell update)"),
                 "bound": "fp32", "achieved": round(achieved_tflops, 3), "peak": round(NOMINAL_FP32_TFLOPS, 1),
                 "unit": "TFLOP/s", "frac": round(achieved_tflops / NOMINAL_FP32_TFLOPS, 4), "traffic": traffic,
                 "peak_source": "nominal FP32 (148 SMs x 128 lanes x 2 x 1.965 GHz); no measured FP32 peak",
-                "work": f"{n_evals:.4g} in-support kernel evaluations x {FLOP_PER_EVAL} FLOP per frame",
+                "work": (f"{n_evals:.4g} accepted neighbours x {flop_per} FLOP per frame" if ds else
+                         f"{n_evals:.4g} in-support kernel evaluations x {flop_per} FLOP per frame"),
                 "launch_ms": round(ev_ms, 4),
             },
             "roofline_hbm": {

@@ -435,8 +435,13 @@ struct k3dom_calib {
     SceneDev* sc_dev = nullptr;
     SceneOffsets* off_dev = nullptr;
     FrameParams* fp_dev = nullptr;  // one per frame
-    DevStatus* status = nullptr;
-    RayBuffers rb{};
+    // two lanes: frame k bins and sums on lane k % 2 (its own ray buffers, status and stream),
+    // so one frame's ray lists are built while the other frame's sums run
+    static constexpr int kLanes = 2;
+    DevStatus* status = nullptr;  // kLanes entries
+    RayBuffers rb[kLanes]{};
+    cudaStream_t st2 = nullptr;
+    cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
     int ray_points = 0;
     float ray_ls = 0.0f;  // length-scale the list capacity was sized for
     float4 *ftab = nullptr, *htab = nullptr;
@@ -466,6 +471,9 @@ struct k3dom_calib {
         for (void* p : allocs) cudaFree(p);
         ray_allocs.clear();
         allocs.clear();
+        if (ev_fork) cudaEventDestroy(ev_fork);
+        if (ev_join) cudaEventDestroy(ev_join);
+        if (st2) cudaStreamDestroy(st2);
         if (st) cudaStreamDestroy(st);
     }
 };
@@ -486,6 +494,8 @@ TileShape calib_tiles(const DevParams& p) {
     return t;
 }
 
+cudaError_t alloc_ray_lane(k3dom_calib* c, RayBuffers& rb, int max_points, long need, int T);
+
 // Ray buffers for the largest frame at the scene's length-scale: re-made only when the point
 // count or the worst-case list length outgrows them, then with 25 % headroom, so a calibration
 // loop that moves ls a little does not reallocate.
@@ -493,10 +503,19 @@ cudaError_t ensure_ray_buffers(k3dom_calib* c, int max_points, float ls, const S
     const int T = sd.ts.ntx * sd.ts.nty * sd.ts.ntz;
     long need = std::max(ray_entries_bound(sd.p, sd.ts, std::max(max_points, 1), sd.bin_R), 4096L);
     if (need > 0xFFFFFFF0L) need = 0xFFFFFFF0L;
-    if (max_points <= c->ray_points && need <= c->rb.capacity && c->rb.ekeys) return cudaSuccess;
+    if (max_points <= c->ray_points && need <= c->rb[0].capacity && c->rb[0].ekeys) return cudaSuccess;
     for (void* p : c->ray_allocs) cudaFree(p);
     c->ray_allocs.clear();
-    RayBuffers& rb = c->rb;
+    for (int l = 0; l < k3dom_calib::kLanes; ++l) {
+        cudaError_t e = alloc_ray_lane(c, c->rb[l], max_points, need, T);
+        if (e != cudaSuccess) return e;
+    }
+    c->ray_points = std::max(max_points, 1);
+    c->ray_ls = ls;
+    return cudaSuccess;
+}
+
+cudaError_t alloc_ray_lane(k3dom_calib* c, RayBuffers& rb, int max_points, long need, int T) {
     rb = RayBuffers{};
     const int N = std::max(max_points, 1);
     long cap = std::min(need + need / 4, 0xFFFFFFF0L);
@@ -523,8 +542,6 @@ cudaError_t ensure_ray_buffers(k3dom_calib* c, int max_points, float ls, const S
     rb.hist_words = std::max(radix_hist_words(cap, 11), 1L);
     rb.scan_words = scan_u32_tiles(std::max({rb.hist_words, (long)N, (long)T + 1})) + 16;
     if ((e = c->alloc(&rb.hist, rb.hist_words, L)) || (e = c->alloc(&rb.scan_tmp, rb.scan_words, L))) return e;
-    c->ray_points = N;
-    c->ray_ls = ls;
     return cudaSuccess;
 }
 
@@ -578,6 +595,13 @@ k3dom_status compute_sums(k3dom_calib* c, float ls) {
         if ((e = cudaMemcpyAsync(c->off_dev + k, &off, sizeof(off), cudaMemcpyHostToDevice, c->st)) ||
             (e = cudaMemcpyAsync(c->fp_dev + k, &fp, sizeof(fp), cudaMemcpyHostToDevice, c->st)))
             return c->fail(e);
+    }
+    if ((e = cudaEventRecord(c->ev_fork, c->st)) || (e = cudaStreamWaitEvent(c->st2, c->ev_fork, 0)))
+        return c->fail(e);
+    for (int k = 0; k < F; ++k) {
+        const CalibFrame& f = c->frames[k];
+        const int l = k % k3dom_calib::kLanes;
+        cudaStream_t sk = l == 0 ? c->st : c->st2;
         Batch bt;
         bt.S = 1;
         bt.variant = 0;
@@ -590,20 +614,24 @@ k3dom_status compute_sums(k3dom_calib* c, float ls) {
         bt.fp = c->fp_dev + k;
         bt.off = c->off_dev + k;
         long long* acc_k = c->acc + (long)k * 4 * C;
-        if ((e = cudaMemsetAsync(acc_k, 0, sizeof(long long) * 4 * (size_t)C, c->st))) return c->fail(e);
+        if ((e = cudaMemsetAsync(acc_k, 0, sizeof(long long) * 4 * (size_t)C, sk))) return c->fail(e);
         if (f.n > 0) {
-            if ((e = build_ray_lists(bt, f.pts, f.pts + f.n, f.pts + 2 * (long)f.n, c->rb, false, c->status, c->st)))
+            if ((e = build_ray_lists(bt, f.pts, f.pts + f.n, f.pts + 2 * (long)f.n, c->rb[l], false, c->status + l,
+                                     sk)))
                 return c->fail(e);
-            if ((e = launch_bgki_sums(bt, c->rb, c->ftab, c->htab, reinterpret_cast<unsigned long long*>(acc_k),
-                                      c->status, c->num_sms, c->st)))
+            if ((e = launch_bgki_sums(bt, c->rb[l], c->ftab, c->htab, reinterpret_cast<unsigned long long*>(acc_k),
+                                      c->status + l, c->num_sms, sk)))
                 return c->fail(e);
         }
     }
-    DevStatus dst;
-    if ((e = cudaMemcpyAsync(&dst, c->status, sizeof(dst), cudaMemcpyDeviceToHost, c->st)) ||
+    if ((e = cudaEventRecord(c->ev_join, c->st2)) || (e = cudaStreamWaitEvent(c->st, c->ev_join, 0)))
+        return c->fail(e);
+    DevStatus dst[k3dom_calib::kLanes];
+    if ((e = cudaMemcpyAsync(dst, c->status, sizeof(dst), cudaMemcpyDeviceToHost, c->st)) ||
         (e = cudaStreamSynchronize(c->st)))
         return c->fail(e);
-    if (dst.overflow) return K3DOM_ERR_CAPACITY;
+    for (int l = 0; l < k3dom_calib::kLanes; ++l)
+        if (dst[l].overflow) return K3DOM_ERR_CAPACITY;
     c->sums_ls = ls;
     return K3DOM_OK;
 }
@@ -701,10 +729,14 @@ k3dom_status k3dom_calib_create(const k3dom_params* base, int device, k3dom_cali
     d.ls = base->ls;
     d.sigma = 1.0f;
     d.window_radius = base->resolution * 0.866f;
-    if ((e = cudaStreamCreateWithFlags(&c->st, cudaStreamNonBlocking))) return bail(e);
+    if ((e = cudaStreamCreateWithFlags(&c->st, cudaStreamNonBlocking)) ||
+        (e = cudaStreamCreateWithFlags(&c->st2, cudaStreamNonBlocking)) ||
+        (e = cudaEventCreateWithFlags(&c->ev_fork, cudaEventDisableTiming)) ||
+        (e = cudaEventCreateWithFlags(&c->ev_join, cudaEventDisableTiming)))
+        return bail(e);
     if ((e = c->alloc(&c->n0, d.C)) || (e = c->alloc(&c->n1, d.C)) || (e = c->alloc(&c->sc_dev, 1)) ||
         (e = c->alloc(&c->off_dev, kMaxCalibFrames)) || (e = c->alloc(&c->fp_dev, kMaxCalibFrames)) ||
-        (e = c->alloc(&c->status, 1)) || (e = c->alloc(&c->ftab, kKernelTableSize)) ||
+        (e = c->alloc(&c->status, k3dom_calib::kLanes)) || (e = c->alloc(&c->ftab, kKernelTableSize)) ||
         (e = c->alloc(&c->htab, kKernelTableSize)) || (e = c->alloc(&c->sums_out, 4 * (size_t)d.C)) ||
         (e = c->alloc(&c->red, 6)))
         return bail(e);

@@ -978,6 +978,7 @@ __global__ void __launch_bounds__(kEvThreads) k_dsgrid(EvArgs A) {
     unsigned int* counter = COUNT ? &A.status->work_counter2 : &A.status->work_counter;
     uint32_t* part_max = reinterpret_cast<uint32_t*>(A.acc);
     uint32_t* part_flags = part_max + bt.C;
+    unsigned nev = 0;  // accepted neighbours of this lane (the roofline's work count, final pass)
 
     for (;;) {
         if (threadIdx.x == 0) {
@@ -1049,6 +1050,7 @@ __global__ void __launch_bounds__(kEvThreads) k_dsgrid(EvArgs A) {
                         if (nb < quota && ds_is_neighbor(L.x, L.y, L.z, acs, a, sd.wr2)) {
                             ++nb;
                             if (!COUNT) {
+                                ++nev;
                                 if (acs > a.w) all_far = false;
                                 const float o = ds_pocc(L.x, L.y, L.z, a, p.meas_occ_stddev);
                                 if (o > mx) mx = o;
@@ -1099,6 +1101,11 @@ __global__ void __launch_bounds__(kEvThreads) k_dsgrid(EvArgs A) {
             if (threadIdx.x == 0) A.tile_done[it.t] = 0;
         }
         __syncthreads();
+    }
+    if (!COUNT) {
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) nev += __shfl_xor_sync(0xffffffffu, nev, o);
+        if (lane == 0 && nev) atomicAdd(&A.status->kernel_evals, (unsigned long long)nev);
     }
 }
 
