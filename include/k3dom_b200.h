@@ -207,6 +207,13 @@ typedef enum k3dom_cell_field {
 } k3dom_cell_field;
 k3dom_status k3dom_get_cell_field(k3dom_handle* h, k3dom_cell_field field, float* dst,
                                   k3dom_mem mem);
+/* Registered output (no reference counterpart; the reference's node reads the grid after each
+ * updateGrid): from the next frame on, every frame also writes `field` of the selected scene to
+ * dst (C floats; device memory, or pinned host memory -- pageable host memory is refused with
+ * K3DOM_ERR_INVALID_ARGUMENT). The export runs on a side stream as soon as the field is final
+ * and the frame completes only when it has landed, so after k3dom_update_grid returns (or
+ * k3dom_synchronize) dst holds the frame's field. dst == NULL stops it. */
+k3dom_status k3dom_set_output(k3dom_handle* h, k3dom_cell_field field, float* dst, k3dom_mem mem);
 /* start_idx / end_idx per cell (-1 when empty), as particleToGridKernel leaves them. */
 k3dom_status k3dom_get_cell_ranges(k3dom_handle* h, int32_t* start, int32_t* end,
                                    k3dom_mem mem);

@@ -143,6 +143,7 @@ SIGNATURES = {
     "k3dom_get_info": (_ST, [_P, C.POINTER(Info)]),
     "k3dom_index_to_coord": (_ST, [_P, C.c_int32, _F, _F, _F]),
     "k3dom_get_cell_field": (_ST, [_P, C.c_int, _P, C.c_int]),
+    "k3dom_set_output": (_ST, [_P, C.c_int, _P, C.c_int]),
     "k3dom_get_cell_ranges": (_ST, [_P, _P, _P, C.c_int]),
     "k3dom_get_gridcell_aos": (_ST, [_P, _P, C.c_int]),
     "k3dom_get_mappoints": (_ST, [_P, _P, C.c_int]),

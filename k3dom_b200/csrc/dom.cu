@@ -100,7 +100,15 @@ struct k3dom_handle {
     int P = 0, B = 0, C = 0, N = 0, T = 0;
 
     cudaStream_t st = nullptr, st2 = nullptr, st3 = nullptr;  // frame; resampling draws; ray lists
+    cudaStream_t st4 = nullptr;                               // registered output export
     cudaEvent_t ev_fork = nullptr, ev_join = nullptr, ev_bin = nullptr;
+    cudaEvent_t ev_out = nullptr, ev_out_done = nullptr;
+    // registered output (k3dom_set_output): one cell field of one scene, written every frame
+    int out_field = -1, out_scene = 0;
+    void* out_dst = nullptr;
+    k3dom_mem out_mem = K3DOM_MEM_HOST;
+    float* out_buf = nullptr;          // device staging when the destination is host memory
+    DevStatus* status_host = nullptr;  // pinned copy of the status, read after each frame
     cudaEvent_t ev_t[8] = {};
     bool timing = false;
     k3dom_stage_times times{};
@@ -213,16 +221,21 @@ struct k3dom_handle {
         for (void* p : allocs) cudaFree(p);
         allocs.clear();
         if (fp_host) cudaFreeHost(fp_host);
+        if (status_host) cudaFreeHost(status_host);
         if (export_buf) cudaFree(export_buf);
+        if (out_buf) cudaFree(out_buf);
         for (auto& e : ev_t)
             if (e) cudaEventDestroy(e);
         if (ev_fork) cudaEventDestroy(ev_fork);
         if (ev_join) cudaEventDestroy(ev_join);
         if (ev_bin) cudaEventDestroy(ev_bin);
         if (ev_staged) cudaEventDestroy(ev_staged);
+        if (ev_out) cudaEventDestroy(ev_out);
+        if (ev_out_done) cudaEventDestroy(ev_out_done);
         if (st) cudaStreamDestroy(st);
         if (st2) cudaStreamDestroy(st2);
         if (st3) cudaStreamDestroy(st3);
+        if (st4) cudaStreamDestroy(st4);
     }
     CellState cells() const { return cs[0]; }
     Batch batch() const {
@@ -512,12 +525,16 @@ static bool is_pinned_host(const void* p) {
     return a.type == cudaMemoryTypeHost;
 }
 
-// Points of scene s -> device SoA slots of the scene. Host input is staged through pinned
-// memory (the previous frame's copies have completed: set_frame_params waited on them); an
-// interleaved scan in pinned host memory is read in place when the call waits for the frame
-// (sync), so the caller cannot reuse the buffer while the copy is pending.
+// Points of scene s -> device SoA slots of the scene, in two phases. kStage starts the upload
+// of an interleaved host scan into device staging (straight from the caller's memory when it is
+// pinned and the call waits for the frame, so the caller cannot reuse the buffer while the copy
+// is pending; otherwise through pinned memory, whose previous use set_frame_params waited on);
+// the host's finiteness check runs while that copy is in flight. kPlace writes the planes:
+// de-interleaving on the device, or copies of separate x/y/z arrays.
+enum UploadPhase { kStage, kPlace };
+
 k3dom_status upload_points(k3dom_handle* h, int s, const float* xs, const float* ys, const float* zs, int n,
-                           k3dom_mem mem, bool sync) {
+                           k3dom_mem mem, bool sync, UploadPhase phase) {
     if (n == 0) return K3DOM_OK;
     const long N = h->N, o = h->off.point[s];
     float* dx = h->pts + o;
@@ -525,10 +542,8 @@ k3dom_status upload_points(k3dom_handle* h, int s, const float* xs, const float*
     float* dz = h->pts + 2 * N + o;
     const bool interleaved = (ys == nullptr || zs == nullptr);
     cudaError_t e;
-    if (mem == K3DOM_MEM_HOST) {
-        if (interleaved) {
-            // one upload of the interleaved scan (straight from the caller's memory when it is
-            // pinned), then the planes on the device
+    if (mem == K3DOM_MEM_HOST && interleaved) {
+        if (phase == kStage) {
             const float* src = xs;
             if (!sync || !is_pinned_host(xs)) {
                 std::memcpy(h->pts_xyz_pinned + 3 * o, xs, 3 * n * sizeof(float));
@@ -536,37 +551,61 @@ k3dom_status upload_points(k3dom_handle* h, int s, const float* xs, const float*
             }
             if ((e = cudaMemcpyAsync(h->pts_xyz + 3 * o, src, 3 * n * sizeof(float), cudaMemcpyHostToDevice,
                                      h->st)) ||
-                (e = deinterleave(h, h->pts_xyz + 3 * o, n, dx, dy, dz)))
+                (e = cudaEventRecord(h->ev_staged, h->st)))
                 return h->fail(e);
-        } else {
-            float* hx = h->pts_pinned + o;
-            float* hy = h->pts_pinned + N + o;
-            float* hz = h->pts_pinned + 2 * N + o;
-            std::memcpy(hx, xs, n * sizeof(float));
-            std::memcpy(hy, ys, n * sizeof(float));
-            std::memcpy(hz, zs, n * sizeof(float));
-            if ((e = cudaMemcpyAsync(dx, hx, n * sizeof(float), cudaMemcpyHostToDevice, h->st)) ||
-                (e = cudaMemcpyAsync(dy, hy, n * sizeof(float), cudaMemcpyHostToDevice, h->st)) ||
-                (e = cudaMemcpyAsync(dz, hz, n * sizeof(float), cudaMemcpyHostToDevice, h->st)))
-                return h->fail(e);
+            return K3DOM_OK;
         }
-        if ((e = cudaEventRecord(h->ev_staged, h->st))) return h->fail(e);
+        if ((e = deinterleave(h, h->pts_xyz + 3 * o, n, dx, dy, dz))) return h->fail(e);
+        return K3DOM_OK;
+    }
+    if (phase == kStage) return K3DOM_OK;
+    if (mem == K3DOM_MEM_HOST) {
+        float* hx = h->pts_pinned + o;
+        float* hy = h->pts_pinned + N + o;
+        float* hz = h->pts_pinned + 2 * N + o;
+        std::memcpy(hx, xs, n * sizeof(float));
+        std::memcpy(hy, ys, n * sizeof(float));
+        std::memcpy(hz, zs, n * sizeof(float));
+        if ((e = cudaMemcpyAsync(dx, hx, n * sizeof(float), cudaMemcpyHostToDevice, h->st)) ||
+            (e = cudaMemcpyAsync(dy, hy, n * sizeof(float), cudaMemcpyHostToDevice, h->st)) ||
+            (e = cudaMemcpyAsync(dz, hz, n * sizeof(float), cudaMemcpyHostToDevice, h->st)) ||
+            (e = cudaEventRecord(h->ev_staged, h->st)))
+            return h->fail(e);
+    } else if (interleaved) {
+        if ((e = deinterleave(h, xs, n, dx, dy, dz))) return h->fail(e);
     } else {
-        if (interleaved) {
-            if ((e = deinterleave(h, xs, n, dx, dy, dz))) return h->fail(e);
-        } else {
-            if ((e = cudaMemcpyAsync(dx, xs, n * sizeof(float), cudaMemcpyDeviceToDevice, h->st)) ||
-                (e = cudaMemcpyAsync(dy, ys, n * sizeof(float), cudaMemcpyDeviceToDevice, h->st)) ||
-                (e = cudaMemcpyAsync(dz, zs, n * sizeof(float), cudaMemcpyDeviceToDevice, h->st)))
-                return h->fail(e);
-        }
+        if ((e = cudaMemcpyAsync(dx, xs, n * sizeof(float), cudaMemcpyDeviceToDevice, h->st)) ||
+            (e = cudaMemcpyAsync(dy, ys, n * sizeof(float), cudaMemcpyDeviceToDevice, h->st)) ||
+            (e = cudaMemcpyAsync(dz, zs, n * sizeof(float), cudaMemcpyDeviceToDevice, h->st)))
+            return h->fail(e);
     }
     return K3DOM_OK;
 }
 
+// Every scene's points: stage, check host scans for non-finite coordinates (refused before
+// anything reads the staging), place.
+k3dom_status upload_all(k3dom_handle* h, const float* const* xs, const float* const* ys, const float* const* zs,
+                        const int32_t* n, k3dom_mem mem, bool sync, bool check) {
+    k3dom_status st;
+    for (int s = 0; s < h->S; ++s)
+        if ((st = upload_points(h, s, xs[s], ys ? ys[s] : nullptr, zs ? zs[s] : nullptr, n[s], mem, sync, kStage)))
+            return st;
+    if (check && mem == K3DOM_MEM_HOST)
+        for (int s = 0; s < h->S; ++s)
+            if (n[s] > 0 && has_nonfinite_host(xs[s], ys ? ys[s] : nullptr, zs ? zs[s] : nullptr, n[s]))
+                return K3DOM_ERR_INVALID_INPUT;
+    for (int s = 0; s < h->S; ++s)
+        if ((st = upload_points(h, s, xs[s], ys ? ys[s] : nullptr, zs ? zs[s] : nullptr, n[s], mem, sync, kPlace)))
+            return st;
+    return K3DOM_OK;
+}
+
+// Arguments only; host scans are checked for non-finite coordinates while they upload (upload_all).
 k3dom_status check_points(const float* xs, const float* ys, const float* zs, int n, k3dom_mem mem) {
+    (void)ys;
+    (void)zs;
+    (void)mem;
     if (n < 0 || (n > 0 && !xs)) return K3DOM_ERR_INVALID_ARGUMENT;
-    if (mem == K3DOM_MEM_HOST && n > 0 && has_nonfinite_host(xs, ys, zs, n)) return K3DOM_ERR_INVALID_INPUT;
     return K3DOM_OK;
 }
 
@@ -648,6 +687,34 @@ cudaError_t enq_init_particles(k3dom_handle* h) {
     return cudaGetLastError();
 }
 
+// Registered output: the field of the chosen scene is exported on a side stream as soon as the
+// stage it depends on has run (the cell update for masses, velocities, evidence and reweight
+// factors; the births' scan for w_A / w_UA), so its copy overlaps the rest of the frame. The frame
+// joins it at its end (enq_output_join).
+bool output_needs_births(int field) { return field == 12 || field == 13; }
+
+cudaError_t enq_output(k3dom_handle* h) {
+    if (h->out_field < 0 || !h->out_dst) return cudaSuccess;
+    const int s = h->out_scene;
+    const SceneHost& x = h->sc[s];
+    const long co = h->off.cell[s];
+    cudaError_t e;
+    if ((e = cudaEventRecord(h->ev_out, h->st)) || (e = cudaStreamWaitEvent(h->st4, h->ev_out, 0))) return e;
+    float* dev = h->out_mem == K3DOM_MEM_HOST ? h->out_buf : static_cast<float*>(h->out_dst);
+    launch_export_field(x.dp, h->out_field, offset_cells(h->cells(), co), offset_work(h->cw, co),
+                        h->born_cum + co, h->off.part[s], dev, h->st4);
+    if ((e = cudaGetLastError())) return e;
+    if (h->out_mem == K3DOM_MEM_HOST &&
+        (e = cudaMemcpyAsync(h->out_dst, dev, sizeof(float) * (size_t)x.dp.C, cudaMemcpyDeviceToHost, h->st4)))
+        return e;
+    return cudaEventRecord(h->ev_out_done, h->st4);
+}
+
+cudaError_t enq_output_join(k3dom_handle* h) {
+    if (h->out_field < 0 || !h->out_dst) return cudaSuccess;
+    return cudaStreamWaitEvent(h->st, h->ev_out_done, 0);
+}
+
 // The steady-state frame (DOM::updateGrid's branch for updated_time > 0), all scenes.
 cudaError_t enq_frame(k3dom_handle* h) {
     cudaError_t e;
@@ -677,12 +744,15 @@ cudaError_t enq_frame(k3dom_handle* h) {
         return e;
     }
     rec(h, 3);
+    if (!output_needs_births(h->out_field) && (e = enq_output(h))) return e;
     if ((e = enq_persistent(h))) return e;
     rec(h, 4);
     if ((e = enq_births(h))) return e;
     rec(h, 5);
+    if (output_needs_births(h->out_field) && (e = enq_output(h))) return e;
     if ((e = cudaStreamWaitEvent(h->st, h->ev_join, 0))) return e;
     if ((e = enq_resample(h, true))) return e;
+    if ((e = enq_output_join(h))) return e;
     rec(h, 6);
     h->launches_per_frame = (int)(g_launches - l0);
     return cudaSuccess;
@@ -823,6 +893,11 @@ k3dom_status k3dom_batch_create(const k3dom_params* params, int32_t n_scenes, k3
     if ((e = cudaStreamCreateWithFlags(&h->st, cudaStreamNonBlocking))) return bail(e);
     if ((e = cudaStreamCreateWithFlags(&h->st2, cudaStreamNonBlocking))) return bail(e);
     if ((e = cudaStreamCreateWithFlags(&h->st3, cudaStreamNonBlocking))) return bail(e);
+    if ((e = cudaStreamCreateWithFlags(&h->st4, cudaStreamNonBlocking))) return bail(e);
+    if ((e = cudaEventCreateWithFlags(&h->ev_out, cudaEventDisableTiming))) return bail(e);
+    if ((e = cudaEventCreateWithFlags(&h->ev_out_done, cudaEventDisableTiming))) return bail(e);
+    if ((e = cudaMallocHost((void**)&h->status_host, sizeof(DevStatus)))) return bail(e);
+    std::memset(h->status_host, 0, sizeof(DevStatus));
     if ((e = cudaEventCreateWithFlags(&h->ev_bin, cudaEventDisableTiming))) return bail(e);
     if ((e = cudaEventCreateWithFlags(&h->ev_fork, cudaEventDisableTiming))) return bail(e);
     if ((e = cudaEventCreateWithFlags(&h->ev_join, cudaEventDisableTiming))) return bail(e);
@@ -913,6 +988,7 @@ k3dom_status k3dom_destroy(k3dom_handle* h) {
     cudaStreamSynchronize(h->st);
     cudaStreamSynchronize(h->st2);
     cudaStreamSynchronize(h->st3);
+    cudaStreamSynchronize(h->st4);
     h->release();
     delete h;
     return K3DOM_OK;
@@ -1015,14 +1091,11 @@ static cudaError_t copy_cells_back(k3dom_handle* h, int s) {
 }
 
 static k3dom_status finish_sync(k3dom_handle* h) {
-    cudaError_t e = cudaStreamSynchronize(h->st);
+    cudaError_t e = cudaSuccess;
+    if (h->status) e = cudaMemcpyAsync(h->status_host, h->status, sizeof(DevStatus), cudaMemcpyDeviceToHost, h->st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(h->st);
     if (e != cudaSuccess) return h->fail(e);
-    if (h->status) {
-        DevStatus st;
-        e = cudaMemcpy(&st, h->status, sizeof(st), cudaMemcpyDeviceToHost);
-        if (e != cudaSuccess) return h->fail(e);
-        if (st.overflow) return K3DOM_ERR_CAPACITY;
-    }
+    if (h->status && h->status_host->overflow) return K3DOM_ERR_CAPACITY;
     return K3DOM_OK;
 }
 
@@ -1050,10 +1123,7 @@ static k3dom_status update_impl(k3dom_handle* h, const float* t, const float* co
     }
     if ((st = set_frame_params(h, dt.data(), np.data())) != K3DOM_OK) return st;
     const long l_up = g_launches;
-    for (int s = 0; s < S; ++s) {
-        st = upload_points(h, s, xs[s], ys ? ys[s] : nullptr, zs ? zs[s] : nullptr, n[s], mem, sync);
-        if (st != K3DOM_OK) return st;
-    }
+    if ((st = upload_all(h, xs, ys, zs, n, mem, sync, true)) != K3DOM_OK) return st;
     h->launches_upload = (int)(g_launches - l_up);
     cudaError_t e;
     bool timed = false;
@@ -1065,10 +1135,7 @@ static k3dom_status update_impl(k3dom_handle* h, const float* t, const float* co
             // the candidate's upload of this frame's points happened before any re-layout
             // changed the point slots: stage them again
             if ((st = set_frame_params(h, dt.data(), np.data())) != K3DOM_OK) return st;
-            for (int s = 0; s < S; ++s) {
-                st = upload_points(h, s, xs[s], ys ? ys[s] : nullptr, zs ? zs[s] : nullptr, n[s], mem, sync);
-                if (st != K3DOM_OK) return st;
-            }
+            if ((st = upload_all(h, xs, ys, zs, n, mem, sync, false)) != K3DOM_OK) return st;
         }
         if (h->timing || !h->graph_mode || tuning) {
             const bool was = h->timing;
@@ -1098,6 +1165,7 @@ static k3dom_status update_impl(k3dom_handle* h, const float* t, const float* co
         // DOM::initializeParticles (src/k3dom/dom.cu:52-77; src/dsphdmib/dom.cu:55-82)
         if ((e = enq_occupancy(h, true))) return h->fail(e);
         if ((e = enq_init_particles(h))) return h->fail(e);
+        if ((e = enq_output(h)) || (e = enq_output_join(h))) return h->fail(e);
     }
     for (int s = 0; s < S; ++s) {
         SceneHost& x = h->sc[s];
@@ -1260,7 +1328,7 @@ k3dom_status k3dom_grid_cell_occupancy_update(k3dom_handle* h, float dt, const f
     if (s != K3DOM_OK) return s;
     if ((s = grow_points(h, &n)) != K3DOM_OK) return s;
     if ((s = set_frame_params_all(h, dt, n)) != K3DOM_OK) return s;
-    if ((s = upload_points(h, 0, xs, ys, zs, n, mem, false)) != K3DOM_OK) return s;
+    if ((s = upload_all(h, &xs, &ys, &zs, &n, mem, false, true)) != K3DOM_OK) return s;
     if ((e = enq_occupancy(h, false))) return h->fail(e);
     return finish_sync(h);
 }
@@ -1301,7 +1369,7 @@ k3dom_status k3dom_initialize_particles(k3dom_handle* h, const float* xs, const 
     if (s != K3DOM_OK) return s;
     if ((s = grow_points(h, &n)) != K3DOM_OK) return s;
     if ((s = set_frame_params_all(h, 0.0f, n)) != K3DOM_OK) return s;
-    if ((s = upload_points(h, 0, xs, ys, zs, n, mem, false)) != K3DOM_OK) return s;
+    if ((s = upload_all(h, &xs, &ys, &zs, &n, mem, false, true)) != K3DOM_OK) return s;
     if ((e = enq_occupancy(h, true))) return h->fail(e);
     if ((e = enq_init_particles(h))) return h->fail(e);
     return finish_sync(h);
@@ -1427,6 +1495,25 @@ k3dom_status k3dom_get_cell_field(k3dom_handle* h, k3dom_cell_field field, float
     if (mem == K3DOM_MEM_HOST) return deliver(h, dst, out, bytes, mem);
     e = cudaStreamSynchronize(h->st);
     return e == cudaSuccess ? K3DOM_OK : h->fail(e);
+}
+
+k3dom_status k3dom_set_output(k3dom_handle* h, k3dom_cell_field field, float* dst, k3dom_mem mem) {
+    if (!h || (dst && ((int)field < 0 || field >= K3DOM_CELL_FIELD_COUNT))) return K3DOM_ERR_INVALID_ARGUMENT;
+    if (dst && mem == K3DOM_MEM_HOST && !is_pinned_host(dst)) return K3DOM_ERR_INVALID_ARGUMENT;
+    cudaSetDevice(h->device);
+    cudaError_t e = cudaStreamSynchronize(h->st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(h->st4);
+    if (e != cudaSuccess) return h->fail(e);
+    // device staging for a host destination: sized for every cell of the handle, so any scene fits
+    if (dst && mem == K3DOM_MEM_HOST && !h->out_buf &&
+        (e = cudaMalloc((void**)&h->out_buf, sizeof(float) * (size_t)std::max(h->C, 1))))
+        return h->fail(e);
+    h->out_field = dst ? (int)field : -1;
+    h->out_dst = dst;
+    h->out_mem = mem;
+    h->out_scene = h->cur;
+    h->drop_graph();  // the frame graph holds the export: capture it again
+    return K3DOM_OK;
 }
 
 k3dom_status k3dom_get_cell_ranges(k3dom_handle* h, int32_t* start, int32_t* end, k3dom_mem mem) {

@@ -249,6 +249,30 @@ class DOM:
     def indexToCoordZ(self, i: int) -> float: return self.indexToCoord(i)[2]
 
     # -- readback
+    def set_output(self, name: Optional[str], out=None) -> None:
+        """Registered output: every following frame writes cell field `name` of this scene into
+        `out` (a float32 array of grid_cell_count cells in pinned host memory, e.g.
+        torch.empty(n).pin_memory(), or a CUDA tensor) as part of the frame; None stops it."""
+        if name is None or out is None:
+            N.check(self._lib.k3dom_set_output(self._sel(), 0, None, N.MEM_HOST), "set_output")
+            self._output = None
+            return
+        dev = _is_cuda_tensor(out)
+        n = out.numel() if dev or hasattr(out, "numel") else np.asarray(out).size
+        if n != self.grid_cell_count:
+            raise ValueError(f"output needs {self.grid_cell_count} floats, got {n}")
+        if dev:
+            ptr, mem = out.data_ptr(), N.MEM_DEVICE
+        elif hasattr(out, "data_ptr"):
+            ptr, mem = out.data_ptr(), N.MEM_HOST
+        else:
+            arr = np.asarray(out)
+            if arr.dtype != np.float32 or not arr.flags.c_contiguous:
+                raise ValueError("output must be a contiguous float32 array")
+            ptr, mem = arr.ctypes.data, N.MEM_HOST
+        N.check(self._lib.k3dom_set_output(self._sel(), N.CELL_FIELDS[name], ptr, mem), "set_output")
+        self._output = out
+
     def get_cell_field(self, name: str) -> np.ndarray:
         out = np.empty(self.grid_cell_count, np.float32)
         N.check(self._lib.k3dom_get_cell_field(self._sel(), N.CELL_FIELDS[name], _ptr(out), N.MEM_HOST), name)

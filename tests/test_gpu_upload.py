@@ -46,3 +46,66 @@ def test_upload_routes_agree():
     finally:
         for d in doms.values():
             d.close()
+
+
+@pytest.mark.parametrize("graph", [True, False])
+def test_registered_output_equals_readback(graph):
+    """k3dom_set_output: every frame writes the field into pinned host or device memory as part of
+    the frame; after k3dom_update_grid returns it equals what k3dom_get_cell_field reads back.
+    Mass fields are exported after the cell update, w_UA after the births' scan."""
+    cfg = scene.small(seed=23, G=32, Gz=8, res=0.2, P=8192, B=2048, n_points=1500)
+    p = K.make_params("k3dom", **cfg.params)
+    d = K.DOM(p)
+    try:
+        d.set_graph_mode(graph)
+        n = d.grid_cell_count
+        with pytest.raises(K.dom.N.K3domError):
+            d.set_output("occ_mean", np.zeros(n, np.float32))  # pageable host memory is refused
+        for f, field in enumerate(["occ_mean", "occ_mean", "w_UA", "w_UA", "dynamic_mass", "occ_mean"]):
+            host = torch.full((n,), -7.0, dtype=torch.float32).pin_memory()
+            dev = torch.full((n,), -7.0, dtype=torch.float32, device="cuda:0")
+            out = host if f % 2 == 0 else dev
+            d.set_output(field, out)
+            t = 0.1 + 0.1 * f
+            s, pts = cfg.scene.scan(f, t, cfg.n_points)
+            d.updatePose(*s)
+            d.updateGrid(t, pts)
+            got = out.cpu().numpy() if out.is_cuda else out.numpy()
+            np.testing.assert_array_equal(got, d.get_cell_field(field), err_msg=f"frame {f} {field}")
+        d.set_output(None)
+        s, pts = cfg.scene.scan(9, 1.0, cfg.n_points)
+        d.updatePose(*s)
+        d.updateGrid(1.0, pts)  # no output registered: the frame runs without the export
+    finally:
+        d.close()
+
+
+@pytest.mark.parametrize("pinned", [False, True])
+def test_nonfinite_host_scan_is_refused_without_side_effects(pinned):
+    """A host scan with a non-finite coordinate is refused (K3DOM_ERR_INVALID_INPUT) before the
+    frame runs; the handle then continues exactly as one that never saw the refused call."""
+    cfg = scene.small(seed=29, G=32, Gz=8, res=0.2, P=8192, B=2048, n_points=1500)
+    p = K.make_params("k3dom", **cfg.params)
+    a, b = K.DOM(p), K.DOM(p)
+    try:
+        for f in range(4):
+            t = 0.1 + 0.1 * f
+            s, pts = cfg.scene.scan(f, t, cfg.n_points)
+            pts = np.ascontiguousarray(pts, np.float32)
+            if f == 2:
+                bad = pts.copy()
+                bad[777, 1] = np.nan
+                if pinned:
+                    bad = torch.from_numpy(bad).pin_memory().numpy()
+                a.updatePose(*s)
+                with pytest.raises(K.dom.N.K3domError) as e:
+                    a.updateGrid(t, bad)
+                assert e.value.status == 8  # K3DOM_ERR_INVALID_INPUT
+            for d in (a, b):
+                d.updatePose(*s)
+                d.updateGrid(t, pts)
+        for fld in FIELDS:
+            np.testing.assert_array_equal(a.get_cell_field(fld), b.get_cell_field(fld), err_msg=fld)
+    finally:
+        a.close()
+        b.close()
