@@ -40,6 +40,8 @@ namespace k3dom {
 
 constexpr int kChunk = 1024;      // largest number of rays per work item
 constexpr int kKernelTab = 512;  // intervals of the sparse-kernel table over u = d^2 / ls^2
+constexpr int kKernelTabEntries = kKernelTab + 1;  // + a zero entry at u = 1
+static_assert(kKernelTabEntries == kKernelTableSize, "kernel table size");
 constexpr int kEvThreads = 256;
 constexpr int kEvWarps = kEvThreads / 32;
 constexpr int kDsMaxNeighbors = 100;  // measurement_grid.cu:87
@@ -498,17 +500,19 @@ void build_kernel_table(float sigma, double scale, float4* out) {
         const double c3 = -4.5 * y[0] + 13.5 * y[1] - 13.5 * y[2] + 4.5 * y[3];
         out[i] = make_float4((float)c0, (float)c1, (float)c2, (float)c3);
     }
+    out[kKernelTab] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
 }
 
-// Table position of u = d^2 / ls^2: interval i = floor(t) and offset f = t - i, t = u * kKernelTab
-// clamped below kKernelTab. The floor is taken without conversion instructions: t + 2^23 rounded
-// down is 2^23 + floor(t) exactly for 0 <= t < 2^23, whose low mantissa bits are floor(t).
+// Table position t = d^2 * (kKernelTab / ls^2) = u * kKernelTab (the factor kKernelTab is a power
+// of two, so folding it into 1 / ls^2 changes no bit): interval i = floor(t), offset f = t - i.
+// Inside the support (d^2 < ls^2) t <= kKernelTab, and entry kKernelTab is zero, so no clamp is
+// needed. The floor is taken without conversion instructions: t + 2^23 rounded down is
+// 2^23 + floor(t) exactly for 0 <= t < 2^23, whose low mantissa bits are floor(t).
 struct TabPos {
     int i;
     float f;
 };
-__device__ __forceinline__ TabPos tab_pos(float u) {
-    const float t = fminf(u * (float)kKernelTab, (float)kKernelTab - 3.0517578e-05f);
+__device__ __forceinline__ TabPos tab_pos(float t) {
     const float tr = __fadd_rd(t, 8388608.0f);
     TabPos q;
     q.i = __float_as_int(tr) - 0x4B000000;
@@ -519,8 +523,8 @@ __device__ __forceinline__ float tab_eval(const float4* __restrict__ tab, TabPos
     const float4 c = tab[q.i];
     return fmaf(q.f, fmaf(q.f, fmaf(q.f, c.w, c.z), c.y), c.x);
 }
-__device__ __forceinline__ float kernel_tab(const float4* __restrict__ tab, float u) {
-    return tab_eval(tab, tab_pos(u));
+__device__ __forceinline__ float kernel_tab(const float4* __restrict__ tab, float t) {
+    return tab_eval(tab, tab_pos(t));
 }
 
 // mass_update.cu:12-14, 1 - 2 / (1 + exp(2 mass / mass_scale)), with k2 = 2 / mass_scale
@@ -615,13 +619,13 @@ __device__ void k3dom_cell_update(const DevParams& p, double g, int c, double de
 // the FP64 (sub-block, ray) constants of the rays that pass the cull.
 // (dynamic, sized by the work item's ray count so that smaller chunks leave room for more CTAs)
 struct BgkiSmem {
-    float4* ktab;                 // [kKernelTab] sparse-kernel table of the current scene
+    float4* ktab;                 // [kKernelTabEntries] sparse-kernel table of the current scene
     float4 (*stage)[32][3];       // [kEvWarps][32][3]
     float4* a;                    // [chunk] m.x, m.y, m.z, d_m
     double4* c;                   // [chunk] d_m, margin, 1/d_m
 };
 
-constexpr size_t kBgkiFixedBytes = sizeof(float4) * kKernelTab + sizeof(float4) * kEvWarps * 32 * 3;
+constexpr size_t kBgkiFixedBytes = sizeof(float4) * kKernelTabEntries + sizeof(float4) * kEvWarps * 32 * 3;
 
 inline size_t bgki_smem_bytes(int chunk) {
     return ((kBgkiFixedBytes + 31) & ~(size_t)31) + (size_t)chunk * (sizeof(float4) + sizeof(double4));
@@ -630,7 +634,7 @@ inline size_t bgki_smem_bytes(int chunk) {
 __device__ __forceinline__ BgkiSmem bgki_smem(unsigned char* base, int chunk) {
     BgkiSmem S;
     S.ktab = reinterpret_cast<float4*>(base);
-    S.stage = reinterpret_cast<float4(*)[32][3]>(base + sizeof(float4) * kKernelTab);
+    S.stage = reinterpret_cast<float4(*)[32][3]>(base + sizeof(float4) * kKernelTabEntries);
     const size_t off = (kBgkiFixedBytes + 31) & ~(size_t)31;
     S.c = reinterpret_cast<double4*>(base + off);  // 32-byte aligned
     S.a = reinterpret_cast<float4*>(base + off + sizeof(double4) * (size_t)chunk);
@@ -733,12 +737,13 @@ __global__ void __launch_bounds__(kEvThreads, MINB) k_bgki(EvArgs A) {
         const FrameParams fp = bt.fp[it.sc];
         const int coff = bt.off->cell[it.sc];
         const float ls2 = p.ls * p.ls;
-        const float inv_ls2 = 1.0f / ls2;
+        const float tscale = (1.0f / ls2) * (float)kKernelTab;  // d^2 -> table position
         const float hres = 0.5f * p.res;
         const float cull_ls2 = sd.cull_ls2;
         const int nsb = ts.nsbx * ts.nsby * (ts.tz / 2);
         if (it.sc != table_scene) {
-            for (int i = threadIdx.x; i < kKernelTab; i += kEvThreads) S.ktab[i] = A.ktab[it.sc * kKernelTab + i];
+            for (int i = threadIdx.x; i < kKernelTabEntries; i += kEvThreads)
+                S.ktab[i] = A.ktab[it.sc * kKernelTabEntries + i];
             table_scene = it.sc;
         }
         for (int r = threadIdx.x; r < it.nr; r += kEvThreads) {
@@ -758,7 +763,9 @@ __global__ void __launch_bounds__(kEvThreads, MINB) k_bgki(EvArgs A) {
             const float dx = L.x - L.ox, dy = L.y - L.oy, dz = L.z - L.oz;  // exact (nearby floats)
             const float ls2c = L.c >= 0 ? ls2 : -1.0f;  // cells outside the grid take no evidence
             const double ox = L.ox, oy = L.oy, oz = L.oz;
-            long long ao = 0, af = 0;  // sums of kernel values rounded to integer units
+            // sums of kernel values rounded to integer units; the unsigned conversion saturates a
+            // negative table value (the kernel's max(0, .)) to 0
+            unsigned long long ao = 0, af = 0;
             for (int g0 = 0; g0 < nr; g0 += 32) {
                 const int r = g0 + lane;
                 bool hit = false, near = false;
@@ -782,13 +789,13 @@ __global__ void __launch_bounds__(kEvThreads, MINB) k_bgki(EvArgs A) {
                     const float vx = s2.x + dx, vy = s2.y + dy, vz = s2.z + dz;
                     const float d2o = vx * vx + vy * vy + vz * vz;
                     if (d2o < ls2c) {
-                        ao += __float2ll_rn(fmaxf(kernel_tab(S.ktab, d2o * inv_ls2), 0.0f));
+                        ao += __float2ull_rn(kernel_tab(S.ktab, d2o * tscale));
                         ++nev;
                     }
                     float dpar;
                     const float d2f = free_d2(s0, s1, dx, dy, dz, &dpar);
                     if (s2.w + dpar < 0.0f && d2f < ls2c) {  // d_proj < d_m
-                        af += __float2ll_rn(fmaxf(kernel_tab(S.ktab, d2f * inv_ls2), 0.0f));
+                        af += __float2ull_rn(kernel_tab(S.ktab, d2f * tscale));
                         ++nev;
                     }
                 }
@@ -797,7 +804,7 @@ __global__ void __launch_bounds__(kEvThreads, MINB) k_bgki(EvArgs A) {
                     float dpar;
                     const float d2f = free_d2(S.stage[wid][j][0], S.stage[wid][j][1], dx, dy, dz, &dpar);
                     if (d2f < ls2c) {
-                        af += __float2ll_rn(fmaxf(kernel_tab(S.ktab, d2f * inv_ls2), 0.0f));
+                        af += __float2ull_rn(kernel_tab(S.ktab, d2f * tscale));
                         ++nev;
                     }
                 }
@@ -805,9 +812,8 @@ __global__ void __launch_bounds__(kEvThreads, MINB) k_bgki(EvArgs A) {
             }
             if (L.c >= 0) {
                 unsigned long long* ac = A.acc + 2 * (long)(coff + L.c);
-                const long long io = ao, jf = af;
-                if (io) atomicAdd(ac, (unsigned long long)io);
-                if (jf) atomicAdd(ac + 1, (unsigned long long)jf);
+                if (ao) atomicAdd(ac, ao);
+                if (af) atomicAdd(ac + 1, af);
             }
         }
         __threadfence();
@@ -1163,6 +1169,7 @@ static void build_table(double (*fn)(double), double scale, float4* out) {
         const double c3 = -4.5 * y[0] + 13.5 * y[1] - 13.5 * y[2] + 4.5 * y[3];
         out[i] = make_float4((float)c0, (float)c1, (float)c2, (float)c3);
     }
+    out[kKernelTab] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
 }
 
 void build_calib_tables(float4* f_tab, float4* dls_tab) {
@@ -1172,14 +1179,14 @@ void build_calib_tables(float4* f_tab, float4* dls_tab) {
 
 // Shared memory of k_bgki_sums (dynamic, sized by the work item's ray count).
 struct CalibSmem {
-    float4* ftab;            // [kKernelTab] unit kernel f, fixed-point scale folded in
-    float4* htab;            // [kKernelTab] -x f'(x), same scale
+    float4* ftab;            // [kKernelTabEntries] unit kernel f, fixed-point scale folded in
+    float4* htab;            // [kKernelTabEntries] -x f'(x), same scale
     float4 (*stage)[32][3];  // [kEvWarps][32][3]
     float4* a;               // [chunk]
     double4* c;              // [chunk]
 };
 
-constexpr size_t kCalibFixedBytes = 2 * sizeof(float4) * kKernelTab + sizeof(float4) * kEvWarps * 32 * 3;
+constexpr size_t kCalibFixedBytes = 2 * sizeof(float4) * kKernelTabEntries + sizeof(float4) * kEvWarps * 32 * 3;
 
 inline size_t calib_smem_bytes(int chunk) {
     return ((kCalibFixedBytes + 31) & ~(size_t)31) + (size_t)chunk * (sizeof(float4) + sizeof(double4));
@@ -1188,8 +1195,8 @@ inline size_t calib_smem_bytes(int chunk) {
 __device__ __forceinline__ CalibSmem calib_smem(unsigned char* base, int chunk) {
     CalibSmem S;
     S.ftab = reinterpret_cast<float4*>(base);
-    S.htab = S.ftab + kKernelTab;
-    S.stage = reinterpret_cast<float4(*)[32][3]>(base + 2 * sizeof(float4) * kKernelTab);
+    S.htab = S.ftab + kKernelTabEntries;
+    S.stage = reinterpret_cast<float4(*)[32][3]>(base + 2 * sizeof(float4) * kKernelTabEntries);
     const size_t off = (kCalibFixedBytes + 31) & ~(size_t)31;
     S.c = reinterpret_cast<double4*>(base + off);
     S.a = reinterpret_cast<float4*>(base + off + sizeof(double4) * (size_t)chunk);
@@ -1210,7 +1217,7 @@ __global__ void __launch_bounds__(kEvThreads, MINB) k_bgki_sums(EvArgs A, const 
     const unsigned lanes_below = (1u << lane) - 1u;
     const Batch& bt = A.bt;
     const uint32_t total_items = A.item_off[bt.T];
-    for (int i = threadIdx.x; i < kKernelTab; i += kEvThreads) {
+    for (int i = threadIdx.x; i < kKernelTabEntries; i += kEvThreads) {
         S.ftab[i] = A.ktab[i];
         S.htab[i] = htab[i];
     }
@@ -1229,7 +1236,7 @@ __global__ void __launch_bounds__(kEvThreads, MINB) k_bgki_sums(EvArgs A, const 
         const FrameParams fp = bt.fp[it.sc];
         const int coff = bt.off->cell[it.sc];
         const float ls2 = p.ls * p.ls;
-        const float inv_ls2 = 1.0f / ls2;
+        const float tscale = (1.0f / ls2) * (float)kKernelTab;  // d^2 -> table position
         const float hres = 0.5f * p.res;
         const float cull_ls2 = sd.cull_ls2;
         const int nsb = ts.nsbx * ts.nsby * (ts.tz / 2);
@@ -1271,14 +1278,14 @@ __global__ void __launch_bounds__(kEvThreads, MINB) k_bgki_sums(EvArgs A, const 
                     const float vx = s2.x + dx, vy = s2.y + dy, vz = s2.z + dz;
                     const float d2o = vx * vx + vy * vy + vz * vz;
                     if (d2o < ls2c) {
-                        const TabPos q = tab_pos(d2o * inv_ls2);
+                        const TabPos q = tab_pos(d2o * tscale);
                         fo += __float2ll_rn(fmaxf(tab_eval(S.ftab, q), 0.0f));
                         ho += __float2ll_rn(tab_eval(S.htab, q));
                     }
                     float dpar;
                     const float d2f = free_d2(s0, s1, dx, dy, dz, &dpar);
                     if (s2.w + dpar < 0.0f && d2f < ls2c) {
-                        const TabPos q = tab_pos(d2f * inv_ls2);
+                        const TabPos q = tab_pos(d2f * tscale);
                         ff += __float2ll_rn(fmaxf(tab_eval(S.ftab, q), 0.0f));
                         hf += __float2ll_rn(tab_eval(S.htab, q));
                     }
@@ -1287,7 +1294,7 @@ __global__ void __launch_bounds__(kEvThreads, MINB) k_bgki_sums(EvArgs A, const 
                     float dpar;
                     const float d2f = free_d2(S.stage[wid][j][0], S.stage[wid][j][1], dx, dy, dz, &dpar);
                     if (d2f < ls2c) {
-                        const TabPos q = tab_pos(d2f * inv_ls2);
+                        const TabPos q = tab_pos(d2f * tscale);
                         ff += __float2ll_rn(fmaxf(tab_eval(S.ftab, q), 0.0f));
                         hf += __float2ll_rn(tab_eval(S.htab, q));
                     }

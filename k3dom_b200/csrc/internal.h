@@ -140,9 +140,10 @@ cudaError_t launch_ds_evidence(const Batch& bt, RayBuffers& rb, CellState cs, Ce
 int bgki_blocks_per_sm();
 long ds_count_bytes(long items);
 cudaError_t evidence_init();
-// Host: the sparse-kernel table (512 float4) for sigma, every value multiplied by scale.
+// Host: the sparse-kernel table for sigma, every value multiplied by scale: 512 intervals and a
+// zero entry at u = 1 (513 float4), so an index taken at the support's edge needs no clamp.
 void build_kernel_table(float sigma, double scale, float4* out);
-constexpr int kKernelTableSize = 512;
+constexpr int kKernelTableSize = 513;
 // Calibration: unit-amplitude kernel and -x f'(x) tables scaled to units of 2^-kCalibShift.
 constexpr int kCalibShift = 40;
 void build_calib_tables(float4* f_tab, float4* dls_tab);
