@@ -273,7 +273,8 @@ typedef struct k3dom_stage_times {
 k3dom_status k3dom_get_stage_times(k3dom_handle* h, k3dom_stage_times* out);
 k3dom_status k3dom_set_timing(k3dom_handle* h, int enabled);
 
-/* Diagnostics collected on the device: points skipped as non-finite, list overflow. */
+/* Diagnostics collected on the device for the last frame: points skipped as non-finite (device
+ * scans; host scans with such points are refused), ray-list use, work items, evaluations. */
 typedef struct k3dom_diagnostics {
     int64_t nonfinite_points, ray_list_entries, ray_list_capacity, work_items;
     int32_t overflow;

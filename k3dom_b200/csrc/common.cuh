@@ -109,7 +109,7 @@ struct DevStatus {
     unsigned int overflow;
     unsigned int work_counter;  // dynamic work queue of the evidence kernels
     unsigned int work_counter2;
-    unsigned int pad;
+    unsigned int nonfinite_frame;  // points skipped as non-finite in the last frame's binning
     unsigned long long kernel_evals;  // in-support sparse-kernel evaluations of the last frame
 };
 

@@ -1742,7 +1742,7 @@ k3dom_status k3dom_get_diagnostics(k3dom_handle* h, k3dom_diagnostics* out) {
     cudaError_t e = cudaStreamSynchronize(h->st);
     if (e == cudaSuccess) e = cudaMemcpy(&st, h->status, sizeof(st), cudaMemcpyDeviceToHost);
     if (e != cudaSuccess) return h->fail(e);
-    out->nonfinite_points = (int64_t)st.nonfinite_points;
+    out->nonfinite_points = (int64_t)st.nonfinite_frame;
     out->ray_list_entries = (int64_t)st.ray_entries;
     out->ray_list_capacity = h->rb.capacity;
     out->work_items = (int64_t)st.work_items;

@@ -300,6 +300,9 @@ __global__ void k_finish_lists(const uint32_t* __restrict__ item_off, int T, Dev
                                const uint32_t* __restrict__ total) {
     status->work_items = item_off[T];
     status->ray_entries = total[0];
+    // k_ray_count has finished counting this frame's non-finite points: keep the frame's count
+    status->nonfinite_frame = (unsigned int)status->nonfinite_points;
+    status->nonfinite_points = 0;
     status->work_counter = 0;
     status->work_counter2 = 0;
     status->kernel_evals = 0;

@@ -109,3 +109,31 @@ def test_nonfinite_host_scan_is_refused_without_side_effects(pinned):
     finally:
         a.close()
         b.close()
+
+
+def test_nonfinite_device_points_are_skipped_per_frame():
+    """Device scans may hold non-finite coordinates: those points are skipped (they take no
+    evidence, as in the reference, whose comparisons with NaN fail) and counted for the frame.
+    The frame equals the same scan without them."""
+    cfg = scene.small(seed=31, G=32, Gz=8, res=0.2, P=8192, B=2048, n_points=1500)
+    p = K.make_params("k3dom", **cfg.params)
+    a, b = K.DOM(p), K.DOM(p)
+    try:
+        for f in range(3):
+            t = 0.1 + 0.1 * f
+            s, pts = cfg.scene.scan(f, t, cfg.n_points)
+            pts = np.ascontiguousarray(pts, np.float32)
+            bad = pts.copy()
+            bad[[5, 500, 1000], [0, 1, 2]] = [np.nan, np.inf, -np.inf]
+            keep = np.ones(len(pts), bool)
+            keep[[5, 500, 1000]] = False
+            a.updatePose(*s)
+            a.updateGrid(t, torch.from_numpy(bad if f == 1 else pts).to("cuda:0"))
+            b.updatePose(*s)
+            b.updateGrid(t, torch.from_numpy(pts[keep] if f == 1 else pts).to("cuda:0"))
+            assert a.diagnostics()["nonfinite_points"] == (3 if f == 1 else 0)
+            for fld in FIELDS:
+                np.testing.assert_array_equal(a.get_cell_field(fld), b.get_cell_field(fld), err_msg=f"{f} {fld}")
+    finally:
+        a.close()
+        b.close()
