@@ -333,8 +333,16 @@ void fill_scene_evidence(SceneDev& sd, bool ds, float4* ktab) {
         rsup = sqrtf(p.window_radius * p.window_radius + slack) + rsb + 1e-3f * p.res;
     }
     sd.cull_r2 = rsup * rsup;
-    // K3DOM box cull (stage_pair): the support radius with the same slack as rsup
-    const float rls = p.ls * (1.0f + 1e-4f) + 1e-3f * p.res;
+    // box culls (stage_pair, k_dsgrid): the support radius, or the DS window with the FP32 slack
+    // of the reference's neighbour test, plus the same margin as rsup
+    float rls;
+    if (!ds) {
+        rls = p.ls * (1.0f + 1e-4f) + 1e-3f * p.res;
+    } else {
+        const float ext = max_extent(p);
+        const float slack = 64.0f * 5.96e-8f * ext * ext;
+        rls = sqrtf(p.window_radius * p.window_radius + slack) + 1e-3f * p.res;
+    }
     sd.cull_ls2 = rls * rls;
     // fixed point: one kernel value is at most sigma -> at most 2^40 units, leaving 2^23 terms
     // of headroom in a signed 64-bit sum
@@ -978,10 +986,13 @@ constexpr int kMaxTileCells = 16 * 16 * 8;
 
 template <bool COUNT>
 __global__ void __launch_bounds__(kEvThreads) k_dsgrid(EvArgs A) {
-    __shared__ float4 sa[kChunk];
+    __shared__ float4 sa[kChunk];  // (m, |m|^2)
+    __shared__ float4 su[kChunk];  // (m / |m|, 0)
+    __shared__ uint8_t s_cand[kEvWarps][32];
     __shared__ uint32_t s_item;
     __shared__ int s_next_sb, s_last;
-    const int lane = threadIdx.x & 31;
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    const unsigned lanes_below = (1u << lane) - 1u;
     const Batch& bt = A.bt;
     const uint32_t total_items = A.item_off[bt.T];
     unsigned int* counter = COUNT ? &A.status->work_counter2 : &A.status->work_counter;
@@ -1012,7 +1023,11 @@ __global__ void __launch_bounds__(kEvThreads) k_dsgrid(EvArgs A) {
         for (int r = threadIdx.x; r < it.nr; r += kEvThreads) {
             uint32_t rid = A.evals[it.e0 + r];
             if (rid >= (uint32_t)bt.N) rid = 0;
-            sa[r] = A.ray_a[rid];
+            const float4 a = A.ray_a[rid];
+            sa[r] = a;
+            const float len = sqrtf(a.w);
+            const float inv = len > 0.0f ? 1.0f / len : 0.0f;
+            su[r] = make_float4(a.x * inv, a.y * inv, a.z * inv, 0.0f);
         }
         __syncthreads();
         const int nr = it.nr;
@@ -1042,19 +1057,21 @@ __global__ void __launch_bounds__(kEvThreads) k_dsgrid(EvArgs A) {
                     const int r = g0 + lane;
                     bool hit = false;
                     if (r < nr) {
-                        const float4 a = sa[r];
-                        // distance of the sub-block centre to the half-line through m
-                        const float len = sqrtf(a.w);
+                        // box bound on the distance from the half-line through m to the sub-block's
+                        // cell centres (the K3DOM cull's bound, with the window as the radius)
+                        const float4 u = su[r];
                         const float qx = L.ox - hres, qy = L.oy - hres, qz = L.oz - hres;
-                        const float tproj = fmaxf((qx * a.x + qy * a.y + qz * a.z) / len, 0.0f);
-                        const float ex = qx - tproj * a.x / len, ey = qy - tproj * a.y / len,
-                                    ez = qz - tproj * a.z / len;
-                        hit = ex * ex + ey * ey + ez * ez < sd.cull_r2;
+                        const float tproj = fmaxf(qx * u.x + qy * u.y + qz * u.z, 0.0f);
+                        const float Dx = qx - tproj * u.x, Dy = qy - tproj * u.y, Dz = qz - tproj * u.z;
+                        hit = box_reaches(Dx, Dy, Dz, Dx * Dx + Dy * Dy + Dz * Dz, hres, sd.cull_ls2);
                     }
-                    unsigned mask = __ballot_sync(0xffffffffu, hit);
-                    while (mask) {
-                        const int j = __ffs(mask) - 1;
-                        mask &= mask - 1;
+                    // candidates in input order (the first-100 rule counts them in that order)
+                    const unsigned mask = __ballot_sync(0xffffffffu, hit);
+                    if (hit) s_cand[wid][__popc(mask & lanes_below)] = (uint8_t)lane;
+                    __syncwarp();
+                    const int ncand = __popc(mask);
+                    for (int k = 0; k < ncand; ++k) {
+                        const int j = s_cand[wid][k];
                         const float4 a = sa[g0 + j];
                         if (nb < quota && ds_is_neighbor(L.x, L.y, L.z, acs, a, sd.wr2)) {
                             ++nb;
@@ -1066,6 +1083,7 @@ __global__ void __launch_bounds__(kEvThreads) k_dsgrid(EvArgs A) {
                             }
                         }
                     }
+                    __syncwarp();
                     if (!__any_sync(0xffffffffu, nb < quota)) break;
                 }
             }
