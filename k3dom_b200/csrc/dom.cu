@@ -121,7 +121,7 @@ struct k3dom_handle {
 
     Particles A{}, Ss{}, Bp{};
     uint32_t *sorted_keys = nullptr, *perm = nullptr, *alt_k = nullptr, *alt_v = nullptr;
-    SegRec* seg_rec = nullptr;  // piece sums of the segmented per-cell sums, one per 256 sorted slots
+    SegRec* seg_rec = nullptr;  // piece sums of the segmented per-cell sums, one per 128 sorted slots
     int2* res_br = nullptr;     // ancestor brackets of the resampling blocks
     uint32_t *hist = nullptr, *scan_tmp = nullptr;
     long hist_words = 0, scan_tmp_words = 0;

@@ -61,7 +61,7 @@ cudaError_t exact_scan_plan(const ExactTile* tiles, int nt, void* scratch, cudaS
 // particles.cu
 void launch_predict(const Batch& bt, Particles a, cudaStream_t st);
 void launch_shift_particles(int n, Particles a, int mx, int my, int mz, cudaStream_t st);
-// Piece sums of one 256-slot range of the sorted particles (gather + segmented sums): the
+// Piece sums of one 128-slot range of the sorted particles (gather + segmented sums): the
 // range's first piece when its cell began in an earlier range, and its last piece when its cell
 // continues into the next range.
 struct SegRec {

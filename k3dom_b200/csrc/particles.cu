@@ -20,8 +20,12 @@ using namespace k3dom_draws;
 // (src/common/kernel/ego_motion_compensation.cu:12-18) when a map shift is pending. Over all
 // scenes of the batch; the Philox item is the particle's index within its scene and the
 // stored cell index is the global one (scene cell offset + x + G y + G^2 z).
+// One particle per thread (no grid-stride loop): every particle's loads are independent of
+// another's stores, so the scheduler keeps many more of them in flight.
 __global__ void __launch_bounds__(kBlock) k_predict(Batch bt, Particles a) {
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < bt.P; i += gridDim.x * blockDim.x) {
+    {
+        const int i = blockIdx.x * blockDim.x + threadIdx.x;
+        if (i >= bt.P) return;
         const int sc = scene_of(bt.off->part, bt.S, i);
         const DevParams& p = bt.sc[sc].p;
         const FrameParams fp = bt.fp[sc];
@@ -73,7 +77,7 @@ __global__ void __launch_bounds__(kBlock) k_predict(Batch bt, Particles a) {
 void launch_predict(const Batch& bt, Particles a, cudaStream_t st) {
     if (bt.P <= 0) return;
     ++g_launches;
-    k_predict<<<grid_for(bt.P), kBlock, 0, st>>>(bt, a);
+    k_predict<<<div_up(bt.P, kBlock), kBlock, 0, st>>>(bt, a);
 }
 
 __global__ void k_shift_particles(int n, Particles a, int mx, int my, int mz) {
@@ -100,14 +104,14 @@ void launch_shift_particles(int n, Particles a, int mx, int my, int mz, cudaStre
 // (resampling.cu:13-36) is recorded as the sign bit of the sorted weight and applied at
 // resampling.
 //
-// Two levels. Each warp takes 256 sorted slots and finishes every cell whose particles lie in
+// Two levels. Each warp takes 128 sorted slots and finishes every cell whose particles lie in
 // its range (FP64 segmented scan over 32-slot chunks). For a cell that crosses range boundaries
 // it records the piece sums: the range's first piece (SegRec.lead) and its last piece
 // (SegRec.trail). k_seg_fixup then adds, for each cell whose head lies in a range, that range's
 // trail and the lead pieces of the following ranges up to the cell's end. Every sum is formed in
 // a fixed order, so it is deterministic, and no warp walks a long cell alone.
-constexpr int kSegItems = 8;                       // 32-wide chunks per warp range
-constexpr int kSegRange = 32 * kSegItems;          // 256 sorted particles per warp
+constexpr int kSegItems = 4;                       // 32-wide chunks per warp range
+constexpr int kSegRange = 32 * kSegItems;          // 128 sorted particles per warp
 constexpr int kSegWarps = kBlock / 32;
 
 long seg_rec_count(long P) { return P > 0 ? div_up(P, (long)kSegRange) : 1; }
