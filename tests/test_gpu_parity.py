@@ -330,7 +330,7 @@ def test_lockstep_config0_scale(variant):
 
 
 def test_lockstep_crowded_cells():
-    """Cells holding thousands of particles: their sums span many 256-slot ranges of the sorted
+    """Cells holding thousands of particles: their sums span many 128-slot ranges of the sorted
     set (range pieces combined by the fix-up pass), and ranges that lie wholly inside one cell or
     end exactly at a cell boundary. The steady frame checks the sorted set and cell ranges bit for
     bit and the masses built from the sums against the oracle."""
