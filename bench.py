@@ -359,6 +359,12 @@ def run_ours(args):
         rule_name = ["by-size", "8x8x4", "16x16x4", "16x16x8"][tuning["tile_rule"]]
         if rule_name == "by-size":
             rule_name = "16x16x8"  # the rule's choice for grids of >= 2^20 cells
+        issue = None
+        if tr_file.exists() and args.variant == "k3dom":
+            try:
+                issue = json.loads(tr_file.read_text()).get("issue")
+            except Exception:
+                issue = None
         if tr_file.exists() and args.variant == "k3dom":
             try:
                 per = json.loads(tr_file.read_text())["per_tiling"]
@@ -394,6 +400,9 @@ def run_ours(args):
                 "work": (f"{n_evals:.4g} accepted neighbours x {flop_per} FLOP per frame" if ds else
                          f"{n_evals:.4g} in-support kernel evaluations x {flop_per} FLOP per frame"),
                 "launch_ms": round(ev_ms, 4),
+                "note": ("SIMT-issue bound: frac counts only in-support evaluations x FLOP; the lanes outside "
+                         "a ray's support, the FP64 pair set-up and the fixed-point rounding are the rest"),
+                "ncu_issue": issue,
             },
             "roofline_hbm": {
                 "kernels": "particle stages (predict, sort, gather+sums, reweight, births, resampling)",
