@@ -358,6 +358,44 @@ def test_lockstep_crowded_cells():
         run.close()
 
 
+def test_config1_scale_tilings_agree_and_evidence_matches_oracle():
+    """config1 at full size (256 x 256 x 32 voxels, 4,194,304 particles, 120,000-point scans with
+    ego motion): two evidence tilings give bit-identical frames (the evidence is exact fixed
+    point), and the last frame's BGKI evidence matches the FP64 oracle within 1e-5 relative (the
+    lockstep bar, ties allowed as there)."""
+    cfg = scene.config1(seed=7)
+    p = K.make_params("k3dom", **cfg.params)
+    fields = ["free_mass", "static_mass", "dynamic_mass", "pers_mass", "born_mass", "mean_x_vel", "del_occ",
+              "del_free"]
+    doms = [K.DOM(p, "k3dom"), K.DOM(p, "k3dom")]
+    try:
+        pts = None
+        for f in range(3):
+            t = 0.1 + f * cfg.dt
+            s, pts = cfg.scene.scan(f, t, cfg.n_points)
+            for d in doms:
+                d.updatePose(*s)
+                d.updateGrid(t, pts)
+            if f == 0:
+                doms[0].set_tuning(2, 512)   # 16x16x4 tiles, 512 rays per work item
+                doms[1].set_tuning(3, 1024)  # 16x16x8 tiles, 1024 rays per work item
+        a, b = doms
+        for fld in fields:
+            assert np.array_equal(a.get_cell_field(fld), b.get_cell_field(fld), equal_nan=True), fld
+        i = a.info()
+        sensor_rel = np.array([i.sensor_x - i.center_x, i.sensor_y - i.center_y, i.sensor_z - i.center_z],
+                              np.float32)
+        ev = O.bgki(a.grid_size, a.grid_size_z, p.resolution, sensor_rel, p.ls, p.sigma, pts)
+        assert (ev["del_free"] > 0).sum() > 100000 and (ev["del_occ"] > 0).sum() > 10000
+        n, e = rel_ok(a.get_cell_field("del_free"), ev["del_free"], 1e-2 * p.sigma, allow=ev["tie_mass"] * 1.0001)
+        assert n == 0, ("del_free", n, e)
+        n, e = rel_ok(a.get_cell_field("del_occ"), ev["del_occ"], 1e-2 * p.sigma)
+        assert n == 0, ("del_occ", n, e)
+    finally:
+        for d in doms:
+            d.close()
+
+
 def test_draws_equal_oracle():
     for stage in (2, 3, 4):
         for frame in (0, 5):
