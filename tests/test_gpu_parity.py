@@ -396,6 +396,44 @@ def test_config1_scale_tilings_agree_and_evidence_matches_oracle():
             d.close()
 
 
+def test_config1_scale_ds_tilings_agree_and_measurement_matches_oracle():
+    """The DS-PHD/MIB variant at config1's full size: two evidence tilings (and rays per work
+    item, which changes how the first-100 rule is split across chunks) give bit-identical frames,
+    and the last frame's measurement grid matches the oracle's FP32 neighbour sets (the lockstep
+    bars; cells whose pOcc comparisons are within 4 ulp of flipping are left out)."""
+    cfg = scene.config1(seed=7, variant="dsphdmib")
+    p = K.make_params("dsphdmib", **cfg.params)
+    fields = ["occ_mass", "free_mass", "pers_mass", "born_mass", "mean_x_vel", "meas_occ", "meas_free"]
+    doms = [K.DOM(p, "dsphdmib"), K.DOM(p, "dsphdmib")]
+    try:
+        pts = None
+        for f in range(3):
+            t = 0.1 + f * cfg.dt
+            s, pts = cfg.scene.scan(f, t, cfg.n_points)
+            for d in doms:
+                d.updatePose(*s)
+                d.updateGrid(t, pts)
+            if f == 0:
+                doms[0].set_tuning(2, 1024)
+                doms[1].set_tuning(1, 256)
+        a, b = doms
+        for fld in fields:
+            assert np.array_equal(a.get_cell_field(fld), b.get_cell_field(fld), equal_nan=True), fld
+        i = a.info()
+        sensor_rel = np.array([i.sensor_x - i.center_x, i.sensor_y - i.center_y, i.sensor_z - i.center_z],
+                              np.float32)
+        o = O.ds_measgrid(a.grid_size, a.grid_size_z, p.resolution, sensor_rel, p.max_range, p.meas_occ_stddev, pts)
+        ok = o["tie"] == 0
+        assert (o["meas_free"][ok] > 1e-5).sum() > 100000
+        mo, mf = a.get_cell_field("meas_occ"), a.get_cell_field("meas_free")
+        for mine, exp in ((mo, o["meas_occ"]), (mf, o["meas_free"])):
+            np.testing.assert_array_equal(mine[ok] <= 1e-5, exp[ok] <= 1e-5)
+            np.testing.assert_allclose(mine[ok], exp[ok], rtol=2.5e-7, atol=0)
+    finally:
+        for d in doms:
+            d.close()
+
+
 def test_draws_equal_oracle():
     for stage in (2, 3, 4):
         for frame in (0, 5):
