@@ -162,3 +162,33 @@ def test_batch_rejects_bad_arguments():
             batch.scene(0).updateGrid(0.1, np.zeros((3, 3), np.float32))
     finally:
         batch.close()
+
+
+def test_config3_batch_equals_separate_scenes():
+    """The batched benchmark workload at its own size: the 16 uneven config3 scenes (grids of
+    64-256 cells, 2^18-2^22 particles, 10k-200k points) stepped together by one BatchDOM give,
+    scene by scene, the bits that each scene gives alone."""
+    cfgs = scene.config3(seed=0)
+    assert len(cfgs) == 16
+    params = [K.make_params("k3dom", **c.params) for c in cfgs]
+    plain = [K.DOM(p, "k3dom") for p in params]
+    batch = K.BatchDOM(params, "k3dom")
+    try:
+        for f in range(3):
+            ts, pts = [], []
+            for s, (c, d) in enumerate(zip(cfgs, plain)):
+                t = 0.1 + f * c.dt
+                pose, p = c.scene.scan(f, t, c.n_points)
+                d.updatePose(*pose)
+                d.updateGrid(t, p)
+                batch.updatePose(s, *pose)
+                ts.append(t)
+                pts.append(p)
+            batch.update(ts, pts)
+        for s, d in enumerate(plain):
+            assert_same(snapshot(batch.scene(s)), snapshot(d), f"config3 scene {s}")
+            assert np.array_equal(batch.scene(s).ancestors(), d.ancestors()), f"ancestors scene {s}"
+    finally:
+        batch.close()
+        for d in plain:
+            d.close()
