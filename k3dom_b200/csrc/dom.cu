@@ -494,6 +494,18 @@ static bool nonfinite_any(const float* v, long m) {
     return bad != 0;
 }
 
+// Copy m floats and report whether any of them is non-finite, in one pass over the source.
+static bool copy_nonfinite_any(float* __restrict__ dst, const float* __restrict__ v, long m) {
+    uint32_t bad = 0;
+    for (long i = 0; i < m; ++i) {
+        uint32_t u;
+        std::memcpy(&u, v + i, sizeof(u));
+        std::memcpy(dst + i, &u, sizeof(u));
+        bad |= (uint32_t)((u & 0x7F800000u) == 0x7F800000u);
+    }
+    return bad != 0;
+}
+
 bool has_nonfinite_host(const float* xs, const float* ys, const float* zs, int n) {
     const bool inter = (ys == nullptr || zs == nullptr);
     if (inter) return nonfinite_any(xs, 3L * n);
@@ -529,12 +541,14 @@ static bool is_pinned_host(const void* p) {
 // of an interleaved host scan into device staging (straight from the caller's memory when it is
 // pinned and the call waits for the frame, so the caller cannot reuse the buffer while the copy
 // is pending; otherwise through pinned memory, whose previous use set_frame_params waited on);
-// the host's finiteness check runs while that copy is in flight. kPlace writes the planes:
-// de-interleaving on the device, or copies of separate x/y/z arrays.
+// the host's finiteness check runs while that copy is in flight, or during the copy into pinned
+// memory, which then sets *checked and *nonfinite. kPlace writes the planes: de-interleaving on
+// the device, or copies of separate x/y/z arrays.
 enum UploadPhase { kStage, kPlace };
 
 k3dom_status upload_points(k3dom_handle* h, int s, const float* xs, const float* ys, const float* zs, int n,
-                           k3dom_mem mem, bool sync, UploadPhase phase) {
+                           k3dom_mem mem, bool sync, UploadPhase phase, bool* checked = nullptr,
+                           bool* nonfinite = nullptr) {
     if (n == 0) return K3DOM_OK;
     const long N = h->N, o = h->off.point[s];
     float* dx = h->pts + o;
@@ -546,7 +560,9 @@ k3dom_status upload_points(k3dom_handle* h, int s, const float* xs, const float*
         if (phase == kStage) {
             const float* src = xs;
             if (!sync || !is_pinned_host(xs)) {
-                std::memcpy(h->pts_xyz_pinned + 3 * o, xs, 3 * n * sizeof(float));
+                const bool bad = copy_nonfinite_any(h->pts_xyz_pinned + 3 * o, xs, 3L * n);
+                if (checked) *checked = true;
+                if (nonfinite) *nonfinite = bad;
                 src = h->pts_xyz_pinned + 3 * o;
             }
             if ((e = cudaMemcpyAsync(h->pts_xyz + 3 * o, src, 3 * n * sizeof(float), cudaMemcpyHostToDevice,
@@ -587,12 +603,19 @@ k3dom_status upload_points(k3dom_handle* h, int s, const float* xs, const float*
 k3dom_status upload_all(k3dom_handle* h, const float* const* xs, const float* const* ys, const float* const* zs,
                         const int32_t* n, k3dom_mem mem, bool sync, bool check) {
     k3dom_status st;
-    for (int s = 0; s < h->S; ++s)
-        if ((st = upload_points(h, s, xs[s], ys ? ys[s] : nullptr, zs ? zs[s] : nullptr, n[s], mem, sync, kStage)))
+    std::vector<char> checked(h->S, 0);
+    for (int s = 0; s < h->S; ++s) {
+        bool done = false, bad = false;
+        if ((st = upload_points(h, s, xs[s], ys ? ys[s] : nullptr, zs ? zs[s] : nullptr, n[s], mem, sync, kStage,
+                                &done, &bad)))
             return st;
+        if (check && bad) return K3DOM_ERR_INVALID_INPUT;
+        checked[s] = done;
+    }
     if (check && mem == K3DOM_MEM_HOST)
         for (int s = 0; s < h->S; ++s)
-            if (n[s] > 0 && has_nonfinite_host(xs[s], ys ? ys[s] : nullptr, zs ? zs[s] : nullptr, n[s]))
+            if (n[s] > 0 && !checked[s] &&
+                has_nonfinite_host(xs[s], ys ? ys[s] : nullptr, zs ? zs[s] : nullptr, n[s]))
                 return K3DOM_ERR_INVALID_INPUT;
     for (int s = 0; s < h->S; ++s)
         if ((st = upload_points(h, s, xs[s], ys ? ys[s] : nullptr, zs ? zs[s] : nullptr, n[s], mem, sync, kPlace)))
