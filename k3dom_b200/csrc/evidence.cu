@@ -444,6 +444,45 @@ __device__ __forceinline__ CellLoc locate(const DevParams& p, const TileShape& t
     return L;
 }
 
+// Sub-blocks go to the warps nearest to the sensor first. A sub-block's work grows with the rays
+// that pass it, which is largest on the tile's sensor side (rays that end inside the tile never
+// reach its far side, and near the sensor every ray passes close), so the costly sub-blocks start
+// first and the cheap ones fill the end of the work item, where warps that run out of sub-blocks
+// wait at the item's barrier. The sums are exact, so the order changes no result.
+constexpr int kMaxOrderedSb = 64;  // the largest tiling (16x16x8) has 64 sub-blocks
+
+struct SbOrder {
+    float key[kMaxOrderedSb];
+    uint8_t idx[kMaxOrderedSb];
+};
+
+// Phase 1 (thread i < nsb): squared distance of sub-block i's anchor from the sensor.
+__device__ __forceinline__ void sb_order_keys(SbOrder& o, const DevParams& p, const TileShape& ts, int t, int nsb,
+                                              float sx, float sy, float sz) {
+    const int i = threadIdx.x;
+    if (nsb > kMaxOrderedSb || i >= nsb) return;
+    const int tx = t % ts.ntx, ty = (t / ts.ntx) % ts.nty, tz = t / (ts.ntx * ts.nty);
+    const int sbx = i % ts.nsbx, sby = (i / ts.nsbx) % ts.nsby, sbz = i / (ts.nsbx * ts.nsby);
+    float x, y, z;
+    centre_xyz(tx * ts.tx + sbx * 4 + 2, ty * ts.ty + sby * 4 + 2, tz * ts.tz + sbz * 2 + 1, p, sx, sy, sz, &x, &y, &z);
+    o.key[i] = x * x + y * y + z * z;
+}
+
+// Phase 2, after a barrier: sub-block i's place in the order (ties by index).
+__device__ __forceinline__ void sb_order_rank(SbOrder& o, int nsb) {
+    const int i = threadIdx.x;
+    if (nsb > kMaxOrderedSb || i >= nsb) return;
+    const float k = o.key[i];
+    int r = 0;
+    for (int j = 0; j < nsb; ++j) {
+        const float kj = o.key[j];
+        r += (kj < k) || (kj == k && j < i);
+    }
+    o.idx[r] = (uint8_t)i;
+}
+
+__device__ __forceinline__ int sb_at(const SbOrder& o, int n, int nsb) { return nsb > kMaxOrderedSb ? n : o.idx[n]; }
+
 // The work item a CTA holds: its tile (global and scene-local), scene and ray range.
 struct Item {
     int t, lt, sc;
@@ -726,6 +765,7 @@ __global__ void __launch_bounds__(kEvThreads, MINB) k_bgki(EvArgs A) {
     const BgkiSmem S = bgki_smem(smem_raw, A.chunk);
     __shared__ uint32_t s_item;
     __shared__ int s_next_sb, s_last;
+    __shared__ SbOrder s_order;
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
     const unsigned lanes_below = (1u << lane) - 1u;
     const Batch& bt = A.bt;
@@ -763,6 +803,9 @@ __global__ void __launch_bounds__(kEvThreads, MINB) k_bgki(EvArgs A) {
             S.a[r] = A.ray_a[rid];
             S.c[r] = A.ray_c[rid];
         }
+        sb_order_keys(s_order, p, ts, it.lt, nsb, fp.sensor_x, fp.sensor_y, fp.sensor_z);
+        __syncthreads();
+        sb_order_rank(s_order, nsb);
         __syncthreads();
         const int nr = it.nr;
         for (;;) {
@@ -770,6 +813,7 @@ __global__ void __launch_bounds__(kEvThreads, MINB) k_bgki(EvArgs A) {
             if (lane == 0) sb = atomicAdd(&s_next_sb, 1);
             sb = __shfl_sync(0xffffffffu, sb, 0);
             if (sb >= nsb) break;
+            sb = sb_at(s_order, sb, nsb);
             const CellLoc L = locate(p, ts, it.lt, sb, lane, fp.sensor_x, fp.sensor_y, fp.sensor_z);
             const float dx = L.x - L.ox, dy = L.y - L.oy, dz = L.z - L.oz;  // exact (nearby floats)
             const float ls2c = L.c >= 0 ? ls2 : -1.0f;  // cells outside the grid take no evidence
@@ -991,6 +1035,7 @@ __global__ void __launch_bounds__(kEvThreads) k_dsgrid(EvArgs A) {
     __shared__ uint8_t s_cand[kEvWarps][32];
     __shared__ uint32_t s_item;
     __shared__ int s_next_sb, s_last;
+    __shared__ SbOrder s_order;
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
     const unsigned lanes_below = (1u << lane) - 1u;
     const Batch& bt = A.bt;
@@ -1029,6 +1074,9 @@ __global__ void __launch_bounds__(kEvThreads) k_dsgrid(EvArgs A) {
             const float inv = len > 0.0f ? 1.0f / len : 0.0f;
             su[r] = make_float4(a.x * inv, a.y * inv, a.z * inv, 0.0f);
         }
+        sb_order_keys(s_order, p, ts, it.lt, nsb, fp.sensor_x, fp.sensor_y, fp.sensor_z);
+        __syncthreads();
+        sb_order_rank(s_order, nsb);
         __syncthreads();
         const int nr = it.nr;
         for (;;) {
@@ -1036,6 +1084,7 @@ __global__ void __launch_bounds__(kEvThreads) k_dsgrid(EvArgs A) {
             if (lane == 0) sb = atomicAdd(&s_next_sb, 1);
             sb = __shfl_sync(0xffffffffu, sb, 0);
             if (sb >= nsb) break;
+            sb = sb_at(s_order, sb, nsb);
             const CellLoc L = locate(p, ts, it.lt, sb, lane, fp.sensor_x, fp.sensor_y, fp.sensor_z);
             const float acs = __fadd_rn(__fadd_rn(__fmul_rn(L.x, L.x), __fmul_rn(L.y, L.y)), __fmul_rn(L.z, L.z));
             int quota = kDsMaxNeighbors;
@@ -1234,6 +1283,7 @@ __global__ void __launch_bounds__(kEvThreads, MINB) k_bgki_sums(EvArgs A, const 
     const CalibSmem S = calib_smem(smem_raw, A.chunk);
     __shared__ uint32_t s_item;
     __shared__ int s_next_sb;
+    __shared__ SbOrder s_order;
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
     const unsigned lanes_below = (1u << lane) - 1u;
     const Batch& bt = A.bt;
@@ -1267,6 +1317,9 @@ __global__ void __launch_bounds__(kEvThreads, MINB) k_bgki_sums(EvArgs A, const 
             S.a[r] = A.ray_a[rid];
             S.c[r] = A.ray_c[rid];
         }
+        sb_order_keys(s_order, p, ts, it.lt, nsb, fp.sensor_x, fp.sensor_y, fp.sensor_z);
+        __syncthreads();
+        sb_order_rank(s_order, nsb);
         __syncthreads();
         const int nr = it.nr;
         for (;;) {
@@ -1274,6 +1327,7 @@ __global__ void __launch_bounds__(kEvThreads, MINB) k_bgki_sums(EvArgs A, const 
             if (lane == 0) sb = atomicAdd(&s_next_sb, 1);
             sb = __shfl_sync(0xffffffffu, sb, 0);
             if (sb >= nsb) break;
+            sb = sb_at(s_order, sb, nsb);
             const CellLoc L = locate(p, ts, it.lt, sb, lane, fp.sensor_x, fp.sensor_y, fp.sensor_z);
             const float dx = L.x - L.ox, dy = L.y - L.oy, dz = L.z - L.oz;
             const float ls2c = L.c >= 0 ? ls2 : -1.0f;
