@@ -520,7 +520,7 @@ cudaError_t alloc_ray_lane(k3dom_calib* c, RayBuffers& rb, int max_points, long 
     const int N = std::max(max_points, 1);
     long cap = std::min(need + need / 4, 0xFFFFFFF0L);
     rb.capacity = cap;
-    rb.chunk = 512;
+    rb.chunk = kCalibChunk;
     std::vector<void*>* L = &c->ray_allocs;
     cudaError_t e;
     if ((e = c->alloc(&rb.ray_a, N, L)) || (e = c->alloc(&rb.ray_c, N, L)) || (e = c->alloc(&rb.counts, N, L)) ||

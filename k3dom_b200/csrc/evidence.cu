@@ -44,6 +44,8 @@ constexpr int kKernelTabEntries = kKernelTab + 1;  // + a zero entry at u = 1
 static_assert(kKernelTabEntries == kKernelTableSize, "kernel table size");
 constexpr int kEvThreads = 256;
 constexpr int kEvWarps = kEvThreads / 32;
+constexpr int kSmallChunk = 256;  // items up to this many rays run in CTAs of kSmallWarps warps
+constexpr int kSmallWarps = 4;
 constexpr int kDsMaxNeighbors = 100;  // measurement_grid.cu:87
 
 // ================================================================ binning
@@ -670,25 +672,119 @@ __device__ void k3dom_cell_update(const DevParams& p, double g, int c, double de
 // (dynamic, sized by the work item's ray count so that smaller chunks leave room for more CTAs)
 struct BgkiSmem {
     float4* ktab;                 // [kKernelTabEntries] sparse-kernel table of the current scene
-    float4 (*stage)[32][3];       // [kEvWarps][32][3]
+    float4 (*stage)[32][3];       // [warps][32][3]
     float4* a;                    // [chunk] m.x, m.y, m.z, d_m
     double4* c;                   // [chunk] d_m, margin, 1/d_m
+    uint16_t* reg;                // [kRegions][chunk] rays per region of a 16x16 tile (region builds)
 };
 
-constexpr size_t kBgkiFixedBytes = sizeof(float4) * kKernelTabEntries + sizeof(float4) * kEvWarps * 32 * 3;
+// A 16x16-cell tile splits into kRegions columns of 8x8 cells (full tile height); a ray's region
+// list holds it when its segment meets the column's cell-centre box grown by the binning radius
+// (plus a quarter cell), the test that put it in the tile's list, so every ray that can reach a
+// cell of the column is in the column's list. Sub-blocks then cull only their column's rays.
+constexpr int kRegions = 4;
 
-inline size_t bgki_smem_bytes(int chunk) {
-    return ((kBgkiFixedBytes + 31) & ~(size_t)31) + (size_t)chunk * (sizeof(float4) + sizeof(double4));
+__host__ __device__ constexpr size_t bgki_fixed_bytes(int warps) {
+    return ((sizeof(float4) * kKernelTabEntries + sizeof(float4) * (size_t)warps * 32 * 3) + 31) & ~(size_t)31;
 }
 
-__device__ __forceinline__ BgkiSmem bgki_smem(unsigned char* base, int chunk) {
+inline size_t bgki_smem_bytes(int chunk, int warps = kEvWarps, bool regions = false) {
+    return bgki_fixed_bytes(warps) + (size_t)chunk * (sizeof(float4) + sizeof(double4)) +
+           (regions ? (size_t)kRegions * chunk * sizeof(uint16_t) : 0);
+}
+
+__device__ __forceinline__ BgkiSmem bgki_smem(unsigned char* base, int chunk, int warps) {
     BgkiSmem S;
     S.ktab = reinterpret_cast<float4*>(base);
     S.stage = reinterpret_cast<float4(*)[32][3]>(base + sizeof(float4) * kKernelTabEntries);
-    const size_t off = (kBgkiFixedBytes + 31) & ~(size_t)31;
+    const size_t off = bgki_fixed_bytes(warps);
     S.c = reinterpret_cast<double4*>(base + off);  // 32-byte aligned
     S.a = reinterpret_cast<float4*>(base + off + sizeof(double4) * (size_t)chunk);
+    S.reg = reinterpret_cast<uint16_t*>(base + off + (sizeof(double4) + sizeof(float4)) * (size_t)chunk);
     return S;
+}
+
+// Parameter interval [t0, t1] of a + t d inside the slab lo <= u <= hi (empty when t0 > t1).
+__device__ __forceinline__ void slab(float a, float d, float lo, float hi, float* t0, float* t1) {
+    if (d == 0.0f) {
+        const bool in = a >= lo && a <= hi;
+        *t0 = in ? -INFINITY : INFINITY;
+        *t1 = in ? INFINITY : -INFINITY;
+        return;
+    }
+    const float inv = 1.0f / d;
+    const float e0 = (lo - a) * inv, e1 = (hi - a) * inv;
+    *t0 = fminf(e0, e1);
+    *t1 = fmaxf(e0, e1);
+}
+
+// Bit q (q = qx + 2 qy) set when the ray's segment (sensor a -> a + m/res, cell-index space)
+// meets region q's box [x0 + 8 qx, x0 + 8 qx + 7] x [y0 + 8 qy, +7] x [z0, z0 + tz - 1] grown by R.
+__device__ __forceinline__ unsigned region_mask(float ax, float ay, float az, float4 m, float inv_res, float x0,
+                                                float y0, float z0, int tz, float R) {
+    const float dx = m.x * inv_res, dy = m.y * inv_res, dz = m.z * inv_res;
+    float zl, zh;
+    slab(az, dz, z0 - R, z0 + (float)(tz - 1) + R, &zl, &zh);
+    zl = fmaxf(zl, 0.0f);
+    zh = fminf(zh, 1.0f);
+    float xl[2], xh[2], yl[2], yh[2];
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+        slab(ax, dx, x0 + 8.0f * h - R, x0 + 8.0f * h + 7.0f + R, &xl[h], &xh[h]);
+        slab(ay, dy, y0 + 8.0f * h - R, y0 + 8.0f * h + 7.0f + R, &yl[h], &yh[h]);
+    }
+    unsigned q = 0;
+#pragma unroll
+    for (int qy = 0; qy < 2; ++qy)
+#pragma unroll
+        for (int qx = 0; qx < 2; ++qx)
+            if (fmaxf(zl, fmaxf(xl[qx], yl[qy])) <= fminf(zh, fminf(xh[qx], yh[qy]))) q |= 1u << (qx + 2 * qy);
+    return q;
+}
+
+// Stages the item's rays (m, d_m) and FP64 constants in shared memory and, for a 16x16 tile,
+// appends each ray to the lists of the regions it reaches (rcnt zeroed before the call; list
+// order is arbitrary, the sums are exact). Every thread of the block calls it.
+template <int THREADS>
+__device__ __forceinline__ void stage_item_rays(const EvArgs& A, const Item& it, const SceneDev& sd,
+                                                const FrameParams& fp, bool regions, float4* sa, double4* sc,
+                                                uint16_t* reg, int* rcnt) {
+    const DevParams& p = sd.p;
+    const TileShape& ts = sd.ts;
+    const int lane = threadIdx.x & 31;
+    const unsigned lanes_below = (1u << lane) - 1u;
+    BinGeom g;
+    place_sensor(g, p, fp);
+    const float x0 = (float)(it.lt % ts.ntx * 16), y0 = (float)((it.lt / ts.ntx) % ts.nty * 16);
+    const float z0 = (float)(it.lt / (ts.ntx * ts.nty) * ts.tz);
+    for (int r0 = 0; r0 < it.nr; r0 += THREADS) {  // uniform trip count: the ballots below
+        const int r = r0 + (int)threadIdx.x;
+        unsigned qm = 0;
+        if (r < it.nr) {
+            uint32_t rid = A.evals[it.e0 + r];
+            if (rid >= (uint32_t)A.bt.N) rid = 0;  // defensive: never read past the ray arrays
+            const float4 a4 = A.ray_a[rid];
+            sa[r] = a4;
+            sc[r] = A.ray_c[rid];
+            if (regions) qm = region_mask(g.ax, g.ay, g.az, a4, 1.0f / p.res, x0, y0, z0, ts.tz, sd.bin_R + 0.25f);
+        }
+        if (regions) {
+#pragma unroll
+            for (int q = 0; q < kRegions; ++q) {
+                const unsigned b = __ballot_sync(0xffffffffu, (qm >> q) & 1u);
+                if (!b) continue;
+                int base = 0;
+                if (lane == 0) base = atomicAdd(&rcnt[q], __popc(b));
+                base = __shfl_sync(0xffffffffu, base, 0);
+                if ((qm >> q) & 1u) reg[q * A.chunk + base + __popc(b & lanes_below)] = (uint16_t)r;
+            }
+        }
+    }
+}
+
+// Region of sub-block sb in a 16x16 tile (4x4 sub-blocks per layer).
+__device__ __forceinline__ int sb_region(const TileShape& ts, int sb) {
+    return ((sb % ts.nsbx) >> 1) + 2 * (((sb / ts.nsbx) % ts.nsby) >> 1);
 }
 
 // Pair geometry. For the anchor o of a sub-block and a ray m (FP64, once per lane-ray):
@@ -759,13 +855,14 @@ __device__ __forceinline__ float free_d2(const float4& st0, const float4& st1, f
     return qx * qx + qy * qy + qz * qz + al * al;
 }
 
-template <int MINB>
-__global__ void __launch_bounds__(kEvThreads, MINB) k_bgki(EvArgs A) {
+template <int MINB, int THREADS = kEvThreads, bool REGIONS = false>
+__global__ void __launch_bounds__(THREADS, MINB) k_bgki(EvArgs A) {
     extern __shared__ __align__(32) unsigned char smem_raw[];
-    const BgkiSmem S = bgki_smem(smem_raw, A.chunk);
+    const BgkiSmem S = bgki_smem(smem_raw, A.chunk, THREADS / 32);
     __shared__ uint32_t s_item;
     __shared__ int s_next_sb, s_last;
     __shared__ SbOrder s_order;
+    __shared__ int s_rcnt[kRegions];
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
     const unsigned lanes_below = (1u << lane) - 1u;
     const Batch& bt = A.bt;
@@ -778,6 +875,7 @@ __global__ void __launch_bounds__(kEvThreads, MINB) k_bgki(EvArgs A) {
             s_item = atomicAdd(&A.status->work_counter, 1u);
             s_next_sb = 0;
         }
+        if (REGIONS && threadIdx.x < kRegions) s_rcnt[threadIdx.x] = 0;
         __syncthreads();
         const uint32_t item = s_item;
         if (item >= total_items) break;
@@ -793,16 +891,12 @@ __global__ void __launch_bounds__(kEvThreads, MINB) k_bgki(EvArgs A) {
         const float cull_ls2 = sd.cull_ls2;
         const int nsb = ts.nsbx * ts.nsby * (ts.tz / 2);
         if (it.sc != table_scene) {
-            for (int i = threadIdx.x; i < kKernelTabEntries; i += kEvThreads)
+            for (int i = threadIdx.x; i < kKernelTabEntries; i += THREADS)
                 S.ktab[i] = A.ktab[it.sc * kKernelTabEntries + i];
             table_scene = it.sc;
         }
-        for (int r = threadIdx.x; r < it.nr; r += kEvThreads) {
-            uint32_t rid = A.evals[it.e0 + r];
-            if (rid >= (uint32_t)bt.N) rid = 0;  // defensive: never read past the ray arrays
-            S.a[r] = A.ray_a[rid];
-            S.c[r] = A.ray_c[rid];
-        }
+        const bool regions = REGIONS && ts.tx == 16 && ts.ty == 16;
+        stage_item_rays<THREADS>(A, it, sd, fp, regions, S.a, S.c, S.reg, s_rcnt);
         sb_order_keys(s_order, p, ts, it.lt, nsb, fp.sensor_x, fp.sensor_y, fp.sensor_z);
         __syncthreads();
         sb_order_rank(s_order, nsb);
@@ -821,11 +915,18 @@ __global__ void __launch_bounds__(kEvThreads, MINB) k_bgki(EvArgs A) {
             // sums of kernel values rounded to integer units; the unsigned conversion saturates a
             // negative table value (the kernel's max(0, .)) to 0
             unsigned long long ao = 0, af = 0;
-            for (int g0 = 0; g0 < nr; g0 += 32) {
-                const int r = g0 + lane;
+            // the rays to cull: the sub-block's region list, or every ray of the item
+            const int q = sb_region(ts, sb);
+            const int nlist = regions ? s_rcnt[q] : nr;
+            const uint16_t* list = S.reg + q * A.chunk;
+            for (int g0 = 0; g0 < nlist; g0 += 32) {
+                const int j = g0 + lane;
                 bool hit = false, near = false;
                 float4 st[3];
-                if (r < nr) hit = stage_pair(S.a[r], S.c[r], ox, oy, oz, hres, cull_ls2, st, &near);
+                if (j < nlist) {
+                    const int r = regions ? (int)list[j] : j;
+                    hit = stage_pair(S.a[r], S.c[r], ox, oy, oz, hres, cull_ls2, st, &near);
+                }
                 // compact the passing rays into the warp's staging list: near rays first
                 const unsigned mnear = __ballot_sync(0xffffffffu, near);
                 const unsigned mfar = __ballot_sync(0xffffffffu, hit && !near);
@@ -879,7 +980,7 @@ __global__ void __launch_bounds__(kEvThreads, MINB) k_bgki(EvArgs A) {
             __threadfence();
             const int tx = it.lt % ts.ntx, ty = (it.lt / ts.ntx) % ts.nty, tz = it.lt / (ts.ntx * ts.nty);
             const int tile_cells = ts.tx * ts.ty * ts.tz;
-            for (int li = threadIdx.x; li < tile_cells; li += kEvThreads) {
+            for (int li = threadIdx.x; li < tile_cells; li += THREADS) {
                 const int lx = li % ts.tx, ly = (li / ts.tx) % ts.ty, lz = li / (ts.tx * ts.ty);
                 const int ix = tx * ts.tx + lx, iy = ty * ts.ty + ly, iz = tz * ts.tz + lz;
                 if (ix >= p.G || iy >= p.G || iz >= p.Gz) continue;
@@ -1254,12 +1355,14 @@ struct CalibSmem {
     float4 (*stage)[32][3];  // [kEvWarps][32][3]
     float4* a;               // [chunk]
     double4* c;              // [chunk]
+    uint16_t* reg;           // [kRegions][chunk] (region builds)
 };
 
 constexpr size_t kCalibFixedBytes = 2 * sizeof(float4) * kKernelTabEntries + sizeof(float4) * kEvWarps * 32 * 3;
 
-inline size_t calib_smem_bytes(int chunk) {
-    return ((kCalibFixedBytes + 31) & ~(size_t)31) + (size_t)chunk * (sizeof(float4) + sizeof(double4));
+inline size_t calib_smem_bytes(int chunk, bool regions = false) {
+    return ((kCalibFixedBytes + 31) & ~(size_t)31) + (size_t)chunk * (sizeof(float4) + sizeof(double4)) +
+           (regions ? (size_t)kRegions * chunk * sizeof(uint16_t) : 0);
 }
 
 __device__ __forceinline__ CalibSmem calib_smem(unsigned char* base, int chunk) {
@@ -1270,13 +1373,14 @@ __device__ __forceinline__ CalibSmem calib_smem(unsigned char* base, int chunk) 
     const size_t off = (kCalibFixedBytes + 31) & ~(size_t)31;
     S.c = reinterpret_cast<double4*>(base + off);
     S.a = reinterpret_cast<float4*>(base + off + sizeof(double4) * (size_t)chunk);
+    S.reg = reinterpret_cast<uint16_t*>(base + off + (sizeof(double4) + sizeof(float4)) * (size_t)chunk);
     return S;
 }
 
 // acc4: 4 signed 64-bit sums per cell (f occ, f free, -x f' occ, -x f' free), in units. Same
 // tiles, culls and pair geometry as k_bgki; each value is rounded once to an integer number of
 // units (round to nearest even).
-template <int MINB>
+template <int MINB, bool REGIONS = false>
 __global__ void __launch_bounds__(kEvThreads, MINB) k_bgki_sums(EvArgs A, const float4* __restrict__ htab,
                                                                unsigned long long* __restrict__ acc4) {
     extern __shared__ __align__(32) unsigned char smem_raw[];
@@ -1284,6 +1388,7 @@ __global__ void __launch_bounds__(kEvThreads, MINB) k_bgki_sums(EvArgs A, const 
     __shared__ uint32_t s_item;
     __shared__ int s_next_sb;
     __shared__ SbOrder s_order;
+    __shared__ int s_rcnt[kRegions];
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
     const unsigned lanes_below = (1u << lane) - 1u;
     const Batch& bt = A.bt;
@@ -1297,6 +1402,7 @@ __global__ void __launch_bounds__(kEvThreads, MINB) k_bgki_sums(EvArgs A, const 
             s_item = atomicAdd(&A.status->work_counter, 1u);
             s_next_sb = 0;
         }
+        if (REGIONS && threadIdx.x < kRegions) s_rcnt[threadIdx.x] = 0;
         __syncthreads();
         const uint32_t item = s_item;
         if (item >= total_items) break;
@@ -1311,12 +1417,8 @@ __global__ void __launch_bounds__(kEvThreads, MINB) k_bgki_sums(EvArgs A, const 
         const float hres = 0.5f * p.res;
         const float cull_ls2 = sd.cull_ls2;
         const int nsb = ts.nsbx * ts.nsby * (ts.tz / 2);
-        for (int r = threadIdx.x; r < it.nr; r += kEvThreads) {
-            uint32_t rid = A.evals[it.e0 + r];
-            if (rid >= (uint32_t)bt.N) rid = 0;
-            S.a[r] = A.ray_a[rid];
-            S.c[r] = A.ray_c[rid];
-        }
+        const bool regions = REGIONS && ts.tx == 16 && ts.ty == 16;
+        stage_item_rays<kEvThreads>(A, it, sd, fp, regions, S.a, S.c, S.reg, s_rcnt);
         sb_order_keys(s_order, p, ts, it.lt, nsb, fp.sensor_x, fp.sensor_y, fp.sensor_z);
         __syncthreads();
         sb_order_rank(s_order, nsb);
@@ -1333,11 +1435,17 @@ __global__ void __launch_bounds__(kEvThreads, MINB) k_bgki_sums(EvArgs A, const 
             const float ls2c = L.c >= 0 ? ls2 : -1.0f;
             const double ox = L.ox, oy = L.oy, oz = L.oz;
             long long fo = 0, ff = 0, ho = 0, hf = 0;
-            for (int g0 = 0; g0 < nr; g0 += 32) {
-                const int r = g0 + lane;
+            const int q = sb_region(ts, sb);
+            const int nlist = regions ? s_rcnt[q] : nr;
+            const uint16_t* list = S.reg + q * A.chunk;
+            for (int g0 = 0; g0 < nlist; g0 += 32) {
+                const int j = g0 + lane;
                 bool hit = false, near = false;
                 float4 st[3];
-                if (r < nr) hit = stage_pair(S.a[r], S.c[r], ox, oy, oz, hres, cull_ls2, st, &near);
+                if (j < nlist) {
+                    const int r = regions ? (int)list[j] : j;
+                    hit = stage_pair(S.a[r], S.c[r], ox, oy, oz, hres, cull_ls2, st, &near);
+                }
                 const unsigned mnear = __ballot_sync(0xffffffffu, near);
                 const unsigned mfar = __ballot_sync(0xffffffffu, hit && !near);
                 const int nn = __popc(mnear), nh = nn + __popc(mfar);
@@ -1393,9 +1501,10 @@ cudaError_t launch_bgki_sums(const Batch& bt, RayBuffers& rb, const float4* f_ta
     if (rb.chunk < 32 || rb.chunk > kChunk) return cudaErrorInvalidValue;
     EvArgs A = make_args(bt, rb, CellState{}, CellWork{}, false, status);
     A.ktab = f_tab;
-    const size_t sm = calib_smem_bytes(rb.chunk);
-    // 4 CTAs per SM where a 512-ray chunk leaves the shared memory for them, else 3
-    auto kern = rb.chunk <= 512 ? k_bgki_sums<4> : k_bgki_sums<3>;
+    // 4 CTAs per SM with region lists up to kCalibChunk rays per item, else 3 without them
+    const bool small = rb.chunk <= kCalibChunk;
+    const size_t sm = calib_smem_bytes(rb.chunk, small);
+    auto kern = small ? k_bgki_sums<4, true> : k_bgki_sums<3>;
     int per_sm = 1;
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kEvThreads, sm);
     ++g_launches;
@@ -1410,7 +1519,7 @@ int bgki_blocks_per_sm() {
 }
 
 // Work items of up to 512 rays leave shared memory for a fourth CTA per SM; that build is limited
-// to 64 registers. Both builds compute the same sums (exactly), so the choice is speed only.
+// to 64 registers. Items of up to 256 rays run in 128-thread CTAs, 8 per SM. Both builds compute the same sums (exactly), so the choice is speed only.
 cudaError_t launch_k3dom_evidence(const Batch& bt, RayBuffers& rb, CellState cs, CellWork cw, bool first_frame,
                                   DevStatus* status, int grid, cudaStream_t st) {
     if (rb.chunk < 32 || rb.chunk > kChunk) return cudaErrorInvalidValue;
@@ -1420,9 +1529,15 @@ cudaError_t launch_k3dom_evidence(const Batch& bt, RayBuffers& rb, CellState cs,
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     ++g_launches;
-    if (rb.chunk <= 512) {
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_bgki<4>, kEvThreads, sm);
-        k_bgki<4><<<sms * std::max(1, per_sm), kEvThreads, sm, st>>>(A);
+    if (rb.chunk <= kSmallChunk) {
+        // 128-thread CTAs: 8 per SM, and each item's end waits on 4 warps instead of 8
+        const size_t sm4 = bgki_smem_bytes(rb.chunk, kSmallWarps);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_bgki<8, kSmallWarps * 32>, kSmallWarps * 32, sm4);
+        k_bgki<8, kSmallWarps * 32><<<sms * std::max(1, per_sm), kSmallWarps * 32, sm4, st>>>(A);
+    } else if (rb.chunk <= 512) {
+        const size_t smr = bgki_smem_bytes(rb.chunk, kEvWarps, true);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_bgki<4, kEvThreads, true>, kEvThreads, smr);
+        k_bgki<4, kEvThreads, true><<<sms * std::max(1, per_sm), kEvThreads, smr, st>>>(A);
     } else {
         cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_bgki<3>, kEvThreads, sm);
         k_bgki<3><<<sms * std::max(1, per_sm), kEvThreads, sm, st>>>(A);
@@ -1448,14 +1563,17 @@ cudaError_t evidence_init() {
     cudaError_t e = cudaFuncSetAttribute(k_bgki<3>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          (int)bgki_smem_bytes(kChunk));
     if (e != cudaSuccess) return e;
-    if ((e = cudaFuncSetAttribute(k_bgki<4>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                  (int)bgki_smem_bytes(kChunk))))
+    if ((e = cudaFuncSetAttribute(k_bgki<8, kSmallWarps * 32>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)bgki_smem_bytes(kSmallChunk, kSmallWarps))))
+        return e;
+    if ((e = cudaFuncSetAttribute(k_bgki<4, kEvThreads, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)bgki_smem_bytes(512, kEvWarps, true))))
         return e;
     if ((e = cudaFuncSetAttribute(k_bgki_sums<3>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                   (int)calib_smem_bytes(kChunk))))
         return e;
-    return cudaFuncSetAttribute(k_bgki_sums<4>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                (int)calib_smem_bytes(kChunk));
+    return cudaFuncSetAttribute(k_bgki_sums<4, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)calib_smem_bytes(kCalibChunk, true));
 }
 
 }  // namespace k3dom

@@ -360,14 +360,15 @@ def test_lockstep_crowded_cells():
 
 def test_config1_scale_tilings_agree_and_evidence_matches_oracle():
     """config1 at full size (256 x 256 x 32 voxels, 4,194,304 particles, 120,000-point scans with
-    ego motion): two evidence tilings give bit-identical frames (the evidence is exact fixed
-    point), and the last frame's BGKI evidence matches the FP64 oracle within 1e-5 relative (the
-    lockstep bar, ties allowed as there)."""
+    ego motion): three evidence tilings, with 512-, 1024- and 256-ray work items (the last in the
+    128-thread build), give bit-identical frames (the evidence is exact fixed point), and the last
+    frame's BGKI evidence matches the FP64 oracle within 1e-5 relative (the lockstep bar, ties
+    allowed as there)."""
     cfg = scene.config1(seed=7)
     p = K.make_params("k3dom", **cfg.params)
     fields = ["free_mass", "static_mass", "dynamic_mass", "pers_mass", "born_mass", "mean_x_vel", "del_occ",
               "del_free"]
-    doms = [K.DOM(p, "k3dom"), K.DOM(p, "k3dom")]
+    doms = [K.DOM(p, "k3dom"), K.DOM(p, "k3dom"), K.DOM(p, "k3dom")]
     try:
         pts = None
         for f in range(3):
@@ -379,9 +380,11 @@ def test_config1_scale_tilings_agree_and_evidence_matches_oracle():
             if f == 0:
                 doms[0].set_tuning(2, 512)   # 16x16x4 tiles, 512 rays per work item
                 doms[1].set_tuning(3, 1024)  # 16x16x8 tiles, 1024 rays per work item
-        a, b = doms
-        for fld in fields:
-            assert np.array_equal(a.get_cell_field(fld), b.get_cell_field(fld), equal_nan=True), fld
+                doms[2].set_tuning(1, 256)   # 8x8x4 tiles, 256 rays per work item
+        a = doms[0]
+        for b in doms[1:]:
+            for fld in fields:
+                assert np.array_equal(a.get_cell_field(fld), b.get_cell_field(fld), equal_nan=True), fld
         i = a.info()
         sensor_rel = np.array([i.sensor_x - i.center_x, i.sensor_y - i.center_y, i.sensor_z - i.center_z],
                               np.float32)
