@@ -718,11 +718,10 @@ __device__ __forceinline__ void slab(float a, float d, float lo, float hi, float
     *t1 = fmaxf(e0, e1);
 }
 
-// Bit q (q = qx + 2 qy) set when the ray's segment (sensor a -> a + m/res, cell-index space)
-// meets region q's box [x0 + 8 qx, x0 + 8 qx + 7] x [y0 + 8 qy, +7] x [z0, z0 + tz - 1] grown by R.
-__device__ __forceinline__ unsigned region_mask(float ax, float ay, float az, float4 m, float inv_res, float x0,
+// Bit q (q = qx + 2 qy) set when the ray's binned segment a -> a + d (cell-index space) meets
+// region q's box [x0 + 8 qx, x0 + 8 qx + 7] x [y0 + 8 qy, +7] x [z0, z0 + tz - 1] grown by R.
+__device__ __forceinline__ unsigned region_mask(float ax, float ay, float az, float dx, float dy, float dz, float x0,
                                                 float y0, float z0, int tz, float R) {
-    const float dx = m.x * inv_res, dy = m.y * inv_res, dz = m.z * inv_res;
     float zl, zh;
     slab(az, dz, z0 - R, z0 + (float)(tz - 1) + R, &zl, &zh);
     zl = fmaxf(zl, 0.0f);
@@ -766,7 +765,11 @@ __device__ __forceinline__ void stage_item_rays(const EvArgs& A, const Item& it,
             const float4 a4 = A.ray_a[rid];
             sa[r] = a4;
             sc[r] = A.ray_c[rid];
-            if (regions) qm = region_mask(g.ax, g.ay, g.az, a4, 1.0f / p.res, x0, y0, z0, ts.tz, sd.bin_R + 0.25f);
+            if (regions) {
+                const float ir = 1.0f / p.res;  // K3DOM binning segment: sensor -> point
+                qm = region_mask(g.ax, g.ay, g.az, a4.x * ir, a4.y * ir, a4.z * ir, x0, y0, z0, ts.tz,
+                                 sd.bin_R + 0.25f);
+            }
         }
         if (regions) {
 #pragma unroll
@@ -1133,7 +1136,10 @@ template <bool COUNT>
 __global__ void __launch_bounds__(kEvThreads) k_dsgrid(EvArgs A) {
     __shared__ float4 sa[kChunk];  // (m, |m|^2)
     __shared__ float4 su[kChunk];  // (m / |m|, 0)
-    __shared__ uint8_t s_cand[kEvWarps][32];
+    __shared__ uint16_t s_cand[kEvWarps][32];
+    __shared__ uint16_t s_reg[kRegions][kChunk];  // region lists, in input order
+    __shared__ int s_wq[2][kEvWarps][kRegions];     // per-warp region counts of a staging step
+    __shared__ int s_rcnt[kRegions];
     __shared__ uint32_t s_item;
     __shared__ int s_next_sb, s_last;
     __shared__ SbOrder s_order;
@@ -1151,6 +1157,7 @@ __global__ void __launch_bounds__(kEvThreads) k_dsgrid(EvArgs A) {
             s_item = atomicAdd(counter, 1u);
             s_next_sb = 0;
         }
+        if (threadIdx.x < kRegions) s_rcnt[threadIdx.x] = 0;
         __syncthreads();
         const uint32_t item = s_item;
         if (item >= total_items) break;
@@ -1166,14 +1173,57 @@ __global__ void __launch_bounds__(kEvThreads) k_dsgrid(EvArgs A) {
         const int coff = bt.off->cell[it.sc];
         const int nsb = ts.nsbx * ts.nsby * (ts.tz / 2);
         const float hres = 0.5f * p.res;
-        for (int r = threadIdx.x; r < it.nr; r += kEvThreads) {
-            uint32_t rid = A.evals[it.e0 + r];
-            if (rid >= (uint32_t)bt.N) rid = 0;
-            const float4 a = A.ray_a[rid];
-            sa[r] = a;
-            const float len = sqrtf(a.w);
-            const float inv = len > 0.0f ? 1.0f / len : 0.0f;
-            su[r] = make_float4(a.x * inv, a.y * inv, a.z * inv, 0.0f);
+        // Rays staged with their unit directions; in a 16x16 tile each is also listed, in input
+        // order, under the 8x8-cell columns its binned half-line (sensor -> grid exit along m)
+        // meets within the binning radius, so a sub-block visits only its column's rays, still in
+        // input order (the first-100 rule).
+        const bool regions = ts.tx == 16 && ts.ty == 16;
+        BinGeom g;
+        place_sensor(g, p, fp);
+        const float x0 = (float)(it.lt % ts.ntx * 16), y0 = (float)((it.lt / ts.ntx) % ts.nty * 16);
+        const float z0 = (float)(it.lt / (ts.ntx * ts.nty) * ts.tz);
+        const float Lc = sqrtf((float)(2 * p.G * p.G + p.Gz * p.Gz)) + 2.0f * sd.bin_R + 4.0f;  // cells
+        int step = 0;
+        for (int r0 = 0; r0 < it.nr; r0 += kEvThreads, ++step) {  // uniform trip count
+            const int r = r0 + (int)threadIdx.x;
+            unsigned qm = 0;
+            if (r < it.nr) {
+                uint32_t rid = A.evals[it.e0 + r];
+                if (rid >= (uint32_t)bt.N) rid = 0;
+                const float4 a = A.ray_a[rid];
+                sa[r] = a;
+                const float len = sqrtf(a.w);
+                const float inv = len > 0.0f ? 1.0f / len : 0.0f;
+                const float4 u = make_float4(a.x * inv, a.y * inv, a.z * inv, 0.0f);
+                su[r] = u;
+                if (regions)
+                    qm = region_mask(g.ax, g.ay, g.az, u.x * Lc, u.y * Lc, u.z * Lc, x0, y0, z0, ts.tz,
+                                     sd.bin_R + 0.25f);
+            }
+            if (regions) {
+                unsigned b[kRegions];
+#pragma unroll
+                for (int q = 0; q < kRegions; ++q) b[q] = __ballot_sync(0xffffffffu, (qm >> q) & 1u);
+                int(*wq)[kRegions] = s_wq[step & 1];
+                if (lane == 0) {
+#pragma unroll
+                    for (int q = 0; q < kRegions; ++q) wq[wid][q] = __popc(b[q]);
+                }
+                __syncthreads();
+#pragma unroll
+                for (int q = 0; q < kRegions; ++q) {
+                    if (!((qm >> q) & 1u)) continue;
+                    int pos = s_rcnt[q] + __popc(b[q] & lanes_below);
+                    for (int w = 0; w < wid; ++w) pos += wq[w][q];
+                    s_reg[q][pos] = (uint16_t)r;
+                }
+                __syncthreads();
+                if (threadIdx.x < kRegions) {
+                    int t = 0;
+                    for (int w = 0; w < kEvWarps; ++w) t += wq[w][threadIdx.x];
+                    s_rcnt[threadIdx.x] += t;
+                }
+            }
         }
         sb_order_keys(s_order, p, ts, it.lt, nsb, fp.sensor_x, fp.sensor_y, fp.sensor_z);
         __syncthreads();
@@ -1202,11 +1252,14 @@ __global__ void __launch_bounds__(kEvThreads) k_dsgrid(EvArgs A) {
             int nb = 0;
             bool all_far = true;
             float mx = 0.0f;
+            const int q = sb_region(ts, sb);
+            const int nlist = regions ? s_rcnt[q] : nr;
             if (__any_sync(0xffffffffu, quota > 0)) {
-                for (int g0 = 0; g0 < nr; g0 += 32) {
-                    const int r = g0 + lane;
+                for (int g0 = 0; g0 < nlist; g0 += 32) {
+                    const int jl = g0 + lane;
+                    const int r = regions ? (jl < nlist ? (int)s_reg[q][jl] : 0) : jl;
                     bool hit = false;
-                    if (r < nr) {
+                    if (jl < nlist) {
                         // box bound on the distance from the half-line through m to the sub-block's
                         // cell centres (the K3DOM cull's bound, with the window as the radius)
                         const float4 u = su[r];
@@ -1217,12 +1270,11 @@ __global__ void __launch_bounds__(kEvThreads) k_dsgrid(EvArgs A) {
                     }
                     // candidates in input order (the first-100 rule counts them in that order)
                     const unsigned mask = __ballot_sync(0xffffffffu, hit);
-                    if (hit) s_cand[wid][__popc(mask & lanes_below)] = (uint8_t)lane;
+                    if (hit) s_cand[wid][__popc(mask & lanes_below)] = (uint16_t)r;
                     __syncwarp();
                     const int ncand = __popc(mask);
                     for (int k = 0; k < ncand; ++k) {
-                        const int j = s_cand[wid][k];
-                        const float4 a = sa[g0 + j];
+                        const float4 a = sa[s_cand[wid][k]];
                         if (nb < quota && ds_is_neighbor(L.x, L.y, L.z, acs, a, sd.wr2)) {
                             ++nb;
                             if (!COUNT) {
