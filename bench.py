@@ -237,7 +237,7 @@ def run_ours(args):
     torch.cuda.set_device(local)
     cfg = scene_cfg(args.variant, rank)
     W, Kst = args.warmup, args.steps
-    n_tune = 8  # evidence autotuner: one live frame per candidate (k3dom_autotune)
+    n_tune = 16  # evidence autotuner: one live frame per candidate (k3dom_autotune), at most 16
     n_e2e_warm = 3  # untimed end-to-end iterations (first-call costs: export buffer, host staging)
     n_frames = 1 + n_tune + W + Kst + 2 + Kst + 1 + n_e2e_warm + Kst
     log(f"[rank {rank}] generating {n_frames} scans of {cfg.n_points} points")

@@ -310,7 +310,8 @@ k3dom_status k3dom_batch_update_async(k3dom_handle* h, const float* t, const flo
  * 8x8x4; 1: 8x8x4; 2: 16x16x4; 3: 16x16x8) and rays per work item (chunk) change its speed,
  * never its results. k3dom_autotune(h, 1) measures every (rule, chunk in {512, 1024})
  * candidate on the next steady frames, one candidate per frame (those frames are run without
- * the graph), then keeps the fastest. */
+ * the graph), then keeps the fastest. candidate_ms[k] belongs to rule k % 4 with chunk
+ * {512, 1024}[k / 4]. */
 #define K3DOM_TUNE_MAX_CANDIDATES 16
 typedef struct k3dom_tuning {
     int32_t tile_rule, chunk, tuned, tuning, candidates, evidence_blocks;

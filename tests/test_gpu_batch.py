@@ -122,7 +122,8 @@ def test_batch_autotune_keeps_results(device_points):
         tu = batch.tuning()
         assert tu["tuned"] == 1 and tu["tuning"] == 0
         assert all(ms > 0 for ms in tu["candidate_ms"])
-        assert tu["candidate_ms"][tu["tile_rule"] + 4 * (1 if tu["chunk"] == 1024 else 0)] == pytest.approx(
+        # candidate k is (rule k % 4, chunk (512, 1024)[k // 4])
+        assert tu["candidate_ms"][tu["tile_rule"] + 4 * [512, 1024].index(tu["chunk"])] == pytest.approx(
             tu["best_ms"])
     finally:
         batch.close()
