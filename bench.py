@@ -16,7 +16,7 @@ ours           the library through its C ABI: `value` is device-timed frames/s w
 reference      the CPU baseline of the path: the reference has no CPU implementation, so its
                restatement (oracle/, FP64, OpenMP over all host threads) runs the same frames.
 reference-gpu  the reference's own CUDA update (oracle/_ref, built from its sources), frames/s
-               on this GPU (not used by the driver; reported in the design notes).
+               on this GPU (a second reference measurement, reported beside the CPU one).
 
 Multi-GPU: the single-scene update does not shard (replicas only); with torchrun every rank
 runs an independent scene (weak scaling), timed on the device, max over ranks.
