@@ -796,9 +796,9 @@ void read_times(k3dom_handle* h) {
 }
 
 // Evidence tuning: candidates are (tile rule, chunk) pairs measured one per steady frame.
-// (256-ray items, the 128-thread evidence build, are left out: on the benchmark scene the one-frame
-// measurements put 16x16x4 tiles at 256 rays ahead of 512 while the steady graph-replayed frame is
-// 5 % slower with them; set them with k3dom_set_tuning.)
+// (256-ray items, the 128-thread evidence build, are left out: on a 256x256x32-voxel scene with
+// 120,000-point scans the one-frame measurements put 16x16x4 tiles at 256 rays ahead of 512 while
+// the steady graph-replayed frame is 5 % slower with them; set them with k3dom_set_tuning.)
 constexpr int kTuneChunks[2] = {512, 1024};
 constexpr int kTuneCount = kRuleCount * 2;
 static_assert(kTuneCount <= K3DOM_TUNE_MAX_CANDIDATES, "tuning candidates");
