@@ -148,3 +148,37 @@ def test_reference_config_files_load(variant, method, dataset):
     p = K.params_from_yaml(variant, str(REF_CONFIG / method), str(REF_CONFIG / dataset))
     G = int(np.float32(p.size) / np.float32(p.resolution))
     assert G > 0 and p.particle_count == 1_000_000
+
+
+def _zero_args(argtypes):
+    """Null for every pointer argument, zero for every number."""
+    out = []
+    for t in argtypes:
+        if t in (C.c_float, C.c_double):
+            out.append(0.0)
+        elif t in (C.c_int, C.c_int32, C.c_int64, C.c_long, C.c_uint32, C.c_uint64, C.c_ulong, C.c_size_t):
+            out.append(0)
+        else:
+            out.append(None)
+    return out
+
+
+def test_every_entry_point_refuses_a_null_handle():
+    """The reference's DOM has no error path (device asserts trap); here every call that takes a
+    handle returns K3DOM_ERR_INVALID_ARGUMENT for a null one, before touching a device, and the
+    creators refuse a null output slot."""
+    lib = N.load()
+    handle_calls = [n for n, (_, a) in N.SIGNATURES.items()
+                    if a and a[0] is N._P and n not in ("k3dom_exact_prefix_sum_noalloc", "k3dom_last_cuda_error")]
+    assert len(handle_calls) >= 50
+    for name in handle_calls:
+        st = getattr(lib, name)(*_zero_args(N.SIGNATURES[name][1]))
+        assert st == 1, f"{name} returned {st} for a null handle"
+    for name in ("k3dom_create", "k3dom_batch_create", "k3dom_calib_create"):
+        st = getattr(lib, name)(*_zero_args(N.SIGNATURES[name][1]))
+        assert st == 1, f"{name} returned {st} for a null output"
+    assert lib.k3dom_last_cuda_error(None) == b"no handle"
+    # the allocation-free scan: bad sizes and missing buffers are refused, an empty scan is a no-op
+    assert lib.k3dom_exact_prefix_sum_noalloc(None, None, -1, None) == 1
+    assert lib.k3dom_exact_prefix_sum_noalloc(None, None, 5, None) == 1
+    assert lib.k3dom_exact_prefix_sum_noalloc(None, None, 0, None) == 0
