@@ -1133,7 +1133,7 @@ __device__ __forceinline__ float ds_pocc(float x, float y, float z, float4 m, fl
 constexpr int kMaxTileCells = 16 * 16 * 8;
 
 template <bool COUNT>
-__global__ void __launch_bounds__(kEvThreads) k_dsgrid(EvArgs A) {
+__global__ void __launch_bounds__(kEvThreads, COUNT ? 5 : 4) k_dsgrid(EvArgs A) {
     __shared__ float4 sa[kChunk];  // (m, |m|^2)
     __shared__ float4 su[kChunk];  // (m / |m|, 0)
     __shared__ uint16_t s_cand[kEvWarps][32];
@@ -1602,8 +1602,13 @@ cudaError_t launch_ds_evidence(const Batch& bt, RayBuffers& rb, CellState cs, Ce
                                DevStatus* status, int grid, cudaStream_t st) {
     if (rb.chunk < 32 || rb.chunk > kChunk) return cudaErrorInvalidValue;
     EvArgs A = make_args(bt, rb, cs, cw, first_frame, status);
+    // the count pass fits 5 CTAs per SM (47 registers), the final pass 4
+    int dev = 0, sms = 148, per_sm = 1;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_dsgrid<true>, kEvThreads, 0);
     ++g_launches;
-    k_dsgrid<true><<<grid, kEvThreads, 0, st>>>(A);
+    k_dsgrid<true><<<sms * std::max(1, per_sm), kEvThreads, 0, st>>>(A);
     ++g_launches;
     k_dsgrid<false><<<grid, kEvThreads, 0, st>>>(A);
     return cudaGetLastError();
