@@ -651,7 +651,9 @@ __device__ __forceinline__ void res_store(const ResScene& r, int k, int a, const
     anc_out[k] = a;
 }
 
-__global__ void __launch_bounds__(kResThreads)
+// 5 CTAs per SM (48 registers, no spills): the gathers through the ancestor index wait on memory
+// latency, so more resident warps help.
+__global__ void __launch_bounds__(kResThreads, 5)
 k_resample(Batch bt, const float* __restrict__ joint_cum, const uint32_t* __restrict__ dkeys, const int2* br,
            Particles s, Particles b, Particles out, int* __restrict__ anc_out, float* __restrict__ joint_max_out) {
     __shared__ float s_acc[kResStage];
