@@ -150,7 +150,7 @@ struct k3dom_handle {
     bool births_done = false;
     int launches_per_frame = 0;
     int launches_upload = 0;  // kernels of the last frame's point upload (de-interleaving)
-    int bgki_grid = 0, ds_grid = 0;
+    int ds_grid = 0;
     int ds_sized_chunk = 0;  // chunk the DS count buffer was sized for
 
     // evidence tuning
@@ -662,7 +662,7 @@ cudaError_t enq_evidence(k3dom_handle* h, bool first_frame) {
     const Batch bt = h->batch();
     if (h->ds())
         return launch_ds_evidence(bt, h->rb, h->cells(), h->cw, first_frame, h->status, h->ds_grid, h->st);
-    return launch_k3dom_evidence(bt, h->rb, h->cells(), h->cw, first_frame, h->status, h->bgki_grid, h->st);
+    return launch_k3dom_evidence(bt, h->rb, h->cells(), h->cw, first_frame, h->status, h->st);
 }
 
 cudaError_t enq_occupancy(k3dom_handle* h, bool first_frame) {
@@ -890,7 +890,6 @@ k3dom_status k3dom_batch_create(const k3dom_params* params, int32_t n_scenes, k3
     if ((e = cudaGetDeviceProperties(&prop, device))) return bail(e);
     h->num_sms = prop.multiProcessorCount;
     if ((e = sort_init()) || (e = evidence_init())) return bail(e);
-    h->bgki_grid = h->num_sms * bgki_blocks_per_sm();
     h->ds_grid = h->num_sms * 4;
 
     // scene ranges
@@ -1307,7 +1306,7 @@ k3dom_status k3dom_get_tuning(k3dom_handle* h, k3dom_tuning* out) {
     out->best_ms = h->tune_best_ms;
     for (int k = 0; k < kTuneCount && k < (int)h->tune_ms.size() && k < K3DOM_TUNE_MAX_CANDIDATES; ++k)
         out->candidate_ms[k] = h->tune_ms[k];
-    out->evidence_blocks = h->ds() ? h->ds_grid : h->bgki_grid;
+    out->evidence_blocks = h->ds() ? h->ds_grid : k3dom_evidence_blocks(h->rb.chunk);
     return K3DOM_OK;
 }
 

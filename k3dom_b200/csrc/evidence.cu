@@ -1564,37 +1564,51 @@ cudaError_t launch_bgki_sums(const Batch& bt, RayBuffers& rb, const float4* f_ta
     return cudaGetLastError();
 }
 
-int bgki_blocks_per_sm() {
-    int per_sm = 1;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_bgki<3>, kEvThreads, bgki_smem_bytes(kChunk));
-    return std::max(1, per_sm);
+// The K3DOM evidence launch is persistent: one CTA per resident slot of the build the chunk selects
+// (128 threads at <= 256 rays, 256 threads with region lists at <= 512, 256 threads at <= 1024).
+struct BgkiLaunch {
+    int blocks, threads;
+    size_t smem;
+};
+
+static BgkiLaunch bgki_launch(int chunk) {
+    int dev = 0, sms = 148, per_sm = 1;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    BgkiLaunch L;
+    if (chunk <= kSmallChunk) {
+        L.threads = kSmallWarps * 32;
+        L.smem = bgki_smem_bytes(chunk, kSmallWarps);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_bgki<8, kSmallWarps * 32>, L.threads, L.smem);
+    } else if (chunk <= 512) {
+        L.threads = kEvThreads;
+        L.smem = bgki_smem_bytes(chunk, kEvWarps, true);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_bgki<4, kEvThreads, true>, L.threads, L.smem);
+    } else {
+        L.threads = kEvThreads;
+        L.smem = bgki_smem_bytes(chunk);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_bgki<3>, L.threads, L.smem);
+    }
+    L.blocks = sms * std::max(1, per_sm);
+    return L;
 }
+
+int k3dom_evidence_blocks(int chunk) { return bgki_launch(chunk).blocks; }
 
 // Work items of up to 512 rays leave shared memory for a fourth CTA per SM; that build is limited
 // to 64 registers. Items of up to 256 rays run in 128-thread CTAs, 8 per SM. Both builds compute the same sums (exactly), so the choice is speed only.
 cudaError_t launch_k3dom_evidence(const Batch& bt, RayBuffers& rb, CellState cs, CellWork cw, bool first_frame,
-                                  DevStatus* status, int grid, cudaStream_t st) {
+                                  DevStatus* status, cudaStream_t st) {
     if (rb.chunk < 32 || rb.chunk > kChunk) return cudaErrorInvalidValue;
     EvArgs A = make_args(bt, rb, cs, cw, first_frame, status);
-    const size_t sm = bgki_smem_bytes(rb.chunk);
-    int dev = 0, sms = 148, per_sm = 1;
-    cudaGetDevice(&dev);
-    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    const BgkiLaunch L = bgki_launch(rb.chunk);
     ++g_launches;
-    if (rb.chunk <= kSmallChunk) {
-        // 128-thread CTAs: 8 per SM, and each item's end waits on 4 warps instead of 8
-        const size_t sm4 = bgki_smem_bytes(rb.chunk, kSmallWarps);
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_bgki<8, kSmallWarps * 32>, kSmallWarps * 32, sm4);
-        k_bgki<8, kSmallWarps * 32><<<sms * std::max(1, per_sm), kSmallWarps * 32, sm4, st>>>(A);
-    } else if (rb.chunk <= 512) {
-        const size_t smr = bgki_smem_bytes(rb.chunk, kEvWarps, true);
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_bgki<4, kEvThreads, true>, kEvThreads, smr);
-        k_bgki<4, kEvThreads, true><<<sms * std::max(1, per_sm), kEvThreads, smr, st>>>(A);
-    } else {
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_bgki<3>, kEvThreads, sm);
-        k_bgki<3><<<sms * std::max(1, per_sm), kEvThreads, sm, st>>>(A);
-    }
-    (void)grid;
+    if (rb.chunk <= kSmallChunk)  // 128-thread CTAs: 8 per SM, each item's end waits on 4 warps
+        k_bgki<8, kSmallWarps * 32><<<L.blocks, L.threads, L.smem, st>>>(A);
+    else if (rb.chunk <= 512)
+        k_bgki<4, kEvThreads, true><<<L.blocks, L.threads, L.smem, st>>>(A);
+    else
+        k_bgki<3><<<L.blocks, L.threads, L.smem, st>>>(A);
     return cudaGetLastError();
 }
 

@@ -134,10 +134,11 @@ void fill_scene_evidence(SceneDev& sd, bool ds, float4* ktab);
 cudaError_t build_ray_lists(const Batch& bt, const float* xs, const float* ys, const float* zs, RayBuffers& rb,
                             bool ds, DevStatus* status, cudaStream_t st);
 cudaError_t launch_k3dom_evidence(const Batch& bt, RayBuffers& rb, CellState cs, CellWork cw, bool first_frame,
-                                  DevStatus* status, int grid, cudaStream_t st);
+                                  DevStatus* status, cudaStream_t st);
 cudaError_t launch_ds_evidence(const Batch& bt, RayBuffers& rb, CellState cs, CellWork cw, bool first_frame,
                                DevStatus* status, int grid, cudaStream_t st);
-int bgki_blocks_per_sm();
+// CTAs of the K3DOM evidence launch for a chunk size (persistent grid).
+int k3dom_evidence_blocks(int chunk);
 long ds_count_bytes(long items);
 cudaError_t evidence_init();
 // Host: the sparse-kernel table for sigma, every value multiplied by scale: 512 intervals and a
