@@ -155,10 +155,52 @@ def read_peaks() -> tuple[float, str]:
         return FALLBACK_HBM_GBS, "fallback"
 
 
+def stage_bytes(P: int, B: int, C: int, N: int) -> dict:
+    """Algorithmic HBM bytes per frame of each timed stage, minimal FP32 SoA: prediction 60P;
+    assignment = key sort 52P + payload permute 56P + ranges 4P+8C + the per-cell moment sums
+    fused into the gather 16P+12C; occupancy (evidence + cell update) 36C+4P+12N; persistent
+    reweight 12P+4C; births 8C+36B; resampling = joint scan 12(P+B) + draw sort 32P + ancestor
+    gather 60P. Sum: 1.486 GB at 2,097,152 cells, P=4,194,304, B=1,048,576, N=120,000."""
+    return {
+        "predict": 60 * P,
+        "assign": 52 * P + 56 * P + 4 * P + 8 * C + 16 * P + 12 * C,
+        "occupancy": 36 * C + 4 * P + 12 * N,
+        "persistent": 12 * P + 4 * C,
+        "births": 8 * C + 36 * B,
+        "resample": 12 * (P + B) + 32 * P + 60 * P,
+    }
+
+
+PARTICLE_STAGES = ("predict", "assign", "persistent", "births", "resample")
+
+
 def hbm_bytes_particle_stages(P: int, B: int, C: int, N: int) -> float:
-    """Algorithmic bytes of the HBM-bound stages per frame (minimal FP32 SoA)."""
-    return (60 * P + 52 * P + 56 * P + 4 * P + 8 * C + 36 * C + 4 * P + 12 * N + 12 * P + 4 * C + 16 * P + 12 * C
-            + 8 * C + 36 * B + 12 * (P + B) + 32 * P + 60 * P)
+    """Algorithmic bytes of the HBM-bound particle stages per frame (the occupancy stage, which
+    is bound by SIMT issue, is left out)."""
+    b = stage_bytes(P, B, C, N)
+    return float(sum(b[k] for k in PARTICLE_STAGES))
+
+
+def stage_roofline(stage: dict, P: int, B: int, C: int, N: int, hbm_peak: float) -> dict:
+    """Each stage's algorithmic bytes / its CUDA-event time / the HBM peak."""
+    out = {}
+    for k, nbytes in stage_bytes(P, B, C, N).items():
+        ms = stage.get(f"{k}_ms")
+        if not ms:
+            continue
+        gbs = nbytes / (ms * 1e-3) / 1e9
+        out[k] = {"algorithmic_bytes": int(nbytes), "ms": round(ms, 4), "gbs": round(gbs, 1),
+                  "frac": round(gbs / hbm_peak, 4)}
+    return out
+
+
+def workload_name(cfg, variant: str) -> str:
+    """The workload string both arms report (same scene, same frames)."""
+    G = int(np.float32(cfg.params["size"]) / np.float32(cfg.params["resolution"]))
+    Gz = int(np.float32(cfg.params["size_z"]) / np.float32(cfg.params["resolution"]))
+    return (f"{cfg.name}: {variant} steady-state frame, {G}x{G}x{Gz} voxels @{cfg.params['resolution']:g} m, "
+            f"P={cfg.params['particle_count']}, B={cfg.params['new_born_particle_count']}, "
+            f"{cfg.n_points} points/scan, ego motion, 10 Hz")
 
 
 # ------------------------------------------------------------------ frames
@@ -229,191 +271,205 @@ def scene_cfg(variant: str, rank: int):
 
 
 # ------------------------------------------------------------------ arms
-def run_ours(args):
+def measure_plain(args, variant: str, cfg, rank: int, world: int, local: int, dist, sample_clocks: bool) -> dict:
+    """One plain handle on this rank's scene: autotune, warm up, time K graph-replayed frames with
+    the scans in HBM (CUDA events on the handle's stream), then per-stage times, then K frames end
+    to end through k3dom_update_grid (pinned host scan in, occupancy out to pinned host memory)."""
     import torch
 
     import k3dom_b200 as K
-    rank, world, local, dist = dist_setup(args.gpus)
-    torch.cuda.set_device(local)
-    cfg = scene_cfg(args.variant, rank)
+    from k3dom_b200 import _native as N
     W, Kst = args.warmup, args.steps
     n_tune = 16  # evidence autotuner: one live frame per candidate (k3dom_autotune), at most 16
     n_e2e_warm = 3  # untimed end-to-end iterations (first-call costs: export buffer, host staging)
     n_frames = 1 + n_tune + W + Kst + 2 + Kst + 1 + n_e2e_warm + Kst
-    log(f"[rank {rank}] generating {n_frames} scans of {cfg.n_points} points")
+    log(f"[rank {rank}] {variant}: generating {n_frames} scans of {cfg.n_points} points")
     frames = make_frames(cfg, n_frames)
-    p = K.make_params(args.variant, **cfg.params)
-    dom = K.DOM(p, args.variant, device=local)
-    C_, P, B = dom.grid_cell_count, dom.particle_count, dom.new_born_particle_count
-    # scans resident in HBM for the device-timed run
-    dev_pts = [torch.from_numpy(f[2]).to(f"cuda:{local}") for f in frames]
-    torch.cuda.synchronize()
-    idx = 0
+    p = K.make_params(variant, **cfg.params)
+    dom = K.DOM(p, variant, device=local)
+    try:
+        # scans resident in HBM for the device-timed run
+        dev_pts = [torch.from_numpy(f[2]).to(f"cuda:{local}") for f in frames]
+        torch.cuda.synchronize()
 
-    def step_device(i):
-        t, s, _ = frames[i]
-        dom.updatePose(*s)
-        dom.updateGridAsync(t, dev_pts[i])
+        def step_device(i):
+            t, s, _ = frames[i]
+            dom.updatePose(*s)
+            dom.updateGridAsync(t, dev_pts[i])
 
-    # first frame (initialisation), the autotuner's frames, then warm-up; the graph is captured on
-    # the first steady frame after tuning
-    dom.set_graph_mode(True)
-    dom.updatePose(*frames[0][1])
-    dom.updateGrid(frames[0][0], dev_pts[0])
-    idx = 1
-    if args.tile_rule is None:
-        dom.autotune(True)
-        for _ in range(dom.tuning()["candidates"]):
+        # first frame (initialisation), the autotuner's frames, then warm-up; the graph is captured
+        # on the first steady frame after tuning
+        dom.set_graph_mode(True)
+        dom.updatePose(*frames[0][1])
+        dom.updateGrid(frames[0][0], dev_pts[0])
+        idx = 1
+        if args.tile_rule is None:
+            dom.autotune(True)
+            for _ in range(dom.tuning()["candidates"]):
+                step_device(idx)
+                idx += 1
+        else:
+            dom.set_tuning(args.tile_rule, args.chunk)
+        dom.synchronize()
+        tuning = dom.tuning()
+        for _ in range(W):
             step_device(idx)
             idx += 1
-    else:
-        dom.set_tuning(args.tile_rule, args.chunk)
-    dom.synchronize()
-    tuning = dom.tuning()
-    for _ in range(W):
-        step_device(idx)
-        idx += 1
-    dom.synchronize()
-    stream = torch.cuda.ExternalStream(dom.stream())
-    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    props = torch.cuda.get_device_properties(local)
-    uuid = getattr(props, "uuid", None)
-    gpu_id = f"GPU-{uuid}" if uuid is not None else str(local)
-    sampler = ClockSampler(gpu_id) if rank == 0 else None
-    barrier(dist)
-    torch.cuda.synchronize()
-    if sampler:
-        sampler.start()
-        time.sleep(0.3)
-    ev0.record(stream)
-    for _ in range(Kst):
-        step_device(idx)
-        idx += 1
-    ev1.record(stream)
-    dom.synchronize()
-    torch.cuda.synchronize()
-    barrier(dist)
-    clocks = sampler.stop() if sampler else None
-    ms = ev0.elapsed_time(ev1) / Kst
-    ms_max = max_over_ranks(ms, dist)
-    diag = dom.diagnostics()
-    launches = int(diag["kernel_launches_per_frame"])
-
-    # per-stage device times and the evidence kernel's work (events on the handle's stream)
-    dom.set_timing(True)
-    st_acc, evals = [], []
-    for _ in range(2):
-        step_device(idx)
-        idx += 1
         dom.synchronize()
-    for _ in range(min(Kst, 10)):
-        step_device(idx)
-        idx += 1
+        stream = torch.cuda.ExternalStream(dom.stream())
+        ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        props = torch.cuda.get_device_properties(local)
+        uuid = getattr(props, "uuid", None)
+        gpu_id = f"GPU-{uuid}" if uuid is not None else str(local)
+        sampler = ClockSampler(gpu_id) if (rank == 0 and sample_clocks) else None
+        barrier(dist)
+        torch.cuda.synchronize()
+        if sampler:
+            sampler.start()
+            time.sleep(0.3)
+        ev0.record(stream)
+        for _ in range(Kst):
+            step_device(idx)
+            idx += 1
+        ev1.record(stream)
         dom.synchronize()
-        st_acc.append(dom.stage_times())
-        evals.append(dom.diagnostics()["kernel_evaluations"])
-    dom.set_timing(False)
-    diag_after = dom.diagnostics()
-    stage = {k: float(np.mean([s[k] for s in st_acc])) for k in st_acc[0]}
+        torch.cuda.synchronize()
+        barrier(dist)
+        clocks = sampler.stop() if sampler else None
+        ms = ev0.elapsed_time(ev1) / Kst
+        ms_max = max_over_ranks(ms, dist)
+        launches = int(dom.diagnostics()["kernel_launches_per_frame"])
 
-    # end to end through the C ABI: pinned host scan in, per-voxel occupancy out, every frame
-    host_pts = [torch.from_numpy(f[2]).pin_memory() for f in frames]
-    occ_out = torch.empty(C_, dtype=torch.float32).pin_memory()
-    occ_ptr = occ_out.data_ptr()
-    lib = dom._lib
-    from k3dom_b200 import _native as N
-    field = N.CELL_FIELDS["occ_mean" if args.variant == "k3dom" else "occ_prob"]
-    # every frame writes its occupancy into the pinned host buffer (registered output): the
-    # device->host copy is part of each frame, overlapped with the frame's last stages
-    N.check(lib.k3dom_set_output(dom._h, field, occ_ptr, N.MEM_HOST), "set_output")
+        # per-stage device times and the evidence kernel's work (events on the handle's stream)
+        dom.set_timing(True)
+        st_acc, evals = [], []
+        for _ in range(2):
+            step_device(idx)
+            idx += 1
+            dom.synchronize()
+        for _ in range(min(Kst, 10)):
+            step_device(idx)
+            idx += 1
+            dom.synchronize()
+            st_acc.append(dom.stage_times())
+            evals.append(dom.diagnostics()["kernel_evaluations"])
+        dom.set_timing(False)
+        diag_after = dom.diagnostics()
+        stage = {k: float(np.mean([s[k] for s in st_acc])) for k in st_acc[0]}
 
-    def e2e_frame(i):
-        t, s, _ = frames[i]
-        hp = host_pts[i].numpy()
-        dom.updatePose(*s)
-        N.check(lib.k3dom_update_grid(dom._h, float(t), hp.ctypes.data, None, None, hp.shape[0], N.MEM_HOST),
-                "update_grid")
+        # end to end through the C ABI: pinned host scan in, per-voxel occupancy out, every frame
+        host_pts = [torch.from_numpy(f[2]).pin_memory() for f in frames]
+        occ_out = torch.empty(dom.grid_cell_count, dtype=torch.float32).pin_memory()
+        lib = dom._lib
+        field = N.CELL_FIELDS["occ_mean" if variant == "k3dom" else "occ_prob"]
+        # every frame writes its occupancy into the pinned host buffer (registered output): the
+        # device->host copy is part of each frame, overlapped with the frame's last stages
+        N.check(lib.k3dom_set_output(dom._h, field, occ_out.data_ptr(), N.MEM_HOST), "set_output")
 
-    for _ in range(n_e2e_warm):
-        e2e_frame(idx)
-        idx += 1
-    barrier(dist)
-    t0 = time.perf_counter()
-    n_e2e = 0
-    while n_e2e < Kst and idx < len(frames):
-        e2e_frame(idx)
-        idx += 1
-        n_e2e += 1
-    e2e_s = time.perf_counter() - t0
-    e2e_s = max_over_ranks(e2e_s, dist)
-    e2e_fps = world * n_e2e / e2e_s
+        def e2e_frame(i):
+            t, s, _ = frames[i]
+            hp = host_pts[i].numpy()
+            dom.updatePose(*s)
+            N.check(lib.k3dom_update_grid(dom._h, float(t), hp.ctypes.data, None, None, hp.shape[0], N.MEM_HOST),
+                    "update_grid")
 
-    value = world * 1000.0 / ms_max
+        for _ in range(n_e2e_warm):
+            e2e_frame(idx)
+            idx += 1
+        barrier(dist)
+        t0 = time.perf_counter()
+        n_e2e = 0
+        while n_e2e < Kst and idx < len(frames):
+            e2e_frame(idx)
+            idx += 1
+            n_e2e += 1
+        e2e_s = max_over_ranks(time.perf_counter() - t0, dist)
+        return {"ms": ms_max, "value": world * 1000.0 / ms_max, "e2e_fps": world * n_e2e / e2e_s,
+                "launches": launches, "stage": stage, "evals": float(np.mean(evals)), "tuning": tuning,
+                "diag": diag_after, "clocks": clocks, "frames": frames, "C": dom.grid_cell_count,
+                "P": dom.particle_count, "B": dom.new_born_particle_count}
+    finally:
+        dom.close()
+
+
+def evidence_roofline(m: dict, variant: str) -> dict:
+    """The dominant kernel's line: in-support evaluations (K3DOM) or accepted neighbours (DS) x
+    FLOP per unit / its CUDA-event time / the nominal FP32 issue peak."""
+    ev_ms = m["stage"]["evidence_ms"]
+    ds = variant != "k3dom"
+    flop_per = FLOP_PER_DS_NEIGHBOUR if ds else FLOP_PER_EVAL
+    achieved = m["evals"] * flop_per / (ev_ms * 1e-3) / 1e12
+    traffic, issue = None, None
+    tr_file = ROOT / "profiles" / ("dsgrid_traffic.json" if ds else "bgki_traffic.json")
+    rule_name = ["by-size", "8x8x4", "16x16x4", "16x16x8"][m["tuning"]["tile_rule"]]
+    if rule_name == "by-size":
+        rule_name = "16x16x8"  # the rule's choice for grids of >= 2^20 cells
+    if tr_file.exists():
+        try:
+            d = json.loads(tr_file.read_text())
+            issue = d.get("issue")
+            per = d["per_tiling"]
+            hit = per.get(f"{rule_name}@{m['tuning']['chunk']}") or per.get(rule_name) or {}
+            traffic = hit.get("dram_bytes_per_launch")
+        except Exception:
+            traffic = None
+    return {
+        "kernel": ("k_dsgrid (DS measurement grid + fused Dempster update)" if ds else
+                   "k_bgki (sparse BGKI evidence + fused cell update)"),
+        "bound": "fp32", "achieved": round(achieved, 3), "peak": round(NOMINAL_FP32_TFLOPS, 1),
+        "unit": "TFLOP/s", "frac": round(achieved / NOMINAL_FP32_TFLOPS, 4), "traffic": traffic,
+        "peak_source": "nominal FP32 (148 SMs x 128 lanes x 2 x 1.965 GHz); no measured FP32 peak",
+        "work": (f"{m['evals']:.4g} accepted neighbours x {flop_per} FLOP per frame" if ds else
+                 f"{m['evals']:.4g} in-support kernel evaluations x {flop_per} FLOP per frame"),
+        "launch_ms": round(ev_ms, 4),
+        "note": ("SIMT-issue bound: frac counts only in-support evaluations x FLOP; the lanes outside "
+                 "a ray's support, the FP64 pair set-up and the fixed-point rounding are the rest"),
+        "ncu_issue": issue,
+    }
+
+
+def run_ours(args):
+    import torch
+
+    rank, world, local, dist = dist_setup(args.gpus)
+    torch.cuda.set_device(local)
+    cfg = scene_cfg(args.variant, rank)
+    m = measure_plain(args, args.variant, cfg, rank, world, local, dist, sample_clocks=True)
+    Kst, W = args.steps, args.warmup
+    ds_m = None
+    if args.variant == "k3dom" and not args.no_ds:
+        ds_cfg = scene_cfg("dsphdmib", rank)
+        ds_m = measure_plain(args, "dsphdmib", ds_cfg, rank, world, local, dist, sample_clocks=False)
     batch_res = None
     if not args.no_batch:
         batch_res = run_batch(args, local, rank, world, dist)
     out = None
     if rank == 0:
         hbm_peak, peak_src = read_peaks()
-        ev_ms = stage["evidence_ms"]
-        n_evals = float(np.mean(evals))
-        ds = args.variant != "k3dom"
-        flop_per = FLOP_PER_DS_NEIGHBOUR if ds else FLOP_PER_EVAL
-        achieved_tflops = n_evals * flop_per / (ev_ms * 1e-3) / 1e12
-        part_ms = stage["predict_ms"] + stage["assign_ms"] + stage["persistent_ms"] + stage["births_ms"] + \
-            stage["resample_ms"]
+        C_, P, B = m["C"], m["P"], m["B"]
+        stage = m["stage"]
+        part_ms = sum(stage[f"{k}_ms"] for k in PARTICLE_STAGES)
         part_bytes = hbm_bytes_particle_stages(P, B, C_, cfg.n_points)
-        # DRAM bytes of one k_bgki launch at this workload, measured by ncu for the tiling in use
-        traffic = None
-        tr_file = ROOT / "profiles" / "bgki_traffic.json"
-        rule_name = ["by-size", "8x8x4", "16x16x4", "16x16x8"][tuning["tile_rule"]]
-        if rule_name == "by-size":
-            rule_name = "16x16x8"  # the rule's choice for grids of >= 2^20 cells
-        issue = None
-        if tr_file.exists() and args.variant == "k3dom":
-            try:
-                issue = json.loads(tr_file.read_text()).get("issue")
-            except Exception:
-                issue = None
-        if tr_file.exists() and args.variant == "k3dom":
-            try:
-                per = json.loads(tr_file.read_text())["per_tiling"]
-                hit = per.get(f"{rule_name}@{tuning['chunk']}") or per.get(rule_name) or {}
-                traffic = hit.get("dram_bytes_per_launch")
-            except Exception:
-                traffic = None
+        tuning = m["tuning"]
         out = {
-            "metric": METRIC, "value": round(value, 3), "unit": UNIT, "n_gpus": world, "steps": Kst,
-            "warmup": W, "ms_per_step": round(ms_max, 4), "higher_is_better": True, "scaling": "weak",
+            "metric": METRIC, "value": round(m["value"], 3), "unit": UNIT, "n_gpus": world, "steps": Kst,
+            "warmup": W, "ms_per_step": round(m["ms"], 4), "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32 (f64 accumulation)", "data": "synthetic (seeded LiDAR scans)",
             "config": {
-                "workload": f"{cfg.name}: {args.variant} steady-state frame, 256x256x32 voxels @0.1 m, "
-                            f"P={P}, B={B}, {cfg.n_points} points/scan, ego motion, 10 Hz",
+                "workload": workload_name(cfg, args.variant),
                 "voxels": C_, "particles": P, "new_born": B, "points_per_frame": cfg.n_points,
                 "parallelism": f"replicas x{world} (independent scenes)",
                 "l2": "state > L2 (about 1 GB of particle/cell arrays touched per frame)",
                 "graph": True, "evidence_tiling": "autotuned (k3dom_autotune) during warm-up",
             },
-            "e2e": {"value": round(e2e_fps, 3), "unit": UNIT, "h2d_bytes_per_step": int(cfg.n_points * 12),
+            "e2e": {"value": round(m["e2e_fps"], 3), "unit": UNIT, "h2d_bytes_per_step": int(cfg.n_points * 12),
                     "d2h_bytes_per_step": int(C_ * 4),
                     "path": "k3dom_update_grid (synchronous) with the (N, 3) scan in pinned host memory; the "
-                            "frame's occupancy (occ_mean, one float per voxel) lands in pinned host memory "
+                            "frame's occupancy (one float per voxel) lands in pinned host memory "
                             "through k3dom_set_output; host clock around every frame"},
-            "gpu_launches": launches * Kst,
-            "clocks": clocks,
-            "roofline": {
-                "kernel": ("k_dsgrid (DS measurement grid + fused Dempster update)" if ds else
-                           "k_bgki (sparse BGKI evidence + fused cell update)"),
-                "bound": "fp32", "achieved": round(achieved_tflops, 3), "peak": round(NOMINAL_FP32_TFLOPS, 1),
-                "unit": "TFLOP/s", "frac": round(achieved_tflops / NOMINAL_FP32_TFLOPS, 4), "traffic": traffic,
-                "peak_source": "nominal FP32 (148 SMs x 128 lanes x 2 x 1.965 GHz); no measured FP32 peak",
-                "work": (f"{n_evals:.4g} accepted neighbours x {flop_per} FLOP per frame" if ds else
-                         f"{n_evals:.4g} in-support kernel evaluations x {flop_per} FLOP per frame"),
-                "launch_ms": round(ev_ms, 4),
-                "note": ("SIMT-issue bound: frac counts only in-support evaluations x FLOP; the lanes outside "
-                         "a ray's support, the FP64 pair set-up and the fixed-point rounding are the rest"),
-                "ncu_issue": issue,
-            },
+            "gpu_launches": m["launches"] * Kst,
+            "clocks": m["clocks"],
+            "roofline": evidence_roofline(m, args.variant),
             "roofline_hbm": {
                 "kernels": "particle stages (predict, sort, gather+sums, reweight, births, resampling)",
                 "bound": "hbm", "achieved": round(part_bytes / (part_ms * 1e-3) / 1e9, 1), "peak": hbm_peak,
@@ -421,20 +477,33 @@ def run_ours(args):
                 "peak_source": peak_src, "algorithmic_bytes": int(part_bytes), "time_ms": round(part_ms, 4),
             },
             "stage_ms": {k: round(v, 4) for k, v in stage.items()},
-            "evidence_lists": {k: diag_after[k] for k in ("ray_list_entries", "ray_list_capacity", "work_items",
-                                                           "kernel_evaluations")},
+            "stage_roofline": {"peak_gbs": hbm_peak, "peak_source": peak_src,
+                               **stage_roofline(stage, P, B, C_, cfg.n_points, hbm_peak)},
+            "evidence_lists": {k: m["diag"][k] for k in ("ray_list_entries", "ray_list_capacity", "work_items",
+                                                          "kernel_evaluations")},
             "tuning": {"tile_rule": ["by-size", "8x8x4", "16x16x4", "16x16x8"][tuning["tile_rule"]],
                        "chunk": tuning["chunk"], "candidate_ms": [round(x, 3) for x in tuning["candidate_ms"]]},
         }
+        if ds_m is not None:
+            out["ds_frame"] = {
+                "workload": workload_name(ds_cfg, "dsphdmib"), "unit": UNIT,
+                "value": round(ds_m["value"], 3), "ms_per_step": round(ds_m["ms"], 4),
+                "e2e": round(ds_m["e2e_fps"], 3), "gpu_launches_per_frame": ds_m["launches"],
+                "stage_ms": {k: round(v, 4) for k, v in ds_m["stage"].items()},
+                "roofline": evidence_roofline(ds_m, "dsphdmib"),
+                "stage_roofline": stage_roofline(ds_m["stage"], ds_m["P"], ds_m["B"], ds_m["C"], ds_cfg.n_points,
+                                                 hbm_peak),
+                "tuning": {"tile_rule": ["by-size", "8x8x4", "16x16x4", "16x16x8"][ds_m["tuning"]["tile_rule"]],
+                           "chunk": ds_m["tuning"]["chunk"]},
+            }
         if batch_res is not None:
             out["batched"] = batch_res
         if world == 1 and not args.no_grad:
-            out["grad_step"] = run_grad_step(args, local, frame_ms=ms_max)
+            out["grad_step"] = run_grad_step(args, local, frame_ms=m["ms"])
         if world == 1 and not args.no_cpu_baseline:
-            fps, note, cores, n = cpu_oracle_frames(cfg, args.variant, frames, 1, 0, budget_s=60.0)
+            fps, note, cores, n = cpu_oracle_frames(cfg, args.variant, m["frames"], 1, 0, budget_s=60.0)
             out["cpu_baseline"] = {"value": round(fps, 5), "unit": UNIT, "cores": cores, "kind": "port",
                                    "sample": note}
-    dom.close()
     if dist is not None:
         dist.destroy_process_group()
     if out is not None:
@@ -455,9 +524,7 @@ def run_reference_cpu(args):
         "steps": n, "warmup": done.get("warmup", args.warmup), "ms_per_step": round(1000.0 / fps, 2),
         "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded LiDAR scans)",
-        "config": {"workload": f"{cfg.name}: {args.variant} steady-state frame, 256x256x32 voxels @0.1 m, "
-                               f"P={cfg.params['particle_count']}, B={cfg.params['new_born_particle_count']}, "
-                               f"{cfg.n_points} points/scan", "parallelism": "CPU"},
+        "config": {"workload": workload_name(cfg, args.variant), "parallelism": "CPU"},
         "cpu_baseline": {"value": round(fps, 5), "unit": UNIT, "cores": cores, "kind": "port",
                          "sample": note + "; the reference has no CPU implementation of the update"},
         "e2e": {"value": round(fps, 5), "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
@@ -497,8 +564,9 @@ def run_reference_gpu(args):
     print(json.dumps({"impl": "reference-gpu", "metric": METRIC, "value": round(fps, 4), "unit": UNIT,
                       "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
                       "ms_per_step": round(1000 / fps, 3), "higher_is_better": True,
-                      "config": {"workload": f"{cfg.name}: {args.variant} steady-state frame, reference CUDA "
-                                             "(its own updateGrid, host vectors in, synchronising)"}}), flush=True)
+                      "config": {"workload": workload_name(cfg, args.variant),
+                                 "path": "the reference's own CUDA updateGrid (host vectors in, synchronising)"}}),
+          flush=True)
 
 
 def run_batch(args, local: int = 0, rank: int = 0, world: int = 1, dist=None) -> dict:
@@ -678,14 +746,18 @@ def run_grad_step(args, local: int = 0, frame_ms: float | None = None) -> dict:
 
 
 def run_profile_case(args):
-    """A mid-size scene for ncu captures (state > L2, well under a few GB): 128x128x32 voxels at
-    0.1 m, P=1,048,576, B=262,144, 60,000 points; the first frame plus `--steps` frames."""
+    """Scenes for ncu captures, eager frames (no graph), the first frame plus `--steps` frames.
+    medium: 128x128x32 voxels at 0.1 m, P=1,048,576, B=262,144, 60,000 points (state > L2, a few
+    hundred MB on the device). config1: the benchmark's own scene (256x256x32, P=4,194,304,
+    B=1,048,576, 120,000 points; about 1.5 GB on the device) with the tiling given by
+    --profile-tile-rule/--chunk."""
     import k3dom_b200 as K
     from k3dom_b200 import scene
     cfg = scene.config1(seed=5, variant=args.variant)
-    cfg.params.update(size=12.8, particle_count=1 << 20, new_born_particle_count=1 << 18, max_points=60000)
-    cfg.n_points = 60000
-    cfg.scene.max_range = 12.8
+    if args.profile_case == "medium":
+        cfg.params.update(size=12.8, particle_count=1 << 20, new_born_particle_count=1 << 18, max_points=60000)
+        cfg.n_points = 60000
+        cfg.scene.max_range = 12.8
     p = K.make_params(args.variant, **cfg.params)
     dom = K.DOM(p, args.variant)
     if args.profile_tile_rule is not None:
@@ -707,12 +779,13 @@ def main(argv=None):
     ap.add_argument("--impl", choices=["ours", "reference", "reference-gpu"], default="ours")
     ap.add_argument("--variant", choices=["k3dom", "dsphdmib"], default="k3dom")
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--profile-case", choices=["medium"], default=None,
+    ap.add_argument("--profile-case", choices=["medium", "config1"], default=None,
                     help="run a mid-size scene for profiler captures instead of the benchmark")
     ap.add_argument("--workload", choices=["frame", "batch", "grad"], default="frame",
                     help="batch: only the batched-vs-plain line (16 scenes); grad: only the gradient step")
     ap.add_argument("--no-batch", action="store_true", help="skip the batched-vs-plain measurement")
     ap.add_argument("--no-grad", action="store_true", help="skip the gradient-step measurement")
+    ap.add_argument("--no-ds", action="store_true", help="skip the DS-PHD/MIB frame measured beside K3DOM")
     ap.add_argument("--tile-rule", type=int, default=None,
                     help="fixed evidence tile rule instead of autotuning (0 by size, 1 8x8x4, 2 16x16x4, 3 16x16x8)")
     ap.add_argument("--chunk", type=int, default=1024,

@@ -317,6 +317,10 @@ typedef struct k3dom_tuning {
     int32_t tile_rule, chunk, tuned, tuning, candidates, evidence_blocks;
     float best_ms;
     float candidate_ms[K3DOM_TUNE_MAX_CANDIDATES]; /* evidence stage time of each candidate */
+    /* evidence_blocks: CTAs of the K3DOM evidence launch, or of the DS final (update) pass;
+     * evidence_count_blocks: CTAs of the DS count pass (0 for K3DOM). Both grids are
+     * persistent, one CTA per resident slot of the build that runs. */
+    int32_t evidence_count_blocks;
 } k3dom_tuning;
 k3dom_status k3dom_autotune(k3dom_handle* h, int enabled);
 k3dom_status k3dom_get_tuning(k3dom_handle* h, k3dom_tuning* out);
@@ -363,9 +367,15 @@ k3dom_status k3dom_bgki_backward(k3dom_calib* c, const float* theta, float grad_
  * `stream`, a cudaStream_t or NULL) that allocates no memory: its scratch is a fixed 256 KiB
  * array inside the library on each GPU. For callers that may not allocate device memory at
  * run time. The sum is the one the update uses for birth slots and ancestors: each prefix is
- * the correctly rounded exact sum. n <= 33,554,432 (else K3DOM_ERR_CAPACITY). Calls share the
- * scratch: calls that overlap on the GPU race. The first call on a device looks up the
- * scratch address; make it before any stream capture. No counterpart in the reference. */
+ * the correctly rounded exact sum, for finite inputs in [0, 2^23) (-0 counts as 0; inputs
+ * below 2^-56 enter truncated to a multiple of 2^-80). Any other element (negative, NaN,
+ * infinite, >= 2^23) is refused on the device: out[i] is NaN from the first such element on
+ * (the call does not synchronise, so this cannot be a status). n <= 33,554,432 (else
+ * K3DOM_ERR_CAPACITY, nothing enqueued). Calls share the scratch: calls that overlap on the GPU
+ * race. The first call in each CUDA context looks up the scratch address; make it before any
+ * stream capture. Its launches are not counted in any handle's launch figures, and a launch
+ * failure returns K3DOM_ERR_CUDA without consuming an unrelated earlier CUDA error. No
+ * counterpart in the reference. */
 k3dom_status k3dom_exact_prefix_sum_noalloc(const float* in, float* out, int64_t n, void* stream);
 
 const char* k3dom_status_string(k3dom_status s);

@@ -150,7 +150,6 @@ struct k3dom_handle {
     bool births_done = false;
     int launches_per_frame = 0;
     int launches_upload = 0;  // kernels of the last frame's point upload (de-interleaving)
-    int ds_grid = 0;
     int ds_sized_chunk = 0;  // chunk the DS count buffer was sized for
 
     // evidence tuning
@@ -661,7 +660,7 @@ cudaError_t enq_binning(k3dom_handle* h, cudaStream_t s) {
 cudaError_t enq_evidence(k3dom_handle* h, bool first_frame) {
     const Batch bt = h->batch();
     if (h->ds())
-        return launch_ds_evidence(bt, h->rb, h->cells(), h->cw, first_frame, h->status, h->ds_grid, h->st);
+        return launch_ds_evidence(bt, h->rb, h->cells(), h->cw, first_frame, h->status, h->st);
     return launch_k3dom_evidence(bt, h->rb, h->cells(), h->cw, first_frame, h->status, h->st);
 }
 
@@ -890,7 +889,6 @@ k3dom_status k3dom_batch_create(const k3dom_params* params, int32_t n_scenes, k3
     if ((e = cudaGetDeviceProperties(&prop, device))) return bail(e);
     h->num_sms = prop.multiProcessorCount;
     if ((e = sort_init()) || (e = evidence_init())) return bail(e);
-    h->ds_grid = h->num_sms * 4;
 
     // scene ranges
     int P = 0, B = 0, C = 0;
@@ -1306,7 +1304,12 @@ k3dom_status k3dom_get_tuning(k3dom_handle* h, k3dom_tuning* out) {
     out->best_ms = h->tune_best_ms;
     for (int k = 0; k < kTuneCount && k < (int)h->tune_ms.size() && k < K3DOM_TUNE_MAX_CANDIDATES; ++k)
         out->candidate_ms[k] = h->tune_ms[k];
-    out->evidence_blocks = h->ds() ? h->ds_grid : k3dom_evidence_blocks(h->rb.chunk);
+    if (h->ds()) {
+        k3dom_ds_evidence_blocks(&out->evidence_count_blocks, &out->evidence_blocks);
+    } else {
+        out->evidence_blocks = k3dom_evidence_blocks(h->rb.chunk);
+        out->evidence_count_blocks = 0;
+    }
     return K3DOM_OK;
 }
 

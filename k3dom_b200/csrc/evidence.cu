@@ -1612,19 +1612,36 @@ cudaError_t launch_k3dom_evidence(const Batch& bt, RayBuffers& rb, CellState cs,
     return cudaGetLastError();
 }
 
-cudaError_t launch_ds_evidence(const Batch& bt, RayBuffers& rb, CellState cs, CellWork cw, bool first_frame,
-                               DevStatus* status, int grid, cudaStream_t st) {
-    if (rb.chunk < 32 || rb.chunk > kChunk) return cudaErrorInvalidValue;
-    EvArgs A = make_args(bt, rb, cs, cw, first_frame, status);
-    // the count pass fits 5 CTAs per SM (47 registers), the final pass 4
-    int dev = 0, sms = 148, per_sm = 1;
+// The DS launches are persistent too: the count pass and the final pass each get one CTA per
+// resident slot (the count pass fits 5 CTAs per SM at 47 registers, the final pass 4).
+struct DsLaunch {
+    int count_blocks, final_blocks;
+};
+
+static DsLaunch ds_launch() {
+    int dev = 0, sms = 148, per_count = 1, per_final = 1;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_dsgrid<true>, kEvThreads, 0);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_count, k_dsgrid<true>, kEvThreads, 0);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_final, k_dsgrid<false>, kEvThreads, 0);
+    return DsLaunch{sms * std::max(1, per_count), sms * std::max(1, per_final)};
+}
+
+void k3dom_ds_evidence_blocks(int* count_blocks, int* final_blocks) {
+    const DsLaunch L = ds_launch();
+    *count_blocks = L.count_blocks;
+    *final_blocks = L.final_blocks;
+}
+
+cudaError_t launch_ds_evidence(const Batch& bt, RayBuffers& rb, CellState cs, CellWork cw, bool first_frame,
+                               DevStatus* status, cudaStream_t st) {
+    if (rb.chunk < 32 || rb.chunk > kChunk) return cudaErrorInvalidValue;
+    EvArgs A = make_args(bt, rb, cs, cw, first_frame, status);
+    const DsLaunch L = ds_launch();
     ++g_launches;
-    k_dsgrid<true><<<sms * std::max(1, per_sm), kEvThreads, 0, st>>>(A);
+    k_dsgrid<true><<<L.count_blocks, kEvThreads, 0, st>>>(A);
     ++g_launches;
-    k_dsgrid<false><<<grid, kEvThreads, 0, st>>>(A);
+    k_dsgrid<false><<<L.final_blocks, kEvThreads, 0, st>>>(A);
     return cudaGetLastError();
 }
 

@@ -13,6 +13,7 @@
 #include <cuda_runtime.h>
 
 #include "common.cuh"
+#include "fixed128.cuh"
 #include "internal.h"
 #include "scan.cuh"
 
@@ -24,37 +25,6 @@ namespace k3dom {
 constexpr int kExThreads = 256;
 constexpr int kExItems = 8;
 constexpr int kExTile = kExThreads * kExItems;
-constexpr int kFracBits = 80;
-
-// float (>= 0) -> fixed point with kFracBits fractional bits. Negative or non-finite
-// inputs contribute 0 (they cannot occur for weights and born masses).
-__device__ __forceinline__ u128 to_fixed(float f) {
-    uint32_t b = __float_as_uint(f);
-    if (b & 0x80000000u) return 0;
-    uint32_t e = b >> 23, frac = b & 0x7FFFFFu;
-    if (e == 0xFFu) return 0;
-    uint32_t m = e ? (frac | 0x800000u) : frac;
-    int sh = (e ? (int)e : 1) - 150 + kFracBits;  // value = m * 2^(e-150)
-    if (sh >= 0) {
-        if (sh > 127 - 24) return 0;  // out of range (>= 2^47); never reached by masses
-        return (u128)m << sh;
-    }
-    if (sh <= -32) return 0;
-    return (u128)(m >> (-sh));
-}
-
-// Round-to-nearest-even float of v * 2^-kFracBits.
-__device__ __forceinline__ float from_fixed(u128 v) {
-    if (v == 0) return 0.0f;
-    uint64_t hi = (uint64_t)(v >> 64), lo = (uint64_t)v;
-    int lz = hi ? __clzll((long long)hi) : 64 + __clzll((long long)lo);
-    u128 n = v << lz;
-    uint64_t top = (uint64_t)(n >> 64);
-    if ((uint64_t)n != 0) top |= 1ull;  // sticky
-    float f = __ull2float_rn(top);
-    return ldexpf(f, 64 - lz - kFracBits);
-}
-
 struct TwoSeg {
     const float* a;
     long na;

@@ -136,9 +136,11 @@ cudaError_t build_ray_lists(const Batch& bt, const float* xs, const float* ys, c
 cudaError_t launch_k3dom_evidence(const Batch& bt, RayBuffers& rb, CellState cs, CellWork cw, bool first_frame,
                                   DevStatus* status, cudaStream_t st);
 cudaError_t launch_ds_evidence(const Batch& bt, RayBuffers& rb, CellState cs, CellWork cw, bool first_frame,
-                               DevStatus* status, int grid, cudaStream_t st);
+                               DevStatus* status, cudaStream_t st);
 // CTAs of the K3DOM evidence launch for a chunk size (persistent grid).
 int k3dom_evidence_blocks(int chunk);
+// CTAs of the DS count pass and final pass (persistent: one per resident slot of each build).
+void k3dom_ds_evidence_blocks(int* count_blocks, int* final_blocks);
 long ds_count_bytes(long items);
 cudaError_t evidence_init();
 // Host: the sparse-kernel table for sigma, every value multiplied by scale: 512 intervals and a

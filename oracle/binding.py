@@ -260,6 +260,88 @@ def slot_bounds(cum, v):
     return st, en
 
 
+# ---------------------------------------------------------------- map shift and map export
+def map_move(sensor, center, sensor_off, res):
+    """DOM_c::updatePose's integer move (src/common/dom.cu:125-127): static_cast<int> of
+    (sensor - centre - offset) / resolution, every operation in FP32."""
+    s, c, o = f32(sensor), f32(center), f32(sensor_off)
+    q = ((s - c) - o) / np.float32(res)
+    return np.trunc(q).astype(np.int64)
+
+
+def map_shift_fires(move, thresh):
+    """The shift condition of src/common/dom.cu:129."""
+    return bool(np.any(np.abs(move) >= int(thresh)))
+
+
+def shift_gridcells(cells, move, G, Gz, prior_free, prior_static, prior_dynamic, prior_occ):
+    """initGridCellsKernel (src/common/kernel/init.cu:20-34) followed by moveMapKernel
+    (src/common/kernel/ego_motion_compensation.cu:21-41) on a 68-byte GridCell array: a cell
+    whose source x+move lies inside the grid takes the whole source record; every other cell
+    keeps its own record with the priors, start/end = -1, likelihood 1 and p_A 0."""
+    out = np.array(cells, copy=True)
+    C_ = G * G * Gz
+    idx = np.arange(C_, dtype=np.int64)
+    x, y, z = idx % G, (idx % (G * G)) // G, idx // (G * G)
+    nx, ny, nz = x + int(move[0]), y + int(move[1]), z + int(move[2])
+    ok = (nx >= 0) & (nx < G) & (ny >= 0) & (ny < G) & (nz >= 0) & (nz < Gz)
+    init = ~ok
+    out["free_mass"][init] = np.float32(prior_free)
+    out["static_mass"][init] = np.float32(prior_static)
+    out["dynamic_mass"][init] = np.float32(prior_dynamic)
+    out["occ_mass"][init] = np.float32(prior_occ)
+    out["start_idx"][init] = -1
+    out["end_idx"][init] = -1
+    out["likelihood"][init] = np.float32(1.0)
+    out["p_A"][init] = np.float32(0.0)
+    src = (nx + G * ny + G * G * nz)[ok]
+    out[ok] = cells[src]
+    return out
+
+
+def shift_positions(pos, move):
+    """moveParticlesKernel (src/common/kernel/ego_motion_compensation.cu:12-18): pos -= move in
+    FP32."""
+    return (f32(pos) - np.asarray(move, np.float32)[None, :]).astype(np.float32)
+
+
+def index_to_coord(idx, G, res, size, size_z, center):
+    """DOM_c::indexToCoord{X,Y,Z} (include/common/dom.h:70-81), FP32 in the written order."""
+    idx = np.asarray(idx, np.int64)
+    r = np.float32(res)
+    c = f32(center)
+    hx = np.float32(size) / np.float32(2.0)
+    hz = np.float32(size_z) / np.float32(2.0)
+    ix = (idx % G).astype(np.float32)
+    iy = ((idx % (G * G)) // G).astype(np.float32)
+    iz = (idx // (G * G)).astype(np.float32)
+    x = ((ix + np.float32(0.5)) * r - hx) + c[0]
+    y = ((iy + np.float32(0.5)) * r - hx) + c[1]
+    z = ((iz + np.float32(0.5)) * r - hz) + c[2]
+    return np.stack([x, y, z], 1).astype(np.float32)
+
+
+def mappoints(cells, G, res, size, size_z, center):
+    """The node's /map_data point per cell (src/k3dom/k3dom_node.cpp:161-184): indexToCoord,
+    velocity x resolution, occ_mean, dyn_mean and total_mass (include/common/dom_types.h:47-49),
+    dyn_aug = 1.1. Returns (C, 10) float32 in MapPoint's field order."""
+    C_ = cells.shape[0]
+    out = np.empty((C_, 10), np.float32)
+    out[:, 0:3] = index_to_coord(np.arange(C_), G, res, size, size_z, center)
+    r = np.float32(res)
+    out[:, 3] = cells["mean_x_vel"] * r
+    out[:, 4] = cells["mean_y_vel"] * r
+    out[:, 5] = cells["mean_z_vel"] * r
+    f, s, d = cells["free_mass"], cells["static_mass"], cells["dynamic_mass"]
+    with np.errstate(divide="ignore", invalid="ignore"):
+        tm = ((f + s) + d).astype(np.float32)
+        out[:, 6] = (s + d) / tm
+        out[:, 7] = d / tm
+    out[:, 8] = tm
+    out[:, 9] = np.float32(1.1)
+    return out
+
+
 # ---------------------------------------------------------------- reference harness
 GRIDCELL_DTYPE = np.dtype([
     ("start_idx", "<i4"), ("end_idx", "<i4"), ("mu_A", "<f4"), ("mu_UA", "<f4"), ("w_A", "<f4"),
@@ -285,6 +367,7 @@ class Reference:
         sig = {
             "ref_create": (V, [P, C.c_uint64]), "ref_destroy": (None, [V]), "ref_sizes": (None, [V, _I]),
             "ref_update_pose": (None, [V, C.c_float, C.c_float, C.c_float]), "ref_sensor_rel": (None, [V, _F]),
+            "ref_center": (None, [V, _F]), "ref_index_to_coord": (None, [V, _I, C.c_longlong, _F]),
             "ref_set_draws": (None, [V, C.c_uint64, C.c_uint32, C.c_uint32, C.c_uint32]),
             "ref_particle_prediction": (None, [V, C.c_float]), "ref_particle_assignment": (None, [V]),
             "ref_occupancy": (None, [V, C.c_float, _F, _F, _F, C.c_int]), "ref_update_persistent": (None, [V]),
@@ -341,6 +424,17 @@ class Reference:
         s = np.empty(3, np.float32)
         self.lib.ref_sensor_rel(self.h, s)
         return s
+
+    def center(self):
+        c = np.empty(3, np.float32)
+        self.lib.ref_center(self.h, c)
+        return c
+
+    def index_to_coord(self, idx):
+        idx = np.ascontiguousarray(idx, np.int32)
+        out = np.empty((idx.size, 3), np.float32)
+        self.lib.ref_index_to_coord(self.h, idx, idx.size, out)
+        return out
 
     def predict(self, frame, dt):
         self.draws(frame, 1, 6)

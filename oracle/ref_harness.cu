@@ -110,6 +110,26 @@ void ref_update_pose(void* h, float x, float y, float z) { static_cast<RefDOM*>(
 
 void ref_sensor_rel(void* h, float* s) { static_cast<RefDOM*>(h)->sensor_rel(s); }
 
+// DOM_c::getCenterPosition{X,Y,Z} (include/common/dom.h:62-64): the map centre that updatePose's
+// shift rule moves (src/common/dom.cu:125-154).
+void ref_center(void* h, float* c) {
+    RefDOM* d = static_cast<RefDOM*>(h);
+    c[0] = d->getCenterPositionX();
+    c[1] = d->getCenterPositionY();
+    c[2] = d->getCenterPositionZ();
+}
+
+// DOM_c::indexToCoord{X,Y,Z} (include/common/dom.h:70-81) for n cell indices, host side, as the
+// node's publish_mapdata calls them (src/k3dom/k3dom_node.cpp:166-168).
+void ref_index_to_coord(void* h, const int* idx, long long n, float* xyz) {
+    RefDOM* d = static_cast<RefDOM*>(h);
+    for (long long k = 0; k < n; ++k) {
+        xyz[3 * k + 0] = d->indexToCoordX(idx[k]);
+        xyz[3 * k + 1] = d->indexToCoordY(idx[k]);
+        xyz[3 * k + 2] = d->indexToCoordZ(idx[k]);
+    }
+}
+
 void ref_set_draws(void* h, unsigned long long seed, unsigned frame, unsigned stage, unsigned dpi) {
     RefDOM* d = static_cast<RefDOM*>(h);
     const int n = d->states();

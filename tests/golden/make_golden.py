@@ -1,11 +1,12 @@
-"""Generate the golden fixtures tests/golden/{k3dom,dsphdmib}_small.npz.
+"""Generate the golden fixtures tests/golden/{k3dom,dsphdmib}_small.npz and
+tests/golden/k3dom_shift_small.npz.
 
 Runs the reference's own CUDA update (oracle/_ref/libref_*.so, built from the reference's
 sources by oracle/build_ref.sh) stage by stage on a small seeded synthetic scene, with the
 Philox draws injected through the curand shim, and records every stage's inputs and outputs.
 Requires a GPU; run from the repository root:
 
-    python tests/golden/make_golden.py [outdir]
+    python tests/golden/make_golden.py [outdir] [--only shift]
 
 The fixtures are committed; the CPU tests (tests/test_oracle_golden.py) check the oracle
 against them.
@@ -120,11 +121,78 @@ def run(variant: str, out: Path) -> None:
     print(f"wrote {out} ({out.stat().st_size / 1e6:.2f} MB)")
 
 
+SHIFT_FRAMES = 7
+SHIFT_EGO = 6.0  # m/s: 0.6 m = 3 voxels per frame at 0.2 m, so the 5-voxel threshold fires every 2nd frame
+
+
+def run_shift(out: Path) -> None:
+    """Ego motion: the sensor moves 0.6 m per frame, so DOM_c::updatePose shifts the map
+    (src/common/dom.cu:111-158; moveMapKernel / moveParticlesKernel,
+    src/common/kernel/ego_motion_compensation.cu:12-41) every other frame. Recorded around each
+    updatePose: the map centre, the 68-byte cells and the particle positions before and after;
+    and the prediction that follows (its input is the shifted set)."""
+    variant = "k3dom"
+    cfg = scene.small(seed=SEED + 4, variant=variant, ego=SHIFT_EGO, **SIZES)
+    cfg.params["seed"] = 4321
+    p = make_params(variant, **cfg.params)
+    ref = Reference(p, variant)
+    rec = {"seed": np.int64(p.seed), "G": np.int32(ref.G), "Gz": np.int32(ref.Gz), "P": np.int32(ref.P),
+           "B": np.int32(ref.B), "params": np.frombuffer(bytes(p), np.uint8)}
+    t_prev = None
+    for f in range(SHIFT_FRAMES):
+        t = 0.1 + f * cfg.dt
+        s, pts = cfg.scene.scan(f, t, cfg.n_points)
+        rec[f"f{f}_pose"] = np.asarray(s, np.float32)
+        rec[f"f{f}_center_before"] = ref.center()
+        if f > 0:
+            rec[f"f{f}_cells_before"] = ref.cells()
+            rec[f"f{f}_pos_before"] = ref.particles(0)["pos"]
+        ref.update_pose(*s)
+        rec[f"f{f}_center_after"] = ref.center()
+        if f == 0:
+            ref.init_particles(f, pts)
+            ref.finish(t, False)
+        else:
+            rec[f"f{f}_cells_after"] = ref.cells()
+            a = ref.particles(0)
+            rec[f"f{f}_pos_after"] = a["pos"]
+            for k in ("vel", "weight"):
+                rec[f"f{f}_pred_in_{k}"] = a[k]
+            idx = np.arange(ref.C, dtype=np.int32)
+            rec[f"f{f}_coord_idx"] = idx
+            rec[f"f{f}_coords"] = ref.index_to_coord(idx)
+            dt = np.float32(t) - np.float32(t_prev)
+            rec[f"f{f}_dt"] = np.float32(dt)
+            rec[f"f{f}_normals"] = debug_draws(p.seed, f, 1, 0, ref.P)
+            ref.predict(f, dt)
+            out_p = ref.particles(0)
+            for k in ("pos", "vel", "weight", "cell"):
+                rec[f"f{f}_pred_out_{k}"] = out_p[k]
+            ref.assign()
+            ref.occupancy(dt, pts)
+            ref.persistent()
+            ref.births(f)
+            ref.moments()
+            ref.resampling(f)
+            ref.finish(t, True)
+        t_prev = t
+    ref.close()
+    np.savez_compressed(out, **rec)
+    print(f"wrote {out} ({out.stat().st_size / 1e6:.2f} MB)")
+
+
 def main(argv):
-    outdir = Path(argv[1]) if len(argv) > 1 else Path(__file__).resolve().parent
+    args = [a for a in argv[1:] if not a.startswith("--")]
+    only = argv[argv.index("--only") + 1] if "--only" in argv else None
+    if only:
+        args = [a for a in args if a != only]
+    outdir = Path(args[0]) if args else Path(__file__).resolve().parent
     outdir.mkdir(parents=True, exist_ok=True)
-    for v in ("k3dom", "dsphdmib"):
-        run(v, outdir / f"{v}_small.npz")
+    if only in (None, "small"):
+        for v in ("k3dom", "dsphdmib"):
+            run(v, outdir / f"{v}_small.npz")
+    if only in (None, "shift"):
+        run_shift(outdir / "k3dom_shift_small.npz")
     return 0
 
 

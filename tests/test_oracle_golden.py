@@ -416,3 +416,76 @@ def test_ds_update_bit_exact_and_fp64():
         norm = sw32[srt["cell"]] > 1.0
         w[norm] = w[norm] / sw32[srt["cell"]][norm]
         np.testing.assert_array_equal(w, f[f"f{fr}_sorted_after_occ_weight"])
+
+
+# ------------------------------------------------------------------ ego-motion map shift
+def load_shift():
+    path = GOLD / "k3dom_shift_small.npz"
+    if not path.exists():
+        pytest.skip(f"{path.name} not generated")
+    f = np.load(path)
+    return f, N.Params.from_buffer_copy(f["params"].tobytes())
+
+
+def test_map_shift_matches_reference():
+    """DOM_c::updatePose with ego motion (src/common/dom.cu:111-158): the integer move, the shift
+    condition, the new map centre, the shifted 68-byte cells (initGridCellsKernel +
+    moveMapKernel) and the shifted particle positions (moveParticlesKernel) of the oracle equal
+    the reference's, bit for bit, on every frame of a 0.6 m/frame sequence; frames below the
+    threshold leave cells, particles and centre untouched."""
+    f, p = load_shift()
+    G, Gz = int(f["G"]), int(f["Gz"])
+    off = np.array([p.sensor_off_x, p.sensor_off_y, p.sensor_off_z], np.float32)
+    n_shift = 0
+    moves = []
+    for fr in range(1, max(frames(f)) + 1):
+        c0, c1 = f[f"f{fr}_center_before"], f[f"f{fr}_center_after"]
+        mv = O.map_move(f[f"f{fr}_pose"], c0, off, p.resolution)
+        cells0, cells1 = f[f"f{fr}_cells_before"], f[f"f{fr}_cells_after"]
+        pos0, pos1 = f[f"f{fr}_pos_before"], f[f"f{fr}_pos_after"]
+        if O.map_shift_fires(mv, p.map_shift_thresh):
+            n_shift += 1
+            moves.append(mv)
+            exp_c = (c0 + mv.astype(np.float32) * np.float32(p.resolution)).astype(np.float32)
+            np.testing.assert_array_equal(c1, exp_c)
+            exp = O.shift_gridcells(cells0, mv, G, Gz, p.prior_free, p.prior_static, p.prior_dynamic, p.prior_occ)
+            assert exp.tobytes() == cells1.tobytes(), f"frame {fr}: shifted cells"
+            np.testing.assert_array_equal(O.shift_positions(pos0, mv), pos1, err_msg=f"frame {fr}: positions")
+        else:
+            np.testing.assert_array_equal(c1, c0)
+            assert cells0.tobytes() == cells1.tobytes()
+            np.testing.assert_array_equal(pos0, pos1)
+    assert n_shift >= 2, "the sequence must shift the map at least twice"
+    assert any(np.any(m < 0) for m in moves) or any(np.any(m > 0) for m in moves)
+
+
+def test_prediction_after_shift_bit_exact():
+    """The shift folded into prediction: predicting the unshifted set with the pending move
+    subtracted first (orc_predict's shift argument, as the library's k_predict does) equals the
+    reference's moveParticlesKernel followed by predictKernel."""
+    f, p = load_shift()
+    G, Gz = int(f["G"]), int(f["Gz"])
+    off = np.array([p.sensor_off_x, p.sensor_off_y, p.sensor_off_z], np.float32)
+    seen = 0
+    for fr in range(1, max(frames(f)) + 1):
+        mv = O.map_move(f[f"f{fr}_pose"], f[f"f{fr}_center_before"], off, p.resolution)
+        fires = O.map_shift_fires(mv, p.map_shift_thresh)
+        st = {"pos": f[f"f{fr}_pos_before"], "vel": f[f"f{fr}_pred_in_vel"], "weight": f[f"f{fr}_pred_in_weight"]}
+        out = O.predict(st, f[f"f{fr}_normals"], G, Gz, float(f[f"f{fr}_dt"]), p.persistence_prob,
+                        p.stddev_process_noise_position, p.stddev_process_noise_velocity, p.init_max_velocity,
+                        shift=tuple(int(v) for v in mv) if fires else None)
+        for k in ("pos", "vel", "weight", "cell"):
+            np.testing.assert_array_equal(out[k], f[f"f{fr}_pred_out_{k}"], err_msg=f"frame {fr} {k}")
+        seen += fires
+    assert seen >= 2
+
+
+def test_mappoint_coordinates_match_reference_formula():
+    """index_to_coord restates DOM_c::indexToCoord{X,Y,Z} (include/common/dom.h:70-81); the
+    fixture's centres after each shift exercise non-zero map centres."""
+    f, p = load_shift()
+    G = int(f["G"])
+    for fr in range(1, max(frames(f)) + 1):
+        idx = f[f"f{fr}_coord_idx"]
+        got = O.index_to_coord(idx, G, p.resolution, p.size, p.size_z, f[f"f{fr}_center_after"])
+        np.testing.assert_array_equal(got, f[f"f{fr}_coords"])

@@ -44,16 +44,56 @@ def test_noalloc_prefix_sum_matches_update():
         bw = dom.get_particles("birth")["weight"]
         joint = np.concatenate([srt, bw]).astype(np.float32)
         stream = torch.cuda.current_stream().cuda_stream
-        for src, expected in ((born, born_cum), (joint, joint_cum)):  # two calls in a row
-            d_in = torch.from_numpy(src).cuda()
-            d_out = torch.full_like(d_in, float("nan"))
-            torch.cuda.synchronize()
+        inputs = [(torch.from_numpy(src).cuda(), expected) for src, expected in ((born, born_cum), (joint, joint_cum))]
+        outs = [torch.full_like(d_in, float("nan")) for d_in, _ in inputs]
+        torch.cuda.synchronize()
+        for k, ((d_in, expected), d_out) in enumerate(zip(inputs, outs)):  # two calls in a row
+            free0 = torch.cuda.mem_get_info()[0]
             st = lib.k3dom_exact_prefix_sum_noalloc(_ptr(d_in), _ptr(d_out), d_in.numel(), C.c_void_p(stream))
             assert st == 0, N.STATUS_NAMES.get(st)
             torch.cuda.synchronize()
+            if k == 1:
+                # the first call has looked up the scratch and loaded the kernels: the second
+                # one takes no device memory at all
+                assert torch.cuda.mem_get_info()[0] == free0
             np.testing.assert_array_equal(d_out.cpu().numpy(), expected)
         # beyond the fixed scratch: refused before any GPU work
         too_many = 33_554_432 + 1
-        assert lib.k3dom_exact_prefix_sum_noalloc(_ptr(d_in), _ptr(d_out), too_many, None) == 4
+        d_in, _ = inputs[0]
+        assert lib.k3dom_exact_prefix_sum_noalloc(_ptr(d_in), _ptr(outs[0]), too_many, None) == 4
     finally:
         dom.close()
+
+
+def test_noalloc_refused_elements_poison_the_rest():
+    """Outside the exact domain (finite values in [0, 2^23)) an element is refused on the
+    device: every prefix from it on is NaN, every prefix before it is the exact one."""
+    import torch
+
+    from k3dom_b200 import _native as N
+    from oracle import binding as O
+
+    lib = N.load()
+    rng = np.random.default_rng(5)
+    x = rng.uniform(0.0, 4.0, 100_000).astype(np.float32)
+    x[::97] = -0.0  # negative zero counts as zero
+    exp = O.exact_scan(x)
+    for bad_at, bad in ((70_001, np.float32(-1e-3)), (4_096, np.float32(np.nan)), (12, np.float32(np.inf)),
+                        (99_999, np.float32(2.0 ** 23))):
+        y = x.copy()
+        y[bad_at] = bad
+        d_in = torch.from_numpy(y).cuda()
+        d_out = torch.zeros_like(d_in)
+        assert lib.k3dom_exact_prefix_sum_noalloc(_ptr(d_in), _ptr(d_out), y.size, None) == 0
+        torch.cuda.synchronize()
+        got = d_out.cpu().numpy()
+        np.testing.assert_array_equal(got[:bad_at], exp[:bad_at])
+        assert np.all(np.isnan(got[bad_at:])), bad
+    # the largest value inside the domain is still exact
+    y = x.copy()
+    y[3] = np.nextafter(np.float32(2.0 ** 23), np.float32(0))
+    d_in = torch.from_numpy(y).cuda()
+    d_out = torch.zeros_like(d_in)
+    assert lib.k3dom_exact_prefix_sum_noalloc(_ptr(d_in), _ptr(d_out), y.size, None) == 0
+    torch.cuda.synchronize()
+    np.testing.assert_array_equal(d_out.cpu().numpy(), O.exact_scan(y))
