@@ -260,6 +260,13 @@ k3dom_status k3dom_get_resampling_state(k3dom_handle* h, float* joint_cum,
  * uniform). Writes count*per_item floats for items [first, first+count) of frame `frame`. */
 k3dom_status k3dom_debug_draws(uint64_t seed, int32_t frame, int32_t stage, int64_t first,
                                int64_t count, float* dst, k3dom_mem mem);
+/* The particle sort's bounded waits (test hook; no counterpart in the reference). Each pass of
+ * the sort finds the keys of earlier tiles by polling their published counts; a poll loop gives
+ * up after max_polls polls (default 1,048,576, under a second), and the frame then returns
+ * K3DOM_ERR_TIMEOUT (its results are incomplete). skip_tile >= 0 keeps that tile of the first
+ * pass from publishing its counts, so every later tile's wait runs out: how the tests see the
+ * timeout path without a hang. skip_tile = -1 restores normal operation. */
+k3dom_status k3dom_set_sort_wait(k3dom_handle* h, uint32_t max_polls, int32_t skip_tile);
 /* Sets the frame counter used to key the draws (tests align it with a reference run). */
 k3dom_status k3dom_set_frame_index(k3dom_handle* h, int32_t frame);
 

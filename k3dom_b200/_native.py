@@ -155,6 +155,7 @@ SIGNATURES = {
     "k3dom_get_resampling_state": (_ST, [_P, _P, _P, _P, C.c_int]),
     "k3dom_debug_draws": (_ST, [C.c_uint64, C.c_int32, C.c_int32, C.c_int64, C.c_int64, _P, C.c_int]),
     "k3dom_set_frame_index": (_ST, [_P, C.c_int32]),
+    "k3dom_set_sort_wait": (_ST, [_P, C.c_uint32, C.c_int32]),
     "k3dom_get_stage_times": (_ST, [_P, C.POINTER(StageTimes)]),
     "k3dom_set_timing": (_ST, [_P, C.c_int]),
     "k3dom_get_diagnostics": (_ST, [_P, C.POINTER(Diagnostics)]),

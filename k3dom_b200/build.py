@@ -23,7 +23,7 @@ OBJ_DIR = PKG / "_build"
 LIB = OUT_DIR / "libk3dom_b200.so"
 INCLUDE = PKG.parent / "include"
 
-CUDA_SOURCES = ["sort.cu", "exactscan.cu", "particles.cu", "cells.cu", "evidence.cu", "dom.cu", "noalloc.cu", "calib.cu"]
+CUDA_SOURCES = ["sort.cu", "onesweep.cu", "exactscan.cu", "particles.cu", "cells.cu", "evidence.cu", "dom.cu", "noalloc.cu", "calib.cu"]
 CXX_SOURCES = ["params.cpp"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "--extended-lambda"] + ARCH

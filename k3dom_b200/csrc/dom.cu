@@ -125,6 +125,9 @@ struct k3dom_handle {
     int2* res_br = nullptr;     // ancestor brackets of the resampling blocks
     uint32_t *hist = nullptr, *scan_tmp = nullptr;
     long hist_words = 0, scan_tmp_words = 0;
+    uint32_t* os_scratch = nullptr;  // onesweep particle sort: histograms and tile status
+    long os_words = 0;
+    SortWait sort_wait;
     CellState cs[2]{};  // cs[0] live, cs[1] spare for the map shift
     int *start2 = nullptr, *end2 = nullptr;
     CellWork cw{};
@@ -642,9 +645,9 @@ cudaError_t enq_predict(k3dom_handle* h) {
 }
 
 cudaError_t enq_assign(k3dom_handle* h) {
-    cudaError_t e = radix_sort_pairs(reinterpret_cast<const uint32_t*>(h->A.cell), nullptr, h->sorted_keys, h->perm,
-                                     h->alt_k, h->alt_v, h->P, key_bits_for(h->C), h->hist, h->hist_words,
-                                     h->scan_tmp, h->scan_tmp_words, h->st);
+    cudaError_t e = onesweep_sort_pairs(reinterpret_cast<const uint32_t*>(h->A.cell), nullptr, h->sorted_keys,
+                                        h->perm, h->alt_k, h->alt_v, h->P, key_bits_for(h->C), h->os_scratch,
+                                        h->os_words, h->status, h->sort_wait, h->st);
     if (e != cudaSuccess) return e;
     if ((e = cudaMemsetAsync(h->cw.start, 0xFF, sizeof(int) * (size_t)h->C, h->st))) return e;
     if ((e = cudaMemsetAsync(h->cw.end, 0xFF, sizeof(int) * (size_t)h->C, h->st))) return e;
@@ -888,7 +891,7 @@ k3dom_status k3dom_batch_create(const k3dom_params* params, int32_t n_scenes, k3
     cudaDeviceProp prop;
     if ((e = cudaGetDeviceProperties(&prop, device))) return bail(e);
     h->num_sms = prop.multiProcessorCount;
-    if ((e = sort_init()) || (e = evidence_init())) return bail(e);
+    if ((e = sort_init()) || (e = onesweep_init()) || (e = evidence_init())) return bail(e);
 
     // scene ranges
     int P = 0, B = 0, C = 0;
@@ -984,6 +987,8 @@ k3dom_status k3dom_batch_create(const k3dom_params* params, int32_t n_scenes, k3
     h->hist_words = std::max(radix_hist_words(P, 11), 1L);
     h->scan_tmp_words = scan_u32_tiles(h->hist_words) + 16;
     if ((e = h->alloc(&h->hist, h->hist_words)) || (e = h->alloc(&h->scan_tmp, h->scan_tmp_words))) return bail(e);
+    h->os_words = onesweep_scratch_words(P, key_bits_for(h->C));
+    if ((e = h->alloc(&h->os_scratch, h->os_words))) return bail(e);
     // separate sort scratch for the draw sort (it runs concurrently on the second stream); the
     // draw keys carry the scene index above 24 bits, so passes may be up to 11 bits wide
     {
@@ -1119,6 +1124,14 @@ static k3dom_status finish_sync(k3dom_handle* h) {
     if (h->status) e = cudaMemcpyAsync(h->status_host, h->status, sizeof(DevStatus), cudaMemcpyDeviceToHost, h->st);
     if (e == cudaSuccess) e = cudaStreamSynchronize(h->st);
     if (e != cudaSuccess) return h->fail(e);
+    if (h->status && h->status_host->sort_timeout) {
+        // the particle sort's look-back gave up (its output is incomplete): report it once
+        h->status_host->sort_timeout = 0;
+        e = cudaMemsetAsync(&h->status->sort_timeout, 0, sizeof(unsigned int), h->st);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(h->st);
+        if (e != cudaSuccess) return h->fail(e);
+        return K3DOM_ERR_TIMEOUT;
+    }
     if (h->status && h->status_host->overflow) return K3DOM_ERR_CAPACITY;
     return K3DOM_OK;
 }
@@ -1310,6 +1323,14 @@ k3dom_status k3dom_get_tuning(k3dom_handle* h, k3dom_tuning* out) {
         out->evidence_blocks = k3dom_evidence_blocks(h->rb.chunk);
         out->evidence_count_blocks = 0;
     }
+    return K3DOM_OK;
+}
+
+k3dom_status k3dom_set_sort_wait(k3dom_handle* h, uint32_t max_polls, int32_t skip_tile) {
+    if (!h || skip_tile < -1) return K3DOM_ERR_INVALID_ARGUMENT;
+    h->sort_wait.max_polls = max_polls;
+    h->sort_wait.skip_tile = skip_tile;
+    h->drop_graph();  // the captured frame holds the old arguments
     return K3DOM_OK;
 }
 

@@ -35,6 +35,21 @@ cudaError_t radix_sort_pairs_dn(const uint32_t* keys, const uint32_t* vals, uint
                                 uint32_t* scan_tmp, long scan_words, cudaStream_t st);
 cudaError_t sort_init();
 
+// onesweep.cu: the particle sort (one histogram read, then one read and write per 7-bit digit
+// with decoupled look-back). A look-back poll loop gives up after max_polls polls and sets
+// DevStatus::sort_timeout; skip_tile >= 0 keeps that tile of the first pass from publishing its
+// counts (a test hook: every later tile's wait then runs out).
+struct SortWait {
+    uint32_t max_polls = 1u << 20;
+    int skip_tile = -1;
+};
+int onesweep_plan(int key_bits, int* pass_bits);
+long onesweep_scratch_words(long n, int key_bits);
+cudaError_t onesweep_init();
+cudaError_t onesweep_sort_pairs(const uint32_t* keys, const uint32_t* vals, uint32_t* keys_out, uint32_t* vals_out,
+                                uint32_t* alt_k, uint32_t* alt_v, long n, int key_bits, uint32_t* scratch,
+                                long scratch_words, DevStatus* ds, const SortWait& wait, cudaStream_t st);
+
 // exactscan.cu: inclusive prefix sums of non-negative floats, exact in 128-bit fixed
 // point and rounded once to float.
 int exact_scan_tiles(long n);

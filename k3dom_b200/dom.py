@@ -219,6 +219,10 @@ class DOM:
     def setFrameIndex(self, frame: int) -> None:
         N.check(self._lib.k3dom_set_frame_index(self._h, int(frame)), "setFrameIndex")
 
+    def set_sort_wait(self, max_polls: int = 1 << 20, skip_tile: int = -1) -> None:
+        """Test hook of the particle sort's bounded look-back waits (k3dom_set_sort_wait)."""
+        N.check(self._lib.k3dom_set_sort_wait(self._h, int(max_polls), int(skip_tile)), "k3dom_set_sort_wait")
+
     # -- getters (include/common/dom.h:59-83)
     def info(self) -> N.Info:
         i = N.Info()
