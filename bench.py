@@ -603,25 +603,42 @@ def run_batch(args, local: int = 0, rank: int = 0, world: int = 1, dist=None) ->
         torch.cuda.synchronize()
         return max_over_ranks(time.perf_counter() - t0, dist)
 
+    stage_keys = ("predict_ms", "assign_ms", "occupancy_ms", "binning_ms", "evidence_ms", "persistent_ms",
+                  "births_ms", "resample_ms", "total_ms")
+    breakdown = {}
+
     def plain_arm(device_resident: bool) -> float:
         doms = [K.DOM(p, args.variant, device=local) for p in params]
         try:
-            def frame(f):
+            def frame(f, t_shift=0.0):
                 for s, d in enumerate(doms):
                     t, pose, pts = frames[s][f]
                     d.updatePose(*pose)
                     if device_resident:
-                        d.updateGridAsync(t, dev_pts[s][f])
+                        d.updateGridAsync(t + t_shift, dev_pts[s][f])
                         d.synchronize()
                     else:
-                        d.updateGrid(t, pts)
+                        d.updateGrid(t + t_shift, pts)
             for f in range(1 + W):
                 frame(f)
 
             def timed():
                 for f in range(1 + W, n_frames):
                     frame(f)
-            return timed_region(timed)
+            secs = timed_region(timed)
+            if device_resident and S:
+                # per-stage device time of one frame of every scene, summed over the 16 handles
+                for d in doms:
+                    d.set_timing(True)
+                frame(n_frames - 1, t_shift=0.1)
+                frame(n_frames - 1, t_shift=0.2)
+                acc = {k: 0.0 for k in stage_keys}
+                for d in doms:
+                    st_ = d.stage_times()
+                    for k in stage_keys:
+                        acc[k] += st_[k]
+                breakdown["plain_sum_of_scenes"] = {k: round(v, 4) for k, v in acc.items()}
+            return secs
         finally:
             for d in doms:
                 d.close()
@@ -660,7 +677,20 @@ def run_batch(args, local: int = 0, rank: int = 0, world: int = 1, dist=None) ->
                 for f in range(1 + W, n_frames):
                     frame(f)
             secs = timed_region(timed)
-            return secs, tuning, b.diagnostics()["kernel_launches_per_frame"]
+            launches = b.diagnostics()["kernel_launches_per_frame"]
+            if device_resident:
+                # per-stage device time of one batched frame (events on the batch's stream)
+                b.set_timing(True)
+                for k in (1, 2):
+                    for s in range(S):
+                        b.updatePose(s, *frames[s][n_frames - 1][1])
+                    b.update_async([frames[s][n_frames - 1][0] + t_shift + 0.1 * k for s in range(S)],
+                                   [dev_pts[s][n_frames - 1] for s in range(S)])
+                    b.synchronize()
+                st_ = b.stage_times()
+                breakdown["batched"] = {k: round(st_[k], 4) for k in stage_keys}
+                b.set_timing(False)
+            return secs, tuning, launches
         finally:
             b.close()
 
@@ -686,6 +716,7 @@ def run_batch(args, local: int = 0, rank: int = 0, world: int = 1, dist=None) ->
         "plain_loop_device_resident": round(plain_dev, 2), "batched_device_resident": round(batch_dev, 2),
         "speedup_device_resident": round(batch_dev / plain_dev, 3),
         "batched_launches_per_frame": int(launches),
+        "stage_ms": breakdown,
         "tuning": None if tuning is None else {
             "tile_rule": rules[tuning["tile_rule"]], "chunk": tuning["chunk"],
             "candidate_ms": [round(x, 3) for x in tuning["candidate_ms"]]},
