@@ -532,16 +532,16 @@ cudaError_t alloc_ray_lane(k3dom_calib* c, RayBuffers& rb, int max_points, long 
         return e;
     int bits = 1;
     while ((1 << bits) < T + 1) ++bits;
-    int pb[4];
-    if (radix_plan(bits, pb) > 1) {
+    int pb[8];
+    if (onesweep_plan(bits, pb) > 1) {
         if ((e = c->alloc(&rb.ekeys_alt, cap, L)) || (e = c->alloc(&rb.evals_alt, cap, L))) return e;
     } else {
         rb.ekeys_alt = rb.ekeys;
         rb.evals_alt = rb.evals;
     }
-    rb.hist_words = std::max(radix_hist_words(cap, 11), 1L);
-    rb.scan_words = scan_u32_tiles(std::max({rb.hist_words, (long)N, (long)T + 1})) + 16;
-    if ((e = c->alloc(&rb.hist, rb.hist_words, L)) || (e = c->alloc(&rb.scan_tmp, rb.scan_words, L))) return e;
+    rb.os_words = onesweep_scratch_words(cap, bits);
+    rb.scan_words = scan_u32_tiles(std::max((long)N, (long)T + 1)) + 16;
+    if ((e = c->alloc(&rb.os_scratch, rb.os_words, L)) || (e = c->alloc(&rb.scan_tmp, rb.scan_words, L))) return e;
     return cudaSuccess;
 }
 
@@ -617,7 +617,7 @@ k3dom_status compute_sums(k3dom_calib* c, float ls) {
         if ((e = cudaMemsetAsync(acc_k, 0, sizeof(long long) * 4 * (size_t)C, sk))) return c->fail(e);
         if (f.n > 0) {
             if ((e = build_ray_lists(bt, f.pts, f.pts + f.n, f.pts + 2 * (long)f.n, c->rb[l], false, c->status + l,
-                                     sk)))
+                                     SortWait(), sk)))
                 return c->fail(e);
             if ((e = launch_bgki_sums(bt, c->rb[l], c->ftab, c->htab, reinterpret_cast<unsigned long long*>(acc_k),
                                       c->status + l, c->num_sms, sk)))
@@ -630,8 +630,10 @@ k3dom_status compute_sums(k3dom_calib* c, float ls) {
     if ((e = cudaMemcpyAsync(dst, c->status, sizeof(dst), cudaMemcpyDeviceToHost, c->st)) ||
         (e = cudaStreamSynchronize(c->st)))
         return c->fail(e);
-    for (int l = 0; l < k3dom_calib::kLanes; ++l)
+    for (int l = 0; l < k3dom_calib::kLanes; ++l) {
+        if (dst[l].sort_timeout) return K3DOM_ERR_TIMEOUT;  // a bounded wait of the ray-list sort gave up
         if (dst[l].overflow) return K3DOM_ERR_CAPACITY;
+    }
     c->sums_ls = ls;
     return K3DOM_OK;
 }

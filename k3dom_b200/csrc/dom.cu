@@ -123,8 +123,6 @@ struct k3dom_handle {
     uint32_t *sorted_keys = nullptr, *perm = nullptr, *alt_k = nullptr, *alt_v = nullptr;
     SegRec* seg_rec = nullptr;  // piece sums of the segmented per-cell sums, one per 128 sorted slots
     int2* res_br = nullptr;     // ancestor brackets of the resampling blocks
-    uint32_t *hist = nullptr, *scan_tmp = nullptr;
-    long hist_words = 0, scan_tmp_words = 0;
     uint32_t* os_scratch = nullptr;  // onesweep particle sort: histograms and tile status
     long os_words = 0;
     SortWait sort_wait;
@@ -136,8 +134,8 @@ struct k3dom_handle {
     ExactTile *plan_born = nullptr, *plan_joint = nullptr;
     int plan_born_n = 0, plan_joint_n = 0;
     uint32_t *draw_keys = nullptr, *draw_sorted = nullptr, *draw_alt = nullptr;
-    uint32_t *hist_draw = nullptr, *scan_tmp_draw = nullptr;
-    long hist_draw_words = 0, scan_draw_words = 0;
+    uint32_t* os_draw = nullptr;  // onesweep scratch of the draw sort (runs on the second stream)
+    long os_draw_words = 0;
     cudaEvent_t ev_staged = nullptr;  // host staging (frame scalars, points) consumed
     int* ancestors = nullptr;
     float* pts = nullptr;  // device x | y | z, N slots each
@@ -395,8 +393,8 @@ cudaError_t alloc_ray_buffers(k3dom_handle* h) {
         return e;
     int bits = 1;
     while ((1 << bits) < T + 1) ++bits;
-    int pb[4];
-    if (radix_plan(bits, pb) > 1) {
+    int pb[8];
+    if (onesweep_plan(bits, pb) > 1) {
         if ((e = h->alloc(&rb.ekeys_alt, cap, false, L)) || (e = h->alloc(&rb.evals_alt, cap, false, L))) return e;
     } else {
         rb.ekeys_alt = rb.ekeys;
@@ -409,9 +407,9 @@ cudaError_t alloc_ray_buffers(k3dom_handle* h) {
         if ((e = h->alloc(&rb.ds_counts, rb.ds_count_capacity, true, L))) return e;
     }
     // sort/scan scratch of the ray lists (their own: the lists are built beside the particle sort)
-    rb.hist_words = std::max(radix_hist_words(cap, 11), 1L);
-    rb.scan_words = scan_u32_tiles(std::max({rb.hist_words, (long)N, (long)T + 1})) + 16;
-    if ((e = h->alloc(&rb.hist, rb.hist_words, true, L))) return e;
+    rb.os_words = onesweep_scratch_words(cap, bits);
+    rb.scan_words = scan_u32_tiles(std::max((long)N, (long)T + 1)) + 16;
+    if ((e = h->alloc(&rb.os_scratch, rb.os_words, true, L))) return e;
     if ((e = h->alloc(&rb.scan_tmp, rb.scan_words, true, L))) return e;
     if ((e = h->alloc(&h->pts, 3 * (size_t)N, true, L))) return e;
     if ((e = h->alloc(&h->pts_xyz, 3 * (size_t)N, true, L))) return e;
@@ -657,7 +655,8 @@ cudaError_t enq_assign(k3dom_handle* h) {
 
 cudaError_t enq_binning(k3dom_handle* h, cudaStream_t s) {
     const long N = h->N;
-    return build_ray_lists(h->batch(), h->pts, h->pts + N, h->pts + 2 * N, h->rb, h->ds(), h->status, s);
+    return build_ray_lists(h->batch(), h->pts, h->pts + N, h->pts + 2 * N, h->rb, h->ds(), h->status, h->sort_wait,
+                           s);
 }
 
 cudaError_t enq_evidence(k3dom_handle* h, bool first_frame) {
@@ -688,9 +687,10 @@ cudaError_t enq_births(k3dom_handle* h) {
 
 cudaError_t enq_draws(k3dom_handle* h, cudaStream_t s) {
     launch_draw_keys(h->batch(), h->draw_keys, s);
-    return radix_sort_pairs(h->draw_keys, nullptr, h->draw_sorted, nullptr, h->draw_alt, nullptr, h->P,
-                            draw_key_bits(h->S), h->hist_draw, h->hist_draw_words, h->scan_tmp_draw,
-                            h->scan_draw_words, s);
+    SortWait w = h->sort_wait;
+    w.skip_tile = -1;
+    return onesweep_sort_pairs(h->draw_keys, nullptr, h->draw_sorted, nullptr, h->draw_alt, nullptr, h->P,
+                               draw_key_bits(h->S), h->os_draw, h->os_draw_words, h->status, w, s);
 }
 
 cudaError_t enq_resample(k3dom_handle* h, bool draws_ready) {
@@ -983,21 +983,12 @@ k3dom_status k3dom_batch_create(const k3dom_params* params, int32_t n_scenes, k3
     }
     if ((e = h->alloc(&h->draw_keys, P)) || (e = h->alloc(&h->draw_sorted, P)) || (e = h->alloc(&h->draw_alt, P)))
         return bail(e);
-    // sort/scan scratch of the particle sort
-    h->hist_words = std::max(radix_hist_words(P, 11), 1L);
-    h->scan_tmp_words = scan_u32_tiles(h->hist_words) + 16;
-    if ((e = h->alloc(&h->hist, h->hist_words)) || (e = h->alloc(&h->scan_tmp, h->scan_tmp_words))) return bail(e);
+    // sort scratch of the particle sort, and a separate one for the draw sort (it runs
+    // concurrently on the second stream; the draw keys carry the scene index above 24 bits)
     h->os_words = onesweep_scratch_words(P, key_bits_for(h->C));
     if ((e = h->alloc(&h->os_scratch, h->os_words))) return bail(e);
-    // separate sort scratch for the draw sort (it runs concurrently on the second stream); the
-    // draw keys carry the scene index above 24 bits, so passes may be up to 11 bits wide
-    {
-        const long hw = radix_hist_words(P, 11);
-        h->hist_draw_words = hw;
-        h->scan_draw_words = scan_u32_tiles(hw) + 16;
-        if ((e = h->alloc(&h->hist_draw, hw))) return bail(e);
-        if ((e = h->alloc(&h->scan_tmp_draw, h->scan_draw_words))) return bail(e);
-    }
+    h->os_draw_words = onesweep_scratch_words(P, draw_key_bits(h->S));
+    if ((e = h->alloc(&h->os_draw, h->os_draw_words))) return bail(e);
     if ((e = alloc_ray_buffers(h))) return bail(e);
     // DOM_c::initialize (src/common/dom.cu:90-109): cells to priors
     launch_cells_init(h->batch(), h->cs[0], h->cw, h->st);

@@ -376,7 +376,7 @@ long ray_entries_bound(const DevParams& p, const TileShape& ts, int max_points, 
 }
 
 cudaError_t build_ray_lists(const Batch& bt, const float* xs, const float* ys, const float* zs, RayBuffers& rb,
-                            bool ds, DevStatus* status, cudaStream_t st) {
+                            bool ds, DevStatus* status, const SortWait& wait, cudaStream_t st) {
     const int N = bt.N;
     const int T = bt.T;
     ++g_launches;
@@ -388,8 +388,11 @@ cudaError_t build_ray_lists(const Batch& bt, const float* xs, const float* ys, c
                                                rb.ekeys, rb.evals, status);
     int bits = 1;
     while ((1 << bits) < T + 1) ++bits;
-    e = radix_sort_pairs_dn(rb.ekeys, rb.evals, rb.ekeys2, rb.evals2, rb.ekeys_alt, rb.evals_alt, rb.capacity,
-                            rb.total + 2, bits, rb.hist, rb.hist_words, rb.scan_tmp, rb.scan_words, st);
+    // stable: each tile keeps its rays in input order (the DS first-100 rule depends on it)
+    SortWait w = wait;
+    w.skip_tile = -1;
+    e = onesweep_sort_pairs_dn(rb.ekeys, rb.evals, rb.ekeys2, rb.evals2, rb.ekeys_alt, rb.evals_alt, rb.capacity,
+                               rb.total + 2, bits, rb.os_scratch, rb.os_words, status, w, st);
     if (e != cudaSuccess) return e;
     ++g_launches;
     k_tile_start<<<div_up(T + 1, kBlock), kBlock, 0, st>>>(rb.ekeys2, rb.total, T, rb.tile_start);

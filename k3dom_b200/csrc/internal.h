@@ -49,6 +49,11 @@ cudaError_t onesweep_init();
 cudaError_t onesweep_sort_pairs(const uint32_t* keys, const uint32_t* vals, uint32_t* keys_out, uint32_t* vals_out,
                                 uint32_t* alt_k, uint32_t* alt_v, long n, int key_bits, uint32_t* scratch,
                                 long scratch_words, DevStatus* ds, const SortWait& wait, cudaStream_t st);
+// The same with the element count min(*dn, nmax) read on the device (dn may be nullptr).
+cudaError_t onesweep_sort_pairs_dn(const uint32_t* keys, const uint32_t* vals, uint32_t* keys_out, uint32_t* vals_out,
+                                   uint32_t* alt_k, uint32_t* alt_v, long nmax, const uint32_t* dn, int key_bits,
+                                   uint32_t* scratch, long scratch_words, DevStatus* ds, const SortWait& wait,
+                                   cudaStream_t st);
 
 // exactscan.cu: inclusive prefix sums of non-negative floats, exact in 128-bit fixed
 // point and rounded once to float.
@@ -134,9 +139,10 @@ struct RayBuffers {
     uint32_t* tile_done;   // T
     unsigned long long* acc;  // 2*C fixed-point accumulators (K3DOM) / DS partials
     uint8_t* ds_counts;    // DS: per (item, cell) neighbour counts of pass 1
-    uint32_t* hist;
     uint32_t* scan_tmp;
-    long hist_words, scan_words;
+    long scan_words;
+    uint32_t* os_scratch;  // onesweep sort of the entries by tile
+    long os_words;
     uint32_t* total;       // [0] = entries, [2] = entries kept (0 on overflow)
     long capacity;         // entries
     long ds_count_capacity;
@@ -147,7 +153,7 @@ long ray_entries_bound(const DevParams& p, const TileShape& ts, int max_points, 
 // scene's kernel table when ktab is not null.
 void fill_scene_evidence(SceneDev& sd, bool ds, float4* ktab);
 cudaError_t build_ray_lists(const Batch& bt, const float* xs, const float* ys, const float* zs, RayBuffers& rb,
-                            bool ds, DevStatus* status, cudaStream_t st);
+                            bool ds, DevStatus* status, const SortWait& wait, cudaStream_t st);
 cudaError_t launch_k3dom_evidence(const Batch& bt, RayBuffers& rb, CellState cs, CellWork cw, bool first_frame,
                                   DevStatus* status, cudaStream_t st);
 cudaError_t launch_ds_evidence(const Batch& bt, RayBuffers& rb, CellState cs, CellWork cw, bool first_frame,

@@ -18,7 +18,11 @@
 //    look-back, so later tiles count past it), so the output holds the keys and values of the
 //    completed tiles and in-range old contents elsewhere; the later passes then write nothing.
 // 7-bit digits (21-bit cell keys of 2^21 voxels take three passes): 128 digits per tile keep the
-// runs long enough for coalesced writes.
+// runs long enough for coalesced writes. The element count may live in device memory (`dn`,
+// capped at nmax): the grid and scratch are sized for nmax, CTAs whose tile lies past the live
+// count return, and since tiles are handed out in order no CTA waits on one of them. The same
+// sort orders the resampling draws (keys only) and the ray lists (tile of each entry, stable so
+// each tile keeps its rays in input order).
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -39,6 +43,7 @@ constexpr uint32_t kOsAgg = 1u << 30;           // published: this tile's count 
 constexpr uint32_t kOsInc = 2u << 30;           // published: inclusive prefix through this tile
 constexpr uint32_t kOsValue = (1u << 30) - 1u;
 constexpr int kOsHistBlocks = 148 * 4;
+constexpr int kOsWindow = 16;  // predecessor statuses read per look-back step
 
 // scratch layout (uint32 words): counters [kOsMaxPasses + 1] | histograms [passes][128] |
 // digit offsets [passes][128] | tile status [passes][tiles][128]
@@ -88,12 +93,17 @@ struct OsPasses {
     int bits[kOsMaxPasses];
 };
 
+__device__ __forceinline__ long os_count(long nmax, const uint32_t* dn) {
+    return dn ? min((long)*dn, nmax) : nmax;
+}
+
 // Digit histograms of every pass in one read of the keys; the last CTA to finish turns them
 // into each pass's exclusive digit offsets (no CTA waits on another).
-__global__ void __launch_bounds__(kOsThreads) os_hist(const uint32_t* __restrict__ keys, long n, OsPasses ps,
-                                                      OsScratch sc) {
+__global__ void __launch_bounds__(kOsThreads) os_hist(const uint32_t* __restrict__ keys, long nmax,
+                                                      const uint32_t* dn, OsPasses ps, OsScratch sc) {
     __shared__ uint32_t h[kOsMaxPasses][kOsDigits];
     __shared__ bool last;
+    const long n = os_count(nmax, dn);
     for (int i = threadIdx.x; i < ps.np * kOsDigits; i += kOsThreads) (&h[0][0])[i] = 0;
     __syncthreads();
     for (long i = (long)blockIdx.x * kOsThreads + threadIdx.x; i < n; i += (long)gridDim.x * kOsThreads) {
@@ -135,26 +145,29 @@ struct OsSmem {
 // first pass of an argsort). vals_out == nullptr: keys only.
 template <int BITS>
 __global__ void __launch_bounds__(kOsThreads, 4)
-os_pass(const uint32_t* __restrict__ keys_in, const uint32_t* __restrict__ vals_in, long n, int shift, int pass,
-        OsScratch sc, uint32_t* __restrict__ keys_out, uint32_t* __restrict__ vals_out, DevStatus* ds,
-        uint32_t max_polls, int skip_tile) {
+os_pass(const uint32_t* __restrict__ keys_in, const uint32_t* __restrict__ vals_in, long nmax, const uint32_t* dn,
+        int shift, int pass, OsScratch sc, uint32_t* __restrict__ keys_out, uint32_t* __restrict__ vals_out,
+        DevStatus* ds, uint32_t max_polls, int skip_tile) {
     constexpr int NB = 1 << BITS;
     constexpr int NW = kOsThreads / 32;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     OsSmem& S = *reinterpret_cast<OsSmem*>(smem_raw);
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
     const unsigned lt_mask = (1u << lane) - 1u;
-    const long ntiles = (n + kOsTile - 1) / kOsTile;
+    const long cap_tiles = (nmax + kOsTile - 1) / kOsTile;  // the grid and the status layout
+    const long n = os_count(nmax, dn);
+    const long ntiles = (n + kOsTile - 1) / kOsTile;        // live tiles
     // after a timeout in an earlier pass this pass's input is incomplete, so its digit counts no
     // longer match the histograms: write nothing (every output slot keeps an in-range value)
     if (pass > 0 && *(volatile unsigned int*)&ds->sort_timeout) return;
     if (threadIdx.x == 0) S.tile = atomicAdd(&sc.counters[pass], 1u);
-    for (int i = threadIdx.x; i < NW * NB; i += kOsThreads) (&S.cnt[0][0])[i] = 0;
+    // the counters' rows are kOsDigits wide whatever the pass's width: clear them all
+    for (int i = threadIdx.x; i < NW * kOsDigits; i += kOsThreads) (&S.cnt[0][0])[i] = 0;
     __syncthreads();
     const long tile = S.tile;
-    if (tile >= ntiles) return;  // the grid is exactly ntiles CTAs
+    if (tile >= ntiles) return;  // past the live count (the grid covers nmax)
     const long tbase = tile * kOsTile;
-    uint32_t* status = sc.status + ((long)pass * ntiles) * kOsDigits;
+    uint32_t* status = sc.status + ((long)pass * cap_tiles) * kOsDigits;
 
     // stable rank within the tile: warp w holds keys [w*512, w*512 + 512) in (item, lane) order
     uint32_t key[kOsItems], val[kOsItems];
@@ -196,25 +209,41 @@ os_pass(const uint32_t* __restrict__ keys_in, const uint32_t* __restrict__ vals_
         const uint32_t ex = block_exclusive_scan<uint32_t, kOsThreads>(count, S.scan_tmp, &tot);
         if (threadIdx.x < NB) S.digit_start[threadIdx.x] = ex;
     }
-    // decoupled look-back: keys of this digit in all earlier tiles
+    // decoupled look-back: keys of this digit in all earlier tiles. The statuses of kOsWindow
+    // predecessors are read at once (independent loads) and summed in order up to the first
+    // inclusive prefix; a predecessor not yet published ends the step there and is polled again.
+    // Tiles that start together publish only their counts at first, so a walk of one tile per
+    // dependent load would grow with the tile's distance from the last inclusive prefix.
     bool timed_out = false;
     if (threadIdx.x < NB) {
         const int d = threadIdx.x;
         uint32_t excl = 0;
         uint32_t polls = 0;
-        for (long j = tile - 1; j >= 0;) {
-            const uint32_t s = ld_acquire(&status[j * kOsDigits + d]);
-            if ((s & ~kOsValue) == 0u) {  // not yet published
+        long j = tile - 1;
+        while (j >= 0) {
+            uint32_t st_w[kOsWindow];
+#pragma unroll
+            for (int w = 0; w < kOsWindow; ++w)
+                st_w[w] = (j - w >= 0) ? ld_acquire(&status[(j - w) * kOsDigits + d]) : kOsInc;
+            int used = 0;
+            bool done = false;
+#pragma unroll
+            for (int w = 0; w < kOsWindow; ++w) {
+                if (done || used < w) continue;          // stopped at an earlier entry of the window
+                if ((st_w[w] & ~kOsValue) == 0u) continue;  // not yet published: poll it again
+                excl += st_w[w] & kOsValue;               // tiles before 0 read as an empty prefix
+                used = w + 1;
+                if (st_w[w] & kOsInc) done = true;
+            }
+            if (done) break;
+            if (used == 0) {
                 if (polls++ >= max_polls) {
                     timed_out = true;
                     break;
                 }
                 __nanosleep(64);
-                continue;
             }
-            excl += s & kOsValue;
-            if (s & kOsInc) break;
-            --j;
+            j -= used;
         }
         if (!timed_out && tile != skip_tile) st_release(&status[tile * kOsDigits + d], kOsInc | (excl + count));
         S.global_base[d] = sc.digit_off[pass * kOsDigits + d] + excl - S.digit_start[d];
@@ -245,13 +274,13 @@ os_pass(const uint32_t* __restrict__ keys_in, const uint32_t* __restrict__ vals_
 }
 
 template <int BITS>
-static cudaError_t os_launch(const uint32_t* kin, const uint32_t* vin, long n, int shift, int pass, OsScratch sc,
-                             uint32_t* kout, uint32_t* vout, DevStatus* ds, uint32_t max_polls, int skip_tile,
-                             cudaStream_t st) {
-    const long ntiles = div_up(n, (long)kOsTile);
+static cudaError_t os_launch(const uint32_t* kin, const uint32_t* vin, long nmax, const uint32_t* dn, int shift,
+                             int pass, OsScratch sc, uint32_t* kout, uint32_t* vout, DevStatus* ds,
+                             uint32_t max_polls, int skip_tile, cudaStream_t st) {
+    const long ntiles = div_up(nmax, (long)kOsTile);
     ++g_launches;
-    os_pass<BITS><<<(unsigned)ntiles, kOsThreads, sizeof(OsSmem), st>>>(kin, vin, n, shift, pass, sc, kout, vout, ds,
-                                                                       max_polls, skip_tile);
+    os_pass<BITS><<<(unsigned)ntiles, kOsThreads, sizeof(OsSmem), st>>>(kin, vin, nmax, dn, shift, pass, sc, kout,
+                                                                       vout, ds, max_polls, skip_tile);
     return cudaGetLastError();
 }
 
@@ -263,9 +292,10 @@ cudaError_t onesweep_init() {
     return e;
 }
 
-cudaError_t onesweep_sort_pairs(const uint32_t* keys, const uint32_t* vals, uint32_t* keys_out, uint32_t* vals_out,
-                                uint32_t* alt_k, uint32_t* alt_v, long n, int key_bits, uint32_t* scratch,
-                                long scratch_words, DevStatus* ds, const SortWait& wait, cudaStream_t st) {
+cudaError_t onesweep_sort_pairs_dn(const uint32_t* keys, const uint32_t* vals, uint32_t* keys_out, uint32_t* vals_out,
+                                   uint32_t* alt_k, uint32_t* alt_v, long n, const uint32_t* dn, int key_bits,
+                                   uint32_t* scratch, long scratch_words, DevStatus* ds, const SortWait& wait,
+                                   cudaStream_t st) {
     if (n <= 0) return cudaSuccess;
     if (n > (long)kOsValue || !ds) return cudaErrorInvalidValue;
     OsPasses ps;
@@ -282,7 +312,7 @@ cudaError_t onesweep_sort_pairs(const uint32_t* keys, const uint32_t* vals, uint
     if (e != cudaSuccess) return e;
     ++g_launches;
     const long hist_grid = std::min((long)kOsHistBlocks, (long)div_up(n, (long)kOsThreads));
-    os_hist<<<(unsigned)hist_grid, kOsThreads, 0, st>>>(keys, n, ps, sc);
+    os_hist<<<(unsigned)hist_grid, kOsThreads, 0, st>>>(keys, n, dn, ps, sc);
     const uint32_t* ck = keys;
     const uint32_t* cv = vals;
     for (int p = 0; p < ps.np; ++p) {
@@ -291,19 +321,26 @@ cudaError_t onesweep_sort_pairs(const uint32_t* keys, const uint32_t* vals, uint
         uint32_t* ov = vals_out ? (to_out ? vals_out : alt_v) : nullptr;
         const int skip = p == 0 ? wait.skip_tile : -1;
         switch (ps.bits[p]) {
-            case 1: e = os_launch<1>(ck, cv, n, ps.shift[p], p, sc, ok, ov, ds, wait.max_polls, skip, st); break;
-            case 2: e = os_launch<2>(ck, cv, n, ps.shift[p], p, sc, ok, ov, ds, wait.max_polls, skip, st); break;
-            case 3: e = os_launch<3>(ck, cv, n, ps.shift[p], p, sc, ok, ov, ds, wait.max_polls, skip, st); break;
-            case 4: e = os_launch<4>(ck, cv, n, ps.shift[p], p, sc, ok, ov, ds, wait.max_polls, skip, st); break;
-            case 5: e = os_launch<5>(ck, cv, n, ps.shift[p], p, sc, ok, ov, ds, wait.max_polls, skip, st); break;
-            case 6: e = os_launch<6>(ck, cv, n, ps.shift[p], p, sc, ok, ov, ds, wait.max_polls, skip, st); break;
-            default: e = os_launch<7>(ck, cv, n, ps.shift[p], p, sc, ok, ov, ds, wait.max_polls, skip, st); break;
+            case 1: e = os_launch<1>(ck, cv, n, dn, ps.shift[p], p, sc, ok, ov, ds, wait.max_polls, skip, st); break;
+            case 2: e = os_launch<2>(ck, cv, n, dn, ps.shift[p], p, sc, ok, ov, ds, wait.max_polls, skip, st); break;
+            case 3: e = os_launch<3>(ck, cv, n, dn, ps.shift[p], p, sc, ok, ov, ds, wait.max_polls, skip, st); break;
+            case 4: e = os_launch<4>(ck, cv, n, dn, ps.shift[p], p, sc, ok, ov, ds, wait.max_polls, skip, st); break;
+            case 5: e = os_launch<5>(ck, cv, n, dn, ps.shift[p], p, sc, ok, ov, ds, wait.max_polls, skip, st); break;
+            case 6: e = os_launch<6>(ck, cv, n, dn, ps.shift[p], p, sc, ok, ov, ds, wait.max_polls, skip, st); break;
+            default: e = os_launch<7>(ck, cv, n, dn, ps.shift[p], p, sc, ok, ov, ds, wait.max_polls, skip, st); break;
         }
         if (e != cudaSuccess) return e;
         ck = ok;
         cv = ov;
     }
     return cudaSuccess;
+}
+
+cudaError_t onesweep_sort_pairs(const uint32_t* keys, const uint32_t* vals, uint32_t* keys_out, uint32_t* vals_out,
+                                uint32_t* alt_k, uint32_t* alt_v, long n, int key_bits, uint32_t* scratch,
+                                long scratch_words, DevStatus* ds, const SortWait& wait, cudaStream_t st) {
+    return onesweep_sort_pairs_dn(keys, vals, keys_out, vals_out, alt_k, alt_v, n, nullptr, key_bits, scratch,
+                                  scratch_words, ds, wait, st);
 }
 
 }  // namespace k3dom
