@@ -43,7 +43,7 @@ constexpr uint32_t kOsAgg = 1u << 30;           // published: this tile's count 
 constexpr uint32_t kOsInc = 2u << 30;           // published: inclusive prefix through this tile
 constexpr uint32_t kOsValue = (1u << 30) - 1u;
 constexpr int kOsHistBlocks = 148 * 4;
-constexpr int kOsWindow = 16;  // predecessor statuses read per look-back step
+constexpr int kOsWindow = 8;  // predecessor statuses read per look-back step
 
 // scratch layout (uint32 words): counters [kOsMaxPasses + 1] | histograms [passes][128] |
 // digit offsets [passes][128] | tile status [passes][tiles][128]
@@ -209,6 +209,20 @@ os_pass(const uint32_t* __restrict__ keys_in, const uint32_t* __restrict__ vals_
         const uint32_t ex = block_exclusive_scan<uint32_t, kOsThreads>(count, S.scan_tmp, &tot);
         if (threadIdx.x < NB) S.digit_start[threadIdx.x] = ex;
     }
+    __syncthreads();
+    // the tile in digit order in shared memory (positions need no earlier tile), so the keys
+    // leave the registers before the look-back
+#pragma unroll
+    for (int j = 0; j < kOsItems; ++j) {
+        const long i = tbase + wid * (kOsItems * 32) + j * 32 + lane;
+        if (i < n) {
+            const uint32_t d = (key[j] >> shift) & (NB - 1);
+            const uint32_t pos = S.digit_start[d] + S.cnt[wid][d] + rank[j];
+            S.keys[pos] = key[j];
+            S.vals[pos] = val[j];
+        }
+    }
+    __syncthreads();
     // decoupled look-back: keys of this digit in all earlier tiles. The statuses of kOsWindow
     // predecessors are read at once (independent loads) and summed in order up to the first
     // inclusive prefix; a predecessor not yet published ends the step there and is polled again.
@@ -252,17 +266,6 @@ os_pass(const uint32_t* __restrict__ keys_in, const uint32_t* __restrict__ vals_
         if (threadIdx.x == 0) atomicOr(&ds->sort_timeout, 1u);
         return;
     }
-#pragma unroll
-    for (int j = 0; j < kOsItems; ++j) {
-        const long i = tbase + wid * (kOsItems * 32) + j * 32 + lane;
-        if (i < n) {
-            const uint32_t d = (key[j] >> shift) & (NB - 1);
-            const uint32_t pos = S.digit_start[d] + S.cnt[wid][d] + rank[j];
-            S.keys[pos] = key[j];
-            S.vals[pos] = val[j];
-        }
-    }
-    __syncthreads();
     const int valid_n = (int)min((long)kOsTile, n - tbase);
     for (int k = threadIdx.x; k < valid_n; k += kOsThreads) {
         const uint32_t kk = S.keys[k];
