@@ -121,6 +121,13 @@ struct k3dom_handle {
 
     Particles A{}, Ss{}, Bp{};
     uint32_t *sorted_keys = nullptr, *perm = nullptr, *alt_k = nullptr, *alt_v = nullptr;
+    // The persistent set lives in A (structure of arrays; written by resampling, the first frame
+    // and k3dom_set_particles) and, after prediction, in 32-byte records X (what the assignment
+    // gathers). Which of the two holds the current set is tracked at enqueue time; every full
+    // frame ends with A current, so a captured frame's replays leave both flags as they were.
+    float4* X = nullptr;
+    bool a_current = true;   // A holds the current persistent set
+    bool x_current = false;  // X holds it
     SegRec* seg_rec = nullptr;  // piece sums of the segmented per-cell sums, one per 128 sorted slots
     int2* res_br = nullptr;     // ancestor brackets of the resampling blocks
     uint32_t* os_scratch = nullptr;  // onesweep particle sort: histograms and tile status
@@ -637,19 +644,37 @@ void rec(k3dom_handle* h, int i) {
 }
 
 // --- enqueue helpers (no synchronisation) ---
+// The persistent set as structure of arrays in A (unpacked from X when prediction left it there).
+cudaError_t ensure_a_current(k3dom_handle* h) {
+    if (h->a_current) return cudaSuccess;
+    launch_unpack_records(h->P, h->X, h->A, h->st);
+    h->a_current = true;
+    return cudaGetLastError();
+}
+
 cudaError_t enq_predict(k3dom_handle* h) {
-    launch_predict(h->batch(), h->A, h->st);
+    cudaError_t e = ensure_a_current(h);
+    if (e != cudaSuccess) return e;
+    launch_predict(h->batch(), h->A, h->X, h->st);
+    h->a_current = false;
+    h->x_current = true;
     return cudaGetLastError();
 }
 
 cudaError_t enq_assign(k3dom_handle* h) {
+    // the records the gather reads (prediction wrote them; otherwise packed from A, whose cell
+    // indices are always current)
+    if (!h->x_current) {
+        launch_pack_records(h->P, h->A, h->X, h->st);
+        h->x_current = true;
+    }
     cudaError_t e = onesweep_sort_pairs(reinterpret_cast<const uint32_t*>(h->A.cell), nullptr, h->sorted_keys,
                                         h->perm, h->alt_k, h->alt_v, h->P, key_bits_for(h->C), h->os_scratch,
                                         h->os_words, h->status, h->sort_wait, h->st);
     if (e != cudaSuccess) return e;
     if ((e = cudaMemsetAsync(h->cw.start, 0xFF, sizeof(int) * (size_t)h->C, h->st))) return e;
     if ((e = cudaMemsetAsync(h->cw.end, 0xFF, sizeof(int) * (size_t)h->C, h->st))) return e;
-    launch_gather_segsum(h->batch(), h->A, h->Ss, h->sorted_keys, h->perm, h->cw, h->seg_rec, h->st);
+    launch_gather_segsum(h->batch(), h->X, h->Ss, h->sorted_keys, h->perm, h->cw, h->seg_rec, h->st);
     return cudaGetLastError();
 }
 
@@ -702,6 +727,8 @@ cudaError_t enq_resample(k3dom_handle* h, bool draws_ready) {
     if ((e = exact_scan_plan(h->plan_joint, h->plan_joint_n, h->exact_scratch, h->st))) return e;
     launch_resample(h->batch(), h->joint_cum, h->draw_sorted, h->Ss, h->Bp, h->A, h->ancestors, h->joint_max,
                     h->res_br, h->st);
+    h->a_current = true;
+    h->x_current = false;
     return cudaGetLastError();
 }
 
@@ -709,6 +736,8 @@ cudaError_t enq_init_particles(k3dom_handle* h) {
     cudaError_t e = exact_scan_plan(h->plan_born, h->plan_born_n, h->exact_scratch, h->st);
     if (e != cudaSuccess) return e;
     launch_init_particles(h->batch(), h->born_cum, h->A, h->st);
+    h->a_current = true;
+    h->x_current = false;
     return cudaGetLastError();
 }
 
@@ -940,6 +969,7 @@ k3dom_status k3dom_batch_create(const k3dom_params* params, int32_t n_scenes, k3
     if ((e = h->alloc_particles(&h->A, P)) || (e = h->alloc_particles(&h->Ss, P)) ||
         (e = h->alloc_particles(&h->Bp, B)))
         return bail(e);
+    if ((e = h->alloc(&h->X, 2 * (size_t)P))) return bail(e);
     if ((e = h->alloc(&h->sorted_keys, P)) || (e = h->alloc(&h->perm, P)) || (e = h->alloc(&h->alt_k, P)) ||
         (e = h->alloc(&h->alt_v, P)) || (e = h->alloc(&h->seg_rec, seg_rec_count(P))) ||
         (e = h->alloc(&h->res_br, res_bracket_count(P))))
@@ -1051,6 +1081,8 @@ k3dom_status k3dom_batch_update_pose(k3dom_handle* h, int32_t scene, float x, fl
         if (sh.shift_pending) {
             // a second shift before any prediction: apply the first to the particles now so
             // each subtraction rounds exactly as moveParticlesKernel's would
+            if ((e = ensure_a_current(h))) return h->fail(e);
+            h->x_current = false;
             launch_shift_particles(sh.dp.P, offset_particles(h->A, h->off.part[scene]), sh.pending_shift[0],
                                    sh.pending_shift[1], sh.pending_shift[2], h->st);
         }
@@ -1649,6 +1681,7 @@ k3dom_status k3dom_get_particles(k3dom_handle* h, k3dom_particle_set set, float*
     if (!pick_set(h, set, &q, &n)) return K3DOM_ERR_INVALID_ARGUMENT;
     const cudaMemcpyKind k = mem == K3DOM_MEM_HOST ? cudaMemcpyDeviceToHost : cudaMemcpyDeviceToDevice;
     cudaError_t e;
+    if (set == K3DOM_PARTICLES_PERSISTENT && (e = ensure_a_current(h))) return h->fail(e);
     auto strided = [&](float* dst, const float* a, const float* b, const float* c) -> cudaError_t {
         cudaError_t r;
         if ((r = cudaMemcpy2DAsync(dst, 3 * sizeof(float), a, sizeof(float), sizeof(float), n, k, h->st))) return r;
@@ -1695,6 +1728,9 @@ k3dom_status k3dom_set_particles(k3dom_handle* h, k3dom_particle_set set, const 
     if (set == K3DOM_PARTICLES_SORTED && (!cell_idx || h->S != 1)) return K3DOM_ERR_INVALID_ARGUMENT;
     const cudaMemcpyKind k = mem == K3DOM_MEM_HOST ? cudaMemcpyHostToDevice : cudaMemcpyDeviceToDevice;
     cudaError_t e;
+    // the fields not given keep their values: make A hold the whole current set first
+    if ((e = ensure_a_current(h))) return h->fail(e);
+    if (set == K3DOM_PARTICLES_PERSISTENT) h->x_current = false;
     auto strided = [&](const float* src, float* a, float* b, float* c) -> cudaError_t {
         cudaError_t r;
         if ((r = cudaMemcpy2DAsync(a, sizeof(float), src, 3 * sizeof(float), sizeof(float), n, k, h->st))) return r;
@@ -1721,7 +1757,10 @@ k3dom_status k3dom_set_particles(k3dom_handle* h, k3dom_particle_set set, const 
         k_iota<<<div_up(n, 256), 256, 0, h->st>>>(h->perm, n);
         if ((e = cudaMemsetAsync(h->cw.start, 0xFF, sizeof(int) * (size_t)h->C, h->st))) return h->fail(e);
         if ((e = cudaMemsetAsync(h->cw.end, 0xFF, sizeof(int) * (size_t)h->C, h->st))) return h->fail(e);
-        launch_gather_segsum(h->batch(), h->Ss, h->Ss, h->sorted_keys, h->perm, h->cw, h->seg_rec, h->st);
+        // the gather reads records: pack the sorted set into X (A holds the persistent set)
+        launch_pack_records(n, h->Ss, h->X, h->st);
+        h->x_current = false;
+        launch_gather_segsum(h->batch(), h->X, h->Ss, h->sorted_keys, h->perm, h->cw, h->seg_rec, h->st);
     }
     e = cudaStreamSynchronize(h->st);
     return e == cudaSuccess ? K3DOM_OK : h->fail(e);

@@ -79,7 +79,11 @@ size_t exact_plan_scratch_bytes(int ntiles);
 cudaError_t exact_scan_plan(const ExactTile* tiles, int nt, void* scratch, cudaStream_t st);
 
 // particles.cu
-void launch_predict(const Batch& bt, Particles a, cudaStream_t st);
+// Prediction reads the structure-of-arrays set a and writes each particle as a 32-byte record
+// (x[2i] = px py pz vx, x[2i+1] = vy vz w assoc) plus its cell index a.cell.
+void launch_predict(const Batch& bt, Particles a, float4* x, cudaStream_t st);
+void launch_pack_records(int n, Particles a, float4* x, cudaStream_t st);
+void launch_unpack_records(int n, const float4* x, Particles a, cudaStream_t st);
 void launch_shift_particles(int n, Particles a, int mx, int my, int mz, cudaStream_t st);
 // Piece sums of one 128-slot range of the sorted particles (gather + segmented sums): the
 // range's first piece when its cell began in an earlier range, and its last piece when its cell
@@ -91,7 +95,7 @@ struct SegRec {
     int trail_head;   // position of the last piece's cell head; -1: no such piece
 };
 long seg_rec_count(long P);
-void launch_gather_segsum(const Batch& bt, Particles a, Particles s, const uint32_t* sorted_keys,
+void launch_gather_segsum(const Batch& bt, const float4* x, Particles s, const uint32_t* sorted_keys,
                           const uint32_t* perm, CellWork cw, SegRec* rec, cudaStream_t st);
 void launch_reweight(const Batch& bt, Particles s, const uint32_t* sorted_keys, CellWork cw, cudaStream_t st);
 void launch_births(const Batch& bt, const float* born, const float* born_cum, Particles b, cudaStream_t st);

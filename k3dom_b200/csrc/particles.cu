@@ -22,7 +22,10 @@ using namespace k3dom_draws;
 // stored cell index is the global one (scene cell offset + x + G y + G^2 z).
 // One particle per thread (no grid-stride loop): every particle's loads are independent of
 // another's stores, so the scheduler keeps many more of them in flight.
-__global__ void __launch_bounds__(kBlock) k_predict(Batch bt, Particles a) {
+// The predicted particle goes out as one 32-byte record (x[2i] = px py pz vx, x[2i+1] = vy vz w
+// assoc) plus its cell index in a.cell: the assignment then gathers each particle in one sector
+// through the sort permutation, which jumps by several voxels' worth of particles.
+__global__ void __launch_bounds__(kBlock) k_predict(Batch bt, Particles a, float4* __restrict__ x) {
     {
         const int i = blockIdx.x * blockDim.x + threadIdx.x;
         if (i >= bt.P) return;
@@ -67,17 +70,45 @@ __global__ void __launch_bounds__(kBlock) k_predict(Batch bt, Particles a) {
         const int ix = clampv(f2i_trunc(px), 0, Gi - 1);
         const int iy = clampv(f2i_trunc(py), 0, Gi - 1);
         const int iz = clampv(f2i_trunc(pz), 0, Gzi - 1);
-        a.px[i] = px; a.py[i] = py; a.pz[i] = pz;
-        a.vx[i] = vx; a.vy[i] = vy; a.vz[i] = vz;
-        a.w[i] = w;
+        x[2 * (long)i] = make_float4(px, py, pz, vx);
+        x[2 * (long)i + 1] = make_float4(vy, vz, w, __uint_as_float((uint32_t)a.assoc[i]));
         a.cell[i] = bt.off->cell[sc] + ix + Gi * iy + Gi * Gi * iz;
     }
 }
 
-void launch_predict(const Batch& bt, Particles a, cudaStream_t st) {
+void launch_predict(const Batch& bt, Particles a, float4* x, cudaStream_t st) {
     if (bt.P <= 0) return;
     ++g_launches;
-    k_predict<<<div_up(bt.P, kBlock), kBlock, 0, st>>>(bt, a);
+    k_predict<<<div_up(bt.P, kBlock), kBlock, 0, st>>>(bt, a, x);
+}
+
+// Between the structure-of-arrays set and its 32-byte records (the layout k_predict writes).
+__global__ void k_pack_records(int n, Particles a, float4* __restrict__ x) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    x[2 * (long)i] = make_float4(a.px[i], a.py[i], a.pz[i], a.vx[i]);
+    x[2 * (long)i + 1] = make_float4(a.vy[i], a.vz[i], a.w[i], __uint_as_float((uint32_t)a.assoc[i]));
+}
+
+__global__ void k_unpack_records(int n, const float4* __restrict__ x, Particles a) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const float4 r0 = x[2 * (long)i], r1 = x[2 * (long)i + 1];
+    a.px[i] = r0.x; a.py[i] = r0.y; a.pz[i] = r0.z; a.vx[i] = r0.w;
+    a.vy[i] = r1.x; a.vz[i] = r1.y; a.w[i] = r1.z;
+    a.assoc[i] = (uint8_t)__float_as_uint(r1.w);
+}
+
+void launch_pack_records(int n, Particles a, float4* x, cudaStream_t st) {
+    if (n <= 0) return;
+    ++g_launches;
+    k_pack_records<<<div_up(n, kBlock), kBlock, 0, st>>>(n, a, x);
+}
+
+void launch_unpack_records(int n, const float4* x, Particles a, cudaStream_t st) {
+    if (n <= 0) return;
+    ++g_launches;
+    k_unpack_records<<<div_up(n, kBlock), kBlock, 0, st>>>(n, x, a);
 }
 
 __global__ void k_shift_particles(int n, Particles a, int mx, int my, int mz) {
@@ -140,7 +171,7 @@ __device__ __forceinline__ void put_sums(CellWork cw, uint32_t key, double w, do
 }
 
 __global__ void __launch_bounds__(kBlock)
-k_gather_segsum(Batch bt, Particles a, Particles s, const uint32_t* __restrict__ keys,
+k_gather_segsum(Batch bt, const float4* __restrict__ x, Particles s, const uint32_t* __restrict__ keys,
                 const uint32_t* __restrict__ perm, CellWork cw, SegRec* __restrict__ rec) {
     const int lane = threadIdx.x & 31;
     const long warp_global = (long)blockIdx.x * kSegWarps + (threadIdx.x >> 5);
@@ -161,8 +192,7 @@ k_gather_segsum(Batch bt, Particles a, Particles s, const uint32_t* __restrict__
     }
     __syncwarp();
     // the particles of one 32-slot chunk, loaded one chunk ahead of their stores (the next chunk's
-    // loads are in flight while this one is stored and scanned; the slots differ, so this holds
-    // for an in-place gather too)
+    // loads are in flight while this one is stored and scanned)
     struct Chunk {
         uint32_t key, next_key;
         float px, py, pz, vx, vy, vz, w;
@@ -175,11 +205,11 @@ k_gather_segsum(Batch bt, Particles a, Particles s, const uint32_t* __restrict__
         c.key = valid ? keys[pos] : 0xFFFFFFFEu;
         c.next_key = (pos + 1 < P) ? keys[pos + 1] : 0xFFFFFFFDu;
         if (valid) {
-            const uint32_t src = perm[pos];
-            c.px = a.px[src]; c.py = a.py[src]; c.pz = a.pz[src];
-            c.vx = a.vx[src]; c.vy = a.vy[src]; c.vz = a.vz[src];
-            c.w = a.w[src];
-            c.assoc = a.assoc[src];
+            const long src = perm[pos];
+            const float4 r0 = x[2 * src], r1 = x[2 * src + 1];  // one 32-byte sector
+            c.px = r0.x; c.py = r0.y; c.pz = r0.z; c.vx = r0.w;
+            c.vy = r1.x; c.vz = r1.y; c.w = r1.z;
+            c.assoc = (uint8_t)__float_as_uint(r1.w);
         }
         return c;
     };
@@ -293,12 +323,12 @@ k_seg_fixup(long nrec, const SegRec* __restrict__ rec, const uint32_t* __restric
     put_sums(cw, keys[head], sw, sx, sy, sz, head, end);
 }
 
-void launch_gather_segsum(const Batch& bt, Particles a, Particles s, const uint32_t* sorted_keys,
+void launch_gather_segsum(const Batch& bt, const float4* x, Particles s, const uint32_t* sorted_keys,
                           const uint32_t* perm, CellWork cw, SegRec* rec, cudaStream_t st) {
     if (bt.P <= 0) return;
     const long warps = div_up((long)bt.P, (long)kSegRange);
     g_launches += 2;
-    k_gather_segsum<<<div_up(warps, (long)kSegWarps), kBlock, 0, st>>>(bt, a, s, sorted_keys, perm, cw, rec);
+    k_gather_segsum<<<div_up(warps, (long)kSegWarps), kBlock, 0, st>>>(bt, x, s, sorted_keys, perm, cw, rec);
     k_seg_fixup<<<div_up(warps, (long)kBlock), kBlock, 0, st>>>(warps, rec, sorted_keys, cw);
 }
 
