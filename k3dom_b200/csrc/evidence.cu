@@ -861,26 +861,6 @@ __device__ __forceinline__ float free_d2(const float4& st0, const float4& st1, f
     return qx * qx + qy * qy + qz * qz + al * al;
 }
 
-// The same for the two cells of a lane's column, (dx, dy, dz) and the cell above it
-// (dx, dy, dz + hz): the upper cell's perpendicular offset is q + h - (h.u) u with h = (0, 0, hz),
-// so |q'|^2 = |q|^2 + hz (2 q_z + hz (1 - u_z^2)) (q is perpendicular to u), and its along-ray
-// coordinate is dpar + hz u_z. Every term is O(ls), so the update keeps the FP32 accuracy of the
-// direct form. Returns the lower cell's squared distance; *d2_1 the upper cell's.
-__device__ __forceinline__ float free_d2_pair(const float4& st0, const float4& st1, float dx, float dy, float dz,
-                                              float hz, float* dpar0, float* dpar1, float* d2_1) {
-    const float dp = dx * st1.x + dy * st1.y + dz * st1.z;
-    const float qx = st0.x + dx - dp * st1.x, qy = st0.y + dy - dp * st1.y, qz = st0.z + dz - dp * st1.z;
-    const float qq = qx * qx + qy * qy + qz * qz;
-    const float al0 = fminf(st0.w + dp, 0.0f) + fmaxf(st1.w + dp, 0.0f);
-    const float dp1 = fmaf(hz, st1.z, dp);
-    const float qq1 = fmaf(hz, fmaf(2.0f, qz, hz * fmaf(-st1.z, st1.z, 1.0f)), qq);
-    const float al1 = fminf(st0.w + dp1, 0.0f) + fmaxf(st1.w + dp1, 0.0f);
-    *dpar0 = dp;
-    *dpar1 = dp1;
-    *d2_1 = fmaf(al1, al1, qq1);
-    return fmaf(al0, al0, qq);
-}
-
 template <int MINB, int THREADS = kEvThreads, bool REGIONS = false>
 __global__ void __launch_bounds__(THREADS, MINB) k_bgki(EvArgs A) {
     extern __shared__ __align__(32) unsigned char smem_raw[];
@@ -934,20 +914,13 @@ __global__ void __launch_bounds__(THREADS, MINB) k_bgki(EvArgs A) {
             sb = __shfl_sync(0xffffffffu, sb, 0);
             if (sb >= nsb) break;
             sb = sb_at(s_order, sb, nsb);
-            // lane = (x, y) column of the 4x4x2 sub-block (lane & 15) and ray stream (lane >> 4):
-            // each half-warp covers the whole sub-block for one ray, a lane both cells of its column
-            const int col = lane & 15, stream = lane >> 4;
-            const CellLoc L0 = locate(p, ts, it.lt, sb, col, fp.sensor_x, fp.sensor_y, fp.sensor_z);
-            const CellLoc L1 = locate(p, ts, it.lt, sb, col | 16, fp.sensor_x, fp.sensor_y, fp.sensor_z);
-            const float dx = L0.x - L0.ox, dy = L0.y - L0.oy;  // exact (nearby floats)
-            const float dz = L0.z - L0.oz;
-            const float hz = (L1.z - L1.oz) - dz;  // the column's z step (one cell)
-            const float ls2c0 = L0.c >= 0 ? ls2 : -1.0f;  // cells outside the grid take no evidence
-            const float ls2c1 = L1.c >= 0 ? ls2 : -1.0f;
-            const double ox = L0.ox, oy = L0.oy, oz = L0.oz;
-            // sums of kernel values rounded to integer units (cell z0, cell z1); the unsigned
-            // conversion saturates a negative table value (the kernel's max(0, .)) to 0
-            unsigned long long ao0 = 0, af0 = 0, ao1 = 0, af1 = 0;
+            const CellLoc L = locate(p, ts, it.lt, sb, lane, fp.sensor_x, fp.sensor_y, fp.sensor_z);
+            const float dx = L.x - L.ox, dy = L.y - L.oy, dz = L.z - L.oz;  // exact (nearby floats)
+            const float ls2c = L.c >= 0 ? ls2 : -1.0f;  // cells outside the grid take no evidence
+            const double ox = L.ox, oy = L.oy, oz = L.oz;
+            // sums of kernel values rounded to integer units; the unsigned conversion saturates a
+            // negative table value (the kernel's max(0, .)) to 0
+            unsigned long long ao = 0, af = 0;
             // the rays to cull: the sub-block's region list, or every ray of the item
             const int q = sb_region(ts, sb);
             const int nlist = regions ? s_rcnt[q] : nr;
@@ -972,66 +945,37 @@ __global__ void __launch_bounds__(THREADS, MINB) k_bgki(EvArgs A) {
                 }
                 __syncwarp();
                 // rays whose point's sphere can reach the sub-block: occupied (mass_update.cu:48-52)
-                // and free (:54-71) evidence; two rays per step, one per half-warp
-                for (int j2 = 0; j2 < nn; j2 += 2) {
-                    const int jr = j2 + stream;
-                    if (jr < nn) {
-                        const float4 s0 = S.stage[wid][jr][0], s1 = S.stage[wid][jr][1], s2 = S.stage[wid][jr][2];
-                        const float vx = s2.x + dx, vy = s2.y + dy, vz = s2.z + dz;
-                        const float d2o0 = vx * vx + vy * vy + vz * vz;
-                        // the cell above: v + (0, 0, hz)
-                        const float d2o1 = fmaf(hz, fmaf(2.0f, vz, hz), d2o0);
-                        if (d2o0 < ls2c0) {
-                            ao0 += __float2ull_rn(kernel_tab(S.ktab, d2o0 * tscale));
-                            ++nev;
-                        }
-                        if (d2o1 < ls2c1) {
-                            ao1 += __float2ull_rn(kernel_tab(S.ktab, d2o1 * tscale));
-                            ++nev;
-                        }
-                        float dpar0, dpar1, d2f1;
-                        const float d2f0 = free_d2_pair(s0, s1, dx, dy, dz, hz, &dpar0, &dpar1, &d2f1);
-                        if (s2.w + dpar0 < 0.0f && d2f0 < ls2c0) {  // d_proj < d_m
-                            af0 += __float2ull_rn(kernel_tab(S.ktab, d2f0 * tscale));
-                            ++nev;
-                        }
-                        if (s2.w + dpar1 < 0.0f && d2f1 < ls2c1) {
-                            af1 += __float2ull_rn(kernel_tab(S.ktab, d2f1 * tscale));
-                            ++nev;
-                        }
+                // and free (:54-71) evidence
+                for (int j = 0; j < nn; ++j) {
+                    const float4 s0 = S.stage[wid][j][0], s1 = S.stage[wid][j][1], s2 = S.stage[wid][j][2];
+                    const float vx = s2.x + dx, vy = s2.y + dy, vz = s2.z + dz;
+                    const float d2o = vx * vx + vy * vy + vz * vz;
+                    if (d2o < ls2c) {
+                        ao += __float2ull_rn(kernel_tab(S.ktab, d2o * tscale));
+                        ++nev;
+                    }
+                    float dpar;
+                    const float d2f = free_d2(s0, s1, dx, dy, dz, &dpar);
+                    if (s2.w + dpar < 0.0f && d2f < ls2c) {  // d_proj < d_m
+                        af += __float2ull_rn(kernel_tab(S.ktab, d2f * tscale));
+                        ++nev;
                     }
                 }
                 // the other rays: free evidence only
-                for (int j2 = nn; j2 < nh; j2 += 2) {
-                    const int jr = j2 + stream;
-                    if (jr < nh) {
-                        float dpar0, dpar1, d2f1;
-                        const float d2f0 = free_d2_pair(S.stage[wid][jr][0], S.stage[wid][jr][1], dx, dy, dz, hz,
-                                                        &dpar0, &dpar1, &d2f1);
-                        if (d2f0 < ls2c0) {
-                            af0 += __float2ull_rn(kernel_tab(S.ktab, d2f0 * tscale));
-                            ++nev;
-                        }
-                        if (d2f1 < ls2c1) {
-                            af1 += __float2ull_rn(kernel_tab(S.ktab, d2f1 * tscale));
-                            ++nev;
-                        }
+                for (int j = nn; j < nh; ++j) {
+                    float dpar;
+                    const float d2f = free_d2(S.stage[wid][j][0], S.stage[wid][j][1], dx, dy, dz, &dpar);
+                    if (d2f < ls2c) {
+                        af += __float2ull_rn(kernel_tab(S.ktab, d2f * tscale));
+                        ++nev;
                     }
                 }
                 __syncwarp();
             }
-            // the two streams hold partial sums of the same cells: combine, then stream 0 adds
-            // the column's lower cell and stream 1 its upper cell
-            ao0 += __shfl_xor_sync(0xffffffffu, ao0, 16);
-            af0 += __shfl_xor_sync(0xffffffffu, af0, 16);
-            ao1 += __shfl_xor_sync(0xffffffffu, ao1, 16);
-            af1 += __shfl_xor_sync(0xffffffffu, af1, 16);
-            const int cmine = stream ? L1.c : L0.c;
-            const unsigned long long aom = stream ? ao1 : ao0, afm = stream ? af1 : af0;
-            if (cmine >= 0) {
-                unsigned long long* ac = A.acc + 2 * (long)(coff + cmine);
-                if (aom) atomicAdd(ac, aom);
-                if (afm) atomicAdd(ac + 1, afm);
+            if (L.c >= 0) {
+                unsigned long long* ac = A.acc + 2 * (long)(coff + L.c);
+                if (ao) atomicAdd(ac, ao);
+                if (af) atomicAdd(ac + 1, af);
             }
         }
         __threadfence();

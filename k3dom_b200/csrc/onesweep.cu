@@ -44,6 +44,7 @@ constexpr uint32_t kOsInc = 2u << 30;           // published: inclusive prefix t
 constexpr uint32_t kOsValue = (1u << 30) - 1u;
 constexpr int kOsHistBlocks = 148 * 4;
 constexpr int kOsWindow = 8;  // predecessor statuses read per look-back step
+constexpr int kOsPassBlocks = 3;  // CTAs per SM of a pass (its registers: tile loads in flight)
 
 // scratch layout (uint32 words): counters [kOsMaxPasses + 1] | histograms [passes][128] |
 // digit offsets [passes][128] | tile status [passes][tiles][128]
@@ -144,7 +145,7 @@ struct OsSmem {
 // One pass of BITS bits at `shift`. vals_in == nullptr: the value is the input position (the
 // first pass of an argsort). vals_out == nullptr: keys only.
 template <int BITS>
-__global__ void __launch_bounds__(kOsThreads, 4)
+__global__ void __launch_bounds__(kOsThreads, kOsPassBlocks)
 os_pass(const uint32_t* __restrict__ keys_in, const uint32_t* __restrict__ vals_in, long nmax, const uint32_t* dn,
         int shift, int pass, OsScratch sc, uint32_t* __restrict__ keys_out, uint32_t* __restrict__ vals_out,
         DevStatus* ds, uint32_t max_polls, int skip_tile) {
@@ -160,119 +161,129 @@ os_pass(const uint32_t* __restrict__ keys_in, const uint32_t* __restrict__ vals_
     // after a timeout in an earlier pass this pass's input is incomplete, so its digit counts no
     // longer match the histograms: write nothing (every output slot keeps an in-range value)
     if (pass > 0 && *(volatile unsigned int*)&ds->sort_timeout) return;
-    if (threadIdx.x == 0) S.tile = atomicAdd(&sc.counters[pass], 1u);
-    // the counters' rows are kOsDigits wide whatever the pass's width: clear them all
-    for (int i = threadIdx.x; i < NW * kOsDigits; i += kOsThreads) (&S.cnt[0][0])[i] = 0;
-    __syncthreads();
-    const long tile = S.tile;
-    if (tile >= ntiles) return;  // past the live count (the grid covers nmax)
-    const long tbase = tile * kOsTile;
     uint32_t* status = sc.status + ((long)pass * cap_tiles) * kOsDigits;
+    // persistent CTAs: each takes tiles from the counter until none is left
+    for (;;) {
+        if (threadIdx.x == 0) S.tile = atomicAdd(&sc.counters[pass], 1u);
+        // the counters' rows are kOsDigits wide whatever the pass's width: clear them all
+        for (int i = threadIdx.x; i < NW * kOsDigits; i += kOsThreads) (&S.cnt[0][0])[i] = 0;
+        __syncthreads();
+        const long tile = S.tile;
+        if (tile >= ntiles) return;  // no live tile left
+        const long tbase = tile * kOsTile;
 
-    // stable rank within the tile: warp w holds keys [w*512, w*512 + 512) in (item, lane) order
-    uint32_t key[kOsItems], val[kOsItems];
-    uint16_t rank[kOsItems];
-#pragma unroll
-    for (int j = 0; j < kOsItems; ++j) {
-        const long i = tbase + wid * (kOsItems * 32) + j * 32 + lane;
-        const bool valid = i < n;
-        key[j] = valid ? keys_in[i] : 0u;
-        val[j] = valid ? (vals_in ? vals_in[i] : (uint32_t)i) : 0u;
-        const uint32_t d = valid ? ((key[j] >> shift) & (NB - 1)) : 0xFFFFFFFFu;
-        const unsigned peers = __match_any_sync(0xffffffffu, d);
-        const int leader = __ffs(peers) - 1;
-        uint32_t base = 0;
-        if (valid && lane == leader) {
-            base = S.cnt[wid][d];
-            S.cnt[wid][d] = (uint16_t)(base + __popc(peers));
+        // stable rank within the tile: warp w holds keys [w*512, w*512 + 512) in (item, lane) order;
+        // every load of the tile is issued before the ranking
+        uint32_t key[kOsItems], val[kOsItems];
+        uint16_t rank[kOsItems];
+    #pragma unroll
+        for (int j = 0; j < kOsItems; ++j) {
+            const long i = tbase + wid * (kOsItems * 32) + j * 32 + lane;
+            const bool valid = i < n;
+            key[j] = valid ? keys_in[i] : 0u;
+            val[j] = valid ? (vals_in ? vals_in[i] : (uint32_t)i) : 0u;
         }
-        base = __shfl_sync(0xffffffffu, base, leader);
-        rank[j] = (uint16_t)(base + __popc(peers & lt_mask));
-        __syncwarp();
-    }
-    __syncthreads();
-    // per digit: warp offsets (exclusive over warps) and the tile's count
-    uint32_t count = 0;
-    if (threadIdx.x < NB) {
-        const int d = threadIdx.x;
-#pragma unroll
-        for (int w = 0; w < NW; ++w) {
-            const uint32_t c = S.cnt[w][d];
-            S.cnt[w][d] = (uint16_t)count;
-            count += c;
-        }
-        if (tile != skip_tile) st_release(&status[tile * kOsDigits + d], kOsAgg | count);
-    }
-    // tile-local digit starts
-    {
-        uint32_t tot;
-        const uint32_t ex = block_exclusive_scan<uint32_t, kOsThreads>(count, S.scan_tmp, &tot);
-        if (threadIdx.x < NB) S.digit_start[threadIdx.x] = ex;
-    }
-    __syncthreads();
-    // the tile in digit order in shared memory (positions need no earlier tile), so the keys
-    // leave the registers before the look-back
-#pragma unroll
-    for (int j = 0; j < kOsItems; ++j) {
-        const long i = tbase + wid * (kOsItems * 32) + j * 32 + lane;
-        if (i < n) {
-            const uint32_t d = (key[j] >> shift) & (NB - 1);
-            const uint32_t pos = S.digit_start[d] + S.cnt[wid][d] + rank[j];
-            S.keys[pos] = key[j];
-            S.vals[pos] = val[j];
-        }
-    }
-    __syncthreads();
-    // decoupled look-back: keys of this digit in all earlier tiles. The statuses of kOsWindow
-    // predecessors are read at once (independent loads) and summed in order up to the first
-    // inclusive prefix; a predecessor not yet published ends the step there and is polled again.
-    // Tiles that start together publish only their counts at first, so a walk of one tile per
-    // dependent load would grow with the tile's distance from the last inclusive prefix.
-    bool timed_out = false;
-    if (threadIdx.x < NB) {
-        const int d = threadIdx.x;
-        uint32_t excl = 0;
-        uint32_t polls = 0;
-        long j = tile - 1;
-        while (j >= 0) {
-            uint32_t st_w[kOsWindow];
-#pragma unroll
-            for (int w = 0; w < kOsWindow; ++w)
-                st_w[w] = (j - w >= 0) ? ld_acquire(&status[(j - w) * kOsDigits + d]) : kOsInc;
-            int used = 0;
-            bool done = false;
-#pragma unroll
-            for (int w = 0; w < kOsWindow; ++w) {
-                if (done || used < w) continue;          // stopped at an earlier entry of the window
-                if ((st_w[w] & ~kOsValue) == 0u) continue;  // not yet published: poll it again
-                excl += st_w[w] & kOsValue;               // tiles before 0 read as an empty prefix
-                used = w + 1;
-                if (st_w[w] & kOsInc) done = true;
+    #pragma unroll
+        for (int j = 0; j < kOsItems; ++j) {
+            const long i = tbase + wid * (kOsItems * 32) + j * 32 + lane;
+            const bool valid = i < n;
+            const uint32_t d = valid ? ((key[j] >> shift) & (NB - 1)) : 0xFFFFFFFFu;
+            const unsigned peers = __match_any_sync(0xffffffffu, d);
+            const int leader = __ffs(peers) - 1;
+            uint32_t base = 0;
+            if (valid && lane == leader) {
+                base = S.cnt[wid][d];
+                S.cnt[wid][d] = (uint16_t)(base + __popc(peers));
             }
-            if (done) break;
-            if (used == 0) {
-                if (polls++ >= max_polls) {
-                    timed_out = true;
-                    break;
+            base = __shfl_sync(0xffffffffu, base, leader);
+            rank[j] = (uint16_t)(base + __popc(peers & lt_mask));
+            __syncwarp();
+        }
+        __syncthreads();
+        // per digit: warp offsets (exclusive over warps) and the tile's count
+        uint32_t count = 0;
+        if (threadIdx.x < NB) {
+            const int d = threadIdx.x;
+    #pragma unroll
+            for (int w = 0; w < NW; ++w) {
+                const uint32_t c = S.cnt[w][d];
+                S.cnt[w][d] = (uint16_t)count;
+                count += c;
+            }
+            if (tile != skip_tile) st_release(&status[tile * kOsDigits + d], kOsAgg | count);
+        }
+        // tile-local digit starts
+        {
+            uint32_t tot;
+            const uint32_t ex = block_exclusive_scan<uint32_t, kOsThreads>(count, S.scan_tmp, &tot);
+            if (threadIdx.x < NB) S.digit_start[threadIdx.x] = ex;
+        }
+        __syncthreads();
+        // the tile in digit order in shared memory (positions need no earlier tile), so the keys
+        // leave the registers before the look-back
+    #pragma unroll
+        for (int j = 0; j < kOsItems; ++j) {
+            const long i = tbase + wid * (kOsItems * 32) + j * 32 + lane;
+            if (i < n) {
+                const uint32_t d = (key[j] >> shift) & (NB - 1);
+                const uint32_t pos = S.digit_start[d] + S.cnt[wid][d] + rank[j];
+                S.keys[pos] = key[j];
+                S.vals[pos] = val[j];
+            }
+        }
+        __syncthreads();
+        // decoupled look-back: keys of this digit in all earlier tiles. The statuses of kOsWindow
+        // predecessors are read at once (independent loads) and summed in order up to the first
+        // inclusive prefix; a predecessor not yet published ends the step there and is polled again.
+        // Tiles that start together publish only their counts at first, so a walk of one tile per
+        // dependent load would grow with the tile's distance from the last inclusive prefix.
+        bool timed_out = false;
+        if (threadIdx.x < NB) {
+            const int d = threadIdx.x;
+            uint32_t excl = 0;
+            uint32_t polls = 0;
+            long j = tile - 1;
+            while (j >= 0) {
+                uint32_t st_w[kOsWindow];
+    #pragma unroll
+                for (int w = 0; w < kOsWindow; ++w)
+                    st_w[w] = (j - w >= 0) ? ld_acquire(&status[(j - w) * kOsDigits + d]) : kOsInc;
+                int used = 0;
+                bool done = false;
+    #pragma unroll
+                for (int w = 0; w < kOsWindow; ++w) {
+                    if (done || used < w) continue;          // stopped at an earlier entry of the window
+                    if ((st_w[w] & ~kOsValue) == 0u) continue;  // not yet published: poll it again
+                    excl += st_w[w] & kOsValue;               // tiles before 0 read as an empty prefix
+                    used = w + 1;
+                    if (st_w[w] & kOsInc) done = true;
                 }
-                __nanosleep(64);
+                if (done) break;
+                if (used == 0) {
+                    if (polls++ >= max_polls) {
+                        timed_out = true;
+                        break;
+                    }
+                    __nanosleep(64);
+                }
+                j -= used;
             }
-            j -= used;
+            if (!timed_out && tile != skip_tile) st_release(&status[tile * kOsDigits + d], kOsInc | (excl + count));
+            S.global_base[d] = sc.digit_off[pass * kOsDigits + d] + excl - S.digit_start[d];
         }
-        if (!timed_out && tile != skip_tile) st_release(&status[tile * kOsDigits + d], kOsInc | (excl + count));
-        S.global_base[d] = sc.digit_off[pass * kOsDigits + d] + excl - S.digit_start[d];
-    }
-    if (__syncthreads_or(timed_out)) {
-        if (threadIdx.x == 0) atomicOr(&ds->sort_timeout, 1u);
-        return;
-    }
-    const int valid_n = (int)min((long)kOsTile, n - tbase);
-    for (int k = threadIdx.x; k < valid_n; k += kOsThreads) {
-        const uint32_t kk = S.keys[k];
-        const uint32_t d = (kk >> shift) & (NB - 1);
-        const uint32_t dest = S.global_base[d] + k;
-        if (keys_out) keys_out[dest] = kk;
-        if (vals_out) vals_out[dest] = S.vals[k];
+        if (__syncthreads_or(timed_out)) {
+            if (threadIdx.x == 0) atomicOr(&ds->sort_timeout, 1u);
+            return;
+        }
+        const int valid_n = (int)min((long)kOsTile, n - tbase);
+        for (int k = threadIdx.x; k < valid_n; k += kOsThreads) {
+            const uint32_t kk = S.keys[k];
+            const uint32_t d = (kk >> shift) & (NB - 1);
+            const uint32_t dest = S.global_base[d] + k;
+            if (keys_out) keys_out[dest] = kk;
+            if (vals_out) vals_out[dest] = S.vals[k];
+        }
+        __syncthreads();  // the shared tile is reused by the next iteration
     }
 }
 
@@ -280,9 +291,15 @@ template <int BITS>
 static cudaError_t os_launch(const uint32_t* kin, const uint32_t* vin, long nmax, const uint32_t* dn, int shift,
                              int pass, OsScratch sc, uint32_t* kout, uint32_t* vout, DevStatus* ds,
                              uint32_t max_polls, int skip_tile, cudaStream_t st) {
-    const long ntiles = div_up(nmax, (long)kOsTile);
+    // persistent grid: at most one CTA per resident slot (tiles are handed out by the counter, in
+    // order, so a CTA only ever waits on tiles that running CTAs hold or have finished)
+    int dev = 0, sms = 148, per_sm = 1;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, os_pass<BITS>, kOsThreads, sizeof(OsSmem));
+    const long grid = std::min((long)div_up(nmax, (long)kOsTile), (long)sms * std::max(per_sm, 1));
     ++g_launches;
-    os_pass<BITS><<<(unsigned)ntiles, kOsThreads, sizeof(OsSmem), st>>>(kin, vin, nmax, dn, shift, pass, sc, kout,
+    os_pass<BITS><<<(unsigned)grid, kOsThreads, sizeof(OsSmem), st>>>(kin, vin, nmax, dn, shift, pass, sc, kout,
                                                                        vout, ds, max_polls, skip_tile);
     return cudaGetLastError();
 }

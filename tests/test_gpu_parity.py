@@ -167,6 +167,8 @@ class Lockstep:
                          ("born_mass", "born"), ("pred_mass", "pred")]:
             got = lib.get_cell_field(fld)
             n, e = rel_ok(got[ok], o[key][ok], 1e-3)
+            if n:
+                self.dump_cells(fld, key, got, o, ev, cells_in, sums, has, ok)
             assert n == 0, (fld, n, e)
             self.report[f"max_rel_{fld}"] = max(self.report.get(f"max_rel_{fld}", 0.0), float(e))
         dscale = np.maximum(np.abs(o["dyn"]), 1e-3)
@@ -180,6 +182,21 @@ class Lockstep:
                 assert n == 0, (fld, n, e)
                 self.report["max_rel_mean_vel"] = max(self.report.get("max_rel_mean_vel", 0.0), float(e))
         return o, ev
+
+    def dump_cells(self, fld, key, got, o, ev, cells_in, sums, has, ok):
+        """Prints every input and output of the worst cells of a failed mass bar."""
+        err = np.abs(got.astype(np.float64) - o[key]) / np.maximum(np.abs(o[key]), 1e-3)
+        err[~ok] = 0
+        lib = self.lib
+        fields = {k: lib.get_cell_field(k) for k in ("free_mass", "static_mass", "dynamic_mass", "born_mass",
+                                                     "pred_mass", "pers_mass", "del_occ", "del_free")}
+        for c in np.argsort(-err)[:6]:
+            print(f"cell {c} err {err[c]:.3g} has {has[c]} in f/s/d {cells_in['free_mass'][c]:.9g} "
+                  f"{cells_in['static_mass'][c]:.9g} {cells_in['dynamic_mass'][c]:.9g} start {cells_in['start_idx'][c]}")
+            print("   oracle", {k: float(o[k][c]) for k in ("free", "static", "dyn", "born", "pred", "pers")},
+                  "sum_w", float(sums[0][c]), "ev", float(ev["del_occ"][c]), float(ev["del_free"][c]),
+                  "tie", float(ev["tie_mass"][c]))
+            print("   lib   ", {k: float(v[c]) for k, v in fields.items()})
 
     def check_mu(self, o, ok):
         """The reweight factor mu_UA = pers / pred (update_persistent_particles.cu:17-55) against
@@ -239,9 +256,14 @@ class Lockstep:
             ref.init_particles(0, pts)
             r = ref.particles(0)
             np.testing.assert_array_equal(r["vel"], got["vel"])  # draws are per slot: identical
-            # slots: initParticlesKernel1 (init_new_particles.cu:54-68) on the reference's FP32 scan
-            self.count("init_slot_flips_vs_ref", self.slot_flips(got["cell"], r["cell"], cum, self.P, prev_cell,
-                                                                 "first-frame slots"))
+            # slots: initParticlesKernel1 (init_new_particles.cu:54-68). The reference formed its own
+            # born masses (its FP32 evidence), so its slots are held to the slot rule applied to
+            # those masses, exactly, with flips only within the FP32 bound of its thrust scan
+            ref_cum = O.exact_scan(ref.born())
+            o_ref = O.init_particles(ref_cum, self.P, self.G, self.p.init_max_velocity, self.p.particle_min_vel,
+                                     O.uniforms(self.p.seed, 0, 2, 0, self.P), prev_cell=prev_cell)
+            self.count("init_slot_flips_vs_ref", self.slot_flips(o_ref["cell"], r["cell"], ref_cum, self.P,
+                                                                 prev_cell, "first-frame slots"))
             ref.finish(t, False)
         lib.finishFrame(t)
         self.t_prev = t
@@ -350,8 +372,12 @@ class Lockstep:
             # (dsphdmib/kernel/mass_update.cu:52-60, update_persistent_particles.cu:49-55)
             c = srt["cell"]
             d = o_ds["div"][c]
-            exp = o_ds["mu"][c] * np.abs(base.astype(np.float64)) / np.where(d > 0, d, 1.0)
-            scale = np.maximum(np.abs(exp), 1e-9 * float(np.abs(base).max()))
+            wd = np.abs(base.astype(np.float64)) / np.where(d > 0, d, 1.0)
+            exp = o_ds["mu"][c] * wd
+            # mu = pers / pred carries pers's error on the occupied-mass scale (the bar of check_ds)
+            pred = np.where(o_ds["pred"][c] > 0, o_ds["pred"][c], 1.0)
+            mscale = np.maximum(np.abs(o_ds["mu"][c]), np.maximum(np.abs(o_ds["occ"][c]), 1e-4) / pred)
+            scale = np.maximum(wd * mscale, 1e-30)
             err = np.abs(np.abs(w2.astype(np.float64)) - exp) / scale
             assert err.max() < RTOL, ("DS reweight", float(err.max()))
             self.count("ds_divided_cells", int((o_ds["div"] > 0).sum()))
