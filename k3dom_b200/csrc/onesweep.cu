@@ -43,7 +43,7 @@ constexpr uint32_t kOsAgg = 1u << 30;           // published: this tile's count 
 constexpr uint32_t kOsInc = 2u << 30;           // published: inclusive prefix through this tile
 constexpr uint32_t kOsValue = (1u << 30) - 1u;
 constexpr int kOsHistBlocks = 148 * 4;
-constexpr int kOsWindow = 8;  // predecessor statuses read per look-back step
+constexpr int kOsWindow = 16;  // predecessor statuses read per look-back step
 constexpr int kOsPassBlocks = 3;  // CTAs per SM of a pass (its registers: tile loads in flight)
 
 // scratch layout (uint32 words): counters [kOsMaxPasses + 1] | histograms [passes][128] |
@@ -79,13 +79,15 @@ long onesweep_scratch_words(long n, int key_bits) {
     return (kOsMaxPasses + 1) + 2L * np * kOsDigits + (long)np * tiles * kOsDigits;
 }
 
-__device__ __forceinline__ uint32_t ld_acquire(const uint32_t* p) {
+// A tile's status word carries its flag and its count together and guards no other data, so
+// relaxed (coherent, unordered) accesses at device scope suffice.
+__device__ __forceinline__ uint32_t ld_status(const uint32_t* p) {
     uint32_t v;
-    asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    asm volatile("ld.relaxed.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
     return v;
 }
-__device__ __forceinline__ void st_release(uint32_t* p, uint32_t v) {
-    asm volatile("st.release.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+__device__ __forceinline__ void st_status(uint32_t* p, uint32_t v) {
+    asm volatile("st.relaxed.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
 }
 
 struct OsPasses {
@@ -210,7 +212,7 @@ os_pass(const uint32_t* __restrict__ keys_in, const uint32_t* __restrict__ vals_
                 S.cnt[w][d] = (uint16_t)count;
                 count += c;
             }
-            if (tile != skip_tile) st_release(&status[tile * kOsDigits + d], kOsAgg | count);
+            if (tile != skip_tile) st_status(&status[tile * kOsDigits + d], kOsAgg | count);
         }
         // tile-local digit starts
         {
@@ -247,7 +249,7 @@ os_pass(const uint32_t* __restrict__ keys_in, const uint32_t* __restrict__ vals_
                 uint32_t st_w[kOsWindow];
     #pragma unroll
                 for (int w = 0; w < kOsWindow; ++w)
-                    st_w[w] = (j - w >= 0) ? ld_acquire(&status[(j - w) * kOsDigits + d]) : kOsInc;
+                    st_w[w] = (j - w >= 0) ? ld_status(&status[(j - w) * kOsDigits + d]) : kOsInc;
                 int used = 0;
                 bool done = false;
     #pragma unroll
@@ -268,7 +270,7 @@ os_pass(const uint32_t* __restrict__ keys_in, const uint32_t* __restrict__ vals_
                 }
                 j -= used;
             }
-            if (!timed_out && tile != skip_tile) st_release(&status[tile * kOsDigits + d], kOsInc | (excl + count));
+            if (!timed_out && tile != skip_tile) st_status(&status[tile * kOsDigits + d], kOsInc | (excl + count));
             S.global_base[d] = sc.digit_off[pass * kOsDigits + d] + excl - S.digit_start[d];
         }
         if (__syncthreads_or(timed_out)) {
