@@ -10,8 +10,11 @@ Bars
     ranges, first-frame and birth slots, birth velocities, ancestors and the resampled set
     (against the oracle, whose exact prefix sums the library reproduces); the map shift of
     cells, map centre and particles;
-  * 1e-5 relative against the FP64 oracle (floor 1e-3 of the mass scale): masses, born,
-    persistent and predicted masses, mean velocities, the reweight factor mu_UA;
+  * 1e-5 relative (floor 1e-3 of the mass scale): the evidence against the FP64 oracle; masses,
+    born, persistent and predicted masses, mean velocities and the reweight factor mu_UA against
+    the FP64 update of the library's own evidence; masses end to end against the FP64 oracle,
+    with the FP64 update's own change between the two evidence values as the allowance (the
+    update moves mass by ~sqrt(evidence), so near zero evidence it is ill-conditioned);
   * against the reference: predictions and the sorted set are bit-exact; every slot and
     ancestor that differs from the reference's lies within the worst-case FP32 rounding bound
     of its thrust prefix sum of a boundary (tie rule; the flips are counted and printed); the
