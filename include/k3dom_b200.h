@@ -324,10 +324,10 @@ typedef struct k3dom_tuning {
     int32_t tile_rule, chunk, tuned, tuning, candidates, evidence_blocks;
     float best_ms;
     float candidate_ms[K3DOM_TUNE_MAX_CANDIDATES]; /* evidence stage time of each candidate */
-    /* evidence_blocks: CTAs of the evidence launch (K3DOM) or of the DS measurement pass, both
-     * persistent (one CTA per resident slot of the build that runs); evidence_fixup_blocks: CTAs
-     * of the DS pass that applies the first-100 rule to the cells past it (0 for K3DOM). */
-    int32_t evidence_fixup_blocks;
+    /* evidence_blocks: CTAs of the K3DOM evidence launch, or of the DS final (update) pass;
+     * evidence_count_blocks: CTAs of the DS count pass (0 for K3DOM). Both grids are
+     * persistent, one CTA per resident slot of the build that runs. */
+    int32_t evidence_count_blocks;
 } k3dom_tuning;
 k3dom_status k3dom_autotune(k3dom_handle* h, int enabled);
 k3dom_status k3dom_get_tuning(k3dom_handle* h, k3dom_tuning* out);

@@ -107,7 +107,7 @@ class Tuning(C.Structure):
     _fields_ = [
         ("tile_rule", C.c_int32), ("chunk", C.c_int32), ("tuned", C.c_int32), ("tuning", C.c_int32),
         ("candidates", C.c_int32), ("evidence_blocks", C.c_int32), ("best_ms", C.c_float),
-        ("candidate_ms", C.c_float * 16), ("evidence_fixup_blocks", C.c_int32),
+        ("candidate_ms", C.c_float * 16), ("evidence_count_blocks", C.c_int32),
     ]
 
 

@@ -159,6 +159,7 @@ struct k3dom_handle {
     bool births_done = false;
     int launches_per_frame = 0;
     int launches_upload = 0;  // kernels of the last frame's point upload (de-interleaving)
+    int ds_sized_chunk = 0;  // chunk the DS count buffer was sized for
 
     // evidence tuning
     int tile_rule = kRuleBySize;
@@ -408,7 +409,10 @@ cudaError_t alloc_ray_buffers(k3dom_handle* h) {
         rb.evals_alt = rb.evals;
     }
     if (h->ds()) {
-        if ((e = h->alloc(&rb.ds_over, std::max(h->C, 1), true, L))) return e;
+        h->ds_sized_chunk = std::max(32, h->chunk);
+        const long items_max = T + cap / h->ds_sized_chunk + 2;
+        rb.ds_count_capacity = ds_count_bytes(items_max);
+        if ((e = h->alloc(&rb.ds_counts, rb.ds_count_capacity, true, L))) return e;
     }
     // sort/scan scratch of the ray lists (their own: the lists are built beside the particle sort)
     rb.os_words = onesweep_scratch_words(cap, bits);
@@ -838,7 +842,7 @@ cudaError_t apply_tuning(k3dom_handle* h, int rule, int chunk) {
     if (e == cudaSuccess) e = cudaStreamSynchronize(h->st3);
     if (e != cudaSuccess) return e;
     // a smaller chunk makes more work items than the DS count buffer was sized for
-    const bool relayout = rule != h->tile_rule;
+    const bool relayout = rule != h->tile_rule || (h->ds() && chunk < h->ds_sized_chunk);
     h->tile_rule = rule;
     h->chunk = chunk;
     h->drop_graph();
@@ -1339,10 +1343,10 @@ k3dom_status k3dom_get_tuning(k3dom_handle* h, k3dom_tuning* out) {
     for (int k = 0; k < kTuneCount && k < (int)h->tune_ms.size() && k < K3DOM_TUNE_MAX_CANDIDATES; ++k)
         out->candidate_ms[k] = h->tune_ms[k];
     if (h->ds()) {
-        k3dom_ds_evidence_blocks(&out->evidence_blocks, &out->evidence_fixup_blocks);
+        k3dom_ds_evidence_blocks(&out->evidence_count_blocks, &out->evidence_blocks);
     } else {
         out->evidence_blocks = k3dom_evidence_blocks(h->rb.chunk);
-        out->evidence_fixup_blocks = 0;
+        out->evidence_count_blocks = 0;
     }
     return K3DOM_OK;
 }

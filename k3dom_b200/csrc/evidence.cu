@@ -307,7 +307,6 @@ __global__ void k_finish_lists(const uint32_t* __restrict__ item_off, int T, Dev
     status->nonfinite_points = 0;
     status->work_counter = 0;
     status->work_counter2 = 0;
-    status->ds_overflow = 0;
     status->kernel_evals = 0;
 }
 
@@ -520,7 +519,8 @@ struct EvArgs {
     const float4* ktab;  // S tables of kKernelTab entries, fixed-point scale folded in
     uint32_t* tile_done;
     unsigned long long* acc;
-    uint32_t* ds_over;  // DS: cells whose neighbours exceed the first-100 limit (capacity C)
+    uint8_t* ds_counts;
+    long ds_count_capacity;
     CellState cs;
     CellWork cw;
     DevStatus* status;
@@ -1135,13 +1135,8 @@ __device__ __forceinline__ float ds_pocc(float x, float y, float z, float4 m, fl
 // measurement-to-mass step for the whole tile.
 constexpr int kMaxTileCells = 16 * 16 * 8;
 
-// One pass over every (tile, chunk) work item. Per cell it gathers the number of neighbours (each
-// chunk counts at most kDsMaxNeighbors + 1, enough to tell a cell that exceeds the limit), and the
-// max occupied value and the all-farther flag of the first kDsMaxNeighbors neighbours the chunk
-// holds. A cell with at most kDsMaxNeighbors neighbours over all chunks has had every neighbour
-// counted, which is the first-100 rule's result; the last CTA of a tile updates those cells and
-// lists the others, which k_ds_overflow then measures with the rule itself.
-__global__ void __launch_bounds__(kEvThreads, 4) k_dsgrid(EvArgs A) {
+template <bool COUNT>
+__global__ void __launch_bounds__(kEvThreads, COUNT ? 5 : 4) k_dsgrid(EvArgs A) {
     __shared__ float4 sa[kChunk];  // (m, |m|^2)
     __shared__ float4 su[kChunk];  // (m / |m|, 0)
     __shared__ uint16_t s_cand[kEvWarps][32];
@@ -1155,11 +1150,10 @@ __global__ void __launch_bounds__(kEvThreads, 4) k_dsgrid(EvArgs A) {
     const unsigned lanes_below = (1u << lane) - 1u;
     const Batch& bt = A.bt;
     const uint32_t total_items = A.item_off[bt.T];
-    unsigned int* counter = &A.status->work_counter;
+    unsigned int* counter = COUNT ? &A.status->work_counter2 : &A.status->work_counter;
     uint32_t* part_max = reinterpret_cast<uint32_t*>(A.acc);
     uint32_t* part_flags = part_max + bt.C;
-    uint32_t* part_count = part_flags + bt.C;
-    unsigned nev = 0;  // accepted neighbours of this lane (the roofline's work count)
+    unsigned nev = 0;  // accepted neighbours of this lane (the roofline's work count, final pass)
 
     for (;;) {
         if (threadIdx.x == 0) {
@@ -1171,6 +1165,10 @@ __global__ void __launch_bounds__(kEvThreads, 4) k_dsgrid(EvArgs A) {
         const uint32_t item = s_item;
         if (item >= total_items) break;
         const Item it = item_of(bt, A.item_off, A.tile_start, item, A.chunk);
+        if (COUNT && (it.n_items == 1 || it.k == it.n_items - 1)) {  // uniform across the block
+            __syncthreads();
+            continue;
+        }
         const SceneDev& sd = bt.sc[it.sc];
         const DevParams& p = sd.p;
         const TileShape ts = sd.ts;
@@ -1243,8 +1241,17 @@ __global__ void __launch_bounds__(kEvThreads, 4) k_dsgrid(EvArgs A) {
             sb = sb_at(s_order, sb, nsb);
             const CellLoc L = locate(p, ts, it.lt, sb, lane, fp.sensor_x, fp.sensor_y, fp.sensor_z);
             const float acs = __fadd_rn(__fadd_rn(__fmul_rn(L.x, L.x), __fmul_rn(L.y, L.y)), __fmul_rn(L.z, L.z));
-            // one past the limit tells a cell that exceeds it (counted over chunks)
-            const int quota = L.c < 0 ? 0 : kDsMaxNeighbors + 1;
+            int quota = kDsMaxNeighbors;
+            if (!COUNT && it.n_items > 1) {
+                int pre = 0;
+                const long base = (long)A.item_off[it.t] * kMaxTileCells;
+                for (uint32_t kk = 0; kk < it.k; ++kk) {
+                    const long idx = base + (long)kk * kMaxTileCells + L.local;
+                    pre += (idx < A.ds_count_capacity) ? (int)A.ds_counts[idx] : 0;
+                }
+                quota = max(0, kDsMaxNeighbors - pre);
+            }
+            if (L.c < 0) quota = 0;
             int nb = 0;
             bool all_far = true;
             float mx = 0.0f;
@@ -1272,7 +1279,8 @@ __global__ void __launch_bounds__(kEvThreads, 4) k_dsgrid(EvArgs A) {
                     for (int k = 0; k < ncand; ++k) {
                         const float4 a = sa[s_cand[wid][k]];
                         if (nb < quota && ds_is_neighbor(L.x, L.y, L.z, acs, a, sd.wr2)) {
-                            if (++nb <= kDsMaxNeighbors) {
+                            ++nb;
+                            if (!COUNT) {
                                 ++nev;
                                 if (acs > a.w) all_far = false;
                                 const float o = ds_pocc(L.x, L.y, L.z, a, p.meas_occ_stddev);
@@ -1284,12 +1292,20 @@ __global__ void __launch_bounds__(kEvThreads, 4) k_dsgrid(EvArgs A) {
                     if (!__any_sync(0xffffffffu, nb < quota)) break;
                 }
             }
-            if (L.c >= 0 && nb > 0) {
+            if (COUNT) {
+                if (L.c >= 0) {
+                    const long idx = (long)item * kMaxTileCells + L.local;
+                    if (idx < A.ds_count_capacity) A.ds_counts[idx] = (uint8_t)nb;
+                }
+            } else if (L.c >= 0 && nb > 0) {
                 const int c = coff + L.c;
-                atomicAdd(&part_count[c], (uint32_t)nb);
                 atomicMax(&part_max[c], __float_as_uint(mx));
                 atomicOr(&part_flags[c], 1u | (all_far ? 0u : 2u));
             }
+        }
+        if (COUNT) {
+            __syncthreads();
+            continue;
         }
         __threadfence();
         __syncthreads();
@@ -1306,15 +1322,8 @@ __global__ void __launch_bounds__(kEvThreads, 4) k_dsgrid(EvArgs A) {
                 const int c = coff + ix + p.G * iy + p.G * p.G * iz;
                 const uint32_t m = __ldcg(&part_max[c]);
                 const uint32_t f = __ldcg(&part_flags[c]);
-                const uint32_t nbr = __ldcg(&part_count[c]);
                 if (m) __stcg(&part_max[c], 0u);
                 if (f) __stcg(&part_flags[c], 0u);
-                if (nbr) __stcg(&part_count[c], 0u);
-                if (nbr > (uint32_t)kDsMaxNeighbors) {  // the first-100 rule binds: k_ds_overflow
-                    const uint32_t slot = atomicAdd(&A.status->ds_overflow, 1u);
-                    if (slot < (uint32_t)bt.C) A.ds_over[slot] = c;
-                    continue;
-                }
                 float x, y, z;
                 centre_xyz(ix, iy, iz, p, fp.sensor_x, fp.sensor_y, fp.sensor_z, &x, &y, &z);
                 const float acs = __fadd_rn(__fadd_rn(__fmul_rn(x, x), __fmul_rn(y, y)), __fmul_rn(z, z));
@@ -1325,64 +1334,10 @@ __global__ void __launch_bounds__(kEvThreads, 4) k_dsgrid(EvArgs A) {
         }
         __syncthreads();
     }
+    if (!COUNT) {
 #pragma unroll
-    for (int o = 16; o > 0; o >>= 1) nev += __shfl_xor_sync(0xffffffffu, nev, o);
-    if (lane == 0 && nev) atomicAdd(&A.status->kernel_evals, (unsigned long long)nev);
-}
-
-// Cells with more than kDsMaxNeighbors neighbours: one warp per cell walks its tile's rays in
-// input order (the tile's entries, sorted stably by tile), tests each with the reference's FP32
-// test, and takes the first kDsMaxNeighbors (measurement_grid.cu:86-101), then updates the cell.
-// The tile's list holds every ray that can be a neighbour of its cells, so this is the same
-// neighbour sequence the chunks saw.
-__global__ void __launch_bounds__(kEvThreads) k_ds_overflow(EvArgs A) {
-    const int lane = threadIdx.x & 31;
-    const unsigned lanes_below = (1u << lane) - 1u;
-    const Batch& bt = A.bt;
-    const long n = min((long)A.status->ds_overflow, (long)bt.C);
-    const long warps = (long)gridDim.x * (kEvThreads / 32);
-    for (long w = (long)blockIdx.x * (kEvThreads / 32) + (threadIdx.x >> 5); w < n; w += warps) {
-        const int c = (int)A.ds_over[w];
-        const int sc = scene_of(bt.off->cell, bt.S, c);
-        const SceneDev& sd = bt.sc[sc];
-        const DevParams& p = sd.p;
-        const TileShape& ts = sd.ts;
-        const FrameParams fp = bt.fp[sc];
-        const int local = c - bt.off->cell[sc];
-        const int ix = local % p.G, iy = (local / p.G) % p.G, iz = local / (p.G * p.G);
-        const int t = bt.off->tile[sc] + ix / ts.tx + ts.ntx * (iy / ts.ty + ts.nty * (iz / ts.tz));
-        const uint32_t e0 = A.tile_start[t], e1 = A.tile_start[t + 1];
-        float x, y, z;
-        centre_xyz(ix, iy, iz, p, fp.sensor_x, fp.sensor_y, fp.sensor_z, &x, &y, &z);
-        const float acs = __fadd_rn(__fadd_rn(__fmul_rn(x, x), __fmul_rn(y, y)), __fmul_rn(z, z));
-        int nb = 0;
-        bool all_far = true;
-        float mx = 0.0f;
-        for (uint32_t base = e0; base < e1 && nb < kDsMaxNeighbors; base += 32) {
-            const uint32_t e = base + (uint32_t)lane;
-            bool hit = false;
-            float4 a = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
-            if (e < e1) {
-                uint32_t rid = A.evals[e];
-                if (rid >= (uint32_t)bt.N) rid = 0;
-                a = A.ray_a[rid];
-                hit = ds_is_neighbor(x, y, z, acs, a, sd.wr2);
-            }
-            const unsigned mask = __ballot_sync(0xffffffffu, hit);
-            if (hit && nb + __popc(mask & lanes_below) < kDsMaxNeighbors) {
-                if (acs > a.w) all_far = false;
-                const float o = ds_pocc(x, y, z, a, p.meas_occ_stddev);
-                if (o > mx) mx = o;
-            }
-            nb = min(kDsMaxNeighbors, nb + __popc(mask));
-        }
-        all_far = __all_sync(0xffffffffu, all_far);
-#pragma unroll
-        for (int o = 16; o > 0; o >>= 1) mx = fmaxf(mx, __shfl_xor_sync(0xffffffffu, mx, o));
-        if (lane == 0) {
-            const DsMeas mc = ds_meas_from(p, acs, nb > 0 ? 1 : 0, all_far, mx);
-            ds_cell_update(p, c, mc, A.cs, A.cw, A.first_frame != 0);
-        }
+        for (int o = 16; o > 0; o >>= 1) nev += __shfl_xor_sync(0xffffffffu, nev, o);
+        if (lane == 0 && nev) atomicAdd(&A.status->kernel_evals, (unsigned long long)nev);
     }
 }
 
@@ -1399,7 +1354,8 @@ static EvArgs make_args(const Batch& bt, RayBuffers& rb, CellState cs, CellWork 
     A.ktab = rb.ktab;
     A.tile_done = rb.tile_done;
     A.acc = rb.acc;
-    A.ds_over = rb.ds_over;
+    A.ds_counts = rb.ds_counts;
+    A.ds_count_capacity = rb.ds_count_capacity;
     A.cs = cs;
     A.cw = cw;
     A.status = status;
@@ -1659,24 +1615,25 @@ cudaError_t launch_k3dom_evidence(const Batch& bt, RayBuffers& rb, CellState cs,
     return cudaGetLastError();
 }
 
-// The DS launches: the measurement pass is persistent (one CTA per resident slot, 4 per SM), and
-// the overflow pass gives each listed cell a warp.
+// The DS launches are persistent too: the count pass and the final pass each get one CTA per
+// resident slot (the count pass fits 5 CTAs per SM at 47 registers, the final pass 4).
 struct DsLaunch {
-    int main_blocks, fixup_blocks;
+    int count_blocks, final_blocks;
 };
 
 static DsLaunch ds_launch() {
-    int dev = 0, sms = 148, per_sm = 1;
+    int dev = 0, sms = 148, per_count = 1, per_final = 1;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_dsgrid, kEvThreads, 0);
-    return DsLaunch{sms * std::max(1, per_sm), sms * 4};
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_count, k_dsgrid<true>, kEvThreads, 0);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_final, k_dsgrid<false>, kEvThreads, 0);
+    return DsLaunch{sms * std::max(1, per_count), sms * std::max(1, per_final)};
 }
 
-void k3dom_ds_evidence_blocks(int* main_blocks, int* fixup_blocks) {
+void k3dom_ds_evidence_blocks(int* count_blocks, int* final_blocks) {
     const DsLaunch L = ds_launch();
-    *main_blocks = L.main_blocks;
-    *fixup_blocks = L.fixup_blocks;
+    *count_blocks = L.count_blocks;
+    *final_blocks = L.final_blocks;
 }
 
 cudaError_t launch_ds_evidence(const Batch& bt, RayBuffers& rb, CellState cs, CellWork cw, bool first_frame,
@@ -1685,11 +1642,13 @@ cudaError_t launch_ds_evidence(const Batch& bt, RayBuffers& rb, CellState cs, Ce
     EvArgs A = make_args(bt, rb, cs, cw, first_frame, status);
     const DsLaunch L = ds_launch();
     ++g_launches;
-    k_dsgrid<<<L.main_blocks, kEvThreads, 0, st>>>(A);
+    k_dsgrid<true><<<L.count_blocks, kEvThreads, 0, st>>>(A);
     ++g_launches;
-    k_ds_overflow<<<L.fixup_blocks, kEvThreads, 0, st>>>(A);
+    k_dsgrid<false><<<L.final_blocks, kEvThreads, 0, st>>>(A);
     return cudaGetLastError();
 }
+
+long ds_count_bytes(long items) { return items * (long)kMaxTileCells; }
 
 cudaError_t evidence_init() {
     cudaError_t e = cudaFuncSetAttribute(k_bgki<3>, cudaFuncAttributeMaxDynamicSharedMemorySize,

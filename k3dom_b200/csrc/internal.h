@@ -144,13 +144,14 @@ struct RayBuffers {
     uint32_t* item_off;    // T+1 work-item offsets per tile
     uint32_t* tile_done;   // T
     unsigned long long* acc;  // 2*C fixed-point accumulators (K3DOM) / DS partials
-    uint32_t* ds_over;     // DS: cells past the first-100 limit, for the overflow pass (capacity C)
+    uint8_t* ds_counts;    // DS: per (item, cell) neighbour counts of pass 1
     uint32_t* scan_tmp;
     long scan_words;
     uint32_t* os_scratch;  // onesweep sort of the entries by tile
     long os_words;
     uint32_t* total;       // [0] = entries, [2] = entries kept (0 on overflow)
     long capacity;         // entries
+    long ds_count_capacity;
     int chunk;             // rays per work item
 };
 long ray_entries_bound(const DevParams& p, const TileShape& ts, int max_points, float bin_R);
@@ -165,8 +166,9 @@ cudaError_t launch_ds_evidence(const Batch& bt, RayBuffers& rb, CellState cs, Ce
                                DevStatus* status, cudaStream_t st);
 // CTAs of the K3DOM evidence launch for a chunk size (persistent grid).
 int k3dom_evidence_blocks(int chunk);
-// CTAs of the DS measurement pass (persistent) and of its overflow pass.
-void k3dom_ds_evidence_blocks(int* main_blocks, int* fixup_blocks);
+// CTAs of the DS count pass and final pass (persistent: one per resident slot of each build).
+void k3dom_ds_evidence_blocks(int* count_blocks, int* final_blocks);
+long ds_count_bytes(long items);
 cudaError_t evidence_init();
 // Host: the sparse-kernel table for sigma, every value multiplied by scale: 512 intervals and a
 // zero entry at u = 1 (513 float4), so an index taken at the support's edge needs no clamp.
