@@ -675,7 +675,7 @@ __device__ void k3dom_cell_update(const DevParams& p, double g, int c, double de
 // (dynamic, sized by the work item's ray count so that smaller chunks leave room for more CTAs)
 struct BgkiSmem {
     float4* ktab;                 // [kKernelTabEntries] sparse-kernel table of the current scene
-    float4 (*stage)[32][3];       // [warps][32][3]
+    float* stage;                 // [warps][kStageWarpFloats] pair records of the passing rays
     float4* a;                    // [chunk] m.x, m.y, m.z, d_m
     double4* c;                   // [chunk] d_m, margin, 1/d_m
     uint16_t* reg;                // [kRegions][chunk] rays per region of a 16x16 tile (region builds)
@@ -687,8 +687,19 @@ struct BgkiSmem {
 // cell of the column is in the column's list. Sub-blocks then cull only their column's rays.
 constexpr int kRegions = 4;
 
+// A pair record holds the staged constants of two rays a, b interleaved per component, so that one
+// 8-byte register pair feeds a packed instruction:
+//   float4 0: (perp0.x, perp0.y) of a, b     1: (perp0.z, par0)
+//   float4 2: (u.x, u.y)                     3: (u.z, par0 - margin)
+//   float4 4: (occ0.x, occ0.y)               5: (occ0.z, par0 - d_m)
+// each float4 as (a, b, a, b); a seventh float4 pads the record so that the 32 lanes' scalar
+// stores spread over the banks.
+constexpr int kStagePairFloats = 28;
+constexpr int kStageWarpFloats = 16 * kStagePairFloats;
+
 __host__ __device__ constexpr size_t bgki_fixed_bytes(int warps) {
-    return ((sizeof(float4) * kKernelTabEntries + sizeof(float4) * (size_t)warps * 32 * 3) + 31) & ~(size_t)31;
+    return ((sizeof(float4) * kKernelTabEntries + sizeof(float) * (size_t)warps * kStageWarpFloats) + 31) &
+           ~(size_t)31;
 }
 
 inline size_t bgki_smem_bytes(int chunk, int warps = kEvWarps, bool regions = false) {
@@ -699,7 +710,7 @@ inline size_t bgki_smem_bytes(int chunk, int warps = kEvWarps, bool regions = fa
 __device__ __forceinline__ BgkiSmem bgki_smem(unsigned char* base, int chunk, int warps) {
     BgkiSmem S;
     S.ktab = reinterpret_cast<float4*>(base);
-    S.stage = reinterpret_cast<float4(*)[32][3]>(base + sizeof(float4) * kKernelTabEntries);
+    S.stage = reinterpret_cast<float*>(base + sizeof(float4) * kKernelTabEntries);
     const size_t off = bgki_fixed_bytes(warps);
     S.c = reinterpret_cast<double4*>(base + off);  // 32-byte aligned
     S.a = reinterpret_cast<float4*>(base + off + sizeof(double4) * (size_t)chunk);
@@ -861,6 +872,98 @@ __device__ __forceinline__ float free_d2(const float4& st0, const float4& st1, f
     return qx * qx + qy * qy + qz * qz + al * al;
 }
 
+// Two FP32 values in one 8-byte register pair for the packed f32x2 instructions of sm_100a: one
+// instruction applies the same IEEE operation (round to nearest unless stated) to both halves, so
+// each half equals the scalar operation on it.
+struct F2 {
+    unsigned long long v;
+    static __device__ __forceinline__ F2 of(float a, float b) {
+        F2 r;
+        asm("mov.b64 %0, {%1, %2};" : "=l"(r.v) : "f"(a), "f"(b));
+        return r;
+    }
+    __device__ __forceinline__ void split(float& a, float& b) const {
+        asm("mov.b64 {%0, %1}, %2;" : "=f"(a), "=f"(b) : "l"(v));
+    }
+};
+__device__ __forceinline__ F2 add2(F2 a, F2 b) {
+    F2 d;
+    asm("add.rn.f32x2 %0, %1, %2;" : "=l"(d.v) : "l"(a.v), "l"(b.v));
+    return d;
+}
+__device__ __forceinline__ F2 add2_rd(F2 a, F2 b) {  // rounded toward -infinity
+    F2 d;
+    asm("add.rm.f32x2 %0, %1, %2;" : "=l"(d.v) : "l"(a.v), "l"(b.v));
+    return d;
+}
+__device__ __forceinline__ F2 sub2(F2 a, F2 b) {
+    F2 d;
+    asm("sub.rn.f32x2 %0, %1, %2;" : "=l"(d.v) : "l"(a.v), "l"(b.v));
+    return d;
+}
+__device__ __forceinline__ F2 mul2(F2 a, F2 b) {
+    F2 d;
+    asm("mul.rn.f32x2 %0, %1, %2;" : "=l"(d.v) : "l"(a.v), "l"(b.v));
+    return d;
+}
+__device__ __forceinline__ F2 fma2(F2 a, F2 b, F2 c) {
+    F2 d;
+    asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(d.v) : "l"(a.v), "l"(b.v), "l"(c.v));
+    return d;
+}
+
+// free_d2 for the two rays of a pair record (float4 0-3): the same operations in the same order.
+__device__ __forceinline__ F2 free_d2x2(const float4& b0, const float4& b1, const float4& b2, const float4& b3,
+                                        F2 DX, F2 DY, F2 DZ, F2* dpar) {
+    const F2 ux = F2::of(b2.x, b2.y), uy = F2::of(b2.z, b2.w), uz = F2::of(b3.x, b3.y);
+    const F2 dp = fma2(DZ, uz, fma2(DY, uy, mul2(DX, ux)));
+    const F2 ndp = mul2(dp, F2::of(-1.0f, -1.0f));  // exact
+    const F2 qx = fma2(ndp, ux, add2(F2::of(b0.x, b0.y), DX));
+    const F2 qy = fma2(ndp, uy, add2(F2::of(b0.z, b0.w), DY));
+    const F2 qz = fma2(ndp, uz, add2(F2::of(b1.x, b1.y), DZ));
+    float a0, a1, e0, e1;
+    add2(F2::of(b1.z, b1.w), dp).split(a0, a1);  // d_proj
+    add2(F2::of(b3.z, b3.w), dp).split(e0, e1);  // d_proj - margin
+    const F2 al = add2(F2::of(fminf(a0, 0.0f), fminf(a1, 0.0f)), F2::of(fmaxf(e0, 0.0f), fmaxf(e1, 0.0f)));
+    *dpar = dp;
+    return fma2(al, al, fma2(qz, qz, fma2(qy, qy, mul2(qx, qx))));
+}
+
+// tab_pos for two squared distances: t = d^2 * tscale, then the floor without conversions.
+struct TabPos2 {
+    TabPos a, b;
+};
+__device__ __forceinline__ TabPos2 tab_pos2(F2 d2, F2 tscale) {
+    const F2 c23 = F2::of(8388608.0f, 8388608.0f);
+    const F2 t = mul2(d2, tscale);
+    const F2 tr = add2_rd(t, c23);
+    const F2 f = sub2(t, sub2(tr, c23));
+    float ra, rb;
+    tr.split(ra, rb);
+    TabPos2 q;
+    q.a.i = __float_as_int(ra) - 0x4B000000;
+    q.b.i = __float_as_int(rb) - 0x4B000000;
+    f.split(q.a.f, q.b.f);
+    return q;
+}
+
+// Writes the three staged float4 of a passing ray into half (slot & 1) of pair record slot / 2.
+__device__ __forceinline__ void stage_put(float* stg, int slot, const float4 st[3]) {
+    float* d = stg + (slot >> 1) * kStagePairFloats + (slot & 1);
+    d[0] = st[0].x; d[2] = st[0].y; d[4] = st[0].z; d[6] = st[0].w;
+    d[8] = st[1].x; d[10] = st[1].y; d[12] = st[1].z; d[14] = st[1].w;
+    d[16] = st[2].x; d[18] = st[2].y; d[20] = st[2].z; d[22] = st[2].w;
+}
+
+// A pad ray in slot (odd, < 32): perpendicular and point offsets of 1e15 put every cell at a
+// squared distance near 3e30 (finite in FP32, far beyond ls^2), and d_proj - d_m = d_proj = 0
+// fails the d_proj < d_m test, so the pad adds nothing.
+__device__ __forceinline__ void stage_pad(float* stg, int slot) {
+    const float4 big = make_float4(1e15f, 1e15f, 1e15f, 0.0f);
+    const float4 st[3] = {big, make_float4(0.0f, 0.0f, 0.0f, 0.0f), big};
+    stage_put(stg, slot, st);
+}
+
 template <int MINB, int THREADS = kEvThreads, bool REGIONS = false>
 __global__ void __launch_bounds__(THREADS, MINB) k_bgki(EvArgs A) {
     extern __shared__ __align__(32) unsigned char smem_raw[];
@@ -918,6 +1021,8 @@ __global__ void __launch_bounds__(THREADS, MINB) k_bgki(EvArgs A) {
             const float dx = L.x - L.ox, dy = L.y - L.oy, dz = L.z - L.oz;  // exact (nearby floats)
             const float ls2c = L.c >= 0 ? ls2 : -1.0f;  // cells outside the grid take no evidence
             const double ox = L.ox, oy = L.oy, oz = L.oz;
+            const F2 DX = F2::of(dx, dx), DY = F2::of(dy, dy), DZ = F2::of(dz, dz), TS = F2::of(tscale, tscale);
+            float* stg = S.stage + wid * kStageWarpFloats;
             // sums of kernel values rounded to integer units; the unsigned conversion saturates a
             // negative table value (the kernel's max(0, .)) to 0
             unsigned long long ao = 0, af = 0;
@@ -933,42 +1038,47 @@ __global__ void __launch_bounds__(THREADS, MINB) k_bgki(EvArgs A) {
                     const int r = regions ? (int)list[j] : j;
                     hit = stage_pair(S.a[r], S.c[r], ox, oy, oz, hres, cull_ls2, st, &near);
                 }
-                // compact the passing rays into the warp's staging list: near rays first
+                // compact the passing rays into the warp's staging list, near rays first, two rays
+                // to a pair record; an odd count ends in a pad ray that reaches no cell
                 const unsigned mnear = __ballot_sync(0xffffffffu, near);
                 const unsigned mfar = __ballot_sync(0xffffffffu, hit && !near);
                 const int nn = __popc(mnear), nh = nn + __popc(mfar);
-                if (hit) {
-                    float4* dst = S.stage[wid][near ? __popc(mnear & lanes_below) : nn + __popc(mfar & lanes_below)];
-                    dst[0] = st[0];
-                    dst[1] = st[1];
-                    if (near) dst[2] = st[2];
-                }
+                if (hit) stage_put(stg, near ? __popc(mnear & lanes_below) : nn + __popc(mfar & lanes_below), st);
+                if ((nh & 1) && lane == 0) stage_pad(stg, nh);
                 __syncwarp();
-                // rays whose point's sphere can reach the sub-block: occupied (mass_update.cu:48-52)
-                // and free (:54-71) evidence
-                for (int j = 0; j < nn; ++j) {
-                    const float4 s0 = S.stage[wid][j][0], s1 = S.stage[wid][j][1], s2 = S.stage[wid][j][2];
-                    const float vx = s2.x + dx, vy = s2.y + dy, vz = s2.z + dz;
-                    const float d2o = vx * vx + vy * vy + vz * vz;
-                    if (d2o < ls2c) {
-                        ao += __float2ull_rn(kernel_tab(S.ktab, d2o * tscale));
-                        ++nev;
-                    }
-                    float dpar;
-                    const float d2f = free_d2(s0, s1, dx, dy, dz, &dpar);
-                    if (s2.w + dpar < 0.0f && d2f < ls2c) {  // d_proj < d_m
-                        af += __float2ull_rn(kernel_tab(S.ktab, d2f * tscale));
-                        ++nev;
-                    }
+                // pairs holding a ray whose point's sphere can reach the sub-block: occupied
+                // (mass_update.cu:48-52) and free (:54-71) evidence; a far ray sharing such a pair
+                // adds nothing through the occupied term or the d_proj < d_m test (see stage_pair)
+                const int npn = (nn + 1) >> 1, npa = (nh + 1) >> 1;
+                for (int k = 0; k < npn; ++k) {
+                    const float4* B = reinterpret_cast<const float4*>(stg + k * kStagePairFloats);
+                    const float4 b0 = B[0], b1 = B[1], b2 = B[2], b3 = B[3], b4 = B[4], b5 = B[5];
+                    const F2 vx = add2(F2::of(b4.x, b4.y), DX), vy = add2(F2::of(b4.z, b4.w), DY);
+                    const F2 vz = add2(F2::of(b5.x, b5.y), DZ);
+                    const F2 d2o = fma2(vz, vz, fma2(vy, vy, mul2(vx, vx)));
+                    F2 dp;
+                    const F2 d2f = free_d2x2(b0, b1, b2, b3, DX, DY, DZ, &dp);
+                    const F2 toend = add2(F2::of(b5.z, b5.w), dp);  // d_proj - d_m
+                    float oa, ob, fa, fb, ea, eb;
+                    d2o.split(oa, ob);
+                    d2f.split(fa, fb);
+                    toend.split(ea, eb);
+                    const TabPos2 po = tab_pos2(d2o, TS), pf = tab_pos2(d2f, TS);
+                    if (oa < ls2c) { ao += __float2ull_rn(tab_eval(S.ktab, po.a)); ++nev; }
+                    if (ob < ls2c) { ao += __float2ull_rn(tab_eval(S.ktab, po.b)); ++nev; }
+                    if (ea < 0.0f && fa < ls2c) { af += __float2ull_rn(tab_eval(S.ktab, pf.a)); ++nev; }
+                    if (eb < 0.0f && fb < ls2c) { af += __float2ull_rn(tab_eval(S.ktab, pf.b)); ++nev; }
                 }
-                // the other rays: free evidence only
-                for (int j = nn; j < nh; ++j) {
-                    float dpar;
-                    const float d2f = free_d2(S.stage[wid][j][0], S.stage[wid][j][1], dx, dy, dz, &dpar);
-                    if (d2f < ls2c) {
-                        af += __float2ull_rn(kernel_tab(S.ktab, d2f * tscale));
-                        ++nev;
-                    }
+                // the other pairs: free evidence only
+                for (int k = npn; k < npa; ++k) {
+                    const float4* B = reinterpret_cast<const float4*>(stg + k * kStagePairFloats);
+                    F2 dp;
+                    const F2 d2f = free_d2x2(B[0], B[1], B[2], B[3], DX, DY, DZ, &dp);
+                    float fa, fb;
+                    d2f.split(fa, fb);
+                    const TabPos2 pf = tab_pos2(d2f, TS);
+                    if (fa < ls2c) { af += __float2ull_rn(tab_eval(S.ktab, pf.a)); ++nev; }
+                    if (fb < ls2c) { af += __float2ull_rn(tab_eval(S.ktab, pf.b)); ++nev; }
                 }
                 __syncwarp();
             }
