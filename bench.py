@@ -781,9 +781,27 @@ def run_profile_case(args):
     medium: 128x128x32 voxels at 0.1 m, P=1,048,576, B=262,144, 60,000 points (state > L2, a few
     hundred MB on the device). config1: the benchmark's own scene (256x256x32, P=4,194,304,
     B=1,048,576, 120,000 points; about 1.5 GB on the device) with the tiling given by
-    --profile-tile-rule/--chunk."""
+    --profile-tile-rule/--chunk. batch: the 16 scenes of the batched measurement in one BatchDOM
+    (a few GB on the device)."""
     import k3dom_b200 as K
     from k3dom_b200 import scene
+    if args.profile_case == "batch":
+        cfgs = scene.config3(seed=args.batch_seed, n_scenes=args.scenes, variant=args.variant)
+        b = K.BatchDOM([K.make_params(args.variant, **c.params) for c in cfgs], args.variant)
+        if args.profile_tile_rule is not None:
+            b.set_tuning(args.profile_tile_rule, args.chunk)
+        for f in range(1 + args.steps):
+            ts, clouds = [], []
+            for s, c in enumerate(cfgs):
+                t = 0.1 + f * c.dt
+                sensor, pts = c.scene.scan(f, t, c.n_points)
+                b.updatePose(s, *sensor)
+                ts.append(t)
+                clouds.append(pts)
+            b.update(ts, clouds)
+        log("profile case done", b.diagnostics())
+        b.close()
+        return
     cfg = scene.config1(seed=5, variant=args.variant)
     if args.profile_case == "medium":
         cfg.params.update(size=12.8, particle_count=1 << 20, new_born_particle_count=1 << 18, max_points=60000)
@@ -810,7 +828,7 @@ def main(argv=None):
     ap.add_argument("--impl", choices=["ours", "reference", "reference-gpu"], default="ours")
     ap.add_argument("--variant", choices=["k3dom", "dsphdmib"], default="k3dom")
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--profile-case", choices=["medium", "config1"], default=None,
+    ap.add_argument("--profile-case", choices=["medium", "config1", "batch"], default=None,
                     help="run a mid-size scene for profiler captures instead of the benchmark")
     ap.add_argument("--workload", choices=["frame", "batch", "grad"], default="frame",
                     help="batch: only the batched-vs-plain line (16 scenes); grad: only the gradient step")

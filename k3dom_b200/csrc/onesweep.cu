@@ -101,7 +101,12 @@ __device__ __forceinline__ long os_count(long nmax, const uint32_t* dn) {
 }
 
 // Digit histograms of every pass in one read of the keys; the last CTA to finish turns them
-// into each pass's exclusive digit offsets (no CTA waits on another).
+// into each pass's exclusive digit offsets (no CTA waits on another). Each thread counts a run of
+// kOsHistRun consecutive keys and adds each digit's run length with one shared atomic: the
+// particles keep their cell order from frame to frame, so their keys arrive nearly sorted and
+// one atomic per key would serialise on a few shared counters.
+constexpr int kOsHistRun = 8;
+
 __global__ void __launch_bounds__(kOsThreads) os_hist(const uint32_t* __restrict__ keys, long nmax,
                                                       const uint32_t* dn, OsPasses ps, OsScratch sc) {
     __shared__ uint32_t h[kOsMaxPasses][kOsDigits];
@@ -109,9 +114,39 @@ __global__ void __launch_bounds__(kOsThreads) os_hist(const uint32_t* __restrict
     const long n = os_count(nmax, dn);
     for (int i = threadIdx.x; i < ps.np * kOsDigits; i += kOsThreads) (&h[0][0])[i] = 0;
     __syncthreads();
-    for (long i = (long)blockIdx.x * kOsThreads + threadIdx.x; i < n; i += (long)gridDim.x * kOsThreads) {
-        const uint32_t k = keys[i];
-        for (int p = 0; p < ps.np; ++p) atomicAdd(&h[p][(k >> ps.shift[p]) & ((1u << ps.bits[p]) - 1u)], 1u);
+    const long stride = (long)gridDim.x * kOsThreads * kOsHistRun;
+    const bool vec = (reinterpret_cast<uintptr_t>(keys) & 15u) == 0;
+    for (long base = ((long)blockIdx.x * kOsThreads + threadIdx.x) * kOsHistRun; base < n; base += stride) {
+        uint32_t k[kOsHistRun];
+        if (vec && base + kOsHistRun <= n) {  // 16-byte aligned: base is a multiple of 8 keys
+            const uint4 a = __ldg(reinterpret_cast<const uint4*>(keys + base));
+            const uint4 b = __ldg(reinterpret_cast<const uint4*>(keys + base) + 1);
+            k[0] = a.x; k[1] = a.y; k[2] = a.z; k[3] = a.w;
+            k[4] = b.x; k[5] = b.y; k[6] = b.z; k[7] = b.w;
+        } else {
+#pragma unroll
+            for (int i = 0; i < kOsHistRun; ++i) k[i] = base + i < n ? keys[base + i] : 0u;
+        }
+        const int m = (int)min((long)kOsHistRun, n - base);
+#pragma unroll
+        for (int p = 0; p < kOsMaxPasses; ++p) {
+            if (p >= ps.np) break;
+            const uint32_t mask = (1u << ps.bits[p]) - 1u;
+            const int sh = ps.shift[p];
+            uint32_t cur = (k[0] >> sh) & mask, run = 1;
+#pragma unroll
+            for (int i = 1; i < kOsHistRun; ++i) {
+                if (i >= m) break;
+                const uint32_t d = (k[i] >> sh) & mask;
+                if (d != cur) {
+                    atomicAdd(&h[p][cur], run);
+                    cur = d;
+                    run = 0;
+                }
+                ++run;
+            }
+            atomicAdd(&h[p][cur], run);
+        }
     }
     __syncthreads();
     for (int i = threadIdx.x; i < ps.np * kOsDigits; i += kOsThreads) {

@@ -446,7 +446,7 @@ k_slot_marks(Batch bt, const float* __restrict__ cum, int* __restrict__ marks) {
     }
 }
 
-constexpr int kBirthItems = 4;
+constexpr int kBirthItems = 1;  // slots per thread: one, so that every store of a slot is coalesced
 constexpr int kBirthTile = kBlock * kBirthItems;  // slots per block
 
 // (head, value): head = a scene's first slot (the running maximum restarts there)
