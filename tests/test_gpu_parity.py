@@ -182,14 +182,17 @@ class Lockstep:
             return O.k3dom_update(dt, self.p.gamma, self.p.birth_prob, self.p.mass_scale, e, cells_in["free_mass"],
                                   cells_in["static_mass"], cells_in["dynamic_mass"], has, *sums)
         o_lib = update(ev_lib)
-        half = {k: 0.5 * np.spacing(np.abs(v).astype(np.float32)).astype(np.float64) for k, v in ev_lib.items()}
-        corners = [update({"del_occ": ev_lib["del_occ"] + so * half["del_occ"],
-                           "del_free": ev_lib["del_free"] + sf * half["del_free"]})
+        half = {k: np.where(v > 0, 0.5 * np.spacing(np.abs(v).astype(np.float32)).astype(np.float64), 0.0)
+                for k, v in ev_lib.items()}
+        # (evidence is never negative: a zero stays zero)
+        corners = [update({"del_occ": np.maximum(ev_lib["del_occ"] + so * half["del_occ"], 0.0),
+                           "del_free": np.maximum(ev_lib["del_free"] + sf * half["del_free"], 0.0)})
                    for so in (-1.0, 1.0) for sf in (-1.0, 1.0)]
         for fld, key in [("free_mass", "free"), ("static_mass", "static"), ("dynamic_mass", "dyn"),
                          ("born_mass", "born"), ("pred_mass", "pred")]:
             got = lib.get_cell_field(fld)
             export = np.max([np.abs(c[key] - o_lib[key]) for c in corners], axis=0)
+            assert np.isfinite(export).all(), (fld, "allowance")
             n, e = rel_ok(got[ok], o_lib[key][ok], 1e-3, allow=export[ok])
             if n:
                 self.dump_cells(fld, key, got, o_lib, ev, cells_in, sums, has, ok)
