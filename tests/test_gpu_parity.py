@@ -170,24 +170,33 @@ class Lockstep:
         # z = del * sum of masses, i.e. by ~sqrt(del), and between static and dynamic mass by
         # (del_occ - del_free)+ and (del_free - del_occ)+: near zero evidence, and where the two
         # evidence terms nearly cancel, it turns small evidence differences into larger mass
-        # differences. So the masses are held (a) to the FP64 update applied to the library's own
-        # evidence, 1e-5 plus what the update moves within the FP32 rounding of that evidence as
-        # exported (the library updates from the exact sums), and (b) end to end to the FP64
-        # oracle, with (a)'s allowance plus what the FP64 update itself moves between the two
-        # evidence values; the cells that need an allowance are counted.
+        # differences; and the prediction splits (free + dynamic) into dynamic = the particles'
+        # weight sum and free = the rest, which cancels where the two are close. So the masses are
+        # held (a) to the FP64 update applied to the library's own inputs (its evidence, and the
+        # per-cell weight sums it stores in FP32 as the reference's GridCell does), 1e-5 plus what
+        # the update moves within the FP32 rounding of those inputs (the library updates from the
+        # exact evidence sums and rounds each FP64 weight sum once), and (b) end to end to the
+        # FP64 oracle, with (a)'s allowance plus what the FP64 update itself moves between the
+        # two sets of inputs; the cells that need an allowance are counted.
         ev_lib = {"del_occ": lib.get_cell_field("del_occ").astype(np.float64),
                   "del_free": lib.get_cell_field("del_free").astype(np.float64)}
+        sums_lib = tuple(np.asarray(x, np.float32).astype(np.float64) for x in sums)
 
-        def update(e):
+        def update(e, sw=None):
+            s_ = sums_lib if sw is None else (sw,) + sums_lib[1:]
             return O.k3dom_update(dt, self.p.gamma, self.p.birth_prob, self.p.mass_scale, e, cells_in["free_mass"],
-                                  cells_in["static_mass"], cells_in["dynamic_mass"], has, *sums)
+                                  cells_in["static_mass"], cells_in["dynamic_mass"], has, *s_)
+
+        def half_ulp(v):
+            return np.where(v > 0, 0.5 * np.spacing(np.abs(v).astype(np.float32)).astype(np.float64), 0.0)
         o_lib = update(ev_lib)
-        half = {k: np.where(v > 0, 0.5 * np.spacing(np.abs(v).astype(np.float32)).astype(np.float64), 0.0)
-                for k, v in ev_lib.items()}
-        # (evidence is never negative: a zero stays zero)
+        half = {k: half_ulp(v) for k, v in ev_lib.items()}
+        hw = half_ulp(sums_lib[0])
+        # (evidence and weight sums are never negative: a zero stays zero)
         corners = [update({"del_occ": np.maximum(ev_lib["del_occ"] + so * half["del_occ"], 0.0),
-                           "del_free": np.maximum(ev_lib["del_free"] + sf * half["del_free"], 0.0)})
-                   for so in (-1.0, 1.0) for sf in (-1.0, 1.0)]
+                           "del_free": np.maximum(ev_lib["del_free"] + sf * half["del_free"], 0.0)},
+                          np.maximum(sums_lib[0] + sw * hw, 0.0))
+                   for so in (-1.0, 1.0) for sf in (-1.0, 1.0) for sw in (-1.0, 1.0)]
         for fld, key in [("free_mass", "free"), ("static_mass", "static"), ("dynamic_mass", "dyn"),
                          ("born_mass", "born"), ("pred_mass", "pred")]:
             got = lib.get_cell_field(fld)
