@@ -780,11 +780,17 @@ cudaError_t enq_frame(k3dom_handle* h) {
     if ((e = enq_draws(h, h->st2))) return e;
     if ((e = cudaEventRecord(h->ev_join, h->st2))) return e;
     // the ray lists depend on the points only: built beside prediction and assignment, except
-    // when each stage is timed on its own
+    // when each stage is timed on its own. K3DOM's evidence needs only the lists, so it runs there
+    // too, and the cells are updated once both sides are done; DS's evidence pass needs the
+    // particles' per-cell counts throughout and follows assignment.
     const bool overlap = !h->timing;
+    const bool split = overlap && !h->ds();
     if (overlap) {
         if ((e = cudaStreamWaitEvent(h->st3, h->ev_fork, 0))) return e;
         if ((e = enq_binning(h, h->st3))) return e;
+        if (split && (e = launch_k3dom_evidence(h->batch(), h->rb, h->cells(), h->cw, false, h->status, h->st3,
+                                                false)))
+            return e;
         if ((e = cudaEventRecord(h->ev_bin, h->st3))) return e;
     }
     rec(h, 0);
@@ -792,7 +798,10 @@ cudaError_t enq_frame(k3dom_handle* h) {
     rec(h, 1);
     if ((e = enq_assign(h))) return e;
     rec(h, 2);
-    if (overlap) {
+    if (split) {
+        if ((e = cudaStreamWaitEvent(h->st, h->ev_bin, 0))) return e;
+        if ((e = launch_k3dom_update_cells(h->batch(), h->rb, h->cells(), h->cw, h->status, h->st))) return e;
+    } else if (overlap) {
         if ((e = cudaStreamWaitEvent(h->st, h->ev_bin, 0))) return e;
         if ((e = enq_evidence(h, false))) return e;
     } else if ((e = enq_occupancy(h, false))) {
@@ -947,9 +956,14 @@ k3dom_status k3dom_batch_create(const k3dom_params* params, int32_t n_scenes, k3
     h->B = B;
     h->C = C;
 
-    if ((e = cudaStreamCreateWithFlags(&h->st, cudaStreamNonBlocking))) return bail(e);
-    if ((e = cudaStreamCreateWithFlags(&h->st2, cudaStreamNonBlocking))) return bail(e);
-    if ((e = cudaStreamCreateWithFlags(&h->st3, cudaStreamNonBlocking))) return bail(e);
+    // the frame's own stream at the highest priority: where the evidence kernel runs beside
+    // prediction and assignment (on st3), the block scheduler hands freed SM slots to the
+    // particle stages first, which the evidence waits for at the cell update
+    int prio_low = 0, prio_high = 0;
+    if ((e = cudaDeviceGetStreamPriorityRange(&prio_low, &prio_high))) return bail(e);
+    if ((e = cudaStreamCreateWithPriority(&h->st, cudaStreamNonBlocking, prio_high))) return bail(e);
+    if ((e = cudaStreamCreateWithPriority(&h->st2, cudaStreamNonBlocking, prio_low))) return bail(e);
+    if ((e = cudaStreamCreateWithPriority(&h->st3, cudaStreamNonBlocking, prio_low))) return bail(e);
     if ((e = cudaStreamCreateWithFlags(&h->st4, cudaStreamNonBlocking))) return bail(e);
     if ((e = cudaEventCreateWithFlags(&h->ev_out, cudaEventDisableTiming))) return bail(e);
     if ((e = cudaEventCreateWithFlags(&h->ev_out_done, cudaEventDisableTiming))) return bail(e);
@@ -1218,7 +1232,9 @@ static k3dom_status update_impl(k3dom_handle* h, const float* t, const float* co
                 }
                 if (e != cudaSuccess) return h->fail(e);
                 h->graph = g;
-                if ((e = cudaGraphInstantiate(&h->graph_exec, g, 0))) return h->fail(e);
+                // the kernels keep their streams' priorities inside the graph
+                if ((e = cudaGraphInstantiate(&h->graph_exec, g, cudaGraphInstantiateFlagUseNodePriority)))
+                    return h->fail(e);
             }
             if ((e = cudaGraphLaunch(h->graph_exec, h->st))) return h->fail(e);
         }

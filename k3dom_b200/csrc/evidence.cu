@@ -526,6 +526,7 @@ struct EvArgs {
     DevStatus* status;
     int first_frame;
     int chunk;  // rays per work item (<= kChunk)
+    int fuse_update;  // K3DOM: the last CTA of a tile updates its cells (else k_k3dom_update_cells)
 };
 
 // ================================================================ K3DOM
@@ -1088,6 +1089,10 @@ __global__ void __launch_bounds__(THREADS, MINB) k_bgki(EvArgs A) {
                 if (af) atomicAdd(ac + 1, af);
             }
         }
+        if (!A.fuse_update) {  // the cells are updated by k_k3dom_update_cells after this kernel
+            __syncthreads();
+            continue;
+        }
         __threadfence();
         __syncthreads();
         if (threadIdx.x == 0) s_last = (atomicAdd(&A.tile_done[it.t], 1u) == it.n_items - 1) ? 1 : 0;
@@ -1471,6 +1476,7 @@ static EvArgs make_args(const Batch& bt, RayBuffers& rb, CellState cs, CellWork 
     A.status = status;
     A.first_frame = first_frame ? 1 : 0;
     A.chunk = rb.chunk;
+    A.fuse_update = 1;
     return A;
 }
 
@@ -1711,9 +1717,10 @@ int k3dom_evidence_blocks(int chunk) { return bgki_launch(chunk).blocks; }
 // Work items of up to 512 rays leave shared memory for a fourth CTA per SM; that build is limited
 // to 64 registers. Items of up to 256 rays run in 128-thread CTAs, 8 per SM. Both builds compute the same sums (exactly), so the choice is speed only.
 cudaError_t launch_k3dom_evidence(const Batch& bt, RayBuffers& rb, CellState cs, CellWork cw, bool first_frame,
-                                  DevStatus* status, cudaStream_t st) {
+                                  DevStatus* status, cudaStream_t st, bool fuse_update) {
     if (rb.chunk < 32 || rb.chunk > kChunk) return cudaErrorInvalidValue;
     EvArgs A = make_args(bt, rb, cs, cw, first_frame, status);
+    A.fuse_update = fuse_update ? 1 : 0;
     const BgkiLaunch L = bgki_launch(rb.chunk);
     ++g_launches;
     if (rb.chunk <= kSmallChunk)  // 128-thread CTAs: 8 per SM, each item's end waits on 4 warps
@@ -1722,6 +1729,32 @@ cudaError_t launch_k3dom_evidence(const Batch& bt, RayBuffers& rb, CellState cs,
         k_bgki<4, kEvThreads, true><<<L.blocks, L.threads, L.smem, st>>>(A);
     else
         k_bgki<3><<<L.blocks, L.threads, L.smem, st>>>(A);
+    return cudaGetLastError();
+}
+
+// The cell update of k_bgki's tile tails as a pass of its own over every cell: a steady frame
+// accumulates the evidence beside prediction and assignment (the evidence needs only the ray
+// lists) and updates the cells once the particles' per-cell sums are in. Each cell's two
+// fixed-point sums are read and cleared, then k3dom_cell_update runs as in the tail: same inputs,
+// same bits.
+__global__ void __launch_bounds__(kBlock) k_k3dom_update_cells(EvArgs A) {
+    const Batch& bt = A.bt;
+    ulonglong2* acc = reinterpret_cast<ulonglong2*>(A.acc);  // (occupied, free) per cell
+    for (long c = (long)blockIdx.x * blockDim.x + threadIdx.x; c < bt.C; c += (long)gridDim.x * blockDim.x) {
+        const int sc = scene_of(bt.off->cell, bt.S, (int)c);
+        const SceneDev& sd = bt.sc[sc];
+        const ulonglong2 v = acc[c];
+        if (v.x || v.y) acc[c] = make_ulonglong2(0ull, 0ull);
+        k3dom_cell_update(sd.p, bt.fp[sc].gamma_dt, (int)c, (double)(long long)v.x * sd.fx_inv,
+                          (double)(long long)v.y * sd.fx_inv, A.cs, A.cw, A.first_frame != 0);
+    }
+}
+
+cudaError_t launch_k3dom_update_cells(const Batch& bt, RayBuffers& rb, CellState cs, CellWork cw, DevStatus* status,
+                                      cudaStream_t st) {
+    const EvArgs A = make_args(bt, rb, cs, cw, false, status);
+    ++g_launches;
+    k_k3dom_update_cells<<<grid_for(bt.C), kBlock, 0, st>>>(A);
     return cudaGetLastError();
 }
 

@@ -161,7 +161,10 @@ void fill_scene_evidence(SceneDev& sd, bool ds, float4* ktab);
 cudaError_t build_ray_lists(const Batch& bt, const float* xs, const float* ys, const float* zs, RayBuffers& rb,
                             bool ds, DevStatus* status, const SortWait& wait, cudaStream_t st);
 cudaError_t launch_k3dom_evidence(const Batch& bt, RayBuffers& rb, CellState cs, CellWork cw, bool first_frame,
-                                  DevStatus* status, cudaStream_t st);
+                                  DevStatus* status, cudaStream_t st, bool fuse_update = true);
+// The cell update of a K3DOM frame whose evidence ran with fuse_update = false.
+cudaError_t launch_k3dom_update_cells(const Batch& bt, RayBuffers& rb, CellState cs, CellWork cw, DevStatus* status,
+                                      cudaStream_t st);
 cudaError_t launch_ds_evidence(const Batch& bt, RayBuffers& rb, CellState cs, CellWork cw, bool first_frame,
                                DevStatus* status, cudaStream_t st);
 // CTAs of the K3DOM evidence launch for a chunk size (persistent grid).
