@@ -216,6 +216,8 @@ struct k3dom_handle {
         graph = nullptr;
     }
     void free_ray_buffers() {
+        if (rb.ktex) cudaDestroyTextureObject(rb.ktex);
+        rb.ktex = 0;
         for (void* p : ray_allocs) cudaFree(p);
         ray_allocs.clear();
         if (pts_pinned) cudaFreeHost(pts_pinned);
@@ -382,6 +384,7 @@ cudaError_t alloc_ray_buffers(k3dom_handle* h) {
     std::vector<void*>* L = &h->ray_allocs;
     cudaError_t e;
     if ((e = h->alloc(&rb.ktab, (size_t)h->S * kKernelTableSize, true, L))) return e;
+    if ((e = make_kernel_table_texture(rb, h->S))) return e;
     if ((e = layout_points_tiles(h))) return e;
     long cap = 0;
     for (int s = 0; s < h->S; ++s)

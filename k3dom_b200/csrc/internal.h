@@ -131,6 +131,7 @@ struct RayBuffers {
     float4* ray_a;         // m.x, m.y, m.z, d_m (K3DOM) | |m|^2 (DS)
     double4* ray_c;        // d_m, margin, 1/d_m, 0 in FP64 (K3DOM)
     float4* ktab;          // per scene: sparse-kernel table with the fixed-point scale folded in
+    cudaTextureObject_t ktex;  // ktab read through the texture path (k_bgki), 0 when not made
     uint32_t* counts;      // per point slot: number of tiles touched
     uint32_t* offsets;     // exclusive scan of counts
     uint32_t* ekeys;       // entries: global tile id
@@ -155,6 +156,8 @@ struct RayBuffers {
     int chunk;             // rays per work item
 };
 long ray_entries_bound(const DevParams& p, const TileShape& ts, int max_points, float bin_R);
+// Texture object over the S kernel tables (point sampling, FP32 as stored), for k_bgki.
+cudaError_t make_kernel_table_texture(RayBuffers& rb, int S);
 // Per-scene evidence constants (binning radius, cull radius, fixed-point scale); writes the
 // scene's kernel table when ktab is not null.
 void fill_scene_evidence(SceneDev& sd, bool ds, float4* ktab);
