@@ -460,7 +460,8 @@ def run_ours(args):
                 "voxels": C_, "particles": P, "new_born": B, "points_per_frame": cfg.n_points,
                 "parallelism": f"replicas x{world} (independent scenes)",
                 "l2": "state > L2 (about 1 GB of particle/cell arrays touched per frame)",
-                "graph": True, "evidence_tiling": "autotuned (k3dom_autotune) during warm-up",
+                "graph": True, "evidence_tiling": ("autotuned (k3dom_autotune) during warm-up" if args.tile_rule is None
+                                                else f"fixed (--tile-rule {args.tile_rule} --chunk {args.chunk})"),
             },
             "e2e": {"value": round(m["e2e_fps"], 3), "unit": UNIT, "h2d_bytes_per_step": int(cfg.n_points * 12),
                     "d2h_bytes_per_step": int(C_ * 4),
