@@ -126,7 +126,6 @@ struct k3dom_handle {
     // gathers). Which of the two holds the current set is tracked at enqueue time; every full
     // frame ends with A current, so a captured frame's replays leave both flags as they were.
     float4* X = nullptr;
-    int* slot_marks = nullptr;  // births: first slot of each cell that owns slots
     bool a_current = true;   // A holds the current persistent set
     bool x_current = false;  // X holds it
     SegRec* seg_rec = nullptr;  // piece sums of the segmented per-cell sums, one per 128 sorted slots
@@ -710,7 +709,7 @@ cudaError_t enq_persistent(k3dom_handle* h) {
 cudaError_t enq_births(k3dom_handle* h) {
     cudaError_t e = exact_scan_plan(h->plan_born, h->plan_born_n, h->exact_scratch, h->st);
     if (e != cudaSuccess) return e;
-    launch_births(h->batch(), h->cells().born_m, h->born_cum, h->slot_marks, h->Bp, h->st);
+    launch_births(h->batch(), h->cells().born_m, h->born_cum, h->Bp, h->st);
     return cudaGetLastError();
 }
 
@@ -988,7 +987,6 @@ k3dom_status k3dom_batch_create(const k3dom_params* params, int32_t n_scenes, k3
         (e = h->alloc_particles(&h->Bp, B)))
         return bail(e);
     if ((e = h->alloc(&h->X, 2 * (size_t)P))) return bail(e);
-    if ((e = h->alloc(&h->slot_marks, std::max(B, 1)))) return bail(e);
     if ((e = h->alloc(&h->sorted_keys, P)) || (e = h->alloc(&h->perm, P)) || (e = h->alloc(&h->alt_k, P)) ||
         (e = h->alloc(&h->alt_v, P)) || (e = h->alloc(&h->seg_rec, seg_rec_count(P))) ||
         (e = h->alloc(&h->res_br, res_bracket_count(P))))

@@ -98,9 +98,7 @@ long seg_rec_count(long P);
 void launch_gather_segsum(const Batch& bt, const float4* x, Particles s, const uint32_t* sorted_keys,
                           const uint32_t* perm, CellWork cw, SegRec* rec, cudaStream_t st);
 void launch_reweight(const Batch& bt, Particles s, const uint32_t* sorted_keys, CellWork cw, cudaStream_t st);
-// marks: B_total ints of scratch (the first slot of each cell that owns slots).
-void launch_births(const Batch& bt, const float* born, const float* born_cum, int* marks, Particles b,
-                   cudaStream_t st);
+void launch_births(const Batch& bt, const float* born, const float* born_cum, Particles b, cudaStream_t st);
 void launch_init_particles(const Batch& bt, const float* born_cum, Particles a, cudaStream_t st);
 void launch_joint_prepare(const Batch& bt, Particles s, Particles b, cudaStream_t st);
 int draw_key_bits(int S);

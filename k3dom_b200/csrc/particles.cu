@@ -424,95 +424,15 @@ __device__ __forceinline__ void cell_centre_idx(int c, int G, float* x, float* y
 }
 
 // ---------------------------------------------------------------- births
-// initNewParticlesKernel1/2 (init_new_particles.cu:106-183). Cell j owns slots
-// [start(j), bound(j)) and the bounds are monotone in j, so the owner of slot s is the last cell
-// whose (non-empty) range starts at or before s, provided s < bound of that cell: every cell that
-// owns slots marks its first slot (k_slot_marks), and each block of slots takes a segmented
-// running maximum of the marks, seeded with one binary search for the slot before the block.
-// This replaces a 21-step dependent binary search per slot. Slots beyond the last cell's range
-// keep the previous frame's cell and association, exactly as the reference leaves them
-// unwritten. The penalty of penalizeStaticParticlesKernel (resampling.cu:35-42) is recorded in
-// the sign bit of the weight.
+// initNewParticlesKernel1/2 (init_new_particles.cu:106-183). One thread per birth slot
+// finds its cell by binary search instead of each cell looping over its slots. Slots
+// beyond the last cell's range keep the previous frame's cell and association, exactly as
+// the reference leaves them unwritten. The penalty of penalizeStaticParticlesKernel
+// (resampling.cu:35-42) is recorded in the sign bit of the weight.
 __global__ void __launch_bounds__(kBlock)
-k_slot_marks(Batch bt, const float* __restrict__ cum, int* __restrict__ marks) {
-    for (int g = blockIdx.x * blockDim.x + threadIdx.x; g < bt.C; g += gridDim.x * blockDim.x) {
-        const int sc = scene_of(bt.off->cell, bt.S, g);
-        const DevParams& p = bt.sc[sc].p;
-        const int coff = bt.off->cell[sc];
-        const SlotMap m = make_slotmap(cum + coff, p.C, p.B);
-        const int j = g - coff;
-        const int st = m.start(j), en = m.bound(j);
-        if (en > st && st >= 0 && st < p.B) marks[bt.off->birth[sc] + st] = j;
-    }
-}
-
-constexpr int kBirthItems = 1;  // slots per thread: one, so that every store of a slot is coalesced
-constexpr int kBirthTile = kBlock * kBirthItems;  // slots per block
-
-// (head, value): head = a scene's first slot (the running maximum restarts there)
-struct MaxSeg {
-    int head, v;
-};
-__device__ __forceinline__ MaxSeg max_seg(MaxSeg a, MaxSeg b) {  // a before b
-    return MaxSeg{a.head | b.head, b.head ? b.v : max(a.v, b.v)};
-}
-
-__global__ void __launch_bounds__(kBlock)
-k_births(Batch bt, const float* __restrict__ born, const float* __restrict__ cum, const int* __restrict__ marks,
-         Particles b) {
-    __shared__ MaxSeg s_warp[kBlock / 32];
-    __shared__ int s_carry;
-    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-    const int g0 = blockIdx.x * kBirthTile;
-    if (threadIdx.x == 0) {
-        // the owner of the slot before the block (-1: none, or the block starts a scene)
-        int carry = -1;
-        if (g0 > 0 && g0 < bt.B) {
-            const int sc = scene_of(bt.off->birth, bt.S, g0 - 1);
-            const int s = g0 - 1 - bt.off->birth[sc];
-            const DevParams& p = bt.sc[sc].p;
-            const SlotMap m = make_slotmap(cum + bt.off->cell[sc], p.C, p.B);
-            const int j = m.owner(s);
-            carry = j < p.C ? j : -1;
-        }
-        s_carry = carry;
-    }
-    // this thread's slots and their marks, then the running maximum within the thread
-    MaxSeg v[kBirthItems];
-    int scs[kBirthItems];
-#pragma unroll
-    for (int q = 0; q < kBirthItems; ++q) {
-        const int g = g0 + threadIdx.x * kBirthItems + q;
-        int sc = 0, head = 0, mk = -1;
-        if (g < bt.B) {
-            sc = scene_of(bt.off->birth, bt.S, g);
-            head = g == bt.off->birth[sc];
-            mk = marks[g];
-        }
-        scs[q] = sc;
-        v[q] = MaxSeg{head, mk};
-        if (q > 0) v[q] = max_seg(v[q - 1], v[q]);
-    }
-    // inclusive scan of the thread totals over the block
-    MaxSeg t = v[kBirthItems - 1];
-#pragma unroll
-    for (int d = 1; d < 32; d <<= 1) {
-        const MaxSeg o{__shfl_up_sync(0xffffffffu, t.head, d), __shfl_up_sync(0xffffffffu, t.v, d)};
-        if (lane >= d) t = max_seg(o, t);
-    }
-    if (lane == 31) s_warp[wid] = t;
-    __syncthreads();
-    MaxSeg before{0, s_carry};  // everything before this thread's first slot
-    for (int w = 0; w < wid; ++w) before = max_seg(before, s_warp[w]);
-    {
-        const MaxSeg o{__shfl_up_sync(0xffffffffu, t.head, 1), __shfl_up_sync(0xffffffffu, t.v, 1)};
-        if (lane > 0) before = max_seg(before, o);
-    }
-#pragma unroll
-    for (int q = 0; q < kBirthItems; ++q) {
-        const int g = g0 + threadIdx.x * kBirthItems + q;
-        if (g >= bt.B) break;
-        const int sc = scs[q];
+k_births(Batch bt, const float* __restrict__ born, const float* __restrict__ cum, Particles b) {
+    for (int g = blockIdx.x * blockDim.x + threadIdx.x; g < bt.B; g += gridDim.x * blockDim.x) {
+        const int sc = scene_of(bt.off->birth, bt.S, g);
         const DevParams& p = bt.sc[sc].p;
         const FrameParams& fp = bt.fp[sc];
         const int s = g - bt.off->birth[sc];  // slot within the scene
@@ -520,8 +440,7 @@ k_births(Batch bt, const float* __restrict__ born, const float* __restrict__ cum
         const int C = p.C;
         const float p_A = p.p_A;
         const SlotMap m = make_slotmap(cum + coff, C, p.B);
-        const MaxSeg own = max_seg(before, v[q]);
-        int j = own.v >= 0 && s < m.bound(own.v) ? own.v : C;
+        int j = m.owner(s);
         bool assoc;
         int n, st;
         if (j < C) {
@@ -558,13 +477,10 @@ k_births(Batch bt, const float* __restrict__ born, const float* __restrict__ cum
     }
 }
 
-void launch_births(const Batch& bt, const float* born, const float* born_cum, int* marks, Particles b,
-                   cudaStream_t st) {
+void launch_births(const Batch& bt, const float* born, const float* born_cum, Particles b, cudaStream_t st) {
     if (bt.B <= 0) return;
-    cudaMemsetAsync(marks, 0xFF, sizeof(int) * (size_t)bt.B, st);  // -1: no cell starts here
-    g_launches += 2;
-    k_slot_marks<<<grid_for(bt.C), kBlock, 0, st>>>(bt, born_cum, marks);
-    k_births<<<div_up(bt.B, kBirthTile), kBlock, 0, st>>>(bt, born, born_cum, marks, b);
+    ++g_launches;
+    k_births<<<grid_for(bt.B), kBlock, 0, st>>>(bt, born, born_cum, b);
 }
 
 // ---------------------------------------------------------------- first frame
