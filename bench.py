@@ -340,24 +340,9 @@ def measure_plain(args, variant: str, cfg, rank: int, world: int, local: int, di
         ms_max = max_over_ranks(ms, dist)
         launches = int(dom.diagnostics()["kernel_launches_per_frame"])
 
-        # per-stage device times and the evidence kernel's work (events on the handle's stream)
-        dom.set_timing(True)
-        st_acc, evals = [], []
-        for _ in range(2):
-            step_device(idx)
-            idx += 1
-            dom.synchronize()
-        for _ in range(min(Kst, 10)):
-            step_device(idx)
-            idx += 1
-            dom.synchronize()
-            st_acc.append(dom.stage_times())
-            evals.append(dom.diagnostics()["kernel_evaluations"])
-        dom.set_timing(False)
-        diag_after = dom.diagnostics()
-        stage = {k: float(np.mean([s[k] for s in st_acc])) for k in st_acc[0]}
-
-        # end to end through the C ABI: pinned host scan in, per-voxel occupancy out, every frame
+        # end to end on the frames right after the device-timed ones, so that the two rates see
+        # the same stretch of the scene
+        # (through the C ABI: pinned host scan in, per-voxel occupancy out, every frame)
         host_pts = [torch.from_numpy(f[2]).pin_memory() for f in frames]
         occ_out = torch.empty(dom.grid_cell_count, dtype=torch.float32).pin_memory()
         lib = dom._lib
@@ -384,6 +369,25 @@ def measure_plain(args, variant: str, cfg, rank: int, world: int, local: int, di
             idx += 1
             n_e2e += 1
         e2e_s = max_over_ranks(time.perf_counter() - t0, dist)
+        N.check(lib.k3dom_set_output(dom._h, 0, None, N.MEM_HOST), "set_output")
+
+        # per-stage device times and the evidence kernel's work (events on the handle's stream)
+        dom.set_timing(True)
+        st_acc, evals = [], []
+        for _ in range(2):
+            step_device(idx)
+            idx += 1
+            dom.synchronize()
+        for _ in range(min(Kst, 10)):
+            step_device(idx)
+            idx += 1
+            dom.synchronize()
+            st_acc.append(dom.stage_times())
+            evals.append(dom.diagnostics()["kernel_evaluations"])
+        dom.set_timing(False)
+        diag_after = dom.diagnostics()
+        stage = {k: float(np.mean([s[k] for s in st_acc])) for k in st_acc[0]}
+
         return {"ms": ms_max, "value": world * 1000.0 / ms_max, "e2e_fps": world * n_e2e / e2e_s,
                 "launches": launches, "stage": stage, "evals": float(np.mean(evals)), "tuning": tuning,
                 "diag": diag_after, "clocks": clocks, "frames": frames, "C": dom.grid_cell_count,
