@@ -17,10 +17,13 @@
 //    position a CTA writes is still correct (an abandoned tile published its counts before its
 //    look-back, so later tiles count past it), so the output holds the keys and values of the
 //    completed tiles and in-range old contents elsewhere; the later passes then write nothing.
-// 7-bit digits (21-bit cell keys of 2^21 voxels take three passes): 128 digits per tile keep the
-// runs long enough for coalesced writes. The element count may live in device memory (`dn`,
-// capped at nmax): the grid and scratch are sized for nmax, CTAs whose tile lies past the live
-// count return, and since tiles are handed out in order no CTA waits on one of them. The same
+// Digits of up to 8 bits, a key of b bits taking ceil(b / 8) passes of (nearly) equal width:
+// the 21-bit cell keys of 2^21 voxels three passes of 7 bits, the 24-bit resampling draws three
+// of 8 (four passes of 6 before: the draws' sort runs beside the particle sort and slowed it);
+// up to 256 digits per tile keep the runs long enough for coalesced writes. The element count
+// may live in device memory (`dn`, capped at nmax): the grid and scratch are sized for nmax,
+// CTAs whose tile lies past the live count return, and since tiles are handed out in order no
+// CTA waits on one of them. The same
 // sort orders the resampling draws (keys only) and the ray lists (tile of each entry, stable so
 // each tile keeps its rays in input order).
 #include <cuda_runtime.h>
@@ -36,7 +39,7 @@ namespace k3dom {
 constexpr int kOsThreads = 256;
 constexpr int kOsItems = 16;
 constexpr int kOsTile = kOsThreads * kOsItems;  // 4096 keys
-constexpr int kOsMaxBits = 7;
+constexpr int kOsMaxBits = 8;
 constexpr int kOsDigits = 1 << kOsMaxBits;
 constexpr int kOsMaxPasses = 5;                 // up to 35-bit keys (uint32 keys need at most 5)
 constexpr uint32_t kOsAgg = 1u << 30;           // published: this tile's count of the digit
@@ -46,8 +49,8 @@ constexpr int kOsHistBlocks = 148 * 4;
 constexpr int kOsWindow = 16;  // predecessor statuses read per look-back step
 constexpr int kOsPassBlocks = 3;  // CTAs per SM of a pass (its registers: tile loads in flight)
 
-// scratch layout (uint32 words): counters [kOsMaxPasses + 1] | histograms [passes][128] |
-// digit offsets [passes][128] | tile status [passes][tiles][128]
+// scratch layout (uint32 words): counters [kOsMaxPasses + 1] | histograms [passes][kOsDigits] |
+// digit offsets [passes][kOsDigits] | tile status [passes][tiles][kOsDigits]
 struct OsScratch {
     uint32_t* counters;  // tile counter of each pass, then the histogram CTAs' done counter
     uint32_t* hist;
@@ -384,7 +387,8 @@ cudaError_t onesweep_sort_pairs_dn(const uint32_t* keys, const uint32_t* vals, u
             case 4: e = os_launch<4>(ck, cv, n, dn, ps.shift[p], p, sc, ok, ov, ds, wait.max_polls, skip, st); break;
             case 5: e = os_launch<5>(ck, cv, n, dn, ps.shift[p], p, sc, ok, ov, ds, wait.max_polls, skip, st); break;
             case 6: e = os_launch<6>(ck, cv, n, dn, ps.shift[p], p, sc, ok, ov, ds, wait.max_polls, skip, st); break;
-            default: e = os_launch<7>(ck, cv, n, dn, ps.shift[p], p, sc, ok, ov, ds, wait.max_polls, skip, st); break;
+            case 7: e = os_launch<7>(ck, cv, n, dn, ps.shift[p], p, sc, ok, ov, ds, wait.max_polls, skip, st); break;
+            default: e = os_launch<8>(ck, cv, n, dn, ps.shift[p], p, sc, ok, ov, ds, wait.max_polls, skip, st); break;
         }
         if (e != cudaSuccess) return e;
         ck = ok;

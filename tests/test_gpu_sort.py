@@ -17,8 +17,8 @@ from oracle import binding as O
 pytestmark = pytest.mark.gpu
 
 
-def make_dom(P):
-    cfg = scene.small(seed=19, G=32, Gz=8, res=0.2, P=P, B=max(P // 4, 1), n_points=1500)
+def make_dom(P, G=32, Gz=8):
+    cfg = scene.small(seed=19, G=G, Gz=Gz, res=0.2, P=P, B=max(P // 4, 1), n_points=1500)
     cfg.params["seed"] = 77
     p = K.make_params("k3dom", **cfg.params)
     return cfg, K.DOM(p, "k3dom")
@@ -60,11 +60,14 @@ def test_sort_wait_timeout_is_reported_and_the_handle_recovers():
         dom.close()
 
 
-@pytest.mark.parametrize("P", [1000, 4095, 4096, 4097, 262144 + 123])
-def test_sort_sizes_and_ragged_tiles(P):
+@pytest.mark.parametrize("P,G,Gz", [(1000, 32, 8), (4095, 32, 8), (4096, 32, 8), (4097, 32, 8),
+                                    (262144 + 123, 32, 8), (262144 + 123, 64, 16)])
+def test_sort_sizes_and_ragged_tiles(P, G, Gz):
     """Particle counts around the 4,096-key tile (one key, a partial tile, exact tiles, one more)
-    and a large ragged count: permutation, sorted keys and cell ranges equal the oracle's."""
-    cfg, dom = make_dom(P)
+    and a large ragged count: permutation, sorted keys and cell ranges equal the oracle's. The
+    32x32x8 grid's 13-bit keys take passes of 7 and 6 bits, the 64x64x16 grid's 16-bit keys two of
+    8 bits (the widest digit)."""
+    cfg, dom = make_dom(P, G, Gz)
     try:
         frame(cfg, dom, 0)
         rng = np.random.default_rng(P)
