@@ -866,17 +866,6 @@ __device__ __forceinline__ bool stage_pair(const float4& a, const double4& cd, d
     return hit;
 }
 
-// Squared distance from the cell at offset (dx, dy, dz) from the anchor to the free segment
-// [0, margin u] of a staged ray (st0, st1); *dpar = delta.u.
-__device__ __forceinline__ float free_d2(const float4& st0, const float4& st1, float dx, float dy, float dz,
-                                         float* dpar) {
-    const float dp = dx * st1.x + dy * st1.y + dz * st1.z;
-    const float qx = st0.x + dx - dp * st1.x, qy = st0.y + dy - dp * st1.y, qz = st0.z + dz - dp * st1.z;
-    const float al = fminf(st0.w + dp, 0.0f) + fmaxf(st1.w + dp, 0.0f);
-    *dpar = dp;
-    return qx * qx + qy * qy + qz * qz + al * al;
-}
-
 // Two FP32 values in one 8-byte register pair for the packed f32x2 instructions of sm_100a: one
 // instruction applies the same IEEE operation (round to nearest unless stated) to both halves, so
 // each half equals the scalar operation on it.
@@ -917,7 +906,10 @@ __device__ __forceinline__ F2 fma2(F2 a, F2 b, F2 c) {
     return d;
 }
 
-// free_d2 for the two rays of a pair record (float4 0-3): the same operations in the same order.
+// Squared distances from the cell at offset (dx, dy, dz) from the anchor to the free segments
+// [0, margin u] of the two rays of a pair record (float4 0-3); *dpar = delta.u for each:
+// dp = delta.u, q = p + delta - dp u, al = min(par0 + dp, 0) + max(par0 - margin + dp, 0),
+// d^2 = |q|^2 + al^2.
 __device__ __forceinline__ F2 free_d2x2(const float4& b0, const float4& b1, const float4& b2, const float4& b3,
                                         F2 DX, F2 DY, F2 DZ, F2* dpar) {
     const F2 ux = F2::of(b2.x, b2.y), uy = F2::of(b2.z, b2.w), uz = F2::of(b3.x, b3.y);
@@ -1528,13 +1520,14 @@ void build_calib_tables(float4* f_tab, float4* dls_tab) {
 struct CalibSmem {
     float4* ftab;            // [kKernelTabEntries] unit kernel f, fixed-point scale folded in
     float4* htab;            // [kKernelTabEntries] -x f'(x), same scale
-    float4 (*stage)[32][3];  // [kEvWarps][32][3]
+    float* stage;            // [kEvWarps][kStageWarpFloats] pair records, as in k_bgki
     float4* a;               // [chunk]
     double4* c;              // [chunk]
     uint16_t* reg;           // [kRegions][chunk] (region builds)
 };
 
-constexpr size_t kCalibFixedBytes = 2 * sizeof(float4) * kKernelTabEntries + sizeof(float4) * kEvWarps * 32 * 3;
+constexpr size_t kCalibFixedBytes =
+    2 * sizeof(float4) * kKernelTabEntries + sizeof(float) * (size_t)kEvWarps * kStageWarpFloats;
 
 inline size_t calib_smem_bytes(int chunk, bool regions = false) {
     return ((kCalibFixedBytes + 31) & ~(size_t)31) + (size_t)chunk * (sizeof(float4) + sizeof(double4)) +
@@ -1545,7 +1538,7 @@ __device__ __forceinline__ CalibSmem calib_smem(unsigned char* base, int chunk) 
     CalibSmem S;
     S.ftab = reinterpret_cast<float4*>(base);
     S.htab = S.ftab + kKernelTabEntries;
-    S.stage = reinterpret_cast<float4(*)[32][3]>(base + 2 * sizeof(float4) * kKernelTabEntries);
+    S.stage = reinterpret_cast<float*>(base + 2 * sizeof(float4) * kKernelTabEntries);
     const size_t off = (kCalibFixedBytes + 31) & ~(size_t)31;
     S.c = reinterpret_cast<double4*>(base + off);
     S.a = reinterpret_cast<float4*>(base + off + sizeof(double4) * (size_t)chunk);
@@ -1610,10 +1603,17 @@ __global__ void __launch_bounds__(kEvThreads, MINB) k_bgki_sums(EvArgs A, const 
             const float dx = L.x - L.ox, dy = L.y - L.oy, dz = L.z - L.oz;
             const float ls2c = L.c >= 0 ? ls2 : -1.0f;
             const double ox = L.ox, oy = L.oy, oz = L.oz;
+            const F2 DX = F2::of(dx, dx), DY = F2::of(dy, dy), DZ = F2::of(dz, dz), TS = F2::of(tscale, tscale);
+            float* stg = S.stage + wid * kStageWarpFloats;
             long long fo = 0, ff = 0, ho = 0, hf = 0;
             const int q = sb_region(ts, sb);
             const int nlist = regions ? s_rcnt[q] : nr;
             const uint16_t* list = S.reg + q * A.chunk;
+            // one in-support evaluation: f (clamped at 0, as the kernel is) and -x f' at position t
+            auto eval = [&](TabPos t, long long& f, long long& h) {
+                f += __float2ll_rn(fmaxf(tab_eval(S.ftab, t), 0.0f));
+                h += __float2ll_rn(tab_eval(S.htab, t));
+            };
             for (int g0 = 0; g0 < nlist; g0 += 32) {
                 const int j = g0 + lane;
                 bool hit = false, near = false;
@@ -1622,41 +1622,47 @@ __global__ void __launch_bounds__(kEvThreads, MINB) k_bgki_sums(EvArgs A, const 
                     const int r = regions ? (int)list[j] : j;
                     hit = stage_pair(S.a[r], S.c[r], ox, oy, oz, hres, cull_ls2, st, &near);
                 }
+                // the staging of k_bgki: near rays first, two to a pair record, a pad ray last
                 const unsigned mnear = __ballot_sync(0xffffffffu, near);
                 const unsigned mfar = __ballot_sync(0xffffffffu, hit && !near);
                 const int nn = __popc(mnear), nh = nn + __popc(mfar);
-                if (hit) {
-                    float4* dst = S.stage[wid][near ? __popc(mnear & lanes_below) : nn + __popc(mfar & lanes_below)];
-                    dst[0] = st[0];
-                    dst[1] = st[1];
-                    if (near) dst[2] = st[2];
-                }
+                if (hit) stage_put(stg, near ? __popc(mnear & lanes_below) : nn + __popc(mfar & lanes_below), st);
+                if ((nh & 1) && lane == 0) stage_pad(stg, nh);
                 __syncwarp();
-                for (int j = 0; j < nn; ++j) {
-                    const float4 s0 = S.stage[wid][j][0], s1 = S.stage[wid][j][1], s2 = S.stage[wid][j][2];
-                    const float vx = s2.x + dx, vy = s2.y + dy, vz = s2.z + dz;
-                    const float d2o = vx * vx + vy * vy + vz * vz;
-                    if (d2o < ls2c) {
-                        const TabPos q = tab_pos(d2o * tscale);
-                        fo += __float2ll_rn(fmaxf(tab_eval(S.ftab, q), 0.0f));
-                        ho += __float2ll_rn(tab_eval(S.htab, q));
+                const int npn = (nn + 1) >> 1, npa = (nh + 1) >> 1;
+                for (int k = 0; k < npn; ++k) {
+                    const float4* B = reinterpret_cast<const float4*>(stg + k * kStagePairFloats);
+                    {  // occupied term
+                        const float4 b4 = B[4], b5 = B[5];
+                        const F2 vx = add2(F2::of(b4.x, b4.y), DX), vy = add2(F2::of(b4.z, b4.w), DY);
+                        const F2 vz = add2(F2::of(b5.x, b5.y), DZ);
+                        const F2 d2o = fma2(vz, vz, fma2(vy, vy, mul2(vx, vx)));
+                        float oa, ob;
+                        d2o.split(oa, ob);
+                        const TabPos2 po = tab_pos2(d2o, TS);
+                        if (oa < ls2c) eval(po.a, fo, ho);
+                        if (ob < ls2c) eval(po.b, fo, ho);
                     }
-                    float dpar;
-                    const float d2f = free_d2(s0, s1, dx, dy, dz, &dpar);
-                    if (s2.w + dpar < 0.0f && d2f < ls2c) {
-                        const TabPos q = tab_pos(d2f * tscale);
-                        ff += __float2ll_rn(fmaxf(tab_eval(S.ftab, q), 0.0f));
-                        hf += __float2ll_rn(tab_eval(S.htab, q));
-                    }
+                    F2 dp;
+                    const F2 d2f = free_d2x2(B[0], B[1], B[2], B[3], DX, DY, DZ, &dp);
+                    const float4 b5 = B[5];
+                    const F2 toend = add2(F2::of(b5.z, b5.w), dp);  // d_proj - d_m
+                    float fa, fb, ea, eb;
+                    d2f.split(fa, fb);
+                    toend.split(ea, eb);
+                    const TabPos2 pf = tab_pos2(d2f, TS);
+                    if (ea < 0.0f && fa < ls2c) eval(pf.a, ff, hf);
+                    if (eb < 0.0f && fb < ls2c) eval(pf.b, ff, hf);
                 }
-                for (int j = nn; j < nh; ++j) {
-                    float dpar;
-                    const float d2f = free_d2(S.stage[wid][j][0], S.stage[wid][j][1], dx, dy, dz, &dpar);
-                    if (d2f < ls2c) {
-                        const TabPos q = tab_pos(d2f * tscale);
-                        ff += __float2ll_rn(fmaxf(tab_eval(S.ftab, q), 0.0f));
-                        hf += __float2ll_rn(tab_eval(S.htab, q));
-                    }
+                for (int k = npn; k < npa; ++k) {
+                    const float4* B = reinterpret_cast<const float4*>(stg + k * kStagePairFloats);
+                    F2 dp;
+                    const F2 d2f = free_d2x2(B[0], B[1], B[2], B[3], DX, DY, DZ, &dp);
+                    float fa, fb;
+                    d2f.split(fa, fb);
+                    const TabPos2 pf = tab_pos2(d2f, TS);
+                    if (fa < ls2c) eval(pf.a, ff, hf);
+                    if (fb < ls2c) eval(pf.b, ff, hf);
                 }
                 __syncwarp();
             }

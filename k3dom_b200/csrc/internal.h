@@ -180,7 +180,7 @@ void build_kernel_table(float sigma, double scale, float4* out);
 constexpr int kKernelTableSize = 513;
 // Rays per calibration work item: the largest chunk whose evidence-sums build keeps 4 CTAs per
 // SM with its per-region ray lists in shared memory.
-constexpr int kCalibChunk = 480;
+constexpr int kCalibChunk = 448;
 // Calibration: unit-amplitude kernel and -x f'(x) tables scaled to units of 2^-kCalibShift.
 constexpr int kCalibShift = 40;
 void build_calib_tables(float4* f_tab, float4* dls_tab);
