@@ -503,7 +503,7 @@ cudaError_t ensure_ray_buffers(k3dom_calib* c, int max_points, float ls, const S
     const int T = sd.ts.ntx * sd.ts.nty * sd.ts.ntz;
     long need = std::max(ray_entries_bound(sd.p, sd.ts, std::max(max_points, 1), sd.bin_R), 4096L);
     if (need > 0xFFFFFFF0L) need = 0xFFFFFFF0L;
-    if (max_points <= c->ray_points && need <= c->rb[0].capacity && c->rb[0].ekeys) return cudaSuccess;
+    if (max_points <= c->ray_points && need <= c->rb[0].capacity && c->rb[0].evals2) return cudaSuccess;
     for (void* p : c->ray_allocs) cudaFree(p);
     c->ray_allocs.clear();
     for (int l = 0; l < k3dom_calib::kLanes; ++l) {
@@ -524,11 +524,14 @@ cudaError_t alloc_ray_lane(k3dom_calib* c, RayBuffers& rb, int max_points, long 
     std::vector<void*>* L = &c->ray_allocs;
     cudaError_t e;
     if ((e = c->alloc(&rb.ray_a, N, L)) || (e = c->alloc(&rb.ray_c, N, L)) || (e = c->alloc(&rb.counts, N, L)) ||
-        (e = c->alloc(&rb.offsets, N, L)) || (e = c->alloc(&rb.ekeys, cap, L)) || (e = c->alloc(&rb.evals, cap, L)) ||
-        (e = c->alloc(&rb.ekeys2, cap, L)) || (e = c->alloc(&rb.evals2, cap, L)) ||
-        (e = c->alloc(&rb.tile_start, T + 1, L)) || (e = c->alloc(&rb.tile_items, T, L)) ||
-        (e = c->alloc(&rb.item_off, T + 1, L)) || (e = c->alloc(&rb.tile_done, T, L)) ||
-        (e = c->alloc(&rb.total, 4, L)))
+        (e = c->alloc(&rb.evals2, cap, L)) || (e = c->alloc(&rb.tile_start, T + 1, L)) ||
+        (e = c->alloc(&rb.item_off, T + 1, L)) || (e = c->alloc(&rb.tile_done, T, L)) || (e = c->alloc(&rb.total, 4, L)))
+        return e;
+    if (placed_lists(false, T))  // lists placed per tile through tallies and cursors
+        return (e = c->alloc(&rb.tile_tally, T, L)) ? e : c->alloc(&rb.tile_cursor, T, L);
+    // lists sorted by tile
+    if ((e = c->alloc(&rb.offsets, N, L)) || (e = c->alloc(&rb.ekeys, cap, L)) || (e = c->alloc(&rb.evals, cap, L)) ||
+        (e = c->alloc(&rb.ekeys2, cap, L)) || (e = c->alloc(&rb.tile_items, T, L)))
         return e;
     int bits = 1;
     while ((1 << bits) < T + 1) ++bits;

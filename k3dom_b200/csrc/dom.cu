@@ -374,6 +374,8 @@ cudaError_t layout_points_tiles(k3dom_handle* h) {
     return cudaStreamSynchronize(h->st);
 }
 
+static cudaError_t alloc_points(k3dom_handle* h);
+
 // Buffers sized by the point slots and tiles: ray data, entry lists, tile lists, points.
 cudaError_t alloc_ray_buffers(k3dom_handle* h) {
     h->drop_graph();
@@ -394,12 +396,20 @@ cudaError_t alloc_ray_buffers(k3dom_handle* h) {
     rb.chunk = h->chunk;
     const int N = h->N, T = h->T;
     if ((e = h->alloc(&rb.ray_a, N, true, L)) || (e = h->alloc(&rb.ray_c, N, true, L)) ||
-        (e = h->alloc(&rb.counts, N, true, L)) || (e = h->alloc(&rb.offsets, N, true, L)) ||
-        (e = h->alloc(&rb.ekeys, cap, false, L)) || (e = h->alloc(&rb.evals, cap, false, L)) ||
-        (e = h->alloc(&rb.ekeys2, cap, false, L)) || (e = h->alloc(&rb.evals2, cap, false, L)) ||
-        (e = h->alloc(&rb.tile_start, T + 1, true, L)) || (e = h->alloc(&rb.tile_items, T, true, L)) ||
-        (e = h->alloc(&rb.item_off, T + 1, true, L)) || (e = h->alloc(&rb.tile_done, T, true, L)) ||
-        (e = h->alloc(&rb.acc, 2 * (size_t)h->C, true, L)) || (e = h->alloc(&rb.total, 4, true, L)))
+        (e = h->alloc(&rb.counts, N, true, L)) || (e = h->alloc(&rb.evals2, cap, false, L)) ||
+        (e = h->alloc(&rb.tile_start, T + 1, true, L)) || (e = h->alloc(&rb.item_off, T + 1, true, L)) ||
+        (e = h->alloc(&rb.tile_done, T, true, L)) || (e = h->alloc(&rb.acc, 2 * (size_t)h->C, true, L)) ||
+        (e = h->alloc(&rb.total, 4, true, L)))
+        return e;
+    if (placed_lists(h->ds(), T)) {  // per-tile tallies and cursors
+        if ((e = h->alloc(&rb.tile_tally, T, true, L)) || (e = h->alloc(&rb.tile_cursor, T, true, L))) return e;
+        return alloc_points(h);
+    }
+    // sorted lists: entries in ray order, sorted by tile with their own sort/scan scratch (the
+    // lists are built beside the particle sort)
+    if ((e = h->alloc(&rb.offsets, N, true, L)) || (e = h->alloc(&rb.ekeys, cap, false, L)) ||
+        (e = h->alloc(&rb.evals, cap, false, L)) || (e = h->alloc(&rb.ekeys2, cap, false, L)) ||
+        (e = h->alloc(&rb.tile_items, T, true, L)))
         return e;
     int bits = 1;
     while ((1 << bits) < T + 1) ++bits;
@@ -416,11 +426,18 @@ cudaError_t alloc_ray_buffers(k3dom_handle* h) {
         rb.ds_count_capacity = ds_count_bytes(items_max);
         if ((e = h->alloc(&rb.ds_counts, rb.ds_count_capacity, true, L))) return e;
     }
-    // sort/scan scratch of the ray lists (their own: the lists are built beside the particle sort)
     rb.os_words = onesweep_scratch_words(cap, bits);
     rb.scan_words = scan_u32_tiles(std::max((long)N, (long)T + 1)) + 16;
     if ((e = h->alloc(&rb.os_scratch, rb.os_words, true, L))) return e;
     if ((e = h->alloc(&rb.scan_tmp, rb.scan_words, true, L))) return e;
+    return alloc_points(h);
+}
+
+// The frame's point buffers: device scan (de-interleaved), its (x, y, z) upload and pinned staging.
+static cudaError_t alloc_points(k3dom_handle* h) {
+    const int N = h->N;
+    std::vector<void*>* L = &h->ray_allocs;
+    cudaError_t e;
     if ((e = h->alloc(&h->pts, 3 * (size_t)N, true, L))) return e;
     if ((e = h->alloc(&h->pts_xyz, 3 * (size_t)N, true, L))) return e;
     if ((e = cudaMallocHost((void**)&h->pts_pinned, 3 * (size_t)N * sizeof(float)))) return e;

@@ -13,16 +13,18 @@
 // ls, the DS window is 0.866 res wide -- so each ray is binned to the tiles of cells its
 // support can reach (segment sensor->point with radius ls for K3DOM, the half-line through
 // the point with the window radius for DS). Tiles of all scenes share one global numbering
-// (scene tile offset + local tile), so one sort builds every scene's lists. A tile's list keeps
-// rays in input order (stable sort by tile). One CTA takes one (tile, chunk of rays) work item
+// (scene tile offset + local tile), so one pass builds every scene's lists. K3DOM places each
+// ray into its tiles' ranges through per-tile tallies and cursors (its exact sums make the order
+// within a tile immaterial); DS keeps a tile's rays in input order (a stable sort by tile), as
+// its first-100 rule needs. One CTA takes one (tile, chunk of rays) work item
 // from a device work counter and stages the chunk's rays in shared memory; its warps pull the
 // tile's 4x4x2-cell sub-blocks from a block-local counter, cull 32 rays at a time with one
 // ballot, and every lane evaluates the surviving rays for its own cell.
 //
 // K3DOM evidence is summed in fixed point: each kernel value is rounded once to an integer
-// number of units of 2^-k sigma (the table carries the scale), summed exactly (FP64 within a
-// chunk, 64-bit integer atomics across chunks), so a cell's evidence is the same for any
-// tiling, chunking or scheduling. The
+// number of units of 2^-k sigma (the table carries the scale), summed exactly in 64-bit
+// integers (per lane, then atomics across sub-blocks and chunks), so a cell's evidence is the
+// same for any tiling, chunking, ray order or scheduling. The
 // last CTA to finish a tile's chunks runs the cell update for the whole tile. No block ever
 // waits on another.
 #include <cuda_runtime.h>
@@ -204,11 +206,21 @@ __device__ __forceinline__ BinGeom scene_geom(const SceneDev& sd, const FramePar
 }
 
 // Pass 1 over every point slot of every scene: per-ray constants and the number of tiles the
-// ray's support reaches (0 for slots past the scene's point count).
+// ray's support reaches (0 for slots past the scene's point count). TALLY (placed lists): each
+// reached tile's ray count is also added to tile_tally, through a block histogram of the T tiles
+// in shared memory (the tiles around a sensor are reached by nearly every ray: one global atomic
+// per block and tile instead of one per ray).
+template <bool TALLY>
 __global__ void k_ray_count(Batch bt, const float* __restrict__ xs, const float* __restrict__ ys,
                             const float* __restrict__ zs, int ds, float4* __restrict__ ra,
-                            double4* __restrict__ rc, uint32_t* __restrict__ counts, DevStatus* status) {
-    if (blockIdx.x == 0 && threadIdx.x == 0) status->overflow = 0u;  // per-frame flag (set by k_ray_emit)
+                            double4* __restrict__ rc, uint32_t* __restrict__ counts,
+                            uint32_t* __restrict__ tile_tally, DevStatus* status) {
+    extern __shared__ uint32_t s_tally[];  // [T] (TALLY)
+    if (blockIdx.x == 0 && threadIdx.x == 0) status->overflow = 0u;  // per-frame flag (set by k_ray_emit / k_tile_ranges)
+    if (TALLY) {
+        for (int t = threadIdx.x; t < bt.T; t += blockDim.x) s_tally[t] = 0u;
+        __syncthreads();
+    }
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < bt.N; i += gridDim.x * blockDim.x) {
         const int sc = scene_of(bt.off->point, bt.S, i);
         const FrameParams f = bt.fp[sc];
@@ -227,11 +239,22 @@ __global__ void k_ray_count(Batch bt, const float* __restrict__ xs, const float*
         rc[i] = cc;
         uint32_t c = 0;
         if (r.ok) {
-            for_each_tile(g, r.bx, r.by, r.bz, [&](int) { ++c; });
+            const uint32_t toff = (uint32_t)bt.off->tile[sc];
+            for_each_tile(g, r.bx, r.by, r.bz, [&](int t) {
+                ++c;
+                if (TALLY) atomicAdd(&s_tally[toff + (uint32_t)t], 1u);
+            });
         } else if (!(isfinite(mx) && isfinite(my) && isfinite(mz))) {
             atomicAdd(&status->nonfinite_points, 1ull);
         }
         counts[i] = c;
+    }
+    if (TALLY) {
+        __syncthreads();
+        for (int t = threadIdx.x; t < bt.T; t += blockDim.x) {
+            const uint32_t v = s_tally[t];
+            if (v) atomicAdd(&tile_tally[t], v);
+        }
     }
 }
 
@@ -310,6 +333,110 @@ __global__ void k_finish_lists(const uint32_t* __restrict__ item_off, int T, Dev
     status->kernel_evals = 0;
 }
 
+// K3DOM lists without a sort. The evidence sums are exact integers, so the order of a tile's
+// rays changes no result; k_ray_count<true> has tallied each tile's rays, this pass turns the
+// tallies into ranges (tile_start, and a cursor per tile for k_ray_place) and clears them for the
+// next frame, counts the work items per tile and their offsets, and ends the frame's list
+// counters as k_finish_lists does. One block: a batch holds at most a few tens of thousands of
+// tiles. On overflow (more entries than the list holds) every range is empty.
+constexpr int kRangeThreads = 1024;
+__global__ void __launch_bounds__(kRangeThreads)
+    k_tile_ranges(uint32_t* __restrict__ tile_tally, int T, int chunk, long capacity, uint32_t* __restrict__ tile_start,
+                  uint32_t* __restrict__ cursor, uint32_t* __restrict__ item_off, uint32_t* __restrict__ total,
+                  DevStatus* status) {
+    __shared__ unsigned long long sm[kRangeThreads / 32 + 1];
+    const int per = (T + kRangeThreads - 1) / kRangeThreads;
+    const int t0 = min(T, (int)threadIdx.x * per), t1 = min(T, t0 + per);
+    unsigned long long n = 0;
+    for (int t = t0; t < t1; ++t) n += tile_tally[t];
+    unsigned long long entries;
+    const unsigned long long base = block_exclusive_scan<unsigned long long, kRangeThreads>(n, sm, &entries);
+    const bool over = entries > (unsigned long long)capacity;
+    unsigned long long o = over ? 0ull : base;
+    unsigned long long ni = 0;
+    for (int t = t0; t < t1; ++t) {
+        const uint32_t c = over ? 0u : tile_tally[t];
+        tile_start[t] = (uint32_t)o;
+        cursor[t] = (uint32_t)o;
+        o += c;
+        ni += c == 0 ? 1u : (c + chunk - 1) / chunk;
+    }
+    unsigned long long items;
+    const unsigned long long ibase = block_exclusive_scan<unsigned long long, kRangeThreads>(ni, sm, &items);
+    unsigned long long io = ibase;
+    for (int t = t0; t < t1; ++t) {
+        const uint32_t c = over ? 0u : tile_tally[t];
+        item_off[t] = (uint32_t)io;
+        io += c == 0 ? 1u : (c + chunk - 1) / chunk;
+        tile_tally[t] = 0u;
+    }
+    if (threadIdx.x == 0) {
+        const uint32_t e32 = (uint32_t)min(entries, 0xFFFFFFFFull);
+        tile_start[T] = over ? 0u : e32;
+        item_off[T] = (uint32_t)items;
+        total[0] = e32;
+        total[2] = over ? 0u : e32;
+        if (over) atomicOr(&status->overflow, 1u);
+        status->work_items = (uint32_t)items;
+        status->ray_entries = e32;
+        // k_ray_count has finished counting this frame's non-finite points: keep the frame's count
+        status->nonfinite_frame = (unsigned int)status->nonfinite_points;
+        status->nonfinite_points = 0;
+        status->work_counter = 0;
+        status->work_counter2 = 0;
+        status->kernel_evals = 0;
+    }
+}
+
+// Pass 2 of the placed lists: each ray takes one slot in the range of each tile it reaches, at
+// most as many tiles as it tallied (the same enumeration as the tally's, on the same values), and
+// never a slot past the list. A block first counts
+// its rays' entries per tile in shared memory, reserves them with one atomic per tile on the
+// tile's cursor, then hands the reserved slots out in shared memory. The segment's far end is
+// formed from the staged ray constants as prep_ray forms it.
+template <typename F>
+__device__ __forceinline__ void for_each_placed_tile(const Batch& bt, const float4* __restrict__ ra,
+                                                     const uint32_t* __restrict__ counts, F f) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < bt.N; i += gridDim.x * blockDim.x) {
+        const uint32_t cnt = counts[i];
+        if (cnt == 0u) continue;
+        const int sc = scene_of(bt.off->point, bt.S, i);
+        const SceneDev& sd = bt.sc[sc];
+        const BinGeom g = scene_geom(sd, bt.fp[sc]);
+        const float4 a = ra[i];
+        const float bx = g.ax + a.x / sd.p.res, by = g.ay + a.y / sd.p.res, bz = g.az + a.z / sd.p.res;
+        const uint32_t toff = (uint32_t)bt.off->tile[sc];
+        uint32_t k = 0;
+        for_each_tile(g, bx, by, bz, [&](int t) {
+            if (k < cnt) {
+                f(i, toff + (uint32_t)t);
+                ++k;
+            }
+        });
+    }
+}
+
+__global__ void k_ray_place(Batch bt, const float4* __restrict__ ra, const uint32_t* __restrict__ counts,
+                            uint32_t* __restrict__ cursor, const uint32_t* __restrict__ total,
+                            uint32_t* __restrict__ evals) {
+    extern __shared__ uint32_t s_slot[];  // [T]: the block's entries per tile, then its next slot
+    const uint32_t n = total[2];
+    if (n == 0u) return;  // overflow, or no entries (the same for every thread)
+    for (int t = threadIdx.x; t < bt.T; t += blockDim.x) s_slot[t] = 0u;
+    __syncthreads();
+    for_each_placed_tile(bt, ra, counts, [&](int, uint32_t gt) { atomicAdd(&s_slot[gt], 1u); });
+    __syncthreads();
+    for (int t = threadIdx.x; t < bt.T; t += blockDim.x) {
+        const uint32_t v = s_slot[t];
+        if (v) s_slot[t] = atomicAdd(&cursor[t], v);
+    }
+    __syncthreads();
+    for_each_placed_tile(bt, ra, counts, [&](int i, uint32_t gt) {
+        const uint32_t pos = atomicAdd(&s_slot[gt], 1u);
+        if (pos < n) evals[pos] = (uint32_t)i;
+    });
+}
+
 // Largest |c| of a cell centre seen from a sensor inside or near the grid [m].
 static float max_extent(const DevParams& p) { return 2.0f * ((float)p.G * p.res * 1.7320508f + p.size_z); }
 
@@ -379,8 +506,24 @@ cudaError_t build_ray_lists(const Batch& bt, const float* xs, const float* ys, c
                             bool ds, DevStatus* status, const SortWait& wait, cudaStream_t st) {
     const int N = bt.N;
     const int T = bt.T;
+    if (placed_lists(ds, T)) {  // K3DOM: tally, ranges, place
+        const size_t hist = sizeof(uint32_t) * (size_t)T;
+        ++g_launches;
+        k_ray_count<true><<<grid_for(N), kBlock, hist, st>>>(bt, xs, ys, zs, 0, rb.ray_a, rb.ray_c, rb.counts,
+                                                              rb.tile_tally, status);
+        ++g_launches;
+        k_tile_ranges<<<1, kRangeThreads, 0, st>>>(rb.tile_tally, T, rb.chunk, rb.capacity, rb.tile_start,
+                                                   rb.tile_cursor, rb.item_off, rb.total, status);
+        ++g_launches;
+        k_ray_place<<<grid_for(N), kBlock, hist, st>>>(bt, rb.ray_a, rb.counts, rb.tile_cursor, rb.total,
+                                                        rb.evals2);
+        return cudaGetLastError();
+    }
+    // DS (and batches with more tiles than a block histogram holds): entries in ray order, then a
+    // stable sort by tile
     ++g_launches;
-    k_ray_count<<<grid_for(N), kBlock, 0, st>>>(bt, xs, ys, zs, ds ? 1 : 0, rb.ray_a, rb.ray_c, rb.counts, status);
+    k_ray_count<false><<<grid_for(N), kBlock, 0, st>>>(bt, xs, ys, zs, ds ? 1 : 0, rb.ray_a, rb.ray_c, rb.counts,
+                                                        nullptr, status);
     cudaError_t e = scan_u32_exclusive(rb.counts, rb.offsets, N, rb.scan_tmp, rb.total, st);
     if (e != cudaSuccess) return e;
     ++g_launches;

@@ -131,11 +131,13 @@ struct RayBuffers {
     float4* ktab;          // per scene: sparse-kernel table with the fixed-point scale folded in
     cudaTextureObject_t ktex;  // ktab read through the texture path (k_bgki), 0 when not made
     uint32_t* counts;      // per point slot: number of tiles touched
-    uint32_t* offsets;     // exclusive scan of counts
-    uint32_t* ekeys;       // entries: global tile id
-    uint32_t* evals;       // entries: point slot
-    uint32_t* ekeys2;      // sorted
-    uint32_t* evals2;
+    uint32_t* offsets;     // exclusive scan of counts (DS)
+    uint32_t* ekeys;       // entries: global tile id (DS)
+    uint32_t* evals;       // entries: point slot (DS)
+    uint32_t* ekeys2;      // sorted (DS)
+    uint32_t* evals2;      // the lists: point slots grouped by tile (K3DOM: placed, DS: sorted)
+    uint32_t* tile_tally;  // T: rays per tile (K3DOM), zero between frames
+    uint32_t* tile_cursor; // T: next free slot of each tile's range (K3DOM)
     uint32_t* ekeys_alt;
     uint32_t* evals_alt;
     uint32_t* tile_start;  // T+1
@@ -154,6 +156,10 @@ struct RayBuffers {
     int chunk;             // rays per work item
 };
 long ray_entries_bound(const DevParams& p, const TileShape& ts, int max_points, float bin_R);
+// K3DOM ray lists are placed per tile through block histograms of all T tiles in shared memory
+// (48 KB at most); DS lists, and batches with more tiles, are sorted by tile.
+constexpr int kPlacedMaxTiles = 12288;
+inline bool placed_lists(bool ds, int T) { return !ds && T <= kPlacedMaxTiles; }
 // Texture object over the S kernel tables (point sampling, FP32 as stored), for k_bgki.
 cudaError_t make_kernel_table_texture(RayBuffers& rb, int S);
 // Per-scene evidence constants (binning radius, cull radius, fixed-point scale); writes the
