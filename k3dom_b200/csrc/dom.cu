@@ -401,8 +401,10 @@ cudaError_t alloc_ray_buffers(k3dom_handle* h) {
         (e = h->alloc(&rb.tile_done, T, true, L)) || (e = h->alloc(&rb.acc, 2 * (size_t)h->C, true, L)) ||
         (e = h->alloc(&rb.total, 4, true, L)))
         return e;
-    if (placed_lists(h->ds(), T)) {  // per-tile tallies and cursors
-        if ((e = h->alloc(&rb.tile_tally, T, true, L)) || (e = h->alloc(&rb.tile_cursor, T, true, L))) return e;
+    if (placed_lists(h->ds(), T)) {  // per-tile tallies and per-block offsets
+        if ((e = h->alloc(&rb.tile_tally, T, true, L)) ||
+            (e = h->alloc(&rb.block_base, (size_t)bin_blocks(N) * T, true, L)))
+            return e;
         return alloc_points(h);
     }
     // sorted lists: entries in ray order, sorted by tile with their own sort/scan scratch (the

@@ -14,7 +14,7 @@
 // support can reach (segment sensor->point with radius ls for K3DOM, the half-line through
 // the point with the window radius for DS). Tiles of all scenes share one global numbering
 // (scene tile offset + local tile), so one pass builds every scene's lists. K3DOM places each
-// ray into its tiles' ranges through per-tile tallies and cursors (its exact sums make the order
+// ray into its tiles' ranges through per-block tallies of each tile (its exact sums make the order
 // within a tile immaterial); DS keeps a tile's rays in input order (a stable sort by tile), as
 // its first-100 rule needs. One CTA takes one (tile, chunk of rays) work item
 // from a device work counter and stages the chunk's rays in shared memory; its warps pull the
@@ -209,12 +209,14 @@ __device__ __forceinline__ BinGeom scene_geom(const SceneDev& sd, const FramePar
 // ray's support reaches (0 for slots past the scene's point count). TALLY (placed lists): each
 // reached tile's ray count is also added to tile_tally, through a block histogram of the T tiles
 // in shared memory (the tiles around a sensor are reached by nearly every ray: one global atomic
-// per block and tile instead of one per ray).
+// per block and tile instead of one per ray); the value that atomic returns is the block's first
+// slot in the tile's range (relative to its start), kept in block_base for k_ray_place.
 template <bool TALLY>
 __global__ void k_ray_count(Batch bt, const float* __restrict__ xs, const float* __restrict__ ys,
                             const float* __restrict__ zs, int ds, float4* __restrict__ ra,
                             double4* __restrict__ rc, uint32_t* __restrict__ counts,
-                            uint32_t* __restrict__ tile_tally, DevStatus* status) {
+                            uint32_t* __restrict__ tile_tally, uint32_t* __restrict__ block_base,
+                            DevStatus* status) {
     extern __shared__ uint32_t s_tally[];  // [T] (TALLY)
     if (blockIdx.x == 0 && threadIdx.x == 0) status->overflow = 0u;  // per-frame flag (set by k_ray_emit / k_tile_ranges)
     if (TALLY) {
@@ -251,9 +253,10 @@ __global__ void k_ray_count(Batch bt, const float* __restrict__ xs, const float*
     }
     if (TALLY) {
         __syncthreads();
+        uint32_t* row = block_base + (size_t)blockIdx.x * bt.T;
         for (int t = threadIdx.x; t < bt.T; t += blockDim.x) {
             const uint32_t v = s_tally[t];
-            if (v) atomicAdd(&tile_tally[t], v);
+            if (v) row[t] = atomicAdd(&tile_tally[t], v);
         }
     }
 }
@@ -335,15 +338,14 @@ __global__ void k_finish_lists(const uint32_t* __restrict__ item_off, int T, Dev
 
 // K3DOM lists without a sort. The evidence sums are exact integers, so the order of a tile's
 // rays changes no result; k_ray_count<true> has tallied each tile's rays, this pass turns the
-// tallies into ranges (tile_start, and a cursor per tile for k_ray_place) and clears them for the
+// tallies into ranges (tile_start) and clears them for the
 // next frame, counts the work items per tile and their offsets, and ends the frame's list
 // counters as k_finish_lists does. One block: a batch holds at most a few tens of thousands of
 // tiles. On overflow (more entries than the list holds) every range is empty.
 constexpr int kRangeThreads = 1024;
 __global__ void __launch_bounds__(kRangeThreads)
     k_tile_ranges(uint32_t* __restrict__ tile_tally, int T, int chunk, long capacity, uint32_t* __restrict__ tile_start,
-                  uint32_t* __restrict__ cursor, uint32_t* __restrict__ item_off, uint32_t* __restrict__ total,
-                  DevStatus* status) {
+                  uint32_t* __restrict__ item_off, uint32_t* __restrict__ total, DevStatus* status) {
     __shared__ unsigned long long sm[kRangeThreads / 32 + 1];
     const int per = (T + kRangeThreads - 1) / kRangeThreads;
     const int t0 = min(T, (int)threadIdx.x * per), t1 = min(T, t0 + per);
@@ -357,7 +359,6 @@ __global__ void __launch_bounds__(kRangeThreads)
     for (int t = t0; t < t1; ++t) {
         const uint32_t c = over ? 0u : tile_tally[t];
         tile_start[t] = (uint32_t)o;
-        cursor[t] = (uint32_t)o;
         o += c;
         ni += c == 0 ? 1u : (c + chunk - 1) / chunk;
     }
@@ -388,12 +389,11 @@ __global__ void __launch_bounds__(kRangeThreads)
     }
 }
 
-// Pass 2 of the placed lists: each ray takes one slot in the range of each tile it reaches, at
-// most as many tiles as it tallied (the same enumeration as the tally's, on the same values), and
-// never a slot past the list. A block first counts
-// its rays' entries per tile in shared memory, reserves them with one atomic per tile on the
-// tile's cursor, then hands the reserved slots out in shared memory. The segment's far end is
-// formed from the staged ray constants as prep_ray forms it.
+// Pass 2 of the placed lists, on the grid of the tally (the same rays in each block): each ray
+// takes one slot in the range of each tile it reaches, at most as many tiles as it tallied (the
+// same enumeration as the tally's, on the same values), from the block's own share of the range,
+// and never a slot past the list. The segment's far end is formed from the staged ray constants
+// as prep_ray forms it.
 template <typename F>
 __device__ __forceinline__ void for_each_placed_tile(const Batch& bt, const float4* __restrict__ ra,
                                                      const uint32_t* __restrict__ counts, F f) {
@@ -417,25 +417,24 @@ __device__ __forceinline__ void for_each_placed_tile(const Batch& bt, const floa
 }
 
 __global__ void k_ray_place(Batch bt, const float4* __restrict__ ra, const uint32_t* __restrict__ counts,
-                            uint32_t* __restrict__ cursor, const uint32_t* __restrict__ total,
-                            uint32_t* __restrict__ evals) {
-    extern __shared__ uint32_t s_slot[];  // [T]: the block's entries per tile, then its next slot
+                            const uint32_t* __restrict__ tile_start, const uint32_t* __restrict__ block_base,
+                            const uint32_t* __restrict__ total, uint32_t* __restrict__ evals) {
+    extern __shared__ uint32_t s_slot[];  // [T]: the block's next slot in each tile's range
     const uint32_t n = total[2];
     if (n == 0u) return;  // overflow, or no entries (the same for every thread)
-    for (int t = threadIdx.x; t < bt.T; t += blockDim.x) s_slot[t] = 0u;
-    __syncthreads();
-    for_each_placed_tile(bt, ra, counts, [&](int, uint32_t gt) { atomicAdd(&s_slot[gt], 1u); });
-    __syncthreads();
-    for (int t = threadIdx.x; t < bt.T; t += blockDim.x) {
-        const uint32_t v = s_slot[t];
-        if (v) s_slot[t] = atomicAdd(&cursor[t], v);
-    }
+    const uint32_t* row = block_base + (size_t)blockIdx.x * bt.T;
+    // rows of tiles this block does not reach hold stale values that are never used
+    for (int t = threadIdx.x; t < bt.T; t += blockDim.x) s_slot[t] = tile_start[t] + row[t];
     __syncthreads();
     for_each_placed_tile(bt, ra, counts, [&](int i, uint32_t gt) {
         const uint32_t pos = atomicAdd(&s_slot[gt], 1u);
         if (pos < n) evals[pos] = (uint32_t)i;
     });
 }
+
+// Blocks of the two placed-list passes (the same grid for both): at most kBinBlocksMax rows of
+// block_base.
+int bin_blocks(long n) { return (int)std::max(1L, std::min((n + kBlock - 1) / kBlock, (long)kBinBlocksMax)); }
 
 // Largest |c| of a cell centre seen from a sensor inside or near the grid [m].
 static float max_extent(const DevParams& p) { return 2.0f * ((float)p.G * p.res * 1.7320508f + p.size_z); }
@@ -508,22 +507,23 @@ cudaError_t build_ray_lists(const Batch& bt, const float* xs, const float* ys, c
     const int T = bt.T;
     if (placed_lists(ds, T)) {  // K3DOM: tally, ranges, place
         const size_t hist = sizeof(uint32_t) * (size_t)T;
+        const int blocks = bin_blocks(N);
         ++g_launches;
-        k_ray_count<true><<<grid_for(N), kBlock, hist, st>>>(bt, xs, ys, zs, 0, rb.ray_a, rb.ray_c, rb.counts,
-                                                              rb.tile_tally, status);
+        k_ray_count<true><<<blocks, kBlock, hist, st>>>(bt, xs, ys, zs, 0, rb.ray_a, rb.ray_c, rb.counts,
+                                                         rb.tile_tally, rb.block_base, status);
         ++g_launches;
         k_tile_ranges<<<1, kRangeThreads, 0, st>>>(rb.tile_tally, T, rb.chunk, rb.capacity, rb.tile_start,
-                                                   rb.tile_cursor, rb.item_off, rb.total, status);
+                                                   rb.item_off, rb.total, status);
         ++g_launches;
-        k_ray_place<<<grid_for(N), kBlock, hist, st>>>(bt, rb.ray_a, rb.counts, rb.tile_cursor, rb.total,
-                                                        rb.evals2);
+        k_ray_place<<<blocks, kBlock, hist, st>>>(bt, rb.ray_a, rb.counts, rb.tile_start, rb.block_base, rb.total,
+                                                   rb.evals2);
         return cudaGetLastError();
     }
     // DS (and batches with more tiles than a block histogram holds): entries in ray order, then a
     // stable sort by tile
     ++g_launches;
     k_ray_count<false><<<grid_for(N), kBlock, 0, st>>>(bt, xs, ys, zs, ds ? 1 : 0, rb.ray_a, rb.ray_c, rb.counts,
-                                                        nullptr, status);
+                                                        nullptr, nullptr, status);
     cudaError_t e = scan_u32_exclusive(rb.counts, rb.offsets, N, rb.scan_tmp, rb.total, st);
     if (e != cudaSuccess) return e;
     ++g_launches;

@@ -137,7 +137,8 @@ struct RayBuffers {
     uint32_t* ekeys2;      // sorted (DS)
     uint32_t* evals2;      // the lists: point slots grouped by tile (K3DOM: placed, DS: sorted)
     uint32_t* tile_tally;  // T: rays per tile (K3DOM), zero between frames
-    uint32_t* tile_cursor; // T: next free slot of each tile's range (K3DOM)
+    uint32_t* block_base;  // [bin_blocks(N)][T]: each binning block's first slot in each tile's range,
+                           // relative to the range's start (K3DOM)
     uint32_t* ekeys_alt;
     uint32_t* evals_alt;
     uint32_t* tile_start;  // T+1
@@ -160,6 +161,8 @@ long ray_entries_bound(const DevParams& p, const TileShape& ts, int max_points, 
 // (48 KB at most); DS lists, and batches with more tiles, are sorted by tile.
 constexpr int kPlacedMaxTiles = 12288;
 inline bool placed_lists(bool ds, int T) { return !ds && T <= kPlacedMaxTiles; }
+constexpr int kBinBlocksMax = 1024;
+int bin_blocks(long n);  // blocks of the placed-list passes
 // Texture object over the S kernel tables (point sampling, FP32 as stored), for k_bgki.
 cudaError_t make_kernel_table_texture(RayBuffers& rb, int S);
 // Per-scene evidence constants (binning radius, cull radius, fixed-point scale); writes the
