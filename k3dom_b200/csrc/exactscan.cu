@@ -18,6 +18,7 @@
 #include "scan.cuh"
 
 #include <algorithm>
+#include <cstdint>
 #include <vector>
 
 namespace k3dom {
@@ -140,7 +141,9 @@ __device__ __forceinline__ u128 group_prefix(const u128* __restrict__ gsum, int 
     return r;
 }
 
-__global__ void exact_tab_apply(const ExactTile* __restrict__ tiles, int nt, const u128* __restrict__ tsum,
+// 4 CTAs per SM (64 registers): the pass waits on its loads with few warps otherwise
+__global__ void __launch_bounds__(kExThreads, 4) exact_tab_apply(const ExactTile* __restrict__ tiles, int nt,
+                                                                const u128* __restrict__ tsum,
                                 const u128* __restrict__ gsum) {
     __shared__ u128 sm[kExThreads / 32 + 1];
     const int b = blockIdx.x;
@@ -149,21 +152,40 @@ __global__ void exact_tab_apply(const ExactTile* __restrict__ tiles, int nt, con
     const int f = t.seg_first;
     const u128 pre_f = group_prefix(gsum, f / kExGroup) + tsum[f];
     const int base = threadIdx.x * kExItems;
-    u128 v[kExItems];
+    // the inputs stay in registers as floats and are converted twice (cheaper than holding
+    // eight 128-bit values across the block scan)
+    // a full tile with 16-byte aligned ranges moves its 8 values per thread as two float4
+    const bool vec = t.n == kExTile &&
+                     ((reinterpret_cast<uintptr_t>(t.in) | reinterpret_cast<uintptr_t>(t.out)) & 15u) == 0;
+    float x[kExItems];
+    if (vec) {
+        const float4* p = reinterpret_cast<const float4*>(t.in + base);
+        const float4 a = p[0], c = p[1];
+        x[0] = a.x; x[1] = a.y; x[2] = a.z; x[3] = a.w;
+        x[4] = c.x; x[5] = c.y; x[6] = c.z; x[7] = c.w;
+    } else {
+#pragma unroll
+        for (int j = 0; j < kExItems; ++j) x[j] = (base + j < t.n) ? t.in[base + j] : 0.0f;
+    }
     u128 s = 0;
 #pragma unroll
-    for (int j = 0; j < kExItems; ++j) {
-        const int i = base + j;
-        v[j] = (i < t.n) ? to_fixed(t.in[i]) : (u128)0;
-        s += v[j];
-    }
+    for (int j = 0; j < kExItems; ++j) s += to_fixed(x[j]);
     u128 tot;
     u128 run = (pre_b - pre_f) + block_exclusive_scan<u128, kExThreads>(s, sm, &tot);
+    float y[kExItems];
 #pragma unroll
     for (int j = 0; j < kExItems; ++j) {
-        const int i = base + j;
-        run += v[j];
-        if (i < t.n) t.out[i] = from_fixed(run);
+        run += to_fixed(x[j]);
+        y[j] = from_fixed(run);
+    }
+    if (vec) {
+        float4* q = reinterpret_cast<float4*>(t.out + base);
+        q[0] = make_float4(y[0], y[1], y[2], y[3]);
+        q[1] = make_float4(y[4], y[5], y[6], y[7]);
+    } else {
+#pragma unroll
+        for (int j = 0; j < kExItems; ++j)
+            if (base + j < t.n) t.out[base + j] = y[j];
     }
 }
 
