@@ -101,7 +101,7 @@ struct k3dom_handle {
 
     cudaStream_t st = nullptr, st2 = nullptr, st3 = nullptr;  // frame; resampling draws; ray lists
     cudaStream_t st4 = nullptr;                               // registered output export
-    cudaEvent_t ev_fork = nullptr, ev_join = nullptr, ev_bin = nullptr;
+    cudaEvent_t ev_fork = nullptr, ev_join = nullptr, ev_bin = nullptr, ev_cells = nullptr;
     cudaEvent_t ev_out = nullptr, ev_out_done = nullptr;
     // registered output (k3dom_set_output): one cell field of one scene, written every frame
     int out_field = -1, out_scene = 0;
@@ -238,6 +238,7 @@ struct k3dom_handle {
         if (ev_fork) cudaEventDestroy(ev_fork);
         if (ev_join) cudaEventDestroy(ev_join);
         if (ev_bin) cudaEventDestroy(ev_bin);
+        if (ev_cells) cudaEventDestroy(ev_cells);
         if (ev_staged) cudaEventDestroy(ev_staged);
         if (ev_out) cudaEventDestroy(ev_out);
         if (ev_out_done) cudaEventDestroy(ev_out_done);
@@ -720,8 +721,8 @@ cudaError_t enq_occupancy(k3dom_handle* h, bool first_frame) {
     return enq_evidence(h, first_frame);
 }
 
-cudaError_t enq_persistent(k3dom_handle* h) {
-    launch_reweight(h->batch(), h->Ss, h->sorted_keys, h->cw, h->st);
+cudaError_t enq_persistent(k3dom_handle* h, cudaStream_t s) {
+    launch_reweight(h->batch(), h->Ss, h->sorted_keys, h->cw, s);
     return cudaGetLastError();
 }
 
@@ -830,7 +831,15 @@ cudaError_t enq_frame(k3dom_handle* h) {
     }
     rec(h, 3);
     if (!output_needs_births(h->out_field) && (e = enq_output(h))) return e;
-    if ((e = enq_persistent(h))) return e;
+    if (overlap) {
+        // the reweight needs the cells' factors only, the births the born masses: the reweight
+        // runs on the draws' stream beside the births, and resampling waits for both
+        if ((e = cudaEventRecord(h->ev_cells, h->st)) || (e = cudaStreamWaitEvent(h->st2, h->ev_cells, 0)) ||
+            (e = enq_persistent(h, h->st2)) || (e = cudaEventRecord(h->ev_join, h->st2)))
+            return e;
+    } else if ((e = enq_persistent(h, h->st))) {
+        return e;
+    }
     rec(h, 4);
     if ((e = enq_births(h))) return e;
     rec(h, 5);
@@ -991,6 +1000,7 @@ k3dom_status k3dom_batch_create(const k3dom_params* params, int32_t n_scenes, k3
     if ((e = cudaMallocHost((void**)&h->status_host, sizeof(DevStatus)))) return bail(e);
     std::memset(h->status_host, 0, sizeof(DevStatus));
     if ((e = cudaEventCreateWithFlags(&h->ev_bin, cudaEventDisableTiming))) return bail(e);
+    if ((e = cudaEventCreateWithFlags(&h->ev_cells, cudaEventDisableTiming))) return bail(e);
     if ((e = cudaEventCreateWithFlags(&h->ev_fork, cudaEventDisableTiming))) return bail(e);
     if ((e = cudaEventCreateWithFlags(&h->ev_join, cudaEventDisableTiming))) return bail(e);
     if ((e = cudaEventCreateWithFlags(&h->ev_staged, cudaEventDisableTiming))) return bail(e);
@@ -1446,7 +1456,7 @@ k3dom_status k3dom_grid_cell_occupancy_update(k3dom_handle* h, float dt, const f
 
 k3dom_status k3dom_update_persistent_particles(k3dom_handle* h) {
     STAGE_BEGIN
-    if ((e = enq_persistent(h))) return h->fail(e);
+    if ((e = enq_persistent(h, h->st))) return h->fail(e);
     return finish_sync(h);
 }
 

@@ -748,12 +748,32 @@ __device__ __forceinline__ float calc_norm(float weight_sum, float rho_p) {
 // updates of the persistent-particle and moment stages. Masses are stored in FP32; the update
 // is evaluated in FP64 (it has several cancelling differences) and rounded once.
 // g = gamma^dt of the frame.
+// A cell's inputs to the update, loaded together so that their reads overlap (the particle sums
+// are read whether or not the cell holds particles; they are used only when it does).
+struct CellIn {
+    float m_f, m_s, m_d, sum_w, wvx, wvy, wvz;
+    int start;
+};
+__device__ __forceinline__ CellIn load_cell_in(const CellState& cs, const CellWork& cw, int c, bool first_frame) {
+    CellIn in;
+    in.m_f = cs.free_m[c];
+    in.m_s = cs.static_m[c];
+    in.m_d = cs.dyn_m[c];
+    in.start = first_frame ? -1 : cw.start[c];
+    in.sum_w = cw.sum_w[c];
+    in.wvx = cw.sum_wvx[c];
+    in.wvy = cw.sum_wvy[c];
+    in.wvz = cw.sum_wvz[c];
+    return in;
+}
+
 __device__ void k3dom_cell_update(const DevParams& p, double g, int c, double del_occ, double del_free,
                                   CellState cs, CellWork cw, bool first_frame) {
-    double m_f = cs.free_m[c], m_s = cs.static_m[c], m_d = cs.dyn_m[c];
-    const int start = first_frame ? -1 : cw.start[c];
+    const CellIn in = load_cell_in(cs, cw, c, first_frame);
+    double m_f = in.m_f, m_s = in.m_s, m_d = in.m_d;
+    const int start = in.start;
     const bool has = start >= 0;
-    const double dyn_pred = has ? (double)cw.sum_w[c] : 0.0;
+    const double dyn_pred = has ? (double)in.sum_w : 0.0;
     const double k2 = 2.0 / (double)p.mass_scale;
     const double pred_total = (m_f + m_d) * g;
     // predict_mass (:79-84)
@@ -810,9 +830,9 @@ __device__ void k3dom_cell_update(const DevParams& p, double g, int c, double de
     double vx = 0.0, vy = 0.0, vz = 0.0;
     if (has && pers > 0.0) {
         const double q = mu_UA / pers;
-        vx = q * (double)cw.sum_wvx[c];
-        vy = q * (double)cw.sum_wvy[c];
-        vz = q * (double)cw.sum_wvz[c];
+        vx = q * (double)in.wvx;
+        vy = q * (double)in.wvy;
+        vz = q * (double)in.wvz;
     }
     cs.mvx[c] = (float)vx;
     cs.mvy[c] = (float)vy;
@@ -1922,7 +1942,8 @@ cudaError_t launch_k3dom_update_cells(const Batch& bt, RayBuffers& rb, CellState
                                       cudaStream_t st) {
     const EvArgs A = make_args(bt, rb, cs, cw, false, status);
     ++g_launches;
-    k_k3dom_update_cells<<<grid_for(bt.C), kBlock, 0, st>>>(A);
+    // one thread per cell: the update is latency bound, so every cell's reads are in flight at once
+    k_k3dom_update_cells<<<div_up(bt.C, kBlock), kBlock, 0, st>>>(A);
     return cudaGetLastError();
 }
 
