@@ -746,8 +746,8 @@ cudaError_t enq_resample(k3dom_handle* h, bool draws_ready) {
     if (!draws_ready) {
         if ((e = enq_draws(h, h->st))) return e;
     }
-    launch_joint_prepare(h->batch(), h->Ss, h->Bp, h->st);
-    if ((e = exact_scan_plan(h->plan_joint, h->plan_joint_n, h->exact_scratch, h->st))) return e;
+    // the joint weights' prefix; the penalised (sign-bit) weights count as 0 and are cleared
+    if ((e = exact_scan_plan(h->plan_joint, h->plan_joint_n, h->exact_scratch, h->st, true))) return e;
     launch_resample(h->batch(), h->joint_cum, h->draw_sorted, h->Ss, h->Bp, h->A, h->ancestors, h->joint_max,
                     h->res_br, h->st);
     h->a_current = true;
@@ -1036,10 +1036,10 @@ k3dom_status k3dom_batch_create(const k3dom_params* params, int32_t n_scenes, k3
         std::vector<ExactTile> pb, pj;
         for (int s = 0; s < n_scenes; ++s) {
             const SceneHost& x = h->sc[s];
-            const float* in1[1] = {h->cs[0].born_m + h->off.cell[s]};
+            float* in1[1] = {h->cs[0].born_m + h->off.cell[s]};
             const long n1[1] = {x.dp.C};
             exact_plan_add(pb, in1, n1, 1, h->born_cum + h->off.cell[s]);
-            const float* in2[2] = {h->Ss.w + h->off.part[s], h->Bp.w + h->off.birth[s]};
+            float* in2[2] = {h->Ss.w + h->off.part[s], h->Bp.w + h->off.birth[s]};
             const long n2[2] = {x.dp.P, x.dp.B};
             exact_plan_add(pj, in2, n2, 2, h->joint_cum + h->off.joint[s]);
         }

@@ -141,7 +141,9 @@ __device__ __forceinline__ u128 group_prefix(const u128* __restrict__ gsum, int 
     return r;
 }
 
-// 4 CTAs per SM (64 registers): the pass waits on its loads with few warps otherwise
+// 4 CTAs per SM (64 registers): the pass waits on its loads with few warps otherwise. CLEAR: the
+// tile's sign-bit inputs (which the scan counts as 0) are set to +0 in place.
+template <bool CLEAR>
 __global__ void __launch_bounds__(kExThreads, 4) exact_tab_apply(const ExactTile* __restrict__ tiles, int nt,
                                                                 const u128* __restrict__ tsum,
                                 const u128* __restrict__ gsum) {
@@ -167,6 +169,11 @@ __global__ void __launch_bounds__(kExThreads, 4) exact_tab_apply(const ExactTile
 #pragma unroll
         for (int j = 0; j < kExItems; ++j) x[j] = (base + j < t.n) ? t.in[base + j] : 0.0f;
     }
+    if (CLEAR) {
+#pragma unroll
+        for (int j = 0; j < kExItems; ++j)
+            if (signbit(x[j]) && base + j < t.n) t.in[base + j] = 0.0f;
+    }
     u128 s = 0;
 #pragma unroll
     for (int j = 0; j < kExItems; ++j) s += to_fixed(x[j]);
@@ -191,7 +198,7 @@ __global__ void __launch_bounds__(kExThreads, 4) exact_tab_apply(const ExactTile
 
 int exact_plan_tiles(long n) { return div_up(n, kExTile); }
 
-void exact_plan_add(std::vector<ExactTile>& plan, const float* const* in, const long* n, int pieces, float* out) {
+void exact_plan_add(std::vector<ExactTile>& plan, float* const* in, const long* n, int pieces, float* out) {
     const int first = (int)plan.size();
     long o = 0;
     for (int k = 0; k < pieces; ++k) {
@@ -211,7 +218,7 @@ size_t exact_plan_scratch_bytes(int ntiles) {
     return ((size_t)ntiles + (size_t)div_up(ntiles, kExGroup) + 2) * sizeof(u128);
 }
 
-cudaError_t exact_scan_plan(const ExactTile* tiles, int nt, void* scratch, cudaStream_t st) {
+cudaError_t exact_scan_plan(const ExactTile* tiles, int nt, void* scratch, cudaStream_t st, bool clear_signed) {
     if (nt <= 0) return cudaSuccess;
     u128* tsum = reinterpret_cast<u128*>(scratch);
     u128* gsum = tsum + nt;
@@ -221,7 +228,10 @@ cudaError_t exact_scan_plan(const ExactTile* tiles, int nt, void* scratch, cudaS
     ++g_launches;
     exact_tab_groups<<<ng, kExThreads, 0, st>>>(tsum, nt, gsum);
     ++g_launches;
-    exact_tab_apply<<<nt, kExThreads, 0, st>>>(tiles, nt, tsum, gsum);
+    if (clear_signed)
+        exact_tab_apply<true><<<nt, kExThreads, 0, st>>>(tiles, nt, tsum, gsum);
+    else
+        exact_tab_apply<false><<<nt, kExThreads, 0, st>>>(tiles, nt, tsum, gsum);
     return cudaGetLastError();
 }
 

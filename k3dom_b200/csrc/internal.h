@@ -68,15 +68,17 @@ cudaError_t exact_scan_float2(const float* a, long na, const float* b, long nb, 
 // Segmented exact scan driven by a plan of tiles (each <= 2048 elements, one contiguous input
 // and output range, and the index of its segment's first tile).
 struct ExactTile {
-    const float* in;
+    float* in;  // writable: a scan may clear its sign-bit inputs in place
     float* out;
     int n;
     int seg_first;
 };
 // Appends one segment made of `pieces` input ranges, written contiguously from `out`.
-void exact_plan_add(std::vector<ExactTile>& plan, const float* const* in, const long* n, int pieces, float* out);
+void exact_plan_add(std::vector<ExactTile>& plan, float* const* in, const long* n, int pieces, float* out);
 size_t exact_plan_scratch_bytes(int ntiles);
-cudaError_t exact_scan_plan(const ExactTile* tiles, int nt, void* scratch, cudaStream_t st);
+// clear_signed: every input with its sign bit set (counted as 0 by the scan) is also set to +0 in
+// place, the penalty step of resampling.cu:13-36 folded into the joint weights' scan.
+cudaError_t exact_scan_plan(const ExactTile* tiles, int nt, void* scratch, cudaStream_t st, bool clear_signed = false);
 
 // particles.cu
 // Prediction reads the structure-of-arrays set a and writes each particle as a 32-byte record
@@ -100,7 +102,6 @@ void launch_gather_segsum(const Batch& bt, const float4* x, Particles s, const u
 void launch_reweight(const Batch& bt, Particles s, const uint32_t* sorted_keys, CellWork cw, cudaStream_t st);
 void launch_births(const Batch& bt, const float* born, const float* born_cum, Particles b, cudaStream_t st);
 void launch_init_particles(const Batch& bt, const float* born_cum, Particles a, cudaStream_t st);
-void launch_joint_prepare(const Batch& bt, Particles s, Particles b, cudaStream_t st);
 int draw_key_bits(int S);
 void launch_draw_keys(const Batch& bt, uint32_t* keys, cudaStream_t st);
 long res_bracket_count(long P);

@@ -521,26 +521,6 @@ void launch_init_particles(const Batch& bt, const float* born_cum, Particles a, 
 }
 
 // ---------------------------------------------------------------- resampling
-// Penalty (resampling.cu:13-36): weights flagged slow become 0, in place, as the reference
-// leaves them; the flags are cleared.
-__global__ void k_joint_prepare(int P, int B, Particles s, Particles b) {
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < P + B; i += gridDim.x * blockDim.x) {
-        if (i < P) {
-            const float w = s.w[i];
-            s.w[i] = signbit(w) ? 0.0f : w;
-        } else {
-            const float w = b.w[i - P];
-            b.w[i - P] = signbit(w) ? 0.0f : w;
-        }
-    }
-}
-
-void launch_joint_prepare(const Batch& bt, Particles s, Particles b, cudaStream_t st) {
-    if (bt.P + bt.B <= 0) return;
-    ++g_launches;
-    k_joint_prepare<<<grid_for((long)bt.P + bt.B), kBlock, 0, st>>>(bt.P, bt.B, s, b);
-}
-
 // Resampling draws as 24-bit keys of 1 - u: sorting the keys ascending orders the draws
 // u * joint_max ascending for any joint_max >= 0, so the draws can be sorted before the
 // weights exist (resamplingGenerateRandomNumbersKernel + thrust::sort, resampling.cu:38-53,
