@@ -523,12 +523,15 @@ cudaError_t alloc_ray_lane(k3dom_calib* c, RayBuffers& rb, int max_points, long 
     rb.chunk = kCalibChunk;
     std::vector<void*>* L = &c->ray_allocs;
     cudaError_t e;
-    if ((e = c->alloc(&rb.ray_a, N, L)) || (e = c->alloc(&rb.ray_c, N, L)) || (e = c->alloc(&rb.counts, N, L)) ||
+    if ((e = c->alloc(&rb.ray_a, N, L)) || (e = c->alloc(&rb.ray_c, N, L)) ||
+        (e = c->alloc(&rb.counts, (size_t)kRayThreads * N, L)) ||
         (e = c->alloc(&rb.evals2, cap, L)) || (e = c->alloc(&rb.tile_start, T + 1, L)) ||
         (e = c->alloc(&rb.item_off, T + 1, L)) || (e = c->alloc(&rb.tile_done, T, L)) || (e = c->alloc(&rb.total, 4, L)))
         return e;
     if (placed_lists(false, T))  // lists placed per tile through tallies and per-block offsets
-        return (e = c->alloc(&rb.tile_tally, T, L)) ? e : c->alloc(&rb.block_base, (size_t)bin_blocks(N) * T, L);
+        return (e = c->alloc(&rb.tile_tally, T, L))
+                   ? e
+                   : c->alloc(&rb.block_base, (size_t)bin_blocks((long)kRayThreads * N) * T, L);
     // lists sorted by tile
     if ((e = c->alloc(&rb.offsets, N, L)) || (e = c->alloc(&rb.ekeys, cap, L)) || (e = c->alloc(&rb.evals, cap, L)) ||
         (e = c->alloc(&rb.ekeys2, cap, L)) || (e = c->alloc(&rb.tile_items, T, L)))

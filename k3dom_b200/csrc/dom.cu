@@ -397,14 +397,14 @@ cudaError_t alloc_ray_buffers(k3dom_handle* h) {
     rb.chunk = h->chunk;
     const int N = h->N, T = h->T;
     if ((e = h->alloc(&rb.ray_a, N, true, L)) || (e = h->alloc(&rb.ray_c, N, true, L)) ||
-        (e = h->alloc(&rb.counts, N, true, L)) || (e = h->alloc(&rb.evals2, cap, false, L)) ||
+        (e = h->alloc(&rb.counts, (size_t)kRayThreads * N, true, L)) || (e = h->alloc(&rb.evals2, cap, false, L)) ||
         (e = h->alloc(&rb.tile_start, T + 1, true, L)) || (e = h->alloc(&rb.item_off, T + 1, true, L)) ||
         (e = h->alloc(&rb.tile_done, T, true, L)) || (e = h->alloc(&rb.acc, 2 * (size_t)h->C, true, L)) ||
         (e = h->alloc(&rb.total, 4, true, L)))
         return e;
     if (placed_lists(h->ds(), T)) {  // per-tile tallies and per-block offsets
         if ((e = h->alloc(&rb.tile_tally, T, true, L)) ||
-            (e = h->alloc(&rb.block_base, (size_t)bin_blocks(N) * T, true, L)))
+            (e = h->alloc(&rb.block_base, (size_t)bin_blocks((long)kRayThreads * N) * T, true, L)))
             return e;
         return alloc_points(h);
     }

@@ -57,15 +57,16 @@ struct BinGeom {
     int G, Gz, tx, ty, tz, ntx, nty, ntz;
 };
 
-__device__ __forceinline__ bool seg_box(const float a[3], const float d[3], const float l[3], const float h[3],
-                                        float t0, float t1) {
+// Whether the segment a + t d, t in [t0, t1], meets the box [l, h]; inv[k] = 1 / d[k] (unused
+// where d[k] = 0).
+__device__ __forceinline__ bool seg_box(const float a[3], const float d[3], const float inv[3], const float l[3],
+                                        const float h[3], float t0, float t1) {
 #pragma unroll
     for (int k = 0; k < 3; ++k) {
         if (d[k] == 0.0f) {
             if (a[k] < l[k] || a[k] > h[k]) return false;
         } else {
-            const float inv = 1.0f / d[k];
-            const float e0 = (l[k] - a[k]) * inv, e1 = (h[k] - a[k]) * inv;
+            const float e0 = (l[k] - a[k]) * inv[k], e1 = (h[k] - a[k]) * inv[k];
             t0 = fmaxf(t0, fminf(e0, e1));
             t1 = fminf(t1, fmaxf(e0, e1));
         }
@@ -73,11 +74,22 @@ __device__ __forceinline__ bool seg_box(const float a[3], const float d[3], cons
     return t0 <= t1;
 }
 
-// Visit every tile whose cell-centre box, grown by R, meets the segment a -> b.
+// v[k] for k in {0, 1, 2} by selects (a run-time index into a local array would go through
+// local memory).
+template <typename T>
+__device__ __forceinline__ T sel3(T v0, T v1, T v2, int k) { return k == 0 ? v0 : (k == 1 ? v1 : v2); }
+
+// Visit every tile whose cell-centre box, grown by R, meets the segment a -> b; only the slabs
+// (layers of tiles across the ray's dominant axis) first, first + step, ... of them, so that
+// `step` threads can share one ray. The reciprocals 1 / d are formed once per ray.
 template <typename F>
-__device__ __forceinline__ void for_each_tile(const BinGeom& g, float bx, float by, float bz, F f) {
+__device__ __forceinline__ void for_each_tile(const BinGeom& g, float bx, float by, float bz, F f, int first = 0,
+                                              int step = 1) {
     const float a[3] = {g.ax, g.ay, g.az};
     const float d[3] = {bx - g.ax, by - g.ay, bz - g.az};
+    float inv[3];
+#pragma unroll
+    for (int k = 0; k < 3; ++k) inv[k] = d[k] != 0.0f ? 1.0f / d[k] : 0.0f;
     const float glo[3] = {-g.R, -g.R, -g.R};
     const float ghi[3] = {(float)(g.G - 1) + g.R, (float)(g.G - 1) + g.R, (float)(g.Gz - 1) + g.R};
     float t0 = 0.0f, t1 = 1.0f;
@@ -86,54 +98,59 @@ __device__ __forceinline__ void for_each_tile(const BinGeom& g, float bx, float 
         if (d[k] == 0.0f) {
             if (a[k] < glo[k] || a[k] > ghi[k]) return;
         } else {
-            const float inv = 1.0f / d[k];
-            const float e0 = (glo[k] - a[k]) * inv, e1 = (ghi[k] - a[k]) * inv;
+            const float e0 = (glo[k] - a[k]) * inv[k], e1 = (ghi[k] - a[k]) * inv[k];
             t0 = fmaxf(t0, fminf(e0, e1));
             t1 = fminf(t1, fmaxf(e0, e1));
         }
     }
     if (t0 > t1) return;
     int A = 0;
-    if (fabsf(d[1]) > fabsf(d[A])) A = 1;
-    if (fabsf(d[2]) > fabsf(d[A])) A = 2;
+    float dmax = fabsf(d[0]);
+    if (fabsf(d[1]) > dmax) {
+        A = 1;
+        dmax = fabsf(d[1]);
+    }
+    if (fabsf(d[2]) > dmax) A = 2;
     const int Bx = (A + 1) % 3, Cx = (A + 2) % 3;
-    const int ts[3] = {g.tx, g.ty, g.tz}, nt[3] = {g.ntx, g.nty, g.ntz};
-    const float pa0 = a[A] + d[A] * t0, pa1 = a[A] + d[A] * t1;
-    int ta0 = (int)floorf((fminf(pa0, pa1) - g.R) / (float)ts[A]);
-    int ta1 = (int)floorf((fmaxf(pa0, pa1) + g.R) / (float)ts[A]);
+    // the dominant axis A and the two others, B and C
+    const float aA = sel3(a[0], a[1], a[2], A), dA = sel3(d[0], d[1], d[2], A), invA = sel3(inv[0], inv[1], inv[2], A);
+    const float aB = sel3(a[0], a[1], a[2], Bx), dB = sel3(d[0], d[1], d[2], Bx);
+    const float aC = sel3(a[0], a[1], a[2], Cx), dC = sel3(d[0], d[1], d[2], Cx);
+    const int tsA = sel3(g.tx, g.ty, g.tz, A), tsB = sel3(g.tx, g.ty, g.tz, Bx), tsC = sel3(g.tx, g.ty, g.tz, Cx);
+    const int ntA = sel3(g.ntx, g.nty, g.ntz, A), ntB = sel3(g.ntx, g.nty, g.ntz, Bx);
+    const int ntC = sel3(g.ntx, g.nty, g.ntz, Cx);
+    const float pa0 = aA + dA * t0, pa1 = aA + dA * t1;
+    int ta0 = (int)floorf((fminf(pa0, pa1) - g.R) / (float)tsA);
+    int ta1 = (int)floorf((fmaxf(pa0, pa1) + g.R) / (float)tsA);
     ta0 = max(ta0, 0);
-    ta1 = min(ta1, nt[A] - 1);
-    for (int ta = ta0; ta <= ta1; ++ta) {
-        const float slo = (float)(ta * ts[A]) - g.R, shi = (float)(ta * ts[A] + ts[A] - 1) + g.R;
+    ta1 = min(ta1, ntA - 1);
+    for (int ta = ta0 + first; ta <= ta1; ta += step) {
+        const float slo = (float)(ta * tsA) - g.R, shi = (float)(ta * tsA + tsA - 1) + g.R;
         float s0 = t0, s1 = t1;
-        if (d[A] != 0.0f) {
-            const float inv = 1.0f / d[A];
-            const float e0 = (slo - a[A]) * inv, e1 = (shi - a[A]) * inv;
+        if (dA != 0.0f) {
+            const float e0 = (slo - aA) * invA, e1 = (shi - aA) * invA;
             s0 = fmaxf(s0, fminf(e0, e1));
             s1 = fminf(s1, fmaxf(e0, e1));
-        } else if (a[A] < slo || a[A] > shi) {
+        } else if (aA < slo || aA > shi) {
             continue;
         }
         if (s0 > s1) continue;
-        const float b0 = a[Bx] + d[Bx] * s0, b1 = a[Bx] + d[Bx] * s1;
-        const float c0 = a[Cx] + d[Cx] * s0, c1 = a[Cx] + d[Cx] * s1;
-        int tb0 = max((int)floorf((fminf(b0, b1) - g.R) / (float)ts[Bx]), 0);
-        int tb1 = min((int)floorf((fmaxf(b0, b1) + g.R) / (float)ts[Bx]), nt[Bx] - 1);
-        int tc0 = max((int)floorf((fminf(c0, c1) - g.R) / (float)ts[Cx]), 0);
-        int tc1 = min((int)floorf((fmaxf(c0, c1) + g.R) / (float)ts[Cx]), nt[Cx] - 1);
+        const float b0 = aB + dB * s0, b1 = aB + dB * s1;
+        const float c0 = aC + dC * s0, c1 = aC + dC * s1;
+        int tb0 = max((int)floorf((fminf(b0, b1) - g.R) / (float)tsB), 0);
+        int tb1 = min((int)floorf((fmaxf(b0, b1) + g.R) / (float)tsB), ntB - 1);
+        int tc0 = max((int)floorf((fminf(c0, c1) - g.R) / (float)tsC), 0);
+        int tc1 = min((int)floorf((fmaxf(c0, c1) + g.R) / (float)tsC), ntC - 1);
         for (int tb = tb0; tb <= tb1; ++tb) {
             for (int tc = tc0; tc <= tc1; ++tc) {
-                int t3[3];
-                t3[A] = ta;
-                t3[Bx] = tb;
-                t3[Cx] = tc;
-                float l[3], h[3];
-#pragma unroll
-                for (int k = 0; k < 3; ++k) {
-                    l[k] = (float)(t3[k] * ts[k]) - g.R;
-                    h[k] = (float)(t3[k] * ts[k] + ts[k] - 1) + g.R;
-                }
-                if (seg_box(a, d, l, h, t0, t1)) f(t3[0] + g.ntx * (t3[1] + g.nty * t3[2]));
+                // the tile's (x, y, z) index: ta along A, tb along B, tc along C
+                const int tx = A == 0 ? ta : (Bx == 0 ? tb : tc);
+                const int ty = A == 1 ? ta : (Bx == 1 ? tb : tc);
+                const int tz = A == 2 ? ta : (Bx == 2 ? tb : tc);
+                const float l[3] = {(float)(tx * g.tx) - g.R, (float)(ty * g.ty) - g.R, (float)(tz * g.tz) - g.R};
+                const float h[3] = {(float)(tx * g.tx + g.tx - 1) + g.R, (float)(ty * g.ty + g.ty - 1) + g.R,
+                                    (float)(tz * g.tz + g.tz - 1) + g.R};
+                if (seg_box(a, d, inv, l, h, t0, t1)) f(tx + g.ntx * (ty + g.nty * tz));
             }
         }
     }
@@ -210,7 +227,9 @@ __device__ __forceinline__ BinGeom scene_geom(const SceneDev& sd, const FramePar
 // reached tile's ray count is also added to tile_tally, through a block histogram of the T tiles
 // in shared memory (the tiles around a sensor are reached by nearly every ray: one global atomic
 // per block and tile instead of one per ray); the value that atomic returns is the block's first
-// slot in the tile's range (relative to its start), kept in block_base for k_ray_place.
+// slot in the tile's range (relative to its start), kept in block_base for k_ray_place. TALLY
+// also gives each ray two threads (the ray's even and odd slabs of tiles, counts per thread):
+// the walk is latency bound, and 120,000 rays make only 25 warps per SM.
 template <bool TALLY>
 __global__ void k_ray_count(Batch bt, const float* __restrict__ xs, const float* __restrict__ ys,
                             const float* __restrict__ zs, int ds, float4* __restrict__ ra,
@@ -223,11 +242,14 @@ __global__ void k_ray_count(Batch bt, const float* __restrict__ xs, const float*
         for (int t = threadIdx.x; t < bt.T; t += blockDim.x) s_tally[t] = 0u;
         __syncthreads();
     }
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < bt.N; i += gridDim.x * blockDim.x) {
+    constexpr int kPer = TALLY ? kRayThreads : 1;  // threads per ray
+    const long nt = (long)bt.N * kPer;
+    for (long tid = (long)blockIdx.x * blockDim.x + threadIdx.x; tid < nt; tid += (long)gridDim.x * blockDim.x) {
+        const int i = (int)(tid / kPer), half = (int)(tid % kPer);
         const int sc = scene_of(bt.off->point, bt.S, i);
         const FrameParams f = bt.fp[sc];
         if (i - bt.off->point[sc] >= f.n_points) {
-            counts[i] = 0;
+            counts[tid] = 0;
             continue;
         }
         const SceneDev& sd = bt.sc[sc];
@@ -237,19 +259,24 @@ __global__ void k_ray_count(Batch bt, const float* __restrict__ xs, const float*
         float4 a;
         double4 cc;
         const RayPrep r = prep_ray(sd.p, g, mx, my, mz, ds != 0, &a, &cc);
-        ra[i] = a;
-        rc[i] = cc;
+        if (half == 0) {
+            ra[i] = a;
+            rc[i] = cc;
+        }
         uint32_t c = 0;
         if (r.ok) {
             const uint32_t toff = (uint32_t)bt.off->tile[sc];
-            for_each_tile(g, r.bx, r.by, r.bz, [&](int t) {
-                ++c;
-                if (TALLY) atomicAdd(&s_tally[toff + (uint32_t)t], 1u);
-            });
-        } else if (!(isfinite(mx) && isfinite(my) && isfinite(mz))) {
+            for_each_tile(
+                g, r.bx, r.by, r.bz,
+                [&](int t) {
+                    ++c;
+                    if (TALLY) atomicAdd(&s_tally[toff + (uint32_t)t], 1u);
+                },
+                half, kPer);
+        } else if (half == 0 && !(isfinite(mx) && isfinite(my) && isfinite(mz))) {
             atomicAdd(&status->nonfinite_points, 1ull);
         }
-        counts[i] = c;
+        counts[tid] = c;
     }
     if (TALLY) {
         __syncthreads();
@@ -397,8 +424,10 @@ __global__ void __launch_bounds__(kRangeThreads)
 template <typename F>
 __device__ __forceinline__ void for_each_placed_tile(const Batch& bt, const float4* __restrict__ ra,
                                                      const uint32_t* __restrict__ counts, F f) {
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < bt.N; i += gridDim.x * blockDim.x) {
-        const uint32_t cnt = counts[i];
+    const long nt = (long)bt.N * kRayThreads;
+    for (long tid = (long)blockIdx.x * blockDim.x + threadIdx.x; tid < nt; tid += (long)gridDim.x * blockDim.x) {
+        const int i = (int)(tid / kRayThreads), half = (int)(tid % kRayThreads);
+        const uint32_t cnt = counts[tid];
         if (cnt == 0u) continue;
         const int sc = scene_of(bt.off->point, bt.S, i);
         const SceneDev& sd = bt.sc[sc];
@@ -407,12 +436,15 @@ __device__ __forceinline__ void for_each_placed_tile(const Batch& bt, const floa
         const float bx = g.ax + a.x / sd.p.res, by = g.ay + a.y / sd.p.res, bz = g.az + a.z / sd.p.res;
         const uint32_t toff = (uint32_t)bt.off->tile[sc];
         uint32_t k = 0;
-        for_each_tile(g, bx, by, bz, [&](int t) {
-            if (k < cnt) {
-                f(i, toff + (uint32_t)t);
-                ++k;
-            }
-        });
+        for_each_tile(
+            g, bx, by, bz,
+            [&](int t) {
+                if (k < cnt) {
+                    f(i, toff + (uint32_t)t);
+                    ++k;
+                }
+            },
+            half, kRayThreads);
     }
 }
 
@@ -507,7 +539,7 @@ cudaError_t build_ray_lists(const Batch& bt, const float* xs, const float* ys, c
     const int T = bt.T;
     if (placed_lists(ds, T)) {  // K3DOM: tally, ranges, place
         const size_t hist = sizeof(uint32_t) * (size_t)T;
-        const int blocks = bin_blocks(N);
+        const int blocks = bin_blocks((long)N * kRayThreads);
         ++g_launches;
         k_ray_count<true><<<blocks, kBlock, hist, st>>>(bt, xs, ys, zs, 0, rb.ray_a, rb.ray_c, rb.counts,
                                                          rb.tile_tally, rb.block_base, status);

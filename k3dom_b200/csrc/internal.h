@@ -131,14 +131,14 @@ struct RayBuffers {
     double4* ray_c;        // d_m, margin, 1/d_m, 0 in FP64 (K3DOM)
     float4* ktab;          // per scene: sparse-kernel table with the fixed-point scale folded in
     cudaTextureObject_t ktex;  // ktab read through the texture path (k_bgki), 0 when not made
-    uint32_t* counts;      // per point slot: number of tiles touched
+    uint32_t* counts;      // [kRayThreads * N] tiles touched per point slot (DS) or per thread of a slot
     uint32_t* offsets;     // exclusive scan of counts (DS)
     uint32_t* ekeys;       // entries: global tile id (DS)
     uint32_t* evals;       // entries: point slot (DS)
     uint32_t* ekeys2;      // sorted (DS)
     uint32_t* evals2;      // the lists: point slots grouped by tile (K3DOM: placed, DS: sorted)
     uint32_t* tile_tally;  // T: rays per tile (K3DOM), zero between frames
-    uint32_t* block_base;  // [bin_blocks(N)][T]: each binning block's first slot in each tile's range,
+    uint32_t* block_base;  // [bin_blocks(kRayThreads N)][T]: each binning block's first slot in each tile's range,
                            // relative to the range's start (K3DOM)
     uint32_t* ekeys_alt;
     uint32_t* evals_alt;
@@ -163,7 +163,8 @@ long ray_entries_bound(const DevParams& p, const TileShape& ts, int max_points, 
 constexpr int kPlacedMaxTiles = 12288;
 inline bool placed_lists(bool ds, int T) { return !ds && T <= kPlacedMaxTiles; }
 constexpr int kBinBlocksMax = 1024;
-int bin_blocks(long n);  // blocks of the placed-list passes
+int bin_blocks(long n);  // blocks of the placed-list passes over n threads
+constexpr int kRayThreads = 2;  // threads per ray in the placed-list passes
 // Texture object over the S kernel tables (point sampling, FP32 as stored), for k_bgki.
 cudaError_t make_kernel_table_texture(RayBuffers& rb, int S);
 // Per-scene evidence constants (binning radius, cull radius, fixed-point scale); writes the
