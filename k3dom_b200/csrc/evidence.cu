@@ -173,8 +173,9 @@ struct RayPrep {
 
 // Per-ray constants. K3DOM: (m, d_m) and (m/d_m, margin), d_m and margin as the reference
 // forms them (mass_update.cu:29-31,55). DS: (m, |m|^2) as measurement_grid.cu:90.
+// consts = false: only ok and the segment's far end (K3DOM), for a second thread of the ray.
 __device__ __forceinline__ RayPrep prep_ray(const DevParams& p, const BinGeom& g, float mx, float my, float mz,
-                                           bool ds, float4* ra, double4* rc) {
+                                           bool ds, float4* ra, double4* rc, bool consts = true) {
     RayPrep r;
     r.ok = isfinite(mx) && isfinite(my) && isfinite(mz);
     r.bx = r.by = r.bz = 0.0f;
@@ -182,7 +183,11 @@ __device__ __forceinline__ RayPrep prep_ray(const DevParams& p, const BinGeom& g
     *rc = make_double4(0.0, 0.0, 0.0, 0.0);
     if (!r.ok) return r;
     const float sq = __fadd_rn(__fadd_rn(__fmul_rn(mx, mx), __fmul_rn(my, my)), __fmul_rn(mz, mz));
-    if (!ds) {
+    if (!ds && !consts) {
+        r.bx = g.ax + mx / p.res;
+        r.by = g.ay + my / p.res;
+        r.bz = g.az + mz / p.res;
+    } else if (!ds) {
         // d_m and the margin point (mass_update.cu:29-31,55) in FP64; a zero-length ray gets
         // 1/d_m = 0, which turns its free evidence off as the reference's NaN comparisons do
         const double dmd = sqrt((double)mx * mx + (double)my * my + (double)mz * mz);
@@ -258,7 +263,7 @@ __global__ void k_ray_count(Batch bt, const float* __restrict__ xs, const float*
         if (f.has_transform) apply_transform(f, &mx, &my, &mz);
         float4 a;
         double4 cc;
-        const RayPrep r = prep_ray(sd.p, g, mx, my, mz, ds != 0, &a, &cc);
+        const RayPrep r = prep_ray(sd.p, g, mx, my, mz, ds != 0, &a, &cc, half == 0);
         if (half == 0) {
             ra[i] = a;
             rc[i] = cc;
