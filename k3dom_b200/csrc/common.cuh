@@ -112,7 +112,7 @@ struct DevStatus {
     unsigned int nonfinite_frame;  // points skipped as non-finite in the last frame's binning
     unsigned long long kernel_evals;  // in-support sparse-kernel evaluations of the last frame
     unsigned int sort_timeout;        // a bounded look-back wait of the particle sort gave up
-    unsigned int pad_;
+    unsigned int copy_timeout;        // a bounded wait for a bulk copy gave up (its cells skipped)
 };
 
 // Particle set, SoA (ParticlesSoA, include/common/dom_types.h:76-167; post_weight is

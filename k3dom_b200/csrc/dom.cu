@@ -1193,10 +1193,11 @@ static k3dom_status finish_sync(k3dom_handle* h) {
     if (h->status) e = cudaMemcpyAsync(h->status_host, h->status, sizeof(DevStatus), cudaMemcpyDeviceToHost, h->st);
     if (e == cudaSuccess) e = cudaStreamSynchronize(h->st);
     if (e != cudaSuccess) return h->fail(e);
-    if (h->status && h->status_host->sort_timeout) {
-        // the particle sort's look-back gave up (its output is incomplete): report it once
-        h->status_host->sort_timeout = 0;
-        e = cudaMemsetAsync(&h->status->sort_timeout, 0, sizeof(unsigned int), h->st);
+    if (h->status && (h->status_host->sort_timeout || h->status_host->copy_timeout)) {
+        // a bounded device wait gave up (the particle sort's look-back, or a bulk copy of the
+        // cell update): its output is incomplete; report it once
+        h->status_host->sort_timeout = h->status_host->copy_timeout = 0;
+        e = cudaMemsetAsync(&h->status->sort_timeout, 0, 2 * sizeof(unsigned int), h->st);
         if (e == cudaSuccess) e = cudaStreamSynchronize(h->st);
         if (e != cudaSuccess) return h->fail(e);
         return K3DOM_ERR_TIMEOUT;

@@ -804,9 +804,9 @@ __device__ __forceinline__ CellIn load_cell_in(const CellState& cs, const CellWo
     return in;
 }
 
-__device__ void k3dom_cell_update(const DevParams& p, double g, int c, double del_occ, double del_free,
-                                  CellState cs, CellWork cw, bool first_frame) {
-    const CellIn in = load_cell_in(cs, cw, c, first_frame);
+// The update of cell c from its inputs `in` (outputs written to cs, cw).
+__device__ void k3dom_cell_update_in(const DevParams& p, double g, int c, double del_occ, double del_free,
+                                     const CellIn& in, CellState cs, CellWork cw, bool first_frame) {
     double m_f = in.m_f, m_s = in.m_s, m_d = in.m_d;
     const int start = in.start;
     const bool has = start >= 0;
@@ -874,6 +874,11 @@ __device__ void k3dom_cell_update(const DevParams& p, double g, int c, double de
     cs.mvx[c] = (float)vx;
     cs.mvy[c] = (float)vy;
     cs.mvz[c] = (float)vz;
+}
+
+__device__ __forceinline__ void k3dom_cell_update(const DevParams& p, double g, int c, double del_occ,
+                                                  double del_free, CellState cs, CellWork cw, bool first_frame) {
+    k3dom_cell_update_in(p, g, c, del_occ, del_free, load_cell_in(cs, cw, c, first_frame), cs, cw, first_frame);
 }
 
 // Shared memory of k_bgki: one chunk of rays and a per-warp staging area for the FP64
@@ -1961,6 +1966,118 @@ __global__ void __launch_bounds__(kBlock) k_k3dom_update_cells(EvArgs A) {
     }
 }
 
+// The same pass with each CTA's inputs brought into shared memory by bulk copies: the pass is
+// latency bound on its per-cell reads, and one cp.async.bulk per input array (8 arrays of 1,024
+// cells and the fixed-point sums, 48 KB per CTA, completed on one mbarrier) puts all of a CTA's
+// bytes in flight at once without holding them in registers. The copies are plain (no cluster
+// multicast) and read this GPU's own memory. Every array base is 16-byte aligned (checked by the
+// launcher) and a full tile starts at a multiple of 4 KB, as the copies require; the last, partial
+// tile reads its cells directly. The wait is bounded: when it runs out the CTA records
+// copy_timeout, waits (bounded again) for its copies to land, and skips its cells.
+constexpr int kUcCells = 1024;
+constexpr int kUcThreads = 256;
+constexpr uint32_t kUcMaxPolls = 1u << 22;
+constexpr size_t kUcSmem = 8 * sizeof(float) * kUcCells + sizeof(ulonglong2) * kUcCells;
+
+__device__ __forceinline__ uint32_t smem_addr(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ void bulk_load(void* dst, const void* src, uint32_t bytes, uint64_t* bar) {
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];"
+                 :
+                 : "r"(smem_addr(dst)), "l"(src), "r"(bytes), "r"(smem_addr(bar))
+                 : "memory");
+}
+
+// Polls the barrier's phase 0 at most max_polls times; true once it has completed.
+__device__ __forceinline__ bool bar_wait(uint64_t* bar, uint32_t max_polls) {
+    for (uint32_t it = 0; it < max_polls; ++it) {
+        uint32_t done;
+        asm volatile(
+            "{\n\t.reg .pred p;\n\t"
+            "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], 0;\n\t"
+            "selp.u32 %0, 1, 0, p;\n\t}"
+            : "=r"(done)
+            : "r"(smem_addr(bar))
+            : "memory");
+        if (done) return true;
+    }
+    return false;
+}
+
+__global__ void __launch_bounds__(kUcThreads) k_k3dom_update_cells_bulk(EvArgs A) {
+    extern __shared__ __align__(16) unsigned char uc_smem[];
+    __shared__ __align__(8) uint64_t bar;
+    const Batch& bt = A.bt;
+    ulonglong2* acc = reinterpret_cast<ulonglong2*>(A.acc);
+    const long c0 = (long)blockIdx.x * kUcCells;
+    const int n = (int)min((long)kUcCells, (long)bt.C - c0);
+    const bool first = A.first_frame != 0;
+    if (n < kUcCells) {  // the partial last tile: direct reads (the same update)
+        for (int i = threadIdx.x; i < n; i += kUcThreads) {
+            const int c = (int)(c0 + i);
+            const int sc = scene_of(bt.off->cell, bt.S, c);
+            const SceneDev& sd = bt.sc[sc];
+            const ulonglong2 v = acc[c];
+            if (v.x || v.y) acc[c] = make_ulonglong2(0ull, 0ull);
+            k3dom_cell_update(sd.p, bt.fp[sc].gamma_dt, c, (double)(long long)v.x * sd.fx_inv,
+                              (double)(long long)v.y * sd.fx_inv, A.cs, A.cw, first);
+        }
+        return;
+    }
+    float* s_f = reinterpret_cast<float*>(uc_smem);
+    float* s_s = s_f + kUcCells;
+    float* s_d = s_s + kUcCells;
+    int* s_start = reinterpret_cast<int*>(s_d + kUcCells);
+    float* s_w = reinterpret_cast<float*>(s_start + kUcCells);
+    float* s_vx = s_w + kUcCells;
+    float* s_vy = s_vx + kUcCells;
+    float* s_vz = s_vy + kUcCells;
+    ulonglong2* s_acc = reinterpret_cast<ulonglong2*>(s_vz + kUcCells);
+    if (threadIdx.x == 0) {
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_addr(&bar)) : "memory");
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        constexpr uint32_t fb = sizeof(float) * kUcCells;
+        constexpr uint32_t total = 8 * fb + sizeof(ulonglong2) * kUcCells;
+        asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_addr(&bar)), "r"(total)
+                     : "memory");
+        bulk_load(s_f, A.cs.free_m + c0, fb, &bar);
+        bulk_load(s_s, A.cs.static_m + c0, fb, &bar);
+        bulk_load(s_d, A.cs.dyn_m + c0, fb, &bar);
+        bulk_load(s_start, A.cw.start + c0, fb, &bar);
+        bulk_load(s_w, A.cw.sum_w + c0, fb, &bar);
+        bulk_load(s_vx, A.cw.sum_wvx + c0, fb, &bar);
+        bulk_load(s_vy, A.cw.sum_wvy + c0, fb, &bar);
+        bulk_load(s_vz, A.cw.sum_wvz + c0, fb, &bar);
+        bulk_load(s_acc, acc + c0, sizeof(ulonglong2) * kUcCells, &bar);
+    }
+    if (!bar_wait(&bar, kUcMaxPolls)) {
+        if (threadIdx.x == 0) atomicOr(&A.status->copy_timeout, 1u);
+        bar_wait(&bar, kUcMaxPolls);  // the copies still write this CTA's shared memory
+        return;
+    }
+    for (int i = threadIdx.x; i < kUcCells; i += kUcThreads) {
+        const int c = (int)(c0 + i);
+        const int sc = scene_of(bt.off->cell, bt.S, c);
+        const SceneDev& sd = bt.sc[sc];
+        const ulonglong2 v = s_acc[i];
+        if (v.x || v.y) acc[c] = make_ulonglong2(0ull, 0ull);
+        CellIn in;
+        in.m_f = s_f[i];
+        in.m_s = s_s[i];
+        in.m_d = s_d[i];
+        in.start = first ? -1 : s_start[i];
+        in.sum_w = s_w[i];
+        in.wvx = s_vx[i];
+        in.wvy = s_vy[i];
+        in.wvz = s_vz[i];
+        k3dom_cell_update_in(sd.p, bt.fp[sc].gamma_dt, c, (double)(long long)v.x * sd.fx_inv,
+                             (double)(long long)v.y * sd.fx_inv, in, A.cs, A.cw, first);
+    }
+}
+
 cudaError_t make_kernel_table_texture(RayBuffers& rb, int S) {
     rb.ktex = 0;
     cudaResourceDesc rd = {};
@@ -1979,6 +2096,15 @@ cudaError_t launch_k3dom_update_cells(const Batch& bt, RayBuffers& rb, CellState
                                       cudaStream_t st) {
     const EvArgs A = make_args(bt, rb, cs, cw, false, status);
     ++g_launches;
+    const uintptr_t bases = reinterpret_cast<uintptr_t>(cs.free_m) | reinterpret_cast<uintptr_t>(cs.static_m) |
+                            reinterpret_cast<uintptr_t>(cs.dyn_m) | reinterpret_cast<uintptr_t>(cw.start) |
+                            reinterpret_cast<uintptr_t>(cw.sum_w) | reinterpret_cast<uintptr_t>(cw.sum_wvx) |
+                            reinterpret_cast<uintptr_t>(cw.sum_wvy) | reinterpret_cast<uintptr_t>(cw.sum_wvz) |
+                            reinterpret_cast<uintptr_t>(rb.acc);
+    if ((bases & 15u) == 0) {  // the bulk copies' alignment (cudaMalloc gives 256 bytes)
+        k_k3dom_update_cells_bulk<<<div_up(bt.C, kUcCells), kUcThreads, kUcSmem, st>>>(A);
+        return cudaGetLastError();
+    }
     // one thread per cell: the update is latency bound, so every cell's reads are in flight at once
     k_k3dom_update_cells<<<div_up(bt.C, kBlock), kBlock, 0, st>>>(A);
     return cudaGetLastError();
@@ -2032,8 +2158,12 @@ cudaError_t evidence_init() {
     if ((e = cudaFuncSetAttribute(k_bgki_sums<3>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                   (int)calib_smem_bytes(kChunk))))
         return e;
-    return cudaFuncSetAttribute(k_bgki_sums<4, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                (int)calib_smem_bytes(kCalibChunk, true));
+    if ((e = cudaFuncSetAttribute(k_bgki_sums<4, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)calib_smem_bytes(kCalibChunk, true))))
+        return e;
+    // 48 KB of copies plus the static barrier: above the default per-CTA limit
+    return cudaFuncSetAttribute(k_k3dom_update_cells_bulk, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)kUcSmem);
 }
 
 }  // namespace k3dom
