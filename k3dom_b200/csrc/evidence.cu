@@ -1969,8 +1969,8 @@ __global__ void __launch_bounds__(kBlock) k_k3dom_update_cells(EvArgs A) {
 // The same pass with each CTA's inputs brought into shared memory by bulk copies: the pass is
 // latency bound on its per-cell reads, and one cp.async.bulk per input array (8 arrays of 1,024
 // cells and the fixed-point sums, 48 KB per CTA, completed on one mbarrier) puts all of a CTA's
-// bytes in flight at once without holding them in registers. The copies are plain (no cluster
-// multicast) and read this GPU's own memory. Every array base is 16-byte aligned (checked by the
+// bytes in flight at once without holding them in registers. Each copy is a plain one-CTA copy of
+// this GPU's own memory. Every array base is 16-byte aligned (checked by the
 // launcher) and a full tile starts at a multiple of 4 KB, as the copies require; the last, partial
 // tile reads its cells directly. The wait is bounded: when it runs out the CTA records
 // copy_timeout, waits (bounded again) for its copies to land, and skips its cells.
