@@ -4,7 +4,10 @@ dominant axis, and each candidate tile's cell-centre box grown by R is tested ag
 segment in FP32. The placed ray lists give each ray two threads, one per alternate slab
 (first = 0, 1; step = 2). This restates the walk and checks, against brute force, that every
 tile holding a cell centre within R of the segment is visited, and that the two threads'
-walks split the full walk with nothing missed or repeated. CPU only."""
+walks split the full walk with nothing missed or repeated, and that no walk exceeds the per-ray
+bound the lists are sized by. CPU only."""
+import math
+
 import numpy as np
 
 f32 = np.float32
@@ -99,3 +102,40 @@ def test_walk_covers_support_and_halves_split_it():
         assert need <= set(full), f"ray {r}: tiles within R not visited: {sorted(need - set(full))[:5]}"
         checked += len(need)
     assert checked > 500
+
+
+def entries_bound(R, G, Gz, ts):
+    """Tiles one ray can reach at most: the per-ray factor of the list capacity
+    (evidence.cu: ray_entries_bound, restated)."""
+    Rb = float(R) + 0.01
+    nt = [G // ts[0], G // ts[1], Gz // ts[2]]
+    worst = 0
+    for A in range(3):
+        per_slab = 1
+        for k in (1, 2):
+            o = (A + k) % 3
+            per_slab *= min(math.ceil((ts[A] + 4.0 * Rb) / ts[o]) + 1, nt[o])
+        worst = max(worst, per_slab * nt[A])
+    return min(worst, nt[0] * nt[1] * nt[2])
+
+
+def test_walk_stays_within_the_list_capacity():
+    """The ray lists are sized by a per-ray bound on the tiles a walk visits (times the point
+    slots); no ray's walk may exceed it, whatever its direction and length, for each tile shape."""
+    rng = np.random.default_rng(11)
+    G, Gz = 64, 32
+    R = f32(0.3 / 0.1 * (1 + 1e-4) + 1e-3)
+    for ts in ((16, 16, 4), (16, 16, 8), (8, 8, 4)):
+        bound = entries_bound(R, G, Gz, ts)
+        worst = 0
+        for r in range(150):
+            a = rng.uniform([0, 0, 0], [G, G, Gz]).astype(np.float32)
+            u = rng.normal(size=3)
+            u /= np.linalg.norm(u)
+            if r % 5 == 0:  # along an axis or a diagonal of the grid
+                u = np.eye(3)[r % 3] if r % 2 else np.array([1.0, 1.0, 0.5]) / 1.5
+            b = (a + u * rng.uniform(1, 2 * G)).astype(np.float32)
+            n = len(walk([f32(v) for v in a], [f32(v) for v in b], R, G, Gz, ts))
+            worst = max(worst, n)
+            assert n <= bound, (ts, r, n, bound)
+        assert worst > 0
